@@ -1,0 +1,106 @@
+/*
+ * qs_oracle.h — CPU oracle of the quasi-static xi-layer loop (TEST
+ * INFRASTRUCTURE ONLY: the checker the GPU path is compared against; never
+ * part of the product path).
+ *
+ * A plain FP64 C++ restatement of the reference's live host path:
+ *   movepart_splitlayer.cpp:25-1711   (march, layer, plasma push, deposit,
+ *                                      guard exchange)
+ *   movefieldshydrolinlayersplit.cpp:222-1671 (Guess / Iterate spectral solve)
+ *   movebeam.cpp:14-774               (beam push + 3-D CIC deposit)
+ * with its own half-integer transforms implementing the FFTW REDFT11 /
+ * RODFT11 definitions (FFTW 3 is a system library of the reference, not
+ * vendored, version unpinned).
+ *
+ * Parity status: the transforms are pinned against scipy.fft dct/dst type 4
+ * (the same published definitions) and direct O(N^2) sums; the push, solver
+ * and beam are pinned by known-answer tests derived from the reference
+ * formulas.  The reference itself cannot be built here (it needs FFTW3,
+ * HDF5 and MPI), so no reference outputs pin them: parity unpinned for the
+ * push/solver/beam beyond those known-answer tests.
+ */
+#ifndef QS_ORACLE_H
+#define QS_ORACLE_H
+
+#include <stdint.h>
+#include "../include/qsb200.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct qso qso;
+
+void qso_set_threads(int n);
+int qso_get_threads(void);
+
+int qso_create(const qs_config* cfg, qso** out);
+void qso_destroy(qso* o);
+
+int qso_load_beam(qso* o, int64_t n, const int32_t* i, const int32_t* j,
+                  const int32_t* k, const double* x, const double* y,
+                  const double* z, const double* px, const double* py,
+                  const double* pz, const double* w);
+int qso_get_beam(qso* o, int64_t n, int32_t* i, int32_t* j, int32_t* k,
+                 double* x, double* y, double* z, double* px, double* py,
+                 double* pz, double* w);
+int64_t qso_beam_count(const qso* o);
+
+int qso_load_front_plasma(qso* o, int64_t n, const int32_t* cell,
+                          const double* y, const double* z, const double* px,
+                          const double* py, const double* pz, const double* w);
+int64_t qso_plasma_count(const qso* o);
+/* Particles of the layer in flight, reported in the order they were loaded
+ * (particle id order), with their current cell. */
+int qso_get_plasma(qso* o, int64_t n, int32_t* cell, double* y, double* z,
+                   double* px, double* py, double* pz, double* w);
+
+int qso_set_layer(qso* o, int which, int field, const double* data);
+int qso_get_layer(qso* o, int which, int field, double* out);
+int qso_get_field3d(qso* o, int field, int layer, double* out);
+int qso_set_beam_currents(qso* o, int field, int layer, const double* data);
+int qso_get_beam_currents(qso* o, int field, int layer, double* out);
+int qso_get_onaxis_ex(qso* o, double* out);
+
+int qso_step(qso* o);
+int qso_move_beam_particles(qso* o);
+int qso_move_all_split_layers(qso* o);
+int qso_begin_march(qso* o);
+int qso_layer_begin(qso* o, int iLayer, int iSplit);
+int qso_move_split_layer(qso* o, int iLayer, int iSplit);
+int qso_guess_fields(qso* o, int iLayer, int iSplit);
+int qso_move_particles_layer(qso* o, int iLayer, int iSplit, int iFullStep);
+int qso_iterate_fields(qso* o, int iLayer, int iSplit, int iter,
+                       double* rel_err);
+int qso_layer_end(qso* o, int iLayer, int iSplit);
+
+/* 1-D and 2-D half-integer transforms, unnormalised FFTW definitions.
+ * 2-D: nz x ny planes (y fastest), kind_z along z, kind_y along y.
+ * direct != 0 selects the O(N^2) sums instead of the FFT algorithm. */
+int qso_dtt1d(int n, int kind, const double* in, double* out, int direct);
+int qso_transform2d(int nz, int ny, int kind_z, int kind_y, int batch,
+                    const double* in, double* out, int direct);
+
+/* Kernel-level oracle of one plasma sub-push over a particle array
+ * (MoveParticlesLayerSplit + DepositCurrentsInCellSplit + the periodic fold
+ * of ExchangeCurrentsSplit).  P and C hold 6 interior planes each
+ * (Ex,Ey,Ez,Bx,By,Bz); dep holds 4 planes (Jx,Jy,Jz,Dens) that are ADDED to;
+ * dep_cell receives the cell (j + ny*k, folded) of each particle's last
+ * deposit; on full != 0 the particle state is updated in place (and in CIC
+ * mode cell[] too).  The f32 variant runs the same arithmetic in float;
+ * precise != 0 selects the cell-relative position update (the FP32 path's
+ * form) instead of the reference's ytmp + j form. */
+int qso_push_layer_f64(const qs_config* cfg, int64_t n, int32_t* cell,
+                       double* y, double* z, double* px, double* py,
+                       double* pz, const double* w, const double* P,
+                       const double* C, double* dep, int32_t* dep_cell,
+                       int full, int precise);
+int qso_push_layer_f32(const qs_config* cfg, int64_t n, int32_t* cell,
+                       float* y, float* z, float* px, float* py, float* pz,
+                       const float* w, const float* P, const float* C,
+                       float* dep, int32_t* dep_cell, int full, int precise);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
