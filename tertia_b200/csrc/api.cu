@@ -1,0 +1,1173 @@
+// api.cu — the C ABI of include/qsb200.h and the engine that runs the
+// quasi-static xi-march on one GPU.
+//
+// Data layout in HBM (T = float, or double in QS_PREC_FP64):
+//   f3   : (nx+1) layers x 6 planes (Ex,Ey,Ez,Bx,By,Bz)    Mesh::p_CellArray fields
+//   b3   : (nx+1) layers x 2 planes (RhoBeam, JxBeam)      beam currents
+//   src3 : (nx+1) layers x 4 planes (Jx,Jy,Jz,Dens)        only with store_sources
+//   P / C layer fields alias f3 during the march: C of the last split of layer
+//   i is f3[i] and P of layer i is f3[i+1], so the reference's copies
+//   P <- Array[i+1], P <- C, Array[i] <- P (movepart_splitlayer.cpp:170-187,
+//   423-428, 467-473) cost nothing.
+//   Spectral state: two banks of 12 planes [Rho,Ex,Ey,Ez,Bx,By,Bz,Jx,Jy,Jz,
+//   Rb,Jxb]; the bank of the previous (layer, split) is the P state
+//   (RhoP, E*P, J*P, RhoBeamP), swapped at every layer end.
+//   Plasma particles: SoA grouped by cell; beam particles: SoA, FP64.
+// A plane is ny*nz values, index j + ny*k.
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "qs_common.cuh"
+#include "qs_internal.h"
+#include "dtt_tc.h"
+
+namespace qs {
+
+static thread_local std::string g_create_error;
+
+struct EngineBase {
+    qs_config cfg{};
+    int My = 0, Mz = 0, L = 0, S = 1, nIter = 1;
+    size_t plane = 0;
+    int dev = 0;
+    cudaStream_t st = nullptr;
+    int* d_err = nullptr;
+    std::string err;
+    int64_t launches = 0;
+    uint64_t step_count = 0;
+    double phase = 0;
+    virtual ~EngineBase() {}
+
+    qs_status fail(qs_status s, const char* fmt, ...) {
+        char buf[512];
+        va_list ap;
+        va_start(ap, fmt);
+        vsnprintf(buf, sizeof buf, fmt, ap);
+        va_end(ap);
+        err = buf;
+        return s;
+    }
+    qs_status cuda_fail(cudaError_t e, const char* what) {
+        return fail(e == cudaErrorMemoryAllocation ? QS_ERR_OOM : QS_ERR_CUDA, "%s: %s", what,
+                    cudaGetErrorString(e));
+    }
+
+    virtual qs_status init() = 0;
+    virtual qs_status load_beam(int64_t, const int32_t*, const int32_t*, const int32_t*,
+                                const double*, const double*, const double*, const double*,
+                                const double*, const double*, const double*) = 0;
+    virtual qs_status get_beam(int64_t, int32_t*, int32_t*, int32_t*, double*, double*, double*,
+                               double*, double*, double*, double*) = 0;
+    virtual int64_t beam_count() const = 0;
+    virtual qs_status load_front(int64_t, const int32_t*, const double*, const double*,
+                                 const double*, const double*, const double*, const double*) = 0;
+    virtual qs_status seed_front(uint64_t) = 0;
+    virtual int64_t plasma_count() const = 0;
+    virtual qs_status get_plasma(int64_t, int32_t*, double*, double*, double*, double*, double*,
+                                 double*) = 0;
+    virtual qs_status set_layer(int, int, const double*) = 0;
+    virtual qs_status get_layer(int, int, double*) = 0;
+    virtual qs_status get_field3d(int, int, double*) = 0;
+    virtual qs_status set_beam_currents(int, int, const double*) = 0;
+    virtual qs_status get_beam_currents(int, int, double*) = 0;
+    virtual qs_status get_onaxis(double*) = 0;
+    virtual qs_status move_beam() = 0;
+    virtual qs_status march() = 0;
+    virtual qs_status begin_march() = 0;
+    virtual qs_status layer_begin(int, int) = 0;
+    virtual qs_status move_split_layer(int, int) = 0;
+    virtual qs_status guess(int, int) = 0;
+    virtual qs_status push(int, int, int) = 0;
+    virtual qs_status iterate(int, int, int, double*) = 0;
+    virtual qs_status layer_end(int, int) = 0;
+    virtual qs_status transform2d(int, int, int, const double*, double*) = 0;
+    virtual qs_status transform2d_dev(int, int, int, const void*, void*) = 0;
+
+    qs_status check_device() {
+        cudaError_t e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) return cuda_fail(e, "stream synchronize");
+        int h = 0;
+        e = cudaMemcpy(&h, d_err, sizeof(int), cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) return cuda_fail(e, "error flag read");
+        if (h) {
+            cudaMemset(d_err, 0, sizeof(int));
+            if (h & DEV_ERR_BEAM_CURRENT)
+                return fail(QS_ERR_BEAM_CURRENT, "Too large beam current (|JxBeam| > 10)");
+            if (h & DEV_ERR_RANGE)
+                return fail(QS_ERR_PARTICLE_RANGE, "particle in-cell fraction outside [0,1]");
+            if (h & DEV_ERR_TIMEOUT) return fail(QS_ERR_TIMEOUT, "bounded device wait gave up");
+            return fail(QS_ERR_DEVICE, "device error flag 0x%x", h);
+        }
+        return QS_OK;
+    }
+};
+
+#define CK(x)                                              \
+    do {                                                   \
+        cudaError_t e_ = (x);                              \
+        if (e_ != cudaSuccess) return cuda_fail(e_, #x);   \
+    } while (0)
+
+// transform kinds
+constexpr int CC = QS_REDFT11, SS = QS_RODFT11;
+// spectral bank planes
+enum { SP_RHO = 0, SP_EX, SP_EY, SP_EZ, SP_BX, SP_BY, SP_BZ, SP_JX, SP_JY, SP_JZ, SP_RB, SP_JXB,
+       SP_N };
+
+template <class T>
+struct Engine : EngineBase {
+    bool tc = false;            // split-precision tensor-core transforms
+    int tc_mode = 0;
+    T* f3 = nullptr;
+    T* b3 = nullptr;
+    T* src3 = nullptr;
+    T* splitbuf = nullptr;      // 2 x 6 planes (NxSplit > 1 and stand-alone use)
+    T* srcbuf = nullptr;        // 2 x 4 planes (P and C sources)
+    T* Pf = nullptr;
+    T* Cf = nullptr;
+    T* Psrc = nullptr;
+    T* Csrc = nullptr;
+    T* Cbeam = nullptr;         // 2 planes
+    T* bank = nullptr;          // 2 x SP_N planes
+    int cur = 0;                // bank index of the current (layer, split)
+    bool p_valid = true;        // P-bank spectra match the P real planes
+    T* scratch = nullptr;       // transform intermediate, 8 planes
+    T* mats = nullptr;          // transform matrices
+    DttMats<T> my, mz;
+    TcTransformer* tcx = nullptr;
+    T* onaxis_d = nullptr;
+    T* stage = nullptr;         // conversion staging, 8 planes
+    double* stage_d = nullptr;  // double staging, 8 planes
+    // plasma
+    int64_t np = 0, np_cap = 0;
+    int32_t* pcell = nullptr;
+    T *py = nullptr, *pz = nullptr, *ppx = nullptr, *ppy = nullptr, *ppz = nullptr, *pw = nullptr;
+    bool front_pending = false;
+    // beam
+    int64_t nb = 0, nb_cap = 0;
+    int32_t *bi = nullptr, *bj = nullptr, *bk = nullptr;
+    double *bx = nullptr, *by = nullptr, *bz = nullptr, *bpx = nullptr, *bpy = nullptr,
+           *bpz = nullptr, *bw = nullptr;
+    // graph of the march
+    cudaGraphExec_t gexec = nullptr;
+    int64_t graph_kernels = 0;
+    bool capturing = false;
+    int64_t capture_count = 0;
+    struct HostState { T *Pf, *Cf, *Psrc, *Csrc; int cur; } graph_end{};
+    bool marched = false;
+
+    T* bankp(int b, int p) { return bank + ((size_t)b * SP_N + p) * plane; }
+    T* f3layer(int i) { return f3 + (size_t)i * 6 * plane; }
+
+    void count(int n) {
+        if (capturing) capture_count += n;
+        else launches += n;
+    }
+
+    ~Engine() override {
+        if (gexec) cudaGraphExecDestroy(gexec);
+        delete tcx;
+        void* ptrs[] = {f3, b3, src3, splitbuf, srcbuf, Cbeam, bank, scratch, mats, onaxis_d,
+                        stage, stage_d, pcell, py, pz, ppx, ppy, ppz, pw, bi, bj, bk, bx, by, bz,
+                        bpx, bpy, bpz, bw, d_err};
+        for (void* p : ptrs)
+            if (p) cudaFree(p);
+        if (st) cudaStreamDestroy(st);
+    }
+
+    template <class U>
+    qs_status alloc(U** p, size_t n, const char* what) {
+        cudaError_t e = cudaMalloc((void**)p, n * sizeof(U) + 16);
+        if (e != cudaSuccess) return cuda_fail(e, what);
+        return QS_OK;
+    }
+
+    qs_status init() override {
+        plane = (size_t)My * Mz;
+        CK(cudaSetDevice(dev));
+        CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+        qs_status s;
+        if ((s = alloc(&d_err, 1, "error flag"))) return s;
+        CK(cudaMemset(d_err, 0, sizeof(int)));
+        if ((s = alloc(&f3, (size_t)(L + 1) * 6 * plane, "field store"))) return s;
+        CK(cudaMemset(f3, 0, (size_t)(L + 1) * 6 * plane * sizeof(T)));
+        if ((s = alloc(&b3, (size_t)(L + 1) * 2 * plane, "beam current store"))) return s;
+        CK(cudaMemset(b3, 0, (size_t)(L + 1) * 2 * plane * sizeof(T)));
+        if (cfg.store_sources) {
+            if ((s = alloc(&src3, (size_t)(L + 1) * 4 * plane, "source store"))) return s;
+            CK(cudaMemset(src3, 0, (size_t)(L + 1) * 4 * plane * sizeof(T)));
+        }
+        if ((s = alloc(&splitbuf, 12 * plane, "split layers"))) return s;
+        CK(cudaMemset(splitbuf, 0, 12 * plane * sizeof(T)));
+        if ((s = alloc(&srcbuf, 8 * plane, "source layers"))) return s;
+        CK(cudaMemset(srcbuf, 0, 8 * plane * sizeof(T)));
+        if ((s = alloc(&Cbeam, 2 * plane, "beam layer"))) return s;
+        CK(cudaMemset(Cbeam, 0, 2 * plane * sizeof(T)));
+        if ((s = alloc(&bank, 2 * SP_N * plane, "spectral banks"))) return s;
+        CK(cudaMemset(bank, 0, 2 * SP_N * plane * sizeof(T)));
+        if ((s = alloc(&scratch, 8 * plane, "transform scratch"))) return s;
+        if ((s = alloc(&stage, 8 * plane, "staging"))) return s;
+        if ((s = alloc(&stage_d, 8 * plane, "staging"))) return s;
+        if ((s = alloc(&onaxis_d, (size_t)L, "on-axis"))) return s;
+        CK(cudaMemset(onaxis_d, 0, L * sizeof(T)));
+        // transform matrices 2 cos / 2 sin (pi (j+1/2)(k+1/2)/n); the angle is
+        // reduced exactly in integers: (2j+1)(2k+1) mod 8n in units of pi/(4n)
+        const size_t ny2 = (size_t)My * My, nz2 = (size_t)Mz * Mz;
+        if ((s = alloc(&mats, 2 * ny2 + 2 * nz2, "transform matrices"))) return s;
+        std::vector<T> hm(2 * ny2 + 2 * nz2);
+        auto fill = [&](T* out, int n, int kind) {
+            for (int k = 0; k < n; k++)
+                for (int j = 0; j < n; j++) {
+                    long long q = ((long long)(2 * j + 1) * (2 * k + 1)) % (8LL * n);
+                    double a = M_PI * (double)q / (4.0 * n);
+                    out[(size_t)k * n + j] = (T)(2.0 * (kind == CC ? std::cos(a) : std::sin(a)));
+                }
+        };
+        fill(hm.data(), My, CC);
+        fill(hm.data() + ny2, My, SS);
+        fill(hm.data() + 2 * ny2, Mz, CC);
+        fill(hm.data() + 2 * ny2 + nz2, Mz, SS);
+        CK(cudaMemcpy(mats, hm.data(), hm.size() * sizeof(T), cudaMemcpyHostToDevice));
+        my.m[CC] = mats;
+        my.m[SS] = mats + ny2;
+        mz.m[CC] = mats + 2 * ny2;
+        mz.m[SS] = mats + 2 * ny2 + nz2;
+        if (tc) {
+            std::string msg;
+            tcx = TcTransformer::create(tc_mode, My, Mz, st, msg);
+            if (!tcx) return fail(QS_ERR_UNSUPPORTED, "tensor-core transform: %s", msg.c_str());
+        }
+        Pf = splitbuf;
+        Cf = splitbuf + 6 * plane;
+        Psrc = srcbuf;
+        Csrc = srcbuf + 4 * plane;
+        cur = 0;
+        CK(cudaStreamSynchronize(st));
+        return QS_OK;
+    }
+
+    // ---------------------------------------------------------- transforms
+    void xform(const DttJob<T>& job) {
+        if (tc) {
+            count(tcx->run(job.nf, (const void* const*)job.in, (void* const*)job.out, job.kz,
+                           job.ky, (double)job.scale, sizeof(T), st));
+        } else {
+            count(run_dtt_simt<T>(job, My, Mz, my, mz, scratch, st));
+        }
+    }
+
+    DttJob<T> job_stack(const T* in_stack, int nf, T* const* outs, const int* kz, const int* ky,
+                        T scale) {
+        DttJob<T> j;
+        j.nf = nf;
+        for (int f = 0; f < nf; f++) {
+            j.in[f] = in_stack + (size_t)f * plane;
+            j.out[f] = outs[f];
+            j.kz[f] = kz[f];
+            j.ky[f] = ky[f];
+        }
+        j.scale = scale;
+        return j;
+    }
+
+    T inv_scale() const { return (T)(1.0 / (4.0 * (double)My * (double)Mz)); }
+
+    // ------------------------------------------------------------ particles
+    qs_status ensure_plasma(int64_t n) {
+        if (n <= np_cap) return QS_OK;
+        void* old[] = {pcell, py, pz, ppx, ppy, ppz, pw};
+        for (void* p : old)
+            if (p) cudaFree(p);
+        qs_status s;
+        if ((s = alloc(&pcell, n, "plasma"))) return s;
+        if ((s = alloc(&py, n, "plasma"))) return s;
+        if ((s = alloc(&pz, n, "plasma"))) return s;
+        if ((s = alloc(&ppx, n, "plasma"))) return s;
+        if ((s = alloc(&ppy, n, "plasma"))) return s;
+        if ((s = alloc(&ppz, n, "plasma"))) return s;
+        if ((s = alloc(&pw, n, "plasma"))) return s;
+        np_cap = n;
+        if (gexec) {  // the captured march baked the old pointers
+            cudaGraphExecDestroy(gexec);
+            gexec = nullptr;
+        }
+        return QS_OK;
+    }
+
+    qs_status ensure_beam(int64_t n) {
+        if (n <= nb_cap) return QS_OK;
+        void* old[] = {bi, bj, bk, bx, by, bz, bpx, bpy, bpz, bw};
+        for (void* p : old)
+            if (p) cudaFree(p);
+        qs_status s;
+        if ((s = alloc(&bi, n, "beam"))) return s;
+        if ((s = alloc(&bj, n, "beam"))) return s;
+        if ((s = alloc(&bk, n, "beam"))) return s;
+        if ((s = alloc(&bx, n, "beam"))) return s;
+        if ((s = alloc(&by, n, "beam"))) return s;
+        if ((s = alloc(&bz, n, "beam"))) return s;
+        if ((s = alloc(&bpx, n, "beam"))) return s;
+        if ((s = alloc(&bpy, n, "beam"))) return s;
+        if ((s = alloc(&bpz, n, "beam"))) return s;
+        if ((s = alloc(&bw, n, "beam"))) return s;
+        nb_cap = n;
+        return QS_OK;
+    }
+
+    qs_status load_beam(int64_t n, const int32_t* i, const int32_t* j, const int32_t* k,
+                        const double* x, const double* y, const double* z, const double* px,
+                        const double* py_, const double* pz_, const double* w) override {
+        if (n < 0 || (n > 0 && (!i || !j || !k || !x || !y || !z || !px || !py_ || !pz_ || !w)))
+            return fail(QS_ERR_INVALID, "qs_load_beam: bad arguments");
+        qs_status s = ensure_beam(n);
+        if (s) return s;
+        nb = n;
+        if (!n) return QS_OK;
+        CK(cudaMemcpyAsync(bi, i, n * 4, cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(bj, j, n * 4, cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(bk, k, n * 4, cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(bx, x, n * 8, cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(by, y, n * 8, cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(bz, z, n * 8, cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(bpx, px, n * 8, cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(bpy, py_, n * 8, cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(bpz, pz_, n * 8, cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(bw, w, n * 8, cudaMemcpyHostToDevice, st));
+        CK(cudaStreamSynchronize(st));
+        return QS_OK;
+    }
+
+    qs_status get_beam(int64_t n, int32_t* i, int32_t* j, int32_t* k, double* x, double* y,
+                       double* z, double* px, double* py_, double* pz_, double* w) override {
+        if (n != nb) return fail(QS_ERR_INVALID, "qs_get_beam: n=%lld, beam has %lld",
+                                 (long long)n, (long long)nb);
+        if (!n) return QS_OK;
+        struct { void* h; const void* d; size_t sz; } c[] = {
+            {i, bi, 4}, {j, bj, 4}, {k, bk, 4}, {x, bx, 8}, {y, by, 8}, {z, bz, 8},
+            {px, bpx, 8}, {py_, bpy, 8}, {pz_, bpz, 8}, {w, bw, 8}};
+        for (auto& e : c)
+            if (e.h) CK(cudaMemcpyAsync(e.h, e.d, n * e.sz, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        return QS_OK;
+    }
+    int64_t beam_count() const override { return nb; }
+
+    qs_status load_front(int64_t n, const int32_t* cell, const double* y, const double* z,
+                         const double* px, const double* py_, const double* pz_,
+                         const double* w) override {
+        if (n < 0 || (n > 0 && (!cell || !y || !z || !px || !py_ || !pz_ || !w)))
+            return fail(QS_ERR_INVALID, "qs_load_front_plasma: bad arguments");
+        int32_t prev = -1;
+        for (int64_t p = 0; p < n; p++) {
+            if (cell[p] < 0 || (size_t)cell[p] >= plane || cell[p] < prev)
+                return fail(QS_ERR_INVALID, "qs_load_front_plasma: cells must be grouped in "
+                                            "ascending order within [0, ny*nz)");
+            prev = cell[p];
+        }
+        qs_status s = ensure_plasma(n);
+        if (s) return s;
+        np = n;
+        if (n) {
+            CK(cudaMemcpyAsync(pcell, cell, n * 4, cudaMemcpyHostToDevice, st));
+            const double* src[6] = {y, z, px, py_, pz_, w};
+            T* dst[6] = {py, pz, ppx, ppy, ppz, pw};
+            for (int c = 0; c < 6; c++) {
+                // stage through stage_d in chunks of 8 planes
+                size_t chunk = 8 * plane;
+                for (int64_t o = 0; o < n; o += (int64_t)chunk) {
+                    size_t m = (size_t)std::min<int64_t>((int64_t)chunk, n - o);
+                    CK(cudaMemcpyAsync(stage_d, src[c] + o, m * 8, cudaMemcpyHostToDevice, st));
+                    count(launch_convert<T>(stage_d, 1, dst[c] + o, m, st));
+                }
+            }
+            CK(cudaStreamSynchronize(st));
+        }
+        front_pending = true;
+        return QS_OK;
+    }
+
+    qs_status seed_front(uint64_t step) override {
+        const int ppc = cfg.ppc;
+        if (ppc < 1 || ppc > 16) return fail(QS_ERR_INVALID, "ppc must be in [1,16]");
+        qs_status s = ensure_plasma((int64_t)plane * ppc);
+        if (s) return s;
+        np = (int64_t)plane * ppc;
+        // in-cell lattice of Mesh::SeedParticles (mesh.cpp:436-470), head first
+        double oy[16], oz[16];
+        int iside = (int)(std::pow((double)(ppc - 1), 0.5) + 1.0);
+        for (int is = 0; is < ppc; is++) {
+            double y, z;
+            if (ppc == 1 || ppc == 2 || ppc == 3) {
+                y = z = 0.5;
+            } else if (ppc == 4) {
+                y = 1. / 3. * (1. + is % 2);
+                z = 1. / 3. * (1. + is / 2);
+            } else {
+                int iz = is / iside, iy = is - iside * iz;
+                y = 1. / iside * (iy + .5);
+                z = 1. / iside * (iz + .5);
+            }
+            oy[is] = y;
+            oz[is] = z;
+        }
+        const double weight = cfg.plasma_density / ppc;   // Specie::GetWeight()*dens
+        count(launch_seed_front<T>(My, Mz, ppc, oy, oz, cfg.plasma_px0, cfg.plasma_py0,
+                                   cfg.plasma_pz0, cfg.pspread_x, cfg.pspread_y, cfg.pspread_z,
+                                   weight, cfg.seed, step, pcell, py, pz, ppx, ppy, ppz, pw, st));
+        CK(cudaGetLastError());
+        front_pending = true;
+        return QS_OK;
+    }
+
+    int64_t plasma_count() const override { return np; }
+
+    qs_status get_plasma(int64_t n, int32_t* cell, double* y, double* z, double* px,
+                         double* py_, double* pz_, double* w) override {
+        if (n != np) return fail(QS_ERR_INVALID, "qs_get_plasma: n mismatch");
+        if (!n) return QS_OK;
+        if (cell) CK(cudaMemcpyAsync(cell, pcell, n * 4, cudaMemcpyDeviceToHost, st));
+        double* dst[6] = {y, z, px, py_, pz_, w};
+        T* src[6] = {py, pz, ppx, ppy, ppz, pw};
+        for (int c = 0; c < 6; c++) {
+            if (!dst[c]) continue;
+            size_t chunk = 8 * plane;
+            for (int64_t o = 0; o < n; o += (int64_t)chunk) {
+                size_t m = (size_t)std::min<int64_t>((int64_t)chunk, n - o);
+                count(launch_convert_back<T>(src[c] + o, stage_d, m, st));
+                CK(cudaMemcpyAsync(dst[c] + o, stage_d, m * 8, cudaMemcpyDeviceToHost, st));
+                CK(cudaStreamSynchronize(st));
+            }
+        }
+        CK(cudaStreamSynchronize(st));
+        return QS_OK;
+    }
+
+    // --------------------------------------------------------- plane I/O
+    qs_status put_plane(T* dst, const double* src) {
+        CK(cudaMemcpyAsync(stage_d, src, plane * 8, cudaMemcpyHostToDevice, st));
+        count(launch_convert<T>(stage_d, 1, dst, plane, st));
+        CK(cudaStreamSynchronize(st));
+        return QS_OK;
+    }
+    qs_status get_plane(const T* src, double* dst) {
+        count(launch_convert_back<T>(src, stage_d, plane, st));
+        CK(cudaMemcpyAsync(dst, stage_d, plane * 8, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        return QS_OK;
+    }
+
+    T* layer_plane(int which, int field) {
+        T* F = which == QS_LAYER_P ? Pf : Cf;
+        T* Sr = which == QS_LAYER_P ? Psrc : Csrc;
+        if (field >= QS_F_EX && field <= QS_F_BZ) return F + (size_t)field * plane;
+        if (field >= QS_F_JX && field <= QS_F_JZ) return Sr + (size_t)(field - QS_F_JX) * plane;
+        if (field == QS_F_DENS) return Sr + 3 * plane;
+        if (which == QS_LAYER_C && field == QS_F_RHOBEAM) return Cbeam;
+        if (which == QS_LAYER_C && field == QS_F_JXBEAM) return Cbeam + plane;
+        return nullptr;
+    }
+
+    qs_status set_layer(int which, int field, const double* data) override {
+        if ((which != QS_LAYER_P && which != QS_LAYER_C) || !data)
+            return fail(QS_ERR_INVALID, "qs_set_layer: bad arguments");
+        T* p = layer_plane(which, field);
+        if (!p) return fail(QS_ERR_INVALID, "qs_set_layer: field %d not settable", field);
+        if (which == QS_LAYER_P) p_valid = false;
+        return put_plane(p, data);
+    }
+
+    qs_status get_layer(int which, int field, double* out) override {
+        if ((which != QS_LAYER_P && which != QS_LAYER_C) || !out)
+            return fail(QS_ERR_INVALID, "qs_get_layer: bad arguments");
+        T* p = layer_plane(which, field);
+        if (!p) return fail(QS_ERR_INVALID, "qs_get_layer: field %d not readable", field);
+        return get_plane(p, out);
+    }
+
+    qs_status get_field3d(int field, int layer, double* out) override {
+        if (!out || layer < 0 || layer > L) return fail(QS_ERR_INVALID, "qs_get_field3d: bad layer");
+        if (field >= QS_F_EX && field <= QS_F_BZ)
+            return get_plane(f3layer(layer) + (size_t)field * plane, out);
+        if (field >= QS_F_JX && field <= QS_F_DENS) {
+            if (!src3) return fail(QS_ERR_STATE, "sources are stored only with store_sources=1");
+            int q = field == QS_F_DENS ? 3 : field - QS_F_JX;
+            return get_plane(src3 + ((size_t)layer * 4 + q) * plane, out);
+        }
+        return fail(QS_ERR_INVALID, "qs_get_field3d: bad field");
+    }
+
+    T* beam_plane(int field, int layer) {
+        int q = field == QS_F_RHOBEAM ? 0 : (field == QS_F_JXBEAM ? 1 : -1);
+        if (q < 0 || layer < 0 || layer > L) return nullptr;
+        return b3 + ((size_t)layer * 2 + q) * plane;
+    }
+    qs_status set_beam_currents(int field, int layer, const double* data) override {
+        T* p = beam_plane(field, layer);
+        if (!p || !data) return fail(QS_ERR_INVALID, "qs_set_beam_currents: bad arguments");
+        return put_plane(p, data);
+    }
+    qs_status get_beam_currents(int field, int layer, double* out) override {
+        T* p = beam_plane(field, layer);
+        if (!p || !out) return fail(QS_ERR_INVALID, "qs_get_beam_currents: bad arguments");
+        return get_plane(p, out);
+    }
+
+    qs_status get_onaxis(double* out) override {
+        if (!out) return fail(QS_ERR_INVALID, "qs_get_onaxis_ex: null");
+        std::vector<T> h(L);
+        CK(cudaMemcpyAsync(h.data(), onaxis_d, L * sizeof(T), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        for (int i = 0; i < L; i++) out[i] = (double)h[i];
+        return QS_OK;
+    }
+
+    // ------------------------------------------------------------- beam push
+    qs_status move_beam() override {
+        CK(cudaMemsetAsync(b3, 0, (size_t)(L + 1) * 2 * plane * sizeof(T), st));
+        BeamArgs<T> a{};
+        a.n = nb;
+        a.L = L; a.My = My; a.Mz = Mz;
+        a.bi = bi; a.bj = bj; a.bk = bk;
+        a.x = bx; a.y = by; a.z = bz; a.px = bpx; a.py = bpy; a.pz = bpz; a.w = bw;
+        a.fields3d = f3;
+        a.beam3d = b3;
+        a.plane = plane;
+        a.ts = cfg.ts; a.hx = cfg.hx; a.hy = cfg.hy; a.hz = cfg.hz;
+        a.q2m = cfg.beam_q2m; a.polarity = cfg.beam_polarity;
+        a.bxe = cfg.bx_ext; a.bye = cfg.by_ext; a.bze = cfg.bz_ext;
+        a.syn_min = cfg.syn_min;
+        a.elaser_photon = 1.2398e-4 / cfg.wavelength;
+        a.synchrotron = cfg.synchrotron;
+        a.err = d_err;
+        count(launch_beam_push<T>(a, st));
+        CK(cudaGetLastError());
+        return QS_OK;
+    }
+
+    // --------------------------------------------------------- the march
+    SpecArgs<T> spec_args() {
+        SpecArgs<T> a{};
+        a.ny = My; a.nz = Mz;
+        const double Ylength = My * cfg.hy, Zlength = Mz * cfg.hz;
+        a.piY = (T)(M_PI / Ylength);
+        a.piZ = (T)(M_PI / Zlength);
+        a.hx = (T)(cfg.hx / S);
+        double d = std::fabs(cfg.plasma_density * cfg.plasma_q2m);
+        if (d == 0.0) d = 1.0;
+        a.dens = (T)d;
+        const int pb = cur ^ 1, cb = cur;
+        a.RhoP = bankp(pb, SP_RHO); a.ExP = bankp(pb, SP_EX); a.EyP = bankp(pb, SP_EY);
+        a.EzP = bankp(pb, SP_EZ); a.JxP = bankp(pb, SP_JX); a.JyP = bankp(pb, SP_JY);
+        a.JzP = bankp(pb, SP_JZ); a.Rbp = bankp(pb, SP_RB);
+        a.Rb = bankp(cb, SP_RB); a.Jxb = bankp(cb, SP_JXB);
+        a.Jx = bankp(cb, SP_JX); a.Jy = bankp(cb, SP_JY); a.Jz = bankp(cb, SP_JZ);
+        a.Rho = bankp(cb, SP_RHO);
+        a.Ex = bankp(cb, SP_EX); a.Ey = bankp(cb, SP_EY); a.Ez = bankp(cb, SP_EZ);
+        a.Bx = bankp(cb, SP_BX); a.By = bankp(cb, SP_BY); a.Bz = bankp(cb, SP_BZ);
+        return a;
+    }
+
+    qs_status begin_march() override {
+        if (!front_pending) {
+            qs_status s = seed_front(step_count);
+            if (s) return s;
+        }
+        front_pending = false;
+        return begin_march_device();
+    }
+
+    // the device part of MoveAllSplitLayers' set-up (capturable)
+    qs_status begin_march_device() {
+        if (src3) CK(cudaMemsetAsync(src3, 0, (size_t)(L + 1) * 4 * plane * sizeof(T), st));
+        Psrc = srcbuf;
+        Csrc = srcbuf + 4 * plane;
+        CK(cudaMemsetAsync(srcbuf, 0, 8 * plane * sizeof(T), st));
+        cur = 0;
+        p_valid = true;
+        Pf = f3layer(L);
+        Cf = f3layer(L - 1);
+        marched = true;
+        return QS_OK;
+    }
+
+    qs_status layer_begin(int iLayer, int iSplit) override {
+        if (iLayer < 0 || iLayer >= L || iSplit < 0 || iSplit >= S)
+            return fail(QS_ERR_INVALID, "qs_layer_begin: bad layer/split");
+        if (iSplit == 0) Pf = f3layer(iLayer + 1);
+        else Pf = Cf;
+        Cf = (iSplit == S - 1) ? f3layer(iLayer) : splitbuf + (size_t)(iSplit & 1) * 6 * plane;
+        count(launch_beam_layer<T>(b3 + (size_t)iLayer * 2 * plane,
+                                   b3 + (size_t)(iLayer + 1) * 2 * plane, S, iSplit, Cbeam, plane,
+                                   d_err, st));
+        return QS_OK;
+    }
+
+    qs_status guess(int iLayer, int iSplit) override {
+        const int pb = cur ^ 1, cb = cur;
+        if (iLayer == L - 1) {
+            // :430-445 the head layer zeroes the spectral arrays; the P
+            // spectra are then rebuilt from P (zero on split 0)
+            CK(cudaMemsetAsync(bankp(pb, SP_RB), 0, plane * sizeof(T), st));
+            if (iSplit == 0 && p_valid)
+                CK(cudaMemsetAsync(bankp(pb, 0), 0, (size_t)SP_RB * plane * sizeof(T), st));
+        }
+        if (!p_valid) {
+            // P planes were set from outside: transform them like :717-743
+            T* outs[7] = {bankp(pb, SP_RHO), bankp(pb, SP_EX), bankp(pb, SP_EY),
+                          bankp(pb, SP_EZ), bankp(pb, SP_JX), bankp(pb, SP_JY),
+                          bankp(pb, SP_JZ)};
+            const T* ins[7] = {Psrc + 3 * plane, Pf, Pf + plane, Pf + 2 * plane, Psrc,
+                               Psrc + plane, Psrc + 2 * plane};
+            const int kz[7] = {CC, CC, CC, SS, CC, CC, SS};
+            const int ky[7] = {CC, CC, SS, CC, CC, SS, CC};
+            // stack into stage then transform
+            for (int f = 0; f < 7; f++)
+                CK(cudaMemcpyAsync(stage + (size_t)f * plane, ins[f], plane * sizeof(T),
+                                   cudaMemcpyDeviceToDevice, st));
+            xform(job_stack(stage, 7, outs, kz, ky, T(1)));
+            p_valid = true;
+        }
+        {   // beam spectra of C (:717-718)
+            T* outs[2] = {bankp(cb, SP_RB), bankp(cb, SP_JXB)};
+            const int kz[2] = {CC, CC}, ky[2] = {CC, CC};
+            xform(job_stack(Cbeam, 2, outs, kz, ky, T(1)));
+        }
+        count(launch_predictor<T>(spec_args(), st));
+        {   // :946-967, :1004-1061 (E, B into C; the predicted Rho and J planes
+            // are cleared before any use by the push that follows)
+            T* outs[6] = {Cf, Cf + plane, Cf + 2 * plane, Cf + 3 * plane, Cf + 4 * plane,
+                          Cf + 5 * plane};
+            const int kz[6] = {CC, CC, SS, SS, SS, CC};
+            const int ky[6] = {CC, SS, CC, SS, CC, SS};
+            xform(job_stack(bankp(cb, SP_EX), 6, outs, kz, ky, inv_scale()));
+        }
+        CK(cudaGetLastError());
+        return QS_OK;
+    }
+
+    qs_status push(int iLayer, int iSplit, int full) override {
+        (void)iLayer; (void)iSplit;
+        CK(cudaMemsetAsync(Csrc, 0, 4 * plane * sizeof(T), st));   // ClearCurrentsSplit
+        PushArgs<T> a{};
+        a.n = np;
+        a.My = My; a.Mz = Mz;
+        a.cell = pcell;
+        a.y = py; a.z = pz; a.px = ppx; a.py = ppy; a.pz = ppz; a.w = pw;
+        a.P = Pf; a.C = Cf; a.dep = Csrc;
+        a.cell_out = pcell;
+        a.dep_cell = nullptr;
+        a.plane = plane;
+        a.hx = (T)(cfg.hx / S); a.hy = (T)cfg.hy; a.hz = (T)cfg.hz;
+        a.q2m = (T)cfg.plasma_q2m;
+        a.djx0 = (T)cfg.plasma_djx0; a.djy0 = (T)cfg.plasma_djy0; a.djz0 = (T)cfg.plasma_djz0;
+        a.drho0 = (T)cfg.plasma_drho0;
+        a.bxe = (T)cfg.bx_ext; a.bye = (T)cfg.by_ext; a.bze = (T)cfg.bz_ext;
+        a.full = full;
+        a.err = d_err;
+        const bool precise = sizeof(T) == 4;
+        count(launch_push<T>(a, cfg.shape, precise, st));
+        CK(cudaGetLastError());
+        return QS_OK;
+    }
+
+    qs_status iterate(int iLayer, int iSplit, int iter, double* rel_err) override {
+        (void)iLayer; (void)iSplit;
+        const int cb = cur;
+        std::vector<double> oldE;
+        if (rel_err) {
+            CK(cudaStreamSynchronize(st));
+            oldE.resize(3 * plane);
+            for (int c = 0; c < 3; c++) {
+                qs_status s = get_plane(Cf + c * plane, oldE.data() + c * plane);
+                if (s) return s;
+            }
+        }
+        {   // :1343-1345
+            T* outs[3] = {bankp(cb, SP_JX), bankp(cb, SP_JY), bankp(cb, SP_JZ)};
+            const int kz[3] = {CC, CC, SS}, ky[3] = {CC, SS, CC};
+            xform(job_stack(Csrc, 3, outs, kz, ky, T(1)));
+        }
+        count(launch_corrector<T>(spec_args(), st));
+        if (iter < 0) {   // the last iterate also stores Dens (:1517-1602)
+            T* outs[7] = {Csrc + 3 * plane, Cf, Cf + plane, Cf + 2 * plane, Cf + 3 * plane,
+                          Cf + 4 * plane, Cf + 5 * plane};
+            const int kz[7] = {CC, CC, CC, SS, SS, SS, CC};
+            const int ky[7] = {CC, CC, SS, CC, SS, CC, SS};
+            xform(job_stack(bankp(cb, SP_RHO), 7, outs, kz, ky, inv_scale()));
+        } else {
+            T* outs[6] = {Cf, Cf + plane, Cf + 2 * plane, Cf + 3 * plane, Cf + 4 * plane,
+                          Cf + 5 * plane};
+            const int kz[6] = {CC, CC, SS, SS, SS, CC};
+            const int ky[6] = {CC, SS, CC, SS, CC, SS};
+            xform(job_stack(bankp(cb, SP_EX), 6, outs, kz, ky, inv_scale()));
+        }
+        CK(cudaGetLastError());
+        if (rel_err) {
+            std::vector<double> nw(plane);
+            double mx[3] = {1e-5, 1e-5, 1e-5}, df[3] = {0, 0, 0};
+            for (int c = 0; c < 3; c++) {
+                qs_status s = get_plane(Cf + c * plane, nw.data());
+                if (s) return s;
+                for (size_t n = 0; n < plane; n++) {
+                    mx[c] = std::max(mx[c], std::fabs(nw[n]));
+                    df[c] = std::max(df[c], std::fabs(oldE[c * plane + n] - nw[n]));
+                }
+            }
+            *rel_err = std::max(std::max(df[0] / mx[0], df[1] / mx[1]), df[2] / mx[2]);
+        }
+        return QS_OK;
+    }
+
+    qs_status move_split_layer(int iLayer, int iSplit) override {
+        qs_status s = guess(iLayer, iSplit);
+        if (s) return s;
+        for (int it = 0; it < nIter; it++) {
+            if ((s = push(iLayer, iSplit, 0))) return s;
+            if ((s = iterate(iLayer, iSplit, it, nullptr))) return s;
+        }
+        if ((s = push(iLayer, iSplit, 1))) return s;
+        return iterate(iLayer, iSplit, -1, nullptr);
+    }
+
+    qs_status layer_end(int iLayer, int iSplit) override {
+        cur ^= 1;
+        std::swap(Psrc, Csrc);
+        if (iSplit == S - 1 && src3)
+            CK(cudaMemcpyAsync(src3 + (size_t)iLayer * 4 * plane, Psrc, 4 * plane * sizeof(T),
+                               cudaMemcpyDeviceToDevice, st));
+        return QS_OK;
+    }
+
+    qs_status march_device() {
+        qs_status s = begin_march_device();
+        if (s) return s;
+        for (int i = L - 1; i >= 0; i--)
+            for (int sp = 0; sp < S; sp++) {
+                if ((s = layer_begin(i, sp))) return s;
+                if ((s = move_split_layer(i, sp))) return s;
+                if ((s = layer_end(i, sp))) return s;
+            }
+        count(launch_onaxis<T>(f3, L, plane, (size_t)(My / 2) + (size_t)My * (Mz / 2), onaxis_d, st));
+        return QS_OK;
+    }
+
+    qs_status march() override {
+        if (!front_pending) {
+            qs_status s = seed_front(step_count);
+            if (s) return s;
+        }
+        front_pending = false;
+        if (!cfg.use_graph) return march_device();
+        if (!gexec) {
+            cudaGraph_t g = nullptr;
+            CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+            capturing = true;
+            capture_count = 0;
+            qs_status s = march_device();
+            capturing = false;
+            cudaError_t e = cudaStreamEndCapture(st, &g);
+            if (s) {
+                if (g) cudaGraphDestroy(g);
+                return s;
+            }
+            if (e != cudaSuccess) return cuda_fail(e, "march capture");
+            e = cudaGraphInstantiate(&gexec, g, 0);
+            cudaGraphDestroy(g);
+            if (e != cudaSuccess) {
+                gexec = nullptr;
+                return cuda_fail(e, "march graph instantiate");
+            }
+            graph_kernels = capture_count;
+            graph_end = HostState{Pf, Cf, Psrc, Csrc, cur};
+        }
+        CK(cudaGraphLaunch(gexec, st));
+        launches += graph_kernels;
+        Pf = graph_end.Pf; Cf = graph_end.Cf; Psrc = graph_end.Psrc; Csrc = graph_end.Csrc;
+        cur = graph_end.cur;
+        p_valid = true;
+        marched = true;
+        return QS_OK;
+    }
+
+    // ------------------------------------------------------ raw transforms
+    qs_status transform2d(int kz, int ky, int batch, const double* in, double* out) override {
+        if (batch < 0 || !in || !out || (kz != CC && kz != SS) || (ky != CC && ky != SS))
+            return fail(QS_ERR_INVALID, "qs_transform2d: bad arguments");
+        for (int b0 = 0; b0 < batch; b0 += 4) {
+            int nf = std::min(4, batch - b0);
+            CK(cudaMemcpyAsync(stage_d, in + (size_t)b0 * plane, nf * plane * 8,
+                               cudaMemcpyHostToDevice, st));
+            count(launch_convert<T>(stage_d, 1, stage, nf * plane, st));
+            T* outs[4];
+            int kza[4], kya[4];
+            for (int f = 0; f < nf; f++) {
+                outs[f] = stage + (size_t)(4 + f) * plane;
+                kza[f] = kz;
+                kya[f] = ky;
+            }
+            xform(job_stack(stage, nf, outs, kza, kya, T(1)));
+            count(launch_convert_back<T>(stage + 4 * plane, stage_d, nf * plane, st));
+            CK(cudaMemcpyAsync(out + (size_t)b0 * plane, stage_d, nf * plane * 8,
+                               cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+        }
+        CK(cudaGetLastError());
+        return QS_OK;
+    }
+
+    qs_status transform2d_dev(int kz, int ky, int batch, const void* d_in, void* d_out) override {
+        if (batch < 0 || !d_in || !d_out || (kz != CC && kz != SS) || (ky != CC && ky != SS))
+            return fail(QS_ERR_INVALID, "qs_transform2d_dev: bad arguments");
+        const T* in = (const T*)d_in;
+        T* out = (T*)d_out;
+        for (int b0 = 0; b0 < batch; b0 += kMaxXfFields) {
+            int nf = std::min(kMaxXfFields, batch - b0);
+            T* outs[kMaxXfFields];
+            int kza[kMaxXfFields], kya[kMaxXfFields];
+            for (int f = 0; f < nf; f++) {
+                outs[f] = out + (size_t)(b0 + f) * plane;
+                kza[f] = kz;
+                kya[f] = ky;
+            }
+            xform(job_stack(in + (size_t)b0 * plane, nf, outs, kza, kya, T(1)));
+        }
+        CK(cudaGetLastError());
+        return QS_OK;
+    }
+};
+
+}  // namespace qs
+
+using namespace qs;
+
+struct qs_handle {
+    EngineBase* e;
+};
+
+static qs_status validate(const qs_config* c, std::string& why) {
+    if (!c) { why = "null config"; return QS_ERR_INVALID; }
+    if (c->ny < 8 || c->nz < 8 || c->nx < 1) { why = "need ny, nz >= 8 and nx >= 1"; return QS_ERR_INVALID; }
+    if (c->ny % 8 || c->nz % 8) { why = "ny and nz must be multiples of 8"; return QS_ERR_INVALID; }
+    if (c->nx_split < 1 || c->n_iter < 0) { why = "nx_split >= 1 and n_iter >= 0"; return QS_ERR_INVALID; }
+    if (c->ppc < 1 || c->ppc > 16) { why = "ppc must be in [1,16]"; return QS_ERR_INVALID; }
+    if (!(c->hx > 0) || !(c->hy > 0) || !(c->hz > 0)) { why = "cell sizes must be > 0"; return QS_ERR_INVALID; }
+    if (c->shape != QS_SHAPE_NGP && c->shape != QS_SHAPE_CIC) { why = "bad shape"; return QS_ERR_INVALID; }
+    if (c->precision < QS_PREC_FP64 || c->precision > QS_PREC_BF16X6) { why = "bad precision"; return QS_ERR_INVALID; }
+    if (!(c->wavelength > 0)) { why = "wavelength must be > 0"; return QS_ERR_INVALID; }
+    return QS_OK;
+}
+
+extern "C" {
+
+qs_status qs_config_default(qs_config* c) {
+    if (!c) return QS_ERR_INVALID;
+    memset(c, 0, sizeof *c);
+    c->ny = c->nz = 128;
+    c->nx = 256;
+    c->nx_split = 1;
+    c->n_iter = 1;
+    c->ppc = 4;
+    c->hx = c->hy = c->hz = 0.05;
+    c->ts = 1.0;
+    c->plasma_density = 1.0;
+    c->plasma_q2m = -1.0;
+    c->plasma_djx0 = c->plasma_djy0 = c->plasma_djz0 = c->plasma_drho0 = -1.0;
+    c->beam_q2m = -1.0;
+    c->beam_polarity = -1.0;
+    c->syn_min = 100.0;
+    c->wavelength = 0.001;
+    c->synchrotron = 1;
+    c->precision = QS_PREC_FP32;
+    c->shape = QS_SHAPE_NGP;
+    c->device = 0;
+    c->store_sources = 0;
+    c->use_graph = 1;
+    c->seed = 12345;
+    return QS_OK;
+}
+
+qs_status qs_create(const qs_config* cfg, qs_handle** out) {
+    if (!out) return QS_ERR_INVALID;
+    *out = nullptr;
+    std::string why;
+    qs_status s = validate(cfg, why);
+    if (s) {
+        g_create_error = why;
+        return s;
+    }
+    EngineBase* e = nullptr;
+    bool tc = cfg->precision >= QS_PREC_TF32X3;
+    if (cfg->precision == QS_PREC_FP64) e = new (std::nothrow) Engine<double>();
+    else {
+        auto* ef = new (std::nothrow) Engine<float>();
+        if (ef) {
+            ef->tc = tc;
+            ef->tc_mode = cfg->precision;
+        }
+        e = ef;
+    }
+    if (!e) {
+        g_create_error = "out of host memory";
+        return QS_ERR_OOM;
+    }
+    e->cfg = *cfg;
+    e->My = cfg->ny;
+    e->Mz = cfg->nz;
+    e->L = cfg->nx;
+    e->S = cfg->nx_split;
+    e->nIter = cfg->n_iter;
+    e->dev = cfg->device;
+    s = e->init();
+    if (s) {
+        g_create_error = e->err;
+        delete e;
+        return s;
+    }
+    qs_handle* h = new (std::nothrow) qs_handle{e};
+    if (!h) {
+        delete e;
+        g_create_error = "out of host memory";
+        return QS_ERR_OOM;
+    }
+    *out = h;
+    return QS_OK;
+}
+
+qs_status qs_destroy(qs_handle* h) {
+    if (!h) return QS_ERR_INVALID;
+    if (h->e) {
+        cudaSetDevice(h->e->dev);
+        delete h->e;
+    }
+    delete h;
+    return QS_OK;
+}
+
+const char* qs_last_error(const qs_handle* h) {
+    if (!h) return g_create_error.c_str();
+    return h->e->err.c_str();
+}
+
+const char* qs_status_string(qs_status s) {
+    switch (s) {
+        case QS_OK: return "ok";
+        case QS_ERR_INVALID: return "invalid argument";
+        case QS_ERR_CUDA: return "CUDA error";
+        case QS_ERR_OOM: return "out of device memory";
+        case QS_ERR_DEVICE: return "device error flag";
+        case QS_ERR_BEAM_CURRENT: return "too large beam current";
+        case QS_ERR_PARTICLE_RANGE: return "particle outside its cell";
+        case QS_ERR_UNSUPPORTED: return "unsupported";
+        case QS_ERR_TIMEOUT: return "device wait timed out";
+        case QS_ERR_STATE: return "call out of sequence";
+    }
+    return "unknown status";
+}
+
+#define H_OR_INVALID(h)                   \
+    if (!(h) || !(h)->e) return QS_ERR_INVALID; \
+    EngineBase* E = (h)->e;               \
+    if (cudaSetDevice(E->dev) != cudaSuccess) return E->fail(QS_ERR_CUDA, "cudaSetDevice failed");
+
+qs_status qs_sync(qs_handle* h) {
+    H_OR_INVALID(h);
+    return E->check_device();
+}
+
+qs_status qs_get_stream(qs_handle* h, void** stream) {
+    if (!h || !stream) return QS_ERR_INVALID;
+    *stream = (void*)h->e->st;
+    return QS_OK;
+}
+
+qs_status qs_load_beam(qs_handle* h, int64_t n, const int32_t* i, const int32_t* j,
+                       const int32_t* k, const double* x, const double* y, const double* z,
+                       const double* px, const double* py, const double* pz, const double* w) {
+    H_OR_INVALID(h);
+    return E->load_beam(n, i, j, k, x, y, z, px, py, pz, w);
+}
+
+qs_status qs_get_beam(qs_handle* h, int64_t n, int32_t* i, int32_t* j, int32_t* k, double* x,
+                      double* y, double* z, double* px, double* py, double* pz, double* w) {
+    H_OR_INVALID(h);
+    return E->get_beam(n, i, j, k, x, y, z, px, py, pz, w);
+}
+
+int64_t qs_beam_count(const qs_handle* h) { return h ? h->e->beam_count() : -1; }
+
+qs_status qs_load_front_plasma(qs_handle* h, int64_t n, const int32_t* cell, const double* y,
+                               const double* z, const double* px, const double* py,
+                               const double* pz, const double* w) {
+    H_OR_INVALID(h);
+    return E->load_front(n, cell, y, z, px, py, pz, w);
+}
+
+qs_status qs_seed_front_plasma(qs_handle* h, uint64_t step) {
+    H_OR_INVALID(h);
+    qs_status s = E->seed_front(step);
+    if (s) return s;
+    return E->check_device();
+}
+
+int64_t qs_plasma_count(const qs_handle* h) { return h ? h->e->plasma_count() : -1; }
+
+qs_status qs_get_plasma(qs_handle* h, int64_t n, int32_t* cell, double* y, double* z, double* px,
+                        double* py, double* pz, double* w) {
+    H_OR_INVALID(h);
+    return E->get_plasma(n, cell, y, z, px, py, pz, w);
+}
+
+qs_status qs_set_layer(qs_handle* h, int which, int field, const double* data) {
+    H_OR_INVALID(h);
+    return E->set_layer(which, field, data);
+}
+qs_status qs_get_layer(qs_handle* h, int which, int field, double* out) {
+    H_OR_INVALID(h);
+    return E->get_layer(which, field, out);
+}
+qs_status qs_get_field3d(qs_handle* h, int field, int layer, double* out) {
+    H_OR_INVALID(h);
+    return E->get_field3d(field, layer, out);
+}
+qs_status qs_set_beam_currents(qs_handle* h, int field, int layer, const double* data) {
+    H_OR_INVALID(h);
+    return E->set_beam_currents(field, layer, data);
+}
+qs_status qs_get_beam_currents(qs_handle* h, int field, int layer, double* out) {
+    H_OR_INVALID(h);
+    return E->get_beam_currents(field, layer, out);
+}
+qs_status qs_get_onaxis_ex(qs_handle* h, double* out) {
+    H_OR_INVALID(h);
+    return E->get_onaxis(out);
+}
+qs_status qs_get_psi(qs_handle* h, double* out) {
+    H_OR_INVALID(h);
+    if (!out) return QS_ERR_INVALID;
+    std::vector<double> ex(E->L);
+    qs_status s = E->get_onaxis(ex.data());
+    if (s) return s;
+    // psi(nx) = 0 ahead of the box; trapezoid in xi towards the tail
+    double psi = 0.0, prev = 0.0;
+    for (int i = E->L - 1; i >= 0; i--) {
+        psi += E->cfg.hx * 0.5 * (ex[i] + prev);
+        out[i] = psi;
+        prev = ex[i];
+    }
+    return QS_OK;
+}
+
+qs_status qs_step(qs_handle* h) {
+    H_OR_INVALID(h);
+    E->phase += E->cfg.ts;   // step.cpp:33
+    qs_status s = E->move_beam();
+    if (s) return s;
+    s = E->march();
+    if (s) return s;
+    E->step_count++;
+    return E->check_device();
+}
+
+qs_status qs_move_beam_particles(qs_handle* h) {
+    H_OR_INVALID(h);
+    qs_status s = E->move_beam();
+    if (s) return s;
+    return E->check_device();
+}
+
+qs_status qs_move_all_split_layers(qs_handle* h) {
+    H_OR_INVALID(h);
+    qs_status s = E->march();
+    if (s) return s;
+    E->step_count++;
+    return E->check_device();
+}
+
+qs_status qs_begin_march(qs_handle* h) {
+    H_OR_INVALID(h);
+    qs_status s = E->begin_march();
+    if (s) return s;
+    return E->check_device();
+}
+qs_status qs_layer_begin(qs_handle* h, int iLayer, int iSplit) {
+    H_OR_INVALID(h);
+    qs_status s = E->layer_begin(iLayer, iSplit);
+    if (s) return s;
+    return E->check_device();
+}
+qs_status qs_move_split_layer(qs_handle* h, int iLayer, int iSplit) {
+    H_OR_INVALID(h);
+    if (iLayer < 0 || iLayer >= E->L || iSplit < 0 || iSplit >= E->S) return QS_ERR_INVALID;
+    qs_status s = E->move_split_layer(iLayer, iSplit);
+    if (s) return s;
+    return E->check_device();
+}
+qs_status qs_guess_fields(qs_handle* h, int iLayer, int iSplit) {
+    H_OR_INVALID(h);
+    if (iLayer < 0 || iLayer >= E->L || iSplit < 0 || iSplit >= E->S) return QS_ERR_INVALID;
+    qs_status s = E->guess(iLayer, iSplit);
+    if (s) return s;
+    return E->check_device();
+}
+qs_status qs_move_particles_layer(qs_handle* h, int iLayer, int iSplit, int iFullStep) {
+    H_OR_INVALID(h);
+    qs_status s = E->push(iLayer, iSplit, iFullStep);
+    if (s) return s;
+    return E->check_device();
+}
+qs_status qs_iterate_fields(qs_handle* h, int iLayer, int iSplit, int iter, double* rel_err) {
+    H_OR_INVALID(h);
+    qs_status s = E->iterate(iLayer, iSplit, iter, rel_err);
+    if (s) return s;
+    return E->check_device();
+}
+qs_status qs_layer_end(qs_handle* h, int iLayer, int iSplit) {
+    H_OR_INVALID(h);
+    if (iLayer < 0 || iLayer >= E->L || iSplit < 0 || iSplit >= E->S) return QS_ERR_INVALID;
+    qs_status s = E->layer_end(iLayer, iSplit);
+    if (s) return s;
+    return E->check_device();
+}
+
+qs_status qs_transform2d(qs_handle* h, int kind_z, int kind_y, int batch, const double* in,
+                         double* out) {
+    H_OR_INVALID(h);
+    qs_status s = E->transform2d(kind_z, kind_y, batch, in, out);
+    if (s) return s;
+    return E->check_device();
+}
+
+qs_status qs_transform2d_dev(qs_handle* h, int kind_z, int kind_y, int batch, const void* d_in,
+                             void* d_out) {
+    H_OR_INVALID(h);
+    return E->transform2d_dev(kind_z, kind_y, batch, d_in, d_out);
+}
+
+qs_status qs_step_host(qs_handle* h, int64_t n_beam, const int32_t* i, const int32_t* j,
+                       const int32_t* k, const double* x, const double* y, const double* z,
+                       const double* px, const double* py, const double* pz, const double* w,
+                       int32_t* i_out, int32_t* j_out, int32_t* k_out, double* x_out,
+                       double* y_out, double* z_out, double* px_out, double* py_out,
+                       double* pz_out, double* onaxis_ex_out) {
+    H_OR_INVALID(h);
+    qs_status s = E->load_beam(n_beam, i, j, k, x, y, z, px, py, pz, w);
+    if (s) return s;
+    s = qs_step(h);
+    if (s) return s;
+    if (i_out || j_out || k_out || x_out || y_out || z_out || px_out || py_out || pz_out) {
+        s = E->get_beam(n_beam, i_out, j_out, k_out, x_out, y_out, z_out, px_out, py_out, pz_out,
+                        nullptr);
+        if (s) return s;
+    }
+    if (onaxis_ex_out) return E->get_onaxis(onaxis_ex_out);
+    return QS_OK;
+}
+
+int64_t qs_kernel_launches(const qs_handle* h) { return h ? h->e->launches : -1; }
+
+}  // extern "C"

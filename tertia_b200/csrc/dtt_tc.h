@@ -1,0 +1,21 @@
+// dtt_tc.h — split-precision half-integer transforms on the tcgen05 tensor
+// cores (host interface).
+#pragma once
+#include <cuda_runtime.h>
+#include <string>
+
+namespace qs {
+
+class TcTransformer {
+public:
+    // mode: QS_PREC_TF32X3 / QS_PREC_BF16X3 / QS_PREC_BF16X6.  Returns nullptr
+    // (with a reason) when the sizes or the mode are not supported.
+    static TcTransformer* create(int mode, int ny, int nz, cudaStream_t st, std::string& why);
+    virtual ~TcTransformer() {}
+    // nf fields: out_f = scale * A_z(kz_f) in_f A_y(ky_f); in_f are nz x ny
+    // planes stored consecutively from in[0]; returns the kernels launched.
+    virtual int run(int nf, const void* const* in, void* const* out, const int* kz,
+                    const int* ky, double scale, int elem_size, cudaStream_t st) = 0;
+};
+
+}  // namespace qs

@@ -1,0 +1,72 @@
+// qs_internal.h — host-side launchers shared by the CUDA translation units.
+#pragma once
+#include "qs_common.cuh"
+
+namespace qs {
+
+// Per-mode spectral maps of the Guess / Iterate solve.
+template <class T>
+struct SpecArgs {
+    int ny, nz;
+    T piY, piZ;          // M_PI/Ylength, M_PI/Zlength
+    T hx, dens;
+    const T *RhoP, *ExP, *EyP, *EzP, *JxP, *JyP, *JzP;   // P spectral state
+    const T *Rb, *Rbp, *Jxb;                              // beam spectra (C, P)
+    const T *Jx, *Jy, *Jz;                                // forward of the C deposit
+    T* Rho;                                               // in/out spectral rho
+    T *Ex, *Ey, *Ez, *Bx, *By, *Bz;                       // spectral outputs
+};
+
+template <class T>
+int launch_predictor(const SpecArgs<T>& a, cudaStream_t st);
+template <class T>
+int launch_corrector(const SpecArgs<T>& a, cudaStream_t st);
+
+// C-layer beam currents for (iLayer, iSplit): the xi-interpolation of
+// movepart_splitlayer.cpp:330-348 plus the |JxBeam| > 10 check.
+template <class T>
+int launch_beam_layer(const T* cur, const T* nxt, int S, int s, T* out, size_t plane, int* err,
+                      cudaStream_t st);
+
+template <class T>
+int launch_onaxis(const T* fields3d, int L, size_t plane, size_t idx, T* out, cudaStream_t st);
+
+template <class T>
+int launch_seed_front(int My, int Mz, int ppc, const double* offs_y, const double* offs_z,
+                      double px0, double py0, double pz0, double sx, double sy, double sz,
+                      double weight, uint64_t seed, uint64_t step, int32_t* cell, T* y, T* z,
+                      T* px, T* py, T* pz, T* w, cudaStream_t st);
+
+template <class T>
+int launch_convert(const void* src, int src_is_double, T* dst, size_t n, cudaStream_t st);
+template <class T>
+int launch_convert_back(const T* src, double* dst, size_t n, cudaStream_t st);
+
+// Transforms.
+template <class T>
+int run_dtt_simt(const DttJob<T>& job, int ny, int nz, const DttMats<T>& my,
+                 const DttMats<T>& mz, T* scratch, cudaStream_t st);
+
+template <class T>
+int launch_push(const PushArgs<T>& a, int shape, bool precise, cudaStream_t st);
+
+// Beam push + 3-D CIC deposit (movebeam.cpp:14-774).
+template <class T>
+struct BeamArgs {
+    int64_t n;
+    int L, My, Mz;
+    int32_t *bi, *bj, *bk;
+    double *x, *y, *z, *px, *py, *pz;
+    const double* w;
+    const T* fields3d;    // (L+1) layers x 6 planes
+    T* beam3d;            // (L+1) layers x 2 planes (RhoBeam, JxBeam)
+    size_t plane;
+    double ts, hx, hy, hz, q2m, polarity, bxe, bye, bze;
+    double syn_min, elaser_photon;
+    int synchrotron;
+    int* err;
+};
+template <class T>
+int launch_beam_push(const BeamArgs<T>& a, cudaStream_t st);
+
+}  // namespace qs

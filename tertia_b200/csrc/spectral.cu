@@ -1,0 +1,256 @@
+// spectral.cu — per-mode maps of the half-integer spectral field solve and
+// the small per-layer kernels around them.
+//
+// Predictor: GuessFieldsHydroLinLayerSplit's linearised step
+// (movefieldshydrolinlayersplit.cpp:808-900; dead GPU twin
+// linearized_kernel, linearized.cu:11-103).  Corrector:
+// IterateFieldsHydroLinLayerSplit (:1374-1477; twin
+// linearizedIteratekernel, linearized.cu:105-209).  The expression order is
+// the reference's and the file is compiled with -fmad=false.
+//
+// The P-layer spectra (RhoP, E*P, J*P) are the previous layer's final
+// spectra carried in HBM: the reference recomputes them by transforming the
+// P layer's real planes (:569-623, :717-743), which are the inverse
+// transforms of exactly those spectra, so the forward-of-inverse is skipped.
+#include <cmath>
+
+#include "qs_common.cuh"
+#include "qs_internal.h"
+
+namespace qs {
+
+template <class T>
+__global__ void predictor_kernel(SpecArgs<T> a) {
+    const int n1 = blockIdx.x * blockDim.x + threadIdx.x;
+    const int N = a.ny * a.nz;
+    if (n1 >= N) return;
+    const int j = n1 % a.ny, k = n1 / a.ny;
+    const T d = a.dens, hx = a.hx;
+    const T akz = a.piZ * (T(k) + T(0.5));
+    const T aky = a.piY * (T(j) + T(0.5));
+    const T ak2 = aky * aky + akz * akz;
+    const T rp = a.RhoP[n1];
+    const T jxp = a.JxP[n1], jyp = a.JyP[n1], jzp = a.JzP[n1];
+    const T exp_ = a.ExP[n1], eyp = a.EyP[n1], ezp = a.EzP[n1];
+    const T rb = a.Rb[n1], rbp = a.Rbp[n1];
+    const T propagator = (T(4) - d * hx * hx) / (T(4) + d * hx * hx);
+    const T denominator = T(4) + d * hx * hx;
+    const T rho = propagator * rp - (rb + rbp) * d * hx * hx / denominator +
+                  T(4) * exp_ * hx * (ak2 + d) / denominator;
+    const T ex = propagator * exp_ - T(2) * (T(2) * rp + rb + rbp) * d * hx / ((ak2 + d) * denominator);
+    const T ey = -eyp + aky * (rb + rbp + rp + rho) / (d + ak2);
+    const T ez = -ezp + akz * (rb + rbp + rp + rho) / (d + ak2);
+    const T jy = jyp + hx * d * (ey + eyp) / T(2);
+    const T jz = jzp + hx * d * (ez + ezp) / T(2);
+    const T jx = jxp + hx * d * (ex + exp_) / T(2);
+    const T jxb = a.Jxb[n1];
+    a.Rho[n1] = rho;
+    a.Ex[n1] = ex;
+    a.Ey[n1] = ey;
+    a.Ez[n1] = ez;
+    a.Bx[n1] = -aky / ak2 * jz + akz / ak2 * jy;
+    a.By[n1] = (-akz * (jx + jxb) + d * ez) / ak2;
+    a.Bz[n1] = (aky * (jx + jxb) - d * ey) / ak2;
+}
+
+template <class T>
+__global__ void corrector_kernel(SpecArgs<T> a) {
+    const int n1 = blockIdx.x * blockDim.x + threadIdx.x;
+    const int N = a.ny * a.nz;
+    if (n1 >= N) return;
+    const int j = n1 % a.ny, k = n1 / a.ny;
+    const T d = a.dens, hx = a.hx;
+    const T akz = a.piZ * (T(k) + T(0.5));
+    const T aky = a.piY * (T(j) + T(0.5));
+    const T ak2 = aky * aky + akz * akz;
+    const T rp = a.RhoP[n1];
+    const T jx = a.Jx[n1], jy = a.Jy[n1], jz = a.Jz[n1];
+    const T rho = rp + jx - a.JxP[n1] - hx * (aky * (jy + a.JyP[n1]) + akz * (jz + a.JzP[n1])) / T(2);
+    const T rb = a.Rb[n1], rbp = a.Rbp[n1];
+    const T eyp = a.EyP[n1], ezp = a.EzP[n1];
+    const T rho_old = a.Rho[n1];
+    const T newEx = -(aky * jy + akz * jz) / ak2;
+    const T newEy = -eyp + aky * (rb + rbp + rp + rho_old) / (d + ak2);
+    const T newEz = -ezp + akz * (rb + rbp + rp + rho_old) / (d + ak2);
+    const T jxb = a.Jxb[n1];
+    a.Ey[n1] = newEy;
+    a.Ez[n1] = newEz;
+    a.Rho[n1] = rho;
+    a.Ex[n1] = newEx;
+    a.Bx[n1] = -aky / ak2 * jz + akz / ak2 * jy;
+    a.By[n1] = (-akz * (jx + jxb) + d * newEz) / ak2;
+    a.Bz[n1] = (aky * (jx + jxb) - d * newEy) / ak2;
+}
+
+template <class T>
+int launch_predictor(const SpecArgs<T>& a, cudaStream_t st) {
+    const int N = a.ny * a.nz;
+    predictor_kernel<T><<<(N + 255) / 256, 256, 0, st>>>(a);
+    return 1;
+}
+template <class T>
+int launch_corrector(const SpecArgs<T>& a, cudaStream_t st) {
+    const int N = a.ny * a.nz;
+    corrector_kernel<T><<<(N + 255) / 256, 256, 0, st>>>(a);
+    return 1;
+}
+
+// out[0] = RhoBeam, out[1] = JxBeam of the C layer.
+template <class T>
+__global__ void beam_layer_kernel(const T* __restrict__ cur, const T* __restrict__ nxt, int S,
+                                  int s, T* __restrict__ out, size_t plane, int* err) {
+    const size_t n = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= plane) return;
+    T r, jx;
+    if (S == 1) {
+        r = cur[n];
+        jx = cur[plane + n];
+    } else {
+        const T Sd = T(S);
+        r = (cur[n] * (Sd - T(s)) + nxt[n] * T(s)) / Sd;
+        jx = (cur[plane + n] * (Sd - T(s)) + nxt[plane + n] * T(s)) / Sd;
+    }
+    out[n] = r;
+    out[plane + n] = jx;
+    if (fabs((double)jx) > 10.0) atomicOr(err, DEV_ERR_BEAM_CURRENT);
+}
+
+template <class T>
+int launch_beam_layer(const T* cur, const T* nxt, int S, int s, T* out, size_t plane, int* err,
+                      cudaStream_t st) {
+    beam_layer_kernel<T><<<(unsigned)((plane + 255) / 256), 256, 0, st>>>(cur, nxt, S, s, out,
+                                                                          plane, err);
+    return 1;
+}
+
+template <class T>
+__global__ void onaxis_kernel(const T* __restrict__ f3, int L, size_t plane, size_t idx,
+                              T* __restrict__ out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < L) out[i] = f3[(size_t)i * 6 * plane + idx];
+}
+
+template <class T>
+int launch_onaxis(const T* fields3d, int L, size_t plane, size_t idx, T* out, cudaStream_t st) {
+    onaxis_kernel<T><<<(L + 255) / 256, 256, 0, st>>>(fields3d, L, plane, idx, out);
+    return 1;
+}
+
+// ---- front-layer seeding with a counter-based generator.
+// Philox4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11): 10 rounds of the
+// published multiply-xor bijection with Weyl key schedule.
+struct U4 { uint32_t x, y, z, w; };
+
+__device__ __forceinline__ U4 philox_round(U4 c, uint32_t k0, uint32_t k1) {
+    const uint32_t M0 = 0xD2511F53u, M1 = 0xCD9E8D57u;
+    const uint32_t lo0 = M0 * c.x, hi0 = __umulhi(M0, c.x);
+    const uint32_t lo1 = M1 * c.z, hi1 = __umulhi(M1, c.z);
+    return U4{hi1 ^ c.y ^ k0, lo1, hi0 ^ c.w ^ k1, lo0};
+}
+
+__device__ U4 philox4x32_10(U4 c, uint32_t k0, uint32_t k1) {
+    const uint32_t W0 = 0x9E3779B9u, W1 = 0xBB67AE85u;
+#pragma unroll
+    for (int r = 0; r < 10; r++) {
+        c = philox_round(c, k0, k1);
+        k0 += W0;
+        k1 += W1;
+    }
+    return c;
+}
+
+__device__ __forceinline__ void box_muller(uint32_t a, uint32_t b, double& n0, double& n1) {
+    const double u1 = ((double)a + 0.5) * 2.3283064365386963e-10;  // 2^-32
+    const double u2 = ((double)b + 0.5) * 2.3283064365386963e-10;
+    const double r = sqrt(-2.0 * log(u1));
+    double s, c;
+    sincospi(2.0 * u2, &s, &c);
+    n0 = r * c;
+    n1 = r * s;
+}
+
+struct SeedOffs { double y[16], z[16]; };
+
+template <class T>
+__global__ void seed_front_kernel(int My, int Mz, int ppc, SeedOffs offs, double px0, double py0,
+                                  double pz0, double sx, double sy, double sz, double weight,
+                                  uint64_t seed, uint64_t step, int32_t* cell, T* y, T* z, T* px,
+                                  T* py, T* pz, T* w) {
+    const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t n = (int64_t)My * Mz * ppc;
+    if (p >= n) return;
+    const int c = (int)(p / ppc), s = (int)(p % ppc);
+    const uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32);
+    // counter = (particle index, step): one block of 4 words gives 4 normals
+    const U4 r0 = philox4x32_10(
+        U4{(uint32_t)p, (uint32_t)(p >> 32), (uint32_t)step, (uint32_t)(step >> 32)}, k0, k1);
+    double g0, g1, g2, g3;
+    box_muller(r0.x, r0.y, g0, g1);
+    box_muller(r0.z, r0.w, g2, g3);
+    cell[p] = c;
+    y[p] = (T)offs.y[s];
+    z[p] = (T)offs.z[s];
+    px[p] = (T)(px0 + sx * g0);
+    py[p] = (T)(py0 + sy * g1);
+    pz[p] = (T)(pz0 + sz * g2);
+    w[p] = (T)weight;
+}
+
+template <class T>
+int launch_seed_front(int My, int Mz, int ppc, const double* offs_y, const double* offs_z,
+                      double px0, double py0, double pz0, double sx, double sy, double sz,
+                      double weight, uint64_t seed, uint64_t step, int32_t* cell, T* y, T* z,
+                      T* px, T* py, T* pz, T* w, cudaStream_t st) {
+    SeedOffs o{};
+    for (int s = 0; s < ppc && s < 16; s++) {
+        o.y[s] = offs_y[s];
+        o.z[s] = offs_z[s];
+    }
+    const int64_t n = (int64_t)My * Mz * ppc;
+    seed_front_kernel<T><<<(unsigned)((n + 255) / 256), 256, 0, st>>>(
+        My, Mz, ppc, o, px0, py0, pz0, sx, sy, sz, weight, seed, step, cell, y, z, px, py, pz, w);
+    return 1;
+}
+
+template <class T>
+__global__ void convert_kernel(const void* __restrict__ src, int is_double, T* __restrict__ dst,
+                               size_t n) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    dst[i] = is_double ? (T)((const double*)src)[i] : (T)((const float*)src)[i];
+}
+template <class T>
+__global__ void convert_back_kernel(const T* __restrict__ src, double* __restrict__ dst, size_t n) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) dst[i] = (double)src[i];
+}
+template <class T>
+int launch_convert(const void* src, int src_is_double, T* dst, size_t n, cudaStream_t st) {
+    if (!n) return 0;
+    convert_kernel<T><<<(unsigned)((n + 255) / 256), 256, 0, st>>>(src, src_is_double, dst, n);
+    return 1;
+}
+template <class T>
+int launch_convert_back(const T* src, double* dst, size_t n, cudaStream_t st) {
+    if (!n) return 0;
+    convert_back_kernel<T><<<(unsigned)((n + 255) / 256), 256, 0, st>>>(src, dst, n);
+    return 1;
+}
+
+#define QS_INST(T)                                                                              \
+    template int launch_predictor<T>(const SpecArgs<T>&, cudaStream_t);                         \
+    template int launch_corrector<T>(const SpecArgs<T>&, cudaStream_t);                         \
+    template int launch_beam_layer<T>(const T*, const T*, int, int, T*, size_t, int*,           \
+                                      cudaStream_t);                                            \
+    template int launch_onaxis<T>(const T*, int, size_t, size_t, T*, cudaStream_t);            \
+    template int launch_seed_front<T>(int, int, int, const double*, const double*, double,      \
+                                      double, double, double, double, double, double,           \
+                                      uint64_t, uint64_t, int32_t*, T*, T*, T*, T*, T*, T*,     \
+                                      cudaStream_t);                                            \
+    template int launch_convert<T>(const void*, int, T*, size_t, cudaStream_t);                 \
+    template int launch_convert_back<T>(const T*, double*, size_t, cudaStream_t);
+QS_INST(float)
+QS_INST(double)
+#undef QS_INST
+
+}  // namespace qs

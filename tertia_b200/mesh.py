@@ -1,0 +1,235 @@
+"""Python mirror of the reference's Mesh call surface over the C ABI.
+
+Method names follow the reference (mesh.h:55-76, step.cpp:24):
+MoveAllSplitLayers, MoveSplitLayer, GuessFieldsHydroLinLayerSplit,
+MoveParticlesLayerSplit, IterateFieldsHydroLinLayerSplit, MoveBeamParticles,
+Step; the snake_case names are the same calls.  Every call raises QsError
+carrying the library's qs_status where the reference would have exit()ed.
+All arrays are host numpy arrays; the device copies live in the handle.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import abi
+from .abi import QsConfig, QsError, load_library
+
+
+def _p(a, ctype):
+    return a.ctypes.data_as(C.POINTER(ctype)) if a is not None else None
+
+
+def _f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def _i32(a):
+    return np.ascontiguousarray(a, dtype=np.int32)
+
+
+class Mesh:
+    """One quasi-static box on one GPU (a qs_handle)."""
+
+    def __init__(self, cfg: QsConfig):
+        self._L = load_library()
+        self.cfg = cfg.copy()
+        h = C.c_void_p()
+        st = self._L.qs_create(C.byref(self.cfg), C.byref(h))
+        if st != 0:
+            raise QsError(st, self._L.qs_last_error(None).decode())
+        self._h = h
+        self.plane = cfg.ny * cfg.nz
+
+    # -------------------------------------------------------------- plumbing
+    def _chk(self, st: int, what: str):
+        if st != 0:
+            msg = self._L.qs_last_error(self._h).decode() if self._h else ""
+            raise QsError(st, f"{what}: {msg}")
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.qs_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def sync(self):
+        self._chk(self._L.qs_sync(self._h), "qs_sync")
+
+    def stream(self) -> int:
+        s = C.c_void_p()
+        self._chk(self._L.qs_get_stream(self._h, C.byref(s)), "qs_get_stream")
+        return s.value or 0
+
+    def kernel_launches(self) -> int:
+        return int(self._L.qs_kernel_launches(self._h))
+
+    # -------------------------------------------------------------- state
+    def load_beam(self, b: dict):
+        n = len(b["x"])
+        ii, jj, kk = (_i32(b[k]) for k in "ijk")
+        f = [_f64(b[k]) for k in ("x", "y", "z", "px", "py", "pz", "w")]
+        self._chk(self._L.qs_load_beam(self._h, n, _p(ii, C.c_int32), _p(jj, C.c_int32),
+                                       _p(kk, C.c_int32), *[_p(a, C.c_double) for a in f]),
+                  "qs_load_beam")
+
+    def get_beam(self) -> dict:
+        n = int(self._L.qs_beam_count(self._h))
+        out = {k: np.empty(n, dtype=np.int32) for k in "ijk"}
+        out.update({k: np.empty(n) for k in ("x", "y", "z", "px", "py", "pz", "w")})
+        self._chk(self._L.qs_get_beam(self._h, n, *[_p(out[k], C.c_int32) for k in "ijk"],
+                                      *[_p(out[k], C.c_double) for k in
+                                        ("x", "y", "z", "px", "py", "pz", "w")]),
+                  "qs_get_beam")
+        return out
+
+    def load_front_plasma(self, p: dict):
+        n = len(p["y"])
+        cell = _i32(p["cell"])
+        f = [_f64(p[k]) for k in ("y", "z", "px", "py", "pz", "w")]
+        self._chk(self._L.qs_load_front_plasma(self._h, n, _p(cell, C.c_int32),
+                                               *[_p(a, C.c_double) for a in f]),
+                  "qs_load_front_plasma")
+
+    def seed_front_plasma(self, step: int):
+        self._chk(self._L.qs_seed_front_plasma(self._h, int(step)), "qs_seed_front_plasma")
+
+    def get_plasma(self) -> dict:
+        n = int(self._L.qs_plasma_count(self._h))
+        out = {"cell": np.empty(n, dtype=np.int32)}
+        out.update({k: np.empty(n) for k in ("y", "z", "px", "py", "pz", "w")})
+        self._chk(self._L.qs_get_plasma(self._h, n, _p(out["cell"], C.c_int32),
+                                        *[_p(out[k], C.c_double) for k in
+                                          ("y", "z", "px", "py", "pz", "w")]), "qs_get_plasma")
+        return out
+
+    def _plane(self):
+        return np.empty(self.plane, dtype=np.float64)
+
+    def _shape(self, a):
+        return a.reshape(self.cfg.nz, self.cfg.ny)
+
+    def set_layer(self, which: int, field: int, data):
+        d = _f64(data).reshape(-1)
+        self._chk(self._L.qs_set_layer(self._h, which, field, _p(d, C.c_double)), "qs_set_layer")
+
+    def get_layer(self, which: int, field: int):
+        out = self._plane()
+        self._chk(self._L.qs_get_layer(self._h, which, field, _p(out, C.c_double)), "qs_get_layer")
+        return self._shape(out)
+
+    def get_field3d(self, field: int, layer: int):
+        out = self._plane()
+        self._chk(self._L.qs_get_field3d(self._h, field, layer, _p(out, C.c_double)),
+                  "qs_get_field3d")
+        return self._shape(out)
+
+    def set_beam_currents(self, field: int, layer: int, data):
+        d = _f64(data).reshape(-1)
+        self._chk(self._L.qs_set_beam_currents(self._h, field, layer, _p(d, C.c_double)),
+                  "qs_set_beam_currents")
+
+    def get_beam_currents(self, field: int, layer: int):
+        out = self._plane()
+        self._chk(self._L.qs_get_beam_currents(self._h, field, layer, _p(out, C.c_double)),
+                  "qs_get_beam_currents")
+        return self._shape(out)
+
+    def onaxis_ex(self):
+        out = np.empty(self.cfg.nx)
+        self._chk(self._L.qs_get_onaxis_ex(self._h, _p(out, C.c_double)), "qs_get_onaxis_ex")
+        return out
+
+    def psi(self):
+        out = np.empty(self.cfg.nx)
+        self._chk(self._L.qs_get_psi(self._h, _p(out, C.c_double)), "qs_get_psi")
+        return out
+
+    # -------------------------------------------------------------- the path
+    def step(self):
+        self._chk(self._L.qs_step(self._h), "qs_step")
+
+    def move_beam_particles(self):
+        self._chk(self._L.qs_move_beam_particles(self._h), "qs_move_beam_particles")
+
+    def move_all_split_layers(self):
+        self._chk(self._L.qs_move_all_split_layers(self._h), "qs_move_all_split_layers")
+
+    def begin_march(self):
+        self._chk(self._L.qs_begin_march(self._h), "qs_begin_march")
+
+    def layer_begin(self, i: int, s: int = 0):
+        self._chk(self._L.qs_layer_begin(self._h, i, s), "qs_layer_begin")
+
+    def move_split_layer(self, i: int, s: int = 0):
+        self._chk(self._L.qs_move_split_layer(self._h, i, s), "qs_move_split_layer")
+
+    def guess_fields(self, i: int, s: int = 0):
+        self._chk(self._L.qs_guess_fields(self._h, i, s), "qs_guess_fields")
+
+    def move_particles_layer(self, i: int, s: int, full: int):
+        self._chk(self._L.qs_move_particles_layer(self._h, i, s, int(full)),
+                  "qs_move_particles_layer")
+
+    def iterate_fields(self, i: int, s: int, it: int) -> float:
+        e = C.c_double(0.0)
+        self._chk(self._L.qs_iterate_fields(self._h, i, s, it, C.byref(e)), "qs_iterate_fields")
+        return e.value
+
+    def layer_end(self, i: int, s: int = 0):
+        self._chk(self._L.qs_layer_end(self._h, i, s), "qs_layer_end")
+
+    def transform2d(self, x, kind_z: int, kind_y: int):
+        x = _f64(x)
+        nz, ny = x.shape[-2:]
+        if (nz, ny) != (self.cfg.nz, self.cfg.ny):
+            raise ValueError("planes must be nz x ny")
+        batch = int(np.prod(x.shape[:-2])) if x.ndim > 2 else 1
+        out = np.empty_like(x)
+        self._chk(self._L.qs_transform2d(self._h, kind_z, kind_y, batch, _p(x, C.c_double),
+                                         _p(out, C.c_double)), "qs_transform2d")
+        return out
+
+    def step_host(self, b: dict, want_beam: bool = True):
+        """One step through host buffers (beam in, beam and on-axis Ex out)."""
+        n = len(b["x"])
+        ii, jj, kk = (_i32(b[k]) for k in "ijk")
+        f = [_f64(b[k]) for k in ("x", "y", "z", "px", "py", "pz", "w")]
+        out = {k: np.empty(n, dtype=np.int32) for k in "ijk"}
+        out.update({k: np.empty(n) for k in ("x", "y", "z", "px", "py", "pz")})
+        ex = np.empty(self.cfg.nx)
+        outs_i = [_p(out[k], C.c_int32) if want_beam else None for k in "ijk"]
+        outs_f = [_p(out[k], C.c_double) if want_beam else None
+                  for k in ("x", "y", "z", "px", "py", "pz")]
+        self._chk(self._L.qs_step_host(self._h, n, _p(ii, C.c_int32), _p(jj, C.c_int32),
+                                       _p(kk, C.c_int32), *[_p(a, C.c_double) for a in f],
+                                       *outs_i, *outs_f, _p(ex, C.c_double)), "qs_step_host")
+        out["w"] = f[-1]
+        return (out if want_beam else None), ex
+
+    # reference-named aliases (mesh.h:55-76, step.cpp:24)
+    Step = step
+    MoveBeamParticles = move_beam_particles
+    MoveAllSplitLayers = move_all_split_layers
+    MoveSplitLayer = move_split_layer
+    GuessFieldsHydroLinLayerSplit = guess_fields
+
+    def MoveParticlesLayerSplit(self, iLayer, iSplit, iFullStep, part=1.0):
+        if part != 1.0:
+            raise QsError(abi.QS_ERR_UNSUPPORTED, "part != 1 is not used by the split march")
+        self.move_particles_layer(iLayer, iSplit, iFullStep)
+
+    def IterateFieldsHydroLinLayerSplit(self, iLayer, iSplit, N_iter):
+        return self.iterate_fields(iLayer, iSplit, N_iter)
