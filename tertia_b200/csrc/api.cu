@@ -239,7 +239,7 @@ struct Engine : EngineBase {
         mz.m[SS] = mats + 2 * ny2 + nz2;
         if (tc) {
             std::string msg;
-            tcx = TcTransformer::create(tc_mode, My, Mz, st, msg);
+            tcx = TcTransformer::create(tc_mode, My, Mz, d_err, msg);
             if (!tcx) return fail(QS_ERR_UNSUPPORTED, "tensor-core transform: %s", msg.c_str());
         }
         Pf = splitbuf;

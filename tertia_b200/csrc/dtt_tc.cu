@@ -570,20 +570,12 @@ public:
 
 }  // namespace
 
-int* g_tc_err_flag = nullptr;
-
-TcTransformer* TcTransformer::create(int mode, int ny, int nz, cudaStream_t st, std::string& why) {
-    (void)st;
+TcTransformer* TcTransformer::create(int mode, int ny, int nz, int* err_flag, std::string& why) {
     auto* t = new TcImpl();
     t->mode = mode;
     t->ny = ny;
     t->nz = nz;
-    t->err = g_tc_err_flag;
-    if (!t->err) {
-        why = "error flag not set";
-        delete t;
-        return nullptr;
-    }
+    t->err = err_flag;
     if (!t->init(why)) {
         delete t;
         return nullptr;

@@ -10,7 +10,7 @@ class TcTransformer {
 public:
     // mode: QS_PREC_TF32X3 / QS_PREC_BF16X3 / QS_PREC_BF16X6.  Returns nullptr
     // (with a reason) when the sizes or the mode are not supported.
-    static TcTransformer* create(int mode, int ny, int nz, cudaStream_t st, std::string& why);
+    static TcTransformer* create(int mode, int ny, int nz, int* err_flag, std::string& why);
     virtual ~TcTransformer() {}
     // nf fields: out_f = scale * A_z(kz_f) in_f A_y(ky_f); in_f are nz x ny
     // planes stored consecutively from in[0]; returns the kernels launched.
