@@ -1,0 +1,409 @@
+#!/usr/bin/env python
+"""Benchmark of the quasi-static xi-layer loop: particle-layer pushes/s.
+
+One step = one beam time step of the reference's Domain::Step (step.cpp:24):
+driver-beam push + 3-D CIC deposit, then the full xi-march over every layer
+(front seeding, Guess, nIter x (push, Iterate), full push, Iterate).
+One particle-layer push = one plasma macro-particle carried across one
+xi-layer (all nIter+1 sub-pushes counted once): Np * layers per step.
+
+Default workload (N=1): c1, 512 x 512 transverse cells, 1024 layers, 4 ppc
+(1,048,576 plasma particles per layer), thermal sigma_p = 0.01, 1e6 driver
+particles, synthetic seeded inputs.  The field store (6.4 GB) and beam-current
+store (2.1 GB) are far larger than L2, so every step streams from HBM.
+
+  python bench.py [--gpus N --steps K --warmup W --precision tf32x3]
+  python bench.py --impl reference     # the reference's CPU path (oracle port)
+
+Under torchrun (N>1) every rank runs an independent replica: the march is
+serial in xi and does not shard (replicas only, no collective in the path).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+METRIC = "particle-layer pushes/s"
+UNIT = "pushes/s"
+CLASSES = ["push_deposit", "transform_gemm", "transform_split", "spectral_maps",
+           "beam_layer", "beam_push", "front_seed", "other"]
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="c1")
+    ap.add_argument("--precision", default="tf32x3")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-fp64", action="store_true", help="skip the FP64-plain comparison")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0,
+                    help="target seconds of the bounded CPU sample")
+    return ap.parse_args()
+
+
+# ------------------------------------------------------------------ helpers
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.rows = []
+        self.proc = None
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "200", "-i", str(self.device)],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+            return
+        def reader():
+            for line in self.proc.stdout:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 9:
+                    self.rows.append(parts)
+        self.thread = threading.Thread(target=reader, daemon=True)
+        self.thread.start()
+
+    def stop(self):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in self.rows:
+            try:
+                sm.append(float(r[1]))
+                mx = float(r[2])
+            except ValueError:
+                continue
+            for name, v in zip(names, r[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return p["hbm_gbs"], p["bf16_tflops"], p.get("bf16_tflops_sustained", p["bf16_tflops"]), \
+            "measured"
+    except Exception:
+        return 6650.0, 1590.0, 1400.0, "fallback"
+
+
+def traffic_record(kernel: str, workload: str, precision: str):
+    """Per-launch DRAM bytes of the dominant kernel from the committed ncu
+    summary (profiles/traffic.json), or None."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+            t = json.load(f)
+        return t.get(f"{kernel}:{workload}:{precision}")
+    except Exception:
+        return None
+
+
+def cpu_sample(w, target_s: float):
+    """Time the oracle (the reference's FP64 CPU path restated) on a bounded
+    sample of the same workload: the full transverse grid, a few layers near
+    the front (per-layer cost does not depend on the beam)."""
+    import numpy as np
+    from oracle import binding as ob
+    from tertia_b200 import workload as wl
+    cores = os.cpu_count() or 1
+    ob.set_threads(cores)
+
+    def run(layers):
+        cfg = w.cfg.copy()
+        cfg.nx = layers
+        cfg.precision = 0
+        o = ob.Oracle(cfg)
+        b = wl.sample_beam(cfg, wl.BeamSpec(16))
+        o.load_beam(b)
+        o.load_front_plasma(wl.front_plasma(cfg, seed=3))
+        t = time.perf_counter()
+        o.move_all_split_layers()
+        dt = time.perf_counter() - t
+        o.close()
+        return dt
+
+    t1 = run(2) / 2
+    layers = max(2, min(256, int(target_s / max(t1, 1e-3))))
+    dt = run(layers)
+    np_layer = w.cfg.ny * w.cfg.nz * w.cfg.ppc
+    return {"value": np_layer * layers * w.cfg.nx_split / dt, "unit": UNIT, "cores": cores,
+            "kind": "port",
+            "sample": f"oracle FP64 xi-march of {layers} layers of the {w.cfg.ny}x{w.cfg.nz} "
+                      f"grid ({np_layer} particles/layer), {dt:.1f} s on {cores} threads"}
+
+
+# ------------------------------------------------------------------ our arm
+def run_ours(args):
+    import numpy as np
+    import torch
+    from tertia_b200 import workload as wl
+    from tertia_b200.abi import PRECISIONS
+    from tertia_b200.mesh import Mesh
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    w = wl.make_workload(args.workload, args.precision)
+    cfg = w.cfg
+    cfg.device = local
+    cfg.seed = 12345 + rank
+    beam = wl.workload_beam(w)
+    npl = cfg.ny * cfg.nz * cfg.ppc
+    pushes_per_step = npl * cfg.nx * cfg.nx_split
+
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        import torch.distributed as dist
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    m = Mesh(cfg)
+    m.load_beam(beam)
+    stream = torch.cuda.ExternalStream(m.stream())
+    for _ in range(args.warmup):
+        m.step()
+    # ---------------- timed region: K steps, device events on the handle's stream
+    clocks = ClockSampler(local)
+    clocks.start()
+    l0 = m.kernel_launches()
+    barrier()
+    torch.cuda.synchronize()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        m.step()
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    ms = ev0.elapsed_time(ev1) / args.steps
+    clk = clocks.stop()
+    launches = m.kernel_launches() - l0
+    ms_max = max_over_ranks(ms)
+    value = world * pushes_per_step / (ms_max / 1e3)
+    onaxis = m.onaxis_ex()
+
+    # ---------------- e2e: the public C ABI with host buffers (pinned)
+    n = len(beam["x"])
+    pin = {}
+    for k in ("i", "j", "k"):
+        t = torch.empty(n, dtype=torch.int32, pin_memory=True)
+        t.numpy()[:] = beam[k]
+        pin[k] = t
+    for k in ("x", "y", "z", "px", "py", "pz", "w"):
+        t = torch.empty(n, dtype=torch.float64, pin_memory=True)
+        t.numpy()[:] = beam[k]
+        pin[k] = t
+    host = {k: v.numpy() for k, v in pin.items()}
+    out_pin = {k: torch.empty(n, dtype=torch.int32 if k in "ijk" else torch.float64,
+                              pin_memory=True).numpy() for k in ("i", "j", "k", "x", "y", "z",
+                                                                 "px", "py", "pz")}
+    e2e_steps = max(1, args.steps)
+    m.step_host(host, out=out_pin)           # warm the host path
+    barrier()
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    for _ in range(e2e_steps):
+        res, ex = m.step_host(host, out=out_pin)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    e2e_ms = max_over_ranks(ev0.elapsed_time(ev1) / e2e_steps)
+    h2d = n * (3 * 4 + 7 * 8)
+    d2h = n * (3 * 4 + 6 * 8) + cfg.nx * 8
+
+    # ---------------- per-kernel timing over one more step (events per launch)
+    m.profile_enable(True)
+    torch.cuda.synchronize()
+    m.step()
+    prof = m.profile_read()
+    m.profile_enable(False)
+    m.close()
+
+    # ---------------- FP64 plain path on the same inputs: speed and Ez error
+    fp64 = None
+    if not args.no_fp64:
+        c64 = cfg.copy()
+        c64.precision = PRECISIONS["fp64"]
+        c32 = cfg.copy()
+        ref = {}
+        for tag, c in (("fp64", c64), ("ours", c32)):
+            mm = Mesh(c)
+            mm.load_beam(beam)
+            mm.step()                   # identical first step from identical inputs
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            mm.step()
+            torch.cuda.synchronize()
+            ref[tag] = (mm.onaxis_ex(), time.perf_counter() - t0)
+            mm.close()
+        e64, t64 = ref["fp64"]
+        eo, _ = ref["ours"]
+        err = float(np.linalg.norm(eo - e64) / np.linalg.norm(e64))
+        fp64 = {"value": pushes_per_step / t64, "unit": UNIT, "ms_per_step": t64 * 1e3,
+                "ez_rel_l2_vs_fp64": err,
+                "speedup": (pushes_per_step / (ms / 1e3)) / (pushes_per_step / t64)}
+
+    # ---------------- roofline of the dominant kernel
+    hbm, bf16, bf16_sus, src = peaks()
+    dom = max(prof, key=lambda k: prof[k][0])
+    dom_ms, dom_n = prof[dom]
+    L, N, S, nit = cfg.nx, cfg.ny, cfg.nx_split, cfg.n_iter
+    if dom == "transform_gemm":
+        # algorithmic flops: 4 N^3 per 2-D transform (two K=N passes of 2 N^3),
+        # transforms per (layer, split): 2 + 6 + (nIter+1)*3 + nIter*6 + 7
+        per_layer = 2 + 6 + (nit + 1) * 3 + nit * 6 + 7
+        flops = 4.0 * cfg.ny * cfg.nz * (cfg.ny + cfg.nz) / 2.0 * per_layer * L * S
+        achieved = flops / (dom_ms / 1e3) / 1e12
+        roof = {"bound": "tensor", "achieved": achieved, "peak": bf16_sus, "unit": "TFLOP/s",
+                "frac": achieved / bf16_sus,
+                "peak_source": f"bf16_tflops_sustained of {src}",
+                "flops_per_launch": flops / max(dom_n, 1),
+                "executed_flop_multiplier": {"bf16x3": 3, "tf32x3": 6, "bf16x6": 6}.get(
+                    args.precision, 1)}
+    elif dom == "push_deposit":
+        # 44 B/particle for a half sub-push, 64 B for the full one (FP32 SoA)
+        b_half, b_full = 44.0, 64.0
+        nbytes = npl * (nit * b_half + b_full) * L * S
+        achieved = nbytes / (dom_ms / 1e3) / 1e9
+        roof = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                "frac": achieved / hbm, "peak_source": f"hbm_gbs of {src}",
+                "bytes_per_launch": nbytes / max(dom_n, 1)}
+    else:
+        roof = {"bound": "hbm", "achieved": None, "peak": hbm, "unit": "GB/s", "frac": None}
+    roof["kernel"] = dom
+    roof["avg_launch_us"] = dom_ms * 1e3 / max(dom_n, 1)
+    tr = traffic_record(dom, args.workload, args.precision)
+    roof["traffic"] = tr.get("bytes_per_launch") if tr else None
+    roof["kernel_ms_per_step"] = {k: round(v[0], 3) for k, v in prof.items()}
+    roof["kernel_launches_per_step"] = {k: v[1] for k, v in prof.items()}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_sample(w, args.cpu_seconds)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"{w.name}: {w.description}", "ny": cfg.ny, "nz": cfg.nz,
+                       "layers": cfg.nx, "ppc": cfg.ppc, "plasma_particles_per_layer": npl,
+                       "beam_particles": n, "n_iter": cfg.n_iter, "nx_split": cfg.nx_split,
+                       "precision": args.precision, "shape": "ngp",
+                       "step": "one beam step: beam push + full xi-march",
+                       "l2": "inputs larger than L2 (field store 6.4 GB, beam currents 2.1 GB)",
+                       "parallelism": f"replicas x{world}"},
+            "e2e": {"value": world * pushes_per_step / (e2e_ms / 1e3), "unit": UNIT,
+                    "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "ms_per_step": e2e_ms},
+            "gpu_launches": launches,
+            "roofline": roof,
+            "cpu_baseline": cpu,
+            "fp64_plain": fp64,
+            "clocks": clk,
+            "onaxis_ex_max": float(np.max(np.abs(onaxis))),
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+# ------------------------------------------------------------ reference arm
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    from tertia_b200 import workload as wl
+    w = wl.make_workload(args.workload)
+    per_step = max(1.0, min(6.0, 150.0 / max(1, args.steps + args.warmup)))
+    for _ in range(args.warmup):
+        cpu_sample(w, per_step)
+    vals = []
+    last = None
+    for _ in range(args.steps):
+        last = cpu_sample(w, per_step)
+        vals.append(last["value"])
+    value = statistics.median(vals)
+    cpu = dict(last)
+    cpu["value"] = value
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "impl": "reference",
+        "config": {"workload": f"{w.name}: {w.description}", "ny": w.cfg.ny, "nz": w.cfg.nz,
+                   "layers": w.cfg.nx, "ppc": w.cfg.ppc,
+                   "sampled": "each step times a bounded sample of layers of this workload",
+                   "parallelism": "host threads"},
+        "cpu_baseline": cpu,
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "the reference cannot be built here (needs FFTW3, HDF5, MPI); this times the "
+                "oracle's C++ restatement of its FP64 host path",
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

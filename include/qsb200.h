@@ -253,6 +253,18 @@ qs_status qs_step_host(qs_handle* h, int64_t n_beam,
  * (graph replays count their nodes). */
 int64_t qs_kernel_launches(const qs_handle* h);
 
+/* Per-kernel timing, the counterpart of the reference's stage timers
+ * (timeBegin/timeEnd/timePrint, CUDA_WRAP/cuda_wrap_control.cu:74-116, and
+ * GUESS_TIME_PRINT, movefieldshydrolinlayersplit.cpp:1159-1168).  While
+ * enabled, the march runs launch by launch (no graph replay) with a CUDA event
+ * pair around every kernel on the handle's stream. */
+qs_status qs_profile_enable(qs_handle* h, int on);
+/* Milliseconds and launch counts per kernel class since the last read:
+ * 0 push/deposit, 1 transform GEMM, 2 transform operand split, 3 spectral
+ * maps, 4 beam layer set-up, 5 beam push, 6 front seeding, 7 other.
+ * Resets the counters. */
+qs_status qs_profile_read(qs_handle* h, double* ms, int64_t* launches, int n);
+
 #ifdef __cplusplus
 }
 #endif

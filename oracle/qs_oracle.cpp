@@ -808,32 +808,64 @@ struct Oracle {
         }
         // The reference deposits into the guard ring and folds it in
         // ExchangeCurrentsSplit; depositing with the periodic fold directly
-        // is the same sum.
-        DepositSink<double> sink;
-        sink.My = My;
-        sink.Mz = Mz;
-        for (int f = 0; f < 4; f++) sink.d[f] = D[f].data();
-        std::vector<std::vector<int>> newC;
-        if (iFullStep) newC = listsC;
-        for (int k = 0; k < Mz; k++)
-            for (int j = 0; j < My; j++) {
-                size_t c = (size_t)j + (size_t)My * k;
-                for (int id : listsP[c]) {
-                    double& y = ppy[id];
-                    double& z = ppz[id];
-                    if (!(y >= 0 && y <= 1 && z >= 0 && z <= 1)) return QS_ERR_PARTICLE_RANGE;
-                    int jc = j, kc = k;
-                    push_one<double>(pp, Ps, Cs, sink, jc, kc, y, z, ppx_[id], ppy_[id],
-                                     ppz_[id], pw[id], iFullStep != 0);
-                    if (iFullStep) {
-                        int nc = jc + My * kc;
-                        newC[nc].insert(newC[nc].begin(), id);  // p->p_Next = cnew.p_Particles
-                        pcell[id] = nc;
+        // is the same sum.  Rows of cells are pushed in parallel with
+        // thread-private deposit planes; the relinks are applied afterwards
+        // in the reference's processing order (cells k-major, list order).
+        int nthreads = 1;
+#ifdef _OPENMP
+        nthreads = omp_get_max_threads();
+#endif
+        std::vector<std::vector<double>> Dt((size_t)nthreads);
+        std::vector<std::vector<std::pair<int, int>>> moves((size_t)Mz);
+        int bad = 0;
+#pragma omp parallel
+        {
+            int t = 0;
+#ifdef _OPENMP
+            t = omp_get_thread_num();
+#endif
+            std::vector<double>& Dl = Dt[(size_t)t];
+            Dl.assign(4 * nI, 0.0);
+            DepositSink<double> sink;
+            sink.My = My;
+            sink.Mz = Mz;
+            for (int f = 0; f < 4; f++) sink.d[f] = Dl.data() + f * nI;
+#pragma omp for schedule(static)
+            for (int k = 0; k < Mz; k++) {
+                for (int j = 0; j < My; j++) {
+                    size_t c = (size_t)j + (size_t)My * k;
+                    for (int id : listsP[c]) {
+                        double& y = ppy[id];
+                        double& z = ppz[id];
+                        if (!(y >= 0 && y <= 1 && z >= 0 && z <= 1)) {
+#pragma omp atomic write
+                            bad = 1;
+                            continue;
+                        }
+                        int jc = j, kc = k;
+                        push_one<double>(pp, Ps, Cs, sink, jc, kc, y, z, ppx_[id], ppy_[id],
+                                         ppz_[id], pw[id], iFullStep != 0);
+                        if (iFullStep) moves[(size_t)k].push_back({id, jc + My * kc});
                     }
                 }
-                if (iFullStep) listsP[c].clear();   // pcc.p_Particles = p_next
             }
-        if (iFullStep) listsC.swap(newC);
+        }
+        if (bad) return QS_ERR_PARTICLE_RANGE;
+        for (int t = 0; t < nthreads; t++) {
+            if (Dt[(size_t)t].empty()) continue;
+            for (int f = 0; f < 4; f++)
+                for (size_t n = 0; n < nI; n++) D[f][n] += Dt[(size_t)t][f * nI + n];
+        }
+        if (iFullStep) {
+            std::vector<std::vector<int>> newC = listsC;
+            for (int k = 0; k < Mz; k++)
+                for (auto& mv : moves[(size_t)k]) {
+                    newC[(size_t)mv.second].insert(newC[(size_t)mv.second].begin(), mv.first);
+                    pcell[mv.first] = mv.second;   // p->p_Next = cnew.p_Particles
+                }
+            for (auto& l : listsP) l.clear();    // pcc.p_Particles = p_next
+            listsC.swap(newC);
+        }
         for (int k = 0; k < Mz; k++)
             for (int j = 0; j < My; j++) {
                 size_t n = (size_t)j + (size_t)My * k, g = gidx(j, k);

@@ -177,6 +177,8 @@ def _declare(L):
                                [f64p] * 6 + [f64p])
     L.qs_kernel_launches.argtypes = [P]
     L.qs_kernel_launches.restype = C.c_int64
+    L.qs_profile_enable.argtypes = [P, C.c_int]
+    L.qs_profile_read.argtypes = [P, f64p, C.POINTER(C.c_int64), C.c_int]
 
 
 # Every symbol include/qsb200.h declares (checked against the library by a test).
@@ -189,5 +191,8 @@ EXPORTED_SYMBOLS = [
     "qs_move_beam_particles", "qs_move_all_split_layers", "qs_begin_march", "qs_layer_begin",
     "qs_move_split_layer", "qs_guess_fields", "qs_move_particles_layer", "qs_iterate_fields",
     "qs_layer_end", "qs_transform2d", "qs_transform2d_dev", "qs_step_host",
-    "qs_kernel_launches",
+    "qs_kernel_launches", "qs_profile_enable", "qs_profile_read",
 ]
+
+KERNEL_CLASSES = ["push_deposit", "transform_gemm", "transform_split", "spectral_maps",
+                  "beam_layer", "beam_push", "front_seed", "other"]

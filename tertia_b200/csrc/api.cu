@@ -41,7 +41,61 @@ struct EngineBase {
     int64_t launches = 0;
     uint64_t step_count = 0;
     double phase = 0;
-    virtual ~EngineBase() {}
+    bool capturing = false;
+    int64_t capture_count = 0;
+    // per-kernel timing (qs_profile_*): an event pair around every launch
+    bool prof = false;
+    std::vector<cudaEvent_t> ev_pool;
+    size_t ev_next = 0;
+    std::vector<std::pair<int, size_t>> prof_recs;
+    double prof_ms[KC_N] = {};
+    int64_t prof_n[KC_N] = {};
+    virtual ~EngineBase() {
+        for (cudaEvent_t e : ev_pool) cudaEventDestroy(e);
+    }
+
+    void count(int n) {
+        if (capturing) capture_count += n;
+        else launches += n;
+    }
+    cudaEvent_t ev_get() {
+        if (ev_next == ev_pool.size()) {
+            cudaEvent_t e = nullptr;
+            cudaEventCreate(&e);
+            ev_pool.push_back(e);
+        }
+        return ev_pool[ev_next++];
+    }
+    // launch through f() (returns the kernels it launched) as class cls
+    template <class F>
+    int klaunch(int cls, F&& f) {
+        if (prof && !capturing) {
+            const size_t i0 = ev_next;
+            cudaEventRecord(ev_get(), st);
+            const int n = f();
+            cudaEventRecord(ev_get(), st);
+            prof_recs.push_back({cls, i0});
+            prof_n[cls] += n;
+            count(n);
+            return n;
+        }
+        const int n = f();
+        count(n);
+        return n;
+    }
+    qs_status resolve_profile() {
+        cudaError_t e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) return cuda_fail(e, "profile synchronize");
+        for (auto& r : prof_recs) {
+            float ms = 0.f;
+            e = cudaEventElapsedTime(&ms, ev_pool[r.second], ev_pool[r.second + 1]);
+            if (e != cudaSuccess) return cuda_fail(e, "profile event");
+            prof_ms[r.first] += ms;
+        }
+        prof_recs.clear();
+        ev_next = 0;
+        return QS_OK;
+    }
 
     qs_status fail(qs_status s, const char* fmt, ...) {
         char buf[512];
@@ -156,18 +210,11 @@ struct Engine : EngineBase {
     // graph of the march
     cudaGraphExec_t gexec = nullptr;
     int64_t graph_kernels = 0;
-    bool capturing = false;
-    int64_t capture_count = 0;
     struct HostState { T *Pf, *Cf, *Psrc, *Csrc; int cur; } graph_end{};
     bool marched = false;
 
     T* bankp(int b, int p) { return bank + ((size_t)b * SP_N + p) * plane; }
     T* f3layer(int i) { return f3 + (size_t)i * 6 * plane; }
-
-    void count(int n) {
-        if (capturing) capture_count += n;
-        else launches += n;
-    }
 
     ~Engine() override {
         if (gexec) cudaGraphExecDestroy(gexec);
@@ -254,10 +301,17 @@ struct Engine : EngineBase {
     // ---------------------------------------------------------- transforms
     void xform(const DttJob<T>& job) {
         if (tc) {
-            count(tcx->run(job.nf, (const void* const*)job.in, (void* const*)job.out, job.kz,
-                           job.ky, (double)job.scale, sizeof(T), st));
+            for (int stage = 0; stage < 3; stage++)
+                klaunch(stage == 0 ? KC_SPLIT : KC_GEMM, [&] {
+                    return tcx->run_stage(stage, job.nf, (const void* const*)job.in,
+                                          (void* const*)job.out, job.kz, job.ky,
+                                          (double)job.scale, st);
+                });
         } else {
-            count(run_dtt_simt<T>(job, My, Mz, my, mz, scratch, st));
+            for (int pass = 0; pass < 2; pass++)
+                klaunch(KC_GEMM, [&] {
+                    return run_dtt_simt_pass<T>(pass, job, My, Mz, my, mz, scratch, st);
+                });
         }
     }
 
@@ -382,7 +436,7 @@ struct Engine : EngineBase {
                 for (int64_t o = 0; o < n; o += (int64_t)chunk) {
                     size_t m = (size_t)std::min<int64_t>((int64_t)chunk, n - o);
                     CK(cudaMemcpyAsync(stage_d, src[c] + o, m * 8, cudaMemcpyHostToDevice, st));
-                    count(launch_convert<T>(stage_d, 1, dst[c] + o, m, st));
+                    klaunch(KC_MISC, [&] { return launch_convert<T>(stage_d, 1, dst[c] + o, m, st); });
                 }
             }
             CK(cudaStreamSynchronize(st));
@@ -416,9 +470,12 @@ struct Engine : EngineBase {
             oz[is] = z;
         }
         const double weight = cfg.plasma_density / ppc;   // Specie::GetWeight()*dens
-        count(launch_seed_front<T>(My, Mz, ppc, oy, oz, cfg.plasma_px0, cfg.plasma_py0,
-                                   cfg.plasma_pz0, cfg.pspread_x, cfg.pspread_y, cfg.pspread_z,
-                                   weight, cfg.seed, step, pcell, py, pz, ppx, ppy, ppz, pw, st));
+        klaunch(KC_SEED, [&] {
+            return launch_seed_front<T>(My, Mz, ppc, oy, oz, cfg.plasma_px0, cfg.plasma_py0,
+                                        cfg.plasma_pz0, cfg.pspread_x, cfg.pspread_y,
+                                        cfg.pspread_z, weight, cfg.seed, step, pcell, py, pz, ppx,
+                                        ppy, ppz, pw, st);
+        });
         CK(cudaGetLastError());
         front_pending = true;
         return QS_OK;
@@ -438,7 +495,7 @@ struct Engine : EngineBase {
             size_t chunk = 8 * plane;
             for (int64_t o = 0; o < n; o += (int64_t)chunk) {
                 size_t m = (size_t)std::min<int64_t>((int64_t)chunk, n - o);
-                count(launch_convert_back<T>(src[c] + o, stage_d, m, st));
+                klaunch(KC_MISC, [&] { return launch_convert_back<T>(src[c] + o, stage_d, m, st); });
                 CK(cudaMemcpyAsync(dst[c] + o, stage_d, m * 8, cudaMemcpyDeviceToHost, st));
                 CK(cudaStreamSynchronize(st));
             }
@@ -450,12 +507,12 @@ struct Engine : EngineBase {
     // --------------------------------------------------------- plane I/O
     qs_status put_plane(T* dst, const double* src) {
         CK(cudaMemcpyAsync(stage_d, src, plane * 8, cudaMemcpyHostToDevice, st));
-        count(launch_convert<T>(stage_d, 1, dst, plane, st));
+        klaunch(KC_MISC, [&] { return launch_convert<T>(stage_d, 1, dst, plane, st); });
         CK(cudaStreamSynchronize(st));
         return QS_OK;
     }
     qs_status get_plane(const T* src, double* dst) {
-        count(launch_convert_back<T>(src, stage_d, plane, st));
+        klaunch(KC_MISC, [&] { return launch_convert_back<T>(src, stage_d, plane, st); });
         CK(cudaMemcpyAsync(dst, stage_d, plane * 8, cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
         return QS_OK;
@@ -544,7 +601,7 @@ struct Engine : EngineBase {
         a.elaser_photon = 1.2398e-4 / cfg.wavelength;
         a.synchrotron = cfg.synchrotron;
         a.err = d_err;
-        count(launch_beam_push<T>(a, st));
+        klaunch(KC_BEAM_PUSH, [&] { return launch_beam_push<T>(a, st); });
         CK(cudaGetLastError());
         return QS_OK;
     }
@@ -601,9 +658,11 @@ struct Engine : EngineBase {
         if (iSplit == 0) Pf = f3layer(iLayer + 1);
         else Pf = Cf;
         Cf = (iSplit == S - 1) ? f3layer(iLayer) : splitbuf + (size_t)(iSplit & 1) * 6 * plane;
-        count(launch_beam_layer<T>(b3 + (size_t)iLayer * 2 * plane,
-                                   b3 + (size_t)(iLayer + 1) * 2 * plane, S, iSplit, Cbeam, plane,
-                                   d_err, st));
+        klaunch(KC_BEAM_LAYER, [&] {
+            return launch_beam_layer<T>(b3 + (size_t)iLayer * 2 * plane,
+                                        b3 + (size_t)(iLayer + 1) * 2 * plane, S, iSplit, Cbeam,
+                                        plane, d_err, st);
+        });
         return QS_OK;
     }
 
@@ -637,7 +696,7 @@ struct Engine : EngineBase {
             const int kz[2] = {CC, CC}, ky[2] = {CC, CC};
             xform(job_stack(Cbeam, 2, outs, kz, ky, T(1)));
         }
-        count(launch_predictor<T>(spec_args(), st));
+        klaunch(KC_SPECTRAL, [&] { return launch_predictor<T>(spec_args(), st); });
         {   // :946-967, :1004-1061 (E, B into C; the predicted Rho and J planes
             // are cleared before any use by the push that follows)
             T* outs[6] = {Cf, Cf + plane, Cf + 2 * plane, Cf + 3 * plane, Cf + 4 * plane,
@@ -670,7 +729,7 @@ struct Engine : EngineBase {
         a.full = full;
         a.err = d_err;
         const bool precise = sizeof(T) == 4;
-        count(launch_push<T>(a, cfg.shape, precise, st));
+        klaunch(KC_PUSH, [&] { return launch_push<T>(a, cfg.shape, precise, st); });
         CK(cudaGetLastError());
         return QS_OK;
     }
@@ -692,7 +751,7 @@ struct Engine : EngineBase {
             const int kz[3] = {CC, CC, SS}, ky[3] = {CC, SS, CC};
             xform(job_stack(Csrc, 3, outs, kz, ky, T(1)));
         }
-        count(launch_corrector<T>(spec_args(), st));
+        klaunch(KC_SPECTRAL, [&] { return launch_corrector<T>(spec_args(), st); });
         if (iter < 0) {   // the last iterate also stores Dens (:1517-1602)
             T* outs[7] = {Csrc + 3 * plane, Cf, Cf + plane, Cf + 2 * plane, Cf + 3 * plane,
                           Cf + 4 * plane, Cf + 5 * plane};
@@ -752,7 +811,10 @@ struct Engine : EngineBase {
                 if ((s = move_split_layer(i, sp))) return s;
                 if ((s = layer_end(i, sp))) return s;
             }
-        count(launch_onaxis<T>(f3, L, plane, (size_t)(My / 2) + (size_t)My * (Mz / 2), onaxis_d, st));
+        klaunch(KC_MISC, [&] {
+            return launch_onaxis<T>(f3, L, plane, (size_t)(My / 2) + (size_t)My * (Mz / 2), onaxis_d,
+                                    st);
+        });
         return QS_OK;
     }
 
@@ -762,7 +824,7 @@ struct Engine : EngineBase {
             if (s) return s;
         }
         front_pending = false;
-        if (!cfg.use_graph) return march_device();
+        if (!cfg.use_graph || prof) return march_device();
         if (!gexec) {
             cudaGraph_t g = nullptr;
             CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
@@ -802,7 +864,7 @@ struct Engine : EngineBase {
             int nf = std::min(4, batch - b0);
             CK(cudaMemcpyAsync(stage_d, in + (size_t)b0 * plane, nf * plane * 8,
                                cudaMemcpyHostToDevice, st));
-            count(launch_convert<T>(stage_d, 1, stage, nf * plane, st));
+            klaunch(KC_MISC, [&] { return launch_convert<T>(stage_d, 1, stage, nf * plane, st); });
             T* outs[4];
             int kza[4], kya[4];
             for (int f = 0; f < nf; f++) {
@@ -811,7 +873,7 @@ struct Engine : EngineBase {
                 kya[f] = ky;
             }
             xform(job_stack(stage, nf, outs, kza, kya, T(1)));
-            count(launch_convert_back<T>(stage + 4 * plane, stage_d, nf * plane, st));
+            klaunch(KC_MISC, [&] { return launch_convert_back<T>(stage + 4 * plane, stage_d, nf * plane, st); });
             CK(cudaMemcpyAsync(out + (size_t)b0 * plane, stage_d, nf * plane * 8,
                                cudaMemcpyDeviceToHost, st));
             CK(cudaStreamSynchronize(st));
@@ -1169,5 +1231,35 @@ qs_status qs_step_host(qs_handle* h, int64_t n_beam, const int32_t* i, const int
 }
 
 int64_t qs_kernel_launches(const qs_handle* h) { return h ? h->e->launches : -1; }
+
+qs_status qs_profile_enable(qs_handle* h, int on) {
+    H_OR_INVALID(h);
+    qs_status s = E->resolve_profile();
+    if (s) return s;
+    E->prof = on != 0;
+    for (int c = 0; c < KC_N; c++) {
+        E->prof_ms[c] = 0;
+        E->prof_n[c] = 0;
+    }
+    return QS_OK;
+}
+
+qs_status qs_profile_read(qs_handle* h, double* ms, int64_t* launches, int n) {
+    H_OR_INVALID(h);
+    if (n < 0 || (n > 0 && (!ms || !launches))) return QS_ERR_INVALID;
+    qs_status s = E->resolve_profile();
+    if (s) return s;
+    for (int c = 0; c < n && c < KC_N; c++) {
+        ms[c] = E->prof_ms[c];
+        launches[c] = E->prof_n[c];
+        E->prof_ms[c] = 0;
+        E->prof_n[c] = 0;
+    }
+    for (int c = KC_N; c < n; c++) {
+        ms[c] = 0;
+        launches[c] = 0;
+    }
+    return QS_OK;
+}
 
 }  // extern "C"

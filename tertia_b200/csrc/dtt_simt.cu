@@ -120,26 +120,40 @@ void launch_pass<double>(const DttPassArgs<double>& a, int nf, cudaStream_t st) 
 }
 
 template <class T>
-int run_dtt_simt(const DttJob<T>& job, int ny, int nz, const DttMats<T>& my,
-                 const DttMats<T>& mz, T* scratch, cudaStream_t st) {
+int run_dtt_simt_pass(int pass, const DttJob<T>& job, int ny, int nz, const DttMats<T>& my,
+                      const DttMats<T>& mz, T* scratch, cudaStream_t st) {
     if (job.nf <= 0) return 0;
     const size_t plane = (size_t)ny * nz;
-    DttPassArgs<T> p1{}, p2{};
+    DttPassArgs<T> a{};
     for (int f = 0; f < job.nf; f++) {
-        p1.in[f] = job.in[f];
-        p1.mat[f] = my.m[job.ky[f]];
-        p1.out[f] = scratch + f * plane;
-        p2.in[f] = scratch + f * plane;
-        p2.mat[f] = mz.m[job.kz[f]];
-        p2.out[f] = job.out[f];
+        if (pass == 0) {
+            a.in[f] = job.in[f];
+            a.mat[f] = my.m[job.ky[f]];
+            a.out[f] = scratch + f * plane;
+        } else {
+            a.in[f] = scratch + f * plane;
+            a.mat[f] = mz.m[job.kz[f]];
+            a.out[f] = job.out[f];
+        }
     }
-    p1.R = nz; p1.K = ny; p1.scale = T(1);
-    p2.R = ny; p2.K = nz; p2.scale = job.scale;
-    launch_pass<T>(p1, job.nf, st);
-    launch_pass<T>(p2, job.nf, st);
-    return 2;
+    if (pass == 0) { a.R = nz; a.K = ny; a.scale = T(1); }
+    else { a.R = ny; a.K = nz; a.scale = job.scale; }
+    launch_pass<T>(a, job.nf, st);
+    return 1;
 }
 
+template <class T>
+int run_dtt_simt(const DttJob<T>& job, int ny, int nz, const DttMats<T>& my,
+                 const DttMats<T>& mz, T* scratch, cudaStream_t st) {
+    return run_dtt_simt_pass<T>(0, job, ny, nz, my, mz, scratch, st) +
+           run_dtt_simt_pass<T>(1, job, ny, nz, my, mz, scratch, st);
+}
+
+template int run_dtt_simt_pass<float>(int, const DttJob<float>&, int, int, const DttMats<float>&,
+                                      const DttMats<float>&, float*, cudaStream_t);
+template int run_dtt_simt_pass<double>(int, const DttJob<double>&, int, int,
+                                       const DttMats<double>&, const DttMats<double>&, double*,
+                                       cudaStream_t);
 template int run_dtt_simt<float>(const DttJob<float>&, int, int, const DttMats<float>&,
                                  const DttMats<float>&, float*, cudaStream_t);
 template int run_dtt_simt<double>(const DttJob<double>&, int, int, const DttMats<double>&,

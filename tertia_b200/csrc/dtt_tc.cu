@@ -538,33 +538,47 @@ public:
             tcx::dtt_tc_kernel<0, 3, 3><<<grid, tcx::THREADS, smem_bytes, st>>>(A, B, p);
     }
 
+    int run_stage(int stage, int nf, const void* const* in, void* const* out, const int* kz,
+                  const int* ky, double scale, cudaStream_t st) override {
+        if (nf <= 0 || nf > kMaxXfFields) return 0;
+        const size_t plane = (size_t)ny * nz;
+        if (stage == 0) {
+            tcx::PtrPack pk{};
+            for (int f = 0; f < nf; f++) pk.p[f] = (const float*)in[f];
+            dim3 sg((unsigned)((plane + 255) / 256), nf);
+            if (kind == 0)
+                tcx::split_planes_kernel_v<0><<<sg, 256, 0, st>>>(pk, nf, plane, nsplit, splitA);
+            else
+                tcx::split_planes_kernel_v<1><<<sg, 256, 0, st>>>(pk, nf, plane, nsplit, splitA);
+            return 1;
+        }
+        tcx::Params p{};
+        p.nsplit = nsplit;
+        p.nterm = nterm;
+        for (int t = 0; t < 6; t++) { p.ta[t] = ta[t]; p.tb[t] = tb[t]; }
+        p.err = err;
+        if (stage == 1) {   // along y: splitA (nz x ny rows) -> splitB, transposed
+            p.R = nz; p.K = ny;
+            for (int f = 0; f < nf; f++) p.kind[f] = ky[f];
+            p.rowsA = 8 * nz; p.rowsB = 2 * ny;
+            p.out_split = 1; p.out_base = splitB; p.scale = 1.0f;
+            launch_gemm(mapA1, mapB1, p, nf, st);
+        } else {            // along z: splitB (ny x nz rows) -> FP32 destination
+            p.R = ny; p.K = nz;
+            for (int f = 0; f < nf; f++) { p.kind[f] = kz[f]; p.out[f] = (float*)out[f]; }
+            p.rowsA = 8 * ny; p.rowsB = 2 * nz;
+            p.out_split = 0; p.out_base = nullptr; p.scale = (float)scale;
+            launch_gemm(mapA2, mapB2, p, nf, st);
+        }
+        return 1;
+    }
+
     int run(int nf, const void* const* in, void* const* out, const int* kz, const int* ky,
             double scale, int elem_size, cudaStream_t st) override {
-        if (nf <= 0) return 0;
-        if (elem_size != 4 || nf > kMaxXfFields) return 0;
-        const size_t plane = (size_t)ny * nz;
-        tcx::PtrPack pk{};
-        for (int f = 0; f < nf; f++) pk.p[f] = (const float*)in[f];
-        dim3 sg((unsigned)((plane + 255) / 256), nf);
-        if (kind == 0) tcx::split_planes_kernel_v<0><<<sg, 256, 0, st>>>(pk, nf, plane, nsplit, splitA);
-        else tcx::split_planes_kernel_v<1><<<sg, 256, 0, st>>>(pk, nf, plane, nsplit, splitA);
-
-        tcx::Params p1{};
-        p1.R = nz; p1.K = ny;
-        p1.nsplit = nsplit; p1.nterm = nterm;
-        for (int t = 0; t < 6; t++) { p1.ta[t] = ta[t]; p1.tb[t] = tb[t]; }
-        for (int f = 0; f < nf; f++) p1.kind[f] = ky[f];
-        p1.rowsA = 8 * nz; p1.rowsB = 2 * ny;
-        p1.out_split = 1; p1.out_base = splitB; p1.scale = 1.0f; p1.err = err;
-        launch_gemm(mapA1, mapB1, p1, nf, st);
-
-        tcx::Params p2 = p1;
-        p2.R = ny; p2.K = nz;
-        for (int f = 0; f < nf; f++) { p2.kind[f] = kz[f]; p2.out[f] = (float*)out[f]; }
-        p2.rowsA = 8 * ny; p2.rowsB = 2 * nz;
-        p2.out_split = 0; p2.out_base = nullptr; p2.scale = (float)scale;
-        launch_gemm(mapA2, mapB2, p2, nf, st);
-        return 3;
+        if (elem_size != 4) return 0;
+        int n = 0;
+        for (int s = 0; s < 3; s++) n += run_stage(s, nf, in, out, kz, ky, scale, st);
+        return n;
     }
 };
 

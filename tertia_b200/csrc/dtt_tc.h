@@ -16,6 +16,10 @@ public:
     // planes stored consecutively from in[0]; returns the kernels launched.
     virtual int run(int nf, const void* const* in, void* const* out, const int* kz,
                     const int* ky, double scale, int elem_size, cudaStream_t st) = 0;
+    // the three launches of run(), separately (for per-kernel timing):
+    // stage 0 splits the inputs, stage 1 is the y pass, stage 2 the z pass.
+    virtual int run_stage(int stage, int nf, const void* const* in, void* const* out,
+                          const int* kz, const int* ky, double scale, cudaStream_t st) = 0;
 };
 
 }  // namespace qs

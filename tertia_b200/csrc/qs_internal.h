@@ -46,6 +46,15 @@ int launch_convert_back(const T* src, double* dst, size_t n, cudaStream_t st);
 template <class T>
 int run_dtt_simt(const DttJob<T>& job, int ny, int nz, const DttMats<T>& my,
                  const DttMats<T>& mz, T* scratch, cudaStream_t st);
+template <class T>
+int run_dtt_simt_pass(int pass, const DttJob<T>& job, int ny, int nz, const DttMats<T>& my,
+                      const DttMats<T>& mz, T* scratch, cudaStream_t st);
+
+// kernel classes of the per-kernel timing (qs_profile_read)
+enum KernelClass {
+    KC_PUSH = 0, KC_GEMM = 1, KC_SPLIT = 2, KC_SPECTRAL = 3, KC_BEAM_LAYER = 4,
+    KC_BEAM_PUSH = 5, KC_SEED = 6, KC_MISC = 7, KC_N = 8
+};
 
 template <class T>
 int launch_push(const PushArgs<T>& a, int shape, bool precise, cudaStream_t st);

@@ -76,6 +76,17 @@ class Mesh:
     def kernel_launches(self) -> int:
         return int(self._L.qs_kernel_launches(self._h))
 
+    def profile_enable(self, on: bool = True):
+        self._chk(self._L.qs_profile_enable(self._h, int(on)), "qs_profile_enable")
+
+    def profile_read(self) -> dict:
+        n = len(abi.KERNEL_CLASSES)
+        ms = np.zeros(n)
+        cnt = np.zeros(n, dtype=np.int64)
+        self._chk(self._L.qs_profile_read(self._h, _p(ms, C.c_double), _p(cnt, C.c_int64), n),
+                  "qs_profile_read")
+        return {k: (float(ms[i]), int(cnt[i])) for i, k in enumerate(abi.KERNEL_CLASSES)}
+
     # -------------------------------------------------------------- state
     def load_beam(self, b: dict):
         n = len(b["x"])
@@ -202,13 +213,15 @@ class Mesh:
                                          _p(out, C.c_double)), "qs_transform2d")
         return out
 
-    def step_host(self, b: dict, want_beam: bool = True):
-        """One step through host buffers (beam in, beam and on-axis Ex out)."""
+    def step_host(self, b: dict, want_beam: bool = True, out: dict | None = None):
+        """One step through host buffers (beam in, beam and on-axis Ex out).
+        `out` may supply the output arrays (e.g. views of pinned memory)."""
         n = len(b["x"])
         ii, jj, kk = (_i32(b[k]) for k in "ijk")
         f = [_f64(b[k]) for k in ("x", "y", "z", "px", "py", "pz", "w")]
-        out = {k: np.empty(n, dtype=np.int32) for k in "ijk"}
-        out.update({k: np.empty(n) for k in ("x", "y", "z", "px", "py", "pz")})
+        if out is None:
+            out = {k: np.empty(n, dtype=np.int32) for k in "ijk"}
+            out.update({k: np.empty(n) for k in ("x", "y", "z", "px", "py", "pz")})
         ex = np.empty(self.cfg.nx)
         outs_i = [_p(out[k], C.c_int32) if want_beam else None for k in "ijk"]
         outs_f = [_p(out[k], C.c_double) if want_beam else None
