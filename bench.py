@@ -37,7 +37,7 @@ if ROOT not in sys.path:
 METRIC = "particle-layer pushes/s"
 UNIT = "pushes/s"
 CLASSES = ["push_deposit", "transform_gemm", "transform_split", "spectral_maps",
-           "beam_layer", "beam_push", "front_seed", "other"]
+           "beam_spectra", "beam_push", "front_seed", "other"]
 
 
 def parse():

@@ -195,4 +195,4 @@ EXPORTED_SYMBOLS = [
 ]
 
 KERNEL_CLASSES = ["push_deposit", "transform_gemm", "transform_split", "spectral_maps",
-                  "beam_layer", "beam_push", "front_seed", "other"]
+                  "beam_spectra", "beam_push", "front_seed", "other"]

@@ -17,8 +17,9 @@ BASE = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "
         "-Xptxas", "-warn-spills"]
 # Translation units whose arithmetic must follow the reference's expression
 # order without FMA contraction (bit-exact FP64 against the oracle).
-NO_FMAD = {"push.cu", "spectral.cu", "beam.cu"}
-SOURCES = ["api.cu", "dtt_simt.cu", "dtt_tc.cu", "push.cu", "spectral.cu", "beam.cu"]
+NO_FMAD = {"push_f64.cu", "spectral.cu", "beam.cu"}
+SOURCES = ["api.cu", "dtt_simt.cu", "dtt_tc.cu", "push_f64.cu", "push_f32.cu", "spectral.cu",
+           "beam.cu"]
 
 
 def nvcc() -> str:

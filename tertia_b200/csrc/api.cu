@@ -186,7 +186,11 @@ struct Engine : EngineBase {
     T* Cf = nullptr;
     T* Psrc = nullptr;
     T* Csrc = nullptr;
-    T* Cbeam = nullptr;         // 2 planes
+    T* Cbeam = nullptr;         // 2 planes (C-layer beam currents, on request)
+    T* sb3 = nullptr;           // (nx+1) layers x 2 planes: spectra of RhoBeam, JxBeam
+    bool sb3_valid = false;
+    bool in_march = false;      // inside MoveAllSplitLayers (skip output-only work)
+    int cur_layer = -1, cur_split = 0;
     T* bank = nullptr;          // 2 x SP_N planes
     int cur = 0;                // bank index of the current (layer, split)
     bool p_valid = true;        // P-bank spectra match the P real planes
@@ -219,7 +223,7 @@ struct Engine : EngineBase {
     ~Engine() override {
         if (gexec) cudaGraphExecDestroy(gexec);
         delete tcx;
-        void* ptrs[] = {f3, b3, src3, splitbuf, srcbuf, Cbeam, bank, scratch, mats, onaxis_d,
+        void* ptrs[] = {f3, b3, src3, splitbuf, srcbuf, Cbeam, sb3, bank, scratch, mats, onaxis_d,
                         stage, stage_d, pcell, py, pz, ppx, ppy, ppz, pw, bi, bj, bk, bx, by, bz,
                         bpx, bpy, bpz, bw, d_err};
         for (void* p : ptrs)
@@ -255,6 +259,9 @@ struct Engine : EngineBase {
         CK(cudaMemset(srcbuf, 0, 8 * plane * sizeof(T)));
         if ((s = alloc(&Cbeam, 2 * plane, "beam layer"))) return s;
         CK(cudaMemset(Cbeam, 0, 2 * plane * sizeof(T)));
+        if ((s = alloc(&sb3, (size_t)(L + 1) * 2 * plane, "beam spectra"))) return s;
+        CK(cudaMemset(sb3, 0, (size_t)(L + 1) * 2 * plane * sizeof(T)));
+        sb3_valid = true;
         if ((s = alloc(&bank, 2 * SP_N * plane, "spectral banks"))) return s;
         CK(cudaMemset(bank, 0, 2 * SP_N * plane * sizeof(T)));
         if ((s = alloc(&scratch, 8 * plane, "transform scratch"))) return s;
@@ -524,8 +531,6 @@ struct Engine : EngineBase {
         if (field >= QS_F_EX && field <= QS_F_BZ) return F + (size_t)field * plane;
         if (field >= QS_F_JX && field <= QS_F_JZ) return Sr + (size_t)(field - QS_F_JX) * plane;
         if (field == QS_F_DENS) return Sr + 3 * plane;
-        if (which == QS_LAYER_C && field == QS_F_RHOBEAM) return Cbeam;
-        if (which == QS_LAYER_C && field == QS_F_JXBEAM) return Cbeam + plane;
         return nullptr;
     }
 
@@ -533,7 +538,10 @@ struct Engine : EngineBase {
         if ((which != QS_LAYER_P && which != QS_LAYER_C) || !data)
             return fail(QS_ERR_INVALID, "qs_set_layer: bad arguments");
         T* p = layer_plane(which, field);
-        if (!p) return fail(QS_ERR_INVALID, "qs_set_layer: field %d not settable", field);
+        if (!p)
+            return fail(QS_ERR_INVALID,
+                        "qs_set_layer: field %d is not settable (the C-layer beam currents derive "
+                        "from the beam-current store: use qs_set_beam_currents)", field);
         if (which == QS_LAYER_P) p_valid = false;
         return put_plane(p, data);
     }
@@ -541,6 +549,16 @@ struct Engine : EngineBase {
     qs_status get_layer(int which, int field, double* out) override {
         if ((which != QS_LAYER_P && which != QS_LAYER_C) || !out)
             return fail(QS_ERR_INVALID, "qs_get_layer: bad arguments");
+        if (which == QS_LAYER_C && (field == QS_F_RHOBEAM || field == QS_F_JXBEAM)) {
+            // derived from the beam-current store at the current (layer, split)
+            const int i = cur_layer < 0 ? L - 1 : cur_layer;
+            klaunch(KC_MISC, [&] {
+                return launch_beam_layer<T>(b3 + (size_t)i * 2 * plane,
+                                            b3 + (size_t)(i + 1) * 2 * plane, S, cur_split, Cbeam,
+                                            plane, d_err, st);
+            });
+            return get_plane(Cbeam + (field == QS_F_JXBEAM ? plane : 0), out);
+        }
         T* p = layer_plane(which, field);
         if (!p) return fail(QS_ERR_INVALID, "qs_get_layer: field %d not readable", field);
         return get_plane(p, out);
@@ -566,7 +584,41 @@ struct Engine : EngineBase {
     qs_status set_beam_currents(int field, int layer, const double* data) override {
         T* p = beam_plane(field, layer);
         if (!p || !data) return fail(QS_ERR_INVALID, "qs_set_beam_currents: bad arguments");
+        sb3_valid = false;
         return put_plane(p, data);
+    }
+
+    // Spectra of every layer's beam currents (RhoBeam, JxBeam: REDFT11 x
+    // REDFT11, movefieldshydrolinlayersplit.cpp:717-718) in large batches,
+    // once per beam push instead of once per layer; plus the |JxBeam| > 10
+    // check of :618-621.
+    qs_status beam_spectra() {
+        klaunch(KC_BEAM_SPECTRA, [&] { return launch_beam_check<T>(b3, L + 1, plane, d_err, st); });
+        const int np = 2 * (L + 1);
+        if (tc) {
+            for (int b0 = 0; b0 < np; b0 += 64) {
+                const int nf = std::min(64, np - b0);
+                const float* in = (const float*)(b3 + (size_t)b0 * plane);
+                float* out = (float*)(sb3 + (size_t)b0 * plane);
+                klaunch(KC_SPLIT, [&] { return tcx->run_batched(in, out, nf, 1.0, 0, st); });
+                klaunch(KC_GEMM, [&] { return tcx->run_batched(in, out, nf, 1.0, 1, st); });
+                klaunch(KC_GEMM, [&] { return tcx->run_batched(in, out, nf, 1.0, 2, st); });
+            }
+        } else {
+            for (int b0 = 0; b0 < np; b0 += kMaxXfFields) {
+                const int nf = std::min(kMaxXfFields, np - b0);
+                T* outs[kMaxXfFields];
+                int kz[kMaxXfFields], ky[kMaxXfFields];
+                for (int f = 0; f < nf; f++) {
+                    outs[f] = sb3 + (size_t)(b0 + f) * plane;
+                    kz[f] = ky[f] = CC;
+                }
+                xform(job_stack(b3 + (size_t)b0 * plane, nf, outs, kz, ky, T(1)));
+            }
+        }
+        CK(cudaGetLastError());
+        sb3_valid = true;
+        return QS_OK;
     }
     qs_status get_beam_currents(int field, int layer, double* out) override {
         T* p = beam_plane(field, layer);
@@ -603,11 +655,13 @@ struct Engine : EngineBase {
         a.err = d_err;
         klaunch(KC_BEAM_PUSH, [&] { return launch_beam_push<T>(a, st); });
         CK(cudaGetLastError());
-        return QS_OK;
+        return beam_spectra();
     }
 
     // --------------------------------------------------------- the march
-    SpecArgs<T> spec_args() {
+    T* sbp(int layer, int q) { return sb3 + ((size_t)layer * 2 + q) * plane; }
+
+    SpecArgs<T> spec_args(int iLayer, int iSplit) {
         SpecArgs<T> a{};
         a.ny = My; a.nz = Mz;
         const double Ylength = My * cfg.hy, Zlength = Mz * cfg.hz;
@@ -620,13 +674,67 @@ struct Engine : EngineBase {
         const int pb = cur ^ 1, cb = cur;
         a.RhoP = bankp(pb, SP_RHO); a.ExP = bankp(pb, SP_EX); a.EyP = bankp(pb, SP_EY);
         a.EzP = bankp(pb, SP_EZ); a.JxP = bankp(pb, SP_JX); a.JyP = bankp(pb, SP_JY);
-        a.JzP = bankp(pb, SP_JZ); a.Rbp = bankp(pb, SP_RB);
-        a.Rb = bankp(cb, SP_RB); a.Jxb = bankp(cb, SP_JXB);
+        a.JzP = bankp(pb, SP_JZ);
+        // beam of this (layer, split): layers iLayer and iLayer+1 weighted (S-s)/S, s/S
+        a.Rb0 = sbp(iLayer, 0); a.Rb1 = sbp(iLayer + 1, 0);
+        a.Jxb0 = sbp(iLayer, 1); a.Jxb1 = sbp(iLayer + 1, 1);
+        a.wb0 = (T)((double)(S - iSplit) / S);
+        a.wb1 = (T)((double)iSplit / S);
+        // beam of the previous (layer, split); zero on the head layer (:430-445)
+        a.Rbp0 = a.Rb0; a.Rbp1 = a.Rb1; a.wp0 = T(0); a.wp1 = T(0);
+        if (iLayer < L - 1) {
+            if (iSplit > 0) {
+                a.wp0 = (T)((double)(S - iSplit + 1) / S);
+                a.wp1 = (T)((double)(iSplit - 1) / S);
+            } else {
+                a.Rbp0 = sbp(iLayer + 1, 0);
+                a.Rbp1 = sbp(std::min(iLayer + 2, L), 0);
+                a.wp0 = (T)(1.0 / S);
+                a.wp1 = (T)((double)(S - 1) / S);
+            }
+        }
         a.Jx = bankp(cb, SP_JX); a.Jy = bankp(cb, SP_JY); a.Jz = bankp(cb, SP_JZ);
         a.Rho = bankp(cb, SP_RHO);
         a.Ex = bankp(cb, SP_EX); a.Ey = bankp(cb, SP_EY); a.Ez = bankp(cb, SP_EZ);
         a.Bx = bankp(cb, SP_BX); a.By = bankp(cb, SP_BY); a.Bz = bankp(cb, SP_BZ);
+        a.write_b = tc ? 0 : 1;
+        if (tc) {
+            int ns = 0, kd = 0;
+            size_t ts = 0;
+            void* base = nullptr;
+            tcx->split_target(&base, &ns, &kd, &ts);
+            a.split = base; a.nsplit = ns; a.split_kind = kd; a.tstride = ts;
+        }
         return a;
+    }
+
+    // inverse transforms of the spectral E, B (+ Rho) into the C layer
+    void inverse_EB(bool with_rho) {
+        const int cb = cur;
+        const int nf = with_rho ? 7 : 6;
+        T* outs[7] = {Cf, Cf + plane, Cf + 2 * plane, Cf + 3 * plane, Cf + 4 * plane,
+                      Cf + 5 * plane, Csrc + 3 * plane};
+        const int kz[7] = {CC, CC, SS, SS, SS, CC, CC};
+        const int ky[7] = {CC, SS, CC, SS, CC, SS, CC};
+        if (tc) {   // the spectral kernel already wrote the split operand
+            for (int stage = 1; stage <= 2; stage++)
+                klaunch(KC_GEMM, [&] {
+                    return tcx->run_stage(stage, nf, nullptr, (void* const*)outs, kz, ky,
+                                          (double)inv_scale(), st);
+                });
+        } else {
+            DttJob<T> j;
+            j.nf = nf;
+            const int src[7] = {SP_EX, SP_EY, SP_EZ, SP_BX, SP_BY, SP_BZ, SP_RHO};
+            for (int f = 0; f < nf; f++) {
+                j.in[f] = bankp(cb, src[f]);
+                j.out[f] = outs[f];
+                j.kz[f] = kz[f];
+                j.ky[f] = ky[f];
+            }
+            j.scale = inv_scale();
+            xform(j);
+        }
     }
 
     qs_status begin_march() override {
@@ -648,6 +756,8 @@ struct Engine : EngineBase {
         p_valid = true;
         Pf = f3layer(L);
         Cf = f3layer(L - 1);
+        cur_layer = -1;
+        cur_split = 0;
         marched = true;
         return QS_OK;
     }
@@ -658,22 +768,20 @@ struct Engine : EngineBase {
         if (iSplit == 0) Pf = f3layer(iLayer + 1);
         else Pf = Cf;
         Cf = (iSplit == S - 1) ? f3layer(iLayer) : splitbuf + (size_t)(iSplit & 1) * 6 * plane;
-        klaunch(KC_BEAM_LAYER, [&] {
-            return launch_beam_layer<T>(b3 + (size_t)iLayer * 2 * plane,
-                                        b3 + (size_t)(iLayer + 1) * 2 * plane, S, iSplit, Cbeam,
-                                        plane, d_err, st);
-        });
+        cur_layer = iLayer;
+        cur_split = iSplit;
         return QS_OK;
     }
 
     qs_status guess(int iLayer, int iSplit) override {
-        const int pb = cur ^ 1, cb = cur;
-        if (iLayer == L - 1) {
-            // :430-445 the head layer zeroes the spectral arrays; the P
-            // spectra are then rebuilt from P (zero on split 0)
-            CK(cudaMemsetAsync(bankp(pb, SP_RB), 0, plane * sizeof(T), st));
-            if (iSplit == 0 && p_valid)
-                CK(cudaMemsetAsync(bankp(pb, 0), 0, (size_t)SP_RB * plane * sizeof(T), st));
+        const int pb = cur ^ 1;
+        if (!sb3_valid) {
+            qs_status s = beam_spectra();
+            if (s) return s;
+        }
+        if (iLayer == L - 1 && iSplit == 0 && p_valid) {
+            // :430-445 the head layer starts from zero spectra (P is layer nx = 0)
+            CK(cudaMemsetAsync(bankp(pb, 0), 0, (size_t)SP_RB * plane * sizeof(T), st));
         }
         if (!p_valid) {
             // P planes were set from outside: transform them like :717-743
@@ -684,27 +792,16 @@ struct Engine : EngineBase {
                                Psrc + plane, Psrc + 2 * plane};
             const int kz[7] = {CC, CC, CC, SS, CC, CC, SS};
             const int ky[7] = {CC, CC, SS, CC, CC, SS, CC};
-            // stack into stage then transform
             for (int f = 0; f < 7; f++)
                 CK(cudaMemcpyAsync(stage + (size_t)f * plane, ins[f], plane * sizeof(T),
                                    cudaMemcpyDeviceToDevice, st));
             xform(job_stack(stage, 7, outs, kz, ky, T(1)));
             p_valid = true;
         }
-        {   // beam spectra of C (:717-718)
-            T* outs[2] = {bankp(cb, SP_RB), bankp(cb, SP_JXB)};
-            const int kz[2] = {CC, CC}, ky[2] = {CC, CC};
-            xform(job_stack(Cbeam, 2, outs, kz, ky, T(1)));
-        }
-        klaunch(KC_SPECTRAL, [&] { return launch_predictor<T>(spec_args(), st); });
-        {   // :946-967, :1004-1061 (E, B into C; the predicted Rho and J planes
-            // are cleared before any use by the push that follows)
-            T* outs[6] = {Cf, Cf + plane, Cf + 2 * plane, Cf + 3 * plane, Cf + 4 * plane,
-                          Cf + 5 * plane};
-            const int kz[6] = {CC, CC, SS, SS, SS, CC};
-            const int ky[6] = {CC, SS, CC, SS, CC, SS};
-            xform(job_stack(bankp(cb, SP_EX), 6, outs, kz, ky, inv_scale()));
-        }
+        klaunch(KC_SPECTRAL, [&] { return launch_predictor<T>(spec_args(iLayer, iSplit), st); });
+        // :946-967, :1004-1061: E, B into C (the predicted Rho and J planes are
+        // cleared before any use by the push that follows)
+        inverse_EB(false);
         CK(cudaGetLastError());
         return QS_OK;
     }
@@ -726,6 +823,10 @@ struct Engine : EngineBase {
         a.djx0 = (T)cfg.plasma_djx0; a.djy0 = (T)cfg.plasma_djy0; a.djz0 = (T)cfg.plasma_djz0;
         a.drho0 = (T)cfg.plasma_drho0;
         a.bxe = (T)cfg.bx_ext; a.bye = (T)cfg.by_ext; a.bze = (T)cfg.bz_ext;
+        a.sE = (T)(cfg.plasma_q2m * (cfg.hx / S) / 2.0);
+        a.hxhy = (T)((cfg.hx / S) / cfg.hy);
+        a.hxhz = (T)((cfg.hx / S) / cfg.hz);
+        a.invMy = 1.0f / (float)My;
         a.full = full;
         a.err = d_err;
         const bool precise = sizeof(T) == 4;
@@ -735,7 +836,6 @@ struct Engine : EngineBase {
     }
 
     qs_status iterate(int iLayer, int iSplit, int iter, double* rel_err) override {
-        (void)iLayer; (void)iSplit;
         const int cb = cur;
         std::vector<double> oldE;
         if (rel_err) {
@@ -751,20 +851,13 @@ struct Engine : EngineBase {
             const int kz[3] = {CC, CC, SS}, ky[3] = {CC, SS, CC};
             xform(job_stack(Csrc, 3, outs, kz, ky, T(1)));
         }
-        klaunch(KC_SPECTRAL, [&] { return launch_corrector<T>(spec_args(), st); });
-        if (iter < 0) {   // the last iterate also stores Dens (:1517-1602)
-            T* outs[7] = {Csrc + 3 * plane, Cf, Cf + plane, Cf + 2 * plane, Cf + 3 * plane,
-                          Cf + 4 * plane, Cf + 5 * plane};
-            const int kz[7] = {CC, CC, CC, SS, SS, SS, CC};
-            const int ky[7] = {CC, CC, SS, CC, SS, CC, SS};
-            xform(job_stack(bankp(cb, SP_RHO), 7, outs, kz, ky, inv_scale()));
-        } else {
-            T* outs[6] = {Cf, Cf + plane, Cf + 2 * plane, Cf + 3 * plane, Cf + 4 * plane,
-                          Cf + 5 * plane};
-            const int kz[6] = {CC, CC, SS, SS, SS, CC};
-            const int ky[6] = {CC, SS, CC, SS, CC, SS};
-            xform(job_stack(bankp(cb, SP_EX), 6, outs, kz, ky, inv_scale()));
-        }
+        // the last iterate stores Dens too (:1517-1602); inside the march that
+        // real-space density is output only, so it is kept when sources are stored
+        const bool want_rho = iter < 0 && (!in_march || src3 != nullptr);
+        SpecArgs<T> a = spec_args(iLayer, iSplit);
+        a.split_rho = want_rho ? 1 : 0;
+        klaunch(KC_SPECTRAL, [&] { return launch_corrector<T>(a, st); });
+        inverse_EB(want_rho);
         CK(cudaGetLastError());
         if (rel_err) {
             std::vector<double> nw(plane);
@@ -803,6 +896,13 @@ struct Engine : EngineBase {
     }
 
     qs_status march_device() {
+        in_march = true;
+        qs_status s = march_device_body();
+        in_march = false;
+        return s;
+    }
+
+    qs_status march_device_body() {
         qs_status s = begin_march_device();
         if (s) return s;
         for (int i = L - 1; i >= 0; i--)
@@ -824,6 +924,10 @@ struct Engine : EngineBase {
             if (s) return s;
         }
         front_pending = false;
+        if (!sb3_valid) {
+            qs_status s = beam_spectra();
+            if (s) return s;
+        }
         if (!cfg.use_graph || prof) return march_device();
         if (!gexec) {
             cudaGraph_t g = nullptr;

@@ -29,31 +29,32 @@
 #include <cudaTypedefs.h>
 #include <cuda_bf16.h>
 #include <cmath>
+#include <algorithm>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
 #include "dtt_tc.h"
 #include "qs_common.cuh"
+#include "split.cuh"
 
 namespace qs {
 namespace tcx {
 
-constexpr int BM = 128;
-constexpr int BN = 64;
-constexpr int THREADS = 128;
-constexpr int TMEM_COLS = 64;
+constexpr int BM = 128;   // output rows per tile (matrix rows, MMA M)
+constexpr int BN_MAX = 128;   // output columns per tile (data rows, MMA N): 64 or 128
 constexpr uint32_t SPIN_LIMIT = 1u << 22;
 
 struct Params {
-    int R, K;              // rows per field, row length (= transform size)
-    int nsplit;            // operand split terms
-    int nterm;             // product terms
-    int ta[6], tb[6];      // split index of A and B for each product term
-    int kind[kMaxXfFields];
-    int rowsA;             // rows of one split term in the A map (8 * R)
-    int rowsB;             // rows of one split term in the B map (2 * K)
-    int out_split;         // 1: write split planes to out_base
-    void* out_base;        // [term][8][K][R]
+    int R, K;              // data rows per field (output columns), transform size
+    int data_rows;         // rows of one split term in the data map (nfmax * R)
+    int mat_rows;          // rows of one split term in the matrix map (2 * K)
+    int nfmax;             // field capacity of the split operand buffers
+    unsigned long long kindmask;  // bit f: matrix kind (REDFT11 / RODFT11) of field f
+    int promo;             // k-blocks accumulated in TMEM before an FP32 drain
+    int out_split;         // 1: write split terms to out_base [term][nfmax][K][R]
+    int out_contig;        // 1: field f writes to out[0] + f * R * K
+    void* out_base;
     float* out[kMaxXfFields];
     float scale;
     int* err;
@@ -156,63 +157,93 @@ __device__ __forceinline__ void tmem_wait_ld() {
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
-__device__ __forceinline__ float tf32_rna(float x) {
-    uint32_t r;
-    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
-    return __uint_as_float(r);
+#ifdef QS_TC_TRACE
+// stage timestamps of CTA (0,0,0), read by a probe build only
+__device__ long long g_tc_trace[256];
+__device__ __forceinline__ void trace(int slot) {
+    if (blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0 && slot < 256)
+        g_tc_trace[slot] = clock64();
 }
-
-// split an FP32 value into n terms of the low-precision type
-template <int KIND>
-__device__ __forceinline__ void split_value(float v, int n, float (&t)[3]) {
-    float r = v;
-#pragma unroll
-    for (int s = 0; s < 3; s++) {
-        if (s < n) {
-            float h = (KIND == 0) ? __bfloat162float(__float2bfloat16_rn(r)) : tf32_rna(r);
-            t[s] = h;
-            r = r - h;
-        } else {
-            t[s] = 0.f;
-        }
-    }
-}
+#else
+__device__ __forceinline__ void trace(int) {}
+#endif
 
 // ------------------------------------------------------------ the GEMM
-template <int KIND, int NSPLIT, int STAGES>
-__global__ void __launch_bounds__(THREADS, 1)
-    dtt_tc_kernel(const __grid_constant__ CUtensorMap mapA,
-                  const __grid_constant__ CUtensorMap mapB, const Params p) {
+// Product terms (matrix split index, data split index), small terms first.
+template <int NSPLIT>
+struct Terms;
+template <>
+struct Terms<2> {
+    static constexpr int N = 3;
+    __device__ static constexpr int a(int t) { return t == 0 ? 0 : (t == 1 ? 1 : 0); }
+    __device__ static constexpr int b(int t) { return t == 0 ? 1 : 0; }
+};
+template <>
+struct Terms<3> {
+    static constexpr int N = 6;
+    // (0,2) (1,1) (2,0) (0,1) (1,0) (0,0)
+    __device__ static constexpr int a(int t) {
+        return t == 0 ? 0 : t == 1 ? 1 : t == 2 ? 2 : t == 3 ? 0 : t == 4 ? 1 : 0;
+    }
+    __device__ static constexpr int b(int t) {
+        return t == 0 ? 2 : t == 1 ? 1 : t == 2 ? 0 : t == 3 ? 1 : t == 4 ? 0 : 0;
+    }
+};
+
+// Tile: 128 output rows n (rows of the symmetric matrix, the MMA's M side)
+// x 64 output columns m (rows of one field's data, the MMA's N side):
+//   D[n][m] = sum_k mat[n][k] * data_f[m][k] = (data_f . mat)^T [n][m]
+// so TMEM lane = output row and every epilogue thread owns 64 contiguous
+// outputs.  Warps: 0 = TMA producer, 1 = MMA issuer, 2..5 = epilogue (TMEM
+// lane quarter = warp % 4).  The accumulator is double buffered in TMEM and
+// drained every `promo` k-blocks into FP32 registers (partial sums of at most
+// promo*BK products live in the tensor-core accumulator).
+constexpr int EPI_WARPS = 8;   // two per TMEM lane quarter, 64 columns each
+constexpr int THREADS_V2 = 32 * (2 + EPI_WARPS);
+
+template <int KIND, int NSPLIT, int STAGES, int BN>
+__global__ void __launch_bounds__(THREADS_V2, 1)
+    dtt_tc_kernel(const __grid_constant__ CUtensorMap mapM,
+                  const __grid_constant__ CUtensorMap mapD, const Params p) {
     constexpr int ELEM = (KIND == 0) ? 2 : 4;
     constexpr int BK = 128 / ELEM;                  // one 128-byte swizzle row
-    constexpr uint32_t A_TILE = BM * 128;           // 16 KB
-    constexpr uint32_t B_TILE = BN * 128;           // 8 KB
-    constexpr uint32_t STAGE = NSPLIT * (A_TILE + B_TILE);
+    constexpr uint32_t M_TILE = BM * 128;           // matrix tile, 16 KB
+    constexpr uint32_t D_TILE = BN * 128;           // data tile, 8 KB
+    constexpr uint32_t STAGE = NSPLIT * (M_TILE + D_TILE);
+    constexpr int NT = Terms<NSPLIT>::N;
+    constexpr uint32_t TCOLS = 2 * BN;              // two accumulator buffers
 
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
-    __shared__ __align__(8) uint64_t full_bar[STAGES], empty_bar[STAGES], accum_bar;
+    __shared__ __align__(8) uint64_t full_bar[STAGES], empty_bar[STAGES], accf[2], acce[2];
     __shared__ uint32_t tmem_slot;
     __shared__ int abort_flag;
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int f = blockIdx.z;
-    const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
+    const int n0 = blockIdx.x * BM, m0 = blockIdx.y * BN;
     const int nkb = p.K / BK;
+    const int promo = p.promo;
+    const int nchunks = nkb / promo;
+    const int kind = (int)((p.kindmask >> f) & 1ull);
+    if (threadIdx.x == 0) trace(0);
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < STAGES; s++) {
             mbar_init(smem_u32(&full_bar[s]), 1);
             mbar_init(smem_u32(&empty_bar[s]), 1);
         }
-        mbar_init(smem_u32(&accum_bar), 1);
+        for (int b = 0; b < 2; b++) {
+            mbar_init(smem_u32(&accf[b]), 1);
+            mbar_init(smem_u32(&acce[b]), EPI_WARPS);
+        }
         abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (warp == 2) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
                          smem_u32(&tmem_slot)),
-                     "r"(TMEM_COLS)
+                     "r"(TCOLS)
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
@@ -221,156 +252,229 @@ __global__ void __launch_bounds__(THREADS, 1)
     fence_after();
     const uint32_t tmem = tmem_slot;
     volatile int* abortp = &abort_flag;
+    if (threadIdx.x == 0) trace(1);
 
-    if (warp == 0 && lane == 0) {
-        // ---------------- TMA producer
-        const int rowA = f * p.R + m0;
-        const int rowB = p.kind[f] * p.K + n0;
-        int issued = 0;
-        for (int kb = 0; kb < nkb; kb++) {
-            const int s = kb % STAGES;
-            const uint32_t use = kb / STAGES;
-            if (kb >= STAGES && !mbar_wait(smem_u32(&empty_bar[s]), (use - 1) & 1, abortp)) {
+    if (warp == 0) {
+        if (lane == 0) {
+            // ---------------- TMA producer
+            asm volatile("prefetch.tensormap [%0];" ::"l"((uint64_t)&mapM) : "memory");
+            asm volatile("prefetch.tensormap [%0];" ::"l"((uint64_t)&mapD) : "memory");
+            const int rowM = kind * p.K + n0;
+            const int rowD = f * p.R + m0;
+            int issued = 0;
+            for (int kb = 0; kb < nkb; kb++) {
+                const int s = kb % STAGES;
+                const uint32_t use = kb / STAGES;
+                if (kb >= STAGES &&
+                    !mbar_wait(smem_u32(&empty_bar[s]), (use - 1) & 1, abortp)) {
+                    *abortp = 1;
+                    break;
+                }
+                const uint32_t fb = smem_u32(&full_bar[s]);
+                trace(16 + kb);
+                mbar_expect_tx(fb, STAGE);
+                uint8_t* st = smem + (size_t)s * STAGE;
+#pragma unroll
+                for (int t = 0; t < NSPLIT; t++)
+                    tma_load_2d(smem_u32(st + t * M_TILE), &mapM, fb, kb * BK,
+                                t * p.mat_rows + rowM);
+#pragma unroll
+                for (int t = 0; t < NSPLIT; t++)
+                    tma_load_2d(smem_u32(st + NSPLIT * M_TILE + t * D_TILE), &mapD, fb, kb * BK,
+                                t * p.data_rows + rowD);
+                issued = kb + 1;
+            }
+            if (*abortp) {
+                for (int kb = (issued > STAGES ? issued - STAGES : 0); kb < issued; kb++)
+                    mbar_wait(smem_u32(&full_bar[kb % STAGES]), (kb / STAGES) & 1, abortp);
+            }
+        }
+    } else if (warp == 1) {
+        if (lane == 0) {
+            // ---------------- MMA issuer
+            const uint32_t idesc = (1u << 4) | ((KIND == 0 ? 1u : 2u) << 7) |
+                                   ((KIND == 0 ? 1u : 2u) << 10) | ((uint32_t)(BN >> 3) << 17) |
+                                   ((uint32_t)(BM >> 4) << 24);
+            bool ok = true;
+            int kb = 0;
+            for (int c = 0; c < nchunks && ok; c++) {
+                const int b = c & 1;
+                if (c >= 2 && !mbar_wait(smem_u32(&acce[b]), ((c >> 1) - 1) & 1, abortp)) {
+                    *abortp = 1;
+                    ok = false;
+                    break;
+                }
+                fence_after();
+                const uint32_t dt = tmem + (uint32_t)(b * BN);
+                for (int q = 0; q < promo; q++, kb++) {
+                    const int s = kb % STAGES;
+                    if (!mbar_wait(smem_u32(&full_bar[s]), (kb / STAGES) & 1, abortp)) {
+                        *abortp = 1;
+                        ok = false;
+                        break;
+                    }
+                    trace(64 + kb);
+                    fence_after();
+                    const uint32_t st = smem_u32(smem + (size_t)s * STAGE);
+                    const uint64_t dM = sw128_desc(st);
+                    const uint64_t dD = sw128_desc(st + NSPLIT * M_TILE);
+#pragma unroll
+                    for (int t = 0; t < NT; t++) {
+#pragma unroll
+                        for (int kk = 0; kk < 4; kk++) {
+                            // advance the start address (16-byte units) inside the row
+                            const uint64_t a = dM + (uint64_t)((Terms<NSPLIT>::a(t) * M_TILE +
+                                                                kk * 32) >> 4);
+                            const uint64_t bb = dD + (uint64_t)((Terms<NSPLIT>::b(t) * D_TILE +
+                                                                 kk * 32) >> 4);
+                            mma<KIND>(dt, a, bb, idesc, (q | t | kk) != 0);
+                        }
+                    }
+                    mma_commit(smem_u32(&empty_bar[s]));
+                    trace(112 + kb);
+                }
+                if (ok) mma_commit(smem_u32(&accf[b]));
+            }
+        }
+    } else {
+        // ---------------- epilogue: drain every chunk into FP32 registers
+        const int e = warp - 2;                        // epilogue warp 0..7
+        const int qtr = warp & 3;                      // TMEM lane quarter
+        const int half = e >> 2;                       // column half of the tile
+        const int rloc = qtr * 32 + lane;              // tile row owned by this thread
+        constexpr int HC = BN / 2;                     // columns per epilogue warp
+        float acc[HC];
+#pragma unroll
+        for (int i = 0; i < HC; i++) acc[i] = 0.f;
+        bool have = true;
+        for (int c = 0; c < nchunks; c++) {
+            const int b = c & 1;
+            if (!mbar_wait(smem_u32(&accf[b]), (c >> 1) & 1, abortp)) {
+                have = false;
                 *abortp = 1;
                 break;
             }
-            const uint32_t fb = smem_u32(&full_bar[s]);
-            mbar_expect_tx(fb, STAGE);
-            uint8_t* st = smem + (size_t)s * STAGE;
-#pragma unroll
-            for (int t = 0; t < NSPLIT; t++)
-                tma_load_2d(smem_u32(st + t * A_TILE), &mapA, fb, kb * BK, t * p.rowsA + rowA);
-#pragma unroll
-            for (int t = 0; t < NSPLIT; t++)
-                tma_load_2d(smem_u32(st + NSPLIT * A_TILE + t * B_TILE), &mapB, fb, kb * BK,
-                            t * p.rowsB + rowB);
-            issued = kb + 1;
-        }
-        if (*abortp) {
-            // drain the copies this thread put in flight before leaving
-            for (int kb = (issued > STAGES ? issued - STAGES : 0); kb < issued; kb++)
-                mbar_wait(smem_u32(&full_bar[kb % STAGES]), (kb / STAGES) & 1, abortp);
-        }
-    } else if (warp == 1 && lane == 0) {
-        // ---------------- MMA issuer
-        const uint32_t idesc = (1u << 4) | ((KIND == 0 ? 1u : 2u) << 7) |
-                               ((KIND == 0 ? 1u : 2u) << 10) | ((uint32_t)(BN >> 3) << 17) |
-                               ((uint32_t)(BM >> 4) << 24);
-        bool ok = true;
-        for (int kb = 0; kb < nkb && ok; kb++) {
-            const int s = kb % STAGES;
-            if (!mbar_wait(smem_u32(&full_bar[s]), (kb / STAGES) & 1, abortp)) {
-                *abortp = 1;
-                ok = false;
-                break;
-            }
+            if (threadIdx.x == 64) trace(160 + c);
             fence_after();
-            const uint32_t st = smem_u32(smem + (size_t)s * STAGE);
-            for (int t = 0; t < p.nterm; t++) {
-                const uint32_t a = st + p.ta[t] * A_TILE;
-                const uint32_t b = st + NSPLIT * A_TILE + p.tb[t] * B_TILE;
 #pragma unroll
-                for (int kk = 0; kk < 4; kk++) {
-                    mma<KIND>(tmem, sw128_desc(a + kk * 32), sw128_desc(b + kk * 32), idesc,
-                              (kb | t | kk) != 0);
-                }
+            for (int j = 0; j < HC; j += 16) {
+                uint32_t v[16];
+                tmem_ld16(tmem + ((uint32_t)(qtr * 32) << 16) + (uint32_t)(b * BN + half * HC + j),
+                          v);
+                tmem_wait_ld();
+#pragma unroll
+                for (int i = 0; i < 16; i++) acc[j + i] += __uint_as_float(v[i]);
             }
-            mma_commit(smem_u32(&empty_bar[s]));
+            fence_before();
+            __syncwarp();
+            if (lane == 0) {
+                asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&acce[b]))
+                             : "memory");
+            }
         }
-        if (ok) mma_commit(smem_u32(&accum_bar));
-    }
-    __syncwarp();
-
-    // ---------------- epilogue (all 4 warps)
-    const bool have = mbar_wait(smem_u32(&accum_bar), 0, abortp);
-    fence_after();
-    if (have) {
-        const int m = m0 + warp * 32 + lane;    // TMEM lane = tile row
-        const size_t plane = (size_t)p.R * p.K;
+        // every MMA has completed (the last chunk was committed after them),
+        // so the pipeline smem is free: stage the tile there row-major
+        constexpr int LD = BN + 4;
+        float* tile = (float*)smem;
+        if (have) {
+            const float sc = p.scale;
+            float4* trow = (float4*)(tile + (size_t)rloc * LD + half * HC);
 #pragma unroll
-        for (int c = 0; c < BN; c += 16) {
-            uint32_t v[16];
-            tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c, v);
-            tmem_wait_ld();
-            if (!p.out_split) {
-                float* o = p.out[f];
-#pragma unroll
-                for (int jj = 0; jj < 16; jj++) {
-                    const int n = n0 + c + jj;
-                    o[(size_t)n * p.R + m] = __uint_as_float(v[jj]) * p.scale;
-                }
+            for (int i = 0; i < HC / 4; i++)
+                trow[i] = make_float4(acc[4 * i] * sc, acc[4 * i + 1] * sc, acc[4 * i + 2] * sc,
+                                      acc[4 * i + 3] * sc);
+        }
+        asm volatile("bar.sync 1, %0;" ::"r"(32 * EPI_WARPS) : "memory");
+        if (have && !*abortp) {
+            // each warp writes whole rows; a row is BN values, 4 per lane
+            float* o = nullptr;
+            if (p.out_contig) {
+                o = p.out[0] + (size_t)f * p.R * p.K;
             } else {
 #pragma unroll
-                for (int jj = 0; jj < 16; jj++) {
-                    const int n = n0 + c + jj;
-                    const size_t idx = (size_t)f * plane + (size_t)n * p.R + m;
-                    float t[3];
-                    split_value<KIND>(__uint_as_float(v[jj]) * p.scale, NSPLIT, t);
+                for (int i = 0; i < kMaxXfFields; i++)
+                    if (i == f) o = p.out[i];
+            }
+            const size_t plane = (size_t)p.R * p.K;
+            const size_t tstride = (size_t)p.nfmax * plane;
+            constexpr int LPR = BN / 4;                // lanes per row
+            constexpr int RPI = 32 / LPR;              // rows per warp instruction
+            const int sub = lane / LPR, lc = lane % LPR;
+            for (int rr = 0; rr < BM / EPI_WARPS; rr += RPI) {
+                const int r = e * (BM / EPI_WARPS) + rr + sub;
+                const float4 v = *(const float4*)(tile + (size_t)r * LD + lc * 4);
+                const size_t g = (size_t)(n0 + r) * p.R + m0 + lc * 4;
+                if (!p.out_split) {
+                    *(float4*)(o + g) = v;
+                } else {
+                    const float vv[4] = {v.x, v.y, v.z, v.w};
+                    float t[4][3];
+#pragma unroll
+                    for (int q = 0; q < 4; q++) split_value<KIND>(vv[q], NSPLIT, t[q]);
+                    const size_t idx = (size_t)f * plane + g;
                     if (KIND == 0) {
                         __nv_bfloat16* ob = (__nv_bfloat16*)p.out_base;
 #pragma unroll
-                        for (int s = 0; s < NSPLIT; s++)
-                            ob[(size_t)s * 8 * plane + idx] = __float2bfloat16_rn(t[s]);
+                        for (int s = 0; s < NSPLIT; s++) {
+                            __nv_bfloat162 h0 = __floats2bfloat162_rn(t[0][s], t[1][s]);
+                            __nv_bfloat162 h1 = __floats2bfloat162_rn(t[2][s], t[3][s]);
+                            *(uint2*)(ob + (size_t)s * tstride + idx) =
+                                make_uint2(*(uint32_t*)&h0, *(uint32_t*)&h1);
+                        }
                     } else {
                         float* of = (float*)p.out_base;
 #pragma unroll
-                        for (int s = 0; s < NSPLIT; s++) of[(size_t)s * 8 * plane + idx] = t[s];
+                        for (int s = 0; s < NSPLIT; s++)
+                            *(float4*)(of + (size_t)s * tstride + idx) =
+                                make_float4(t[0][s], t[1][s], t[2][s], t[3][s]);
                     }
                 }
             }
+        } else if (lane == 0 && e == 0) {
+            atomicOr(p.err, DEV_ERR_TIMEOUT);
         }
-    } else if (threadIdx.x == 0) {
-        atomicOr(p.err, DEV_ERR_TIMEOUT);
+        if (threadIdx.x == 64) trace(200);
     }
     fence_before();
     __syncthreads();
+    if (threadIdx.x == 0) trace(201);
     if (warp == 2) {
         fence_after();
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
-                     "r"(TMEM_COLS)
+                     "r"(TCOLS)
                      : "memory");
     }
 }
 
-// split nf FP32 planes (R x K each) into the operand terms [term][8][R][K]
-template <int KIND>
-__global__ void split_planes_kernel(const float* const* __restrict__ in_ptrs, int nf, size_t plane,
-                                    int nsplit, void* out) {
-    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+// split nf FP32 planes stored from `in` with stride `stride` into the
+// operand terms [term][8][plane]; 4 values per thread
+template <int KIND, int NSPLIT>
+__global__ void split_planes_kernel(const float* __restrict__ in, size_t stride, int nf,
+                                    size_t plane, size_t tstride, void* __restrict__ out) {
+    const size_t i4 = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) * 4;
     const int f = blockIdx.y;
-    if (i >= plane || f >= nf) return;
-    const float v = in_ptrs[f][i];
-    float t[3];
-    split_value<KIND>(v, nsplit, t);
-    const size_t idx = (size_t)f * plane + i;
+    if (i4 >= plane || f >= nf) return;
+    const float4 v = *(const float4*)(in + (size_t)f * stride + i4);
+    const float vv[4] = {v.x, v.y, v.z, v.w};
+    float t[4][3];
+#pragma unroll
+    for (int e = 0; e < 4; e++) split_value<KIND>(vv[e], NSPLIT, t[e]);
+    const size_t idx = (size_t)f * plane + i4;
     if (KIND == 0) {
         __nv_bfloat16* o = (__nv_bfloat16*)out;
-        for (int s = 0; s < nsplit; s++) o[(size_t)s * 8 * plane + idx] = __float2bfloat16_rn(t[s]);
+#pragma unroll
+        for (int s = 0; s < NSPLIT; s++) {
+            __nv_bfloat162 a = __floats2bfloat162_rn(t[0][s], t[1][s]);
+            __nv_bfloat162 b = __floats2bfloat162_rn(t[2][s], t[3][s]);
+            *(uint2*)(o + (size_t)s * tstride + idx) =
+                make_uint2(*(uint32_t*)&a, *(uint32_t*)&b);
+        }
     } else {
         float* o = (float*)out;
-        for (int s = 0; s < nsplit; s++) o[(size_t)s * 8 * plane + idx] = t[s];
-    }
-}
-
-struct PtrPack {
-    const float* p[kMaxXfFields];
-};
-
-template <int KIND>
-__global__ void split_planes_kernel_v(PtrPack in, int nf, size_t plane, int nsplit, void* out) {
-    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const int f = blockIdx.y;
-    if (i >= plane || f >= nf) return;
-    const float v = in.p[f][i];
-    float t[3];
-    split_value<KIND>(v, nsplit, t);
-    const size_t idx = (size_t)f * plane + i;
-    if (KIND == 0) {
-        __nv_bfloat16* o = (__nv_bfloat16*)out;
-        for (int s = 0; s < nsplit; s++) o[(size_t)s * 8 * plane + idx] = __float2bfloat16_rn(t[s]);
-    } else {
-        float* o = (float*)out;
-        for (int s = 0; s < nsplit; s++) o[(size_t)s * 8 * plane + idx] = t[s];
+#pragma unroll
+        for (int s = 0; s < NSPLIT; s++)
+            *(float4*)(o + (size_t)s * tstride + idx) =
+                make_float4(t[0][s], t[1][s], t[2][s], t[3][s]);
     }
 }
 
@@ -427,19 +531,27 @@ float round_term(double x, bool bf16) {
 
 class TcImpl : public TcTransformer {
 public:
-    int mode = 0, ny = 0, nz = 0, kind = 0, nsplit = 2, nterm = 3, stages = 4;
-    int ta[6] = {0, 0, 1, 0, 1, 2}, tb[6] = {0, 1, 0, 2, 1, 0};
+    int mode = 0, ny = 0, nz = 0, kind = 0, nsplit = 2;
+    int nfmax = 64;
     void* splitA = nullptr;
     void* splitB = nullptr;
     void* matY = nullptr;
     void* matZ = nullptr;
     int* err = nullptr;
-    CUtensorMap mapA1, mapB1, mapA2, mapB2;
-    size_t smem_bytes = 0;
+    // tensor maps: data (N side) for tile widths 64 / 128, matrix (M side)
+    CUtensorMap mapD1[2], mapM1, mapD2[2], mapM2;
+    size_t smem_bytes[2] = {0, 0};
+    int chunk_k = 128;
 
     ~TcImpl() override {
         for (void* p : {splitA, splitB, matY, matZ})
             if (p) cudaFree(p);
+    }
+
+    // pipeline depth of each kernel instantiation (must match launch_gemm)
+    int stages_for(int bnidx) const {
+        if (nsplit == 3) return bnidx ? 2 : 3;
+        return bnidx ? 3 : 4;
     }
 
     bool upload_matrix(int n, void** dst, std::string& why) {
@@ -454,10 +566,10 @@ public:
                     double a = M_PI * (double)q / (4.0 * n);
                     double v = 2.0 * (kd == 0 ? std::cos(a) : std::sin(a));
                     double rem = v;
-                    for (int s = 0; s < nsplit; s++) {
+                    for (int sp = 0; sp < nsplit; sp++) {
                         float t = round_term(rem, bf16);
                         rem -= (double)t;
-                        size_t idx = (size_t)s * 2 * nn + (size_t)kd * nn + r * n + c;
+                        size_t idx = (size_t)sp * 2 * nn + (size_t)kd * nn + r * n + c;
                         if (bf16) {
                             __nv_bfloat16 b = __float2bfloat16_rn(t);
                             memcpy(host.data() + idx * 2, &b, 2);
@@ -478,18 +590,18 @@ public:
     }
 
     bool init(std::string& why) {
-        if (ny % BM_ || nz % BM_) {
+        if (ny % 128 || nz % 128) {
             why = "ny and nz must be multiples of 128 for the tensor-core transforms";
             return false;
         }
-        if (mode == QS_PREC_BF16X3) { kind = 0; nsplit = 2; nterm = 3; stages = 4; }
-        else if (mode == QS_PREC_TF32X3) { kind = 1; nsplit = 2; nterm = 3; stages = 4; }
-        else if (mode == QS_PREC_BF16X6) { kind = 0; nsplit = 3; nterm = 6; stages = 3; }
+        if (mode == QS_PREC_BF16X3) { kind = 0; nsplit = 2; }
+        else if (mode == QS_PREC_TF32X3) { kind = 1; nsplit = 2; }
+        else if (mode == QS_PREC_BF16X6) { kind = 0; nsplit = 3; }
         else { why = "not a tensor-core precision"; return false; }
         const bool bf16 = kind == 0;
         const int elem = bf16 ? 2 : 4;
         const size_t plane = (size_t)ny * nz;
-        const size_t bytes = (size_t)nsplit * 8 * plane * elem;
+        const size_t bytes = (size_t)nsplit * nfmax * plane * elem;
         if (cudaMalloc(&splitA, bytes) != cudaSuccess || cudaMalloc(&splitB, bytes) != cudaSuccess) {
             why = "cudaMalloc of split operands failed";
             return false;
@@ -497,27 +609,32 @@ public:
         cudaMemset(splitA, 0, bytes);
         cudaMemset(splitB, 0, bytes);
         if (!upload_matrix(ny, &matY, why)) return false;
-        if (nz == ny) matZ = nullptr;
-        else if (!upload_matrix(nz, &matZ, why)) return false;
+        if (nz != ny && !upload_matrix(nz, &matZ, why)) return false;
         void* mz = matZ ? matZ : matY;
         const uint32_t bk = 128 / elem;
-        // pass 1: A = splitA [term][8][nz][ny], B = matY [term][2][ny][ny]
-        if (!encode_2d(&mapA1, splitA, bf16, ny, (uint64_t)nsplit * 8 * nz, bk, 128, why)) return false;
-        if (!encode_2d(&mapB1, matY, bf16, ny, (uint64_t)nsplit * 2 * ny, bk, 64, why)) return false;
-        // pass 2: A = splitB [term][8][ny][nz], B = matZ [term][2][nz][nz]
-        if (!encode_2d(&mapA2, splitB, bf16, nz, (uint64_t)nsplit * 8 * ny, bk, 128, why)) return false;
-        if (!encode_2d(&mapB2, mz, bf16, nz, (uint64_t)nsplit * 2 * nz, bk, 64, why)) return false;
-        smem_bytes = (size_t)stages * nsplit * (128 * 128 + 64 * 128) + 1024;
+        for (int b = 0; b < 2; b++) {
+            const uint32_t bn = b ? 128 : 64;
+            // pass 1 (along y): data = splitA [term][nfmax][nz][ny]
+            if (!encode_2d(&mapD1[b], splitA, bf16, ny, (uint64_t)nsplit * nfmax * nz, bk, bn, why))
+                return false;
+            // pass 2 (along z): data = splitB [term][nfmax][ny][nz]
+            if (!encode_2d(&mapD2[b], splitB, bf16, nz, (uint64_t)nsplit * nfmax * ny, bk, bn, why))
+                return false;
+            smem_bytes[b] = (size_t)stages_for(b) * nsplit * (128 * 128 + bn * 128) + 1024;
+        }
+        if (!encode_2d(&mapM1, matY, bf16, ny, (uint64_t)nsplit * 2 * ny, bk, 128, why)) return false;
+        if (!encode_2d(&mapM2, mz, bf16, nz, (uint64_t)nsplit * 2 * nz, bk, 128, why)) return false;
+        chunk_k = 128;
+        if (const char* e = getenv("QS_TC_CHUNK")) chunk_k = atoi(e);
         cudaError_t e = cudaSuccess;
-        if (mode == QS_PREC_BF16X3)
-            e = cudaFuncSetAttribute(tcx::dtt_tc_kernel<0, 2, 4>,
-                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes);
-        else if (mode == QS_PREC_TF32X3)
-            e = cudaFuncSetAttribute(tcx::dtt_tc_kernel<1, 2, 4>,
-                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes);
-        else
-            e = cudaFuncSetAttribute(tcx::dtt_tc_kernel<0, 3, 3>,
-                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes);
+#define QS_SET_SMEM(K, NS, ST, BN, B)                                                              \
+    if (e == cudaSuccess)                                                                          \
+        e = cudaFuncSetAttribute(tcx::dtt_tc_kernel<K, NS, ST, BN>,                                \
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes[B]);
+        if (mode == QS_PREC_BF16X3) { QS_SET_SMEM(0, 2, 4, 64, 0) QS_SET_SMEM(0, 2, 3, 128, 1) }
+        else if (mode == QS_PREC_TF32X3) { QS_SET_SMEM(1, 2, 4, 64, 0) QS_SET_SMEM(1, 2, 3, 128, 1) }
+        else { QS_SET_SMEM(0, 3, 3, 64, 0) QS_SET_SMEM(0, 3, 2, 128, 1) }
+#undef QS_SET_SMEM
         if (e != cudaSuccess) {
             why = std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e);
             return false;
@@ -525,17 +642,69 @@ public:
         return true;
     }
 
-    static constexpr int BM_ = 128;
+    int promo_for(int K) const {
+        const int bk = (kind == 0) ? 64 : 32;
+        const int nkb = K / bk;
+        if (chunk_k <= 0) return nkb;
+        int pr = chunk_k / bk;
+        if (pr < 1) pr = 1;
+        while (pr > 1 && nkb % pr) pr--;
+        return pr;
+    }
 
-    void launch_gemm(const CUtensorMap& A, const CUtensorMap& B, const tcx::Params& p, int nf,
-                     cudaStream_t st) {
-        dim3 grid(p.R / tcx::BM, p.K / tcx::BN, nf);
-        if (mode == QS_PREC_BF16X3)
-            tcx::dtt_tc_kernel<0, 2, 4><<<grid, tcx::THREADS, smem_bytes, st>>>(A, B, p);
-        else if (mode == QS_PREC_TF32X3)
-            tcx::dtt_tc_kernel<1, 2, 4><<<grid, tcx::THREADS, smem_bytes, st>>>(A, B, p);
+    // tile width: 128 when the batch fills the GPU with 128-wide tiles
+    int bn_index(int nf, int R, int K) const { return nf * (R / 128) * (K / 128) >= 96 ? 1 : 0; }
+
+    void launch_gemm(int pass, tcx::Params& p, int nf, cudaStream_t st) {
+        const int b = bn_index(nf, p.R, p.K);
+        const int bn = b ? 128 : 64;
+        dim3 grid(p.K / tcx::BM, p.R / bn, nf);
+        const CUtensorMap& D = pass == 1 ? mapD1[b] : mapD2[b];
+        const CUtensorMap& M = pass == 1 ? mapM1 : mapM2;
+        const int T = tcx::THREADS_V2;
+        const size_t sm = smem_bytes[b];
+        if (mode == QS_PREC_BF16X3) {
+            if (b) tcx::dtt_tc_kernel<0, 2, 3, 128><<<grid, T, sm, st>>>(M, D, p);
+            else tcx::dtt_tc_kernel<0, 2, 4, 64><<<grid, T, sm, st>>>(M, D, p);
+        } else if (mode == QS_PREC_TF32X3) {
+            if (b) tcx::dtt_tc_kernel<1, 2, 3, 128><<<grid, T, sm, st>>>(M, D, p);
+            else tcx::dtt_tc_kernel<1, 2, 4, 64><<<grid, T, sm, st>>>(M, D, p);
+        } else {
+            if (b) tcx::dtt_tc_kernel<0, 3, 2, 128><<<grid, T, sm, st>>>(M, D, p);
+            else tcx::dtt_tc_kernel<0, 3, 3, 64><<<grid, T, sm, st>>>(M, D, p);
+        }
+    }
+
+    void launch_split(const float* base, int nf, cudaStream_t st) {
+        const size_t plane = (size_t)ny * nz;
+        const size_t ts = (size_t)nfmax * plane;
+        dim3 sg((unsigned)((plane / 4 + 255) / 256), nf);
+        if (kind == 0 && nsplit == 2)
+            tcx::split_planes_kernel<0, 2><<<sg, 256, 0, st>>>(base, plane, nf, plane, ts, splitA);
+        else if (kind == 0)
+            tcx::split_planes_kernel<0, 3><<<sg, 256, 0, st>>>(base, plane, nf, plane, ts, splitA);
         else
-            tcx::dtt_tc_kernel<0, 3, 3><<<grid, tcx::THREADS, smem_bytes, st>>>(A, B, p);
+            tcx::split_planes_kernel<1, 2><<<sg, 256, 0, st>>>(base, plane, nf, plane, ts, splitA);
+    }
+
+    void pass_params(int stage, int nf, const int* kz, const int* ky, double scale,
+                     tcx::Params& p) {
+        p.err = err;
+        p.nfmax = nfmax;
+        unsigned long long mask = 0;
+        if (stage == 1) {   // along y: splitA (nz rows of ny) -> splitB, transposed
+            for (int f = 0; f < nf; f++) mask |= (unsigned long long)(ky ? (ky[f] & 1) : 0) << f;
+            p.R = nz; p.K = ny;
+            p.data_rows = nfmax * nz; p.mat_rows = 2 * ny;
+            p.out_split = 1; p.out_base = splitB; p.scale = 1.0f;
+        } else {            // along z: splitB (ny rows of nz) -> FP32 destination
+            for (int f = 0; f < nf; f++) mask |= (unsigned long long)(kz ? (kz[f] & 1) : 0) << f;
+            p.R = ny; p.K = nz;
+            p.data_rows = nfmax * ny; p.mat_rows = 2 * nz;
+            p.out_split = 0; p.out_base = nullptr; p.scale = (float)scale;
+        }
+        p.kindmask = mask;
+        p.promo = promo_for(p.K);
     }
 
     int run_stage(int stage, int nf, const void* const* in, void* const* out, const int* kz,
@@ -543,33 +712,17 @@ public:
         if (nf <= 0 || nf > kMaxXfFields) return 0;
         const size_t plane = (size_t)ny * nz;
         if (stage == 0) {
-            tcx::PtrPack pk{};
-            for (int f = 0; f < nf; f++) pk.p[f] = (const float*)in[f];
-            dim3 sg((unsigned)((plane + 255) / 256), nf);
-            if (kind == 0)
-                tcx::split_planes_kernel_v<0><<<sg, 256, 0, st>>>(pk, nf, plane, nsplit, splitA);
-            else
-                tcx::split_planes_kernel_v<1><<<sg, 256, 0, st>>>(pk, nf, plane, nsplit, splitA);
+            const float* base = (const float*)in[0];
+            for (int f = 1; f < nf; f++)
+                if ((const float*)in[f] != base + (size_t)f * plane) return -1;
+            launch_split(base, nf, st);
             return 1;
         }
         tcx::Params p{};
-        p.nsplit = nsplit;
-        p.nterm = nterm;
-        for (int t = 0; t < 6; t++) { p.ta[t] = ta[t]; p.tb[t] = tb[t]; }
-        p.err = err;
-        if (stage == 1) {   // along y: splitA (nz x ny rows) -> splitB, transposed
-            p.R = nz; p.K = ny;
-            for (int f = 0; f < nf; f++) p.kind[f] = ky[f];
-            p.rowsA = 8 * nz; p.rowsB = 2 * ny;
-            p.out_split = 1; p.out_base = splitB; p.scale = 1.0f;
-            launch_gemm(mapA1, mapB1, p, nf, st);
-        } else {            // along z: splitB (ny x nz rows) -> FP32 destination
-            p.R = ny; p.K = nz;
-            for (int f = 0; f < nf; f++) { p.kind[f] = kz[f]; p.out[f] = (float*)out[f]; }
-            p.rowsA = 8 * ny; p.rowsB = 2 * nz;
-            p.out_split = 0; p.out_base = nullptr; p.scale = (float)scale;
-            launch_gemm(mapA2, mapB2, p, nf, st);
-        }
+        pass_params(stage, nf, kz, ky, scale, p);
+        if (stage == 2)
+            for (int f = 0; f < nf; f++) p.out[f] = (float*)out[f];
+        launch_gemm(stage, p, nf, st);
         return 1;
     }
 
@@ -580,9 +733,44 @@ public:
         for (int s = 0; s < 3; s++) n += run_stage(s, nf, in, out, kz, ky, scale, st);
         return n;
     }
+
+    void split_target(void** base, int* ns, int* kd, size_t* term_stride) override {
+        *base = splitA;
+        *ns = nsplit;
+        *kd = kind;
+        *term_stride = (size_t)nfmax * ny * nz;
+    }
+
+    int run_batched(const float* in, float* out, int nplanes, double scale, int stage,
+                    cudaStream_t st) override {
+        int n = 0;
+        const size_t plane = (size_t)ny * nz;
+        for (int b0 = 0; b0 < nplanes; b0 += nfmax) {
+            const int nf = std::min(nfmax, nplanes - b0);
+            if (stage < 0 || stage == 0) { launch_split(in + (size_t)b0 * plane, nf, st); n++; }
+            for (int ps = 1; ps <= 2; ps++) {
+                if (stage >= 0 && stage != ps) continue;
+                tcx::Params p{};
+                pass_params(ps, nf, nullptr, nullptr, scale, p);
+                if (ps == 2) {
+                    p.out_contig = 1;
+                    p.out[0] = out + (size_t)b0 * plane;
+                }
+                launch_gemm(ps, p, nf, st);
+                n++;
+            }
+        }
+        return n;
+    }
 };
 
 }  // namespace
+
+#ifdef QS_TC_TRACE
+extern "C" int qs_tc_trace_read(long long* out) {
+    return (int)cudaMemcpyFromSymbol(out, tcx::g_tc_trace, sizeof(long long) * 256);
+}
+#endif
 
 TcTransformer* TcTransformer::create(int mode, int ny, int nz, int* err_flag, std::string& why) {
     auto* t = new TcImpl();

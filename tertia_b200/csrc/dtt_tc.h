@@ -20,6 +20,14 @@ public:
     // stage 0 splits the inputs, stage 1 is the y pass, stage 2 the z pass.
     virtual int run_stage(int stage, int nf, const void* const* in, void* const* out,
                           const int* kz, const int* ky, double scale, cudaStream_t st) = 0;
+    // operand buffer a producer may fill directly before run_stage(1..2):
+    // term s of field f at base + (s * term_stride + f * ny*nz) elements,
+    // element type bf16 (kind 0) or tf32-in-float (kind 1)
+    virtual void split_target(void** base, int* nsplit, int* kind, size_t* term_stride) = 0;
+    // REDFT11 x REDFT11 transform of nplanes contiguous planes in batches;
+    // stage < 0 runs all three launches of every batch
+    virtual int run_batched(const float* in, float* out, int nplanes, double scale, int stage,
+                            cudaStream_t st) = 0;
 };
 
 }  // namespace qs

@@ -1,0 +1,414 @@
+// push.cu — plasma macro-particle push across one xi-layer with current /
+// density deposit (reference Mesh::MoveParticlesLayerSplit,
+// movepart_splitlayer.cpp:781-1544, DepositCurrentsInCellSplit :1547-1655,
+// ExchangeCurrentsSplit :1685-1711; dead GPU twin cuMoveSplitParticles,
+// plasma_particles.cu:72-863).
+//
+// Layout: particles are SoA (y, z, px, py, pz, w, cell) grouped by cell in
+// ascending cell order, one thread per particle.  In the reference's live
+// NGP path a particle never leaves its seeded cell (the full-step relink at
+// :1507 uses the outer jtmp = j), so the grouping is permanent and the 4-8
+// particles of a cell sit in consecutive lanes: their deposits are summed
+// with a warp-segmented reduction over runs of equal destination cell and a
+// single lane per run issues the global atomics.  The guard-ring fold of
+// ExchangeCurrentsSplit is done by depositing at (j mod My, k mod Mz).
+//
+// The FP64 kernel (push_f64.cu, compiled with -fmad=false) follows the
+// reference's expression order without contraction and reproduces the oracle
+// bit for bit on identical inputs, cell indices included.  The FP32 kernel
+// (push_f32.cu) uses the same physics with the divisions factored into six
+// reciprocals and FMA contraction allowed: it is instruction bound, not
+// memory bound, and this halves its instruction count.
+#pragma once
+#include "qs_common.cuh"
+#include "qs_internal.h"
+
+namespace qs {
+
+template <class T>
+__device__ __forceinline__ T ld(const T* p) { return __ldg(p); }
+
+template <class T>
+__device__ __forceinline__ T sqrt_t(T x);
+template <>
+__device__ __forceinline__ float sqrt_t<float>(float x) { return __fsqrt_rn(x); }
+template <>
+__device__ __forceinline__ double sqrt_t<double>(double x) { return __dsqrt_rn(x); }
+
+template <class T>
+__device__ __forceinline__ T floor_t(T x);
+template <>
+__device__ __forceinline__ float floor_t<float>(float x) { return floorf(x); }
+template <>
+__device__ __forceinline__ double floor_t<double>(double x) { return floor(x); }
+
+template <class T>
+__device__ __forceinline__ T fabs_t(T x) { return x < T(0) ? -x : x; }
+
+__device__ __forceinline__ int wrap_idx(int j, int M) {
+    // shifts are small (|shift| <= a few cells): avoid the integer modulo
+    while (j >= M) j -= M;
+    while (j < 0) j += M;
+    return j;
+}
+
+// k = cell / My, j = cell % My through a float reciprocal with correction
+// (exact for cell < 2^24)
+__device__ __forceinline__ void cell_jk(int cell, int My, float invMy, int& j, int& k) {
+    int q = (int)((float)cell * invMy);
+    int r = cell - q * My;
+    if (r < 0) { q -= 1; r += My; }
+    else if (r >= My) { q += 1; r -= My; }
+    j = r;
+    k = q;
+}
+
+// Sub-cycled transverse move and deposit of one particle (:1389-1479 with
+// DepositCurrentsInCellSplit :1547-1615 or the CIC of MoveInCell), then the
+// full-step store (:1501-1512).  The first sub-step's deposit is returned in
+// (key, v) for the warp-level reduction; later sub-steps deposit directly.
+template <class T, int SHAPE, bool PRECISE, int NV>
+__device__ __forceinline__ void move_and_deposit(const PushArgs<T>& a, int64_t i, int j, int k,
+                                                 T yp, T zp, T px, T py, T pz, T djx, T djy,
+                                                 T djz, T drho, T dy, T dz, int& key, T (&v)[NV]) {
+    const T one = T(1);
+    const int My = a.My, Mz = a.Mz;
+    const size_t plane = a.plane;
+    T partdx = T(0), step = one;
+    if (fabs_t(dy) > one || fabs_t(dz) > one) {
+        if (fabs_t(dy) > fabs_t(dz)) step = partdx = fabs_t(dy);
+        else step = partdx = fabs_t(dz);
+    }
+    if (partdx < one) partdx = step = one;
+    const T MyT = T(My), MzT = T(Mz);
+    T ytmp = yp, ztmp = zp;
+    int jb = j, kb = k, jj = j, kk = k;
+    bool first = true;
+    while (partdx > T(0)) {
+        T part_step;
+        if (partdx > one) {
+            partdx -= one;
+            part_step = one / step;
+        } else {
+            part_step = partdx / step;
+            partdx = T(0);
+        }
+        if (SHAPE == QS_SHAPE_NGP && !PRECISE) {
+            // reference form (:1420-1437); the added j is the outer j_jump
+            ytmp += dy * part_step + T(j);
+            ztmp += dz * part_step + T(k);
+            while (ytmp > MyT) ytmp -= MyT;
+            while (ytmp < T(0)) ytmp += MyT;
+            while (ztmp > MzT) ztmp -= MzT;
+            while (ztmp < T(0)) ztmp += MzT;
+            jj = (int)ytmp;
+            kk = (int)ztmp;
+            ytmp -= T(jj);
+            ztmp -= T(kk);
+        } else {
+            const T uy = ytmp + dy * part_step;
+            const T uz = ztmp + dz * part_step;
+            const T fy = floor_t<T>(uy), fz = floor_t<T>(uz);
+            T ry = uy - fy, rz = uz - fz;
+            int sy = (int)fy, sz = (int)fz;
+            if (ry >= one) { ry = T(0); sy += 1; }
+            if (rz >= one) { rz = T(0); sz += 1; }
+            const int bj = (SHAPE == QS_SHAPE_NGP) ? j : jb;
+            const int bk = (SHAPE == QS_SHAPE_NGP) ? k : kb;
+            jj = wrap_idx(bj + sy, My);
+            kk = wrap_idx(bk + sz, Mz);
+            ytmp = ry;
+            ztmp = rz;
+            jb = jj;
+            kb = kk;
+        }
+        const T s = part_step;
+        const int fj = wrap_idx(jj, My), fk = wrap_idx(kk, Mz);
+        if (SHAPE == QS_SHAPE_NGP) {
+            const T d0 = djx * s, d1 = djy * s, d2 = djz * s, d3 = drho * s;
+            if (first) {
+                key = fj + My * fk;
+                v[0] = d0; v[1] = d1; v[2] = d2; v[3] = d3;
+            } else {
+                const size_t n = (size_t)fj + (size_t)My * fk;
+                atomicAdd(a.dep + 0 * plane + n, d0);
+                atomicAdd(a.dep + 1 * plane + n, d1);
+                atomicAdd(a.dep + 2 * plane + n, d2);
+                atomicAdd(a.dep + 3 * plane + n, d3);
+            }
+        } else {
+            const T ayp = ytmp, ayc = one - ayp, azp = ztmp, azc = one - azp;
+            const T w00 = ayc * azc, w10 = ayp * azc, w01 = ayc * azp, w11 = ayp * azp;
+            const T q[4] = {djx * s, djy * s, djz * s, drho * s};
+            const T wc[4] = {w00, w10, w01, w11};
+            if (first) {
+                key = fj + My * fk;
+#pragma unroll
+                for (int cnr = 0; cnr < 4; cnr++)
+#pragma unroll
+                    for (int qq = 0; qq < 4; qq++) v[cnr * 4 + qq] = q[qq] * wc[cnr];
+            } else {
+                const int j1 = wrap_idx(fj + 1, My), k1 = wrap_idx(fk + 1, Mz);
+                const size_t nn[4] = {(size_t)fj + (size_t)My * fk,
+                                      (size_t)j1 + (size_t)My * fk,
+                                      (size_t)fj + (size_t)My * k1,
+                                      (size_t)j1 + (size_t)My * k1};
+#pragma unroll
+                for (int cnr = 0; cnr < 4; cnr++)
+#pragma unroll
+                    for (int qq = 0; qq < 4; qq++)
+                        atomicAdd(a.dep + qq * plane + nn[cnr], q[qq] * wc[cnr]);
+            }
+        }
+        first = false;
+    }
+    const int jf = wrap_idx(jj, My), kf = wrap_idx(kk, Mz);
+    if (a.dep_cell) a.dep_cell[i] = jf + My * kf;
+    if (a.full) {
+        a.px[i] = px;
+        a.py[i] = py;
+        a.pz[i] = pz;
+        a.y[i] = ytmp;
+        a.z[i] = ztmp;
+        if (SHAPE == QS_SHAPE_CIC) a.cell_out[i] = jf + My * kf;
+    }
+}
+
+// SHAPE: QS_SHAPE_NGP / QS_SHAPE_CIC.  PRECISE: cell-relative position
+// update (u = frac + d*part_step measured from the base cell) instead of the
+// reference's ytmp + j form; the FP32 kernels use it to keep the in-cell
+// fraction at full float precision.
+template <class T, int SHAPE, bool PRECISE, bool FAST>
+__global__ void __launch_bounds__(256) push_kernel(PushArgs<T> a) {
+    constexpr int NV = (SHAPE == QS_SHAPE_NGP) ? 4 : 16;
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & 31;
+    const int My = a.My, Mz = a.Mz;
+    int key = -1;          // base cell of the first sub-step deposit
+    T v[NV];
+#pragma unroll
+    for (int c = 0; c < NV; c++) v[c] = T(0);
+
+    if (i < a.n) {
+        const T one = T(1), two = T(2), half = T(0.5);
+        const int cell = a.cell[i];
+        int j, k;
+        if (FAST) cell_jk(cell, My, a.invMy, j, k);
+        else { j = cell % My; k = cell / My; }
+        const T yp = a.y[i], zp = a.z[i];
+        T px = a.px[i], py = a.py[i], pz = a.pz[i];
+        const T weight = a.w[i];
+        if (!(yp >= T(0) && yp <= one && zp >= T(0) && zp <= one)) {
+            atomicOr(a.err, DEV_ERR_RANGE);
+        } else {
+            if (FAST) {
+            // ---- FP32: the same update with the divisions factored out
+            const T inv_gp = one / sqrt_t<T>(one + px * px + py * py + pz * pz);
+            const T Vxp = px * inv_gp, Vyp = py * inv_gp, Vzp = pz * inv_gp;
+            const T q2m = a.q2m;
+            const size_t plane = a.plane;
+            T ex, ey, ez, bx, by, bz;
+            if (SHAPE == QS_SHAPE_NGP) {
+                const size_t n = (size_t)cell;
+                ex = half * (ld(a.P + 0 * plane + n) + ld(a.C + 0 * plane + n));
+                ey = half * (ld(a.P + 1 * plane + n) + ld(a.C + 1 * plane + n));
+                ez = half * (ld(a.P + 2 * plane + n) + ld(a.C + 2 * plane + n));
+                bx = half * (ld(a.P + 3 * plane + n) + ld(a.C + 3 * plane + n));
+                by = half * (ld(a.P + 4 * plane + n) + ld(a.C + 4 * plane + n));
+                bz = half * (ld(a.P + 5 * plane + n) + ld(a.C + 5 * plane + n));
+            } else {
+                const T ayc = one - yp, ayp = yp, azc = one - zp, azp = zp;
+                const T acc = ayc * azc, apc = ayp * azc, acp = ayc * azp, app = ayp * azp;
+                const int j1 = wrap_idx(j + 1, My), k1 = wrap_idx(k + 1, Mz);
+                const size_t n00 = (size_t)j + (size_t)My * k, n10 = (size_t)j1 + (size_t)My * k,
+                             n01 = (size_t)j + (size_t)My * k1, n11 = (size_t)j1 + (size_t)My * k1;
+                T g[6];
+#pragma unroll
+                for (int c = 0; c < 6; c++) {
+                    const T* Pc = a.P + c * plane;
+                    const T* Cc = a.C + c * plane;
+                    T vp = acc * ld(Pc + n00) + apc * ld(Pc + n10) + acp * ld(Pc + n01) +
+                           app * ld(Pc + n11);
+                    T vc = acc * ld(Cc + n00) + apc * ld(Cc + n10) + acp * ld(Cc + n01) +
+                           app * ld(Cc + n11);
+                    g[c] = half * (vp + vc);
+                }
+                ex = g[0]; ey = g[1]; ez = g[2]; bx = g[3]; by = g[4]; bz = g[5];
+            }
+            const T inv1 = one / (one - Vxp);
+            const T kE = a.sE * inv1;                 // q2m*hx/2 / (1 - Vx)
+            ex *= kE;
+            ey *= kE;
+            ez *= kE;
+            px += ex;
+            py += ey;
+            pz += ez;
+            const T gamma_r = one / sqrt_t<T>(one + px * px + py * py + pz * pz);
+            const T kB = gamma_r * kE;               // gamma_r*q2m/(1-Vx)*hx/2
+            bx = (bx + a.bxe) * kB;
+            by = (by + a.bye) * kB;
+            bz = (bz + a.bze) * kB;
+            const T co = two / (one + bx * bx + by * by + bz * bz);
+            const T p3x = (py * bz - pz * by + px) * co;
+            const T p3y = (pz * bx - px * bz + py) * co;
+            const T p3z = (px * by - py * bx + pz) * co;
+            px += ex + (p3y * bz - p3z * by);
+            py += ey + (p3z * bx - p3x * bz);
+            pz += ez + (p3x * by - p3y * bx);
+            const T inv_g = one / sqrt_t<T>(one + px * px + py * py + pz * pz);
+            const T Vxm = px * inv_g, Vym = py * inv_g, Vzm = pz * inv_g;
+            const T Vx = half * (Vxm + Vxp);
+            const T Vy = half * (Vym + Vyp);
+            const T Vz = half * (Vzm + Vzp);
+            const T inv2 = one / (one - Vx);
+            const T wq = weight * inv2;
+            const T djx = wq * a.djx0 * Vxm;
+            const T djy = wq * a.djy0 * Vym;
+            const T djz = wq * a.djz0 * Vzm;
+            const T drho = wq * a.drho0;
+            const T dy = Vy * a.hxhy * inv2;
+            const T dz = Vz * a.hxhz * inv2;
+            move_and_deposit<T, SHAPE, PRECISE, NV>(a, i, j, k, yp, zp, px, py, pz, djx, djy, djz,
+                                                   drho, dy, dz, key, v);
+            } else {
+            T gammap = sqrt_t<T>(one + px * px + py * py + pz * pz);
+            T Vx = px / gammap;
+            const T Vxp = Vx, Vyp = py / gammap, Vzp = pz / gammap;
+            const T q2m = a.q2m;
+            const size_t plane = a.plane;
+            T ex, ey, ez, bx, by, bz;
+            if (SHAPE == QS_SHAPE_NGP) {
+                const size_t n = (size_t)cell;
+                ex = half * (ld(a.P + 0 * plane + n) + ld(a.C + 0 * plane + n));
+                ey = half * (ld(a.P + 1 * plane + n) + ld(a.C + 1 * plane + n));
+                ez = half * (ld(a.P + 2 * plane + n) + ld(a.C + 2 * plane + n));
+                bx = half * (ld(a.P + 3 * plane + n) + ld(a.C + 3 * plane + n));
+                by = half * (ld(a.P + 4 * plane + n) + ld(a.C + 4 * plane + n));
+                bz = half * (ld(a.P + 5 * plane + n) + ld(a.C + 5 * plane + n));
+            } else {
+                const T ayc = one - yp, ayp = yp, azc = one - zp, azp = zp;
+                const T acc = ayc * azc, apc = ayp * azc, acp = ayc * azp, app = ayp * azp;
+                const int j1 = wrap_idx(j + 1, My), k1 = wrap_idx(k + 1, Mz);
+                const size_t n00 = (size_t)j + (size_t)My * k, n10 = (size_t)j1 + (size_t)My * k,
+                             n01 = (size_t)j + (size_t)My * k1, n11 = (size_t)j1 + (size_t)My * k1;
+                T g[6];
+#pragma unroll
+                for (int c = 0; c < 6; c++) {
+                    const T* Pc = a.P + c * plane;
+                    const T* Cc = a.C + c * plane;
+                    T vp = acc * ld(Pc + n00) + apc * ld(Pc + n10) + acp * ld(Pc + n01) +
+                           app * ld(Pc + n11);
+                    T vc = acc * ld(Cc + n00) + apc * ld(Cc + n10) + acp * ld(Cc + n01) +
+                           app * ld(Cc + n11);
+                    g[c] = half * (vp + vc);
+                }
+                ex = g[0]; ey = g[1]; ez = g[2]; bx = g[3]; by = g[4]; bz = g[5];
+            }
+            const T hx = a.hx;
+            const T sE = q2m * hx / two;
+            ex *= sE;
+            ey *= sE;
+            ez *= sE;
+            px += ex / (one - Vx);
+            py += ey / (one - Vx);
+            pz += ez / (one - Vx);
+            T gamma = sqrt_t<T>(one + px * px + py * py + pz * pz);
+            const T gamma_r = one / gamma;
+            bx += a.bxe;
+            by += a.bye;
+            bz += a.bze;
+            bx = bx * gamma_r * q2m / (one - Vx) * hx / two;
+            by = by * gamma_r * q2m / (one - Vx) * hx / two;
+            bz = bz * gamma_r * q2m / (one - Vx) * hx / two;
+            const T co = two / (one + (bx * bx) + (by * by) + (bz * bz));
+            T p3x = py * bz - pz * by + px;
+            T p3y = pz * bx - px * bz + py;
+            T p3z = px * by - py * bx + pz;
+            p3x *= co;
+            p3y *= co;
+            p3z *= co;
+            const T px_new = p3y * bz - p3z * by;
+            const T py_new = p3z * bx - p3x * bz;
+            const T pz_new = p3x * by - p3y * bx;
+            px += ex / (one - Vx) + px_new;
+            py += ey / (one - Vx) + py_new;
+            pz += ez / (one - Vx) + pz_new;
+            gamma = sqrt_t<T>(one + px * px + py * py + pz * pz);
+            const T Vxm = px / gamma, Vym = py / gamma, Vzm = pz / gamma;
+            Vx = half * (Vxm + Vxp);
+            const T Vy = half * (Vym + Vyp);
+            const T Vz = half * (Vzm + Vzp);
+            T djx = weight * a.djx0 * Vxm;
+            T djy = weight * a.djy0 * Vym;
+            T djz = weight * a.djz0 * Vzm;
+            T drho = weight * a.drho0;
+            djx *= one / (one - Vx);
+            djy *= one / (one - Vx);
+            djz *= one / (one - Vx);
+            drho *= one / (one - Vx);
+            T dy = Vy * hx / a.hy;
+            T dz = Vz * hx / a.hz;
+            dy = dy / (one - Vx);
+            dz = dz / (one - Vx);
+            move_and_deposit<T, SHAPE, PRECISE, NV>(a, i, j, k, yp, zp, px, py, pz, djx, djy, djz,
+                                                   drho, dy, dz, key, v);
+            }
+        }
+    }
+
+    // warp-segmented sum over runs of equal first-deposit cell
+    const unsigned full = 0xffffffffu;
+    const int nextKey = __shfl_down_sync(full, key, 1);
+    const int prevKey = __shfl_up_sync(full, key, 1);
+    const bool last = (lane == 31) || (nextKey != key);
+    const unsigned lastMask = __ballot_sync(full, last);
+    const int end = __ffs(lastMask & (full << lane)) - 1;
+    const bool head = (lane == 0) || (prevKey != key);
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+#pragma unroll
+        for (int c = 0; c < NV; c++) {
+            const T o = __shfl_down_sync(full, v[c], d);
+            if (lane + d <= end) v[c] += o;
+        }
+    }
+    if (head && key >= 0) {
+        const size_t plane = a.plane;
+        if (SHAPE == QS_SHAPE_NGP) {
+            const size_t n = (size_t)key;
+#pragma unroll
+            for (int qq = 0; qq < 4; qq++) atomicAdd(a.dep + qq * plane + n, v[qq]);
+        } else {
+            const int fj = key % My, fk = key / My;
+            const int j1 = wrap_idx(fj + 1, My), k1 = wrap_idx(fk + 1, Mz);
+            const size_t nn[4] = {(size_t)fj + (size_t)My * fk, (size_t)j1 + (size_t)My * fk,
+                                  (size_t)fj + (size_t)My * k1, (size_t)j1 + (size_t)My * k1};
+#pragma unroll
+            for (int cnr = 0; cnr < 4; cnr++)
+#pragma unroll
+                for (int qq = 0; qq < 4; qq++)
+                    atomicAdd(a.dep + qq * plane + nn[cnr], v[cnr * 4 + qq]);
+        }
+    }
+}
+
+template <class T>
+int launch_push(const PushArgs<T>& a, int shape, bool precise, cudaStream_t st) {
+    if (a.n <= 0) return 0;
+    constexpr bool F32 = sizeof(T) == 4;
+    const int threads = 256;
+    const unsigned blocks = (unsigned)((a.n + threads - 1) / threads);
+    if (shape == QS_SHAPE_NGP) {
+        if constexpr (F32) {
+            push_kernel<T, QS_SHAPE_NGP, true, true><<<blocks, threads, 0, st>>>(a);
+        } else {
+            if (precise) push_kernel<T, QS_SHAPE_NGP, true, false><<<blocks, threads, 0, st>>>(a);
+            else push_kernel<T, QS_SHAPE_NGP, false, false><<<blocks, threads, 0, st>>>(a);
+        }
+    } else {
+        push_kernel<T, QS_SHAPE_CIC, true, F32><<<blocks, threads, 0, st>>>(a);
+    }
+    return 1;
+}
+
+}  // namespace qs

@@ -62,6 +62,8 @@ struct PushArgs {
     int32_t* dep_cell;    // optional: folded cell of the last deposit
     size_t plane;
     T hx, hy, hz, q2m, djx0, djy0, djz0, drho0, bxe, bye, bze;
+    T sE, hxhy, hxhz;     // q2m*hx/2, hx/hy, hx/hz (factored FP32 form)
+    float invMy;          // 1/My for the cell index split
     int full;
     int* err;
 };

@@ -11,10 +11,23 @@ struct SpecArgs {
     T piY, piZ;          // M_PI/Ylength, M_PI/Zlength
     T hx, dens;
     const T *RhoP, *ExP, *EyP, *EzP, *JxP, *JyP, *JzP;   // P spectral state
-    const T *Rb, *Rbp, *Jxb;                              // beam spectra (C, P)
+    // beam spectra of this (layer, split): w0*X0 + w1*X1 (the xi-interpolation
+    // of movepart_splitlayer.cpp:330-348 applied to the spectra), and of the
+    // previous (layer, split) for RhoBeamP (weights 0 at the head layer)
+    const T *Rb0, *Rb1, *Jxb0, *Jxb1;
+    T wb0, wb1;
+    const T *Rbp0, *Rbp1;
+    T wp0, wp1;
     const T *Jx, *Jy, *Jz;                                // forward of the C deposit
     T* Rho;                                               // in/out spectral rho
     T *Ex, *Ey, *Ez, *Bx, *By, *Bz;                       // spectral outputs
+    int write_b;         // store Bx, By, Bz spectra (exact-GEMM transforms read them)
+    // split-precision operand of the inverse transform: slots 0..5 = Ex,Ey,Ez,
+    // Bx,By,Bz, slot 6 = Rho when split_rho; term s of slot f at
+    // split + s*tstride + f*ny*nz (bf16 for split_kind 0, tf32 for 1)
+    void* split;
+    int nsplit, split_kind, split_rho;
+    size_t tstride;
 };
 
 template <class T>
@@ -27,6 +40,9 @@ int launch_corrector(const SpecArgs<T>& a, cudaStream_t st);
 template <class T>
 int launch_beam_layer(const T* cur, const T* nxt, int S, int s, T* out, size_t plane, int* err,
                       cudaStream_t st);
+// |JxBeam| > 10 anywhere in the beam-current store (layers x [RhoBeam, JxBeam])
+template <class T>
+int launch_beam_check(const T* b3, int nlayers, size_t plane, int* err, cudaStream_t st);
 
 template <class T>
 int launch_onaxis(const T* fields3d, int L, size_t plane, size_t idx, T* out, cudaStream_t st);
@@ -52,7 +68,7 @@ int run_dtt_simt_pass(int pass, const DttJob<T>& job, int ny, int nz, const DttM
 
 // kernel classes of the per-kernel timing (qs_profile_read)
 enum KernelClass {
-    KC_PUSH = 0, KC_GEMM = 1, KC_SPLIT = 2, KC_SPECTRAL = 3, KC_BEAM_LAYER = 4,
+    KC_PUSH = 0, KC_GEMM = 1, KC_SPLIT = 2, KC_SPECTRAL = 3, KC_BEAM_SPECTRA = 4,
     KC_BEAM_PUSH = 5, KC_SEED = 6, KC_MISC = 7, KC_N = 8
 };
 

@@ -16,8 +16,23 @@
 
 #include "qs_common.cuh"
 #include "qs_internal.h"
+#include "split.cuh"
 
 namespace qs {
+
+template <class T>
+__device__ __forceinline__ void put_split(const SpecArgs<T>& a, int slot, int n1, T v) {
+    const size_t idx = (size_t)slot * a.ny * a.nz + n1;
+    if (a.split_kind == 0) store_split<0>(a.split, a.tstride, idx, (float)v, a.nsplit);
+    else store_split<1>(a.split, a.tstride, idx, (float)v, a.nsplit);
+}
+
+template <class T>
+__device__ __forceinline__ void beam_terms(const SpecArgs<T>& a, int n1, T& rb, T& rbp, T& jxb) {
+    rb = a.wb0 * a.Rb0[n1] + a.wb1 * a.Rb1[n1];
+    jxb = a.wb0 * a.Jxb0[n1] + a.wb1 * a.Jxb1[n1];
+    rbp = a.wp0 * a.Rbp0[n1] + a.wp1 * a.Rbp1[n1];
+}
 
 template <class T>
 __global__ void predictor_kernel(SpecArgs<T> a) {
@@ -32,7 +47,8 @@ __global__ void predictor_kernel(SpecArgs<T> a) {
     const T rp = a.RhoP[n1];
     const T jxp = a.JxP[n1], jyp = a.JyP[n1], jzp = a.JzP[n1];
     const T exp_ = a.ExP[n1], eyp = a.EyP[n1], ezp = a.EzP[n1];
-    const T rb = a.Rb[n1], rbp = a.Rbp[n1];
+    T rb, rbp, jxb;
+    beam_terms(a, n1, rb, rbp, jxb);
     const T propagator = (T(4) - d * hx * hx) / (T(4) + d * hx * hx);
     const T denominator = T(4) + d * hx * hx;
     const T rho = propagator * rp - (rb + rbp) * d * hx * hx / denominator +
@@ -43,14 +59,26 @@ __global__ void predictor_kernel(SpecArgs<T> a) {
     const T jy = jyp + hx * d * (ey + eyp) / T(2);
     const T jz = jzp + hx * d * (ez + ezp) / T(2);
     const T jx = jxp + hx * d * (ex + exp_) / T(2);
-    const T jxb = a.Jxb[n1];
+    const T bx = -aky / ak2 * jz + akz / ak2 * jy;
+    const T by = (-akz * (jx + jxb) + d * ez) / ak2;
+    const T bz = (aky * (jx + jxb) - d * ey) / ak2;
     a.Rho[n1] = rho;
     a.Ex[n1] = ex;
     a.Ey[n1] = ey;
     a.Ez[n1] = ez;
-    a.Bx[n1] = -aky / ak2 * jz + akz / ak2 * jy;
-    a.By[n1] = (-akz * (jx + jxb) + d * ez) / ak2;
-    a.Bz[n1] = (aky * (jx + jxb) - d * ey) / ak2;
+    if (a.write_b) {
+        a.Bx[n1] = bx;
+        a.By[n1] = by;
+        a.Bz[n1] = bz;
+    }
+    if (a.split) {
+        put_split(a, 0, n1, ex);
+        put_split(a, 1, n1, ey);
+        put_split(a, 2, n1, ez);
+        put_split(a, 3, n1, bx);
+        put_split(a, 4, n1, by);
+        put_split(a, 5, n1, bz);
+    }
 }
 
 template <class T>
@@ -66,20 +94,34 @@ __global__ void corrector_kernel(SpecArgs<T> a) {
     const T rp = a.RhoP[n1];
     const T jx = a.Jx[n1], jy = a.Jy[n1], jz = a.Jz[n1];
     const T rho = rp + jx - a.JxP[n1] - hx * (aky * (jy + a.JyP[n1]) + akz * (jz + a.JzP[n1])) / T(2);
-    const T rb = a.Rb[n1], rbp = a.Rbp[n1];
+    T rb, rbp, jxb;
+    beam_terms(a, n1, rb, rbp, jxb);
     const T eyp = a.EyP[n1], ezp = a.EzP[n1];
     const T rho_old = a.Rho[n1];
     const T newEx = -(aky * jy + akz * jz) / ak2;
     const T newEy = -eyp + aky * (rb + rbp + rp + rho_old) / (d + ak2);
     const T newEz = -ezp + akz * (rb + rbp + rp + rho_old) / (d + ak2);
-    const T jxb = a.Jxb[n1];
+    const T bx = -aky / ak2 * jz + akz / ak2 * jy;
+    const T by = (-akz * (jx + jxb) + d * newEz) / ak2;
+    const T bz = (aky * (jx + jxb) - d * newEy) / ak2;
     a.Ey[n1] = newEy;
     a.Ez[n1] = newEz;
     a.Rho[n1] = rho;
     a.Ex[n1] = newEx;
-    a.Bx[n1] = -aky / ak2 * jz + akz / ak2 * jy;
-    a.By[n1] = (-akz * (jx + jxb) + d * newEz) / ak2;
-    a.Bz[n1] = (aky * (jx + jxb) - d * newEy) / ak2;
+    if (a.write_b) {
+        a.Bx[n1] = bx;
+        a.By[n1] = by;
+        a.Bz[n1] = bz;
+    }
+    if (a.split) {
+        put_split(a, 0, n1, newEx);
+        put_split(a, 1, n1, newEy);
+        put_split(a, 2, n1, newEz);
+        put_split(a, 3, n1, bx);
+        put_split(a, 4, n1, by);
+        put_split(a, 5, n1, bz);
+        if (a.split_rho) put_split(a, 6, n1, rho);
+    }
 }
 
 template <class T>
@@ -120,6 +162,21 @@ int launch_beam_layer(const T* cur, const T* nxt, int S, int s, T* out, size_t p
                       cudaStream_t st) {
     beam_layer_kernel<T><<<(unsigned)((plane + 255) / 256), 256, 0, st>>>(cur, nxt, S, s, out,
                                                                           plane, err);
+    return 1;
+}
+
+template <class T>
+__global__ void beam_check_kernel(const T* __restrict__ b3, int nlayers, size_t plane, int* err) {
+    const size_t n = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = blockIdx.y;
+    if (n >= plane || i >= nlayers) return;
+    if (fabs((double)b3[((size_t)i * 2 + 1) * plane + n]) > 10.0) atomicOr(err, DEV_ERR_BEAM_CURRENT);
+}
+
+template <class T>
+int launch_beam_check(const T* b3, int nlayers, size_t plane, int* err, cudaStream_t st) {
+    dim3 g((unsigned)((plane + 255) / 256), nlayers);
+    beam_check_kernel<T><<<g, 256, 0, st>>>(b3, nlayers, plane, err);
     return 1;
 }
 
@@ -243,6 +300,7 @@ int launch_convert_back(const T* src, double* dst, size_t n, cudaStream_t st) {
     template int launch_beam_layer<T>(const T*, const T*, int, int, T*, size_t, int*,           \
                                       cudaStream_t);                                            \
     template int launch_onaxis<T>(const T*, int, size_t, size_t, T*, cudaStream_t);            \
+    template int launch_beam_check<T>(const T*, int, size_t, int*, cudaStream_t);              \
     template int launch_seed_front<T>(int, int, int, const double*, const double*, double,      \
                                       double, double, double, double, double, double,           \
                                       uint64_t, uint64_t, int32_t*, T*, T*, T*, T*, T*, T*,     \

@@ -55,7 +55,10 @@ def test_push_fp64_bitexact(oracle_lib, shape, full):
 
 
 @pytest.mark.parametrize("shape", [QS_SHAPE_NGP, QS_SHAPE_CIC])
-def test_push_fp32_bitexact_vs_float_oracle(oracle_lib, shape):
+def test_push_fp32_matches_float_oracle(oracle_lib, shape):
+    """The FP32 kernel factors the divisions and contracts to FMA, so it
+    matches the oracle's float restatement to FP32 rounding; the deposit cells
+    (where a particle's current lands) agree exactly."""
     cfg = cfg_for("fp32", n=32, layers=4, shape=shape)
     p, P, C = state(cfg, 21 + shape)
     f32 = lambda a: np.asarray(a, dtype=np.float32)
@@ -65,8 +68,10 @@ def test_push_fp32_bitexact_vs_float_oracle(oracle_lib, shape):
     r = oracle_lib.push_layer(cfg, p32["cell"], p32["y"], p32["z"], p32["px"], p32["py"],
                               p32["pz"], p32["w"], f32(P), f32(C), full=True, precise=True,
                               dtype=np.float32)
-    for k in ("y", "z", "px", "py", "pz"):
-        assert np.array_equal(q[k], r[k].astype(np.float64)), k
+    for k in ("px", "py", "pz"):
+        np.testing.assert_allclose(q[k], r[k], rtol=2e-6, atol=2e-7)
+    for k in ("y", "z"):
+        np.testing.assert_allclose(q[k], r[k], rtol=0, atol=2e-6)
     assert np.array_equal(q["cell"], r["cell"])
     assert np.array_equal(dep != 0, r["dep"] != 0)
     np.testing.assert_allclose(dep, r["dep"], rtol=2e-5, atol=1e-6)
