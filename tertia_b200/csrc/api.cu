@@ -206,6 +206,7 @@ struct Engine : EngineBase {
     int32_t* pcell = nullptr;
     T *py = nullptr, *pz = nullptr, *ppx = nullptr, *ppy = nullptr, *ppz = nullptr, *pw = nullptr;
     bool front_pending = false;
+    bool uniform_layout = false;   // particle p in cell p / ppc (lattice seeding)
     // beam
     int64_t nb = 0, nb_cap = 0;
     int32_t *bi = nullptr, *bj = nullptr, *bk = nullptr;
@@ -433,6 +434,9 @@ struct Engine : EngineBase {
         qs_status s = ensure_plasma(n);
         if (s) return s;
         np = n;
+        uniform_layout = (n == (int64_t)plane * cfg.ppc);
+        for (int64_t p = 0; p < n && uniform_layout; p++)
+            if (cell[p] != (int32_t)(p / cfg.ppc)) uniform_layout = false;
         if (n) {
             CK(cudaMemcpyAsync(pcell, cell, n * 4, cudaMemcpyHostToDevice, st));
             const double* src[6] = {y, z, px, py_, pz_, w};
@@ -458,6 +462,7 @@ struct Engine : EngineBase {
         qs_status s = ensure_plasma((int64_t)plane * ppc);
         if (s) return s;
         np = (int64_t)plane * ppc;
+        uniform_layout = true;
         // in-cell lattice of Mesh::SeedParticles (mesh.cpp:436-470), head first
         double oy[16], oz[16];
         int iside = (int)(std::pow((double)(ppc - 1), 0.5) + 1.0);
@@ -827,6 +832,7 @@ struct Engine : EngineBase {
         a.hxhy = (T)((cfg.hx / S) / cfg.hy);
         a.hxhz = (T)((cfg.hx / S) / cfg.hz);
         a.invMy = 1.0f / (float)My;
+        a.uniform_ppc = (cfg.shape == QS_SHAPE_NGP && uniform_layout) ? cfg.ppc : 0;
         a.full = full;
         a.err = d_err;
         const bool precise = sizeof(T) == 4;

@@ -42,7 +42,7 @@ namespace qs {
 namespace tcx {
 
 constexpr int BM = 128;   // output rows per tile (matrix rows, MMA M)
-constexpr int BN_MAX = 128;   // output columns per tile (data rows, MMA N): 64 or 128
+
 constexpr uint32_t SPIN_LIMIT = 1u << 22;
 
 struct Params {

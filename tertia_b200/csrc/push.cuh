@@ -392,6 +392,112 @@ __global__ void __launch_bounds__(256) push_kernel(PushArgs<T> a) {
     }
 }
 
+// ---------------------------------------------------------------------------
+// FP32 NGP push, one thread per cell, for the uniform lattice layout
+// (particle p of the layer sits in cell p / PPC): in the live reference path a
+// particle never leaves its seeded cell, so this layout is permanent.  The
+// cell's fields are gathered once, its PPC particles are read and written as
+// float4 vectors, deposits into the cell itself are summed in registers and
+// flushed with 4 atomics; deposits that land in another cell go straight to
+// global atomics.  Same physics as push_kernel<float, NGP, precise, fast>,
+// with approximate reciprocals (a few ulp) for the divisions.
+template <int PPC>
+__global__ void __launch_bounds__(128) push_cell_kernel(PushArgs<float> a) {
+    static_assert(PPC == 4, "float4 particle vectors");
+    const int cell = blockIdx.x * blockDim.x + threadIdx.x;
+    const int My = a.My, Mz = a.Mz;
+    if (cell >= My * Mz) return;
+    int j, k;
+    cell_jk(cell, My, a.invMy, j, k);
+    const size_t plane = a.plane;
+    const size_t n = (size_t)cell;
+    const float ex0 = 0.5f * (ld(a.P + 0 * plane + n) + ld(a.C + 0 * plane + n));
+    const float ey0 = 0.5f * (ld(a.P + 1 * plane + n) + ld(a.C + 1 * plane + n));
+    const float ez0 = 0.5f * (ld(a.P + 2 * plane + n) + ld(a.C + 2 * plane + n));
+    const float bx0 = 0.5f * (ld(a.P + 3 * plane + n) + ld(a.C + 3 * plane + n)) + a.bxe;
+    const float by0 = 0.5f * (ld(a.P + 4 * plane + n) + ld(a.C + 4 * plane + n)) + a.bye;
+    const float bz0 = 0.5f * (ld(a.P + 5 * plane + n) + ld(a.C + 5 * plane + n)) + a.bze;
+    const size_t base = (size_t)cell * PPC;
+    float4 Y = *(const float4*)(a.y + base), Z = *(const float4*)(a.z + base);
+    float4 PX = *(const float4*)(a.px + base), PY = *(const float4*)(a.py + base);
+    float4 PZ = *(const float4*)(a.pz + base);
+    const float4 W = *(const float4*)(a.w + base);
+    float* yv = &Y.x; float* zv = &Z.x; float* pxv = &PX.x; float* pyv = &PY.x;
+    float* pzv = &PZ.x; const float* wv = &W.x;
+    float own0 = 0.f, own1 = 0.f, own2 = 0.f, own3 = 0.f;
+#pragma unroll
+    for (int q = 0; q < PPC; q++) {
+        const float yp = yv[q], zp = zv[q];
+        if (!(yp >= 0.f && yp <= 1.f && zp >= 0.f && zp <= 1.f)) {
+            atomicOr(a.err, DEV_ERR_RANGE);
+            continue;
+        }
+        float px = pxv[q], py = pyv[q], pz = pzv[q];
+        const float inv_gp = rsqrtf(1.f + px * px + py * py + pz * pz);
+        const float Vxp = px * inv_gp, Vyp = py * inv_gp, Vzp = pz * inv_gp;
+        const float kE = a.sE * __frcp_rn(1.f - Vxp);
+        const float ex = ex0 * kE, ey = ey0 * kE, ez = ez0 * kE;
+        px += ex; py += ey; pz += ez;
+        const float kB = rsqrtf(1.f + px * px + py * py + pz * pz) * kE;
+        const float bx = bx0 * kB, by = by0 * kB, bz = bz0 * kB;
+        const float co = __fdividef(2.f, 1.f + bx * bx + by * by + bz * bz);
+        const float p3x = (py * bz - pz * by + px) * co;
+        const float p3y = (pz * bx - px * bz + py) * co;
+        const float p3z = (px * by - py * bx + pz) * co;
+        px += ex + (p3y * bz - p3z * by);
+        py += ey + (p3z * bx - p3x * bz);
+        pz += ez + (p3x * by - p3y * bx);
+        const float inv_g = rsqrtf(1.f + px * px + py * py + pz * pz);
+        const float Vxm = px * inv_g, Vym = py * inv_g, Vzm = pz * inv_g;
+        const float Vx = 0.5f * (Vxm + Vxp), Vy = 0.5f * (Vym + Vyp), Vz = 0.5f * (Vzm + Vzp);
+        const float inv2 = __frcp_rn(1.f - Vx);
+        const float wq = wv[q] * inv2;
+        const float djx = wq * a.djx0 * Vxm, djy = wq * a.djy0 * Vym, djz = wq * a.djz0 * Vzm;
+        const float drho = wq * a.drho0;
+        const float dy = Vy * a.hxhy * inv2, dz = Vz * a.hxhz * inv2;
+        float partdx = 0.f, step = 1.f;
+        if (fabsf(dy) > 1.f || fabsf(dz) > 1.f) step = partdx = fmaxf(fabsf(dy), fabsf(dz));
+        if (partdx < 1.f) partdx = step = 1.f;
+        float ytmp = yp, ztmp = zp;
+        while (partdx > 0.f) {
+            float ps;
+            if (partdx > 1.f) { partdx -= 1.f; ps = __frcp_rn(step); }
+            else { ps = __fdividef(partdx, step); partdx = 0.f; }
+            // cell-relative update; the base cell stays the seeded cell (the
+            // reference adds the outer j_jump = j at every sub-step)
+            const float uy = ytmp + dy * ps, uz = ztmp + dz * ps;
+            const float fy = floorf(uy), fz = floorf(uz);
+            float ry = uy - fy, rz = uz - fz;
+            int sy = (int)fy, sz = (int)fz;
+            if (ry >= 1.f) { ry = 0.f; sy += 1; }
+            if (rz >= 1.f) { rz = 0.f; sz += 1; }
+            ytmp = ry;
+            ztmp = rz;
+            const float d0 = djx * ps, d1 = djy * ps, d2 = djz * ps, d3 = drho * ps;
+            if (sy == 0 && sz == 0) {
+                own0 += d0; own1 += d1; own2 += d2; own3 += d3;
+            } else {
+                const int jj = wrap_idx(j + sy, My), kk = wrap_idx(k + sz, Mz);
+                const size_t m = (size_t)jj + (size_t)My * kk;
+                atomicAdd(a.dep + 0 * plane + m, d0);
+                atomicAdd(a.dep + 1 * plane + m, d1);
+                atomicAdd(a.dep + 2 * plane + m, d2);
+                atomicAdd(a.dep + 3 * plane + m, d3);
+            }
+        }
+        yv[q] = ytmp; zv[q] = ztmp; pxv[q] = px; pyv[q] = py; pzv[q] = pz;
+    }
+    atomicAdd(a.dep + 0 * plane + n, own0);
+    atomicAdd(a.dep + 1 * plane + n, own1);
+    atomicAdd(a.dep + 2 * plane + n, own2);
+    atomicAdd(a.dep + 3 * plane + n, own3);
+    if (a.full) {
+        *(float4*)(a.y + base) = Y; *(float4*)(a.z + base) = Z;
+        *(float4*)(a.px + base) = PX; *(float4*)(a.py + base) = PY;
+        *(float4*)(a.pz + base) = PZ;
+    }
+}
+
 template <class T>
 int launch_push(const PushArgs<T>& a, int shape, bool precise, cudaStream_t st) {
     if (a.n <= 0) return 0;
@@ -400,6 +506,11 @@ int launch_push(const PushArgs<T>& a, int shape, bool precise, cudaStream_t st) 
     const unsigned blocks = (unsigned)((a.n + threads - 1) / threads);
     if (shape == QS_SHAPE_NGP) {
         if constexpr (F32) {
+            if (a.uniform_ppc == 4 && a.n == (int64_t)a.My * a.Mz * 4 && !a.dep_cell) {
+                const int cells = a.My * a.Mz;
+                push_cell_kernel<4><<<(cells + 127) / 128, 128, 0, st>>>(a);
+                return 1;
+            }
             push_kernel<T, QS_SHAPE_NGP, true, true><<<blocks, threads, 0, st>>>(a);
         } else {
             if (precise) push_kernel<T, QS_SHAPE_NGP, true, false><<<blocks, threads, 0, st>>>(a);

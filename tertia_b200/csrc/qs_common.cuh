@@ -64,6 +64,7 @@ struct PushArgs {
     T hx, hy, hz, q2m, djx0, djy0, djz0, drho0, bxe, bye, bze;
     T sE, hxhy, hxhz;     // q2m*hx/2, hx/hy, hx/hz (factored FP32 form)
     float invMy;          // 1/My for the cell index split
+    int uniform_ppc;      // >0: particle p sits in cell p / uniform_ppc (lattice layout)
     int full;
     int* err;
 };

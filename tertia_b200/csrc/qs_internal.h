@@ -34,6 +34,9 @@ template <class T>
 int launch_predictor(const SpecArgs<T>& a, cudaStream_t st);
 template <class T>
 int launch_corrector(const SpecArgs<T>& a, cudaStream_t st);
+// FP32 forms (spectral_f32.cu); return 0 when the shape is not handled
+int launch_predictor_fast(const SpecArgs<float>& a, cudaStream_t st);
+int launch_corrector_fast(const SpecArgs<float>& a, cudaStream_t st);
 
 // C-layer beam currents for (iLayer, iSplit): the xi-interpolation of
 // movepart_splitlayer.cpp:330-348 plus the |JxBeam| > 10 check.

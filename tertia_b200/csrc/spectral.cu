@@ -126,12 +126,18 @@ __global__ void corrector_kernel(SpecArgs<T> a) {
 
 template <class T>
 int launch_predictor(const SpecArgs<T>& a, cudaStream_t st) {
+    if constexpr (sizeof(T) == 4) {
+        if (launch_predictor_fast(a, st)) return 1;
+    }
     const int N = a.ny * a.nz;
     predictor_kernel<T><<<(N + 255) / 256, 256, 0, st>>>(a);
     return 1;
 }
 template <class T>
 int launch_corrector(const SpecArgs<T>& a, cudaStream_t st) {
+    if constexpr (sizeof(T) == 4) {
+        if (launch_corrector_fast(a, st)) return 1;
+    }
     const int N = a.ny * a.nz;
     corrector_kernel<T><<<(N + 255) / 256, 256, 0, st>>>(a);
     return 1;

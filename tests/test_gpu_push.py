@@ -54,13 +54,25 @@ def test_push_fp64_bitexact(oracle_lib, shape, full):
     np.testing.assert_allclose(dep, r["dep"], rtol=1e-12, atol=1e-14)
 
 
-@pytest.mark.parametrize("shape", [QS_SHAPE_NGP, QS_SHAPE_CIC])
-def test_push_fp32_matches_float_oracle(oracle_lib, shape):
-    """The FP32 kernel factors the divisions and contracts to FMA, so it
-    matches the oracle's float restatement to FP32 rounding; the deposit cells
+def thinned(p):
+    """The lattice with every seventh particle removed (cells stay grouped in
+    ascending order, but not PPC to a cell): the NGP push then takes the
+    one-thread-per-particle kernel instead of the one-thread-per-cell kernel
+    of the full lattice."""
+    keep = np.arange(len(p["y"])) % 7 != 3
+    return {k: np.asarray(v)[keep] for k, v in p.items()}
+
+
+@pytest.mark.parametrize("shape,layout", [(QS_SHAPE_NGP, "lattice"), (QS_SHAPE_NGP, "thinned"),
+                                          (QS_SHAPE_CIC, "lattice")])
+def test_push_fp32_matches_float_oracle(oracle_lib, shape, layout):
+    """The FP32 kernels factor the divisions and contract to FMA, so they
+    match the oracle's float restatement to FP32 rounding; the deposit cells
     (where a particle's current lands) agree exactly."""
     cfg = cfg_for("fp32", n=32, layers=4, shape=shape)
     p, P, C = state(cfg, 21 + shape)
+    if layout == "thinned":
+        p = thinned(p)
     f32 = lambda a: np.asarray(a, dtype=np.float32)
     p32 = {k: (f32(v) if k != "cell" else v) for k, v in p.items()}
     q, dep = gpu_push(cfg, {k: np.asarray(v, dtype=np.float64) for k, v in p32.items()},
