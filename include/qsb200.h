@@ -236,6 +236,24 @@ qs_status qs_transform2d(qs_handle* h, int kind_z, int kind_y, int batch,
 qs_status qs_transform2d_dev(qs_handle* h, int kind_z, int kind_y, int batch,
                              const void* d_in, void* d_out);
 
+/* No counterpart in the reference.  The FP64 transform of qs_transform2d_dev
+ * for callers that cannot allocate device memory (a plugin that may only use
+ * buffers its host framework's allocator hands it, so it cannot hold a
+ * qs_handle, whose creation allocates).  No handle: it runs on the current
+ * device, enqueued on `stream` (a cudaStream_t; NULL = legacy default stream),
+ * and calls no cudaMalloc, cudaFree or other allocating routine.  d_in and
+ * d_out are device arrays of batch nz x ny double planes.  Its only other
+ * memory is a fixed 6 MiB scratch array inside the library's CUDA module,
+ * which each GPU that loads the module holds until the process exits; it
+ * limits ny and nz to 512 (each a multiple of 8): larger sizes return
+ * QS_ERR_INVALID with the reason in qs_last_error(NULL).  The first call on a
+ * device looks up the array's device address (once per device), so make that
+ * first call before any stream capture.  All calls on a device share the
+ * array: calls whose GPU work overlaps (other streams, other host threads)
+ * race and must be ordered by the caller. */
+qs_status qs_transform2d_noalloc(int kind_z, int kind_y, int ny, int nz, int batch,
+                                 const double* d_in, double* d_out, void* stream);
+
 /* One step through host buffers (the e2e entry point): copies the beam in
  * from host, seeds the front plasma, runs qs_step, copies the beam and the
  * on-axis Ex back.  Any out pointer may be NULL to skip that copy. */

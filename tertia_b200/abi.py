@@ -173,6 +173,7 @@ def _declare(L):
     L.qs_iterate_fields.argtypes = [P, C.c_int, C.c_int, C.c_int, f64p]
     L.qs_transform2d.argtypes = [P, C.c_int, C.c_int, C.c_int, f64p, f64p]
     L.qs_transform2d_dev.argtypes = [P, C.c_int, C.c_int, C.c_int, P, P]
+    L.qs_transform2d_noalloc.argtypes = [C.c_int] * 5 + [P, P, P]
     L.qs_step_host.argtypes = ([P, C.c_int64] + [i32p] * 3 + [f64p] * 7 + [i32p] * 3 +
                                [f64p] * 6 + [f64p])
     L.qs_kernel_launches.argtypes = [P]
@@ -190,7 +191,8 @@ EXPORTED_SYMBOLS = [
     "qs_get_beam_currents", "qs_get_onaxis_ex", "qs_get_psi", "qs_step",
     "qs_move_beam_particles", "qs_move_all_split_layers", "qs_begin_march", "qs_layer_begin",
     "qs_move_split_layer", "qs_guess_fields", "qs_move_particles_layer", "qs_iterate_fields",
-    "qs_layer_end", "qs_transform2d", "qs_transform2d_dev", "qs_step_host",
+    "qs_layer_end", "qs_transform2d", "qs_transform2d_dev", "qs_transform2d_noalloc",
+    "qs_step_host",
     "qs_kernel_launches", "qs_profile_enable", "qs_profile_read",
 ]
 

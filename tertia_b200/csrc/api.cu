@@ -30,6 +30,9 @@ namespace qs {
 
 static thread_local std::string g_create_error;
 
+// error text of calls made without a handle (read by qs_last_error(NULL))
+void set_unbound_error(const std::string& why) { g_create_error = why; }
+
 struct EngineBase {
     qs_config cfg{};
     int My = 0, Mz = 0, L = 0, S = 1, nIter = 1;
