@@ -27,6 +27,64 @@ def build(force: bool = False) -> str:
     return _LIB_PATH
 
 
+REF_LIB_PATH = os.path.join(_HERE, "_ref", "libref_linearized.so")
+REFERENCE = "/root/reference"
+
+
+def build_reference() -> str | None:
+    """Compile the reference's CUDA twins of the per-mode spectral maps into
+    oracle/_ref/ (only where the reference checkout is present); returns the
+    library path or None."""
+    if os.path.isdir(os.path.join(REFERENCE, "CUDA_WRAP")):
+        subprocess.run(["make", "-C", _HERE, "ref", f"REFERENCE={REFERENCE}"], check=True,
+                       capture_output=True)
+    return REF_LIB_PATH if os.path.exists(REF_LIB_PATH) else None
+
+
+def reference_lib():
+    """The built reference twins (ref_linearized_loop, ref_linearized_iterate_loop)
+    or None when they were not built."""
+    if not os.path.exists(REF_LIB_PATH):
+        return None
+    L = C.CDLL(REF_LIB_PATH)
+    for name in ("ref_linearized_loop", "ref_linearized_iterate_loop"):
+        getattr(L, name).argtypes = [C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
+                                     C.c_double, C.POINTER(C.c_void_p)]
+    return L
+
+
+def predictor_modes(ny, nz, hx, dens, ylen, zlen, P, beam):
+    """Oracle per-mode predictor.  P: dict RhoP, JxP, JyP, JzP, ExP, EyP, EzP;
+    beam: dict RhoBeam, RhoBeamP, JxBeam (flat float64 arrays of ny*nz).
+    Returns dict Rho, Ex, Ey, Ez, Jx, Jy, Jz, Bx, By, Bz."""
+    out = {k: np.empty(ny * nz) for k in ("Rho", "Ex", "Ey", "Ez", "Jx", "Jy", "Jz", "Bx",
+                                          "By", "Bz")}
+    a = [np.ascontiguousarray(P[k], dtype=np.float64) for k in
+         ("RhoP", "JxP", "JyP", "JzP", "ExP", "EyP", "EzP")]
+    b = [np.ascontiguousarray(beam[k], dtype=np.float64) for k in ("RhoBeam", "RhoBeamP",
+                                                                   "JxBeam")]
+    lib().qso_predictor_modes(ny, nz, hx, dens, ylen, zlen, *a, *b,
+                              *[out[k] for k in ("Rho", "Ex", "Ey", "Ez", "Jx", "Jy", "Jz", "Bx",
+                                                 "By", "Bz")])
+    return out
+
+
+def corrector_modes(ny, nz, hx, dens, ylen, zlen, P, beam, J, rho_old):
+    """Oracle per-mode corrector.  J: dict Jx, Jy, Jz of the C deposit;
+    rho_old: the C-layer rho spectrum before the update.
+    Returns dict Rho, Ex, Ey, Ez, Bx, By, Bz."""
+    out = {k: np.empty(ny * nz) for k in ("Ex", "Ey", "Ez", "Bx", "By", "Bz")}
+    out["Rho"] = np.array(rho_old, dtype=np.float64)
+    a = [np.ascontiguousarray(P[k], dtype=np.float64) for k in
+         ("RhoP", "JxP", "JyP", "JzP", "EyP", "EzP")]
+    b = [np.ascontiguousarray(beam[k], dtype=np.float64) for k in ("RhoBeam", "RhoBeamP",
+                                                                   "JxBeam")]
+    j = [np.ascontiguousarray(J[k], dtype=np.float64) for k in ("Jx", "Jy", "Jz")]
+    lib().qso_corrector_modes(ny, nz, hx, dens, ylen, zlen, *a, *b, *j,
+                              *[out[k] for k in ("Rho", "Ex", "Ey", "Ez", "Bx", "By", "Bz")])
+    return out
+
+
 def _stale() -> bool:
     lib_t = os.path.getmtime(_LIB_PATH)
     srcs = [os.path.join(_HERE, "qs_oracle.cpp"), os.path.join(_HERE, "qs_oracle.h"),
@@ -56,6 +114,10 @@ def _declare(L):
     L.qso_create.argtypes = [C.POINTER(QsConfig), C.POINTER(P)]
     L.qso_destroy.argtypes = [P]
     L.qso_destroy.restype = None
+    L.qso_predictor_modes.argtypes = [C.c_int, C.c_int] + [C.c_double] * 4 + [_f64p] * 20
+    L.qso_predictor_modes.restype = None
+    L.qso_corrector_modes.argtypes = [C.c_int, C.c_int] + [C.c_double] * 4 + [_f64p] * 19
+    L.qso_corrector_modes.restype = None
     L.qso_set_threads.argtypes = [C.c_int]
     L.qso_set_threads.restype = None
     L.qso_get_threads.restype = C.c_int

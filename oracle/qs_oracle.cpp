@@ -457,6 +457,92 @@ int push_layer_arrays(const qs_config* cfg, int64_t n, int32_t* cell, T* y, T* z
 // ---------------------------------------------------------------------------
 enum { NPL = 12 };  // Ex Ey Ez Bx By Bz Jx Jy Jz Dens RhoBeam JxBeam
 
+// Per-mode linear predictor of GuessFieldsHydroLinLayerSplit
+// (movefieldshydrolinlayersplit.cpp:808-900; the same formulas as the
+// reference's CUDA twin linearized_kernel, CUDA_WRAP/linearized.cu:11-103).
+// Inputs: P-layer spectra and beam spectra; outputs: C-layer spectra.
+extern "C" void qso_predictor_modes(int ny, int nz, double hx, double d, double Ylength,
+                                    double Zlength, const double* fRhoP, const double* fJxP,
+                                    const double* fJyP, const double* fJzP, const double* fExP,
+                                    const double* fEyP, const double* fEzP,
+                                    const double* fRhoBeam, const double* fRhoBeamP,
+                                    const double* fJxBeam, double* fRho, double* fEx,
+                                    double* fEy, double* fEz, double* fJx, double* fJy,
+                                    double* fJz, double* fBx, double* fBy, double* fBz) {
+    const double hxs = hx;
+    for (int k = 0; k < nz; k++)
+        for (int j = 0; j < ny; j++) {
+            double akz = M_PI / Zlength * (k + 0.5);
+            double aky = M_PI / Ylength * (j + 0.5);
+            double ak2 = aky * aky + akz * akz;
+            size_t n1 = (size_t)j + (size_t)ny * k;
+            double rp = fRhoP[n1];
+            double jxp = fJxP[n1];
+            double jyp = fJyP[n1];
+            double jzp = fJzP[n1];
+            double exp_ = fExP[n1];
+            double eyp = fEyP[n1];
+            double ezp = fEzP[n1];
+            double rb = fRhoBeam[n1];
+            double rbp = fRhoBeamP[n1];
+            double propagator = (4. - d * hxs * hxs) / (4. + d * hxs * hxs);
+            double denominator = 4. + d * hxs * hxs;
+            fRho[n1] = propagator * rp - (rb + rbp) * d * hxs * hxs / denominator +
+                       4. * exp_ * hxs * (ak2 + d) / denominator;
+            fEx[n1] = propagator * exp_ -
+                      2. * (2. * rp + rb + rbp) * d * hxs / ((ak2 + d) * denominator);
+            fEy[n1] = -eyp + aky * (rb + rbp + rp + fRho[n1]) / (d + ak2);
+            fEz[n1] = -ezp + akz * (rb + rbp + rp + fRho[n1]) / (d + ak2);
+            fJy[n1] = jyp + hxs * d * (fEy[n1] + eyp) / 2.;
+            fJz[n1] = jzp + hxs * d * (fEz[n1] + ezp) / 2.;
+            fJx[n1] = jxp + hxs * d * (fEx[n1] + exp_) / 2.;
+            fBx[n1] = -aky / ak2 * fJz[n1] + akz / ak2 * fJy[n1];
+            fBy[n1] = (-akz * (fJx[n1] + fJxBeam[n1]) + d * fEz[n1]) / ak2;
+            fBz[n1] = (aky * (fJx[n1] + fJxBeam[n1]) - d * fEy[n1]) / ak2;
+        }
+}
+
+// Per-mode corrector of IterateFieldsHydroLinLayerSplit
+// (movefieldshydrolinlayersplit.cpp:1374-1477; the same formulas as the
+// reference's CUDA twin linearizedIteratekernel, CUDA_WRAP/linearized.cu:105-209).
+// fRho holds rho_old on entry and the new rho on exit.
+extern "C" void qso_corrector_modes(int ny, int nz, double hx, double d, double Ylength,
+                                    double Zlength, const double* fRhoP, const double* fJxP,
+                                    const double* fJyP, const double* fJzP, const double* fEyP,
+                                    const double* fEzP, const double* fRhoBeam,
+                                    const double* fRhoBeamP, const double* fJxBeam,
+                                    const double* fJx, const double* fJy, const double* fJz,
+                                    double* fRho, double* fEx, double* fEy, double* fEz,
+                                    double* fBx, double* fBy, double* fBz) {
+    const double hxs = hx;
+    for (int k = 0; k < nz; k++)
+        for (int j = 0; j < ny; j++) {
+            double akz = M_PI / Zlength * (k + 0.5);
+            double aky = M_PI / Ylength * (j + 0.5);
+            double ak2 = aky * aky + akz * akz;
+            size_t n1 = (size_t)j + (size_t)ny * k;
+            double rp = fRhoP[n1];
+            double jy = fJy[n1];
+            double jz = fJz[n1];
+            double rho = rp + fJx[n1] - fJxP[n1] -
+                         hxs * (aky * (jy + fJyP[n1]) + akz * (jz + fJzP[n1])) / 2.;
+            double rb = fRhoBeam[n1];
+            double rbp = fRhoBeamP[n1];
+            double eyp = fEyP[n1];
+            double ezp = fEzP[n1];
+            double newEx = -(aky * jy + akz * jz) / ak2;
+            double newEy = -eyp + aky * (rb + rbp + rp + fRho[n1]) / (d + ak2);
+            double newEz = -ezp + akz * (rb + rbp + rp + fRho[n1]) / (d + ak2);
+            fEy[n1] = newEy;
+            fEz[n1] = newEz;
+            fRho[n1] = rho;
+            fEx[n1] = newEx;
+            fBx[n1] = -aky / ak2 * fJz[n1] + akz / ak2 * fJy[n1];
+            fBy[n1] = (-akz * (fJx[n1] + fJxBeam[n1]) + d * newEz) / ak2;
+            fBz[n1] = (aky * (fJx[n1] + fJxBeam[n1]) - d * newEy) / ak2;
+        }
+}
+
 struct Oracle {
     qs_config cfg;
     int My = 0, Mz = 0, L = 0, NxSplit = 1, nIter = 1;
@@ -628,42 +714,14 @@ struct Oracle {
         fwd(rJx, fJx, QS_REDFT11, QS_REDFT11);
         fwd(rJy, fJy, QS_REDFT11, QS_RODFT11);
         fwd(rJz, fJz, QS_RODFT11, QS_REDFT11);
-        // :808-900 linear predictor per mode
-        const double hxs = hx;
-        for (int k = 0; k < nz; k++)
-            for (int j = 0; j < ny; j++) {
-                double akz = M_PI / Zlength * (k + 0.5);
-                double aky = M_PI / Ylength * (j + 0.5);
-                double ak2 = aky * aky + akz * akz;
-                size_t n1 = (size_t)j + (size_t)ny * k;
-                if (ak2 == 0.) {
-                    fEx[n1] = fEy[n1] = fEz[n1] = fJx[n1] = fJy[n1] = fJz[n1] = fRho[n1] = 0.;
-                    continue;
-                }
-                double rp = fRhoP[n1] = fRho[n1];
-                double jxp = fJxP[n1] = fJx[n1];
-                double jyp = fJyP[n1] = fJy[n1];
-                double jzp = fJzP[n1] = fJz[n1];
-                double exp_ = fExP[n1] = fEx[n1];
-                double eyp = fEyP[n1] = fEy[n1];
-                double ezp = fEzP[n1] = fEz[n1];
-                double rb = fRhoBeam[n1];
-                double rbp = fRhoBeamP[n1];
-                double propagator = (4. - d * hxs * hxs) / (4. + d * hxs * hxs);
-                double denominator = 4. + d * hxs * hxs;
-                fRho[n1] = propagator * rp - (rb + rbp) * d * hxs * hxs / denominator +
-                           4. * exp_ * hxs * (ak2 + d) / denominator;
-                fEx[n1] = propagator * exp_ -
-                          2. * (2. * rp + rb + rbp) * d * hxs / ((ak2 + d) * denominator);
-                fEy[n1] = -eyp + aky * (rb + rbp + rp + fRho[n1]) / (d + ak2);
-                fEz[n1] = -ezp + akz * (rb + rbp + rp + fRho[n1]) / (d + ak2);
-                fJy[n1] = jyp + hxs * d * (fEy[n1] + eyp) / 2.;
-                fJz[n1] = jzp + hxs * d * (fEz[n1] + ezp) / 2.;
-                fJx[n1] = jxp + hxs * d * (fEx[n1] + exp_) / 2.;
-                fBx[n1] = -aky / ak2 * fJz[n1] + akz / ak2 * fJy[n1];
-                fBy[n1] = (-akz * (fJx[n1] + fJxBeam[n1]) + d * fEz[n1]) / ak2;
-                fBz[n1] = (aky * (fJx[n1] + fJxBeam[n1]) - d * fEy[n1]) / ak2;
-            }
+        // :808-900 linear predictor per mode (P spectra taken from the C arrays)
+        fRhoP = fRho; fJxP = fJx; fJyP = fJy; fJzP = fJz;
+        fExP = fEx; fEyP = fEy; fEzP = fEz;
+        qso_predictor_modes(ny, nz, hx, d, Ylength, Zlength, fRhoP.data(), fJxP.data(),
+                            fJyP.data(), fJzP.data(), fExP.data(), fEyP.data(), fEzP.data(),
+                            fRhoBeam.data(), fRhoBeamP.data(), fJxBeam.data(), fRho.data(),
+                            fEx.data(), fEy.data(), fEz.data(), fJx.data(), fJy.data(),
+                            fJz.data(), fBx.data(), fBy.data(), fBz.data());
         // :946-967 inverse transforms
         fwd(fRho, rRho, QS_REDFT11, QS_REDFT11);
         fwd(fEx, rEx, QS_REDFT11, QS_REDFT11);
@@ -713,37 +771,11 @@ struct Oracle {
         fwd(rJy, fJy, QS_REDFT11, QS_RODFT11);
         fwd(rJz, fJz, QS_RODFT11, QS_REDFT11);
         // :1374-1477 corrector per mode
-        const double hxs = hx;
-        for (int k = 0; k < nz; k++)
-            for (int j = 0; j < ny; j++) {
-                double akz = M_PI / Zlength * (k + 0.5);
-                double aky = M_PI / Ylength * (j + 0.5);
-                double ak2 = aky * aky + akz * akz;
-                size_t n1 = (size_t)j + (size_t)ny * k;
-                if (ak2 == 0.) {
-                    fEx[n1] = fEy[n1] = fEz[n1] = fJx[n1] = fJy[n1] = fJz[n1] = fRho[n1] = 0.;
-                    continue;
-                }
-                double rp = fRhoP[n1];
-                double jy = fJy[n1];
-                double jz = fJz[n1];
-                double rho = rp + fJx[n1] - fJxP[n1] -
-                             hxs * (aky * (jy + fJyP[n1]) + akz * (jz + fJzP[n1])) / 2.;
-                double rb = fRhoBeam[n1];
-                double rbp = fRhoBeamP[n1];
-                double eyp = fEyP[n1];
-                double ezp = fEzP[n1];
-                double newEx = -(aky * jy + akz * jz) / ak2;
-                double newEy = -eyp + aky * (rb + rbp + rp + fRho[n1]) / (d + ak2);
-                double newEz = -ezp + akz * (rb + rbp + rp + fRho[n1]) / (d + ak2);
-                fEy[n1] = newEy;
-                fEz[n1] = newEz;
-                fRho[n1] = rho;
-                fEx[n1] = newEx;
-                fBx[n1] = -aky / ak2 * fJz[n1] + akz / ak2 * fJy[n1];
-                fBy[n1] = (-akz * (fJx[n1] + fJxBeam[n1]) + d * newEz) / ak2;
-                fBz[n1] = (aky * (fJx[n1] + fJxBeam[n1]) - d * newEy) / ak2;
-            }
+        qso_corrector_modes(ny, nz, hx, d, Ylength, Zlength, fRhoP.data(), fJxP.data(),
+                            fJyP.data(), fJzP.data(), fEyP.data(), fEzP.data(),
+                            fRhoBeam.data(), fRhoBeamP.data(), fJxBeam.data(), fJx.data(),
+                            fJy.data(), fJz.data(), fRho.data(), fEx.data(), fEy.data(),
+                            fEz.data(), fBx.data(), fBy.data(), fBz.data());
         // :1517-1533
         fwd(fRho, rRho, QS_REDFT11, QS_REDFT11);
         fwd(fEx, rEx, QS_REDFT11, QS_REDFT11);

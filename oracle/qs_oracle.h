@@ -31,6 +31,23 @@ extern "C" {
 
 typedef struct qso qso;
 
+/* Per-mode spectral maps (FP64), in the argument convention of the
+ * reference's CUDA twins linearized_kernel / linearizedIteratekernel. */
+void qso_predictor_modes(int ny, int nz, double hx, double d, double Ylength,
+                         double Zlength, const double* fRhoP, const double* fJxP,
+                         const double* fJyP, const double* fJzP, const double* fExP,
+                         const double* fEyP, const double* fEzP, const double* fRhoBeam,
+                         const double* fRhoBeamP, const double* fJxBeam, double* fRho,
+                         double* fEx, double* fEy, double* fEz, double* fJx, double* fJy,
+                         double* fJz, double* fBx, double* fBy, double* fBz);
+void qso_corrector_modes(int ny, int nz, double hx, double d, double Ylength,
+                         double Zlength, const double* fRhoP, const double* fJxP,
+                         const double* fJyP, const double* fJzP, const double* fEyP,
+                         const double* fEzP, const double* fRhoBeam, const double* fRhoBeamP,
+                         const double* fJxBeam, const double* fJx, const double* fJy,
+                         const double* fJz, double* fRho, double* fEx, double* fEy,
+                         double* fEz, double* fBx, double* fBy, double* fBz);
+
 void qso_set_threads(int n);
 int qso_get_threads(void);
 
