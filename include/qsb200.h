@@ -254,6 +254,30 @@ qs_status qs_transform2d_dev(qs_handle* h, int kind_z, int kind_y, int batch,
 qs_status qs_transform2d_noalloc(int kind_z, int kind_y, int ny, int nz, int batch,
                                  const double* d_in, double* d_out, void* stream);
 
+/* ------------------------------------------------------------ the adjoint
+ *
+ * Reverse-mode gradient of a loss on the on-axis longitudinal field with
+ * respect to the driver-beam macro-particle weights (no counterpart in the
+ * reference, which has no adjoint; the forward it differentiates is
+ * Mesh::MoveAllSplitLayers, movepart_splitlayer.cpp:25-558, with the beam
+ * currents deposited by the last beam push, movebeam.cpp:662-774).
+ *
+ * qs_adjoint_checkpoints(h, K): from the next march on, store the plasma
+ * particles and the P-bank spectra every K layers (K = 0 turns it off and
+ * frees the storage).  Call it after the front plasma is loaded or seeded.
+ * Supported for the NGP shape and NxSplit = 1. */
+qs_status qs_adjoint_checkpoints(qs_handle* h, int every);
+/* Given dloss_donaxis_ex[nx] = d loss / d (on-axis Ex of layer i) for the last
+ * march (which must have stored checkpoints, with no beam change since),
+ * recompute each K-layer segment from its checkpoint and sweep it in reverse;
+ * writes dloss_dbeam_weight[n_beam] = d loss / d w_p for every beam particle
+ * at its post-push position (particles outside the box get 0).  The sweep
+ * starts at the lowest layer with a nonzero dloss entry.  It reuses the
+ * march's working state: afterwards the plasma arrays are undefined and the
+ * field store may differ from the march's in the last bits (atomic order). */
+qs_status qs_adjoint(qs_handle* h, const double* dloss_donaxis_ex,
+                     double* dloss_dbeam_weight);
+
 /* One step through host buffers (the e2e entry point): copies the beam in
  * from host, seeds the front plasma, runs qs_step, copies the beam and the
  * on-axis Ex back.  Any out pointer may be NULL to skip that copy. */

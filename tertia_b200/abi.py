@@ -176,6 +176,8 @@ def _declare(L):
     L.qs_transform2d_noalloc.argtypes = [C.c_int] * 5 + [P, P, P]
     L.qs_step_host.argtypes = ([P, C.c_int64] + [i32p] * 3 + [f64p] * 7 + [i32p] * 3 +
                                [f64p] * 6 + [f64p])
+    L.qs_adjoint_checkpoints.argtypes = [P, C.c_int]
+    L.qs_adjoint.argtypes = [P, f64p, f64p]
     L.qs_kernel_launches.argtypes = [P]
     L.qs_kernel_launches.restype = C.c_int64
     L.qs_profile_enable.argtypes = [P, C.c_int]
@@ -192,7 +194,7 @@ EXPORTED_SYMBOLS = [
     "qs_move_beam_particles", "qs_move_all_split_layers", "qs_begin_march", "qs_layer_begin",
     "qs_move_split_layer", "qs_guess_fields", "qs_move_particles_layer", "qs_iterate_fields",
     "qs_layer_end", "qs_transform2d", "qs_transform2d_dev", "qs_transform2d_noalloc",
-    "qs_step_host",
+    "qs_adjoint_checkpoints", "qs_adjoint", "qs_step_host",
     "qs_kernel_launches", "qs_profile_enable", "qs_profile_read",
 ]
 

@@ -1,0 +1,443 @@
+// adjoint.cu — reverse-mode (adjoint) kernels of the xi-march.
+//
+// The march maps the driver-beam currents (RhoBeam, JxBeam of every layer)
+// to the fields of every layer through, per layer, a linear spectral
+// predictor, inverse transforms, the plasma push with its current deposit,
+// forward transforms of the currents and the linear spectral corrector
+// (Mesh::MoveSplitLayer, movepart_splitlayer.cpp:561-778).  These kernels are
+// the transposes of those steps; the transforms are their own transposes
+// (the REDFT11 / RODFT11 matrices are symmetric), so the adjoint of a
+// transform is the same transform and the adjoint of the inverse is the
+// transform times 1/(4 ny nz).
+//
+// NGP plasma push (the reference's live shape): a particle keeps its seeded
+// cell, the field gather is at that cell and the deposit cells come from
+// floor() of the sub-cycled position, so positions carry no derivative; the
+// adjoint state of a particle is the adjoint of its momentum.  The push
+// adjoint recomputes the particle's forward update from the stored
+// layer-entry state and back-propagates through it by hand.
+#include <cmath>
+
+#include "qs_common.cuh"
+#include "qs_internal.h"
+
+namespace qs {
+
+namespace {
+
+template <class T>
+__device__ __forceinline__ T ldg_(const T* p) { return __ldg(p); }
+
+__device__ __forceinline__ int wrap_m(int j, int M) {
+    while (j >= M) j -= M;
+    while (j < 0) j += M;
+    return j;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// push adjoint: one thread per particle
+template <class T>
+__global__ void __launch_bounds__(256) push_adjoint_kernel(PushAdjArgs<T> a) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.n) return;
+    const int My = a.My, Mz = a.Mz;
+    const int cell = a.cell[i];
+    const int j = cell % My, k = cell / My;
+    const T one = T(1), half = T(0.5);
+    const T yp = a.y[i], zp = a.z[i];
+    if (!(yp >= T(0) && yp <= one && zp >= T(0) && zp <= one)) return;   // forward skipped it
+    const T px0 = a.px[i], py0 = a.py[i], pz0 = a.pz[i];
+    const T w = a.w[i];
+    const size_t plane = a.plane, n = (size_t)cell;
+    T E[3], B[3];
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+        E[c] = half * (ldg_(a.P + c * plane + n) + ldg_(a.C + c * plane + n));
+        B[c] = half * (ldg_(a.P + (3 + c) * plane + n) + ldg_(a.C + (3 + c) * plane + n));
+    }
+    B[0] += a.bxe; B[1] += a.bye; B[2] += a.bze;
+
+    // ---- forward recompute (the factored form of the push)
+    const T p[3] = {px0, py0, pz0};
+    const T s0 = one + p[0] * p[0] + p[1] * p[1] + p[2] * p[2];
+    const T r0 = one / sqrt(s0);
+    const T Vp[3] = {p[0] * r0, p[1] * r0, p[2] * r0};
+    const T av = one - Vp[0];
+    const T ia = one / av;
+    const T kE = a.sE * ia;
+    const T e[3] = {E[0] * kE, E[1] * kE, E[2] * kE};
+    const T p1[3] = {p[0] + e[0], p[1] + e[1], p[2] + e[2]};
+    const T s1 = one + p1[0] * p1[0] + p1[1] * p1[1] + p1[2] * p1[2];
+    const T r1 = one / sqrt(s1);
+    const T kB = r1 * kE;
+    const T b[3] = {B[0] * kB, B[1] * kB, B[2] * kB};
+    const T q = one + b[0] * b[0] + b[1] * b[1] + b[2] * b[2];
+    const T co = T(2) / q;
+    const T u[3] = {p1[0] + (p1[1] * b[2] - p1[2] * b[1]), p1[1] + (p1[2] * b[0] - p1[0] * b[2]),
+                    p1[2] + (p1[0] * b[1] - p1[1] * b[0])};
+    const T p3[3] = {u[0] * co, u[1] * co, u[2] * co};
+    const T p2[3] = {p1[0] + e[0] + (p3[1] * b[2] - p3[2] * b[1]),
+                     p1[1] + e[1] + (p3[2] * b[0] - p3[0] * b[2]),
+                     p1[2] + e[2] + (p3[0] * b[1] - p3[1] * b[0])};
+    const T s2 = one + p2[0] * p2[0] + p2[1] * p2[1] + p2[2] * p2[2];
+    const T r2 = one / sqrt(s2);
+    const T Vm[3] = {p2[0] * r2, p2[1] * r2, p2[2] * r2};
+    const T V[3] = {half * (Vm[0] + Vp[0]), half * (Vm[1] + Vp[1]), half * (Vm[2] + Vp[2])};
+    const T cv = one - V[0];
+    const T inv2 = one / cv;
+    const T wq = w * inv2;
+    const T dJ0[3] = {a.djx0, a.djy0, a.djz0};
+    const T dy = V[1] * a.hxhy * inv2, dz = V[2] * a.hxhz * inv2;
+
+    // ---- G = sum over sub-steps of part_step * lambda_J(deposit cell)
+    T G[3] = {T(0), T(0), T(0)};
+    {
+        T partdx = T(0), step = one;
+        const T ady = dy < T(0) ? -dy : dy, adz = dz < T(0) ? -dz : dz;
+        if (ady > one || adz > one) step = partdx = (ady > adz ? ady : adz);
+        if (partdx < one) partdx = step = one;
+        T ytmp = yp, ztmp = zp;
+        const T MyT = T(My), MzT = T(Mz);
+        int jj = j, kk = k;
+        while (partdx > T(0)) {
+            T ps;
+            if (partdx > one) { partdx -= one; ps = one / step; }
+            else { ps = partdx / step; partdx = T(0); }
+            if (a.precise) {
+                const T uy = ytmp + dy * ps, uz = ztmp + dz * ps;
+                const T fy = floor(uy), fz = floor(uz);
+                T ry = uy - fy, rz = uz - fz;
+                int sy = (int)fy, sz = (int)fz;
+                if (ry >= one) { ry = T(0); sy += 1; }
+                if (rz >= one) { rz = T(0); sz += 1; }
+                jj = wrap_m(j + sy, My);
+                kk = wrap_m(k + sz, Mz);
+                ytmp = ry;
+                ztmp = rz;
+            } else {
+                ytmp += dy * ps + T(j);
+                ztmp += dz * ps + T(k);
+                while (ytmp > MyT) ytmp -= MyT;
+                while (ytmp < T(0)) ytmp += MyT;
+                while (ztmp > MzT) ztmp -= MzT;
+                while (ztmp < T(0)) ztmp += MzT;
+                jj = (int)ytmp;
+                kk = (int)ztmp;
+                ytmp -= T(jj);
+                ztmp -= T(kk);
+            }
+            const size_t m = (size_t)wrap_m(jj, My) + (size_t)My * wrap_m(kk, Mz);
+#pragma unroll
+            for (int c = 0; c < 3; c++) G[c] += ps * ldg_(a.lamD + c * plane + m);
+        }
+    }
+
+    // ---- backward
+    T bp2[3] = {T(0), T(0), T(0)};
+    if (a.full) {
+        bp2[0] = a.lamPm[i];
+        bp2[1] = a.lamPm[a.n + i];
+        bp2[2] = a.lamPm[2 * a.n + i];
+    }
+    // dj_c = wq dJ0_c Vm_c
+    T bVm[3], bwq = T(0);
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+        bVm[c] = wq * dJ0[c] * G[c];
+        bwq += G[c] * dJ0[c] * Vm[c];
+    }
+    const T binv2 = w * bwq;
+    const T bcv = -inv2 * inv2 * binv2;
+    const T bVx = -bcv;                    // cv = 1 - Vx
+    bVm[0] += half * bVx;
+    T bVp[3] = {half * bVx, T(0), T(0)};
+    // Vm = p2 r2
+    {
+        const T br2 = bVm[0] * p2[0] + bVm[1] * p2[1] + bVm[2] * p2[2];
+        const T f = -r2 * r2 * r2 * br2;
+#pragma unroll
+        for (int c = 0; c < 3; c++) bp2[c] += r2 * bVm[c] + f * p2[c];
+    }
+    // p2 = p1 + e + p3 x b
+    T bp1[3] = {bp2[0], bp2[1], bp2[2]};
+    T be[3] = {bp2[0], bp2[1], bp2[2]};
+    const T bp3[3] = {b[1] * bp2[2] - b[2] * bp2[1], b[2] * bp2[0] - b[0] * bp2[2],
+                      b[0] * bp2[1] - b[1] * bp2[0]};
+    T bb[3] = {bp2[1] * p3[2] - bp2[2] * p3[1], bp2[2] * p3[0] - bp2[0] * p3[2],
+               bp2[0] * p3[1] - bp2[1] * p3[0]};
+    // p3 = co u
+    const T bco = bp3[0] * u[0] + bp3[1] * u[1] + bp3[2] * u[2];
+    const T bu[3] = {co * bp3[0], co * bp3[1], co * bp3[2]};
+    // u = p1 + p1 x b
+    bp1[0] += bu[0] + (b[1] * bu[2] - b[2] * bu[1]);
+    bp1[1] += bu[1] + (b[2] * bu[0] - b[0] * bu[2]);
+    bp1[2] += bu[2] + (b[0] * bu[1] - b[1] * bu[0]);
+    bb[0] += bu[1] * p1[2] - bu[2] * p1[1];
+    bb[1] += bu[2] * p1[0] - bu[0] * p1[2];
+    bb[2] += bu[0] * p1[1] - bu[1] * p1[0];
+    // co = 2 / q, q = 1 + b.b
+    const T bq = -co * co * T(0.5) * bco;
+#pragma unroll
+    for (int c = 0; c < 3; c++) bb[c] += T(2) * b[c] * bq;
+    // b = B kB
+    T bB[3];
+    T bkB = T(0);
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+        bB[c] = kB * bb[c];
+        bkB += B[c] * bb[c];
+    }
+    // kB = r1 kE
+    const T br1 = kE * bkB;
+    T bkE = r1 * bkB;
+    {
+        const T f = -r1 * r1 * r1 * br1;
+#pragma unroll
+        for (int c = 0; c < 3; c++) bp1[c] += f * p1[c];
+    }
+    // p1 = p + e
+    T bp[3];
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+        bp[c] = bp1[c];
+        be[c] += bp1[c];
+    }
+    // e = E kE
+    T bE[3];
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+        bE[c] = kE * be[c];
+        bkE += E[c] * be[c];
+    }
+    // kE = sE / (1 - Vp_x)
+    const T bia = a.sE * bkE;
+    const T bav = -ia * ia * bia;
+    bVp[0] += -bav;
+    // Vp = p r0
+    {
+        const T br0 = bVp[0] * p[0] + bVp[1] * p[1] + bVp[2] * p[2];
+        const T f = -r0 * r0 * r0 * br0;
+#pragma unroll
+        for (int c = 0; c < 3; c++) bp[c] += r0 * bVp[c] + f * p[c];
+    }
+    // momenta adjoint: the full push sets it, the half pushes add to it
+    if (a.full) {
+        a.lamPm[i] = bp[0];
+        a.lamPm[a.n + i] = bp[1];
+        a.lamPm[2 * a.n + i] = bp[2];
+    } else {
+        a.lamPm[i] += bp[0];
+        a.lamPm[a.n + i] += bp[1];
+        a.lamPm[2 * a.n + i] += bp[2];
+    }
+    // fields: E = (P + C)/2 and B = (P + C)/2 + external
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+        atomicAdd(a.lamFP + c * plane + n, half * bE[c]);
+        atomicAdd(a.lamFC + c * plane + n, half * bE[c]);
+        atomicAdd(a.lamFP + (3 + c) * plane + n, half * bB[c]);
+        atomicAdd(a.lamFC + (3 + c) * plane + n, half * bB[c]);
+    }
+}
+
+template <class T>
+int launch_push_adjoint(const PushAdjArgs<T>& a, cudaStream_t st) {
+    if (a.n <= 0) return 0;
+    push_adjoint_kernel<T><<<(unsigned)((a.n + 255) / 256), 256, 0, st>>>(a);
+    return 1;
+}
+
+// ---------------------------------------------------------------------------
+// per-mode adjoints of the spectral maps
+
+template <class T>
+__device__ __forceinline__ void beam_adj(const AdjSpecArgs<T>& a, size_t n, T lrb, T lrbp,
+                                         T ljxb) {
+    if (a.wb0 != T(0)) {
+        a.lRb0[n] += a.wb0 * lrb;
+        a.lJxb0[n] += a.wb0 * ljxb;
+    }
+    if (a.wb1 != T(0)) {
+        a.lRb1[n] += a.wb1 * lrb;
+        a.lJxb1[n] += a.wb1 * ljxb;
+    }
+    if (a.wp0 != T(0)) a.lRbp0[n] += a.wp0 * lrbp;
+    if (a.wp1 != T(0)) a.lRbp1[n] += a.wp1 * lrbp;
+}
+
+template <class T>
+__device__ __forceinline__ T opt(const T* p, size_t n) { return p ? p[n] : T(0); }
+
+template <class T>
+__device__ __forceinline__ void put_lp(const AdjSpecArgs<T>& a, int f, size_t n, T v) {
+    if (a.lP_set) a.lP[f][n] = v;
+    else a.lP[f][n] += v;
+}
+
+// Transpose of corrector_kernel (IterateFieldsHydroLinLayerSplit's per-mode
+// update, movefieldshydrolinlayersplit.cpp:1419-1466).
+template <class T>
+__global__ void corrector_adjoint_kernel(AdjSpecArgs<T> a) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    const int k = blockIdx.y;
+    if (j >= a.ny) return;
+    const size_t n = (size_t)j + (size_t)a.ny * k;
+    const T d = a.dens, hx = a.hx;
+    const T akz = a.piZ * (T(k) + T(0.5));
+    const T aky = a.piY * (T(j) + T(0.5));
+    const T k2 = aky * aky + akz * akz;
+    const T lrho = opt(a.lRho, n);
+    const T lex = opt(a.lE[0], n) + opt(a.lEb[0], n);
+    T ley = opt(a.lE[1], n) + opt(a.lEb[1], n);
+    T lez = opt(a.lE[2], n) + opt(a.lEb[2], n);
+    const T lbx = opt(a.lB[0], n), lby = opt(a.lB[1], n), lbz = opt(a.lB[2], n);
+    // by = (-akz (jx + jxb) + d ez)/k2, bz = (aky (jx + jxb) - d ey)/k2
+    lez += d * lby / k2;
+    ley -= d * lbz / k2;
+    const T ljxs = (-akz * lby + aky * lbz) / k2;          // d(by,bz)/d(jx + jxb)
+    T ljx = lrho + ljxs + opt(a.lJb[0], n);
+    T ljy = -hx * T(0.5) * aky * lrho - aky / k2 * lex + akz / k2 * lbx + opt(a.lJb[1], n);
+    T ljz = -hx * T(0.5) * akz * lrho - akz / k2 * lex - aky / k2 * lbx + opt(a.lJb[2], n);
+    const T lsrc = (aky * ley + akz * lez) / (d + k2);     // src = rb + rbp + rp + rho_old
+    a.lJ[0][n] = ljx;
+    a.lJ[1][n] = ljy;
+    a.lJ[2][n] = ljz;
+    a.lRhoOld[n] = lsrc;
+    // P-bank inputs: 0 RhoP, 1 ExP, 2 EyP, 3 EzP, 4 JxP, 5 JyP, 6 JzP
+    put_lp(a, 0, n, lrho + lsrc);
+    if (a.lP_set) a.lP[1][n] = T(0);
+    put_lp(a, 2, n, -ley);
+    put_lp(a, 3, n, -lez);
+    put_lp(a, 4, n, -lrho);
+    put_lp(a, 5, n, -hx * T(0.5) * aky * lrho);
+    put_lp(a, 6, n, -hx * T(0.5) * akz * lrho);
+    beam_adj(a, n, lsrc, lsrc, ljxs);
+}
+
+// Transpose of predictor_kernel (GuessFieldsHydroLinLayerSplit's per-mode
+// update, movefieldshydrolinlayersplit.cpp:843-872).
+template <class T>
+__global__ void predictor_adjoint_kernel(AdjSpecArgs<T> a) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    const int k = blockIdx.y;
+    if (j >= a.ny) return;
+    const size_t n = (size_t)j + (size_t)a.ny * k;
+    const T d = a.dens, hx = a.hx;
+    const T akz = a.piZ * (T(k) + T(0.5));
+    const T aky = a.piY * (T(j) + T(0.5));
+    const T k2 = aky * aky + akz * akz;
+    const T den = T(4) + d * hx * hx;
+    const T prop = (T(4) - d * hx * hx) / den;
+    const T lrho = opt(a.lRho, n);
+    T lex = opt(a.lE[0], n), ley = opt(a.lE[1], n), lez = opt(a.lE[2], n);
+    const T lbx = opt(a.lB[0], n), lby = opt(a.lB[1], n), lbz = opt(a.lB[2], n);
+    // b from the predicted currents and fields
+    const T ljx = (-akz * lby + aky * lbz) / k2;   // also the jxb adjoint
+    const T ljy = akz * lbx / k2;
+    const T ljz = -aky * lbx / k2;
+    lez += d * lby / k2;
+    ley -= d * lbz / k2;
+    // jx = jxp + hx d (ex + exp)/2 (and y, z)
+    const T hd2 = hx * d * T(0.5);
+    lex += hd2 * ljx;
+    ley += hd2 * ljy;
+    lez += hd2 * ljz;
+    T lexp = hd2 * ljx, leyp = hd2 * ljy, lezp = hd2 * ljz;
+    // ey = -eyp + aky src/(d + k2), src = rb + rbp + rp + rho
+    const T lsrc = (aky * ley + akz * lez) / (d + k2);
+    leyp -= ley;
+    lezp -= lez;
+    const T lrho_t = lrho + lsrc;
+    // rho = prop rp - (rb + rbp) d hx^2/den + 4 exp hx (k2 + d)/den
+    // ex  = prop exp - 2 (2 rp + rb + rbp) d hx / ((k2 + d) den)
+    const T cex = T(2) * d * hx / ((k2 + d) * den);
+    const T lrp = lsrc + prop * lrho_t - T(2) * cex * lex;
+    const T lrb = lsrc - d * hx * hx / den * lrho_t - cex * lex;
+    lexp += T(4) * hx * (k2 + d) / den * lrho_t + prop * lex;
+    put_lp(a, 0, n, lrp);
+    put_lp(a, 1, n, lexp);
+    put_lp(a, 2, n, leyp);
+    put_lp(a, 3, n, lezp);
+    put_lp(a, 4, n, ljx);
+    put_lp(a, 5, n, ljy);
+    put_lp(a, 6, n, ljz);
+    beam_adj(a, n, lrb, lrb, ljx);
+}
+
+template <class T>
+int launch_corrector_adjoint(const AdjSpecArgs<T>& a, cudaStream_t st) {
+    const dim3 g((unsigned)((a.ny + 127) / 128), (unsigned)a.nz);
+    corrector_adjoint_kernel<T><<<g, 128, 0, st>>>(a);
+    return 1;
+}
+
+template <class T>
+int launch_predictor_adjoint(const AdjSpecArgs<T>& a, cudaStream_t st) {
+    const dim3 g((unsigned)((a.ny + 127) / 128), (unsigned)a.nz);
+    predictor_adjoint_kernel<T><<<g, 128, 0, st>>>(a);
+    return 1;
+}
+
+// ---------------------------------------------------------------------------
+// out[idx] += v[layer] for the on-axis loss gradient of one layer
+template <class T>
+__global__ void add_point_kernel(T* plane_ex, size_t idx, const T* v, int layer) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) plane_ex[idx] += v[layer];
+}
+
+template <class T>
+int launch_add_point(T* plane_ex, size_t idx, const T* v, int layer, cudaStream_t st) {
+    add_point_kernel<T><<<1, 32, 0, st>>>(plane_ex, idx, v, layer);
+    return 1;
+}
+
+// ---------------------------------------------------------------------------
+// d loss / d w_p of every beam particle: the transpose of the 3-D CIC deposit
+// of the last beam push (movebeam.cpp:662-774): drho = w polarity,
+// djx = w polarity Vx at the 8 corners of the particle's post-push cell.
+template <class T>
+__global__ void __launch_bounds__(256) beam_weight_grad_kernel(BeamGradArgs<T> a) {
+    const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= a.n) return;
+    const int L = a.L, My = a.My, Mz = a.Mz;
+    const int i = a.bi[p], j = a.bj[p], k = a.bk[p];
+    double g = 0.0;
+    if (i >= 0 && i < L && j >= 0 && j < My && k >= 0 && k < Mz) {
+        const double px = a.px[p], py = a.py[p], pz = a.pz[p];
+        const double Vx = px / sqrt(1. + px * px + py * py + pz * pz);
+        const double ax1 = a.x[p], ax0 = 1. - ax1, ay1 = a.y[p], ay0 = 1. - ay1, az1 = a.z[p],
+                     az0 = 1. - az1;
+        const size_t plane = a.plane;
+        for (int di = 0; di < 2; di++)
+            for (int dj = 0; dj < 2; dj++)
+                for (int dk = 0; dk < 2; dk++) {
+                    const int ii = i + di, jj = j + dj, kk = k + dk;
+                    if (ii > L || jj >= My || kk >= Mz) continue;
+                    const double wc = (di ? ax1 : ax0) * (dj ? ay1 : ay0) * (dk ? az1 : az0);
+                    const size_t m = (size_t)jj + (size_t)My * kk;
+                    g += wc * ((double)a.lb3[((size_t)ii * 2 + 0) * plane + m] +
+                               Vx * (double)a.lb3[((size_t)ii * 2 + 1) * plane + m]);
+                }
+    }
+    a.out[p] = g * a.polarity;
+}
+
+template <class T>
+int launch_beam_weight_grad(const BeamGradArgs<T>& a, cudaStream_t st) {
+    if (a.n <= 0) return 0;
+    beam_weight_grad_kernel<T><<<(unsigned)((a.n + 255) / 256), 256, 0, st>>>(a);
+    return 1;
+}
+
+#define QS_ADJ_INST(T)                                                                   \
+    template int launch_push_adjoint<T>(const PushAdjArgs<T>&, cudaStream_t);            \
+    template int launch_corrector_adjoint<T>(const AdjSpecArgs<T>&, cudaStream_t);       \
+    template int launch_predictor_adjoint<T>(const AdjSpecArgs<T>&, cudaStream_t);       \
+    template int launch_add_point<T>(T*, size_t, const T*, int, cudaStream_t);           \
+    template int launch_beam_weight_grad<T>(const BeamGradArgs<T>&, cudaStream_t);
+QS_ADJ_INST(float)
+QS_ADJ_INST(double)
+
+}  // namespace qs

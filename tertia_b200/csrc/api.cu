@@ -17,6 +17,7 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <new>
 #include <string>
@@ -29,6 +30,7 @@
 namespace qs {
 
 static thread_local std::string g_create_error;
+thread_local bool g_pdl = false;
 
 // error text of calls made without a handle (read by qs_last_error(NULL))
 void set_unbound_error(const std::string& why) { g_create_error = why; }
@@ -144,6 +146,8 @@ struct EngineBase {
     virtual qs_status layer_end(int, int) = 0;
     virtual qs_status transform2d(int, int, int, const double*, double*) = 0;
     virtual qs_status transform2d_dev(int, int, int, const void*, void*) = 0;
+    virtual qs_status adjoint_checkpoints(int) = 0;
+    virtual qs_status adjoint(const double*, double*) = 0;
 
     qs_status check_device() {
         cudaError_t e = cudaStreamSynchronize(st);
@@ -209,6 +213,8 @@ struct Engine : EngineBase {
     int32_t* pcell = nullptr;
     T *py = nullptr, *pz = nullptr, *ppx = nullptr, *ppy = nullptr, *ppz = nullptr, *pw = nullptr;
     bool front_pending = false;
+    // programmatic dependent launch inside the march (QS_PDL=0 turns it off)
+    bool use_pdl = !(getenv("QS_PDL") && getenv("QS_PDL")[0] == '0');
     bool uniform_layout = false;   // particle p in cell p / ppc (lattice seeding)
     // beam
     int64_t nb = 0, nb_cap = 0;
@@ -220,6 +226,19 @@ struct Engine : EngineBase {
     int64_t graph_kernels = 0;
     struct HostState { T *Pf, *Cf, *Psrc, *Csrc; int cur; } graph_end{};
     bool marched = false;
+    // adjoint: layer checkpoints of the last march and the reverse sweep's buffers
+    int ck_every = 0;           // checkpoint every ck_every layers (0: off)
+    bool ck_valid = false;      // the last march stored checkpoints for the current beam
+    int ck_count = 0;
+    T* ck = nullptr;            // ck_count x (5 np + 7 planes)
+    T* seg = nullptr;           // ck_every x (5 np + (nIter+1) x 6 planes)
+    T* lam = nullptr;           // adjoint work planes (see adjoint())
+    T* lam_pm = nullptr;        // 3 x np momentum adjoint
+    T* lam_sb = nullptr;        // (nx+1) x 2 planes: adjoint of the beam spectra
+    T* lam_b3 = nullptr;        // (nx+1) x 2 planes: adjoint of the real beam currents
+    T* d_dloss = nullptr;       // nx: d loss / d on-axis Ex of each layer
+    double* d_gradw = nullptr;  // nb: d loss / d beam weight
+    int64_t adj_np = 0, adj_nb = 0;
 
     T* bankp(int b, int p) { return bank + ((size_t)b * SP_N + p) * plane; }
     T* f3layer(int i) { return f3 + (size_t)i * 6 * plane; }
@@ -229,7 +248,8 @@ struct Engine : EngineBase {
         delete tcx;
         void* ptrs[] = {f3, b3, src3, splitbuf, srcbuf, Cbeam, sb3, bank, scratch, mats, onaxis_d,
                         stage, stage_d, pcell, py, pz, ppx, ppy, ppz, pw, bi, bj, bk, bx, by, bz,
-                        bpx, bpy, bpz, bw, d_err};
+                        bpx, bpy, bpz, bw, d_err, ck, seg, lam, lam_pm, lam_sb, lam_b3,
+                        d_dloss, d_gradw};
         for (void* p : ptrs)
             if (p) cudaFree(p);
         if (st) cudaStreamDestroy(st);
@@ -593,6 +613,7 @@ struct Engine : EngineBase {
         T* p = beam_plane(field, layer);
         if (!p || !data) return fail(QS_ERR_INVALID, "qs_set_beam_currents: bad arguments");
         sb3_valid = false;
+        ck_valid = false;
         return put_plane(p, data);
     }
 
@@ -645,6 +666,7 @@ struct Engine : EngineBase {
 
     // ------------------------------------------------------------- beam push
     qs_status move_beam() override {
+        ck_valid = false;
         CK(cudaMemsetAsync(b3, 0, (size_t)(L + 1) * 2 * plane * sizeof(T), st));
         BeamArgs<T> a{};
         a.n = nb;
@@ -746,6 +768,7 @@ struct Engine : EngineBase {
     }
 
     qs_status begin_march() override {
+        ck_valid = false;   // a march driven piece by piece keeps no checkpoints
         if (!front_pending) {
             qs_status s = seed_front(step_count);
             if (s) return s;
@@ -806,7 +829,11 @@ struct Engine : EngineBase {
             xform(job_stack(stage, 7, outs, kz, ky, T(1)));
             p_valid = true;
         }
-        klaunch(KC_SPECTRAL, [&] { return launch_predictor<T>(spec_args(iLayer, iSplit), st); });
+        {
+            SpecArgs<T> a = spec_args(iLayer, iSplit);
+            a.zero_src = clear_by_maps() ? Csrc : nullptr;   // for the push that follows
+            klaunch(KC_SPECTRAL, [&] { return launch_predictor<T>(a, st); });
+        }
         // :946-967, :1004-1061: E, B into C (the predicted Rho and J planes are
         // cleared before any use by the push that follows)
         inverse_EB(false);
@@ -814,9 +841,15 @@ struct Engine : EngineBase {
         return QS_OK;
     }
 
+    // Inside the march (no source store) the deposit planes are cleared by
+    // the spectral kernel that precedes each push instead of by a memset.
+    bool clear_by_maps() const { return in_march && !src3; }
+
     qs_status push(int iLayer, int iSplit, int full) override {
         (void)iLayer; (void)iSplit;
-        CK(cudaMemsetAsync(Csrc, 0, 4 * plane * sizeof(T), st));   // ClearCurrentsSplit
+        // ClearCurrentsSplit: inside the march the preceding spectral kernel
+        // already cleared Csrc
+        if (!clear_by_maps()) CK(cudaMemsetAsync(Csrc, 0, 4 * plane * sizeof(T), st));
         PushArgs<T> a{};
         a.n = np;
         a.My = My; a.Mz = Mz;
@@ -865,6 +898,9 @@ struct Engine : EngineBase {
         const bool want_rho = iter < 0 && (!in_march || src3 != nullptr);
         SpecArgs<T> a = spec_args(iLayer, iSplit);
         a.split_rho = want_rho ? 1 : 0;
+        // a push follows every Iterate but the last: clear its deposit planes
+        // (the forward J transform above has consumed them)
+        a.zero_src = (clear_by_maps() && iter >= 0) ? Csrc : nullptr;
         klaunch(KC_SPECTRAL, [&] { return launch_corrector<T>(a, st); });
         inverse_EB(want_rho);
         CK(cudaGetLastError());
@@ -906,7 +942,9 @@ struct Engine : EngineBase {
 
     qs_status march_device() {
         in_march = true;
+        g_pdl = use_pdl && !prof;   // event pairs between kernels would break the chain
         qs_status s = march_device_body();
+        g_pdl = false;
         in_march = false;
         return s;
     }
@@ -916,6 +954,8 @@ struct Engine : EngineBase {
         if (s) return s;
         for (int i = L - 1; i >= 0; i--)
             for (int sp = 0; sp < S; sp++) {
+                if (ck_every > 0 && sp == 0 && (L - 1 - i) % ck_every == 0)
+                    if ((s = save_checkpoint((L - 1 - i) / ck_every))) return s;
                 if ((s = layer_begin(i, sp))) return s;
                 if ((s = move_split_layer(i, sp))) return s;
                 if ((s = layer_end(i, sp))) return s;
@@ -937,7 +977,11 @@ struct Engine : EngineBase {
             qs_status s = beam_spectra();
             if (s) return s;
         }
-        if (!cfg.use_graph || prof) return march_device();
+        if (!cfg.use_graph || prof) {
+            qs_status s = march_device();
+            ck_valid = !s && ck_every > 0;
+            return s;
+        }
         if (!gexec) {
             cudaGraph_t g = nullptr;
             CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
@@ -961,11 +1005,312 @@ struct Engine : EngineBase {
             graph_end = HostState{Pf, Cf, Psrc, Csrc, cur};
         }
         CK(cudaGraphLaunch(gexec, st));
+        ck_valid = ck_every > 0;
         launches += graph_kernels;
         Pf = graph_end.Pf; Cf = graph_end.Cf; Psrc = graph_end.Psrc; Csrc = graph_end.Csrc;
         cur = graph_end.cur;
         p_valid = true;
         marched = true;
+        return QS_OK;
+    }
+
+    // ------------------------------------------------------------ adjoint
+    // Checkpoint m holds the state entering layer L-1-m*K: the plasma
+    // particles (y, z, px, py, pz) and the P-bank spectra (Rho, Ex, Ey, Ez,
+    // Jx, Jy, Jz); the P-layer fields are layer L-m*K of the field store.
+    size_t ck_stride() const { return 5 * (size_t)adj_np + 7 * plane; }
+    size_t seg_stride() const { return 5 * (size_t)adj_np + (size_t)(nIter + 1) * 6 * plane; }
+    T* particle_arrays(int c) { T* a[5] = {py, pz, ppx, ppy, ppz}; return a[c]; }
+
+    qs_status save_checkpoint(int m) {
+        if (m >= ck_count || np != adj_np) return fail(QS_ERR_STATE, "checkpoint storage");
+        T* dst = ck + (size_t)m * ck_stride();
+        for (int c = 0; c < 5; c++)
+            CK(cudaMemcpyAsync(dst + (size_t)c * np, particle_arrays(c), np * sizeof(T),
+                               cudaMemcpyDeviceToDevice, st));
+        const int pb = cur ^ 1;
+        T* b = dst + 5 * (size_t)np;
+        CK(cudaMemcpyAsync(b, bankp(pb, SP_RHO), 4 * plane * sizeof(T), cudaMemcpyDeviceToDevice,
+                           st));
+        CK(cudaMemcpyAsync(b + 4 * plane, bankp(pb, SP_JX), 3 * plane * sizeof(T),
+                           cudaMemcpyDeviceToDevice, st));
+        return QS_OK;
+    }
+
+    qs_status restore_checkpoint(int m) {
+        const T* src = ck + (size_t)m * ck_stride();
+        for (int c = 0; c < 5; c++)
+            CK(cudaMemcpyAsync(particle_arrays(c), src + (size_t)c * np, np * sizeof(T),
+                               cudaMemcpyDeviceToDevice, st));
+        const int pb = cur ^ 1;
+        const T* b = src + 5 * (size_t)np;
+        CK(cudaMemcpyAsync(bankp(pb, SP_RHO), b, 4 * plane * sizeof(T), cudaMemcpyDeviceToDevice,
+                           st));
+        CK(cudaMemcpyAsync(bankp(pb, SP_JX), b + 4 * plane, 3 * plane * sizeof(T),
+                           cudaMemcpyDeviceToDevice, st));
+        return QS_OK;
+    }
+
+    qs_status adjoint_checkpoints(int every) override {
+        if (every < 0) return fail(QS_ERR_INVALID, "qs_adjoint_checkpoints: every must be >= 0");
+        if (every > 0 && S != 1)
+            return fail(QS_ERR_UNSUPPORTED, "the adjoint supports NxSplit = 1");
+        if (every > 0 && cfg.shape != QS_SHAPE_NGP)
+            return fail(QS_ERR_UNSUPPORTED, "the adjoint supports the NGP shape");
+        CK(cudaStreamSynchronize(st));
+        void* old[] = {ck, seg, lam, lam_pm, lam_sb, lam_b3, d_dloss};
+        for (void* p : old)
+            if (p) cudaFree(p);
+        ck = seg = lam = lam_pm = lam_sb = lam_b3 = d_dloss = nullptr;
+        ck_every = 0;
+        ck_valid = false;
+        if (gexec) {   // the captured march has (or lacks) the checkpoint copies
+            cudaGraphExecDestroy(gexec);
+            gexec = nullptr;
+        }
+        if (every == 0) return QS_OK;
+        if (np <= 0) return fail(QS_ERR_STATE, "qs_adjoint_checkpoints: no plasma loaded");
+        const int K = std::min(every, L);
+        adj_np = np;
+        ck_count = (L + K - 1) / K;
+        qs_status s;
+        if ((s = alloc(&ck, (size_t)ck_count * ck_stride(), "adjoint checkpoints"))) return s;
+        if ((s = alloc(&seg, (size_t)K * seg_stride(), "adjoint segment"))) return s;
+        if ((s = alloc(&lam, (size_t)LAM_N * plane, "adjoint planes"))) return s;
+        if ((s = alloc(&lam_pm, 3 * (size_t)np, "adjoint momenta"))) return s;
+        if ((s = alloc(&lam_sb, (size_t)(L + 1) * 2 * plane, "adjoint beam spectra"))) return s;
+        if ((s = alloc(&lam_b3, (size_t)(L + 1) * 2 * plane, "adjoint beam currents"))) return s;
+        if ((s = alloc(&d_dloss, (size_t)L, "loss gradient"))) return s;
+        ck_every = K;
+        return QS_OK;
+    }
+
+    // adjoint work planes
+    enum { LAM_C = 0,          // 7: adjoint of this layer's final bank (Rho, Ex..Ez, Jx..Jz)
+           LAM_P = 7,          // 7: adjoint of this layer's P-bank inputs
+           LAM_CF = 14,        // 6: adjoint of this layer's final fields (field store layer i)
+           LAM_PF = 20,        // 6: adjoint of the P-layer fields (layer i+1)
+           LAM_CX = 26,        // 6: adjoint of an intermediate C-layer field set
+           LAM_SPEC = 32,      // 6: adjoint of E, B spectra
+           LAM_J = 38,         // 3: adjoint of the J spectra
+           LAM_D = 41,         // 3: adjoint of the real deposit Jx, Jy, Jz
+           LAM_RHO0 = 44,      // 2: adjoint of rho_old along the corrector chain
+           LAM_N = 46 };
+    T* lamp(int i) { return lam + (size_t)i * plane; }
+    T* lam_sbp(int layer, int q) { return lam_sb + ((size_t)layer * 2 + q) * plane; }
+
+    // recompute the layers c .. lo of one segment from its checkpoint, storing
+    // each layer's entry particles and intermediate C fields
+    qs_status recompute_segment(int m, int c, int lo) {
+        in_march = true;
+        qs_status s = restore_checkpoint(m);
+        for (int i = c; !s && i >= lo; i--) {
+            T* slot = seg + (size_t)(c - i) * seg_stride();
+            for (int q = 0; q < 5; q++)
+                CK(cudaMemcpyAsync(slot + (size_t)q * np, particle_arrays(q), np * sizeof(T),
+                                   cudaMemcpyDeviceToDevice, st));
+            T* fs = slot + 5 * (size_t)np;
+            if ((s = layer_begin(i, 0))) break;
+            if ((s = guess(i, 0))) break;
+            CK(cudaMemcpyAsync(fs, Cf, 6 * plane * sizeof(T), cudaMemcpyDeviceToDevice, st));
+            for (int it = 0; it < nIter && !s; it++) {
+                if ((s = push(i, 0, 0))) break;
+                if ((s = iterate(i, 0, it, nullptr))) break;
+                CK(cudaMemcpyAsync(fs + (size_t)(it + 1) * 6 * plane, Cf, 6 * plane * sizeof(T),
+                                   cudaMemcpyDeviceToDevice, st));
+            }
+            if (s) break;
+            if ((s = push(i, 0, 1))) break;
+            if ((s = iterate(i, 0, -1, nullptr))) break;
+            if ((s = layer_end(i, 0))) break;
+        }
+        in_march = false;
+        return s;
+    }
+
+    // transform `nf` adjoint planes in place of the spectral adjoint: out = scale T(in)
+    void adj_xform(const T* in, T* out, int nf, const int* kz, const int* ky, T scale) {
+        T* outs[6];
+        for (int f = 0; f < nf; f++) outs[f] = out + (size_t)f * plane;
+        xform(job_stack(in, nf, outs, kz, ky, scale));
+    }
+
+    AdjSpecArgs<T> adj_args(int iLayer) {
+        const SpecArgs<T> f = spec_args(iLayer, 0);
+        AdjSpecArgs<T> a{};
+        a.ny = My; a.nz = Mz;
+        a.piY = f.piY; a.piZ = f.piZ; a.hx = f.hx; a.dens = f.dens;
+        a.lRb0 = lam_sbp(iLayer, 0); a.lRb1 = lam_sbp(iLayer + 1, 0);
+        a.lJxb0 = lam_sbp(iLayer, 1); a.lJxb1 = lam_sbp(iLayer + 1, 1);
+        a.wb0 = f.wb0; a.wb1 = f.wb1;
+        a.lRbp0 = lam_sbp(std::min(iLayer + 1, L), 0);
+        a.lRbp1 = lam_sbp(std::min(iLayer + 2, L), 0);
+        a.wp0 = f.wp0; a.wp1 = f.wp1;
+        return a;
+    }
+
+    PushAdjArgs<T> push_adj_args(const T* slot, const T* Cfield, int full) {
+        PushAdjArgs<T> a{};
+        a.n = np; a.My = My; a.Mz = Mz;
+        a.cell = pcell;
+        a.y = slot; a.z = slot + np; a.px = slot + 2 * np; a.py = slot + 3 * np;
+        a.pz = slot + 4 * np; a.w = pw;
+        a.P = Pf; a.C = Cfield;
+        a.lamD = lamp(LAM_D);
+        a.lamPm = lam_pm;
+        a.lamFP = lamp(LAM_PF);
+        a.lamFC = lamp(LAM_CX);
+        a.plane = plane;
+        a.sE = (T)(cfg.plasma_q2m * cfg.hx / 2.0);
+        a.hxhy = (T)(cfg.hx / cfg.hy); a.hxhz = (T)(cfg.hx / cfg.hz);
+        a.djx0 = (T)cfg.plasma_djx0; a.djy0 = (T)cfg.plasma_djy0; a.djz0 = (T)cfg.plasma_djz0;
+        a.bxe = (T)cfg.bx_ext; a.bye = (T)cfg.by_ext; a.bze = (T)cfg.bz_ext;
+        a.full = full;
+        a.precise = sizeof(T) == 4;
+        return a;
+    }
+
+    // reverse sweep over one layer (the transpose of move_split_layer)
+    qs_status adjoint_layer(int i, const T* slot) {
+        const int EBz[6] = {CC, CC, SS, SS, SS, CC}, EBy[6] = {CC, SS, CC, SS, CC, SS};
+        const int Jz[3] = {CC, CC, SS}, Jy[3] = {CC, SS, CC};
+        const T* fs = slot + 5 * (size_t)np;
+        const T sc = inv_scale();
+        Pf = f3layer(i + 1);
+        CK(cudaMemsetAsync(lamp(LAM_PF), 0, 6 * plane * sizeof(T), st));
+        klaunch(KC_MISC, [&] {
+            return launch_add_point<T>(lamp(LAM_CF), (size_t)(My / 2) + (size_t)My * (Mz / 2),
+                                       d_dloss, i, st);
+        });
+        // final Iterate: C fields <- inverse transforms of its E, B
+        adj_xform(lamp(LAM_CF), lamp(LAM_SPEC), 6, EBz, EBy, sc);
+        {
+            AdjSpecArgs<T> a = adj_args(i);
+            a.lRho = lamp(LAM_C + 0);
+            for (int c = 0; c < 3; c++) {
+                a.lE[c] = lamp(LAM_SPEC + c);
+                a.lEb[c] = lamp(LAM_C + 1 + c);
+                a.lB[c] = lamp(LAM_SPEC + 3 + c);
+                a.lJb[c] = lamp(LAM_C + 4 + c);
+                a.lJ[c] = lamp(LAM_J + c);
+            }
+            a.lRhoOld = lamp(LAM_RHO0);
+            for (int f = 0; f < 7; f++) a.lP[f] = lamp(LAM_P + f);
+            a.lP_set = 1;
+            klaunch(KC_SPECTRAL, [&] { return launch_corrector_adjoint<T>(a, st); });
+        }
+        adj_xform(lamp(LAM_J), lamp(LAM_D), 3, Jz, Jy, T(1));
+        CK(cudaMemsetAsync(lamp(LAM_CX), 0, 6 * plane * sizeof(T), st));
+        klaunch(KC_PUSH, [&] {
+            return launch_push_adjoint<T>(push_adj_args(slot, fs + (size_t)nIter * 6 * plane, 1), st);
+        });
+        int rho_in = LAM_RHO0;
+        for (int it = nIter - 1; it >= 0; it--) {
+            adj_xform(lamp(LAM_CX), lamp(LAM_SPEC), 6, EBz, EBy, sc);
+            AdjSpecArgs<T> a = adj_args(i);
+            a.lRho = lamp(rho_in);
+            const int rho_out = rho_in == LAM_RHO0 ? LAM_RHO0 + 1 : LAM_RHO0;
+            for (int c = 0; c < 3; c++) {
+                a.lE[c] = lamp(LAM_SPEC + c);
+                a.lB[c] = lamp(LAM_SPEC + 3 + c);
+                a.lJ[c] = lamp(LAM_J + c);
+            }
+            a.lRhoOld = lamp(rho_out);
+            for (int f = 0; f < 7; f++) a.lP[f] = lamp(LAM_P + f);
+            a.lP_set = 0;
+            klaunch(KC_SPECTRAL, [&] { return launch_corrector_adjoint<T>(a, st); });
+            rho_in = rho_out;
+            adj_xform(lamp(LAM_J), lamp(LAM_D), 3, Jz, Jy, T(1));
+            CK(cudaMemsetAsync(lamp(LAM_CX), 0, 6 * plane * sizeof(T), st));
+            klaunch(KC_PUSH, [&] {
+                return launch_push_adjoint<T>(push_adj_args(slot, fs + (size_t)it * 6 * plane, 0),
+                                              st);
+            });
+        }
+        // Guess: C fields <- inverse transforms of the predicted E, B
+        adj_xform(lamp(LAM_CX), lamp(LAM_SPEC), 6, EBz, EBy, sc);
+        {
+            AdjSpecArgs<T> a = adj_args(i);
+            a.lRho = lamp(rho_in);
+            for (int c = 0; c < 3; c++) {
+                a.lE[c] = lamp(LAM_SPEC + c);
+                a.lB[c] = lamp(LAM_SPEC + 3 + c);
+            }
+            for (int f = 0; f < 7; f++) a.lP[f] = lamp(LAM_P + f);
+            a.lP_set = 0;
+            klaunch(KC_SPECTRAL, [&] { return launch_predictor_adjoint<T>(a, st); });
+        }
+        // hand the P-side adjoints to layer i+1 (its final bank and fields)
+        CK(cudaMemcpyAsync(lamp(LAM_C), lamp(LAM_P), 7 * plane * sizeof(T),
+                           cudaMemcpyDeviceToDevice, st));
+        CK(cudaMemcpyAsync(lamp(LAM_CF), lamp(LAM_PF), 6 * plane * sizeof(T),
+                           cudaMemcpyDeviceToDevice, st));
+        CK(cudaGetLastError());
+        return QS_OK;
+    }
+
+    qs_status adjoint(const double* dloss, double* dw) override {
+        if (!dloss || !dw) return fail(QS_ERR_INVALID, "qs_adjoint: null pointer");
+        if (ck_every <= 0) return fail(QS_ERR_STATE, "qs_adjoint: checkpoints are off");
+        if (!ck_valid || np != adj_np)
+            return fail(QS_ERR_STATE, "qs_adjoint: the last march did not store checkpoints "
+                                      "for the current beam");
+        int lo = -1;
+        for (int i = 0; i < L && lo < 0; i++)
+            if (dloss[i] != 0.0) lo = i;
+        if (nb > adj_nb) {
+            if (d_gradw) cudaFree(d_gradw);
+            d_gradw = nullptr;
+            qs_status s = alloc(&d_gradw, (size_t)nb, "beam weight gradient");
+            if (s) return s;
+            adj_nb = nb;
+        }
+        {
+            std::vector<T> h(L);
+            for (int i = 0; i < L; i++) h[i] = (T)dloss[i];
+            CK(cudaMemcpyAsync(d_dloss, h.data(), L * sizeof(T), cudaMemcpyHostToDevice, st));
+            CK(cudaStreamSynchronize(st));
+        }
+        CK(cudaMemsetAsync(lam, 0, (size_t)LAM_N * plane * sizeof(T), st));
+        CK(cudaMemsetAsync(lam_pm, 0, 3 * (size_t)np * sizeof(T), st));
+        CK(cudaMemsetAsync(lam_sb, 0, (size_t)(L + 1) * 2 * plane * sizeof(T), st));
+        if (lo >= 0) {
+            const int K = ck_every;
+            const int mlo = (L - 1 - lo) / K;
+            for (int m = mlo; m >= 0; m--) {
+                const int c = L - 1 - m * K;
+                const int end = std::max(c - K + 1, lo);
+                cur = 0;
+                qs_status s = recompute_segment(m, c, end);
+                if (s) return s;
+                for (int i = end; i <= c; i++) {
+                    if ((s = adjoint_layer(i, seg + (size_t)(c - i) * seg_stride()))) return s;
+                }
+            }
+        }
+        // beam spectra adjoint -> real beam-current adjoint -> d loss / d w
+        const int CCk[8] = {CC, CC, CC, CC, CC, CC, CC, CC};
+        const int nplanes = 2 * (L + 1);
+        for (int b0 = 0; b0 < nplanes; b0 += 8) {
+            const int nf = std::min(8, nplanes - b0);
+            T* outs[8];
+            for (int f = 0; f < nf; f++) outs[f] = lam_b3 + (size_t)(b0 + f) * plane;
+            xform(job_stack(lam_sb + (size_t)b0 * plane, nf, outs, CCk, CCk, T(1)));
+        }
+        BeamGradArgs<T> g{};
+        g.n = nb; g.L = L; g.My = My; g.Mz = Mz;
+        g.bi = bi; g.bj = bj; g.bk = bk;
+        g.x = bx; g.y = by; g.z = bz; g.px = bpx; g.py = bpy; g.pz = bpz;
+        g.lb3 = lam_b3;
+        g.plane = plane;
+        g.polarity = cfg.beam_polarity;
+        g.out = d_gradw;
+        klaunch(KC_BEAM_PUSH, [&] { return launch_beam_weight_grad<T>(g, st); });
+        CK(cudaGetLastError());
+        if (nb > 0)
+            CK(cudaMemcpyAsync(dw, d_gradw, nb * sizeof(double), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        ck_valid = false;   // the recomputation reused the march's working state
         return QS_OK;
     }
 
@@ -1321,6 +1666,18 @@ qs_status qs_transform2d_dev(qs_handle* h, int kind_z, int kind_y, int batch, co
                              void* d_out) {
     H_OR_INVALID(h);
     return E->transform2d_dev(kind_z, kind_y, batch, d_in, d_out);
+}
+
+qs_status qs_adjoint_checkpoints(qs_handle* h, int every) {
+    H_OR_INVALID(h);
+    return E->adjoint_checkpoints(every);
+}
+
+qs_status qs_adjoint(qs_handle* h, const double* dloss_donaxis_ex, double* dloss_dbeam_weight) {
+    H_OR_INVALID(h);
+    qs_status s = E->adjoint(dloss_donaxis_ex, dloss_dbeam_weight);
+    if (s) return s;
+    return E->check_device();
 }
 
 qs_status qs_step_host(qs_handle* h, int64_t n_beam, const int32_t* i, const int32_t* j,

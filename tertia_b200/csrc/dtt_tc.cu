@@ -37,6 +37,7 @@
 #include "dtt_tc.h"
 #include "qs_common.cuh"
 #include "split.cuh"
+#include "pdl.cuh"
 
 namespace qs {
 namespace tcx {
@@ -253,8 +254,10 @@ __global__ void __launch_bounds__(THREADS_V2, 1)
     const uint32_t tmem = tmem_slot;
     volatile int* abortp = &abort_flag;
     if (threadIdx.x == 0) trace(1);
+    qs::pdl_wait();   // operands and outputs are the previous kernel's
 
     if (warp == 0) {
+        if (lane != 0) qs::pdl_trigger();
         if (lane == 0) {
             // ---------------- TMA producer
             asm volatile("prefetch.tensormap [%0];" ::"l"((uint64_t)&mapM) : "memory");
@@ -284,12 +287,14 @@ __global__ void __launch_bounds__(THREADS_V2, 1)
                                 t * p.data_rows + rowD);
                 issued = kb + 1;
             }
+            qs::pdl_trigger();
             if (*abortp) {
                 for (int kb = (issued > STAGES ? issued - STAGES : 0); kb < issued; kb++)
                     mbar_wait(smem_u32(&full_bar[kb % STAGES]), (kb / STAGES) & 1, abortp);
             }
         }
     } else if (warp == 1) {
+        if (lane != 0) qs::pdl_trigger();
         if (lane == 0) {
             // ---------------- MMA issuer
             const uint32_t idesc = (1u << 4) | ((KIND == 0 ? 1u : 2u) << 7) |
@@ -335,6 +340,7 @@ __global__ void __launch_bounds__(THREADS_V2, 1)
                 }
                 if (ok) mma_commit(smem_u32(&accf[b]));
             }
+            qs::pdl_trigger();
         }
     } else {
         // ---------------- epilogue: drain every chunk into FP32 registers
@@ -372,6 +378,7 @@ __global__ void __launch_bounds__(THREADS_V2, 1)
                              : "memory");
             }
         }
+        qs::pdl_trigger();
         // every MMA has completed (the last chunk was committed after them),
         // so the pipeline smem is free: stage the tile there row-major
         constexpr int LD = BN + 4;
@@ -454,7 +461,9 @@ __global__ void split_planes_kernel(const float* __restrict__ in, size_t stride,
     const size_t i4 = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) * 4;
     const int f = blockIdx.y;
     if (i4 >= plane || f >= nf) return;
+    qs::pdl_wait();
     const float4 v = *(const float4*)(in + (size_t)f * stride + i4);
+    qs::pdl_trigger();
     const float vv[4] = {v.x, v.y, v.z, v.w};
     float t[4][3];
 #pragma unroll
@@ -664,14 +673,14 @@ public:
         const int T = tcx::THREADS_V2;
         const size_t sm = smem_bytes[b];
         if (mode == QS_PREC_BF16X3) {
-            if (b) tcx::dtt_tc_kernel<0, 2, 3, 128><<<grid, T, sm, st>>>(M, D, p);
-            else tcx::dtt_tc_kernel<0, 2, 4, 64><<<grid, T, sm, st>>>(M, D, p);
+            if (b) qs::launch_pdl(tcx::dtt_tc_kernel<0, 2, 3, 128>, grid, dim3(T), sm, st, M, D, p);
+            else qs::launch_pdl(tcx::dtt_tc_kernel<0, 2, 4, 64>, grid, dim3(T), sm, st, M, D, p);
         } else if (mode == QS_PREC_TF32X3) {
-            if (b) tcx::dtt_tc_kernel<1, 2, 3, 128><<<grid, T, sm, st>>>(M, D, p);
-            else tcx::dtt_tc_kernel<1, 2, 4, 64><<<grid, T, sm, st>>>(M, D, p);
+            if (b) qs::launch_pdl(tcx::dtt_tc_kernel<1, 2, 3, 128>, grid, dim3(T), sm, st, M, D, p);
+            else qs::launch_pdl(tcx::dtt_tc_kernel<1, 2, 4, 64>, grid, dim3(T), sm, st, M, D, p);
         } else {
-            if (b) tcx::dtt_tc_kernel<0, 3, 2, 128><<<grid, T, sm, st>>>(M, D, p);
-            else tcx::dtt_tc_kernel<0, 3, 3, 64><<<grid, T, sm, st>>>(M, D, p);
+            if (b) qs::launch_pdl(tcx::dtt_tc_kernel<0, 3, 2, 128>, grid, dim3(T), sm, st, M, D, p);
+            else qs::launch_pdl(tcx::dtt_tc_kernel<0, 3, 3, 64>, grid, dim3(T), sm, st, M, D, p);
         }
     }
 
@@ -680,11 +689,11 @@ public:
         const size_t ts = (size_t)nfmax * plane;
         dim3 sg((unsigned)((plane / 4 + 255) / 256), nf);
         if (kind == 0 && nsplit == 2)
-            tcx::split_planes_kernel<0, 2><<<sg, 256, 0, st>>>(base, plane, nf, plane, ts, splitA);
+            qs::launch_pdl(tcx::split_planes_kernel<0, 2>, sg, dim3(256), 0, st, base, plane, nf, plane, ts, splitA);
         else if (kind == 0)
-            tcx::split_planes_kernel<0, 3><<<sg, 256, 0, st>>>(base, plane, nf, plane, ts, splitA);
+            qs::launch_pdl(tcx::split_planes_kernel<0, 3>, sg, dim3(256), 0, st, base, plane, nf, plane, ts, splitA);
         else
-            tcx::split_planes_kernel<1, 2><<<sg, 256, 0, st>>>(base, plane, nf, plane, ts, splitA);
+            qs::launch_pdl(tcx::split_planes_kernel<1, 2>, sg, dim3(256), 0, st, base, plane, nf, plane, ts, splitA);
     }
 
     void pass_params(int stage, int nf, const int* kz, const int* ky, double scale,

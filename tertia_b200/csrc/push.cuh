@@ -22,6 +22,7 @@
 #pragma once
 #include "qs_common.cuh"
 #include "qs_internal.h"
+#include "pdl.cuh"
 
 namespace qs {
 
@@ -407,6 +408,7 @@ __global__ void __launch_bounds__(128) push_cell_kernel(PushArgs<float> a) {
     const int cell = blockIdx.x * blockDim.x + threadIdx.x;
     const int My = a.My, Mz = a.Mz;
     if (cell >= My * Mz) return;
+    pdl_wait();
     int j, k;
     cell_jk(cell, My, a.invMy, j, k);
     const size_t plane = a.plane;
@@ -487,6 +489,7 @@ __global__ void __launch_bounds__(128) push_cell_kernel(PushArgs<float> a) {
         }
         yv[q] = ytmp; zv[q] = ztmp; pxv[q] = px; pyv[q] = py; pzv[q] = pz;
     }
+    pdl_trigger();
     atomicAdd(a.dep + 0 * plane + n, own0);
     atomicAdd(a.dep + 1 * plane + n, own1);
     atomicAdd(a.dep + 2 * plane + n, own2);
@@ -508,7 +511,7 @@ int launch_push(const PushArgs<T>& a, int shape, bool precise, cudaStream_t st) 
         if constexpr (F32) {
             if (a.uniform_ppc == 4 && a.n == (int64_t)a.My * a.Mz * 4 && !a.dep_cell) {
                 const int cells = a.My * a.Mz;
-                push_cell_kernel<4><<<(cells + 127) / 128, 128, 0, st>>>(a);
+                launch_pdl(push_cell_kernel<4>, dim3((cells + 127) / 128), dim3(128), 0, st, a);
                 return 1;
             }
             push_kernel<T, QS_SHAPE_NGP, true, true><<<blocks, threads, 0, st>>>(a);

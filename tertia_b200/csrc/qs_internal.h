@@ -28,6 +28,9 @@ struct SpecArgs {
     void* split;
     int nsplit, split_kind, split_rho;
     size_t tstride;
+    // optional: 4 planes (the C-layer deposit) cleared by the kernel for the
+    // push that follows it (ClearCurrentsSplit without a separate memset)
+    T* zero_src;
 };
 
 template <class T>
@@ -96,5 +99,78 @@ struct BeamArgs {
 };
 template <class T>
 int launch_beam_push(const BeamArgs<T>& a, cudaStream_t st);
+
+// ---- adjoint (adjoint.cu)
+
+// Push adjoint of one layer: the particles' layer-entry state, the P and C
+// fields the push gathered, and the adjoint of its deposit (Jx, Jy, Jz) in;
+// the adjoint of the momenta (3 x n, in/out: set by the full push, added to
+// by the half pushes) and of the P and C fields (added to) out.
+template <class T>
+struct PushAdjArgs {
+    int64_t n;
+    int My, Mz;
+    const int32_t* cell;
+    const T *y, *z, *px, *py, *pz, *w;
+    const T* P;
+    const T* C;
+    const T* lamD;        // 3 planes
+    T* lamPm;             // 3 x n
+    T* lamFP;             // 6 planes
+    T* lamFC;             // 6 planes
+    size_t plane;
+    T sE, hxhy, hxhz, djx0, djy0, djz0, bxe, bye, bze;
+    int full, precise;
+};
+template <class T>
+int launch_push_adjoint(const PushAdjArgs<T>& a, cudaStream_t st);
+
+// Per-mode adjoint of the predictor / corrector.  Inputs (any may be null =
+// zero): lRho, lE (+ lEb, a second contribution), lB, lJb (adjoint of the
+// corrector's J input that reaches it from the bank).  Outputs: lJ (total
+// adjoint of the corrector's J input), lRhoOld (adjoint of its rho_old), lP
+// (adjoint of the 7 P-bank inputs RhoP, ExP, EyP, EzP, JxP, JyP, JzP; set
+// when lP_set, else added to) and the beam spectra (added to, with the
+// xi-interpolation weights of the forward).
+template <class T>
+struct AdjSpecArgs {
+    int ny, nz;
+    T piY, piZ, hx, dens;
+    const T* lRho;
+    const T* lE[3];
+    const T* lEb[3];
+    const T* lB[3];
+    const T* lJb[3];
+    T* lJ[3];
+    T* lRhoOld;
+    T* lP[7];
+    int lP_set;
+    T *lRb0, *lRb1, *lJxb0, *lJxb1;
+    T wb0, wb1;
+    T *lRbp0, *lRbp1;
+    T wp0, wp1;
+};
+template <class T>
+int launch_corrector_adjoint(const AdjSpecArgs<T>& a, cudaStream_t st);
+template <class T>
+int launch_predictor_adjoint(const AdjSpecArgs<T>& a, cudaStream_t st);
+template <class T>
+int launch_add_point(T* plane_ex, size_t idx, const T* v, int layer, cudaStream_t st);
+
+// d loss / d (beam macro-particle weight) from the adjoint of the real beam
+// currents (lb3: (L+1) layers x 2 planes RhoBeam, JxBeam).
+template <class T>
+struct BeamGradArgs {
+    int64_t n;
+    int L, My, Mz;
+    const int32_t *bi, *bj, *bk;
+    const double *x, *y, *z, *px, *py, *pz;
+    const T* lb3;
+    size_t plane;
+    double polarity;
+    double* out;
+};
+template <class T>
+int launch_beam_weight_grad(const BeamGradArgs<T>& a, cudaStream_t st);
 
 }  // namespace qs

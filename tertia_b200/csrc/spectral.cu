@@ -66,6 +66,8 @@ __global__ void predictor_kernel(SpecArgs<T> a) {
     a.Ex[n1] = ex;
     a.Ey[n1] = ey;
     a.Ez[n1] = ez;
+    if (a.zero_src)
+        for (int q = 0; q < 4; q++) a.zero_src[(size_t)q * N + n1] = T(0);
     if (a.write_b) {
         a.Bx[n1] = bx;
         a.By[n1] = by;
@@ -108,6 +110,8 @@ __global__ void corrector_kernel(SpecArgs<T> a) {
     a.Ez[n1] = newEz;
     a.Rho[n1] = rho;
     a.Ex[n1] = newEx;
+    if (a.zero_src)
+        for (int q = 0; q < 4; q++) a.zero_src[(size_t)q * N + n1] = T(0);
     if (a.write_b) {
         a.Bx[n1] = bx;
         a.By[n1] = by;

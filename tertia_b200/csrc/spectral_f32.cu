@@ -18,6 +18,7 @@
 #include "qs_common.cuh"
 #include "qs_internal.h"
 #include "split.cuh"
+#include "pdl.cuh"
 
 namespace qs {
 namespace {
@@ -57,6 +58,15 @@ __device__ __forceinline__ BeamPair beam_pair(const SpecArgs<float>& a, size_t n
     return b;
 }
 
+// clear two modes of the 4 deposit planes the next push adds to
+__device__ __forceinline__ void zero_src2(const SpecArgs<float>& a, size_t n) {
+    if (a.zero_src) {
+        const size_t N = (size_t)a.ny * a.nz;
+#pragma unroll
+        for (int q = 0; q < 4; q++) st2(a.zero_src + q * N, n, 0.f, 0.f);
+    }
+}
+
 // split terms of two adjacent values into NSPLIT term planes (KIND 0: bf16,
 // KIND 1: tf32 in float storage); idx is even
 template <int KIND, int NSPLIT>
@@ -85,6 +95,7 @@ __global__ void __launch_bounds__(kThreads) predictor_f32_kernel(SpecArgs<float>
     const int j = 2 * (blockIdx.x * kThreads + threadIdx.x);
     const int k = blockIdx.y;
     if (j >= a.ny) return;
+    pdl_wait();
     const size_t n = (size_t)j + (size_t)a.ny * k;
     const float d = a.dens, hx = a.hx;
     const float dh2 = d * hx * hx;
@@ -98,6 +109,7 @@ __global__ void __launch_bounds__(kThreads) predictor_f32_kernel(SpecArgs<float>
                  jzp2 = ld2(a.JzP, n), exp2 = ld2(a.ExP, n), eyp2 = ld2(a.EyP, n),
                  ezp2 = ld2(a.EzP, n);
     const BeamPair b = beam_pair(a, n);
+    pdl_trigger();
     const float rp_[2] = {rp2.x, rp2.y}, jxp_[2] = {jxp2.x, jxp2.y}, jyp_[2] = {jyp2.x, jyp2.y},
                 jzp_[2] = {jzp2.x, jzp2.y}, exp_[2] = {exp2.x, exp2.y},
                 eyp_[2] = {eyp2.x, eyp2.y}, ezp_[2] = {ezp2.x, ezp2.y};
@@ -125,6 +137,7 @@ __global__ void __launch_bounds__(kThreads) predictor_f32_kernel(SpecArgs<float>
     st2(a.Ex, n, ex[0], ex[1]);
     st2(a.Ey, n, ey[0], ey[1]);
     st2(a.Ez, n, ez[0], ez[1]);
+    zero_src2(a, n);
     if (a.write_b) {
         st2(a.Bx, n, bx[0], bx[1]);
         st2(a.By, n, by[0], by[1]);
@@ -143,6 +156,7 @@ __global__ void __launch_bounds__(kThreads) corrector_f32_kernel(SpecArgs<float>
     const int j = 2 * (blockIdx.x * kThreads + threadIdx.x);
     const int k = blockIdx.y;
     if (j >= a.ny) return;
+    pdl_wait();
     const size_t n = (size_t)j + (size_t)a.ny * k;
     const float d = a.dens, hx = a.hx;
     const float akz = a.piZ * ((float)k + 0.5f);
@@ -150,6 +164,7 @@ __global__ void __launch_bounds__(kThreads) corrector_f32_kernel(SpecArgs<float>
                  jxp2 = ld2(a.JxP, n), jyp2 = ld2(a.JyP, n), jzp2 = ld2(a.JzP, n),
                  eyp2 = ld2(a.EyP, n), ezp2 = ld2(a.EzP, n), rold2 = ld2(a.Rho, n);
     const BeamPair b = beam_pair(a, n);
+    pdl_trigger();
     const float rp_[2] = {rp2.x, rp2.y}, jx_[2] = {jx2.x, jx2.y}, jy_[2] = {jy2.x, jy2.y},
                 jz_[2] = {jz2.x, jz2.y}, jxp_[2] = {jxp2.x, jxp2.y}, jyp_[2] = {jyp2.x, jyp2.y},
                 jzp_[2] = {jzp2.x, jzp2.y}, eyp_[2] = {eyp2.x, eyp2.y},
@@ -175,6 +190,7 @@ __global__ void __launch_bounds__(kThreads) corrector_f32_kernel(SpecArgs<float>
     st2(a.Ez, n, ez[0], ez[1]);
     st2(a.Rho, n, rho[0], rho[1]);
     st2(a.Ex, n, ex[0], ex[1]);
+    zero_src2(a, n);
     if (a.write_b) {
         st2(a.Bx, n, bx[0], bx[1]);
         st2(a.By, n, by[0], by[1]);
@@ -206,10 +222,10 @@ int launch_predictor_fast(const SpecArgs<float>& a, cudaStream_t st) {
     if (a.ny % 2 || c < 0) return 0;
     const dim3 g((unsigned)((a.ny / 2 + kThreads - 1) / kThreads), (unsigned)a.nz);
     switch (c) {
-        case 0: predictor_f32_kernel<0, 0><<<g, kThreads, 0, st>>>(a); break;
-        case 1: predictor_f32_kernel<0, 2><<<g, kThreads, 0, st>>>(a); break;
-        case 2: predictor_f32_kernel<1, 2><<<g, kThreads, 0, st>>>(a); break;
-        default: predictor_f32_kernel<0, 3><<<g, kThreads, 0, st>>>(a); break;
+        case 0: launch_pdl(predictor_f32_kernel<0, 0>, g, dim3(kThreads), 0, st, a); break;
+        case 1: launch_pdl(predictor_f32_kernel<0, 2>, g, dim3(kThreads), 0, st, a); break;
+        case 2: launch_pdl(predictor_f32_kernel<1, 2>, g, dim3(kThreads), 0, st, a); break;
+        default: launch_pdl(predictor_f32_kernel<0, 3>, g, dim3(kThreads), 0, st, a); break;
     }
     return 1;
 }
@@ -219,10 +235,10 @@ int launch_corrector_fast(const SpecArgs<float>& a, cudaStream_t st) {
     if (a.ny % 2 || c < 0) return 0;
     const dim3 g((unsigned)((a.ny / 2 + kThreads - 1) / kThreads), (unsigned)a.nz);
     switch (c) {
-        case 0: corrector_f32_kernel<0, 0><<<g, kThreads, 0, st>>>(a); break;
-        case 1: corrector_f32_kernel<0, 2><<<g, kThreads, 0, st>>>(a); break;
-        case 2: corrector_f32_kernel<1, 2><<<g, kThreads, 0, st>>>(a); break;
-        default: corrector_f32_kernel<0, 3><<<g, kThreads, 0, st>>>(a); break;
+        case 0: launch_pdl(corrector_f32_kernel<0, 0>, g, dim3(kThreads), 0, st, a); break;
+        case 1: launch_pdl(corrector_f32_kernel<0, 2>, g, dim3(kThreads), 0, st, a); break;
+        case 2: launch_pdl(corrector_f32_kernel<1, 2>, g, dim3(kThreads), 0, st, a); break;
+        default: launch_pdl(corrector_f32_kernel<0, 3>, g, dim3(kThreads), 0, st, a); break;
     }
     return 1;
 }

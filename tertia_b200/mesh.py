@@ -213,6 +213,12 @@ class Mesh:
                                          _p(out, C.c_double)), "qs_transform2d")
         return out
 
+    def transform2d_dev(self, kind_z: int, kind_y: int, batch: int, d_in: int, d_out: int):
+        """qs_transform2d_dev on device pointers (float, or double in FP64),
+        enqueued on the handle's stream."""
+        self._chk(self._L.qs_transform2d_dev(self._h, kind_z, kind_y, batch, C.c_void_p(d_in),
+                                             C.c_void_p(d_out)), "qs_transform2d_dev")
+
     def step_host(self, b: dict, want_beam: bool = True, out: dict | None = None):
         """One step through host buffers (beam in, beam and on-axis Ex out).
         `out` may supply the output arrays (e.g. views of pinned memory)."""
@@ -231,6 +237,22 @@ class Mesh:
                                        *outs_i, *outs_f, _p(ex, C.c_double)), "qs_step_host")
         out["w"] = f[-1]
         return (out if want_beam else None), ex
+
+    # -------------------------------------------------------------- adjoint
+    def adjoint_checkpoints(self, every: int):
+        """Store layer checkpoints every `every` layers in the next marches."""
+        self._chk(self._L.qs_adjoint_checkpoints(self._h, int(every)), "qs_adjoint_checkpoints")
+
+    def adjoint(self, dloss_donaxis_ex) -> np.ndarray:
+        """d loss / d (beam weight) of every beam particle, given d loss / d
+        (on-axis Ex of each layer) for the last march."""
+        d = _f64(dloss_donaxis_ex).reshape(-1)
+        if d.size != self.cfg.nx:
+            raise ValueError("dloss_donaxis_ex needs one entry per layer")
+        out = np.empty(int(self._L.qs_beam_count(self._h)))
+        self._chk(self._L.qs_adjoint(self._h, _p(d, C.c_double), _p(out, C.c_double)),
+                  "qs_adjoint")
+        return out
 
     # reference-named aliases (mesh.h:55-76, step.cpp:24)
     Step = step

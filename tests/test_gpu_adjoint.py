@@ -1,0 +1,98 @@
+"""The adjoint of the xi-march (qs_adjoint) against central finite differences
+of the loss, and the FP32 adjoint against the FP64 adjoint.
+
+The loss is the on-axis longitudinal wake field (the reference's Ex) summed
+over a window of layers behind the driver; the parameters are the weights of
+xi-bins of the driver's charge profile.  The beam is deposited without moving
+(Ts = 0, no synchrotron loss), so every loss evaluation sees the same beam
+positions."""
+import numpy as np
+import pytest
+import torch
+
+from tertia_b200 import workload as wl
+from tertia_b200.abi import PRECISIONS, QsError
+from tertia_b200.autograd import wake_loss, xi_bins
+
+pytestmark = pytest.mark.gpu
+
+NBINS = 8
+
+
+def setup(prec, layers=48, n=32, every=8):
+    from tertia_b200.mesh import Mesh
+    cfg = wl.small_config(n=n, layers=layers, ts=0.0, synchrotron=0)
+    cfg.precision = PRECISIONS[prec]
+    beam = wl.small_beam(cfg, n=4000, nb=0.3)
+    x = (beam["i"] + beam["x"]) * cfg.hx
+    bins = xi_bins(beam, cfg, NBINS, float(x.min()), float(x.max()) + 1e-9)
+    m = Mesh(cfg)
+    m.load_front_plasma(wl.front_plasma(cfg, thermal=False))
+    m.adjoint_checkpoints(every)
+    # window: a band of layers in the middle of the box, behind the driver
+    coeff = np.zeros(cfg.nx)
+    coeff[layers // 4: layers // 2] = cfg.hx
+    return cfg, m, beam, bins, coeff
+
+
+def loss_at(m, beam, bins, coeff, beta):
+    return float(wake_loss(torch.tensor(beta, dtype=torch.float64), m, beam, bins, coeff))
+
+
+def adjoint_grad(m, beam, bins, coeff, beta):
+    t = torch.tensor(beta, dtype=torch.float64, requires_grad=True)
+    wake_loss(t, m, beam, bins, coeff).backward()
+    return t.grad.numpy().copy()
+
+
+def fd_grad(m, beam, bins, coeff, beta, h=1e-3):
+    g = np.zeros(NBINS)
+    for b in range(NBINS):
+        bp, bm = beta.copy(), beta.copy()
+        bp[b] += h
+        bm[b] -= h
+        g[b] = (loss_at(m, beam, bins, coeff, bp) - loss_at(m, beam, bins, coeff, bm)) / (2 * h)
+    return g
+
+
+def rel(a, b):
+    return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+
+def test_adjoint_fp64_matches_finite_differences():
+    cfg, m, beam, bins, coeff = setup("fp64")
+    beta = np.random.default_rng(5).uniform(0.5, 1.5, NBINS)
+    g = adjoint_grad(m, beam, bins, coeff, beta)
+    fd = fd_grad(m, beam, bins, coeff, beta)
+    assert np.linalg.norm(fd) > 0
+    assert rel(g, fd) < 1e-4, (g, fd)
+    m.close()
+
+
+def test_adjoint_fp32_close_to_fp64_adjoint():
+    beta = np.random.default_rng(6).uniform(0.5, 1.5, NBINS)
+    grads = {}
+    for prec in ("fp64", "fp32"):
+        cfg, m, beam, bins, coeff = setup(prec)
+        grads[prec] = adjoint_grad(m, beam, bins, coeff, beta)
+        m.close()
+    assert rel(grads["fp32"], grads["fp64"]) < 1e-4, grads
+
+
+def test_adjoint_needs_checkpointed_march():
+    cfg, m, beam, bins, coeff = setup("fp64")
+    m.load_beam(beam)
+    m.move_beam_particles()          # a new beam deposit since the last march
+    with pytest.raises(QsError):
+        m.adjoint(coeff)
+    m.close()
+
+
+def test_adjoint_checkpoint_interval_does_not_change_gradient():
+    beta = np.random.default_rng(7).uniform(0.5, 1.5, NBINS)
+    out = []
+    for every in (5, 48):
+        cfg, m, beam, bins, coeff = setup("fp64", every=every)
+        out.append(adjoint_grad(m, beam, bins, coeff, beta))
+        m.close()
+    assert rel(out[0], out[1]) < 1e-9    # atomic order of the FP64 deposits only
