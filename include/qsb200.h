@@ -303,7 +303,8 @@ int64_t qs_kernel_launches(const qs_handle* h);
 qs_status qs_profile_enable(qs_handle* h, int on);
 /* Milliseconds and launch counts per kernel class since the last read:
  * 0 push/deposit, 1 transform GEMM, 2 transform operand split, 3 spectral
- * maps, 4 beam-current spectra, 5 beam push, 6 front seeding, 7 other.
+ * maps, 4 beam-current spectra, 5 beam push, 6 front seeding, 7 other,
+ * 8 regrouping of the CIC plasma by cell.
  * Resets the counters. */
 qs_status qs_profile_read(qs_handle* h, double* ms, int64_t* launches, int n);
 

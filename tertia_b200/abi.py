@@ -199,4 +199,4 @@ EXPORTED_SYMBOLS = [
 ]
 
 KERNEL_CLASSES = ["push_deposit", "transform_gemm", "transform_split", "spectral_maps",
-                  "beam_spectra", "beam_push", "front_seed", "other"]
+                  "beam_spectra", "beam_push", "front_seed", "other", "plasma_regroup"]

@@ -213,6 +213,15 @@ struct Engine : EngineBase {
     int32_t* pcell = nullptr;
     T *py = nullptr, *pz = nullptr, *ppx = nullptr, *ppy = nullptr, *ppz = nullptr, *pw = nullptr;
     bool front_pending = false;
+    // FP32 CIC keeps the plasma grouped by cell (sort.cu): a second set of
+    // particle arrays for the regrouping scatter, load-order ids, per-cell
+    // counts and offsets, and where the grouping stands
+    bool cic_sort = false;
+    int32_t *acell = nullptr, *pid = nullptr, *apid = nullptr;
+    T *ay = nullptr, *az = nullptr, *apx = nullptr, *apy = nullptr, *apz = nullptr, *aw = nullptr;
+    int *cic_cnt = nullptr, *cic_loff = nullptr, *cic_bsum = nullptr, *cic_bpref = nullptr;
+    unsigned* cic_ticket = nullptr;
+    struct Grouping { bool grouped = true, off_valid = false, counted = false, flip = false; } grp;
     // programmatic dependent launch inside the march (QS_PDL=0 turns it off)
     bool use_pdl = !(getenv("QS_PDL") && getenv("QS_PDL")[0] == '0');
     bool uniform_layout = false;   // particle p in cell p / ppc (lattice seeding)
@@ -224,7 +233,7 @@ struct Engine : EngineBase {
     // graph of the march
     cudaGraphExec_t gexec = nullptr;
     int64_t graph_kernels = 0;
-    struct HostState { T *Pf, *Cf, *Psrc, *Csrc; int cur; } graph_end{};
+    struct HostState { T *Pf, *Cf, *Psrc, *Csrc; int cur; Grouping grp; } graph_end{};
     bool marched = false;
     // adjoint: layer checkpoints of the last march and the reverse sweep's buffers
     int ck_every = 0;           // checkpoint every ck_every layers (0: off)
@@ -249,7 +258,8 @@ struct Engine : EngineBase {
         void* ptrs[] = {f3, b3, src3, splitbuf, srcbuf, Cbeam, sb3, bank, scratch, mats, onaxis_d,
                         stage, stage_d, pcell, py, pz, ppx, ppy, ppz, pw, bi, bj, bk, bx, by, bz,
                         bpx, bpy, bpz, bw, d_err, ck, seg, lam, lam_pm, lam_sb, lam_b3,
-                        d_dloss, d_gradw};
+                        d_dloss, d_gradw, acell, pid, apid, ay, az, apx, apy, apz, aw, cic_cnt,
+                        cic_loff, cic_bsum, cic_bpref, cic_ticket};
         for (void* p : ptrs)
             if (p) cudaFree(p);
         if (st) cudaStreamDestroy(st);
@@ -283,6 +293,17 @@ struct Engine : EngineBase {
         CK(cudaMemset(srcbuf, 0, 8 * plane * sizeof(T)));
         if ((s = alloc(&Cbeam, 2 * plane, "beam layer"))) return s;
         CK(cudaMemset(Cbeam, 0, 2 * plane * sizeof(T)));
+        cic_sort = cfg.shape == QS_SHAPE_CIC && sizeof(T) == 4 && My % 32 == 0 && Mz % 4 == 0;
+        if (cic_sort) {
+            const int nb_scan = scan_blocks_count((int)plane);
+            if ((s = alloc(&cic_cnt, plane, "cell counts"))) return s;
+            if ((s = alloc(&cic_loff, plane, "cell offsets"))) return s;
+            if ((s = alloc(&cic_bsum, (size_t)nb_scan, "cell offsets"))) return s;
+            if ((s = alloc(&cic_bpref, (size_t)nb_scan + 1, "cell offsets"))) return s;
+            if ((s = alloc(&cic_ticket, 1, "cell offsets"))) return s;
+            CK(cudaMemset(cic_cnt, 0, plane * sizeof(int)));
+            CK(cudaMemset(cic_ticket, 0, sizeof(unsigned)));
+        }
         if ((s = alloc(&sb3, (size_t)(L + 1) * 2 * plane, "beam spectra"))) return s;
         CK(cudaMemset(sb3, 0, (size_t)(L + 1) * 2 * plane * sizeof(T)));
         sb3_valid = true;
@@ -363,11 +384,64 @@ struct Engine : EngineBase {
     T inv_scale() const { return (T)(1.0 / (4.0 * (double)My * (double)Mz)); }
 
     // ------------------------------------------------------------ particles
+    PlasmaSet<T> cur_set() { return PlasmaSet<T>{pcell, py, pz, ppx, ppy, ppz, pw, pid}; }
+    PlasmaSet<T> alt_set() { return PlasmaSet<T>{acell, ay, az, apx, apy, apz, aw, apid}; }
+    void swap_sets() {
+        std::swap(pcell, acell); std::swap(py, ay); std::swap(pz, az); std::swap(ppx, apx);
+        std::swap(ppy, apy); std::swap(ppz, apz); std::swap(pw, aw); std::swap(pid, apid);
+        grp.flip = !grp.flip;
+    }
+    // a fresh front layer: grouped by cell in load order, counts cleared
+    qs_status cic_fresh_front() {
+        if (!cic_sort || !np) return QS_OK;
+        klaunch(KC_MISC, [&] { return launch_iota(pid, np, st); });
+        CK(cudaMemsetAsync(cic_cnt, 0, plane * sizeof(int), st));
+        grp.grouped = true;
+        grp.off_valid = false;
+        grp.counted = false;
+        return QS_OK;
+    }
+    // make the cell offsets valid for the arrays the next push reads:
+    // regroup after a full push, or count and scan a freshly loaded layer
+    qs_status cic_prepare() {
+        const int ncell = (int)plane;
+        if (!grp.grouped) {
+            klaunch(KC_SORT, [&] {
+                return launch_cell_offsets(cic_cnt, ncell, cic_loff, cic_bsum, cic_bpref, cic_ticket, 0,
+                                           st);
+            });
+            klaunch(KC_SORT, [&] {
+                return launch_scatter<T>(cur_set(), alt_set(), np, cic_cnt, cic_loff, cic_bpref,
+                                         st);
+            });
+            swap_sets();
+            // the scatter rebuilt the arrays in cell order: the offsets hold
+            grp.grouped = true;
+            grp.off_valid = true;
+            grp.counted = false;
+        } else if (!grp.off_valid) {
+            if (!grp.counted)
+                klaunch(KC_SORT, [&] { return launch_count_cells(pcell, np, cic_cnt, st); });
+            klaunch(KC_SORT, [&] {
+                return launch_cell_offsets(cic_cnt, ncell, cic_loff, cic_bsum, cic_bpref, cic_ticket, 1,
+                                           st);
+            });
+            grp.off_valid = true;
+            grp.counted = false;
+        }
+        CK(cudaGetLastError());
+        return QS_OK;
+    }
+
     qs_status ensure_plasma(int64_t n) {
         if (n <= np_cap) return QS_OK;
-        void* old[] = {pcell, py, pz, ppx, ppy, ppz, pw};
+        if (grp.flip) swap_sets();
+        void* old[] = {pcell, py, pz, ppx, ppy, ppz, pw, acell, ay, az, apx, apy, apz, aw, pid,
+                       apid};
         for (void* p : old)
             if (p) cudaFree(p);
+        acell = pid = apid = nullptr;
+        ay = az = apx = apy = apz = aw = nullptr;
         qs_status s;
         if ((s = alloc(&pcell, n, "plasma"))) return s;
         if ((s = alloc(&py, n, "plasma"))) return s;
@@ -376,6 +450,17 @@ struct Engine : EngineBase {
         if ((s = alloc(&ppy, n, "plasma"))) return s;
         if ((s = alloc(&ppz, n, "plasma"))) return s;
         if ((s = alloc(&pw, n, "plasma"))) return s;
+        if (cic_sort) {
+            if ((s = alloc(&acell, n, "plasma"))) return s;
+            if ((s = alloc(&ay, n, "plasma"))) return s;
+            if ((s = alloc(&az, n, "plasma"))) return s;
+            if ((s = alloc(&apx, n, "plasma"))) return s;
+            if ((s = alloc(&apy, n, "plasma"))) return s;
+            if ((s = alloc(&apz, n, "plasma"))) return s;
+            if ((s = alloc(&aw, n, "plasma"))) return s;
+            if ((s = alloc(&pid, n, "plasma"))) return s;
+            if ((s = alloc(&apid, n, "plasma"))) return s;
+        }
         np_cap = n;
         if (gexec) {  // the captured march baked the old pointers
             cudaGraphExecDestroy(gexec);
@@ -456,6 +541,7 @@ struct Engine : EngineBase {
         }
         qs_status s = ensure_plasma(n);
         if (s) return s;
+        if (grp.flip) swap_sets();   // the march graph starts from the first set
         np = n;
         uniform_layout = (n == (int64_t)plane * cfg.ppc);
         for (int64_t p = 0; p < n && uniform_layout; p++)
@@ -475,6 +561,7 @@ struct Engine : EngineBase {
             }
             CK(cudaStreamSynchronize(st));
         }
+        if ((s = cic_fresh_front())) return s;
         front_pending = true;
         return QS_OK;
     }
@@ -484,6 +571,7 @@ struct Engine : EngineBase {
         if (ppc < 1 || ppc > 16) return fail(QS_ERR_INVALID, "ppc must be in [1,16]");
         qs_status s = ensure_plasma((int64_t)plane * ppc);
         if (s) return s;
+        if (grp.flip) swap_sets();   // the march graph starts from the first set
         np = (int64_t)plane * ppc;
         uniform_layout = true;
         // in-cell lattice of Mesh::SeedParticles (mesh.cpp:436-470), head first
@@ -512,6 +600,7 @@ struct Engine : EngineBase {
                                         ppy, ppz, pw, st);
         });
         CK(cudaGetLastError());
+        if ((s = cic_fresh_front())) return s;
         front_pending = true;
         return QS_OK;
     }
@@ -522,6 +611,7 @@ struct Engine : EngineBase {
                          double* py_, double* pz_, double* w) override {
         if (n != np) return fail(QS_ERR_INVALID, "qs_get_plasma: n mismatch");
         if (!n) return QS_OK;
+        if (cic_sort) return get_plasma_by_id(n, cell, y, z, px, py_, pz_, w);
         if (cell) CK(cudaMemcpyAsync(cell, pcell, n * 4, cudaMemcpyDeviceToHost, st));
         double* dst[6] = {y, z, px, py_, pz_, w};
         T* src[6] = {py, pz, ppx, ppy, ppz, pw};
@@ -536,6 +626,32 @@ struct Engine : EngineBase {
             }
         }
         CK(cudaStreamSynchronize(st));
+        return QS_OK;
+    }
+
+    // the regrouped plasma back in load order (each particle carries its id)
+    qs_status get_plasma_by_id(int64_t n, int32_t* cell, double* y, double* z, double* px,
+                               double* py_, double* pz_, double* w) {
+        std::vector<int32_t> id(n), ci(n);
+        CK(cudaMemcpyAsync(id.data(), pid, n * 4, cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(ci.data(), pcell, n * 4, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        if (cell)
+            for (int64_t p = 0; p < n; p++) cell[id[p]] = ci[p];
+        double* dst[6] = {y, z, px, py_, pz_, w};
+        T* src[6] = {py, pz, ppx, ppy, ppz, pw};
+        std::vector<double> tmp(n);
+        for (int c = 0; c < 6; c++) {
+            if (!dst[c]) continue;
+            size_t chunk = 8 * plane;
+            for (int64_t o = 0; o < n; o += (int64_t)chunk) {
+                size_t m = (size_t)std::min<int64_t>((int64_t)chunk, n - o);
+                klaunch(KC_MISC, [&] { return launch_convert_back<T>(src[c] + o, stage_d, m, st); });
+                CK(cudaMemcpyAsync(tmp.data() + o, stage_d, m * 8, cudaMemcpyDeviceToHost, st));
+                CK(cudaStreamSynchronize(st));
+            }
+            for (int64_t p = 0; p < n; p++) dst[c][id[p]] = tmp[p];
+        }
         return QS_OK;
     }
 
@@ -850,6 +966,10 @@ struct Engine : EngineBase {
         // ClearCurrentsSplit: inside the march the preceding spectral kernel
         // already cleared Csrc
         if (!clear_by_maps()) CK(cudaMemsetAsync(Csrc, 0, 4 * plane * sizeof(T), st));
+        if (cic_sort) {
+            qs_status s = cic_prepare();
+            if (s) return s;
+        }
         PushArgs<T> a{};
         a.n = np;
         a.My = My; a.Mz = Mz;
@@ -868,12 +988,24 @@ struct Engine : EngineBase {
         a.hxhy = (T)((cfg.hx / S) / cfg.hy);
         a.hxhz = (T)((cfg.hx / S) / cfg.hz);
         a.invMy = 1.0f / (float)My;
-        a.uniform_ppc = (cfg.shape == QS_SHAPE_NGP && uniform_layout) ? cfg.ppc : 0;
+        // home-cell order of the lattice (the particle arrays are never
+        // reordered; in CIC the current cell may differ from the home cell)
+        a.uniform_ppc = uniform_layout ? cfg.ppc : 0;
         a.full = full;
         a.err = d_err;
+        if (cic_sort) {
+            a.loff = cic_loff;
+            a.bpref = cic_bpref;
+            a.cnt = cic_cnt;
+        }
         const bool precise = sizeof(T) == 4;
         klaunch(KC_PUSH, [&] { return launch_push<T>(a, cfg.shape, precise, st); });
         CK(cudaGetLastError());
+        if (cic_sort && full) {   // particles moved: regroup before the next push
+            grp.grouped = false;
+            grp.off_valid = false;
+            grp.counted = true;
+        }
         return QS_OK;
     }
 
@@ -1002,13 +1134,15 @@ struct Engine : EngineBase {
                 return cuda_fail(e, "march graph instantiate");
             }
             graph_kernels = capture_count;
-            graph_end = HostState{Pf, Cf, Psrc, Csrc, cur};
+            graph_end = HostState{Pf, Cf, Psrc, Csrc, cur, grp};
         }
         CK(cudaGraphLaunch(gexec, st));
         ck_valid = ck_every > 0;
         launches += graph_kernels;
         Pf = graph_end.Pf; Cf = graph_end.Cf; Psrc = graph_end.Psrc; Csrc = graph_end.Csrc;
         cur = graph_end.cur;
+        if (graph_end.grp.flip != grp.flip) swap_sets();
+        grp = graph_end.grp;
         p_valid = true;
         marched = true;
         return QS_OK;

@@ -501,6 +501,223 @@ __global__ void __launch_bounds__(128) push_cell_kernel(PushArgs<float> a) {
     }
 }
 
+// ---------------------------------------------------------------------------
+// FP32 CIC push over particles grouped by cell (the counting sort in sort.cu
+// regroups them after full pushes).  A block owns a tile of 32 x TY cells, one
+// warp per row of 32 cells; the warp pushes the particles of its row 32 at a
+// time (particle-parallel, so dense and empty cells do not unbalance it).
+// The block stages the four corners of each tile cell's fields (P and C
+// averaged) in shared memory for the gather.  Deposits: the warp first sums,
+// over runs of lanes whose particles deposit into the same cell, the 16
+// corner x current values (a 3-level segmented shuffle reduction); one lane
+// per run of up to 8 then adds them to a shared tile of (32+1) x (TY+1)
+// cells; the block flushes the tile with one global atomic per touched cell
+// and current.  Particles outside the tile (moved since the last regrouping)
+// gather and deposit through global memory.  The full push stores the
+// particles in place with their new cell and, when a regrouping follows,
+// counts the new cells.  Same physics as push_kernel<float, CIC, precise,
+// fast> (movepart_layer_CIC.cpp:165-193, 449-496 weights) with approximate
+// reciprocals for the divisions.
+__device__ __forceinline__ int cell_offset(const PushArgs<float>& a, int c) {
+    return a.loff[c] + a.bpref[c >> 10];
+}
+
+template <int TY>
+__global__ void __launch_bounds__(32 * TY) push_cic_warp_kernel(PushArgs<float> a) {
+    constexpr int TX = 32, W = TX + 1, H = TY + 1;
+    __shared__ float Fs[6][4][TY][TX];   // [field][corner][row][col]
+    __shared__ float T[4][H][W];         // deposit tile [current][row][col]
+    const int lane = threadIdx.x & 31, wr = threadIdx.x >> 5;
+    const int My = a.My, Mz = a.Mz;
+    const size_t plane = a.plane;
+    const int tiles_x = My / TX;
+    const int j0 = (blockIdx.x % tiles_x) * TX, k0 = (blockIdx.x / tiles_x) * TY;
+    for (int i = threadIdx.x; i < 4 * H * W; i += 32 * TY) (&T[0][0][0])[i] = 0.f;
+    pdl_wait();
+    {
+        const int j = j0 + lane, k = k0 + wr;
+        const int j1 = wrap_idx(j + 1, My), k1 = wrap_idx(k + 1, Mz);
+        const size_t nn[4] = {(size_t)j + (size_t)My * k, (size_t)j1 + (size_t)My * k,
+                              (size_t)j + (size_t)My * k1, (size_t)j1 + (size_t)My * k1};
+#pragma unroll
+        for (int f = 0; f < 6; f++)
+#pragma unroll
+            for (int r = 0; r < 4; r++)
+                Fs[f][r][wr][lane] =
+                    0.5f * (ld(a.P + f * plane + nn[r]) + ld(a.C + f * plane + nn[r]));
+    }
+    __syncthreads();
+    const int c0 = j0 + My * (k0 + wr);   // this warp's 32 cells: c0 .. c0+31
+    const int pbeg = cell_offset(a, c0);
+    const int pend = (size_t)(c0 + TX) < plane ? cell_offset(a, c0 + TX) : (int)a.n;
+    for (int base = pbeg; base < pend; base += 32) {
+        const int p = base + lane;
+        int key = -1;                     // destination cell of the first sub-step
+        float v[16];
+#pragma unroll
+        for (int i = 0; i < 16; i++) v[i] = 0.f;
+        if (p < pend) {
+            const int cell = a.cell[p];
+            const float yp = a.y[p], zp = a.z[p];
+            if (!(yp >= 0.f && yp <= 1.f && zp >= 0.f && zp <= 1.f)) {
+                atomicOr(a.err, DEV_ERR_RANGE);
+                if (a.full && a.cnt) atomicAdd(a.cnt + cell, 1);   // it stays in its cell
+            } else {
+                int j, k;
+                cell_jk(cell, My, a.invMy, j, k);
+                const float wg[4] = {(1.f - yp) * (1.f - zp), yp * (1.f - zp), (1.f - yp) * zp,
+                                     yp * zp};
+                float g[6];
+                const int tj = j - j0, tk = k - k0;
+                if (tj >= 0 && tj < TX && tk >= 0 && tk < TY) {
+#pragma unroll
+                    for (int f = 0; f < 6; f++)
+                        g[f] = wg[0] * Fs[f][0][tk][tj] + wg[1] * Fs[f][1][tk][tj] +
+                               wg[2] * Fs[f][2][tk][tj] + wg[3] * Fs[f][3][tk][tj];
+                } else {
+                    const int j1 = wrap_idx(j + 1, My), k1 = wrap_idx(k + 1, Mz);
+                    const size_t nn[4] = {(size_t)j + (size_t)My * k, (size_t)j1 + (size_t)My * k,
+                                          (size_t)j + (size_t)My * k1,
+                                          (size_t)j1 + (size_t)My * k1};
+#pragma unroll
+                    for (int f = 0; f < 6; f++) {
+                        float acc = 0.f;
+#pragma unroll
+                        for (int r = 0; r < 4; r++)
+                            acc += wg[r] * 0.5f * (ld(a.P + f * plane + nn[r]) +
+                                                   ld(a.C + f * plane + nn[r]));
+                        g[f] = acc;
+                    }
+                }
+                float px = a.px[p], py = a.py[p], pz = a.pz[p];
+                const float inv_gp = rsqrtf(1.f + px * px + py * py + pz * pz);
+                const float Vxp = px * inv_gp, Vyp = py * inv_gp, Vzp = pz * inv_gp;
+                const float kE = a.sE * __frcp_rn(1.f - Vxp);
+                const float ex = g[0] * kE, ey = g[1] * kE, ez = g[2] * kE;
+                px += ex; py += ey; pz += ez;
+                const float kB = rsqrtf(1.f + px * px + py * py + pz * pz) * kE;
+                const float bx = (g[3] + a.bxe) * kB, by = (g[4] + a.bye) * kB,
+                            bz = (g[5] + a.bze) * kB;
+                const float co = __fdividef(2.f, 1.f + bx * bx + by * by + bz * bz);
+                const float p3x = (py * bz - pz * by + px) * co;
+                const float p3y = (pz * bx - px * bz + py) * co;
+                const float p3z = (px * by - py * bx + pz) * co;
+                px += ex + (p3y * bz - p3z * by);
+                py += ey + (p3z * bx - p3x * bz);
+                pz += ez + (p3x * by - p3y * bx);
+                const float inv_g = rsqrtf(1.f + px * px + py * py + pz * pz);
+                const float Vxm = px * inv_g, Vym = py * inv_g, Vzm = pz * inv_g;
+                const float Vx = 0.5f * (Vxm + Vxp), Vy = 0.5f * (Vym + Vyp),
+                            Vz = 0.5f * (Vzm + Vzp);
+                const float inv2 = __frcp_rn(1.f - Vx);
+                const float wq = a.w[p] * inv2;
+                const float dq[4] = {wq * a.djx0 * Vxm, wq * a.djy0 * Vym, wq * a.djz0 * Vzm,
+                                     wq * a.drho0};
+                const float dy = Vy * a.hxhy * inv2, dz = Vz * a.hxhz * inv2;
+                float partdx = 0.f, step = 1.f;
+                if (fabsf(dy) > 1.f || fabsf(dz) > 1.f)
+                    step = partdx = fmaxf(fabsf(dy), fabsf(dz));
+                if (partdx < 1.f) partdx = step = 1.f;
+                float ytmp = yp, ztmp = zp;
+                int jb = j, kb = k;
+                bool first = true;
+                while (partdx > 0.f) {
+                    float ps;
+                    if (partdx > 1.f) { partdx -= 1.f; ps = __frcp_rn(step); }
+                    else { ps = __fdividef(partdx, step); partdx = 0.f; }
+                    const float uy = ytmp + dy * ps, uz = ztmp + dz * ps;
+                    const float fy = floorf(uy), fz = floorf(uz);
+                    float ry = uy - fy, rz = uz - fz;
+                    int sy = (int)fy, sz = (int)fz;
+                    if (ry >= 1.f) { ry = 0.f; sy += 1; }
+                    if (rz >= 1.f) { rz = 0.f; sz += 1; }
+                    jb = wrap_idx(jb + sy, My);
+                    kb = wrap_idx(kb + sz, Mz);
+                    ytmp = ry;
+                    ztmp = rz;
+                    const float wc[4] = {(1.f - ry) * (1.f - rz), ry * (1.f - rz),
+                                         (1.f - ry) * rz, ry * rz};
+                    if (first) {
+                        key = jb + My * kb;
+#pragma unroll
+                        for (int r = 0; r < 4; r++)
+#pragma unroll
+                            for (int d = 0; d < 4; d++) v[r * 4 + d] = dq[d] * ps * wc[r];
+                        first = false;
+                    } else {
+                        const int jb1 = wrap_idx(jb + 1, My), kb1 = wrap_idx(kb + 1, Mz);
+                        const size_t nd[4] = {(size_t)jb + (size_t)My * kb,
+                                              (size_t)jb1 + (size_t)My * kb,
+                                              (size_t)jb + (size_t)My * kb1,
+                                              (size_t)jb1 + (size_t)My * kb1};
+#pragma unroll
+                        for (int r = 0; r < 4; r++)
+#pragma unroll
+                            for (int d = 0; d < 4; d++)
+                                atomicAdd(a.dep + d * plane + nd[r], dq[d] * ps * wc[r]);
+                    }
+                }
+                if (a.full) {
+                    const int nc = jb + My * kb;
+                    a.y[p] = ytmp; a.z[p] = ztmp; a.px[p] = px; a.py[p] = py; a.pz[p] = pz;
+                    a.cell_out[p] = nc;
+                    if (a.cnt) atomicAdd(a.cnt + nc, 1);
+                }
+            }
+        }
+        // segmented sums over runs of equal destination cell, chunks of <= 8 lanes
+        const unsigned full = 0xffffffffu;
+        const int prevKey = __shfl_up_sync(full, key, 1);
+        const bool start = (lane == 0) || (prevKey != key);
+        const unsigned starts = __ballot_sync(full, start);
+        const int rs = 31 - __clz(starts & (0xffffffffu >> (31 - lane)));   // run start
+        const unsigned after = starts & ~(0xffffffffu >> (31 - lane));       // starts > lane
+        const int re = after ? __ffs(after) - 2 : 31;                        // run end
+#pragma unroll
+        for (int d = 1; d <= 4; d <<= 1) {
+#pragma unroll
+            for (int i = 0; i < 16; i++) {
+                const float o = __shfl_down_sync(full, v[i], d);
+                if (lane + d <= re && ((lane - rs) & (2 * d - 1)) == 0) v[i] += o;
+            }
+        }
+        if (key >= 0 && ((lane - rs) & 7) == 0) {
+            int kj, kk;
+            cell_jk(key, My, a.invMy, kj, kk);
+            const int tj = kj - j0, tk = kk - k0;
+            if (tj >= 0 && tj < TX && tk >= 0 && tk < TY) {
+#pragma unroll
+                for (int d = 0; d < 4; d++) {
+                    atomicAdd(&T[d][tk][tj], v[0 * 4 + d]);
+                    atomicAdd(&T[d][tk][tj + 1], v[1 * 4 + d]);
+                    atomicAdd(&T[d][tk + 1][tj], v[2 * 4 + d]);
+                    atomicAdd(&T[d][tk + 1][tj + 1], v[3 * 4 + d]);
+                }
+            } else {
+                const int kj1 = wrap_idx(kj + 1, My), kk1 = wrap_idx(kk + 1, Mz);
+                const size_t nd[4] = {(size_t)kj + (size_t)My * kk, (size_t)kj1 + (size_t)My * kk,
+                                      (size_t)kj + (size_t)My * kk1,
+                                      (size_t)kj1 + (size_t)My * kk1};
+#pragma unroll
+                for (int r = 0; r < 4; r++)
+#pragma unroll
+                    for (int d = 0; d < 4; d++) atomicAdd(a.dep + d * plane + nd[r], v[r * 4 + d]);
+            }
+        }
+    }
+    pdl_trigger();
+    __syncthreads();
+    for (int i = threadIdx.x; i < H * W; i += 32 * TY) {
+        const int r = i / W, cc = i - r * W;
+        const size_t m = (size_t)wrap_idx(j0 + cc, My) + (size_t)My * wrap_idx(k0 + r, Mz);
+#pragma unroll
+        for (int d = 0; d < 4; d++) {
+            const float x = T[d][r][cc];
+            if (x != 0.f) atomicAdd(a.dep + d * plane + m, x);
+        }
+    }
+}
+
 template <class T>
 int launch_push(const PushArgs<T>& a, int shape, bool precise, cudaStream_t st) {
     if (a.n <= 0) return 0;
@@ -520,6 +737,14 @@ int launch_push(const PushArgs<T>& a, int shape, bool precise, cudaStream_t st) 
             else push_kernel<T, QS_SHAPE_NGP, false, false><<<blocks, threads, 0, st>>>(a);
         }
     } else {
+        if constexpr (F32) {
+            constexpr int TY = 4;
+            if (a.loff && !a.dep_cell) {   // grouped by cell with offsets (the engine checks the shape)
+                launch_pdl(push_cic_warp_kernel<TY>, dim3((a.My / 32) * (a.Mz / TY)),
+                           dim3(32 * TY), 0, st, a);
+                return 1;
+            }
+        }
         push_kernel<T, QS_SHAPE_CIC, true, F32><<<blocks, threads, 0, st>>>(a);
     }
     return 1;

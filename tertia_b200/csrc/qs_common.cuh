@@ -65,6 +65,12 @@ struct PushArgs {
     T sE, hxhy, hxhz;     // q2m*hx/2, hx/hy, hx/hz (factored FP32 form)
     float invMy;          // 1/My for the cell index split
     int uniform_ppc;      // >0: particle p sits in cell p / uniform_ppc (lattice layout)
+    // FP32 CIC over particles grouped by cell: cell c holds particles
+    // loff[c] + bpref[c / 1024] .. (next cell's offset) - 1; the full push
+    // counts the new cells into cnt
+    const int* loff;
+    const int* bpref;
+    int* cnt;
     int full;
     int* err;
 };

@@ -75,7 +75,7 @@ int run_dtt_simt_pass(int pass, const DttJob<T>& job, int ny, int nz, const DttM
 // kernel classes of the per-kernel timing (qs_profile_read)
 enum KernelClass {
     KC_PUSH = 0, KC_GEMM = 1, KC_SPLIT = 2, KC_SPECTRAL = 3, KC_BEAM_SPECTRA = 4,
-    KC_BEAM_PUSH = 5, KC_SEED = 6, KC_MISC = 7, KC_N = 8
+    KC_BEAM_PUSH = 5, KC_SEED = 6, KC_MISC = 7, KC_SORT = 8, KC_N = 9
 };
 
 template <class T>
@@ -99,6 +99,22 @@ struct BeamArgs {
 };
 template <class T>
 int launch_beam_push(const BeamArgs<T>& a, cudaStream_t st);
+
+// ---- grouping the plasma by cell (sort.cu)
+template <class T>
+struct PlasmaSet {
+    int32_t* cell;
+    T *y, *z, *px, *py, *pz, *w;
+    int32_t* id;
+};
+int scan_blocks_count(int ncell);
+int launch_count_cells(const int32_t* cell, int64_t n, int* cnt, cudaStream_t st);
+int launch_cell_offsets(int* cnt, int ncell, int* loff, int* bsum, int* bpref,
+                        unsigned* ticket, int clear, cudaStream_t st);
+template <class T>
+int launch_scatter(const PlasmaSet<T>& in, const PlasmaSet<T>& out, int64_t n, int* cnt,
+                   const int* loff, const int* bpref, cudaStream_t st);
+int launch_iota(int32_t* id, int64_t n, cudaStream_t st);
 
 // ---- adjoint (adjoint.cu)
 

@@ -57,13 +57,20 @@ def test_two_steps_beam_phase_space(oracle_lib, prec):
     assert rel_l2(m.onaxis_ex(), o.onaxis_ex()) < TOL[prec]
 
 
-def test_cic_step_matches_oracle(oracle_lib):
-    cfg = cfg_for("fp64", n=32, layers=32, shape=QS_SHAPE_CIC)
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+def test_cic_step_matches_oracle(oracle_lib, prec):
+    """CIC march (FP32: the one-thread-per-home-cell tile kernel, particles
+    moving between cells) against the FP64 oracle."""
+    cfg = cfg_for(prec, n=32, layers=32, shape=QS_SHAPE_CIC)
     beam = wl.small_beam(cfg, n=4000)
     o, m = run_pair(oracle_lib, cfg, beam, [wl.front_plasma(cfg, seed=3)])
-    assert rel_l2(m.onaxis_ex(), o.onaxis_ex()) < 1e-10
+    assert rel_l2(m.onaxis_ex(), o.onaxis_ex()) < (1e-10 if prec == "fp64" else 5e-4)
     po, pm = o.get_plasma(), m.get_plasma()
-    assert np.array_equal(pm["cell"], po["cell"])
+    if prec == "fp64":
+        assert np.array_equal(pm["cell"], po["cell"])
+    else:
+        assert np.mean(pm["cell"] == po["cell"]) > 0.999
+        assert np.any(po["cell"] != wl.front_plasma(cfg, seed=3)["cell"])   # particles moved
 
 
 def test_fine_grained_sequence_matches_march(oracle_lib):

@@ -57,19 +57,23 @@ def test_push_fp64_bitexact(oracle_lib, shape, full):
 def thinned(p):
     """The lattice with every seventh particle removed (cells stay grouped in
     ascending order, but not PPC to a cell): the NGP push then takes the
-    one-thread-per-particle kernel instead of the one-thread-per-cell kernel
-    of the full lattice."""
+    one-thread-per-particle kernels instead of the one-thread-per-cell
+    kernels of the full lattice."""
     keep = np.arange(len(p["y"])) % 7 != 3
     return {k: np.asarray(v)[keep] for k, v in p.items()}
 
 
-@pytest.mark.parametrize("shape,layout", [(QS_SHAPE_NGP, "lattice"), (QS_SHAPE_NGP, "thinned"),
-                                          (QS_SHAPE_CIC, "lattice")])
-def test_push_fp32_matches_float_oracle(oracle_lib, shape, layout):
+@pytest.mark.parametrize("shape,layout,n", [(QS_SHAPE_NGP, "lattice", 32),
+                                            (QS_SHAPE_NGP, "thinned", 32),
+                                            (QS_SHAPE_CIC, "lattice", 32),
+                                            (QS_SHAPE_CIC, "thinned", 32),
+                                            (QS_SHAPE_CIC, "lattice", 40)])
+def test_push_fp32_matches_float_oracle(oracle_lib, shape, layout, n):
     """The FP32 kernels factor the divisions and contract to FMA, so they
     match the oracle's float restatement to FP32 rounding; the deposit cells
-    (where a particle's current lands) agree exactly."""
-    cfg = cfg_for("fp32", n=32, layers=4, shape=shape)
+    (where a particle's current lands) agree exactly.  CIC grids whose ny is
+    not a multiple of 32 take the one-thread-per-particle CIC kernel."""
+    cfg = cfg_for("fp32", n=n, layers=4, shape=shape)
     p, P, C = state(cfg, 21 + shape)
     if layout == "thinned":
         p = thinned(p)
