@@ -7,12 +7,12 @@ driver-beam push + 3-D CIC deposit, then the full xi-march over every layer
 One particle-layer push = one plasma macro-particle carried across one
 xi-layer (all nIter+1 sub-pushes counted once): Np * layers per step.
 
-Default workload (N=1): c1, 512 x 512 transverse cells, 1024 layers, 4 ppc
+Default workload (N=1): c1 with CIC deposit, 512 x 512 transverse cells, 1024 layers, 4 ppc
 (1,048,576 plasma particles per layer), thermal sigma_p = 0.01, 1e6 driver
 particles, synthetic seeded inputs.  The field store (6.4 GB) and beam-current
 store (2.1 GB) are far larger than L2, so every step streams from HBM.
 
-  python bench.py [--gpus N --steps K --warmup W --precision tf32x3]
+  python bench.py [--gpus N --steps K --warmup W --precision bf16x3 --shape cic]
   python bench.py --impl reference     # the reference's CPU path (oracle port)
 
 Under torchrun (N>1) every rank runs an independent replica: the march is
@@ -37,7 +37,7 @@ if ROOT not in sys.path:
 METRIC = "particle-layer pushes/s"
 UNIT = "pushes/s"
 CLASSES = ["push_deposit", "transform_gemm", "transform_split", "spectral_maps",
-           "beam_spectra", "beam_push", "front_seed", "other"]
+           "beam_spectra", "beam_push", "front_seed", "other", "plasma_regroup"]
 
 
 def parse():
@@ -47,7 +47,13 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="c1")
-    ap.add_argument("--precision", default="tf32x3")
+    ap.add_argument("--precision", default="bf16x3")
+    ap.add_argument("--shape", default="cic", choices=["cic", "ngp"],
+                    help="plasma particle shape: CIC deposit (default) or the reference's "
+                         "live NGP path")
+    ap.add_argument("--layers", type=int, default=0,
+                    help="profiling case: the workload's grid with this many layers and a "
+                         "weak 1e5-particle beam (not a bench line)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64-plain comparison")
     ap.add_argument("--cpu-seconds", type=float, default=12.0,
@@ -177,7 +183,7 @@ def run_ours(args):
     import numpy as np
     import torch
     from tertia_b200 import workload as wl
-    from tertia_b200.abi import PRECISIONS
+    from tertia_b200.abi import PRECISIONS, QS_SHAPE_CIC, QS_SHAPE_NGP
     from tertia_b200.mesh import Mesh
 
     rank, world, local = dist_env()
@@ -189,9 +195,17 @@ def run_ours(args):
                                 device_id=torch.device("cuda", local))
     w = wl.make_workload(args.workload, args.precision)
     cfg = w.cfg
+    cfg.shape = QS_SHAPE_CIC if args.shape == "cic" else QS_SHAPE_NGP
     cfg.device = local
     cfg.seed = 12345 + rank
-    beam = wl.workload_beam(w)
+    if args.layers:
+        cfg.nx = args.layers
+        w.name = f"{w.name}-L{args.layers}"
+        w.description = (f"profiling case: {cfg.ny}x{cfg.nz} grid of {args.workload}, "
+                         f"{args.layers} layers, 1e5-particle beam at n_b/n_0 = 1e-4")
+        beam = wl.sample_beam(cfg, wl.BeamSpec(100_000, nb_over_n0=1e-4))
+    else:
+        beam = wl.workload_beam(w)
     npl = cfg.ny * cfg.nz * cfg.ppc
     pushes_per_step = npl * cfg.nx * cfg.nx_split
 
@@ -263,24 +277,72 @@ def run_ours(args):
     h2d = n * (3 * 4 + 7 * 8)
     d2h = n * (3 * 4 + 6 * 8) + cfg.nx * 8
 
-    # ---------------- per-kernel timing over one more step (events per launch)
+    # ---------------- per-class kernel time over one more step: eager launches,
+    # an event pair around every launch (host launch gaps are included, so
+    # short kernels read long; the shares are cross-checked with ncu)
     m.profile_enable(True)
     torch.cuda.synchronize()
     m.step()
     prof = m.profile_read()
     m.profile_enable(False)
+
+    # ---------------- the dominant kernel timed back to back: the inverse E,B
+    # transform pass of the march (6 planes, one y- or z-pass per launch),
+    # repeated with the launches queued ahead of the GPU
+    gemm = None
+    if args.precision in ("bf16x3", "tf32x3", "bf16x6"):
+        nf = 6
+        xs = torch.randn(nf, cfg.nz, cfg.ny, device="cuda", dtype=torch.float32)
+        ys = torch.empty_like(xs)
+        for _ in range(3):
+            m.transform2d_dev(0, 1, nf, xs.data_ptr(), ys.data_ptr())
+        m.sync()
+        reps = 200
+        ev0.record(stream)
+        for _ in range(reps):
+            m.transform2d_dev(0, 1, nf, xs.data_ptr(), ys.data_ptr())
+        ev1.record(stream)
+        m.sync()
+        loop_ms = ev0.elapsed_time(ev1)
+        m.profile_enable(True)
+        for _ in range(reps):
+            m.transform2d_dev(0, 1, nf, xs.data_ptr(), ys.data_ptr())
+        m.sync()
+        p2 = m.profile_read()
+        m.profile_enable(False)
+        g_ms, g_n = p2["transform_gemm"]
+        s_ms, _ = p2["transform_split"]
+        # the back-to-back loop (no events between launches) gives the time of
+        # one transform = split + 2 passes; the evented run gives the passes'
+        # share of it (its per-launch times include launch gaps)
+        share = g_ms / max(g_ms + s_ms, 1e-12)
+        loop_us = loop_ms * 1e3 / reps
+        gemm = {"planes": nf, "launches_per_transform": 2,
+                "avg_launch_us": loop_us * share / 2.0,
+                "loop_us_per_transform": loop_us, "pass_share_evented": share,
+                "evented_avg_launch_us": g_ms * 1e3 / max(g_n, 1)}
+        del xs, ys
     m.close()
 
-    # ---------------- FP64 plain path on the same inputs: speed and Ez error
+    # ---------------- FP64 plain path on the same inputs: speed and Ez error.
+    # The FP64 path is also run against itself with the beam weights scaled by
+    # (1 + eps): eps = 1e-15 shows the march's response to a last-bit change,
+    # eps = 6e-8 (FP32 rounding scale) the floor that any FP32 computation of
+    # this box faces.  The head quarter of the box is reported separately.
     fp64 = None
     if not args.no_fp64:
         c64 = cfg.copy()
         c64.precision = PRECISIONS["fp64"]
         c32 = cfg.copy()
         ref = {}
-        for tag, c in (("fp64", c64), ("ours", c32)):
+        runs = [("fp64", c64, beam), ("ours", c32, beam)]
+        for tag, eps in (("fp64_pert15", 1e-15), ("fp64_pert7", 6e-8)):
+            bp = dict(beam)
+            bp["w"] = np.asarray(beam["w"]) * (1.0 + eps)
+            runs.append((tag, c64, bp))
+        for tag, c, b in runs:
             mm = Mesh(c)
-            mm.load_beam(beam)
+            mm.load_beam(b)
             mm.step()                   # identical first step from identical inputs
             torch.cuda.synchronize()
             t0 = time.perf_counter()
@@ -289,45 +351,47 @@ def run_ours(args):
             ref[tag] = (mm.onaxis_ex(), time.perf_counter() - t0)
             mm.close()
         e64, t64 = ref["fp64"]
-        eo, _ = ref["ours"]
-        err = float(np.linalg.norm(eo - e64) / np.linalg.norm(e64))
+        rel = lambda a, b: float(np.linalg.norm(a - b) / np.linalg.norm(b))
+        head = slice(3 * cfg.nx // 4, None)    # the head of the box: the highest layers
         fp64 = {"value": pushes_per_step / t64, "unit": UNIT, "ms_per_step": t64 * 1e3,
-                "ez_rel_l2_vs_fp64": err,
-                "speedup": (pushes_per_step / (ms / 1e3)) / (pushes_per_step / t64)}
+                "speedup": (pushes_per_step / (ms / 1e3)) / (pushes_per_step / t64),
+                "ez_rel_l2_vs_fp64": rel(ref["ours"][0], e64),
+                "ez_rel_l2_vs_fp64_head_quarter": rel(ref["ours"][0][head], e64[head]),
+                "ez_rel_l2_fp64_perturbed_1e-15": rel(ref["fp64_pert15"][0], e64),
+                "ez_rel_l2_fp64_perturbed_6e-8": rel(ref["fp64_pert7"][0], e64),
+                "ez_note": "on-axis Ex (the reference's longitudinal field) over all layers "
+                           "after 2 beam steps; perturbed = the FP64 path against itself with "
+                           "the beam weights x (1 + eps)"}
 
     # ---------------- roofline of the dominant kernel
     hbm, bf16, bf16_sus, src = peaks()
     dom = max(prof, key=lambda k: prof[k][0])
-    dom_ms, dom_n = prof[dom]
     L, N, S, nit = cfg.nx, cfg.ny, cfg.nx_split, cfg.n_iter
-    if dom == "transform_gemm":
-        # algorithmic flops: 4 N^3 per 2-D transform (two K=N passes of 2 N^3),
-        # transforms per (layer, split): 2 + 6 + (nIter+1)*3 + nIter*6 + 7
-        per_layer = 2 + 6 + (nit + 1) * 3 + nit * 6 + 7
-        flops = 4.0 * cfg.ny * cfg.nz * (cfg.ny + cfg.nz) / 2.0 * per_layer * L * S
-        achieved = flops / (dom_ms / 1e3) / 1e12
-        roof = {"bound": "tensor", "achieved": achieved, "peak": bf16_sus, "unit": "TFLOP/s",
-                "frac": achieved / bf16_sus,
-                "peak_source": f"bf16_tflops_sustained of {src}",
-                "flops_per_launch": flops / max(dom_n, 1),
-                "executed_flop_multiplier": {"bf16x3": 3, "tf32x3": 6, "bf16x6": 6}.get(
-                    args.precision, 1)}
-    elif dom == "push_deposit":
-        # 44 B/particle for a half sub-push, 64 B for the full one (FP32 SoA)
-        b_half, b_full = 44.0, 64.0
-        nbytes = npl * (nit * b_half + b_full) * L * S
-        achieved = nbytes / (dom_ms / 1e3) / 1e9
-        roof = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                "frac": achieved / hbm, "peak_source": f"hbm_gbs of {src}",
-                "bytes_per_launch": nbytes / max(dom_n, 1)}
+    if gemm:
+        # one launch = one K = N pass over 6 N x N planes: 6 * 2 N^3 algorithmic
+        # flops (the split products, 3x or 6x that, are executed work)
+        flops_launch = gemm["planes"] * 2.0 * cfg.ny * cfg.nz * cfg.ny
+        achieved = flops_launch / (gemm["avg_launch_us"] / 1e6) / 1e12
+        roof = {"bound": "tensor", "achieved": achieved, "peak": bf16, "unit": "TFLOP/s",
+                "frac": achieved / bf16, "peak_source": f"bf16_tflops (burst) of {src}",
+                "kernel": "dtt_tc_kernel (transform pass, 6 planes)",
+                "flops_per_launch": flops_launch, "avg_launch_us": gemm["avg_launch_us"],
+                "executed_flop_multiplier": {"bf16x3": 3, "tf32x3": 3, "bf16x6": 6}[
+                    args.precision],
+                "timing": gemm}
+        # transforms per (layer, split) in the march: 6 (Guess inverse E, B)
+        # + (nIter+1) * (3 forward J + 6 inverse E, B) + 2 beam planes
+        roof["march_transforms_per_layer"] = 6 + (nit + 1) * 9 + 2
     else:
-        roof = {"bound": "hbm", "achieved": None, "peak": hbm, "unit": "GB/s", "frac": None}
-    roof["kernel"] = dom
-    roof["avg_launch_us"] = dom_ms * 1e3 / max(dom_n, 1)
-    tr = traffic_record(dom, args.workload, args.precision)
+        roof = {"bound": "hbm", "achieved": None, "peak": hbm, "unit": "GB/s", "frac": None,
+                "kernel": dom}
+    tr = traffic_record("dtt_tc_kernel" if gemm else dom, args.workload, args.precision)
     roof["traffic"] = tr.get("bytes_per_launch") if tr else None
-    roof["kernel_ms_per_step"] = {k: round(v[0], 3) for k, v in prof.items()}
+    if tr:
+        roof["traffic_source"] = tr.get("source")
+    roof["evented_kernel_ms_per_step"] = {k: round(v[0], 3) for k, v in prof.items()}
     roof["kernel_launches_per_step"] = {k: v[1] for k, v in prof.items()}
+    roof["dominant_class_evented"] = dom
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -342,7 +406,7 @@ def run_ours(args):
             "config": {"workload": f"{w.name}: {w.description}", "ny": cfg.ny, "nz": cfg.nz,
                        "layers": cfg.nx, "ppc": cfg.ppc, "plasma_particles_per_layer": npl,
                        "beam_particles": n, "n_iter": cfg.n_iter, "nx_split": cfg.nx_split,
-                       "precision": args.precision, "shape": "ngp",
+                       "precision": args.precision, "shape": args.shape,
                        "step": "one beam step: beam push + full xi-march",
                        "l2": "inputs larger than L2 (field store 6.4 GB, beam currents 2.1 GB)",
                        "parallelism": f"replicas x{world}"},
@@ -368,7 +432,9 @@ def run_reference(args):
     if rank != 0:
         return
     from tertia_b200 import workload as wl
+    from tertia_b200.abi import QS_SHAPE_CIC, QS_SHAPE_NGP
     w = wl.make_workload(args.workload)
+    w.cfg.shape = QS_SHAPE_CIC if args.shape == "cic" else QS_SHAPE_NGP
     per_step = max(1.0, min(6.0, 150.0 / max(1, args.steps + args.warmup)))
     for _ in range(args.warmup):
         cpu_sample(w, per_step)
@@ -382,12 +448,15 @@ def run_reference(args):
     cpu["value"] = value
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True,
+        "warmup": args.warmup,
+        "ms_per_step": w.cfg.ny * w.cfg.nz * w.cfg.ppc * w.cfg.nx * w.cfg.nx_split / value * 1e3,
+        "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "impl": "reference",
         "config": {"workload": f"{w.name}: {w.description}", "ny": w.cfg.ny, "nz": w.cfg.nz,
-                   "layers": w.cfg.nx, "ppc": w.cfg.ppc,
-                   "sampled": "each step times a bounded sample of layers of this workload",
+                   "layers": w.cfg.nx, "ppc": w.cfg.ppc, "shape": args.shape,
+                   "sampled": "each step times a bounded sample of layers of this workload; "
+                              "ms_per_step is extrapolated to the full march",
                    "parallelism": "host threads"},
         "cpu_baseline": cpu,
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
