@@ -221,7 +221,14 @@ struct Engine : EngineBase {
     T *ay = nullptr, *az = nullptr, *apx = nullptr, *apy = nullptr, *apz = nullptr, *aw = nullptr;
     int *cic_cnt = nullptr, *cic_loff = nullptr, *cic_bsum = nullptr, *cic_bpref = nullptr;
     unsigned* cic_ticket = nullptr;
-    struct Grouping { bool grouped = true, off_valid = false, counted = false, flip = false; } grp;
+    struct Grouping {
+        bool grouped = true, off_valid = false, counted = false, flip = false;
+        int since = 0;   // full pushes since the last regrouping
+    } grp;
+    // regroup after every cic_every-th full push (particles drift about 1% of
+    // a cell per layer, so the push's global-memory fallback for the few that
+    // left their row stays cheap in between); QS_CIC_REGROUP overrides
+    int cic_every = getenv("QS_CIC_REGROUP") ? std::max(1, atoi(getenv("QS_CIC_REGROUP"))) : 2;
     // programmatic dependent launch inside the march (QS_PDL=0 turns it off)
     bool use_pdl = !(getenv("QS_PDL") && getenv("QS_PDL")[0] == '0');
     bool uniform_layout = false;   // particle p in cell p / ppc (lattice seeding)
@@ -399,6 +406,7 @@ struct Engine : EngineBase {
         grp.grouped = true;
         grp.off_valid = false;
         grp.counted = false;
+        grp.since = 0;
         return QS_OK;
     }
     // make the cell offsets valid for the arrays the next push reads:
@@ -988,23 +996,31 @@ struct Engine : EngineBase {
         a.hxhy = (T)((cfg.hx / S) / cfg.hy);
         a.hxhz = (T)((cfg.hx / S) / cfg.hz);
         a.invMy = 1.0f / (float)My;
-        // home-cell order of the lattice (the particle arrays are never
-        // reordered; in CIC the current cell may differ from the home cell)
+        // lattice order (particle p seeded in cell p / ppc): the NGP
+        // one-thread-per-cell kernel relies on it
         a.uniform_ppc = uniform_layout ? cfg.ppc : 0;
         a.full = full;
         a.err = d_err;
+        a.skip_dens = clear_by_maps() ? 1 : 0;   // the march never reads the density deposit
+        bool regroup = false;
         if (cic_sort) {
             a.loff = cic_loff;
             a.bpref = cic_bpref;
-            a.cnt = cic_cnt;
+            regroup = full && grp.since + 1 >= cic_every;
+            a.cnt = regroup ? cic_cnt : nullptr;   // the full push builds the histogram
         }
         const bool precise = sizeof(T) == 4;
         klaunch(KC_PUSH, [&] { return launch_push<T>(a, cfg.shape, precise, st); });
         CK(cudaGetLastError());
-        if (cic_sort && full) {   // particles moved: regroup before the next push
-            grp.grouped = false;
-            grp.off_valid = false;
-            grp.counted = true;
+        if (cic_sort && full) {
+            if (regroup) {   // regroup before the next push
+                grp.grouped = false;
+                grp.off_valid = false;
+                grp.counted = true;
+                grp.since = 0;
+            } else {
+                grp.since++;
+            }
         }
         return QS_OK;
     }

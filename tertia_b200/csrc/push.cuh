@@ -503,36 +503,44 @@ __global__ void __launch_bounds__(128) push_cell_kernel(PushArgs<float> a) {
 
 // ---------------------------------------------------------------------------
 // FP32 CIC push over particles grouped by cell (the counting sort in sort.cu
-// regroups them after full pushes).  A block owns a tile of 32 x TY cells, one
-// warp per row of 32 cells; the warp pushes the particles of its row 32 at a
-// time (particle-parallel, so dense and empty cells do not unbalance it).
-// The block stages the four corners of each tile cell's fields (P and C
-// averaged) in shared memory for the gather.  Deposits: the warp first sums,
-// over runs of lanes whose particles deposit into the same cell, the 16
-// corner x current values (a 3-level segmented shuffle reduction); one lane
-// per run of up to 8 then adds them to a shared tile of (32+1) x (TY+1)
-// cells; the block flushes the tile with one global atomic per touched cell
-// and current.  Particles outside the tile (moved since the last regrouping)
-// gather and deposit through global memory.  The full push stores the
-// particles in place with their new cell and, when a regrouping follows,
-// counts the new cells.  Same physics as push_kernel<float, CIC, precise,
-// fast> (movepart_layer_CIC.cpp:165-193, 449-496 weights) with approximate
-// reciprocals for the divisions.
+// regroups them every few full pushes).  A block owns a tile of 32 x TY
+// cells, one warp per row of 32 cells; the warp pushes the particles of its
+// row 32 at a time (particle-parallel, so dense and empty cells do not
+// unbalance it).  The block stages the four corners of each tile cell's
+// fields (P and C averaged) in shared memory for the gather.  Deposits: the
+// warp sums the ND x 4 corner values over runs of lanes whose particles
+// deposit into the same cell (3-level segmented shuffle reduction, chunks of
+// up to 8 lanes), merges chunks that share a cell (match), and one lane per
+// cell adds them to the warp's per-cell accumulator in shared memory - no
+// shared-memory atomics.  At the end each lane spreads its cell's corner
+// values (the right-hand corners through a shuffle to the next lane), the
+// warps combine their rows in the block tile in two ordered phases, and the
+// tile is flushed with one global atomic per touched cell and current.
+// Particles whose cell or deposit lies outside the warp's row (moved since
+// the last regrouping) gather and deposit through global memory.  ND = 3
+// leaves out the density deposit, which the march does not read.  The full
+// push stores the particles in place with their new cell and, when a
+// regrouping follows, counts the new cells.  Same physics as
+// push_kernel<float, CIC, precise, fast> (movepart_layer_CIC.cpp:165-193,
+// 449-496 weights) with approximate reciprocals for the divisions.
 __device__ __forceinline__ int cell_offset(const PushArgs<float>& a, int c) {
     return a.loff[c] + a.bpref[c >> 10];
 }
 
-template <int TY>
+template <int TY, int ND>
 __global__ void __launch_bounds__(32 * TY) push_cic_warp_kernel(PushArgs<float> a) {
-    constexpr int TX = 32, W = TX + 1, H = TY + 1;
+    constexpr int TX = 32, W = TX + 1, H = TY + 1, NV = 4 * ND;
     __shared__ float Fs[6][4][TY][TX];   // [field][corner][row][col]
-    __shared__ float T[4][H][W];         // deposit tile [current][row][col]
+    __shared__ float Acc[TY][NV][TX];    // per-warp sums [corner*ND + current][cell]
+    __shared__ float T[ND][H][W];        // block deposit tile [current][row][col]
     const int lane = threadIdx.x & 31, wr = threadIdx.x >> 5;
     const int My = a.My, Mz = a.Mz;
     const size_t plane = a.plane;
     const int tiles_x = My / TX;
     const int j0 = (blockIdx.x % tiles_x) * TX, k0 = (blockIdx.x / tiles_x) * TY;
-    for (int i = threadIdx.x; i < 4 * H * W; i += 32 * TY) (&T[0][0][0])[i] = 0.f;
+    for (int i = threadIdx.x; i < ND * H * W; i += 32 * TY) (&T[0][0][0])[i] = 0.f;
+#pragma unroll
+    for (int i = 0; i < NV; i++) Acc[wr][i][lane] = 0.f;
     pdl_wait();
     {
         const int j = j0 + lane, k = k0 + wr;
@@ -547,15 +555,16 @@ __global__ void __launch_bounds__(32 * TY) push_cic_warp_kernel(PushArgs<float> 
                     0.5f * (ld(a.P + f * plane + nn[r]) + ld(a.C + f * plane + nn[r]));
     }
     __syncthreads();
+    const unsigned full = 0xffffffffu;
     const int c0 = j0 + My * (k0 + wr);   // this warp's 32 cells: c0 .. c0+31
     const int pbeg = cell_offset(a, c0);
     const int pend = (size_t)(c0 + TX) < plane ? cell_offset(a, c0 + TX) : (int)a.n;
     for (int base = pbeg; base < pend; base += 32) {
         const int p = base + lane;
         int key = -1;                     // destination cell of the first sub-step
-        float v[16];
+        float v[NV];
 #pragma unroll
-        for (int i = 0; i < 16; i++) v[i] = 0.f;
+        for (int i = 0; i < NV; i++) v[i] = 0.f;
         if (p < pend) {
             const int cell = a.cell[p];
             const float yp = a.y[p], zp = a.z[p];
@@ -642,7 +651,7 @@ __global__ void __launch_bounds__(32 * TY) push_cic_warp_kernel(PushArgs<float> 
 #pragma unroll
                         for (int r = 0; r < 4; r++)
 #pragma unroll
-                            for (int d = 0; d < 4; d++) v[r * 4 + d] = dq[d] * ps * wc[r];
+                            for (int d = 0; d < ND; d++) v[r * ND + d] = dq[d] * ps * wc[r];
                         first = false;
                     } else {
                         const int jb1 = wrap_idx(jb + 1, My), kb1 = wrap_idx(kb + 1, Mz);
@@ -653,7 +662,7 @@ __global__ void __launch_bounds__(32 * TY) push_cic_warp_kernel(PushArgs<float> 
 #pragma unroll
                         for (int r = 0; r < 4; r++)
 #pragma unroll
-                            for (int d = 0; d < 4; d++)
+                            for (int d = 0; d < ND; d++)
                                 atomicAdd(a.dep + d * plane + nd[r], dq[d] * ps * wc[r]);
                     }
                 }
@@ -666,7 +675,6 @@ __global__ void __launch_bounds__(32 * TY) push_cic_warp_kernel(PushArgs<float> 
             }
         }
         // segmented sums over runs of equal destination cell, chunks of <= 8 lanes
-        const unsigned full = 0xffffffffu;
         const int prevKey = __shfl_up_sync(full, key, 1);
         const bool start = (lane == 0) || (prevKey != key);
         const unsigned starts = __ballot_sync(full, start);
@@ -676,42 +684,78 @@ __global__ void __launch_bounds__(32 * TY) push_cic_warp_kernel(PushArgs<float> 
 #pragma unroll
         for (int d = 1; d <= 4; d <<= 1) {
 #pragma unroll
-            for (int i = 0; i < 16; i++) {
+            for (int i = 0; i < NV; i++) {
                 const float o = __shfl_down_sync(full, v[i], d);
                 if (lane + d <= re && ((lane - rs) & (2 * d - 1)) == 0) v[i] += o;
             }
         }
-        if (key >= 0 && ((lane - rs) & 7) == 0) {
+        const bool head = key >= 0 && ((lane - rs) & 7) == 0;
+        const int dd = key - c0;
+        const bool local = head && dd >= 0 && dd < TX;
+        const unsigned lmask = __ballot_sync(full, local);
+        if (local) {
+            // chunks of the same cell (long runs, or runs split by a moved
+            // particle) are merged into their first lane before the store
+            const unsigned peers = __match_any_sync(lmask, key);
+            const int leader = __ffs(peers) - 1;
+            unsigned rest = peers & (peers - 1);
+            while (rest) {
+                const int src = __ffs(rest) - 1;
+                rest &= rest - 1;
+#pragma unroll
+                for (int i = 0; i < NV; i++) {
+                    const float o = __shfl_sync(peers, v[i], src);
+                    if (lane == leader) v[i] += o;
+                }
+            }
+            if (lane == leader) {
+#pragma unroll
+                for (int i = 0; i < NV; i++) Acc[wr][i][dd] += v[i];
+            }
+        } else if (head) {
             int kj, kk;
             cell_jk(key, My, a.invMy, kj, kk);
-            const int tj = kj - j0, tk = kk - k0;
-            if (tj >= 0 && tj < TX && tk >= 0 && tk < TY) {
+            const int kj1 = wrap_idx(kj + 1, My), kk1 = wrap_idx(kk + 1, Mz);
+            const size_t nd[4] = {(size_t)kj + (size_t)My * kk, (size_t)kj1 + (size_t)My * kk,
+                                  (size_t)kj + (size_t)My * kk1, (size_t)kj1 + (size_t)My * kk1};
 #pragma unroll
-                for (int d = 0; d < 4; d++) {
-                    atomicAdd(&T[d][tk][tj], v[0 * 4 + d]);
-                    atomicAdd(&T[d][tk][tj + 1], v[1 * 4 + d]);
-                    atomicAdd(&T[d][tk + 1][tj], v[2 * 4 + d]);
-                    atomicAdd(&T[d][tk + 1][tj + 1], v[3 * 4 + d]);
-                }
-            } else {
-                const int kj1 = wrap_idx(kj + 1, My), kk1 = wrap_idx(kk + 1, Mz);
-                const size_t nd[4] = {(size_t)kj + (size_t)My * kk, (size_t)kj1 + (size_t)My * kk,
-                                      (size_t)kj + (size_t)My * kk1,
-                                      (size_t)kj1 + (size_t)My * kk1};
+            for (int r = 0; r < 4; r++)
 #pragma unroll
-                for (int r = 0; r < 4; r++)
-#pragma unroll
-                    for (int d = 0; d < 4; d++) atomicAdd(a.dep + d * plane + nd[r], v[r * 4 + d]);
-            }
+                for (int d = 0; d < ND; d++) atomicAdd(a.dep + d * plane + nd[r], v[r * ND + d]);
         }
+        __syncwarp();
     }
     pdl_trigger();
+    // spread the per-cell sums to the corners: the lane of cell (l, row) owns
+    // column l of rows row and row+1; the right-hand corners go to lane l+1
+    float row0[ND], row1[ND], edge0[ND], edge1[ND];
+#pragma unroll
+    for (int d = 0; d < ND; d++) {
+        const float c00 = Acc[wr][0 * ND + d][lane], c10 = Acc[wr][1 * ND + d][lane];
+        const float c01 = Acc[wr][2 * ND + d][lane], c11 = Acc[wr][3 * ND + d][lane];
+        const float l10 = __shfl_up_sync(full, c10, 1), l11 = __shfl_up_sync(full, c11, 1);
+        row0[d] = c00 + (lane > 0 ? l10 : 0.f);
+        row1[d] = c01 + (lane > 0 ? l11 : 0.f);
+        edge0[d] = c10;   // used by lane 31 only: column 32
+        edge1[d] = c11;
+    }
+#pragma unroll
+    for (int d = 0; d < ND; d++) {
+        T[d][wr][lane] += row0[d];
+        if (lane == 31) T[d][wr][TX] += edge0[d];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int d = 0; d < ND; d++) {
+        T[d][wr + 1][lane] += row1[d];
+        if (lane == 31) T[d][wr + 1][TX] += edge1[d];
+    }
     __syncthreads();
     for (int i = threadIdx.x; i < H * W; i += 32 * TY) {
         const int r = i / W, cc = i - r * W;
         const size_t m = (size_t)wrap_idx(j0 + cc, My) + (size_t)My * wrap_idx(k0 + r, Mz);
 #pragma unroll
-        for (int d = 0; d < 4; d++) {
+        for (int d = 0; d < ND; d++) {
             const float x = T[d][r][cc];
             if (x != 0.f) atomicAdd(a.dep + d * plane + m, x);
         }
@@ -740,8 +784,11 @@ int launch_push(const PushArgs<T>& a, int shape, bool precise, cudaStream_t st) 
         if constexpr (F32) {
             constexpr int TY = 4;
             if (a.loff && !a.dep_cell) {   // grouped by cell with offsets (the engine checks the shape)
-                launch_pdl(push_cic_warp_kernel<TY>, dim3((a.My / 32) * (a.Mz / TY)),
-                           dim3(32 * TY), 0, st, a);
+                const dim3 grid((a.My / 32) * (a.Mz / TY));
+                if (a.skip_dens)
+                    launch_pdl(push_cic_warp_kernel<TY, 3>, grid, dim3(32 * TY), 0, st, a);
+                else
+                    launch_pdl(push_cic_warp_kernel<TY, 4>, grid, dim3(32 * TY), 0, st, a);
                 return 1;
             }
         }

@@ -71,6 +71,7 @@ struct PushArgs {
     const int* loff;
     const int* bpref;
     int* cnt;
+    int skip_dens;        // 1: leave out the density deposit (plane 3), unused by the caller
     int full;
     int* err;
 };
