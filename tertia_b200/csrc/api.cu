@@ -162,6 +162,9 @@ struct EngineBase {
             if (h & DEV_ERR_RANGE)
                 return fail(QS_ERR_PARTICLE_RANGE, "particle in-cell fraction outside [0,1]");
             if (h & DEV_ERR_TIMEOUT) return fail(QS_ERR_TIMEOUT, "bounded device wait gave up");
+            if (h & DEV_ERR_INTERNAL)
+                return fail(QS_ERR_DEVICE, "internal consistency check failed on the device "
+                                           "(plasma regrouping)");
             return fail(QS_ERR_DEVICE, "device error flag 0x%x", h);
         }
         return QS_OK;
@@ -419,8 +422,8 @@ struct Engine : EngineBase {
                                            st);
             });
             klaunch(KC_SORT, [&] {
-                return launch_scatter<T>(cur_set(), alt_set(), np, cic_cnt, cic_loff, cic_bpref,
-                                         st);
+                return launch_scatter<T>(cur_set(), alt_set(), np, ncell, cic_cnt, cic_loff,
+                                         cic_bpref, d_err, st);
             });
             swap_sets();
             // the scatter rebuilt the arrays in cell order: the offsets hold
@@ -429,7 +432,9 @@ struct Engine : EngineBase {
             grp.counted = false;
         } else if (!grp.off_valid) {
             if (!grp.counted)
-                klaunch(KC_SORT, [&] { return launch_count_cells(pcell, np, cic_cnt, st); });
+                klaunch(KC_SORT, [&] {
+                    return launch_count_cells(pcell, np, ncell, cic_cnt, d_err, st);
+                });
             klaunch(KC_SORT, [&] {
                 return launch_cell_offsets(cic_cnt, ncell, cic_loff, cic_bsum, cic_bpref, cic_ticket, 1,
                                            st);

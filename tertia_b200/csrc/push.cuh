@@ -53,6 +53,12 @@ __device__ __forceinline__ int wrap_idx(int j, int M) {
     return j;
 }
 
+// j within one period of [0, M) (a shift of at most one cell): no loop
+__device__ __forceinline__ int wrap1(int j, int M) {
+    j += (j < 0) ? M : 0;
+    return j - ((j >= M) ? M : 0);
+}
+
 // k = cell / My, j = cell % My through a float reciprocal with correction
 // (exact for cell < 2^24)
 __device__ __forceinline__ void cell_jk(int cell, int My, float invMy, int& j, int& k) {
@@ -527,10 +533,31 @@ __device__ __forceinline__ int cell_offset(const PushArgs<float>& a, int c) {
     return a.loff[c] + a.bpref[c >> 10];
 }
 
+// one CIC sub-step of a particle (cell-relative move from base cell (jb, kb),
+// periodic wrap, the 4 corner weights of the new position)
+__device__ __forceinline__ void cic_substep(float dy, float dz, float ps, float& ytmp,
+                                            float& ztmp, int& jb, int& kb, int My, int Mz,
+                                            float (&wc)[4]) {
+    const float uy = ytmp + dy * ps, uz = ztmp + dz * ps;
+    const float fy = floorf(uy), fz = floorf(uz);
+    float ry = uy - fy, rz = uz - fz;
+    int sy = (int)fy, sz = (int)fz;
+    if (ry >= 1.f) { ry = 0.f; sy += 1; }
+    if (rz >= 1.f) { rz = 0.f; sz += 1; }
+    jb = wrap1(jb + sy, My);   // |dy * ps| <= 1: the shift is at most one cell
+    kb = wrap1(kb + sz, Mz);
+    ytmp = ry;
+    ztmp = rz;
+    wc[0] = (1.f - ry) * (1.f - rz);
+    wc[1] = ry * (1.f - rz);
+    wc[2] = (1.f - ry) * rz;
+    wc[3] = ry * rz;
+}
+
 template <int TY, int ND>
 __global__ void __launch_bounds__(32 * TY) push_cic_warp_kernel(PushArgs<float> a) {
     constexpr int TX = 32, W = TX + 1, H = TY + 1, NV = 4 * ND;
-    __shared__ float Fs[6][4][TY][TX];   // [field][corner][row][col]
+    __shared__ float Fs[6][H][W];        // fields of the tile cells + one row/column (P, C averaged)
     __shared__ float Acc[TY][NV][TX];    // per-warp sums [corner*ND + current][cell]
     __shared__ float T[ND][H][W];        // block deposit tile [current][row][col]
     const int lane = threadIdx.x & 31, wr = threadIdx.x >> 5;
@@ -542,32 +569,40 @@ __global__ void __launch_bounds__(32 * TY) push_cic_warp_kernel(PushArgs<float> 
 #pragma unroll
     for (int i = 0; i < NV; i++) Acc[wr][i][lane] = 0.f;
     pdl_wait();
-    {
-        const int j = j0 + lane, k = k0 + wr;
-        const int j1 = wrap_idx(j + 1, My), k1 = wrap_idx(k + 1, Mz);
-        const size_t nn[4] = {(size_t)j + (size_t)My * k, (size_t)j1 + (size_t)My * k,
-                              (size_t)j + (size_t)My * k1, (size_t)j1 + (size_t)My * k1};
+    for (int i = threadIdx.x; i < H * W; i += 32 * TY) {
+        const int r = i / W, cc = i - r * W;
+        const size_t m = (size_t)wrap1(j0 + cc, My) + (size_t)My * wrap1(k0 + r, Mz);
 #pragma unroll
-        for (int f = 0; f < 6; f++)
-#pragma unroll
-            for (int r = 0; r < 4; r++)
-                Fs[f][r][wr][lane] =
-                    0.5f * (ld(a.P + f * plane + nn[r]) + ld(a.C + f * plane + nn[r]));
+        for (int f = 0; f < 6; f++) Fs[f][r][cc] = 0.5f * (ld(a.P + f * plane + m) + ld(a.C + f * plane + m));
     }
     __syncthreads();
     const unsigned full = 0xffffffffu;
     const int c0 = j0 + My * (k0 + wr);   // this warp's 32 cells: c0 .. c0+31
     const int pbeg = cell_offset(a, c0);
     const int pend = (size_t)(c0 + TX) < plane ? cell_offset(a, c0 + TX) : (int)a.n;
+    // the particle of the next pass is loaded while this one is pushed
+    int nx_cell = 0;
+    float nx_y = 0.f, nx_z = 0.f, nx_px = 0.f, nx_py = 0.f, nx_pz = 0.f, nx_w = 0.f;
+    if (pbeg + lane < pend) {
+        const int q = pbeg + lane;
+        nx_cell = a.cell[q]; nx_y = a.y[q]; nx_z = a.z[q];
+        nx_px = a.px[q]; nx_py = a.py[q]; nx_pz = a.pz[q]; nx_w = a.w[q];
+    }
     for (int base = pbeg; base < pend; base += 32) {
         const int p = base + lane;
+        const int cell = nx_cell;
+        const float yp = nx_y, zp = nx_z, w = nx_w;
+        float px = nx_px, py = nx_py, pz = nx_pz;
+        if (p + 32 < pend) {
+            const int q = p + 32;
+            nx_cell = a.cell[q]; nx_y = a.y[q]; nx_z = a.z[q];
+            nx_px = a.px[q]; nx_py = a.py[q]; nx_pz = a.pz[q]; nx_w = a.w[q];
+        }
         int key = -1;                     // destination cell of the first sub-step
         float v[NV];
 #pragma unroll
         for (int i = 0; i < NV; i++) v[i] = 0.f;
         if (p < pend) {
-            const int cell = a.cell[p];
-            const float yp = a.y[p], zp = a.z[p];
             if (!(yp >= 0.f && yp <= 1.f && zp >= 0.f && zp <= 1.f)) {
                 atomicOr(a.err, DEV_ERR_RANGE);
                 if (a.full && a.cnt) atomicAdd(a.cnt + cell, 1);   // it stays in its cell
@@ -581,10 +616,10 @@ __global__ void __launch_bounds__(32 * TY) push_cic_warp_kernel(PushArgs<float> 
                 if (tj >= 0 && tj < TX && tk >= 0 && tk < TY) {
 #pragma unroll
                     for (int f = 0; f < 6; f++)
-                        g[f] = wg[0] * Fs[f][0][tk][tj] + wg[1] * Fs[f][1][tk][tj] +
-                               wg[2] * Fs[f][2][tk][tj] + wg[3] * Fs[f][3][tk][tj];
+                        g[f] = wg[0] * Fs[f][tk][tj] + wg[1] * Fs[f][tk][tj + 1] +
+                               wg[2] * Fs[f][tk + 1][tj] + wg[3] * Fs[f][tk + 1][tj + 1];
                 } else {
-                    const int j1 = wrap_idx(j + 1, My), k1 = wrap_idx(k + 1, Mz);
+                    const int j1 = wrap1(j + 1, My), k1 = wrap1(k + 1, Mz);
                     const size_t nn[4] = {(size_t)j + (size_t)My * k, (size_t)j1 + (size_t)My * k,
                                           (size_t)j + (size_t)My * k1,
                                           (size_t)j1 + (size_t)My * k1};
@@ -598,7 +633,6 @@ __global__ void __launch_bounds__(32 * TY) push_cic_warp_kernel(PushArgs<float> 
                         g[f] = acc;
                     }
                 }
-                float px = a.px[p], py = a.py[p], pz = a.pz[p];
                 const float inv_gp = rsqrtf(1.f + px * px + py * py + pz * pz);
                 const float Vxp = px * inv_gp, Vyp = py * inv_gp, Vzp = pz * inv_gp;
                 const float kE = a.sE * __frcp_rn(1.f - Vxp);
@@ -619,7 +653,7 @@ __global__ void __launch_bounds__(32 * TY) push_cic_warp_kernel(PushArgs<float> 
                 const float Vx = 0.5f * (Vxm + Vxp), Vy = 0.5f * (Vym + Vyp),
                             Vz = 0.5f * (Vzm + Vzp);
                 const float inv2 = __frcp_rn(1.f - Vx);
-                const float wq = a.w[p] * inv2;
+                const float wq = w * inv2;
                 const float dq[4] = {wq * a.djx0 * Vxm, wq * a.djy0 * Vym, wq * a.djz0 * Vzm,
                                      wq * a.drho0};
                 const float dy = Vy * a.hxhy * inv2, dz = Vz * a.hxhz * inv2;
@@ -629,42 +663,32 @@ __global__ void __launch_bounds__(32 * TY) push_cic_warp_kernel(PushArgs<float> 
                 if (partdx < 1.f) partdx = step = 1.f;
                 float ytmp = yp, ztmp = zp;
                 int jb = j, kb = k;
-                bool first = true;
+                // first sub-step: its deposit goes through the warp reduction
+                float ps;
+                if (partdx > 1.f) { partdx -= 1.f; ps = __frcp_rn(step); }
+                else { ps = __fdividef(partdx, step); partdx = 0.f; }
+                float wc[4];
+                cic_substep(dy, dz, ps, ytmp, ztmp, jb, kb, My, Mz, wc);
+                key = jb + My * kb;
+#pragma unroll
+                for (int r = 0; r < 4; r++)
+#pragma unroll
+                    for (int d = 0; d < ND; d++) v[r * ND + d] = dq[d] * ps * wc[r];
+                // further sub-steps (|dy| or |dz| > 1 cell, rare): direct atomics
                 while (partdx > 0.f) {
-                    float ps;
                     if (partdx > 1.f) { partdx -= 1.f; ps = __frcp_rn(step); }
                     else { ps = __fdividef(partdx, step); partdx = 0.f; }
-                    const float uy = ytmp + dy * ps, uz = ztmp + dz * ps;
-                    const float fy = floorf(uy), fz = floorf(uz);
-                    float ry = uy - fy, rz = uz - fz;
-                    int sy = (int)fy, sz = (int)fz;
-                    if (ry >= 1.f) { ry = 0.f; sy += 1; }
-                    if (rz >= 1.f) { rz = 0.f; sz += 1; }
-                    jb = wrap_idx(jb + sy, My);
-                    kb = wrap_idx(kb + sz, Mz);
-                    ytmp = ry;
-                    ztmp = rz;
-                    const float wc[4] = {(1.f - ry) * (1.f - rz), ry * (1.f - rz),
-                                         (1.f - ry) * rz, ry * rz};
-                    if (first) {
-                        key = jb + My * kb;
+                    cic_substep(dy, dz, ps, ytmp, ztmp, jb, kb, My, Mz, wc);
+                    const int jb1 = wrap1(jb + 1, My), kb1 = wrap1(kb + 1, Mz);
+                    const size_t nd[4] = {(size_t)jb + (size_t)My * kb,
+                                          (size_t)jb1 + (size_t)My * kb,
+                                          (size_t)jb + (size_t)My * kb1,
+                                          (size_t)jb1 + (size_t)My * kb1};
 #pragma unroll
-                        for (int r = 0; r < 4; r++)
+                    for (int r = 0; r < 4; r++)
 #pragma unroll
-                            for (int d = 0; d < ND; d++) v[r * ND + d] = dq[d] * ps * wc[r];
-                        first = false;
-                    } else {
-                        const int jb1 = wrap_idx(jb + 1, My), kb1 = wrap_idx(kb + 1, Mz);
-                        const size_t nd[4] = {(size_t)jb + (size_t)My * kb,
-                                              (size_t)jb1 + (size_t)My * kb,
-                                              (size_t)jb + (size_t)My * kb1,
-                                              (size_t)jb1 + (size_t)My * kb1};
-#pragma unroll
-                        for (int r = 0; r < 4; r++)
-#pragma unroll
-                            for (int d = 0; d < ND; d++)
-                                atomicAdd(a.dep + d * plane + nd[r], dq[d] * ps * wc[r]);
-                    }
+                        for (int d = 0; d < ND; d++)
+                            atomicAdd(a.dep + d * plane + nd[r], dq[d] * ps * wc[r]);
                 }
                 if (a.full) {
                     const int nc = jb + My * kb;
@@ -683,10 +707,11 @@ __global__ void __launch_bounds__(32 * TY) push_cic_warp_kernel(PushArgs<float> 
         const int re = after ? __ffs(after) - 2 : 31;                        // run end
 #pragma unroll
         for (int d = 1; d <= 4; d <<= 1) {
+            const bool take = lane + d <= re && ((lane - rs) & (2 * d - 1)) == 0;
 #pragma unroll
             for (int i = 0; i < NV; i++) {
                 const float o = __shfl_down_sync(full, v[i], d);
-                if (lane + d <= re && ((lane - rs) & (2 * d - 1)) == 0) v[i] += o;
+                if (take) v[i] += o;
             }
         }
         const bool head = key >= 0 && ((lane - rs) & 7) == 0;
@@ -715,7 +740,7 @@ __global__ void __launch_bounds__(32 * TY) push_cic_warp_kernel(PushArgs<float> 
         } else if (head) {
             int kj, kk;
             cell_jk(key, My, a.invMy, kj, kk);
-            const int kj1 = wrap_idx(kj + 1, My), kk1 = wrap_idx(kk + 1, Mz);
+            const int kj1 = wrap1(kj + 1, My), kk1 = wrap1(kk + 1, Mz);
             const size_t nd[4] = {(size_t)kj + (size_t)My * kk, (size_t)kj1 + (size_t)My * kk,
                                   (size_t)kj + (size_t)My * kk1, (size_t)kj1 + (size_t)My * kk1};
 #pragma unroll
@@ -753,7 +778,7 @@ __global__ void __launch_bounds__(32 * TY) push_cic_warp_kernel(PushArgs<float> 
     __syncthreads();
     for (int i = threadIdx.x; i < H * W; i += 32 * TY) {
         const int r = i / W, cc = i - r * W;
-        const size_t m = (size_t)wrap_idx(j0 + cc, My) + (size_t)My * wrap_idx(k0 + r, Mz);
+        const size_t m = (size_t)wrap1(j0 + cc, My) + (size_t)My * wrap1(k0 + r, Mz);
 #pragma unroll
         for (int d = 0; d < ND; d++) {
             const float x = T[d][r][cc];

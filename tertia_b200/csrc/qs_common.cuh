@@ -14,6 +14,7 @@ enum DevErr : int {
     DEV_ERR_RANGE = 1,         // particle fraction outside [0,1] (exit(-212)/exit(-12))
     DEV_ERR_BEAM_CURRENT = 2,  // |JxBeam| > 10 (exit(20))
     DEV_ERR_TIMEOUT = 4,       // a bounded device wait gave up
+    DEV_ERR_INTERNAL = 8,      // an internal consistency check failed (access skipped)
 };
 
 constexpr int kMaxXfFields = 8;

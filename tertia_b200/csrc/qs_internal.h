@@ -108,12 +108,13 @@ struct PlasmaSet {
     int32_t* id;
 };
 int scan_blocks_count(int ncell);
-int launch_count_cells(const int32_t* cell, int64_t n, int* cnt, cudaStream_t st);
+int launch_count_cells(const int32_t* cell, int64_t n, int ncell, int* cnt, int* err,
+                       cudaStream_t st);
 int launch_cell_offsets(int* cnt, int ncell, int* loff, int* bsum, int* bpref,
                         unsigned* ticket, int clear, cudaStream_t st);
 template <class T>
-int launch_scatter(const PlasmaSet<T>& in, const PlasmaSet<T>& out, int64_t n, int* cnt,
-                   const int* loff, const int* bpref, cudaStream_t st);
+int launch_scatter(const PlasmaSet<T>& in, const PlasmaSet<T>& out, int64_t n, int ncell,
+                   int* cnt, const int* loff, const int* bpref, int* err, cudaStream_t st);
 int launch_iota(int32_t* id, int64_t n, cudaStream_t st);
 
 // ---- adjoint (adjoint.cu)

@@ -23,11 +23,16 @@ namespace {
 constexpr int kScanBlock = 1024;
 
 __global__ void __launch_bounds__(256) count_cells_kernel(const int32_t* __restrict__ cell,
-                                                          int64_t n, int* __restrict__ cnt) {
+                                                          int64_t n, int ncell,
+                                                          int* __restrict__ cnt,
+                                                          int* __restrict__ err) {
     pdl_wait();
     const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     pdl_trigger();
-    if (p < n) atomicAdd(cnt + cell[p], 1);
+    if (p >= n) return;
+    const int c = cell[p];
+    if (c < 0 || c >= ncell) atomicOr(err, DEV_ERR_INTERNAL);
+    else atomicAdd(cnt + c, 1);
 }
 
 __device__ __forceinline__ int block_exclusive_scan(int v, int* wsum, int& total) {
@@ -96,15 +101,24 @@ __global__ void __launch_bounds__(kScanBlock) scan_cells_kernel(int* __restrict_
 
 template <class T>
 __global__ void __launch_bounds__(256) scatter_kernel(PlasmaSet<T> in, PlasmaSet<T> out, int64_t n,
-                                                      int* __restrict__ cnt,
+                                                      int ncell, int* __restrict__ cnt,
                                                       const int* __restrict__ loff,
-                                                      const int* __restrict__ bpref) {
+                                                      const int* __restrict__ bpref,
+                                                      int* __restrict__ err) {
     pdl_wait();
     const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= n) return;
     const int c = in.cell[p];
+    if (c < 0 || c >= ncell) {   // a cell the counts never saw: record, skip
+        atomicOr(err, DEV_ERR_INTERNAL);
+        return;
+    }
     const int r = atomicSub(cnt + c, 1) - 1;
     const int64_t q = (int64_t)loff[c] + bpref[c / kScanBlock] + r;
+    if (r < 0 || q < 0 || q >= n) {   // counts out of step with the cells: record, skip
+        atomicOr(err, DEV_ERR_INTERNAL);
+        return;
+    }
     const T y = in.y[p], z = in.z[p], px = in.px[p], py = in.py[p], pz = in.pz[p], w = in.w[p];
     const int32_t id = in.id[p];
     pdl_trigger();
@@ -122,10 +136,11 @@ __global__ void iota_kernel(int32_t* __restrict__ id, int64_t n) {
 
 int scan_blocks_count(int ncell) { return (ncell + kScanBlock - 1) / kScanBlock; }
 
-int launch_count_cells(const int32_t* cell, int64_t n, int* cnt, cudaStream_t st) {
+int launch_count_cells(const int32_t* cell, int64_t n, int ncell, int* cnt, int* err,
+                       cudaStream_t st) {
     if (n <= 0) return 0;
     launch_pdl(count_cells_kernel, dim3((unsigned)((n + 255) / 256)), dim3(256), 0, st, cell, n,
-               cnt);
+               ncell, cnt, err);
     return 1;
 }
 
@@ -138,11 +153,11 @@ int launch_cell_offsets(int* cnt, int ncell, int* loff, int* bsum, int* bpref,
 }
 
 template <class T>
-int launch_scatter(const PlasmaSet<T>& in, const PlasmaSet<T>& out, int64_t n, int* cnt,
-                   const int* loff, const int* bpref, cudaStream_t st) {
+int launch_scatter(const PlasmaSet<T>& in, const PlasmaSet<T>& out, int64_t n, int ncell,
+                   int* cnt, const int* loff, const int* bpref, int* err, cudaStream_t st) {
     if (n <= 0) return 0;
     launch_pdl(scatter_kernel<T>, dim3((unsigned)((n + 255) / 256)), dim3(256), 0, st, in, out, n,
-               cnt, loff, bpref);
+               ncell, cnt, loff, bpref, err);
     return 1;
 }
 
@@ -152,9 +167,9 @@ int launch_iota(int32_t* id, int64_t n, cudaStream_t st) {
     return 1;
 }
 
-template int launch_scatter<float>(const PlasmaSet<float>&, const PlasmaSet<float>&, int64_t, int*,
-                                   const int*, const int*, cudaStream_t);
+template int launch_scatter<float>(const PlasmaSet<float>&, const PlasmaSet<float>&, int64_t, int,
+                                   int*, const int*, const int*, int*, cudaStream_t);
 template int launch_scatter<double>(const PlasmaSet<double>&, const PlasmaSet<double>&, int64_t,
-                                    int*, const int*, const int*, cudaStream_t);
+                                    int, int*, const int*, const int*, int*, cudaStream_t);
 
 }  // namespace qs
