@@ -56,6 +56,7 @@ def parse():
                          "weak 1e5-particle beam (not a bench line)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64-plain comparison")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the c3 adjoint measurement")
     ap.add_argument("--cpu-seconds", type=float, default=12.0,
                     help="target seconds of the bounded CPU sample")
     return ap.parse_args()
@@ -176,6 +177,104 @@ def cpu_sample(w, target_s: float):
             "kind": "port",
             "sample": f"oracle FP64 xi-march of {layers} layers of the {w.cfg.ny}x{w.cfg.nz} "
                       f"grid ({np_layer} particles/layer), {dt:.1f} s on {cores} threads"}
+
+
+# ------------------------------------------------------------------ adjoint (c3)
+def adjoint_measure(precision: str):
+    """The c3 adjoint: 256 x 256 x 2048, 4 ppc, NGP, 1e6-particle driver whose
+    charge profile is 64 xi-bins with seeded weights in [0.5, 1.5]; loss = on-axis
+    Ex integrated over the witness window xi in [-6, -5] behind the driver
+    centre; layer checkpoints every 32 layers.  Reports the forward march and
+    the adjoint times (device events), their ratio, the ratio over the same
+    layer range (the sweep covers only the layers from the head to the window),
+    and the gradient against central differences (h = 1e-3) on a few bins and
+    against the FP64 adjoint on all bins."""
+    import numpy as np
+    import torch
+    from tertia_b200 import workload as wl
+    from tertia_b200.abi import PRECISIONS, QS_SHAPE_NGP
+    from tertia_b200.autograd import xi_bins
+    from tertia_b200.mesh import Mesh
+
+    nbins, every, h = 64, 32, 1e-3
+
+    def setup(prec):
+        w = wl.make_workload("c3", prec)
+        cfg = w.cfg
+        cfg.shape = QS_SHAPE_NGP
+        beam = wl.workload_beam(w)
+        xc = wl.driver_center_x(cfg, w.beams[0].sigma_xi)
+        sx = w.beams[0].sigma_xi
+        bins = xi_bins(beam, cfg, nbins, xc - 4 * sx, xc + 4 * sx)
+        xl = np.arange(cfg.nx) * cfg.hx
+        coeff = np.where((xl >= xc - 6.0) & (xl <= xc - 5.0), cfg.hx, 0.0)
+        m = Mesh(cfg)
+        m.seed_front_plasma(0)
+        m.adjoint_checkpoints(every)
+        return cfg, m, beam, bins, coeff
+
+    beta = np.random.default_rng(3).uniform(0.5, 1.5, nbins)
+
+    def forward(m, beam, bins, coeff, b):
+        bb = dict(beam)
+        bb["w"] = np.asarray(beam["w"]) * b[bins]
+        m.load_beam(bb)
+        m.move_beam_particles()
+        m.move_all_split_layers()
+        return float(np.dot(coeff, m.onaxis_ex()))
+
+    def grad(m, beam, bins, coeff, b):
+        forward(m, beam, bins, coeff, b)
+        dw = m.adjoint(coeff)
+        return np.bincount(bins, weights=np.asarray(beam["w"]) * dw, minlength=nbins)
+
+    cfg, m, beam, bins, coeff = setup(precision)
+    stream = torch.cuda.ExternalStream(m.stream())
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    forward(m, beam, bins, coeff, beta)          # warm-up (captures the march graph)
+    g = grad(m, beam, bins, coeff, beta)          # warm-up of the adjoint
+    bb = dict(beam)
+    bb["w"] = np.asarray(beam["w"]) * beta[bins]
+    m.load_beam(bb)
+    m.move_beam_particles()
+    torch.cuda.synchronize()
+    e0.record(stream)
+    m.move_all_split_layers()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    fwd_ms = e0.elapsed_time(e1)
+    t0 = time.perf_counter()
+    dw = m.adjoint(coeff)
+    torch.cuda.synchronize()
+    adj_ms = (time.perf_counter() - t0) * 1e3
+    g = np.bincount(bins, weights=np.asarray(beam["w"]) * dw, minlength=nbins)
+    lo = int(np.nonzero(coeff)[0].min())
+    swept = cfg.nx - lo
+    # central differences on the 4 bins with the largest gradient
+    top = np.argsort(-np.abs(g))[:4]
+    fd = []
+    for b in top:
+        bp, bm = beta.copy(), beta.copy()
+        bp[b] += h
+        bm[b] -= h
+        fd.append((forward(m, beam, bins, coeff, bp) - forward(m, beam, bins, coeff, bm)) / (2 * h))
+    fd = np.array(fd)
+    m.close()
+    cfg64, m64, beam64, bins64, coeff64 = setup("fp64")
+    g64 = grad(m64, beam64, bins64, coeff64, beta)
+    m64.close()
+    rel = lambda a, b: float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+    return {"workload": "c3: 256x256x2048 NGP, 64 xi-bins, witness window xi in [-6, -5], "
+                        f"checkpoints every {every} layers",
+            "precision": precision, "forward_ms": fwd_ms, "adjoint_ms": adj_ms,
+            "adjoint_over_forward": adj_ms / fwd_ms,
+            "layers_swept": swept, "layers": cfg.nx,
+            "adjoint_over_forward_same_layers": adj_ms / (fwd_ms * swept / cfg.nx),
+            "grad_rel_err_vs_fd_top4": rel(g[top], fd),
+            "grad_rel_err_vs_fp64_adjoint": rel(g, g64),
+            "fd_step": h, "loss_note": "loss = sum over window layers of hx * on-axis Ex",
+            "timing": "forward: device events around the march; adjoint: host wall clock "
+                      "around qs_adjoint (it synchronises)"}
 
 
 # ------------------------------------------------------------------ our arm
@@ -396,6 +495,9 @@ def run_ours(args):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_sample(w, args.cpu_seconds)
+    adjoint = None
+    if rank == 0 and world == 1 and not args.no_adjoint and not args.layers:
+        adjoint = adjoint_measure(args.precision)
 
     if rank == 0:
         line = {
@@ -417,6 +519,7 @@ def run_ours(args):
             "roofline": roof,
             "cpu_baseline": cpu,
             "fp64_plain": fp64,
+            "adjoint": adjoint,
             "clocks": clk,
             "onaxis_ex_max": float(np.max(np.abs(onaxis))),
         }

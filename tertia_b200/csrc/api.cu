@@ -243,7 +243,7 @@ struct Engine : EngineBase {
     // graph of the march
     cudaGraphExec_t gexec = nullptr;
     int64_t graph_kernels = 0;
-    struct HostState { T *Pf, *Cf, *Psrc, *Csrc; int cur; Grouping grp; } graph_end{};
+    struct HostState { T *Pf, *Cf, *Psrc, *Csrc; int cur; Grouping grp; } graph_end{}, adj_end{};
     bool marched = false;
     // adjoint: layer checkpoints of the last march and the reverse sweep's buffers
     int ck_every = 0;           // checkpoint every ck_every layers (0: off)
@@ -257,6 +257,10 @@ struct Engine : EngineBase {
     T* lam_b3 = nullptr;        // (nx+1) x 2 planes: adjoint of the real beam currents
     T* d_dloss = nullptr;       // nx: d loss / d on-axis Ex of each layer
     double* d_gradw = nullptr;  // nb: d loss / d beam weight
+    cudaGraphExec_t adj_exec = nullptr;   // captured sweep for the layers adj_lo .. head
+    int adj_lo = -1;
+    int64_t adj_graph_nb = -1;
+    int64_t adj_kernels = 0;
     int64_t adj_np = 0, adj_nb = 0;
 
     T* bankp(int b, int p) { return bank + ((size_t)b * SP_N + p) * plane; }
@@ -264,6 +268,7 @@ struct Engine : EngineBase {
 
     ~Engine() override {
         if (gexec) cudaGraphExecDestroy(gexec);
+        if (adj_exec) cudaGraphExecDestroy(adj_exec);
         delete tcx;
         void* ptrs[] = {f3, b3, src3, splitbuf, srcbuf, Cbeam, sb3, bank, scratch, mats, onaxis_d,
                         stage, stage_d, pcell, py, pz, ppx, ppy, ppz, pw, bi, bj, bk, bx, by, bz,
@@ -479,7 +484,14 @@ struct Engine : EngineBase {
             cudaGraphExecDestroy(gexec);
             gexec = nullptr;
         }
+        drop_adjoint_graph();
         return QS_OK;
+    }
+
+    void drop_adjoint_graph() {
+        if (adj_exec) cudaGraphExecDestroy(adj_exec);
+        adj_exec = nullptr;
+        adj_lo = -1;
     }
 
     qs_status ensure_beam(int64_t n) {
@@ -499,6 +511,7 @@ struct Engine : EngineBase {
         if ((s = alloc(&bpz, n, "beam"))) return s;
         if ((s = alloc(&bw, n, "beam"))) return s;
         nb_cap = n;
+        drop_adjoint_graph();   // it baked the old beam arrays
         return QS_OK;
     }
 
@@ -750,17 +763,16 @@ struct Engine : EngineBase {
     // REDFT11, movefieldshydrolinlayersplit.cpp:717-718) in large batches,
     // once per beam push instead of once per layer; plus the |JxBeam| > 10
     // check of :618-621.
-    qs_status beam_spectra() {
-        klaunch(KC_BEAM_SPECTRA, [&] { return launch_beam_check<T>(b3, L + 1, plane, d_err, st); });
-        const int np = 2 * (L + 1);
+    // REDFT11 x REDFT11 transforms of np contiguous planes in large batches
+    void batched_cc(const T* in_planes, T* out_planes, int np, int cls) {
         if (tc) {
             for (int b0 = 0; b0 < np; b0 += 64) {
                 const int nf = std::min(64, np - b0);
-                const float* in = (const float*)(b3 + (size_t)b0 * plane);
-                float* out = (float*)(sb3 + (size_t)b0 * plane);
+                const float* in = (const float*)(in_planes + (size_t)b0 * plane);
+                float* out = (float*)(out_planes + (size_t)b0 * plane);
                 klaunch(KC_SPLIT, [&] { return tcx->run_batched(in, out, nf, 1.0, 0, st); });
-                klaunch(KC_GEMM, [&] { return tcx->run_batched(in, out, nf, 1.0, 1, st); });
-                klaunch(KC_GEMM, [&] { return tcx->run_batched(in, out, nf, 1.0, 2, st); });
+                klaunch(cls, [&] { return tcx->run_batched(in, out, nf, 1.0, 1, st); });
+                klaunch(cls, [&] { return tcx->run_batched(in, out, nf, 1.0, 2, st); });
             }
         } else {
             for (int b0 = 0; b0 < np; b0 += kMaxXfFields) {
@@ -768,12 +780,17 @@ struct Engine : EngineBase {
                 T* outs[kMaxXfFields];
                 int kz[kMaxXfFields], ky[kMaxXfFields];
                 for (int f = 0; f < nf; f++) {
-                    outs[f] = sb3 + (size_t)(b0 + f) * plane;
+                    outs[f] = out_planes + (size_t)(b0 + f) * plane;
                     kz[f] = ky[f] = CC;
                 }
-                xform(job_stack(b3 + (size_t)b0 * plane, nf, outs, kz, ky, T(1)));
+                xform(job_stack(in_planes + (size_t)b0 * plane, nf, outs, kz, ky, T(1)));
             }
         }
+    }
+
+    qs_status beam_spectra() {
+        klaunch(KC_BEAM_SPECTRA, [&] { return launch_beam_check<T>(b3, L + 1, plane, d_err, st); });
+        batched_cc(b3, sb3, 2 * (L + 1), KC_GEMM);
         CK(cudaGetLastError());
         sb3_valid = true;
         return QS_OK;
@@ -1223,6 +1240,7 @@ struct Engine : EngineBase {
             cudaGraphExecDestroy(gexec);
             gexec = nullptr;
         }
+        drop_adjoint_graph();
         if (every == 0) return QS_OK;
         if (np <= 0) return fail(QS_ERR_STATE, "qs_adjoint_checkpoints: no plasma loaded");
         const int K = std::min(every, L);
@@ -1404,6 +1422,50 @@ struct Engine : EngineBase {
         return QS_OK;
     }
 
+    // the device part of the adjoint (capturable): clear the adjoints, sweep
+    // the segments from layer lo to the head, then d loss / d beam weight
+    qs_status adjoint_device(int lo) {
+        CK(cudaMemsetAsync(lam, 0, (size_t)LAM_N * plane * sizeof(T), st));
+        CK(cudaMemsetAsync(lam_pm, 0, 3 * (size_t)np * sizeof(T), st));
+        CK(cudaMemsetAsync(lam_sb, 0, (size_t)(L + 1) * 2 * plane * sizeof(T), st));
+        int first = L + 1;   // lowest beam-spectrum layer the sweep touches
+        if (lo >= 0) {
+            const int K = ck_every;
+            const int mlo = (L - 1 - lo) / K;
+            for (int m = mlo; m >= 0; m--) {
+                const int c = L - 1 - m * K;
+                const int end = std::max(c - K + 1, lo);
+                cur = 0;
+                qs_status s = recompute_segment(m, c, end);
+                if (s) return s;
+                for (int i = end; i <= c; i++) {
+                    if ((s = adjoint_layer(i, seg + (size_t)(c - i) * seg_stride()))) return s;
+                }
+            }
+            first = lo;
+        }
+        // beam spectra adjoint -> real beam-current adjoint (layers first..L;
+        // the rest is zero) -> d loss / d w
+        if (first <= L) {
+            CK(cudaMemsetAsync(lam_b3, 0, (size_t)first * 2 * plane * sizeof(T), st));
+            batched_cc(lam_sb + (size_t)first * 2 * plane, lam_b3 + (size_t)first * 2 * plane,
+                       2 * (L + 1 - first), KC_GEMM);
+        } else {
+            CK(cudaMemsetAsync(lam_b3, 0, (size_t)(L + 1) * 2 * plane * sizeof(T), st));
+        }
+        BeamGradArgs<T> g{};
+        g.n = nb; g.L = L; g.My = My; g.Mz = Mz;
+        g.bi = bi; g.bj = bj; g.bk = bk;
+        g.x = bx; g.y = by; g.z = bz; g.px = bpx; g.py = bpy; g.pz = bpz;
+        g.lb3 = lam_b3;
+        g.plane = plane;
+        g.polarity = cfg.beam_polarity;
+        g.out = d_gradw;
+        klaunch(KC_BEAM_PUSH, [&] { return launch_beam_weight_grad<T>(g, st); });
+        CK(cudaGetLastError());
+        return QS_OK;
+    }
+
     qs_status adjoint(const double* dloss, double* dw) override {
         if (!dloss || !dw) return fail(QS_ERR_INVALID, "qs_adjoint: null pointer");
         if (ck_every <= 0) return fail(QS_ERR_STATE, "qs_adjoint: checkpoints are off");
@@ -1419,49 +1481,53 @@ struct Engine : EngineBase {
             qs_status s = alloc(&d_gradw, (size_t)nb, "beam weight gradient");
             if (s) return s;
             adj_nb = nb;
+            drop_adjoint_graph();
         }
+        if (nb != adj_graph_nb) drop_adjoint_graph();   // the beam count is baked in
         {
             std::vector<T> h(L);
             for (int i = 0; i < L; i++) h[i] = (T)dloss[i];
             CK(cudaMemcpyAsync(d_dloss, h.data(), L * sizeof(T), cudaMemcpyHostToDevice, st));
             CK(cudaStreamSynchronize(st));
         }
-        CK(cudaMemsetAsync(lam, 0, (size_t)LAM_N * plane * sizeof(T), st));
-        CK(cudaMemsetAsync(lam_pm, 0, 3 * (size_t)np * sizeof(T), st));
-        CK(cudaMemsetAsync(lam_sb, 0, (size_t)(L + 1) * 2 * plane * sizeof(T), st));
-        if (lo >= 0) {
-            const int K = ck_every;
-            const int mlo = (L - 1 - lo) / K;
-            for (int m = mlo; m >= 0; m--) {
-                const int c = L - 1 - m * K;
-                const int end = std::max(c - K + 1, lo);
-                cur = 0;
-                qs_status s = recompute_segment(m, c, end);
-                if (s) return s;
-                for (int i = end; i <= c; i++) {
-                    if ((s = adjoint_layer(i, seg + (size_t)(c - i) * seg_stride()))) return s;
+        if (cfg.use_graph && !prof) {
+            // the sweep for this range of layers is captured once and replayed
+            if (!adj_exec || adj_lo != lo) {
+                if (adj_exec) cudaGraphExecDestroy(adj_exec);
+                adj_exec = nullptr;
+                cudaGraph_t g = nullptr;
+                CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+                capturing = true;
+                capture_count = 0;
+                g_pdl = use_pdl;
+                qs_status s = adjoint_device(lo);
+                g_pdl = false;
+                capturing = false;
+                cudaError_t e = cudaStreamEndCapture(st, &g);
+                if (s) {
+                    if (g) cudaGraphDestroy(g);
+                    return s;
                 }
+                if (e != cudaSuccess) return cuda_fail(e, "adjoint capture");
+                e = cudaGraphInstantiate(&adj_exec, g, 0);
+                cudaGraphDestroy(g);
+                if (e != cudaSuccess) {
+                    adj_exec = nullptr;
+                    return cuda_fail(e, "adjoint graph instantiate");
+                }
+                adj_lo = lo;
+                adj_graph_nb = nb;
+                adj_kernels = capture_count;
+                adj_end = HostState{Pf, Cf, Psrc, Csrc, cur, grp};
             }
+            CK(cudaGraphLaunch(adj_exec, st));
+            launches += adj_kernels;
+            Pf = adj_end.Pf; Cf = adj_end.Cf; Psrc = adj_end.Psrc; Csrc = adj_end.Csrc;
+            cur = adj_end.cur;
+        } else {
+            qs_status s = adjoint_device(lo);
+            if (s) return s;
         }
-        // beam spectra adjoint -> real beam-current adjoint -> d loss / d w
-        const int CCk[8] = {CC, CC, CC, CC, CC, CC, CC, CC};
-        const int nplanes = 2 * (L + 1);
-        for (int b0 = 0; b0 < nplanes; b0 += 8) {
-            const int nf = std::min(8, nplanes - b0);
-            T* outs[8];
-            for (int f = 0; f < nf; f++) outs[f] = lam_b3 + (size_t)(b0 + f) * plane;
-            xform(job_stack(lam_sb + (size_t)b0 * plane, nf, outs, CCk, CCk, T(1)));
-        }
-        BeamGradArgs<T> g{};
-        g.n = nb; g.L = L; g.My = My; g.Mz = Mz;
-        g.bi = bi; g.bj = bj; g.bk = bk;
-        g.x = bx; g.y = by; g.z = bz; g.px = bpx; g.py = bpy; g.pz = bpz;
-        g.lb3 = lam_b3;
-        g.plane = plane;
-        g.polarity = cfg.beam_polarity;
-        g.out = d_gradw;
-        klaunch(KC_BEAM_PUSH, [&] { return launch_beam_weight_grad<T>(g, st); });
-        CK(cudaGetLastError());
         if (nb > 0)
             CK(cudaMemcpyAsync(dw, d_gradw, nb * sizeof(double), cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
