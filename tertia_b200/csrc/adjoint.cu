@@ -250,6 +250,286 @@ int launch_push_adjoint(const PushAdjArgs<T>& a, cudaStream_t st) {
 }
 
 // ---------------------------------------------------------------------------
+// CIC push adjoint: one thread per particle.  The bilinear gather weights
+// depend on the in-cell position (y, z) and the deposit weights on the
+// position after the move, so besides the momentum adjoint the particle
+// carries the adjoint of its position (lamPos); cells come from floor() and
+// carry none.  The sub-step partition (its number and fractions) is held
+// fixed: exact for the usual single sub-step, first order for |dy|, |dz|
+// above one cell per layer.  Up to kMaxSub sub-steps are differentiated.
+constexpr int kMaxSub = 8;
+
+template <class T>
+__global__ void __launch_bounds__(256) push_adjoint_cic_kernel(PushAdjArgs<T> a) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.n) return;
+    const int My = a.My, Mz = a.Mz;
+    const int cell = a.cell[i];
+    const int j = cell % My, k = cell / My;
+    const T one = T(1), half = T(0.5);
+    const T yp = a.y[i], zp = a.z[i];
+    if (!(yp >= T(0) && yp <= one && zp >= T(0) && zp <= one)) return;   // forward skipped it
+    const T px0 = a.px[i], py0 = a.py[i], pz0 = a.pz[i];
+    const T w = a.w[i];
+    const size_t plane = a.plane;
+    const int j1 = wrap_m(j + 1, My), k1 = wrap_m(k + 1, Mz);
+    const size_t nn[4] = {(size_t)j + (size_t)My * k, (size_t)j1 + (size_t)My * k,
+                          (size_t)j + (size_t)My * k1, (size_t)j1 + (size_t)My * k1};
+    const T wg[4] = {(one - yp) * (one - zp), yp * (one - zp), (one - yp) * zp, yp * zp};
+    T F[6][4];
+    T g[6];
+#pragma unroll
+    for (int f = 0; f < 6; f++) {
+        g[f] = T(0);
+#pragma unroll
+        for (int r = 0; r < 4; r++) {
+            F[f][r] = half * (ldg_(a.P + f * plane + nn[r]) + ldg_(a.C + f * plane + nn[r]));
+            g[f] += wg[r] * F[f][r];
+        }
+    }
+    const T E[3] = {g[0], g[1], g[2]};
+    const T B[3] = {g[3] + a.bxe, g[4] + a.bye, g[5] + a.bze};
+
+    // ---- forward recompute of the push (as in push_adjoint_kernel)
+    const T p[3] = {px0, py0, pz0};
+    const T s0 = one + p[0] * p[0] + p[1] * p[1] + p[2] * p[2];
+    const T r0 = one / sqrt(s0);
+    const T Vp[3] = {p[0] * r0, p[1] * r0, p[2] * r0};
+    const T ia = one / (one - Vp[0]);
+    const T kE = a.sE * ia;
+    const T e[3] = {E[0] * kE, E[1] * kE, E[2] * kE};
+    const T p1[3] = {p[0] + e[0], p[1] + e[1], p[2] + e[2]};
+    const T r1 = one / sqrt(one + p1[0] * p1[0] + p1[1] * p1[1] + p1[2] * p1[2]);
+    const T kB = r1 * kE;
+    const T b[3] = {B[0] * kB, B[1] * kB, B[2] * kB};
+    const T co = T(2) / (one + b[0] * b[0] + b[1] * b[1] + b[2] * b[2]);
+    const T u[3] = {p1[0] + (p1[1] * b[2] - p1[2] * b[1]), p1[1] + (p1[2] * b[0] - p1[0] * b[2]),
+                    p1[2] + (p1[0] * b[1] - p1[1] * b[0])};
+    const T p3[3] = {u[0] * co, u[1] * co, u[2] * co};
+    const T p2[3] = {p1[0] + e[0] + (p3[1] * b[2] - p3[2] * b[1]),
+                     p1[1] + e[1] + (p3[2] * b[0] - p3[0] * b[2]),
+                     p1[2] + e[2] + (p3[0] * b[1] - p3[1] * b[0])};
+    const T r2 = one / sqrt(one + p2[0] * p2[0] + p2[1] * p2[1] + p2[2] * p2[2]);
+    const T Vm[3] = {p2[0] * r2, p2[1] * r2, p2[2] * r2};
+    const T V[3] = {half * (Vm[0] + Vp[0]), half * (Vm[1] + Vp[1]), half * (Vm[2] + Vp[2])};
+    const T inv2 = one / (one - V[0]);
+    const T wq = w * inv2;
+    const T dJ0[3] = {a.djx0, a.djy0, a.djz0};
+    const T dq[3] = {wq * dJ0[0] * Vm[0], wq * dJ0[1] * Vm[1], wq * dJ0[2] * Vm[2]};
+    const T dy = V[1] * a.hxhy * inv2, dz = V[2] * a.hxhz * inv2;
+
+    // ---- sub-steps (cell-relative moves), kept for the backward pass
+    T sry[kMaxSub], srz[kMaxSub], sps[kMaxSub];
+    int sjb[kMaxSub], skb[kMaxSub];
+    int ns = 0;
+    {
+        T partdx = T(0), step = one;
+        const T ady = dy < T(0) ? -dy : dy, adz = dz < T(0) ? -dz : dz;
+        if (ady > one || adz > one) step = partdx = (ady > adz ? ady : adz);
+        if (partdx < one) partdx = step = one;
+        T ytmp = yp, ztmp = zp;
+        int jb = j, kb = k;
+        while (partdx > T(0) && ns < kMaxSub) {
+            T ps;
+            if (partdx > one) { partdx -= one; ps = one / step; }
+            else { ps = partdx / step; partdx = T(0); }
+            const T uy = ytmp + dy * ps, uz = ztmp + dz * ps;
+            const T fy = floor(uy), fz = floor(uz);
+            T ry = uy - fy, rz = uz - fz;
+            int sy = (int)fy, sz = (int)fz;
+            if (ry >= one) { ry = T(0); sy += 1; }
+            if (rz >= one) { rz = T(0); sz += 1; }
+            jb = wrap_m(jb + sy, My);
+            kb = wrap_m(kb + sz, Mz);
+            ytmp = ry;
+            ztmp = rz;
+            sry[ns] = ry; srz[ns] = rz; sps[ns] = ps; sjb[ns] = jb; skb[ns] = kb;
+            ns++;
+        }
+    }
+
+    // ---- backward through the sub-steps: deposits and position chain
+    T lyc = a.full ? a.lamPos[i] : T(0), lzc = a.full ? a.lamPos[a.n + i] : T(0);
+    T ldy = T(0), ldz = T(0);
+    T ldq[3] = {T(0), T(0), T(0)};
+    for (int q = ns - 1; q >= 0; q--) {
+        const T ry = sry[q], rz = srz[q], ps = sps[q];
+        const int jb = sjb[q], kb = skb[q];
+        const int jb1 = wrap_m(jb + 1, My), kb1 = wrap_m(kb + 1, Mz);
+        const size_t nd[4] = {(size_t)jb + (size_t)My * kb, (size_t)jb1 + (size_t)My * kb,
+                              (size_t)jb + (size_t)My * kb1, (size_t)jb1 + (size_t)My * kb1};
+        const T wc[4] = {(one - ry) * (one - rz), ry * (one - rz), (one - ry) * rz, ry * rz};
+        T lwc[4];
+#pragma unroll
+        for (int r = 0; r < 4; r++) {
+            T acc = T(0);
+#pragma unroll
+            for (int d = 0; d < 3; d++) {
+                const T G = ldg_(a.lamD + d * plane + nd[r]);
+                ldq[d] += ps * wc[r] * G;
+                acc += dq[d] * G;
+            }
+            lwc[r] = ps * acc;
+        }
+        const T lry = lyc + (one - rz) * (lwc[1] - lwc[0]) + rz * (lwc[3] - lwc[2]);
+        const T lrz = lzc + (one - ry) * (lwc[2] - lwc[0]) + ry * (lwc[3] - lwc[1]);
+        ldy += lry * ps;
+        ldz += lrz * ps;
+        lyc = lry;      // the position before this sub-step
+        lzc = lrz;
+    }
+    T lyp = lyc, lzp = lzc;
+
+    // ---- backward through the push
+    T bp2[3] = {T(0), T(0), T(0)};
+    if (a.full) {
+        bp2[0] = a.lamPm[i];
+        bp2[1] = a.lamPm[a.n + i];
+        bp2[2] = a.lamPm[2 * a.n + i];
+    }
+    T bVm[3], bwq = T(0);
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+        bVm[c] = wq * dJ0[c] * ldq[c];
+        bwq += ldq[c] * dJ0[c] * Vm[c];
+    }
+    // dy = Vy hxhy inv2, dz = Vz hxhz inv2
+    const T bVy = ldy * a.hxhy * inv2, bVz = ldz * a.hxhz * inv2;
+    const T binv2 = w * bwq + ldy * V[1] * a.hxhy + ldz * V[2] * a.hxhz;
+    const T bVx = inv2 * inv2 * binv2;    // inv2 = 1/(1 - Vx)
+    const T bV[3] = {bVx, bVy, bVz};
+    T bVp[3];
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+        bVm[c] += half * bV[c];
+        bVp[c] = half * bV[c];
+    }
+    {
+        const T br2 = bVm[0] * p2[0] + bVm[1] * p2[1] + bVm[2] * p2[2];
+        const T f = -r2 * r2 * r2 * br2;
+#pragma unroll
+        for (int c = 0; c < 3; c++) bp2[c] += r2 * bVm[c] + f * p2[c];
+    }
+    T bp1[3] = {bp2[0], bp2[1], bp2[2]};
+    T be[3] = {bp2[0], bp2[1], bp2[2]};
+    const T bp3[3] = {b[1] * bp2[2] - b[2] * bp2[1], b[2] * bp2[0] - b[0] * bp2[2],
+                      b[0] * bp2[1] - b[1] * bp2[0]};
+    T bb[3] = {bp2[1] * p3[2] - bp2[2] * p3[1], bp2[2] * p3[0] - bp2[0] * p3[2],
+               bp2[0] * p3[1] - bp2[1] * p3[0]};
+    const T bco = bp3[0] * u[0] + bp3[1] * u[1] + bp3[2] * u[2];
+    const T bu[3] = {co * bp3[0], co * bp3[1], co * bp3[2]};
+    bp1[0] += bu[0] + (b[1] * bu[2] - b[2] * bu[1]);
+    bp1[1] += bu[1] + (b[2] * bu[0] - b[0] * bu[2]);
+    bp1[2] += bu[2] + (b[0] * bu[1] - b[1] * bu[0]);
+    bb[0] += bu[1] * p1[2] - bu[2] * p1[1];
+    bb[1] += bu[2] * p1[0] - bu[0] * p1[2];
+    bb[2] += bu[0] * p1[1] - bu[1] * p1[0];
+    const T bq = -co * co * T(0.5) * bco;
+#pragma unroll
+    for (int c = 0; c < 3; c++) bb[c] += T(2) * b[c] * bq;
+    T bB[3];
+    T bkB = T(0);
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+        bB[c] = kB * bb[c];
+        bkB += B[c] * bb[c];
+    }
+    const T br1 = kE * bkB;
+    T bkE = r1 * bkB;
+    {
+        const T f = -r1 * r1 * r1 * br1;
+#pragma unroll
+        for (int c = 0; c < 3; c++) bp1[c] += f * p1[c];
+    }
+    T bp[3];
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+        bp[c] = bp1[c];
+        be[c] += bp1[c];
+    }
+    T bE[3];
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+        bE[c] = kE * be[c];
+        bkE += E[c] * be[c];
+    }
+    const T bia = a.sE * bkE;
+    bVp[0] += ia * ia * bia;              // ia = 1/(1 - Vp_x)
+    {
+        const T br0 = bVp[0] * p[0] + bVp[1] * p[1] + bVp[2] * p[2];
+        const T f = -r0 * r0 * r0 * br0;
+#pragma unroll
+        for (int c = 0; c < 3; c++) bp[c] += r0 * bVp[c] + f * p[c];
+    }
+    // ---- backward through the gather g_f = sum_r wg_r F_f,r
+    const T bg[6] = {bE[0], bE[1], bE[2], bB[0], bB[1], bB[2]};
+    T bwg[4] = {T(0), T(0), T(0), T(0)};
+#pragma unroll
+    for (int r = 0; r < 4; r++) {
+#pragma unroll
+        for (int f = 0; f < 6; f++) {
+            bwg[r] += bg[f] * F[f][r];
+            const T v = half * wg[r] * bg[f];
+            atomicAdd(a.lamFP + f * plane + nn[r], v);
+            atomicAdd(a.lamFC + f * plane + nn[r], v);
+        }
+    }
+    lyp += (one - zp) * (bwg[1] - bwg[0]) + zp * (bwg[3] - bwg[2]);
+    lzp += (one - yp) * (bwg[2] - bwg[0]) + yp * (bwg[3] - bwg[1]);
+    if (a.full) {
+        a.lamPm[i] = bp[0];
+        a.lamPm[a.n + i] = bp[1];
+        a.lamPm[2 * a.n + i] = bp[2];
+        a.lamPos[i] = lyp;
+        a.lamPos[a.n + i] = lzp;
+    } else {
+        a.lamPm[i] += bp[0];
+        a.lamPm[a.n + i] += bp[1];
+        a.lamPm[2 * a.n + i] += bp[2];
+        a.lamPos[i] += lyp;
+        a.lamPos[a.n + i] += lzp;
+    }
+}
+
+template <class T>
+int launch_push_adjoint_cic(const PushAdjArgs<T>& a, cudaStream_t st) {
+    if (a.n <= 0) return 0;
+    push_adjoint_cic_kernel<T><<<(unsigned)((a.n + 255) / 256), 256, 0, st>>>(a);
+    return 1;
+}
+
+__global__ void invert_ids_kernel(const int32_t* __restrict__ id, int64_t n,
+                                  int32_t* __restrict__ inv) {
+    const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p < n) {
+        const int32_t v = id[p];
+        if (v >= 0 && v < n) inv[v] = (int32_t)p;
+    }
+}
+
+template <class T>
+__global__ void permute_kernel(const int32_t* __restrict__ id_to, const int32_t* __restrict__ inv,
+                               int64_t n, const T* __restrict__ src, T* __restrict__ dst,
+                               int narr) {
+    const int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= n) return;
+    const int32_t v = id_to[q];
+    const int32_t p = (v >= 0 && v < n) ? inv[v] : -1;
+    for (int c = 0; c < narr; c++)
+        dst[(size_t)c * n + q] = (p >= 0 && p < n) ? src[(size_t)c * n + p] : T(0);
+}
+
+template <class T>
+int launch_permute_adjoint(const int32_t* id_from, const int32_t* id_to, int64_t n, int32_t* inv,
+                           const T* src, T* dst, int narr, cudaStream_t st) {
+    if (n <= 0) return 0;
+    const unsigned g = (unsigned)((n + 255) / 256);
+    invert_ids_kernel<<<g, 256, 0, st>>>(id_from, n, inv);
+    permute_kernel<T><<<g, 256, 0, st>>>(id_to, inv, n, src, dst, narr);
+    return 2;
+}
+
+// ---------------------------------------------------------------------------
 // per-mode adjoints of the spectral maps
 
 template <class T>
@@ -433,6 +713,9 @@ int launch_beam_weight_grad(const BeamGradArgs<T>& a, cudaStream_t st) {
 
 #define QS_ADJ_INST(T)                                                                   \
     template int launch_push_adjoint<T>(const PushAdjArgs<T>&, cudaStream_t);            \
+    template int launch_push_adjoint_cic<T>(const PushAdjArgs<T>&, cudaStream_t);        \
+    template int launch_permute_adjoint<T>(const int32_t*, const int32_t*, int64_t,      \
+                                           int32_t*, const T*, T*, int, cudaStream_t);   \
     template int launch_corrector_adjoint<T>(const AdjSpecArgs<T>&, cudaStream_t);       \
     template int launch_predictor_adjoint<T>(const AdjSpecArgs<T>&, cudaStream_t);       \
     template int launch_add_point<T>(T*, size_t, const T*, int, cudaStream_t);           \

@@ -257,6 +257,13 @@ struct Engine : EngineBase {
     T* lam_b3 = nullptr;        // (nx+1) x 2 planes: adjoint of the real beam currents
     T* d_dloss = nullptr;       // nx: d loss / d on-axis Ex of each layer
     double* d_gradw = nullptr;  // nb: d loss / d beam weight
+    // CIC adjoint: checkpointed cells and ids, the cells entering each layer of
+    // a segment, the position adjoint, and the reorder between checkpoints
+    bool cic_adj = false;
+    bool adj_recompute = false;   // recomputing a segment: keep the particle order
+    int32_t *ck_cell = nullptr, *ck_id = nullptr, *seg_cell = nullptr, *adj_inv = nullptr;
+    T* lam_pos = nullptr;
+    T* adj_tmp = nullptr;
     cudaGraphExec_t adj_exec = nullptr;   // captured sweep for the layers adj_lo .. head
     int adj_lo = -1;
     int64_t adj_graph_nb = -1;
@@ -274,7 +281,8 @@ struct Engine : EngineBase {
                         stage, stage_d, pcell, py, pz, ppx, ppy, ppz, pw, bi, bj, bk, bx, by, bz,
                         bpx, bpy, bpz, bw, d_err, ck, seg, lam, lam_pm, lam_sb, lam_b3,
                         d_dloss, d_gradw, acell, pid, apid, ay, az, apx, apy, apz, aw, cic_cnt,
-                        cic_loff, cic_bsum, cic_bpref, cic_ticket};
+                        cic_loff, cic_bsum, cic_bpref, cic_ticket, ck_cell, ck_id, seg_cell,
+                        adj_inv, lam_pos, adj_tmp};
         for (void* p : ptrs)
             if (p) cudaFree(p);
         if (st) cudaStreamDestroy(st);
@@ -1028,13 +1036,13 @@ struct Engine : EngineBase {
         if (cic_sort) {
             a.loff = cic_loff;
             a.bpref = cic_bpref;
-            regroup = full && grp.since + 1 >= cic_every;
+            regroup = full && !adj_recompute && grp.since + 1 >= cic_every;
             a.cnt = regroup ? cic_cnt : nullptr;   // the full push builds the histogram
         }
         const bool precise = sizeof(T) == 4;
         klaunch(KC_PUSH, [&] { return launch_push<T>(a, cfg.shape, precise, st); });
         CK(cudaGetLastError());
-        if (cic_sort && full) {
+        if (cic_sort && full && !adj_recompute) {
             if (regroup) {   // regroup before the next push
                 grp.grouped = false;
                 grp.off_valid = false;
@@ -1206,6 +1214,13 @@ struct Engine : EngineBase {
                            st));
         CK(cudaMemcpyAsync(b + 4 * plane, bankp(pb, SP_JX), 3 * plane * sizeof(T),
                            cudaMemcpyDeviceToDevice, st));
+        if (cic_adj) {   // CIC: the cells move, and the plasma is regrouped (ids)
+            CK(cudaMemcpyAsync(ck_cell + (size_t)m * np, pcell, np * sizeof(int32_t),
+                               cudaMemcpyDeviceToDevice, st));
+            if (cic_sort)
+                CK(cudaMemcpyAsync(ck_id + (size_t)m * np, pid, np * sizeof(int32_t),
+                                   cudaMemcpyDeviceToDevice, st));
+        }
         return QS_OK;
     }
 
@@ -1220,6 +1235,21 @@ struct Engine : EngineBase {
                            st));
         CK(cudaMemcpyAsync(bankp(pb, SP_JX), b + 4 * plane, 3 * plane * sizeof(T),
                            cudaMemcpyDeviceToDevice, st));
+        if (cic_adj) {
+            CK(cudaMemcpyAsync(pcell, ck_cell + (size_t)m * np, np * sizeof(int32_t),
+                               cudaMemcpyDeviceToDevice, st));
+            if (cic_sort) {
+                CK(cudaMemcpyAsync(pid, ck_id + (size_t)m * np, np * sizeof(int32_t),
+                                   cudaMemcpyDeviceToDevice, st));
+                // the recomputation keeps this order (no regrouping): fresh
+                // counts and offsets for it
+                CK(cudaMemsetAsync(cic_cnt, 0, plane * sizeof(int), st));
+                grp.grouped = true;
+                grp.off_valid = false;
+                grp.counted = false;
+                grp.since = 0;
+            }
+        }
         return QS_OK;
     }
 
@@ -1227,13 +1257,13 @@ struct Engine : EngineBase {
         if (every < 0) return fail(QS_ERR_INVALID, "qs_adjoint_checkpoints: every must be >= 0");
         if (every > 0 && S != 1)
             return fail(QS_ERR_UNSUPPORTED, "the adjoint supports NxSplit = 1");
-        if (every > 0 && cfg.shape != QS_SHAPE_NGP)
-            return fail(QS_ERR_UNSUPPORTED, "the adjoint supports the NGP shape");
         CK(cudaStreamSynchronize(st));
-        void* old[] = {ck, seg, lam, lam_pm, lam_sb, lam_b3, d_dloss};
+        void* old[] = {ck, seg, lam, lam_pm, lam_sb, lam_b3, d_dloss, ck_cell, ck_id, seg_cell,
+                       lam_pos, adj_inv, adj_tmp};
         for (void* p : old)
             if (p) cudaFree(p);
-        ck = seg = lam = lam_pm = lam_sb = lam_b3 = d_dloss = nullptr;
+        ck = seg = lam = lam_pm = lam_sb = lam_b3 = d_dloss = lam_pos = adj_tmp = nullptr;
+        ck_cell = ck_id = seg_cell = adj_inv = nullptr;
         ck_every = 0;
         ck_valid = false;
         if (gexec) {   // the captured march has (or lacks) the checkpoint copies
@@ -1254,6 +1284,17 @@ struct Engine : EngineBase {
         if ((s = alloc(&lam_sb, (size_t)(L + 1) * 2 * plane, "adjoint beam spectra"))) return s;
         if ((s = alloc(&lam_b3, (size_t)(L + 1) * 2 * plane, "adjoint beam currents"))) return s;
         if ((s = alloc(&d_dloss, (size_t)L, "loss gradient"))) return s;
+        cic_adj = cfg.shape == QS_SHAPE_CIC;
+        if (cic_adj) {
+            if ((s = alloc(&ck_cell, (size_t)ck_count * np, "adjoint checkpoints"))) return s;
+            if ((s = alloc(&seg_cell, (size_t)K * np, "adjoint segment"))) return s;
+            if ((s = alloc(&lam_pos, 2 * (size_t)np, "adjoint positions"))) return s;
+            if (cic_sort) {
+                if ((s = alloc(&ck_id, (size_t)ck_count * np, "adjoint checkpoints"))) return s;
+                if ((s = alloc(&adj_inv, (size_t)np, "adjoint reorder"))) return s;
+                if ((s = alloc(&adj_tmp, 5 * (size_t)np, "adjoint reorder"))) return s;
+            }
+        }
         ck_every = K;
         return QS_OK;
     }
@@ -1276,11 +1317,15 @@ struct Engine : EngineBase {
     // each layer's entry particles and intermediate C fields
     qs_status recompute_segment(int m, int c, int lo) {
         in_march = true;
+        adj_recompute = true;
         qs_status s = restore_checkpoint(m);
         for (int i = c; !s && i >= lo; i--) {
             T* slot = seg + (size_t)(c - i) * seg_stride();
             for (int q = 0; q < 5; q++)
                 CK(cudaMemcpyAsync(slot + (size_t)q * np, particle_arrays(q), np * sizeof(T),
+                                   cudaMemcpyDeviceToDevice, st));
+            if (cic_adj)
+                CK(cudaMemcpyAsync(seg_cell + (size_t)(c - i) * np, pcell, np * sizeof(int32_t),
                                    cudaMemcpyDeviceToDevice, st));
             T* fs = slot + 5 * (size_t)np;
             if ((s = layer_begin(i, 0))) break;
@@ -1298,6 +1343,7 @@ struct Engine : EngineBase {
             if ((s = layer_end(i, 0))) break;
         }
         in_march = false;
+        adj_recompute = false;
         return s;
     }
 
@@ -1322,10 +1368,12 @@ struct Engine : EngineBase {
         return a;
     }
 
-    PushAdjArgs<T> push_adj_args(const T* slot, const T* Cfield, int full) {
+    PushAdjArgs<T> push_adj_args(const T* slot, const int32_t* slot_cell, const T* Cfield,
+                                 int full) {
         PushAdjArgs<T> a{};
         a.n = np; a.My = My; a.Mz = Mz;
-        a.cell = pcell;
+        a.cell = cic_adj ? slot_cell : pcell;   // NGP: the seeded cells never change
+        a.lamPos = lam_pos;
         a.y = slot; a.z = slot + np; a.px = slot + 2 * np; a.py = slot + 3 * np;
         a.pz = slot + 4 * np; a.w = pw;
         a.P = Pf; a.C = Cfield;
@@ -1344,7 +1392,11 @@ struct Engine : EngineBase {
     }
 
     // reverse sweep over one layer (the transpose of move_split_layer)
-    qs_status adjoint_layer(int i, const T* slot) {
+    int push_adjoint(const PushAdjArgs<T>& a) {
+        return cic_adj ? launch_push_adjoint_cic<T>(a, st) : launch_push_adjoint<T>(a, st);
+    }
+
+    qs_status adjoint_layer(int i, const T* slot, const int32_t* slot_cell) {
         const int EBz[6] = {CC, CC, SS, SS, SS, CC}, EBy[6] = {CC, SS, CC, SS, CC, SS};
         const int Jz[3] = {CC, CC, SS}, Jy[3] = {CC, SS, CC};
         const T* fs = slot + 5 * (size_t)np;
@@ -1375,7 +1427,7 @@ struct Engine : EngineBase {
         adj_xform(lamp(LAM_J), lamp(LAM_D), 3, Jz, Jy, T(1));
         CK(cudaMemsetAsync(lamp(LAM_CX), 0, 6 * plane * sizeof(T), st));
         klaunch(KC_PUSH, [&] {
-            return launch_push_adjoint<T>(push_adj_args(slot, fs + (size_t)nIter * 6 * plane, 1), st);
+            return push_adjoint(push_adj_args(slot, slot_cell, fs + (size_t)nIter * 6 * plane, 1));
         });
         int rho_in = LAM_RHO0;
         for (int it = nIter - 1; it >= 0; it--) {
@@ -1396,8 +1448,7 @@ struct Engine : EngineBase {
             adj_xform(lamp(LAM_J), lamp(LAM_D), 3, Jz, Jy, T(1));
             CK(cudaMemsetAsync(lamp(LAM_CX), 0, 6 * plane * sizeof(T), st));
             klaunch(KC_PUSH, [&] {
-                return launch_push_adjoint<T>(push_adj_args(slot, fs + (size_t)it * 6 * plane, 0),
-                                              st);
+                return push_adjoint(push_adj_args(slot, slot_cell, fs + (size_t)it * 6 * plane, 0));
             });
         }
         // Guess: C fields <- inverse transforms of the predicted E, B
@@ -1427,6 +1478,7 @@ struct Engine : EngineBase {
     qs_status adjoint_device(int lo) {
         CK(cudaMemsetAsync(lam, 0, (size_t)LAM_N * plane * sizeof(T), st));
         CK(cudaMemsetAsync(lam_pm, 0, 3 * (size_t)np * sizeof(T), st));
+        if (lam_pos) CK(cudaMemsetAsync(lam_pos, 0, 2 * (size_t)np * sizeof(T), st));
         CK(cudaMemsetAsync(lam_sb, 0, (size_t)(L + 1) * 2 * plane * sizeof(T), st));
         int first = L + 1;   // lowest beam-spectrum layer the sweep touches
         if (lo >= 0) {
@@ -1435,11 +1487,32 @@ struct Engine : EngineBase {
             for (int m = mlo; m >= 0; m--) {
                 const int c = L - 1 - m * K;
                 const int end = std::max(c - K + 1, lo);
+                if (m < mlo && cic_adj && cic_sort) {
+                    // the particle adjoints are in checkpoint m+1's order (the
+                    // forward regrouped the plasma since checkpoint m): carry
+                    // them to checkpoint m's order, which the recomputation keeps
+                    CK(cudaMemcpyAsync(adj_tmp, lam_pm, 3 * (size_t)np * sizeof(T),
+                                       cudaMemcpyDeviceToDevice, st));
+                    CK(cudaMemcpyAsync(adj_tmp + 3 * (size_t)np, lam_pos,
+                                       2 * (size_t)np * sizeof(T), cudaMemcpyDeviceToDevice, st));
+                    klaunch(KC_MISC, [&] {
+                        return launch_permute_adjoint<T>(ck_id + (size_t)(m + 1) * np,
+                                                         ck_id + (size_t)m * np, np, adj_inv,
+                                                         adj_tmp, lam_pm, 3, st);
+                    });
+                    klaunch(KC_MISC, [&] {
+                        return launch_permute_adjoint<T>(ck_id + (size_t)(m + 1) * np,
+                                                         ck_id + (size_t)m * np, np, adj_inv,
+                                                         adj_tmp + 3 * (size_t)np, lam_pos, 2,
+                                                         st);
+                    });
+                }
                 cur = 0;
                 qs_status s = recompute_segment(m, c, end);
                 if (s) return s;
                 for (int i = end; i <= c; i++) {
-                    if ((s = adjoint_layer(i, seg + (size_t)(c - i) * seg_stride()))) return s;
+                    const int32_t* sc = cic_adj ? seg_cell + (size_t)(c - i) * np : nullptr;
+                    if ((s = adjoint_layer(i, seg + (size_t)(c - i) * seg_stride(), sc))) return s;
                 }
             }
             first = lo;

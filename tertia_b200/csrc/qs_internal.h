@@ -135,12 +135,21 @@ struct PushAdjArgs {
     T* lamPm;             // 3 x n
     T* lamFP;             // 6 planes
     T* lamFC;             // 6 planes
+    T* lamPos;            // CIC: 2 x n adjoint of the in-cell positions y, z (like lamPm)
     size_t plane;
     T sE, hxhy, hxhz, djx0, djy0, djz0, bxe, bye, bze;
     int full, precise;
 };
 template <class T>
 int launch_push_adjoint(const PushAdjArgs<T>& a, cudaStream_t st);
+template <class T>
+int launch_push_adjoint_cic(const PushAdjArgs<T>& a, cudaStream_t st);
+// dst[q] = src[inv[id_to[q]]] for `narr` arrays of n values (T), after
+// inv[id_from[p]] = p: carries per-particle adjoints from one particle order
+// to another
+template <class T>
+int launch_permute_adjoint(const int32_t* id_from, const int32_t* id_to, int64_t n, int32_t* inv,
+                           const T* src, T* dst, int narr, cudaStream_t st);
 
 // Per-mode adjoint of the predictor / corrector.  Inputs (any may be null =
 // zero): lRho, lE (+ lEb, a second contribution), lB, lJb (adjoint of the

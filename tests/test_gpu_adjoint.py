@@ -11,7 +11,7 @@ import pytest
 import torch
 
 from tertia_b200 import workload as wl
-from tertia_b200.abi import PRECISIONS, QsError
+from tertia_b200.abi import PRECISIONS, QS_SHAPE_CIC, QS_SHAPE_NGP, QsError
 from tertia_b200.autograd import wake_loss, xi_bins
 
 pytestmark = pytest.mark.gpu
@@ -19,9 +19,9 @@ pytestmark = pytest.mark.gpu
 NBINS = 8
 
 
-def setup(prec, layers=48, n=32, every=8):
+def setup(prec, layers=48, n=32, every=8, shape=QS_SHAPE_NGP):
     from tertia_b200.mesh import Mesh
-    cfg = wl.small_config(n=n, layers=layers, ts=0.0, synchrotron=0)
+    cfg = wl.small_config(n=n, layers=layers, ts=0.0, synchrotron=0, shape=shape)
     cfg.precision = PRECISIONS[prec]
     beam = wl.small_beam(cfg, n=4000, nb=0.3)
     x = (beam["i"] + beam["x"]) * cfg.hx
@@ -96,3 +96,38 @@ def test_adjoint_checkpoint_interval_does_not_change_gradient():
         out.append(adjoint_grad(m, beam, bins, coeff, beta))
         m.close()
     assert rel(out[0], out[1]) < 1e-9    # atomic order of the FP64 deposits only
+
+
+# ---- CIC: the particles also carry the adjoint of their in-cell position,
+# and the FP32 path regroups the plasma by cell between checkpoints
+
+def test_cic_adjoint_fp64_matches_finite_differences():
+    cfg, m, beam, bins, coeff = setup("fp64", shape=QS_SHAPE_CIC)
+    beta = np.random.default_rng(8).uniform(0.5, 1.5, NBINS)
+    g = adjoint_grad(m, beam, bins, coeff, beta)
+    fd = fd_grad(m, beam, bins, coeff, beta)
+    assert np.linalg.norm(fd) > 0
+    assert rel(g, fd) < 1e-4, (g, fd)
+    m.close()
+
+
+def test_cic_adjoint_fp32_close_to_fp64_adjoint():
+    """FP32 CIC regroups the plasma by cell every second full push; the
+    adjoint carries the particle adjoints across those reorderings."""
+    beta = np.random.default_rng(9).uniform(0.5, 1.5, NBINS)
+    grads = {}
+    for prec in ("fp64", "fp32"):
+        cfg, m, beam, bins, coeff = setup(prec, shape=QS_SHAPE_CIC)
+        grads[prec] = adjoint_grad(m, beam, bins, coeff, beta)
+        m.close()
+    assert rel(grads["fp32"], grads["fp64"]) < 1e-4, grads
+
+
+def test_cic_adjoint_checkpoint_interval_fp32():
+    beta = np.random.default_rng(10).uniform(0.5, 1.5, NBINS)
+    out = []
+    for every in (5, 48):
+        cfg, m, beam, bins, coeff = setup("fp32", every=every, shape=QS_SHAPE_CIC)
+        out.append(adjoint_grad(m, beam, bins, coeff, beta))
+        m.close()
+    assert rel(out[0], out[1]) < 1e-5
