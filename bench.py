@@ -181,18 +181,18 @@ def cpu_sample(w, target_s: float):
 
 # ------------------------------------------------------------------ adjoint (c3)
 def adjoint_measure(precision: str):
-    """The c3 adjoint: 256 x 256 x 2048, 4 ppc, NGP, 1e6-particle driver whose
+    """The c3 adjoint: 256 x 256 x 2048, 4 ppc, CIC, 1e6-particle driver whose
     charge profile is 64 xi-bins with seeded weights in [0.5, 1.5]; loss = on-axis
     Ex integrated over the witness window xi in [-6, -5] behind the driver
     centre; layer checkpoints every 32 layers.  Reports the forward march and
     the adjoint times (device events), their ratio, the ratio over the same
     layer range (the sweep covers only the layers from the head to the window),
-    and the gradient against central differences (h = 1e-3) on a few bins and
-    against the FP64 adjoint on all bins."""
+    and the gradient against central differences (h = 1e-3) on a few bins, in
+    the same precision and in FP64, and against the FP64 adjoint on all bins."""
     import numpy as np
     import torch
     from tertia_b200 import workload as wl
-    from tertia_b200.abi import PRECISIONS, QS_SHAPE_NGP
+    from tertia_b200.abi import QS_SHAPE_CIC
     from tertia_b200.autograd import xi_bins
     from tertia_b200.mesh import Mesh
 
@@ -201,7 +201,12 @@ def adjoint_measure(precision: str):
     def setup(prec):
         w = wl.make_workload("c3", prec)
         cfg = w.cfg
-        cfg.shape = QS_SHAPE_NGP
+        cfg.shape = QS_SHAPE_CIC
+        # the beam is deposited where it stands (no beam motion, no
+        # radiation loss): the loss is then a function of the bin weights
+        # alone, not of the fields an earlier march left for the beam push
+        cfg.ts = 0.0
+        cfg.synchrotron = 0
         beam = wl.workload_beam(w)
         xc = wl.driver_center_x(cfg, w.beams[0].sigma_xi)
         sx = w.beams[0].sigma_xi
@@ -252,26 +257,42 @@ def adjoint_measure(precision: str):
     swept = cfg.nx - lo
     # central differences on the 4 bins with the largest gradient
     top = np.argsort(-np.abs(g))[:4]
-    fd = []
-    for b in top:
-        bp, bm = beta.copy(), beta.copy()
-        bp[b] += h
-        bm[b] -= h
-        fd.append((forward(m, beam, bins, coeff, bp) - forward(m, beam, bins, coeff, bm)) / (2 * h))
-    fd = np.array(fd)
+
+    def fd_of(mm):
+        out = []
+        for b in top:
+            bp, bm = beta.copy(), beta.copy()
+            bp[b] += h
+            bm[b] -= h
+            out.append((forward(mm, beam, bins, coeff, bp) - forward(mm, beam, bins, coeff, bm))
+                       / (2 * h))
+        return np.array(out)
+
+    fd = fd_of(m)
     m.close()
+    cfg32, m32, beam32, bins32, coeff32 = setup("fp32")
+    g32 = grad(m32, beam32, bins32, coeff32, beta)
+    m32.close()
     cfg64, m64, beam64, bins64, coeff64 = setup("fp64")
     g64 = grad(m64, beam64, bins64, coeff64, beta)
+    fd64 = fd_of(m64)
     m64.close()
     rel = lambda a, b: float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
-    return {"workload": "c3: 256x256x2048 NGP, 64 xi-bins, witness window xi in [-6, -5], "
+    return {"workload": "c3: 256x256x2048 CIC, 64 xi-bins, witness window xi in [-6, -5], "
+                        "beam deposited in place (Ts = 0), "
                         f"checkpoints every {every} layers",
             "precision": precision, "forward_ms": fwd_ms, "adjoint_ms": adj_ms,
             "adjoint_over_forward": adj_ms / fwd_ms,
             "layers_swept": swept, "layers": cfg.nx,
             "adjoint_over_forward_same_layers": adj_ms / (fwd_ms * swept / cfg.nx),
             "grad_rel_err_vs_fd_top4": rel(g[top], fd),
+            "grad_rel_err_vs_fp64_fd_top4": rel(g[top], fd64),
             "grad_rel_err_vs_fp64_adjoint": rel(g, g64),
+            "fp32_grad_rel_err_vs_fp64_fd_top4": rel(g32[top], fd64),
+            "fp32_grad_rel_err_vs_fp64_adjoint": rel(g32, g64),
+            "fp64_adjoint_rel_err_vs_fp64_fd_top4": rel(g64[top], fd64),
+            "fd_note": "central differences of the loss; in BF16x3 they carry the FP32 rounding "
+                       "of the loss divided by 2h, hence the FP64 differences as reference",
             "fd_step": h, "loss_note": "loss = sum over window layers of hx * on-axis Ex",
             "timing": "forward: device events around the march; adjoint: host wall clock "
                       "around qs_adjoint (it synchronises)"}

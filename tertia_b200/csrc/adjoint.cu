@@ -254,9 +254,9 @@ int launch_push_adjoint(const PushAdjArgs<T>& a, cudaStream_t st) {
 // depend on the in-cell position (y, z) and the deposit weights on the
 // position after the move, so besides the momentum adjoint the particle
 // carries the adjoint of its position (lamPos); cells come from floor() and
-// carry none.  The sub-step partition (its number and fractions) is held
-// fixed: exact for the usual single sub-step, first order for |dy|, |dz|
-// above one cell per layer.  Up to kMaxSub sub-steps are differentiated.
+// carry none.  The sub-step fractions are differentiated through the step
+// length when |dy| or |dz| exceeds one cell per layer (the number of
+// sub-steps is piecewise constant).  Up to kMaxSub sub-steps are followed.
 constexpr int kMaxSub = 8;
 
 template <class T>
@@ -318,21 +318,41 @@ __global__ void __launch_bounds__(256) push_adjoint_cic_kernel(PushAdjArgs<T> a)
     const T dq[3] = {wq * dJ0[0] * Vm[0], wq * dJ0[1] * Vm[1], wq * dJ0[2] * Vm[2]};
     const T dy = V[1] * a.hxhy * inv2, dz = V[2] * a.hxhz * inv2;
 
-    // ---- sub-steps (cell-relative moves), kept for the backward pass
-    T sry[kMaxSub], srz[kMaxSub], sps[kMaxSub];
+    // ---- sub-steps (cell-relative moves), kept for the backward pass.  With
+    // |dy| or |dz| above one cell the step is the larger of the two and each
+    // sub-step's fraction ps depends on it: d ps / d step is -1/step^2 for the
+    // full sub-steps and nfull/step^2 for the last one.
+    T sry[kMaxSub], srz[kMaxSub], sps[kMaxSub], sdps[kMaxSub];
     int sjb[kMaxSub], skb[kMaxSub];
     int ns = 0;
+    T dstep_dy = T(0), dstep_dz = T(0), step = one;
     {
-        T partdx = T(0), step = one;
+        T partdx = T(0);
         const T ady = dy < T(0) ? -dy : dy, adz = dz < T(0) ? -dz : dz;
-        if (ady > one || adz > one) step = partdx = (ady > adz ? ady : adz);
-        if (partdx < one) partdx = step = one;
+        if (ady > one || adz > one) {
+            step = partdx = (ady > adz ? ady : adz);
+            if (ady > adz) dstep_dy = dy < T(0) ? -one : one;
+            else dstep_dz = dz < T(0) ? -one : one;
+        }
+        if (partdx < one) {
+            partdx = step = one;
+            dstep_dy = dstep_dz = T(0);
+        }
         T ytmp = yp, ztmp = zp;
         int jb = j, kb = k;
+        int nfull = 0;
         while (partdx > T(0) && ns < kMaxSub) {
             T ps;
-            if (partdx > one) { partdx -= one; ps = one / step; }
-            else { ps = partdx / step; partdx = T(0); }
+            if (partdx > one) {
+                partdx -= one;
+                ps = one / step;
+                sdps[ns] = -ps / step;
+                nfull++;
+            } else {
+                ps = partdx / step;
+                partdx = T(0);
+                sdps[ns] = T(nfull) / (step * step);
+            }
             const T uy = ytmp + dy * ps, uz = ztmp + dz * ps;
             const T fy = floor(uy), fz = floor(uz);
             T ry = uy - fy, rz = uz - fz;
@@ -350,10 +370,11 @@ __global__ void __launch_bounds__(256) push_adjoint_cic_kernel(PushAdjArgs<T> a)
 
     // ---- backward through the sub-steps: deposits and position chain
     T lyc = a.full ? a.lamPos[i] : T(0), lzc = a.full ? a.lamPos[a.n + i] : T(0);
-    T ldy = T(0), ldz = T(0);
+    T ldy = T(0), ldz = T(0), lstep = T(0);
     T ldq[3] = {T(0), T(0), T(0)};
     for (int q = ns - 1; q >= 0; q--) {
         const T ry = sry[q], rz = srz[q], ps = sps[q];
+        T lps = T(0);
         const int jb = sjb[q], kb = skb[q];
         const int jb1 = wrap_m(jb + 1, My), kb1 = wrap_m(kb + 1, Mz);
         const size_t nd[4] = {(size_t)jb + (size_t)My * kb, (size_t)jb1 + (size_t)My * kb,
@@ -370,15 +391,20 @@ __global__ void __launch_bounds__(256) push_adjoint_cic_kernel(PushAdjArgs<T> a)
                 acc += dq[d] * G;
             }
             lwc[r] = ps * acc;
+            lps += wc[r] * acc;
         }
         const T lry = lyc + (one - rz) * (lwc[1] - lwc[0]) + rz * (lwc[3] - lwc[2]);
         const T lrz = lzc + (one - ry) * (lwc[2] - lwc[0]) + ry * (lwc[3] - lwc[1]);
         ldy += lry * ps;
         ldz += lrz * ps;
+        lps += lry * dy + lrz * dz;      // u = y + d ps
+        lstep += lps * sdps[q];
         lyc = lry;      // the position before this sub-step
         lzc = lrz;
     }
     T lyp = lyc, lzp = lzc;
+    ldy += lstep * dstep_dy;
+    ldz += lstep * dstep_dz;
 
     // ---- backward through the push
     T bp2[3] = {T(0), T(0), T(0)};
