@@ -170,6 +170,46 @@ qs_status qs_load_front_plasma(qs_handle* h, int64_t n, const int32_t* cell,
  * P0 + N(0, Pspread) from a counter-based generator keyed by (seed, step). */
 qs_status qs_seed_front_plasma(qs_handle* h, uint64_t step);
 int64_t qs_plasma_count(const qs_handle* h);
+
+/* Plasma density profile: Specie::Density (plasma.cpp:6-399) with the
+ * namelist values of Specie (elements.cpp:11-58).  Coordinates as in the
+ * reference: x from the left X boundary plus the phase (the distance the box
+ * has moved), y and z from the axis.  distribution (i_Distribution):
+ *   0 trapezoid, 1 Gaussian ellipsoid, 2 Gaussian channel, 3 curved Gaussian
+ *   channel, 4 parallelepiped, 5 exponential, 6 empty channel, 7 COS-GAUSS,
+ *   8 tanh step, 9 rod, 10 linear step, 11 gradient, 12 periodic. */
+typedef struct qs_density_profile {
+    int32_t distribution;
+    int32_t reserved;                            /* 0                          */
+    double density, density1;                    /* Density, Density1          */
+    double begin, end, plateau_begin, plateau_end;
+    double scale, delta;                         /* Scale, Delta               */
+    double radius, radius_x, radius_y, radius_z;
+    double x0, y0, z0;
+    double xperiod, yperiod, zperiod;
+    double angle_y;                              /* AngleY                     */
+    double y_curvature, z_curvature;             /* Ycurvature, Zcurvature     */
+    double curvature_begin, curvature_end;       /* CurvatureBegin/End         */
+} qs_density_profile;
+
+/* A uniform profile: distribution 0 with density 1 from x = 0 on. */
+qs_status qs_density_profile_default(qs_density_profile* p);
+/* Set the plasma profile (NULL: the uniform cfg.plasma_density again).  With
+ * a profile, qs_seed_front_plasma gives the particles of cell (j, k) the
+ * weight Density(x_front, y_j, z_k)/ppc at the front x = Hx*nx + phase
+ * (mesh.cpp:413-431,471) and weight 0 where the density is not positive (the
+ * reference seeds no particle there; a zero weight deposits exact zeros), and
+ * the Guess/Iterate maps take |Density*q2m| on axis at the head layer
+ * x = Hx*(nx-1) + phase (movefieldshydrolinlayersplit.cpp:236-250; 0 -> 1).
+ * Distribution 12 needs xperiod > 0 (the reference loops forever otherwise). */
+qs_status qs_set_density_profile(qs_handle* h, const qs_density_profile* p);
+/* Specie::Density of the profile set on h at (x, y, z), evaluated on the host
+ * (the uniform density when none is set). */
+qs_status qs_plasma_density(qs_handle* h, double x, double y, double z, double* out);
+/* Phase (Controls f_Phase): the distance the box has moved; qs_step adds Ts
+ * before its beam push (step.cpp:33). */
+qs_status qs_set_phase(qs_handle* h, double phase);
+qs_status qs_get_phase(qs_handle* h, double* phase);
 /* Plasma particles of the layer in flight (after a march: layer 0). */
 qs_status qs_get_plasma(qs_handle* h, int64_t n, int32_t* cell,
                         double* y, double* z, double* px, double* py,

@@ -141,6 +141,12 @@ def _declare(L):
         getattr(L, name).argtypes = [P, C.c_int, C.c_int]
     L.qso_move_particles_layer.argtypes = [P, C.c_int, C.c_int, C.c_int]
     L.qso_iterate_fields.argtypes = [P, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_double)]
+    from tertia_b200.abi import QsDensityProfile
+    L.qso_density.argtypes = [C.POINTER(QsDensityProfile), C.c_double, C.c_double, C.c_double]
+    L.qso_density.restype = C.c_double
+    L.qso_set_density_profile.argtypes = [P, C.POINTER(QsDensityProfile)]
+    L.qso_set_phase.argtypes = [P, C.c_double]
+    L.qso_front_weights.argtypes = [P, _f64p]
     L.qso_dtt1d.argtypes = [C.c_int, C.c_int, _f64p, _f64p, C.c_int]
     L.qso_transform2d.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _f64p, _f64p, C.c_int]
     L.qso_push_layer_f64.argtypes = [C.POINTER(QsConfig), C.c_int64, _i32p] + [_f64p] * 9 + [
@@ -203,6 +209,11 @@ def push_layer(cfg, cell, y, z, px, py, pz, w, P, C_, dep=None, full=False, prec
                 dep_cell=dep_cell)
 
 
+def density(prof, x: float, y: float, z: float) -> float:
+    """Oracle Specie::Density of a QsDensityProfile at (x, y, z)."""
+    return float(lib().qso_density(C.byref(prof), float(x), float(y), float(z)))
+
+
 class Oracle:
     """The oracle mesh: same call surface as tertia_b200.Mesh."""
 
@@ -226,6 +237,19 @@ class Oracle:
 
     def _plane_out(self):
         return np.empty(self.plane, dtype=np.float64)
+
+    def set_density_profile(self, prof):
+        _check(lib().qso_set_density_profile(self._h, C.byref(prof) if prof is not None
+                                             else None), "qso_set_density_profile")
+
+    def set_phase(self, phase: float):
+        _check(lib().qso_set_phase(self._h, float(phase)), "qso_set_phase")
+
+    def front_weights(self):
+        """Weights SeedParticles gives each cell's front particles (ny*nz)."""
+        out = self._plane_out()
+        _check(lib().qso_front_weights(self._h, out), "qso_front_weights")
+        return out
 
     def load_beam(self, b):
         n = len(b["x"])

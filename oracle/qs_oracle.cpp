@@ -543,6 +543,194 @@ extern "C" void qso_corrector_modes(int ny, int nz, double hx, double d, double 
         }
 }
 
+// ---- Specie::Density (plasma.cpp:6-399).  The Specie members the reference
+// defaults on the fly (Radius, RadiusX/Y/Z, Scale) are defaulted in a copy
+// first, as after the reference's first call; the periodic reductions are
+// the reference's loops (bounded).
+struct SpecieProfile {
+    qs_density_profile q;
+    explicit SpecieProfile(const qs_density_profile& p) : q(p) {}
+
+    static double wrap_up(double v, double P, long cap = 100000000L) {
+        while (v > P && cap-- > 0) v -= P;
+        while (v < 0. && cap-- > 0) v += P;
+        return v;
+    }
+    static double wrap_mid(double v, double P, long cap = 100000000L) {
+        while (v > P / 2. && cap-- > 0) v -= P;
+        while (v <= -P / 2. && cap-- > 0) v += P;
+        return v;
+    }
+
+    double operator()(double xco, double yco, double zco) {
+        const double PI_ = 3.1415927;  // domain.h:10
+        double tmp = 0.;
+        double density = q.density, density1 = q.density1;
+        double arg, r2;
+        switch (q.distribution) {
+        case 12:
+            if (xco < q.begin || xco > q.end) return tmp;
+            if (xco < q.plateau_begin) {
+                if (q.scale <= 0) q.scale = 1;
+                return density * exp((xco - q.plateau_begin) / q.scale);
+            }
+            if (xco > q.plateau_end) return density * (q.end - xco) / (q.end - q.plateau_end);
+            if (density1 < 0) density1 = 0.;
+            return wrap_up(xco, q.xperiod) > q.xperiod - q.delta ? density1 : density;
+        case 11:
+            if (xco < 0. || xco < q.begin || xco > q.end) return 0.;
+            if (xco < q.plateau_begin) return density * (xco - q.begin) / (q.plateau_begin - q.begin);
+            if (xco < q.plateau_end) return density * exp((xco - q.plateau_begin) / q.delta);
+            if (xco > q.plateau_end) return density * (q.end - xco) / (q.end - q.plateau_end);
+            return 0.;
+        case 10:
+            if (xco < 0. || xco < q.begin || xco > q.end) return tmp;
+            if (xco < q.plateau_begin) return q.density;
+            if (xco < q.plateau_end)
+                return density + density * q.delta * (xco - q.plateau_begin) /
+                                     (q.plateau_end - q.plateau_begin);
+            if (xco > q.plateau_end) return density * (1. + q.delta);
+            return 0.;
+        case 9:
+            if (xco < q.begin || xco > q.end) return 0.;
+            yco = yco + q.angle_y * (xco - q.begin);
+            if (q.yperiod > 0.) yco = wrap_mid(yco, q.yperiod);
+            if (q.zperiod > 0.) zco = wrap_mid(zco, q.zperiod);
+            if (q.radius <= 0.) q.radius = 1.;
+            if (q.radius_x <= 0.) q.radius_x = q.radius;
+            if (q.radius_y == 0.) q.radius_y = q.radius;
+            if (q.radius_z == 0.) q.radius_z = q.radius;
+            arg = (yco - q.y0) * (yco - q.y0) / q.radius_y / q.radius_y +
+                  (zco - q.z0) * (zco - q.z0) / q.radius_z / q.radius_z;
+            if (q.xperiod > 0.) arg *= 1 + q.delta * sin(2. * PI_ * xco / q.xperiod);
+            if ((q.radius_y > 0 || q.radius_z > 0) && arg > 1) return 0.;
+            if ((q.radius_y < 0 || q.radius_z < 0) && arg < 1) return 0.;
+            return q.density;
+        case 8:
+            if (xco < 0. || xco < q.begin || xco > q.end) return tmp;
+            r2 = yco * yco + zco * zco;
+            if (r2 > q.radius * q.radius) return tmp;
+            if (q.radius_x <= 0.) q.radius_x = 1.;
+            density = 0.5 * (1. - tanh((xco - q.x0) / q.radius_x));
+            return q.density * density;
+        case 7: {
+            if (xco < 0. || xco < q.begin || xco > q.end) return tmp;
+            if (q.radius <= 0.) q.radius = 1.;
+            if (q.radius_x <= 0.) q.radius_x = q.radius;
+            if (q.radius_y <= 0.) q.radius_y = q.radius;
+            if (q.radius_z <= 0.) q.radius_z = q.radius;
+            double front = q.end - q.x0;
+            front = front < q.radius_x ? 1 : q.radius_x * 100.;
+            double arg_front = 0.;
+            if (xco > q.x0) arg_front = (xco - q.x0) / front;
+            arg_front *= arg_front / 2.;
+            arg = (xco - q.x0) / q.radius_x;
+            if (fabs(arg) > sqrt(2. * PI_)) return tmp;
+            density = 0.5 * (1 + cos(sqrt(PI_ / 2.) * arg));
+            double modulation = q.xperiod != 0. ? 1. + q.delta * cos(2 * PI_ * xco / q.xperiod) : 1.;
+            if (modulation <= 0.) modulation = 1.;
+            const double Ry = q.radius_y * modulation, Rz = q.radius_z * modulation;
+            density = density / (modulation * modulation);
+            arg = 0.5 * (yco - q.y0) * (yco - q.y0) / Ry / Ry + 0.5 * (zco - q.z0) * (zco - q.z0) / Rz / Rz;
+            if (arg > 4) return tmp;
+            density *= exp(-arg - arg_front);
+            if (xco > q.plateau_end && xco < q.end) {
+                const double xmid = (q.end + q.plateau_end) / 2.;
+                const double width = q.end - q.plateau_end;
+                density *= 0.5 * (1. - tanh(4. * (xco - xmid) / width));
+            }
+            return q.density * density;
+        }
+        case 6:
+            if (xco < 0. || xco < q.begin || xco > q.end) return tmp;
+            r2 = (yco - q.y0) * (yco - q.y0) + (zco - q.z0) * (zco - q.z0);
+            if (q.radius <= 0.) q.radius = 1.;
+            if (r2 < q.radius * q.radius) density *= q.delta;
+            if (xco < q.plateau_begin) {
+                density *= (xco - q.begin) / (q.plateau_begin - q.begin);
+                return density;
+            }
+            if (xco > q.plateau_end) {
+                density *= (q.end - xco) / (q.end - q.plateau_end);
+                return density;
+            }
+            return density;
+        case 5:
+            if (xco < 0. || xco < q.begin || xco > q.end) return tmp;
+            if (xco < q.plateau_begin)
+                return 0.5 * density * (1. + tanh(5. * (xco - q.begin) / (q.plateau_begin - q.begin)));
+            if (xco > q.plateau_end)
+                return density * (1. + q.delta) * (q.end - xco) / (q.end - q.plateau_end);
+            return q.density * (1. + q.delta * (xco - q.plateau_begin) / (q.plateau_end - q.plateau_begin));
+        case 4:
+            if (q.radius <= 0.) q.radius = 1.;
+            if (q.radius_x <= 0.) q.radius_x = q.radius;
+            if (q.radius_y <= 0.) q.radius_y = q.radius;
+            if (q.radius_z <= 0.) q.radius_z = q.radius;
+            if (fabs(xco - q.x0) > q.radius_x) return 0.;
+            if (fabs(yco - q.y0) > q.radius_y) return 0.;
+            if (fabs(zco - q.z0) > q.radius_z) return 0.;
+            return density;
+        case 3: {
+            if (xco < 0. || xco < q.begin || xco > q.end) return tmp;
+            double y0 = q.y0, z0 = q.z0;
+            if (q.xperiod > 0. && xco > q.curvature_begin && xco < q.curvature_end) {
+                y0 = q.y0 + q.y_curvature * sin(2. * PI_ * xco / q.xperiod);
+                z0 = q.z0 + q.z_curvature * cos(2. * PI_ * xco / q.xperiod);
+            }
+            r2 = (yco - y0) * (yco - y0) + (zco - z0) * (zco - z0);
+            if (q.radius <= 0.) q.radius = 1.;
+            arg = r2 / q.radius / q.radius;
+            if (arg < 2) tmp = q.delta * exp(-arg);
+            if (tmp < 0) tmp = 0.;
+            if (tmp > 1) tmp = 1.;
+            density *= (1. - tmp);
+            if (xco < q.plateau_begin) {
+                density *= (xco - q.begin) / (q.plateau_begin - q.begin);
+                return density;
+            }
+            if (xco > q.plateau_end) {
+                density *= (q.end - xco) / (q.end - q.plateau_end);
+                return density;
+            }
+            return density;
+        }
+        case 2:
+            if (xco < 0. || xco < q.begin || xco > q.end) return tmp;
+            r2 = (yco - q.y0) * (yco - q.y0) + (zco - q.z0) * (zco - q.z0);
+            if (q.radius <= 0.) q.radius = 1.;
+            arg = r2 / q.radius / q.radius;
+            if (arg < 10) tmp = q.delta * exp(-arg);
+            if (tmp < 0) tmp = 0.;
+            if (tmp > 1) tmp = 1.;
+            if (xco < q.plateau_begin)
+                return density * (xco - q.begin) / (q.plateau_begin - q.begin) * (1. - tmp);
+            if (xco > q.plateau_end)
+                return density1 * (q.end - xco) / (q.end - q.plateau_end) * (1. - tmp);
+            return (1. - tmp) * (q.density * (q.plateau_end - xco) + q.density1 * (xco - q.plateau_begin)) /
+                   (q.plateau_end - q.plateau_begin);
+        case 1:
+            if (xco < q.begin || xco > q.end) return 0.;
+            if (q.radius <= 0.) q.radius = 1.;
+            if (q.radius_x <= 0.) q.radius_x = q.radius;
+            if (q.radius_y <= 0.) q.radius_y = q.radius;
+            if (q.radius_z <= 0.) q.radius_z = q.radius;
+            arg = (xco - q.x0) * (xco - q.x0) / q.radius_x / q.radius_x +
+                  (yco - q.y0) * (yco - q.y0) / q.radius_y / q.radius_y +
+                  (zco - q.z0) * (zco - q.z0) / q.radius_z / q.radius_z;
+            if (arg > 16) return tmp;
+            if (q.xperiod <= 0.) q.xperiod = 1.;
+            return q.density * exp(-arg) * (1. + q.delta * cos(2 * PI_ * (xco - q.x0) / q.xperiod));
+        default:
+        case 0:
+            if (xco < 0. || xco < q.begin || xco > q.end) return tmp;
+            if (xco < q.plateau_begin) return density * (xco - q.begin) / (q.plateau_begin - q.begin);
+            if (xco > q.plateau_end) return density * (q.end - xco) / (q.end - q.plateau_end);
+            return q.density;
+        }
+    }
+};
+
 struct Oracle {
     qs_config cfg;
     int My = 0, Mz = 0, L = 0, NxSplit = 1, nIter = 1;
@@ -552,6 +740,8 @@ struct Oracle {
     size_t nI = 0;        // interior plane size
     double hx = 0, hy = 0, hz = 0, Ylength = 0, Zlength = 0, ts = 0;
     double phase = 0;
+    bool have_profile = false;
+    qs_density_profile profile{};
 
     std::vector<double> P[NPL], C[NPL];
     std::vector<double> A;          // layers 0..L, 10 planes each (fields, currents)
@@ -612,10 +802,19 @@ struct Oracle {
         return true;
     }
 
+    double density_at(double xco, double yco, double zco) const {
+        if (!have_profile) return cfg.plasma_density;
+        SpecieProfile sp(profile);
+        return sp(xco, yco, zco);
+    }
     double dens() const {
-        // :237-252 sum over non-beam species of |Density*q2m| at the head,
-        // uniform plasma here; 0 -> 1
-        double d = std::fabs(cfg.plasma_density * cfg.plasma_q2m);
+        // :236-252 |Density*q2m| of the plasma electrons at the head layer
+        // i = l_Mx-1, on axis (j = l_My/2., k = l_Mz/2.); 0 -> 1
+        const int i = L - 1, j = (int)(My / 2.), k = (int)(Mz / 2.);
+        const double xco = cfg.hx * i + phase;   // X(i) = Hx()*i
+        const double yco = hy * j - Ylength / 2.;
+        const double zco = hz * k - Zlength / 2.;
+        double d = std::fabs(density_at(xco, yco, zco) * cfg.plasma_q2m);
         if (d == 0.0) d = 1.0;
         return d;
     }
@@ -1199,6 +1398,42 @@ int qso_create(const qs_config* cfg, qso** out) {
 }
 
 void qso_destroy(qso* o) { delete o; }
+
+double qso_density(const qs_density_profile* p, double x, double y, double z) {
+    if (!p) return 0.0;
+    SpecieProfile sp(*p);
+    return sp(x, y, z);
+}
+
+int qso_set_density_profile(qso* h, const qs_density_profile* p) {
+    if (!h) return QS_ERR_INVALID;
+    h->o.have_profile = p != nullptr;
+    if (p) h->o.profile = *p;
+    return QS_OK;
+}
+
+int qso_set_phase(qso* h, double phase) {
+    if (!h) return QS_ERR_INVALID;
+    h->o.phase = phase;
+    return QS_OK;
+}
+
+int qso_front_weights(qso* h, double* out) {
+    // Mesh::SeedParticles (mesh.cpp:413-471): xco = X(l_Mx) + phase, the
+    // cell's corner in y and z, weight GetWeight()*dens = dens/ppc, no
+    // particle (weight 0 here) where dens <= 0
+    if (!h || !out) return QS_ERR_INVALID;
+    const Oracle& o = h->o;
+    const double xco = o.cfg.hx * o.L + o.phase;
+    for (int k = 0; k < o.Mz; k++)
+        for (int j = 0; j < o.My; j++) {
+            const double yco = o.hy * j - o.Ylength / 2.;
+            const double zco = o.hz * k - o.Zlength / 2.;
+            const double dens = o.density_at(xco, yco, zco);
+            out[j + (size_t)o.My * k] = dens > 0. ? 1. / o.cfg.ppc * dens : 0.0;
+        }
+    return QS_OK;
+}
 
 int qso_load_beam(qso* h, int64_t n, const int32_t* i, const int32_t* j, const int32_t* k,
                   const double* x, const double* y, const double* z, const double* px,

@@ -80,6 +80,14 @@ int qso_get_beam_currents(qso* o, int field, int layer, double* out);
 int qso_get_onaxis_ex(qso* o, double* out);
 
 int qso_step(qso* o);
+/* Specie::Density (plasma.cpp:6-399) of a profile at (x, y, z). */
+double qso_density(const qs_density_profile* p, double x, double y, double z);
+/* The plasma profile (NULL: uniform cfg.plasma_density) and the phase. */
+int qso_set_density_profile(qso* o, const qs_density_profile* p);
+int qso_set_phase(qso* o, double phase);
+/* Weights Mesh::SeedParticles gives the front particles of each cell
+ * (j + ny*k), 0 where it seeds none. */
+int qso_front_weights(qso* o, double* out);
 int qso_move_beam_particles(qso* o);
 int qso_move_all_split_layers(qso* o);
 int qso_begin_march(qso* o);

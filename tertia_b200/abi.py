@@ -112,6 +112,40 @@ def default_config(**overrides) -> QsConfig:
     return c
 
 
+# qs_density_profile distributions (Specie i_Distribution, plasma.cpp)
+DIST_TRAPEZOID, DIST_GAUSS_ELLIPSOID, DIST_GAUSS_CHANNEL, DIST_CURVED_CHANNEL = 0, 1, 2, 3
+DIST_PARALLELEPIPED, DIST_EXPONENTIAL, DIST_EMPTY_CHANNEL, DIST_COS_GAUSS = 4, 5, 6, 7
+DIST_TANH_STEP, DIST_ROD, DIST_LINEAR_STEP, DIST_GRADIENT, DIST_PERIODIC = 8, 9, 10, 11, 12
+
+
+class QsDensityProfile(C.Structure):
+    """Layout-identical mirror of struct qs_density_profile."""
+
+    _fields_ = [("distribution", C.c_int32), ("reserved", C.c_int32)] + [
+        (name, C.c_double) for name in (
+            "density", "density1", "begin", "end", "plateau_begin", "plateau_end", "scale",
+            "delta", "radius", "radius_x", "radius_y", "radius_z", "x0", "y0", "z0", "xperiod",
+            "yperiod", "zperiod", "angle_y", "y_curvature", "z_curvature", "curvature_begin",
+            "curvature_end")]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+def density_profile(**values) -> QsDensityProfile:
+    """A profile from the uniform default (Python twin of
+    qs_density_profile_default; kept identical by a test) with `values` set."""
+    p = QsDensityProfile()
+    p.density = 1.0
+    p.plateau_end = p.end = 1e30
+    p.curvature_end = 1e20
+    for k, v in values.items():
+        if not hasattr(p, k):
+            raise AttributeError(k)
+        setattr(p, k, v)
+    return p
+
+
 _lib = None
 
 
@@ -176,6 +210,12 @@ def _declare(L):
     L.qs_transform2d_noalloc.argtypes = [C.c_int] * 5 + [P, P, P]
     L.qs_step_host.argtypes = ([P, C.c_int64] + [i32p] * 3 + [f64p] * 7 + [i32p] * 3 +
                                [f64p] * 6 + [f64p])
+    L.qs_density_profile_default.argtypes = [C.POINTER(QsDensityProfile)]
+    L.qs_set_density_profile.argtypes = [P, C.POINTER(QsDensityProfile)]
+    L.qs_plasma_density.argtypes = [P, C.c_double, C.c_double, C.c_double,
+                                    C.POINTER(C.c_double)]
+    L.qs_set_phase.argtypes = [P, C.c_double]
+    L.qs_get_phase.argtypes = [P, C.POINTER(C.c_double)]
     L.qs_adjoint_checkpoints.argtypes = [P, C.c_int]
     L.qs_adjoint.argtypes = [P, f64p, f64p]
     L.qs_kernel_launches.argtypes = [P]
@@ -189,6 +229,8 @@ EXPORTED_SYMBOLS = [
     "qs_config_default", "qs_create", "qs_destroy", "qs_last_error", "qs_status_string",
     "qs_sync", "qs_get_stream", "qs_load_beam", "qs_get_beam", "qs_beam_count",
     "qs_load_front_plasma", "qs_seed_front_plasma", "qs_plasma_count", "qs_get_plasma",
+    "qs_density_profile_default", "qs_set_density_profile", "qs_plasma_density",
+    "qs_set_phase", "qs_get_phase",
     "qs_set_layer", "qs_get_layer", "qs_get_field3d", "qs_set_beam_currents",
     "qs_get_beam_currents", "qs_get_onaxis_ex", "qs_get_psi", "qs_step",
     "qs_move_beam_particles", "qs_move_all_split_layers", "qs_begin_march", "qs_layer_begin",

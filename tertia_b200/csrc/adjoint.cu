@@ -590,7 +590,7 @@ __global__ void corrector_adjoint_kernel(AdjSpecArgs<T> a) {
     const int k = blockIdx.y;
     if (j >= a.ny) return;
     const size_t n = (size_t)j + (size_t)a.ny * k;
-    const T d = a.dens, hx = a.hx;
+    const T d = *a.dens_p, hx = a.hx;
     const T akz = a.piZ * (T(k) + T(0.5));
     const T aky = a.piY * (T(j) + T(0.5));
     const T k2 = aky * aky + akz * akz;
@@ -630,7 +630,7 @@ __global__ void predictor_adjoint_kernel(AdjSpecArgs<T> a) {
     const int k = blockIdx.y;
     if (j >= a.ny) return;
     const size_t n = (size_t)j + (size_t)a.ny * k;
-    const T d = a.dens, hx = a.hx;
+    const T d = *a.dens_p, hx = a.hx;
     const T akz = a.piZ * (T(k) + T(0.5));
     const T aky = a.piY * (T(j) + T(0.5));
     const T k2 = aky * aky + akz * akz;

@@ -26,6 +26,7 @@
 #include "qs_common.cuh"
 #include "qs_internal.h"
 #include "dtt_tc.h"
+#include "density.cuh"
 
 namespace qs {
 
@@ -46,6 +47,10 @@ struct EngineBase {
     int64_t launches = 0;
     uint64_t step_count = 0;
     double phase = 0;
+    // plasma density profile (Specie::Density); uniform cfg.plasma_density
+    // when none is set
+    bool have_profile = false;
+    qs_density_profile profile{};
     bool capturing = false;
     int64_t capture_count = 0;
     // per-kernel timing (qs_profile_*): an event pair around every launch
@@ -114,6 +119,23 @@ struct EngineBase {
     qs_status cuda_fail(cudaError_t e, const char* what) {
         return fail(e == cudaErrorMemoryAllocation ? QS_ERR_OOM : QS_ERR_CUDA, "%s: %s", what,
                     cudaGetErrorString(e));
+    }
+
+    // Specie::Density of the plasma electrons at (x, y, z)
+    double density_at(double x, double y, double z) const {
+        if (!have_profile) return cfg.plasma_density;
+        return profile_density(profile, x, y, z);
+    }
+    // the density of the Guess/Iterate maps: |Density*q2m| on axis at the
+    // head layer i = l_Mx-1 (movefieldshydrolinlayersplit.cpp:236-250), 1 when 0
+    double march_density() const {
+        const int j = My / 2, k = Mz / 2;
+        const double x = cfg.hx * (L - 1) + phase;
+        const double y = cfg.hy * j - My * cfg.hy / 2.;
+        const double z = cfg.hz * k - Mz * cfg.hz / 2.;
+        double d = std::fabs(density_at(x, y, z) * cfg.plasma_q2m);
+        if (d == 0.0) d = 1.0;
+        return d;
     }
 
     virtual qs_status init() = 0;
@@ -209,6 +231,8 @@ struct Engine : EngineBase {
     DttMats<T> my, mz;
     TcTransformer* tcx = nullptr;
     T* onaxis_d = nullptr;
+    T* dens_dev = nullptr;      // |Density*q2m| of the march in flight (spectral maps)
+    double dens_set = -1.0;     // the value dens_dev holds (-1: none yet)
     T* stage = nullptr;         // conversion staging, 8 planes
     double* stage_d = nullptr;  // double staging, 8 planes
     // plasma
@@ -279,7 +303,7 @@ struct Engine : EngineBase {
         delete tcx;
         void* ptrs[] = {f3, b3, src3, splitbuf, srcbuf, Cbeam, sb3, bank, scratch, mats, onaxis_d,
                         stage, stage_d, pcell, py, pz, ppx, ppy, ppz, pw, bi, bj, bk, bx, by, bz,
-                        bpx, bpy, bpz, bw, d_err, ck, seg, lam, lam_pm, lam_sb, lam_b3,
+                        bpx, bpy, bpz, bw, d_err, dens_dev, ck, seg, lam, lam_pm, lam_sb, lam_b3,
                         d_dloss, d_gradw, acell, pid, apid, ay, az, apx, apy, apz, aw, cic_cnt,
                         cic_loff, cic_bsum, cic_bpref, cic_ticket, ck_cell, ck_id, seg_cell,
                         adj_inv, lam_pos, adj_tmp};
@@ -337,6 +361,8 @@ struct Engine : EngineBase {
         if ((s = alloc(&stage_d, 8 * plane, "staging"))) return s;
         if ((s = alloc(&onaxis_d, (size_t)L, "on-axis"))) return s;
         CK(cudaMemset(onaxis_d, 0, L * sizeof(T)));
+        if ((s = alloc(&dens_dev, 1, "density"))) return s;
+        if ((s = set_march_density())) return s;
         // transform matrices 2 cos / 2 sin (pi (j+1/2)(k+1/2)/n); the angle is
         // reduced exactly in integers: (2j+1)(2k+1) mod 8n in units of pi/(4n)
         const size_t ny2 = (size_t)My * My, nz2 = (size_t)Mz * Mz;
@@ -626,12 +652,25 @@ struct Engine : EngineBase {
             oy[is] = y;
             oz[is] = z;
         }
-        const double weight = cfg.plasma_density / ppc;   // Specie::GetWeight()*dens
+        SeedFront sf{};
+        sf.My = My; sf.Mz = Mz; sf.ppc = ppc;
+        for (int is = 0; is < ppc; is++) {
+            sf.offs_y[is] = oy[is];
+            sf.offs_z[is] = oz[is];
+        }
+        sf.px0 = cfg.plasma_px0; sf.py0 = cfg.plasma_py0; sf.pz0 = cfg.plasma_pz0;
+        sf.sx = cfg.pspread_x; sf.sy = cfg.pspread_y; sf.sz = cfg.pspread_z;
+        sf.weight = cfg.plasma_density / ppc;   // Specie::GetWeight()*dens
+        sf.use_profile = have_profile ? 1 : 0;
+        sf.prof = profile;
+        // the front layer i = l_Mx and the cell corners (mesh.cpp:415-417)
+        sf.x_front = cfg.hx * L + phase;
+        sf.hy = cfg.hy; sf.hz = cfg.hz;
+        sf.y_half = My * cfg.hy / 2.;
+        sf.z_half = Mz * cfg.hz / 2.;
+        sf.seed = cfg.seed; sf.step = step;
         klaunch(KC_SEED, [&] {
-            return launch_seed_front<T>(My, Mz, ppc, oy, oz, cfg.plasma_px0, cfg.plasma_py0,
-                                        cfg.plasma_pz0, cfg.pspread_x, cfg.pspread_y,
-                                        cfg.pspread_z, weight, cfg.seed, step, pcell, py, pz, ppx,
-                                        ppy, ppz, pw, st);
+            return launch_seed_front<T>(sf, pcell, py, pz, ppx, ppy, ppz, pw, st);
         });
         CK(cudaGetLastError());
         if ((s = cic_fresh_front())) return s;
@@ -852,9 +891,7 @@ struct Engine : EngineBase {
         a.piY = (T)(M_PI / Ylength);
         a.piZ = (T)(M_PI / Zlength);
         a.hx = (T)(cfg.hx / S);
-        double d = std::fabs(cfg.plasma_density * cfg.plasma_q2m);
-        if (d == 0.0) d = 1.0;
-        a.dens = (T)d;
+        a.dens_p = dens_dev;
         const int pb = cur ^ 1, cb = cur;
         a.RhoP = bankp(pb, SP_RHO); a.ExP = bankp(pb, SP_EX); a.EyP = bankp(pb, SP_EY);
         a.EzP = bankp(pb, SP_EZ); a.JxP = bankp(pb, SP_JX); a.JyP = bankp(pb, SP_JY);
@@ -923,6 +960,7 @@ struct Engine : EngineBase {
 
     qs_status begin_march() override {
         ck_valid = false;   // a march driven piece by piece keeps no checkpoints
+        if (qs_status s0 = set_march_density()) return s0;
         if (!front_pending) {
             qs_status s = seed_front(step_count);
             if (s) return s;
@@ -1145,7 +1183,19 @@ struct Engine : EngineBase {
         return QS_OK;
     }
 
+    // Write the density of the spectral maps for the march that follows into
+    // dens_dev (in stream order, outside any captured graph).
+    qs_status set_march_density() {
+        const double d = march_density();
+        if (d == dens_set) return QS_OK;
+        klaunch(KC_MISC, [&] { return launch_set_value<T>(dens_dev, (T)d, st); });
+        CK(cudaGetLastError());
+        dens_set = d;
+        return QS_OK;
+    }
+
     qs_status march() override {
+        if (qs_status s0 = set_march_density()) return s0;
         if (!front_pending) {
             qs_status s = seed_front(step_count);
             if (s) return s;
@@ -1358,7 +1408,7 @@ struct Engine : EngineBase {
         const SpecArgs<T> f = spec_args(iLayer, 0);
         AdjSpecArgs<T> a{};
         a.ny = My; a.nz = Mz;
-        a.piY = f.piY; a.piZ = f.piZ; a.hx = f.hx; a.dens = f.dens;
+        a.piY = f.piY; a.piZ = f.piZ; a.hx = f.hx; a.dens_p = f.dens_p;
         a.lRb0 = lam_sbp(iLayer, 0); a.lRb1 = lam_sbp(iLayer + 1, 0);
         a.lJxb0 = lam_sbp(iLayer, 1); a.lJxb1 = lam_sbp(iLayer + 1, 1);
         a.wb0 = f.wb0; a.wb1 = f.wb1;
@@ -1829,6 +1879,50 @@ qs_status qs_seed_front_plasma(qs_handle* h, uint64_t step) {
 }
 
 int64_t qs_plasma_count(const qs_handle* h) { return h ? h->e->plasma_count() : -1; }
+
+qs_status qs_density_profile_default(qs_density_profile* p) {
+    if (!p) return QS_ERR_INVALID;
+    std::memset(p, 0, sizeof *p);
+    p->distribution = 0;
+    p->density = 1.0;
+    p->plateau_end = p->end = 1e30;
+    p->curvature_end = 1e20;   // the namelist default (elements.cpp:53)
+    return QS_OK;
+}
+
+qs_status qs_set_density_profile(qs_handle* h, const qs_density_profile* p) {
+    H_OR_INVALID(h);
+    if (!p) {
+        E->have_profile = false;
+        return QS_OK;
+    }
+    if (p->distribution == 12 && !(p->xperiod > 0.0))
+        return E->fail(QS_ERR_INVALID, "the periodic profile needs xperiod > 0");
+    E->profile = *p;
+    E->have_profile = true;
+    return QS_OK;
+}
+
+qs_status qs_plasma_density(qs_handle* h, double x, double y, double z, double* out) {
+    H_OR_INVALID(h);
+    if (!out) return E->fail(QS_ERR_INVALID, "out is NULL");
+    *out = E->density_at(x, y, z);
+    return QS_OK;
+}
+
+qs_status qs_set_phase(qs_handle* h, double phase) {
+    H_OR_INVALID(h);
+    if (!std::isfinite(phase)) return E->fail(QS_ERR_INVALID, "phase must be finite");
+    E->phase = phase;
+    return QS_OK;
+}
+
+qs_status qs_get_phase(qs_handle* h, double* phase) {
+    H_OR_INVALID(h);
+    if (!phase) return E->fail(QS_ERR_INVALID, "phase is NULL");
+    *phase = E->phase;
+    return QS_OK;
+}
 
 qs_status qs_get_plasma(qs_handle* h, int64_t n, int32_t* cell, double* y, double* z, double* px,
                         double* py, double* pz, double* w) {

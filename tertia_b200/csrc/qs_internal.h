@@ -9,7 +9,10 @@ template <class T>
 struct SpecArgs {
     int ny, nz;
     T piY, piZ;          // M_PI/Ylength, M_PI/Zlength
-    T hx, dens;
+    T hx;
+    // |Density*q2m| of the maps, in device memory so that a captured march
+    // follows a density that changes from step to step
+    const T* dens_p;
     const T *RhoP, *ExP, *EyP, *EzP, *JxP, *JyP, *JzP;   // P spectral state
     // beam spectra of this (layer, split): w0*X0 + w1*X1 (the xi-interpolation
     // of movepart_splitlayer.cpp:330-348 applied to the spectra), and of the
@@ -53,11 +56,25 @@ int launch_beam_check(const T* b3, int nlayers, size_t plane, int* err, cudaStre
 template <class T>
 int launch_onaxis(const T* fields3d, int L, size_t plane, size_t idx, T* out, cudaStream_t st);
 
+// Front-layer seeding (Mesh::SeedParticles, mesh.cpp:413-548): ppc
+// particles per cell on the in-cell lattice, thermal momenta from a
+// counter-based generator, weight from the uniform density or the profile.
+struct SeedFront {
+    int My, Mz, ppc;
+    double offs_y[16], offs_z[16];
+    double px0, py0, pz0, sx, sy, sz;
+    double weight;               // uniform: Density/ppc
+    int use_profile;             // 1: weight (1/ppc)*Density(x_front, y_j, z_k), 0 where <= 0
+    qs_density_profile prof;
+    double x_front, hy, hz, y_half, z_half;
+    uint64_t seed, step;
+};
 template <class T>
-int launch_seed_front(int My, int Mz, int ppc, const double* offs_y, const double* offs_z,
-                      double px0, double py0, double pz0, double sx, double sy, double sz,
-                      double weight, uint64_t seed, uint64_t step, int32_t* cell, T* y, T* z,
-                      T* px, T* py, T* pz, T* w, cudaStream_t st);
+int launch_seed_front(const SeedFront& s, int32_t* cell, T* y, T* z, T* px, T* py, T* pz, T* w,
+                      cudaStream_t st);
+// one value into device memory, in stream order
+template <class T>
+int launch_set_value(T* dst, T v, cudaStream_t st);
 
 template <class T>
 int launch_convert(const void* src, int src_is_double, T* dst, size_t n, cudaStream_t st);
@@ -161,7 +178,8 @@ int launch_permute_adjoint(const int32_t* id_from, const int32_t* id_to, int64_t
 template <class T>
 struct AdjSpecArgs {
     int ny, nz;
-    T piY, piZ, hx, dens;
+    T piY, piZ, hx;
+    const T* dens_p;
     const T* lRho;
     const T* lE[3];
     const T* lEb[3];

@@ -17,6 +17,7 @@
 #include "qs_common.cuh"
 #include "qs_internal.h"
 #include "split.cuh"
+#include "density.cuh"
 
 namespace qs {
 
@@ -40,7 +41,7 @@ __global__ void predictor_kernel(SpecArgs<T> a) {
     const int N = a.ny * a.nz;
     if (n1 >= N) return;
     const int j = n1 % a.ny, k = n1 / a.ny;
-    const T d = a.dens, hx = a.hx;
+    const T d = *a.dens_p, hx = a.hx;
     const T akz = a.piZ * (T(k) + T(0.5));
     const T aky = a.piY * (T(j) + T(0.5));
     const T ak2 = aky * aky + akz * akz;
@@ -89,7 +90,7 @@ __global__ void corrector_kernel(SpecArgs<T> a) {
     const int N = a.ny * a.nz;
     if (n1 >= N) return;
     const int j = n1 % a.ny, k = n1 / a.ny;
-    const T d = a.dens, hx = a.hx;
+    const T d = *a.dens_p, hx = a.hx;
     const T akz = a.piZ * (T(k) + T(0.5));
     const T aky = a.piY * (T(j) + T(0.5));
     const T ak2 = aky * aky + akz * akz;
@@ -236,46 +237,52 @@ __device__ __forceinline__ void box_muller(uint32_t a, uint32_t b, double& n0, d
     n1 = r * s;
 }
 
-struct SeedOffs { double y[16], z[16]; };
-
 template <class T>
-__global__ void seed_front_kernel(int My, int Mz, int ppc, SeedOffs offs, double px0, double py0,
-                                  double pz0, double sx, double sy, double sz, double weight,
-                                  uint64_t seed, uint64_t step, int32_t* cell, T* y, T* z, T* px,
-                                  T* py, T* pz, T* w) {
+__global__ void seed_front_kernel(SeedFront s, int32_t* cell, T* y, T* z, T* px, T* py, T* pz,
+                                  T* w) {
     const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const int64_t n = (int64_t)My * Mz * ppc;
+    const int64_t n = (int64_t)s.My * s.Mz * s.ppc;
     if (p >= n) return;
-    const int c = (int)(p / ppc), s = (int)(p % ppc);
-    const uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32);
+    const int c = (int)(p / s.ppc), is = (int)(p % s.ppc);
+    const uint32_t k0 = (uint32_t)s.seed, k1 = (uint32_t)(s.seed >> 32);
     // counter = (particle index, step): one block of 4 words gives 4 normals
     const U4 r0 = philox4x32_10(
-        U4{(uint32_t)p, (uint32_t)(p >> 32), (uint32_t)step, (uint32_t)(step >> 32)}, k0, k1);
+        U4{(uint32_t)p, (uint32_t)(p >> 32), (uint32_t)s.step, (uint32_t)(s.step >> 32)}, k0, k1);
     double g0, g1, g2, g3;
     box_muller(r0.x, r0.y, g0, g1);
     box_muller(r0.z, r0.w, g2, g3);
+    double weight = s.weight;
+    if (s.use_profile) {
+        // Density at the cell's corner (mesh.cpp:415-417), GetWeight()*dens (:471)
+        const int j = c % s.My, k = c / s.My;
+        const double dens = profile_density(s.prof, s.x_front, s.hy * j - s.y_half,
+                                            s.hz * k - s.z_half);
+        weight = dens > 0.0 ? (1. / s.ppc) * dens : 0.0;
+    }
     cell[p] = c;
-    y[p] = (T)offs.y[s];
-    z[p] = (T)offs.z[s];
-    px[p] = (T)(px0 + sx * g0);
-    py[p] = (T)(py0 + sy * g1);
-    pz[p] = (T)(pz0 + sz * g2);
+    y[p] = (T)s.offs_y[is];
+    z[p] = (T)s.offs_z[is];
+    px[p] = (T)(s.px0 + s.sx * g0);
+    py[p] = (T)(s.py0 + s.sy * g1);
+    pz[p] = (T)(s.pz0 + s.sz * g2);
     w[p] = (T)weight;
 }
 
 template <class T>
-int launch_seed_front(int My, int Mz, int ppc, const double* offs_y, const double* offs_z,
-                      double px0, double py0, double pz0, double sx, double sy, double sz,
-                      double weight, uint64_t seed, uint64_t step, int32_t* cell, T* y, T* z,
-                      T* px, T* py, T* pz, T* w, cudaStream_t st) {
-    SeedOffs o{};
-    for (int s = 0; s < ppc && s < 16; s++) {
-        o.y[s] = offs_y[s];
-        o.z[s] = offs_z[s];
-    }
-    const int64_t n = (int64_t)My * Mz * ppc;
-    seed_front_kernel<T><<<(unsigned)((n + 255) / 256), 256, 0, st>>>(
-        My, Mz, ppc, o, px0, py0, pz0, sx, sy, sz, weight, seed, step, cell, y, z, px, py, pz, w);
+int launch_seed_front(const SeedFront& s, int32_t* cell, T* y, T* z, T* px, T* py, T* pz, T* w,
+                      cudaStream_t st) {
+    const int64_t n = (int64_t)s.My * s.Mz * s.ppc;
+    seed_front_kernel<T><<<(unsigned)((n + 255) / 256), 256, 0, st>>>(s, cell, y, z, px, py, pz, w);
+    return 1;
+}
+
+template <class T>
+__global__ void set_value_kernel(T* dst, T v) {
+    *dst = v;
+}
+template <class T>
+int launch_set_value(T* dst, T v, cudaStream_t st) {
+    set_value_kernel<T><<<1, 1, 0, st>>>(dst, v);
     return 1;
 }
 
@@ -311,10 +318,9 @@ int launch_convert_back(const T* src, double* dst, size_t n, cudaStream_t st) {
                                       cudaStream_t);                                            \
     template int launch_onaxis<T>(const T*, int, size_t, size_t, T*, cudaStream_t);            \
     template int launch_beam_check<T>(const T*, int, size_t, int*, cudaStream_t);              \
-    template int launch_seed_front<T>(int, int, int, const double*, const double*, double,      \
-                                      double, double, double, double, double, double,           \
-                                      uint64_t, uint64_t, int32_t*, T*, T*, T*, T*, T*, T*,     \
+    template int launch_seed_front<T>(const SeedFront&, int32_t*, T*, T*, T*, T*, T*, T*,       \
                                       cudaStream_t);                                            \
+    template int launch_set_value<T>(T*, T, cudaStream_t);                                      \
     template int launch_convert<T>(const void*, int, T*, size_t, cudaStream_t);                 \
     template int launch_convert_back<T>(const T*, double*, size_t, cudaStream_t);
 QS_INST(float)

@@ -97,7 +97,7 @@ __global__ void __launch_bounds__(kThreads) predictor_f32_kernel(SpecArgs<float>
     if (j >= a.ny) return;
     pdl_wait();
     const size_t n = (size_t)j + (size_t)a.ny * k;
-    const float d = a.dens, hx = a.hx;
+    const float d = *a.dens_p, hx = a.hx;
     const float dh2 = d * hx * hx;
     const float inv_den = 1.f / (4.f + dh2);
     const float propagator = (4.f - dh2) * inv_den;
@@ -158,7 +158,7 @@ __global__ void __launch_bounds__(kThreads) corrector_f32_kernel(SpecArgs<float>
     if (j >= a.ny) return;
     pdl_wait();
     const size_t n = (size_t)j + (size_t)a.ny * k;
-    const float d = a.dens, hx = a.hx;
+    const float d = *a.dens_p, hx = a.hx;
     const float akz = a.piZ * ((float)k + 0.5f);
     const float2 rp2 = ld2(a.RhoP, n), jx2 = ld2(a.Jx, n), jy2 = ld2(a.Jy, n), jz2 = ld2(a.Jz, n),
                  jxp2 = ld2(a.JxP, n), jyp2 = ld2(a.JyP, n), jzp2 = ld2(a.JzP, n),

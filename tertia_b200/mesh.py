@@ -117,6 +117,25 @@ class Mesh:
     def seed_front_plasma(self, step: int):
         self._chk(self._L.qs_seed_front_plasma(self._h, int(step)), "qs_seed_front_plasma")
 
+    def set_density_profile(self, prof):
+        """Specie density profile (abi.QsDensityProfile, or None for the
+        uniform cfg.plasma_density)."""
+        self._chk(self._L.qs_set_density_profile(self._h, C.byref(prof) if prof is not None
+                                                 else None), "qs_set_density_profile")
+
+    def plasma_density(self, x: float, y: float, z: float) -> float:
+        out = C.c_double()
+        self._chk(self._L.qs_plasma_density(self._h, x, y, z, C.byref(out)), "qs_plasma_density")
+        return out.value
+
+    def set_phase(self, phase: float):
+        self._chk(self._L.qs_set_phase(self._h, float(phase)), "qs_set_phase")
+
+    def get_phase(self) -> float:
+        out = C.c_double()
+        self._chk(self._L.qs_get_phase(self._h, C.byref(out)), "qs_get_phase")
+        return out.value
+
     def get_plasma(self) -> dict:
         n = int(self._L.qs_plasma_count(self._h))
         out = {"cell": np.empty(n, dtype=np.int32)}
