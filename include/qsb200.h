@@ -210,6 +210,29 @@ qs_status qs_plasma_density(qs_handle* h, double x, double y, double z, double* 
  * before its beam push (step.cpp:33). */
 qs_status qs_set_phase(qs_handle* h, double phase);
 qs_status qs_get_phase(qs_handle* h, double* phase);
+
+/* xi-pipeline hand-off in the reference's wire format (PackLayer /
+ * UnpackLayer, para.cpp:94-285; LAYER_ATTRIBUTE_NUMBER = 12 and
+ * BEAM_PARTICLE_ATTRIBUTE_NUMBER = 12, CUDA_WRAP/paraLayers.h:4-5): one
+ * double buffer of 12 planes of ny*nz (n = j + ny*k) in the order Bx, By, Bz,
+ * Ex, Ey, Ez, Jx, Jy, Jz, Rho, fftJxBeamHydro, fftRhoBeamHydro, then 12
+ * blocks of Np particle attributes Px, Py, Pz, X, Y, Z, Q2m, Weight, i_X,
+ * i_Y, i_Z, isort, particles cell by cell.  Size 12*ny*nz + 12*Np. */
+int64_t qs_layer_pack_size(const qs_handle* h);
+/* PackLayer + SendLayer's device read (para.cpp:94-150, 286-330): after a
+ * march, the tail layer (layer 0: fields, the currents of its last push, the
+ * corrected Rho, the beam spectra of its last split) and the plasma in
+ * flight.  n must be qs_layer_pack_size(h). */
+qs_status qs_pack_layer(qs_handle* h, double* buf, int64_t n);
+/* ReceiveLayer + UnpackLayer + CUDA_WRAP_setLayerToMesh (para.cpp:332-412,
+ * 175-285; paraCPUlayers.cu:178-297): the received layer becomes the front
+ * (layer nx) of the next march, as below the first rank of the reference's
+ * pipeline (movepart_splitlayer.cpp:105-151): its fields and sources are the
+ * head layer's P, its beam spectra the head's RhoBeamP (:547-551), and its
+ * particles the front plasma.  It serves that one march. */
+qs_status qs_unpack_layer(qs_handle* h, const double* buf, int64_t n);
+/* Drop a received layer that no march has used yet (empty front again). */
+qs_status qs_clear_front_layer(qs_handle* h);
 /* Plasma particles of the layer in flight (after a march: layer 0). */
 qs_status qs_get_plasma(qs_handle* h, int64_t n, int32_t* cell,
                         double* y, double* z, double* px, double* py,

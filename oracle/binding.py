@@ -147,6 +147,10 @@ def _declare(L):
     L.qso_set_density_profile.argtypes = [P, C.POINTER(QsDensityProfile)]
     L.qso_set_phase.argtypes = [P, C.c_double]
     L.qso_front_weights.argtypes = [P, _f64p]
+    L.qso_layer_pack_size.argtypes = [P]
+    L.qso_layer_pack_size.restype = C.c_int64
+    L.qso_pack_layer.argtypes = [P, _f64p, C.c_int64]
+    L.qso_unpack_layer.argtypes = [P, _f64p, C.c_int64]
     L.qso_dtt1d.argtypes = [C.c_int, C.c_int, _f64p, _f64p, C.c_int]
     L.qso_transform2d.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _f64p, _f64p, C.c_int]
     L.qso_push_layer_f64.argtypes = [C.POINTER(QsConfig), C.c_int64, _i32p] + [_f64p] * 9 + [
@@ -244,6 +248,16 @@ class Oracle:
 
     def set_phase(self, phase: float):
         _check(lib().qso_set_phase(self._h, float(phase)), "qso_set_phase")
+
+    def pack_layer(self):
+        n = int(lib().qso_layer_pack_size(self._h))
+        out = np.empty(n)
+        _check(lib().qso_pack_layer(self._h, out, n), "qso_pack_layer")
+        return out
+
+    def unpack_layer(self, buf):
+        b = np.ascontiguousarray(buf, dtype=np.float64)
+        _check(lib().qso_unpack_layer(self._h, b, b.size), "qso_unpack_layer")
 
     def front_weights(self):
         """Weights SeedParticles gives each cell's front particles (ny*nz)."""

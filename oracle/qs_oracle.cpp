@@ -753,6 +753,10 @@ struct Oracle {
     std::map<int, std::vector<std::vector<int>>> stored;   // layer -> lists
     std::vector<std::vector<int>> listsP, listsC;
     bool haveFront = false;
+    // a layer received from the rank ahead (UnpackLayer, para.cpp:175-285):
+    // fields and sources (A plane order, interior nI) and beam spectra
+    bool recvPending = false, recvActive = false;
+    std::vector<double> recvPlanes, recvJxB, recvRhoB;
     std::vector<std::vector<int>> frontLists;
 
     // beam particles
@@ -872,18 +876,23 @@ struct Oracle {
     }
 
     // ---- GuessFieldsHydroLinLayerSplit (movefieldshydrolinlayersplit.cpp:222-1169)
-    int guess(int iLayer, int /*iSplit*/) {
+    int guess(int iLayer, int iSplit) {
         const double d = dens();
         const int ny = My, nz = Mz;
         if (firstCall) {
             firstCall = false;
             alloc_spectral();
         }
-        if (iLayer > L - 2) {  // :430-445, single rank: the head layer
+        if (iLayer > L - 2 && !recvActive) {  // :430-445, the last rank: the head layer
             for (auto* v : {&fEx, &fEy, &fEz, &fBx, &fBy, &fBz, &fJx, &fJy, &fJz, &fRho, &fJxP,
                             &fJyP, &fJzP, &fRhoP, &fExP, &fEyP, &fEzP, &fJxBeam, &fRhoBeam,
                             &fJxBeamP, &fRhoBeamP})
                 std::fill(v->begin(), v->end(), 0.0);
+        }
+        if (recvActive && iLayer == L - 1 && iSplit == 0) {
+            // :547-551 below the first rank: the received beam spectra
+            fJxBeam = recvJxB;
+            fRhoBeam = recvRhoB;
         }
         // :552-558
         fRhoBeamP = fRhoBeam;
@@ -1151,6 +1160,24 @@ struct Oracle {
             for (int f = 6; f < 10; f++)
                 std::fill(A.begin() + aidx(i, f, -G, -G), A.begin() + aidx(i, f, -G, -G) + nyz,
                           0.0);
+        // :105-151 below the first rank the received layer is set into layer
+        // l_Mx (CUDA_WRAP_setLayerToMesh, paraCPUlayers.cu:178-285).  The
+        // reference writes its interior cells only; the guard ring is filled
+        // periodically here, as ExchangeFieldsSplit does for every marched layer.
+        recvActive = recvPending;
+        recvPending = false;
+        if (recvActive) {
+            for (int f = 0; f < 10; f++)
+                for (int k = -G; k < Mz + G - 1; k++)
+                    for (int j = -G; j < My + G - 1; j++) {
+                        const int jj = (j + My) % My, kk = (k + Mz) % Mz;
+                        A[aidx(L, f, j, k)] = recvPlanes[(size_t)f * nI + jj + (size_t)My * kk];
+                    }
+        } else {
+            for (int f = 0; f < 10; f++)
+                std::fill(A.begin() + aidx(L, f, -G, -G), A.begin() + aidx(L, f, -G, -G) + nyz,
+                          0.0);
+        }
         // :63 SeedFrontParticles: the loaded front lists live at layer L
         if (!haveFront) return QS_ERR_STATE;
         stored.clear();
@@ -1415,6 +1442,94 @@ int qso_set_density_profile(qso* h, const qs_density_profile* p) {
 int qso_set_phase(qso* h, double phase) {
     if (!h) return QS_ERR_INVALID;
     h->o.phase = phase;
+    return QS_OK;
+}
+
+// ---- PackLayer / UnpackLayer (para.cpp:94-285): 12 planes (Bx, By, Bz, Ex,
+// Ey, Ez, Jx, Jy, Jz, Rho, fftJxBeamHydro, fftRhoBeamHydro) then 12 particle
+// blocks (Px, Py, Pz, X, Y, Z, Q2m, Weight, i_X, i_Y, i_Z, isort)
+int64_t qso_layer_pack_size(const qso* h) {
+    return h ? 12 * (int64_t)h->o.nI + 12 * (int64_t)h->o.ppy.size() : -1;
+}
+
+int qso_pack_layer(qso* h, double* buf, int64_t n) {
+    if (!h || !buf || n != qso_layer_pack_size(h)) return QS_ERR_INVALID;
+    Oracle& o = h->o;
+    auto it = o.stored.find(0);
+    if (it == o.stored.end()) return QS_ERR_STATE;   // no complete march
+    const size_t nI = o.nI;
+    const int order[10] = {3, 4, 5, 0, 1, 2, 6, 7, 8, 9};   // A planes in pack order
+    for (int k = 0; k < o.Mz; k++)
+        for (int j = 0; j < o.My; j++) {
+            const size_t n1 = (size_t)j + (size_t)o.My * k;
+            for (int f = 0; f < 10; f++) buf[f * nI + n1] = o.A[o.aidx(0, order[f], j, k)];
+            buf[10 * nI + n1] = o.fJxBeam[n1];
+            buf[11 * nI + n1] = o.fRhoBeam[n1];
+        }
+    const int64_t m = (int64_t)o.ppy.size();
+    double* pb = buf + 12 * nI;
+    int64_t r = 0;
+    for (int k = 0; k < o.Mz; k++)           // the layer walk of paraCPUlayers.cu:76-113
+        for (int j = 0; j < o.My; j++)
+            for (int id : it->second[(size_t)j + (size_t)o.My * k]) {
+                if (r >= m) return QS_ERR_STATE;
+                pb[r] = o.ppx_[id];
+                pb[r + m] = o.ppy_[id];
+                pb[r + 2 * m] = o.ppz_[id];
+                pb[r + 3 * m] = 0.0;
+                pb[r + 4 * m] = o.ppy[id];
+                pb[r + 5 * m] = o.ppz[id];
+                pb[r + 6 * m] = o.cfg.plasma_q2m;
+                pb[r + 7 * m] = o.pw[id];
+                pb[r + 8 * m] = 0.0;
+                pb[r + 9 * m] = j;
+                pb[r + 10 * m] = k;
+                pb[r + 11 * m] = 0.0;
+                r++;
+            }
+    return r == m ? QS_OK : QS_ERR_STATE;
+}
+
+int qso_unpack_layer(qso* h, const double* buf, int64_t n) {
+    if (!h || !buf) return QS_ERR_INVALID;
+    Oracle& o = h->o;
+    const int64_t fixed = 12 * (int64_t)o.nI;
+    if (n < fixed || (n - fixed) % 12) return QS_ERR_INVALID;
+    const int64_t m = (n - fixed) / 12;
+    const size_t nI = o.nI;
+    const int order[10] = {3, 4, 5, 0, 1, 2, 6, 7, 8, 9};
+    o.recvPlanes.assign(10 * nI, 0.0);
+    for (int f = 0; f < 10; f++)
+        std::copy(buf + f * nI, buf + (f + 1) * nI, o.recvPlanes.begin() + (size_t)order[f] * nI);
+    o.recvJxB.assign(buf + 10 * nI, buf + 11 * nI);
+    o.recvRhoB.assign(buf + 11 * nI, buf + 12 * nI);
+    // CUDA_WRAP_setLayerToMesh appends each particle to the list of its cell
+    const double* pb = buf + fixed;
+    std::vector<int64_t> ord(m);
+    std::vector<int32_t> cell(m);
+    for (int64_t r = 0; r < m; r++) {
+        const int j = (int)pb[r + 9 * m], k = (int)pb[r + 10 * m];
+        if (j < 0 || j >= o.My || k < 0 || k >= o.Mz) return QS_ERR_INVALID;
+        cell[r] = j + o.My * k;
+        ord[r] = r;
+    }
+    std::stable_sort(ord.begin(), ord.end(), [&](int64_t a, int64_t b) { return cell[a] < cell[b]; });
+    std::vector<int32_t> c(m);
+    std::vector<double> y(m), z(m), px(m), py(m), pz(m), w(m);
+    for (int64_t r = 0; r < m; r++) {
+        const int64_t q = ord[r];
+        c[r] = cell[q];
+        px[r] = pb[q];
+        py[r] = pb[q + m];
+        pz[r] = pb[q + 2 * m];
+        y[r] = pb[q + 4 * m];
+        z[r] = pb[q + 5 * m];
+        w[r] = pb[q + 7 * m];
+    }
+    int st = qso_load_front_plasma(h, m, c.data(), y.data(), z.data(), px.data(), py.data(),
+                                   pz.data(), w.data());
+    if (st) return st;
+    o.recvPending = true;
     return QS_OK;
 }
 

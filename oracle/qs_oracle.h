@@ -88,6 +88,11 @@ int qso_set_phase(qso* o, double phase);
 /* Weights Mesh::SeedParticles gives the front particles of each cell
  * (j + ny*k), 0 where it seeds none. */
 int qso_front_weights(qso* o, double* out);
+/* PackLayer / UnpackLayer (para.cpp:94-285) in the reference's buffer
+ * layout; the unpacked layer is the front of the next march. */
+int64_t qso_layer_pack_size(const qso* o);
+int qso_pack_layer(qso* o, double* buf, int64_t n);
+int qso_unpack_layer(qso* o, const double* buf, int64_t n);
 int qso_move_beam_particles(qso* o);
 int qso_move_all_split_layers(qso* o);
 int qso_begin_march(qso* o);

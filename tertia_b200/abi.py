@@ -215,6 +215,11 @@ def _declare(L):
     L.qs_plasma_density.argtypes = [P, C.c_double, C.c_double, C.c_double,
                                     C.POINTER(C.c_double)]
     L.qs_set_phase.argtypes = [P, C.c_double]
+    L.qs_layer_pack_size.argtypes = [P]
+    L.qs_layer_pack_size.restype = C.c_int64
+    L.qs_pack_layer.argtypes = [P, f64p, C.c_int64]
+    L.qs_unpack_layer.argtypes = [P, f64p, C.c_int64]
+    L.qs_clear_front_layer.argtypes = [P]
     L.qs_get_phase.argtypes = [P, C.POINTER(C.c_double)]
     L.qs_adjoint_checkpoints.argtypes = [P, C.c_int]
     L.qs_adjoint.argtypes = [P, f64p, f64p]
@@ -230,7 +235,8 @@ EXPORTED_SYMBOLS = [
     "qs_sync", "qs_get_stream", "qs_load_beam", "qs_get_beam", "qs_beam_count",
     "qs_load_front_plasma", "qs_seed_front_plasma", "qs_plasma_count", "qs_get_plasma",
     "qs_density_profile_default", "qs_set_density_profile", "qs_plasma_density",
-    "qs_set_phase", "qs_get_phase",
+    "qs_set_phase", "qs_get_phase", "qs_layer_pack_size", "qs_pack_layer", "qs_unpack_layer",
+    "qs_clear_front_layer",
     "qs_set_layer", "qs_get_layer", "qs_get_field3d", "qs_set_beam_currents",
     "qs_get_beam_currents", "qs_get_onaxis_ex", "qs_get_psi", "qs_step",
     "qs_move_beam_particles", "qs_move_all_split_layers", "qs_begin_march", "qs_layer_begin",

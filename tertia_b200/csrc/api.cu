@@ -14,6 +14,7 @@
 //   (RhoP, E*P, J*P, RhoBeamP), swapped at every layer end.
 //   Plasma particles: SoA grouped by cell; beam particles: SoA, FP64.
 // A plane is ny*nz values, index j + ny*k.
+#include <algorithm>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -170,6 +171,10 @@ struct EngineBase {
     virtual qs_status transform2d_dev(int, int, int, const void*, void*) = 0;
     virtual qs_status adjoint_checkpoints(int) = 0;
     virtual qs_status adjoint(const double*, double*) = 0;
+    virtual int64_t pack_size() const = 0;
+    virtual qs_status pack_layer(double*, int64_t) = 0;
+    virtual qs_status unpack_layer(const double*, int64_t) = 0;
+    virtual qs_status clear_front_layer() = 0;
 
     qs_status check_device() {
         cudaError_t e = cudaStreamSynchronize(st);
@@ -240,6 +245,14 @@ struct Engine : EngineBase {
     int32_t* pcell = nullptr;
     T *py = nullptr, *pz = nullptr, *ppx = nullptr, *ppy = nullptr, *ppz = nullptr, *pw = nullptr;
     bool front_pending = false;
+    // xi-pipeline hand-off: a layer received from the rank ahead
+    // (UnpackLayer, para.cpp:175-285) is the front (layer nx) of the next
+    // march: its E, B in field-store layer nx, its sources and beam spectra here
+    bool front_layer = false;
+    bool front_used = false;    // a march has started from it (it serves one march)
+    bool graph_front = false;   // the captured march was built with a received front
+    T* front_src = nullptr;     // Jx, Jy, Jz, Rho of the received layer
+    T* front_beam = nullptr;    // RhoBeam, JxBeam spectra of the received layer
     // FP32 CIC keeps the plasma grouped by cell (sort.cu): a second set of
     // particle arrays for the regrouping scatter, load-order ids, per-cell
     // counts and offsets, and where the grouping stands
@@ -269,6 +282,7 @@ struct Engine : EngineBase {
     int64_t graph_kernels = 0;
     struct HostState { T *Pf, *Cf, *Psrc, *Csrc; int cur; Grouping grp; } graph_end{}, adj_end{};
     bool marched = false;
+    bool tail_ready = false;    // layer 0 of a complete march is in place (qs_pack_layer)
     // adjoint: layer checkpoints of the last march and the reverse sweep's buffers
     int ck_every = 0;           // checkpoint every ck_every layers (0: off)
     bool ck_valid = false;      // the last march stored checkpoints for the current beam
@@ -303,7 +317,7 @@ struct Engine : EngineBase {
         delete tcx;
         void* ptrs[] = {f3, b3, src3, splitbuf, srcbuf, Cbeam, sb3, bank, scratch, mats, onaxis_d,
                         stage, stage_d, pcell, py, pz, ppx, ppy, ppz, pw, bi, bj, bk, bx, by, bz,
-                        bpx, bpy, bpz, bw, d_err, dens_dev, ck, seg, lam, lam_pm, lam_sb, lam_b3,
+                        bpx, bpy, bpz, bw, d_err, dens_dev, front_src, front_beam, ck, seg, lam, lam_pm, lam_sb, lam_b3,
                         d_dloss, d_gradw, acell, pid, apid, ay, az, apx, apy, apz, aw, cic_cnt,
                         cic_loff, cic_bsum, cic_bpref, cic_ticket, ck_cell, ck_id, seg_cell,
                         adj_inv, lam_pos, adj_tmp};
@@ -903,7 +917,12 @@ struct Engine : EngineBase {
         a.wb1 = (T)((double)iSplit / S);
         // beam of the previous (layer, split); zero on the head layer (:430-445)
         a.Rbp0 = a.Rb0; a.Rbp1 = a.Rb1; a.wp0 = T(0); a.wp1 = T(0);
-        if (iLayer < L - 1) {
+        if (iLayer == L - 1 && iSplit == 0 && front_layer) {
+            // below the first rank the head's RhoBeamP is the received layer's
+            // beam spectrum (CUDA_WRAP_setBeamFFT, :547-551)
+            a.Rbp0 = front_beam;
+            a.wp0 = T(1);
+        } else if (iLayer < L - 1 || front_layer) {
             if (iSplit > 0) {
                 a.wp0 = (T)((double)(S - iSplit + 1) / S);
                 a.wp1 = (T)((double)(iSplit - 1) / S);
@@ -961,6 +980,7 @@ struct Engine : EngineBase {
     qs_status begin_march() override {
         ck_valid = false;   // a march driven piece by piece keeps no checkpoints
         if (qs_status s0 = set_march_density()) return s0;
+        if (qs_status s0 = take_front_layer()) return s0;
         if (!front_pending) {
             qs_status s = seed_front(step_count);
             if (s) return s;
@@ -977,11 +997,19 @@ struct Engine : EngineBase {
         CK(cudaMemsetAsync(srcbuf, 0, 8 * plane * sizeof(T), st));
         cur = 0;
         p_valid = true;
+        if (front_layer) {
+            // the received layer is P of the head layer; its spectra are
+            // forward transforms of its planes, as Guess computes them (:717-743)
+            CK(cudaMemcpyAsync(Psrc, front_src, 4 * plane * sizeof(T), cudaMemcpyDeviceToDevice,
+                               st));
+            p_valid = false;
+        }
         Pf = f3layer(L);
         Cf = f3layer(L - 1);
         cur_layer = -1;
         cur_split = 0;
         marched = true;
+        tail_ready = false;
         return QS_OK;
     }
 
@@ -1148,6 +1176,7 @@ struct Engine : EngineBase {
     }
 
     qs_status layer_end(int iLayer, int iSplit) override {
+        if (iLayer == 0 && iSplit == S - 1) tail_ready = true;
         cur ^= 1;
         std::swap(Psrc, Csrc);
         if (iSplit == S - 1 && src3)
@@ -1183,6 +1212,153 @@ struct Engine : EngineBase {
         return QS_OK;
     }
 
+    // ------------------------------------------------- xi-pipeline hand-off
+    // PackLayer / UnpackLayer (para.cpp:94-285).  A received layer serves the
+    // one march that follows it; the march after that starts from the empty
+    // front again unless another layer arrives (the reference receives one
+    // every step, para.cpp:346-412, movepart_splitlayer.cpp:105-151).
+    qs_status take_front_layer() {
+        if (front_layer && front_used) return clear_front_layer();
+        if (front_layer) front_used = true;
+        return QS_OK;
+    }
+
+    qs_status clear_front_layer() override {
+        if (front_layer) CK(cudaMemsetAsync(f3layer(L), 0, 6 * plane * sizeof(T), st));
+        front_layer = false;
+        front_used = false;
+        return QS_OK;
+    }
+
+    int64_t pack_size() const override { return 12 * (int64_t)plane + 12 * np; }
+
+    // Plane order of the hand-off buffer (para.cpp:108-120): Bx, By, Bz, Ex,
+    // Ey, Ez, Jx, Jy, Jz, Rho, fftJxBeamHydro, fftRhoBeamHydro; particle
+    // blocks (:135-146): Px, Py, Pz, X, Y, Z, Q2m, Weight, i_X, i_Y, i_Z, isort.
+    qs_status pack_layer(double* buf, int64_t n) override {
+        if (!buf || n != pack_size())
+            return fail(QS_ERR_INVALID, "qs_pack_layer: n must be qs_layer_pack_size (%lld)",
+                        (long long)pack_size());
+        if (!tail_ready) return fail(QS_ERR_STATE, "qs_pack_layer: no complete march to pack");
+        qs_status s;
+        const size_t P = plane;
+        // the tail layer's fields
+        const int fsrc[6] = {3, 4, 5, 0, 1, 2};
+        for (int f = 0; f < 6; f++)
+            if ((s = get_plane(f3layer(0) + (size_t)fsrc[f] * P, buf + (size_t)f * P))) return s;
+        // its currents: the deposit of its last push, kept as the P sources
+        for (int f = 0; f < 3; f++)
+            if ((s = get_plane(Psrc + (size_t)f * P, buf + (size_t)(6 + f) * P))) return s;
+        // its Rho: the corrected spectral rho, inverse-transformed and
+        // normalised as the Iterate store does (:1546-1602)
+        {
+            T* outs[1] = {stage};
+            const int kz[1] = {CC}, ky[1] = {CC};
+            xform(job_stack(bankp(cur ^ 1, SP_RHO), 1, outs, kz, ky, inv_scale()));
+            CK(cudaGetLastError());
+            if ((s = get_plane(stage, buf + 9 * P))) return s;
+        }
+        // the beam spectra of its last split (fft_of_JxBeam, fft_of_RhoBeam)
+        {
+            std::vector<double> t0(P), t1(P);
+            const double w0 = 1.0 / S, w1 = (double)(S - 1) / S;
+            for (int q = 0; q < 2; q++) {
+                if ((s = get_plane(sbp(0, q), t0.data()))) return s;
+                if (S > 1 && (s = get_plane(sbp(1, q), t1.data()))) return s;
+                double* out = buf + (q == 0 ? 11 : 10) * P;
+                for (size_t i = 0; i < P; i++) out[i] = S > 1 ? w0 * t0[i] + w1 * t1[i] : t0[i];
+            }
+        }
+        // the plasma in flight, cell by cell (k outer, j inner, as the layer
+        // walk of paraCPUlayers.cu:76-113), load order within a cell
+        const int64_t m = np;
+        if (m > 0) {
+            std::vector<int32_t> cell(m);
+            std::vector<double> y(m), z(m), px(m), py_(m), pz_(m), w(m);
+            if ((s = get_plasma(m, cell.data(), y.data(), z.data(), px.data(), py_.data(),
+                                pz_.data(), w.data())))
+                return s;
+            std::vector<int64_t> ord(m);
+            for (int64_t p = 0; p < m; p++) ord[p] = p;
+            std::stable_sort(ord.begin(), ord.end(),
+                             [&](int64_t a, int64_t b) { return cell[a] < cell[b]; });
+            double* pb = buf + 12 * P;
+            for (int64_t r = 0; r < m; r++) {
+                const int64_t p = ord[r];
+                pb[r] = px[p];
+                pb[r + m] = py_[p];
+                pb[r + 2 * m] = pz_[p];
+                pb[r + 3 * m] = 0.0;                     // in-cell xi: plasma enters at x = 0
+                pb[r + 4 * m] = y[p];
+                pb[r + 5 * m] = z[p];
+                pb[r + 6 * m] = cfg.plasma_q2m;
+                pb[r + 7 * m] = w[p];
+                pb[r + 8 * m] = 0.0;                     // the layer index i_X
+                pb[r + 9 * m] = (double)(cell[p] % My);
+                pb[r + 10 * m] = (double)(cell[p] / My);
+                pb[r + 11 * m] = 0.0;                    // isort: the plasma electrons
+            }
+        }
+        return QS_OK;
+    }
+
+    qs_status unpack_layer(const double* buf, int64_t n) override {
+        const int64_t fixed = 12 * (int64_t)plane;
+        if (!buf || n < fixed || (n - fixed) % 12)
+            return fail(QS_ERR_INVALID, "qs_unpack_layer: n must be 12*ny*nz + 12*Np");
+        const int64_t m = (n - fixed) / 12;
+        const double* pb = buf + fixed;
+        std::vector<int32_t> cell(m);
+        for (int64_t r = 0; r < m; r++) {
+            const double jd = pb[r + 9 * m], kd = pb[r + 10 * m];
+            if (!(jd >= 0 && jd < My && kd >= 0 && kd < Mz) || jd != (double)(int)jd ||
+                kd != (double)(int)kd)
+                return fail(QS_ERR_INVALID, "qs_unpack_layer: particle %lld has cell (%g, %g) "
+                                            "outside the layer", (long long)r, jd, kd);
+            const double yy = pb[r + 4 * m], zz = pb[r + 5 * m];
+            if (!(yy >= 0 && yy <= 1 && zz >= 0 && zz <= 1))
+                return fail(QS_ERR_PARTICLE_RANGE, "qs_unpack_layer: particle %lld has in-cell "
+                                                   "position outside [0,1]", (long long)r);
+            if (pb[r + 6 * m] != cfg.plasma_q2m || pb[r + 11 * m] != 0.0)
+                return fail(QS_ERR_UNSUPPORTED, "qs_unpack_layer: particle %lld is not of the "
+                                                "plasma electron species", (long long)r);
+            cell[r] = (int32_t)jd + My * (int32_t)kd;
+        }
+        std::vector<int64_t> ord(m);
+        for (int64_t r = 0; r < m; r++) ord[r] = r;
+        std::stable_sort(ord.begin(), ord.end(),
+                         [&](int64_t a, int64_t b) { return cell[a] < cell[b]; });
+        std::vector<int32_t> c2(m);
+        std::vector<double> y(m), z(m), px(m), py_(m), pz_(m), w(m);
+        for (int64_t r = 0; r < m; r++) {
+            const int64_t q = ord[r];
+            c2[r] = cell[q];
+            px[r] = pb[q];
+            py_[r] = pb[q + m];
+            pz_[r] = pb[q + 2 * m];
+            y[r] = pb[q + 4 * m];
+            z[r] = pb[q + 5 * m];
+            w[r] = pb[q + 7 * m];
+        }
+        qs_status s;
+        if (!front_src && (s = alloc(&front_src, 4 * plane, "received layer"))) return s;
+        if (!front_beam && (s = alloc(&front_beam, 2 * plane, "received layer"))) return s;
+        const size_t P = plane;
+        const int fdst[6] = {3, 4, 5, 0, 1, 2};
+        for (int f = 0; f < 6; f++)
+            if ((s = put_plane(f3layer(L) + (size_t)fdst[f] * P, buf + (size_t)f * P))) return s;
+        for (int f = 0; f < 4; f++)
+            if ((s = put_plane(front_src + (size_t)f * P, buf + (size_t)(6 + f) * P))) return s;
+        if ((s = put_plane(front_beam, buf + 11 * P))) return s;       // RhoBeam
+        if ((s = put_plane(front_beam + P, buf + 10 * P))) return s;   // JxBeam
+        if ((s = load_front(m, c2.data(), y.data(), z.data(), px.data(), py_.data(), pz_.data(),
+                            w.data())))
+            return s;
+        front_layer = true;
+        front_used = false;
+        return QS_OK;
+    }
+
     // Write the density of the spectral maps for the march that follows into
     // dens_dev (in stream order, outside any captured graph).
     qs_status set_march_density() {
@@ -1196,6 +1372,7 @@ struct Engine : EngineBase {
 
     qs_status march() override {
         if (qs_status s0 = set_march_density()) return s0;
+        if (qs_status s0 = take_front_layer()) return s0;
         if (!front_pending) {
             qs_status s = seed_front(step_count);
             if (s) return s;
@@ -1207,10 +1384,15 @@ struct Engine : EngineBase {
         }
         if (!cfg.use_graph || prof) {
             qs_status s = march_device();
-            ck_valid = !s && ck_every > 0;
+            ck_valid = !s && ck_every > 0 && !front_layer;
             return s;
         }
+        if (gexec && graph_front != front_layer) {   // the head layer's set-up differs
+            cudaGraphExecDestroy(gexec);
+            gexec = nullptr;
+        }
         if (!gexec) {
+            graph_front = front_layer;
             cudaGraph_t g = nullptr;
             CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
             capturing = true;
@@ -1233,7 +1415,7 @@ struct Engine : EngineBase {
             graph_end = HostState{Pf, Cf, Psrc, Csrc, cur, grp};
         }
         CK(cudaGraphLaunch(gexec, st));
-        ck_valid = ck_every > 0;
+        ck_valid = ck_every > 0 && !front_layer;
         launches += graph_kernels;
         Pf = graph_end.Pf; Cf = graph_end.Cf; Psrc = graph_end.Psrc; Csrc = graph_end.Csrc;
         cur = graph_end.cur;
@@ -1241,6 +1423,7 @@ struct Engine : EngineBase {
         grp = graph_end.grp;
         p_valid = true;
         marched = true;
+        tail_ready = true;
         return QS_OK;
     }
 
@@ -1592,6 +1775,9 @@ struct Engine : EngineBase {
     qs_status adjoint(const double* dloss, double* dw) override {
         if (!dloss || !dw) return fail(QS_ERR_INVALID, "qs_adjoint: null pointer");
         if (ck_every <= 0) return fail(QS_ERR_STATE, "qs_adjoint: checkpoints are off");
+        if (front_layer)
+            return fail(QS_ERR_UNSUPPORTED, "qs_adjoint: the march started from a received layer; "
+                                            "the adjoint starts from the empty front");
         if (!ck_valid || np != adj_np)
             return fail(QS_ERR_STATE, "qs_adjoint: the last march did not store checkpoints "
                                       "for the current beam");
@@ -1915,6 +2101,29 @@ qs_status qs_set_phase(qs_handle* h, double phase) {
     if (!std::isfinite(phase)) return E->fail(QS_ERR_INVALID, "phase must be finite");
     E->phase = phase;
     return QS_OK;
+}
+
+int64_t qs_layer_pack_size(const qs_handle* h) { return h && h->e ? h->e->pack_size() : -1; }
+
+qs_status qs_pack_layer(qs_handle* h, double* buf, int64_t n) {
+    H_OR_INVALID(h);
+    qs_status s = E->pack_layer(buf, n);
+    if (s) return s;
+    return E->check_device();
+}
+
+qs_status qs_unpack_layer(qs_handle* h, const double* buf, int64_t n) {
+    H_OR_INVALID(h);
+    qs_status s = E->unpack_layer(buf, n);
+    if (s) return s;
+    return E->check_device();
+}
+
+qs_status qs_clear_front_layer(qs_handle* h) {
+    H_OR_INVALID(h);
+    qs_status s = E->clear_front_layer();
+    if (s) return s;
+    return E->check_device();
 }
 
 qs_status qs_get_phase(qs_handle* h, double* phase) {

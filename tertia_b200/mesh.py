@@ -136,6 +136,22 @@ class Mesh:
         self._chk(self._L.qs_get_phase(self._h, C.byref(out)), "qs_get_phase")
         return out.value
 
+    def pack_layer(self) -> np.ndarray:
+        """PackLayer: the tail layer and the plasma in flight after a march, in
+        the reference's hand-off buffer layout."""
+        n = int(self._L.qs_layer_pack_size(self._h))
+        out = np.empty(n)
+        self._chk(self._L.qs_pack_layer(self._h, _p(out, C.c_double), n), "qs_pack_layer")
+        return out
+
+    def unpack_layer(self, buf):
+        """UnpackLayer: the received layer is the front of the next march."""
+        b = _f64(buf)
+        self._chk(self._L.qs_unpack_layer(self._h, _p(b, C.c_double), b.size), "qs_unpack_layer")
+
+    def clear_front_layer(self):
+        self._chk(self._L.qs_clear_front_layer(self._h), "qs_clear_front_layer")
+
     def get_plasma(self) -> dict:
         n = int(self._L.qs_plasma_count(self._h))
         out = {"cell": np.empty(n, dtype=np.int32)}
