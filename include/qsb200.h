@@ -50,7 +50,8 @@ typedef enum qs_status {
 /* Arithmetic of the layer loop. */
 typedef enum qs_precision {
     QS_PREC_FP64 = 0,    /* plain FP64 everywhere (the FP64 GPU path)               */
-    QS_PREC_FP32 = 1,    /* FP32 push/deposit, FP32 transforms (exact FP32 GEMM)    */
+    QS_PREC_FP32 = 1,    /* FP32 push/deposit, FP32 transforms: half-length complex
+                            FFTs for power-of-two sizes, else FP32 matrix passes */
     QS_PREC_TF32X3 = 2,  /* FP32 push/deposit, transforms as 3-term TF32 split
                             products on the tcgen05 tensor cores, FP32 accumulate   */
     QS_PREC_BF16X3 = 3,  /* as above with 3-term BF16 split products               */

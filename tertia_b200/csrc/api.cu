@@ -235,6 +235,7 @@ struct Engine : EngineBase {
     T* mats = nullptr;          // transform matrices
     DttMats<T> my, mz;
     TcTransformer* tcx = nullptr;
+    DttFft* fftx = nullptr;     // FP32 transforms through FFTs (power-of-two sizes)
     T* onaxis_d = nullptr;
     T* dens_dev = nullptr;      // |Density*q2m| of the march in flight (spectral maps)
     double dens_set = -1.0;     // the value dens_dev holds (-1: none yet)
@@ -315,6 +316,7 @@ struct Engine : EngineBase {
         if (gexec) cudaGraphExecDestroy(gexec);
         if (adj_exec) cudaGraphExecDestroy(adj_exec);
         delete tcx;
+        delete fftx;
         void* ptrs[] = {f3, b3, src3, splitbuf, srcbuf, Cbeam, sb3, bank, scratch, mats, onaxis_d,
                         stage, stage_d, pcell, py, pz, ppx, ppy, ppz, pw, bi, bj, bk, bx, by, bz,
                         bpx, bpy, bpz, bw, d_err, dens_dev, front_src, front_beam, ck, seg, lam, lam_pm, lam_sb, lam_b3,
@@ -403,6 +405,9 @@ struct Engine : EngineBase {
             std::string msg;
             tcx = TcTransformer::create(tc_mode, My, Mz, d_err, msg);
             if (!tcx) return fail(QS_ERR_UNSUPPORTED, "tensor-core transform: %s", msg.c_str());
+        } else if (sizeof(T) == 4) {
+            fftx = DttFft::create(My, Mz);   // other sizes keep the FP32 matrix passes
+            CK(cudaGetLastError());
         }
         Pf = splitbuf;
         Cf = splitbuf + 6 * plane;
@@ -422,6 +427,10 @@ struct Engine : EngineBase {
                                           (void* const*)job.out, job.kz, job.ky,
                                           (double)job.scale, st);
                 });
+        } else if (fftx) {
+            if constexpr (sizeof(T) == 4)
+                for (int pass = 0; pass < 2; pass++)
+                    klaunch(KC_GEMM, [&] { return fftx->run_pass(pass, job, scratch, st); });
         } else {
             for (int pass = 0; pass < 2; pass++)
                 klaunch(KC_GEMM, [&] {

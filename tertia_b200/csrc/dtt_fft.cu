@@ -1,0 +1,537 @@
+// dtt_fft.cu — FP32 half-integer transforms (FFTW REDFT11 / RODFT11, the
+// reference's plans at movefieldshydrolinlayersplit.cpp:389-427) through a
+// complex FFT of half the length, for power-of-two sizes 32 .. 2048.
+//
+// A DCT-IV of length n is an n/2-point complex FFT between a pre- and a
+// post-twiddle (the standard reduction; e.g. Britanak, Yip and Rao,
+// "Discrete Cosine and Sine Transforms", 2007):
+//   z_i = (x[2i] + i x[n-1-2i]) e^{-i pi i/n},   Z = FFT_{n/2}(z),
+//   s_i = Z_i e^{-i pi (i+1/4)/n},   y[2i] = 2 Re s_i,   y[n-1-2i] = -2 Im s_i.
+// A DST-IV is the DCT-IV of the reversed input with the odd outputs negated.
+// The FFT is the Stockham autosort formulation of Govindaraju et al.
+// ("High performance discrete Fourier transforms on graphics processors",
+// SC 2008): a radix-16 pass, then radix-8 passes (4/2 for the rest), each
+// thread holding one radix-R butterfly group in registers and the sequence in
+// shared memory between passes.  Every twiddle comes from one table of
+// e^{-2 pi i k/(n/2)} built in FP64 on the host, so the error is that of an
+// FP32 FFT (a few 1e-7 relative), well below the split-precision GEMMs'.
+//
+// A 2-D transform is two kernels over a batch of planes (nz rows of ny, y
+// fastest): rows along y into a scratch plane, then columns along z into the
+// destination with the output scale.  Both read and write each plane once.
+#include <cmath>
+#include <vector>
+
+#include "qs_common.cuh"
+#include "qs_internal.h"
+#include "pdl.cuh"
+
+namespace qs {
+namespace fft {
+
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+    return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+
+template <int R>
+__device__ __forceinline__ int bitrev(int i) {
+    constexpr int B = R == 2 ? 1 : R == 4 ? 2 : R == 8 ? 3 : 4;
+    return (int)(__brev((unsigned)i) >> (32 - B));
+}
+
+// e^{-2 pi i k/16} for k = 0..7 (cos and sin of multiples of pi/8)
+constexpr float kC8 = 0.923879532511286756f;   // cos(pi/8)
+constexpr float kS8 = 0.382683432365089772f;   // sin(pi/8)
+constexpr float kR2 = 0.707106781186547524f;   // cos(pi/4)
+
+// x * e^{-2 pi i k/16}, with the multiplications by 1 and -i left out
+template <int K>
+__device__ __forceinline__ float2 rot16(float2 x) {
+    static_assert(K >= 0 && K < 8, "rot16");
+    if constexpr (K == 0) return x;
+    else if constexpr (K == 4) return make_float2(x.y, -x.x);
+    else if constexpr (K == 2) return make_float2(kR2 * (x.x + x.y), kR2 * (x.y - x.x));
+    else if constexpr (K == 6) return make_float2(kR2 * (x.y - x.x), -kR2 * (x.x + x.y));
+    else {
+        constexpr float c = K == 1 ? kC8 : K == 3 ? kS8 : K == 5 ? -kS8 : -kC8;
+        constexpr float s = K == 1 ? kS8 : K == 3 ? kC8 : K == 5 ? kC8 : kS8;
+        return make_float2(c * x.x + s * x.y, c * x.y - s * x.x);
+    }
+}
+
+// one radix-2 stage of butterflies of length LEN over the R registers
+template <int R, int LEN, int T>
+__device__ __forceinline__ void dit_stage_t(float2 (&v)[R]) {
+    if constexpr (T < LEN / 2) {
+#pragma unroll
+        for (int s = 0; s < R; s += LEN) {
+            const float2 u = v[s + T];
+            const float2 x = rot16<T * (16 / LEN)>(v[s + T + LEN / 2]);
+            v[s + T] = cadd(u, x);
+            v[s + T + LEN / 2] = csub(u, x);
+        }
+        dit_stage_t<R, LEN, T + 1>(v);
+    }
+}
+template <int R, int LEN>
+__device__ __forceinline__ void dit_stages(float2 (&v)[R]) {
+    if constexpr (LEN <= R) {
+        dit_stage_t<R, LEN, 0>(v);
+        dit_stages<R, 2 * LEN>(v);
+    }
+}
+
+// R-point forward DFT in registers (radix-2, decimation in time, R <= 16,
+// constant twiddles).  The input is loaded in bit-reversed order
+// (v[i] = x[bitrev(i)]), so only memory addresses are permuted and every
+// register index is static; the output is in natural order.
+template <int R>
+__device__ __forceinline__ void dft(float2 (&v)[R]) {
+    dit_stages<R, 2>(v);
+}
+
+// Exchanges between passes: a sequence whose threads share one warp only
+// needs the warp to meet; wider ones need the whole block.
+template <bool WARP>
+__device__ __forceinline__ void seq_sync() {
+    if constexpr (WARP) __syncwarp();
+    else __syncthreads();
+}
+
+// load, twiddle and transform butterfly group j of a pass (registers only)
+template <int M, int R, int NS, class At>
+__device__ __forceinline__ void stockham_group(float2 (&v)[R], const float2* W, At at, int j,
+                                               const float2* tw) {
+#pragma unroll
+    for (int i = 0; i < R; i++) {
+        const int r = bitrev<R>(i);
+        v[i] = W[at(j + r * (M / R))];
+        if (i) v[i] = cmul(v[i], tw[(j % NS) * r * (M / (NS * R))]);
+    }
+    dft<R>(v);
+}
+
+template <int R, int NS, class At>
+__device__ __forceinline__ void stockham_store(const float2 (&v)[R], float2* W, At at, int j) {
+    const int d = (j / NS) * NS * R + (j % NS);
+#pragma unroll
+    for (int r = 0; r < R; r++) W[at(d + r * NS)] = v[r];
+}
+
+// One Stockham pass of radix R after NS points have been combined: every
+// thread of a sequence (T = M/16 of them) does (M/R)/T butterfly groups
+// (1, 2, 4 or 8).  `at(e)` maps element e of this thread's sequence to its
+// shared-memory slot.
+template <int M, int R, int NS, bool WARP, class At>
+__device__ __forceinline__ void stockham_pass(float2* W, At at, int jt, const float2* tw) {
+    constexpr int T = M / 16;
+    constexpr int G = (M / R) / T;
+    static_assert(G == 1 || G == 2 || G == 4 || G == 8, "groups per thread");
+    if constexpr (G == 1) {
+        float2 v[R];
+        stockham_group<M, R, NS>(v, W, at, jt, tw);
+        seq_sync<WARP>();
+        stockham_store<R, NS>(v, W, at, jt);
+    } else {
+        float2 v[G][R];
+#pragma unroll
+        for (int g = 0; g < G; g++) stockham_group<M, R, NS>(v[g], W, at, jt + g * T, tw);
+        seq_sync<WARP>();
+#pragma unroll
+        for (int g = 0; g < G; g++) stockham_store<R, NS>(v[g], W, at, jt + g * T);
+    }
+    seq_sync<WARP>();
+}
+
+// The last pass keeps its butterfly groups in registers: thread jt ends up
+// with Z_q for q = jt + T*m in slot m (m < 16), and Z_{M-1-q} sits in slot
+// 15 - m of thread T-1-jt.
+template <int M, int R, int NS, class At>
+__device__ __forceinline__ void final_pass(const float2* W, At at, int jt, const float2* tw,
+                                           float2 (&fin)[16]) {
+    constexpr int T = M / 16;
+    constexpr int G = (M / R) / T;
+    static_assert(NS * R == M && G * R == 16, "final pass");
+#pragma unroll
+    for (int g = 0; g < G; g++) {
+        float2 v[R];
+        stockham_group<M, R, NS>(v, W, at, jt + g * T, tw);
+#pragma unroll
+        for (int r = 0; r < R; r++) fin[g + G * r] = v[r];
+    }
+}
+
+// the passes after the first radix-16 one (radix 16, then the remaining factor)
+template <int M, int NS, bool WARP>
+struct Passes {
+    static constexpr int R = (M / NS) >= 16 ? 16 : (M / NS);
+    template <class At>
+    __device__ __forceinline__ static void run(float2* W, At at, int jt, const float2* tw,
+                                               float2 (&fin)[16]) {
+        if constexpr (NS * R == M) {
+            final_pass<M, R, NS>(W, at, jt, tw, fin);
+        } else {
+            stockham_pass<M, R, NS, WARP>(W, at, jt, tw);
+            Passes<M, NS * R, WARP>::run(W, at, jt, tw, fin);
+        }
+    }
+};
+
+struct RowArgs {
+    const float* in[kMaxXfFields];
+    float* out[kMaxXfFields];
+    int kind[kMaxXfFields];   // QS_REDFT11 / QS_RODFT11 of each field
+    int nrows;                // rows per plane
+    int total;                // nf * nrows
+    float scale;
+    const float2* tab;        // tw[M], pre[M], post[M]
+};
+
+template <int M>
+__host__ __device__ constexpr int row_threads() {
+    return (M / 16) > 64 ? (M / 16) : 64;
+}
+
+// Transform along the contiguous axis: each sequence of T = M/16 threads
+// takes one row of n = 2M values (small blocks, so that the rows of a batch
+// spread evenly over the SMs).  Thread jt holds the pairs P[jt + T*b]
+// (P[i] = (x[2i], x[2i+1])); the mirrored element x[n-1-2i] of the
+// pre-twiddle and the mirrored output of the post-twiddle belong to thread
+// T-1-jt, a shuffle away when a row lies within one warp.  Shared slot of
+// element e: e + e/16 (one pad per 16 keeps the stride-16 stores of the first
+// pass free of bank conflicts).
+template <int M>
+__global__ void __launch_bounds__(row_threads<M>()) fft_rows_kernel(RowArgs a) {
+    constexpr int T = M / 16;
+    constexpr int NT = row_threads<M>();
+    constexpr int SEQ = NT / T;
+    constexpr int LD = M + M / 16;
+    constexpr bool WARP = T <= 32;
+    __shared__ float2 W[SEQ * LD];
+    __shared__ float2 tws[M];
+    __shared__ float2 posts[M];
+    for (int i = threadIdx.x; i < M; i += NT) {
+        tws[i] = a.tab[i];
+        posts[i] = a.tab[2 * M + i];
+    }
+    const int s = threadIdx.x / T, jt = threadIdx.x % T;
+    const int row = blockIdx.x * SEQ + s;
+    const bool valid = row < a.total;
+    const int f = valid ? row / a.nrows : 0, k = valid ? row % a.nrows : 0;
+    float2* Ws = W + s * LD;
+    auto at = [](int e) { return e + (e >> 4); };
+    pdl_wait();
+    const float* inf = a.in[0];
+    float* outf = a.out[0];
+    int kind = a.kind[0];
+#pragma unroll
+    for (int q = 1; q < kMaxXfFields; q++)
+        if (q == f) { inf = a.in[q]; outf = a.out[q]; kind = a.kind[q]; }
+    const float2* P = reinterpret_cast<const float2*>(inf + (size_t)k * 2 * M);
+    const float2* pre = a.tab + M;
+    // the 16 pairs of this thread in bit-reversed order, the pre-twiddle
+    float2 p[16], w[16];
+#pragma unroll
+    for (int b = 0; b < 16; b++) {
+        const int i = jt + bitrev<16>(b) * T;
+        p[b] = valid ? P[i] : make_float2(0.f, 0.f);
+        w[b] = __ldg(pre + i);
+    }
+    float2 v[16];
+    if constexpr (WARP) {
+        // x[n-1-2i] = P[M-1-i].y: slot 15-b of thread T-1-jt
+#pragma unroll
+        for (int b = 0; b < 16; b++) {
+            const float mirror = __shfl_xor_sync(0xffffffffu, p[15 - b].y, T - 1);
+            const float2 z = kind == QS_REDFT11 ? make_float2(p[b].x, mirror)
+                                                : make_float2(mirror, p[b].x);
+            v[b] = cmul(z, w[b]);
+        }
+    } else {
+#pragma unroll
+        for (int b = 0; b < 16; b++) {
+            const int i = jt + bitrev<16>(b) * T;
+            const float mirror = valid ? P[M - 1 - i].y : 0.f;
+            const float2 z = kind == QS_REDFT11 ? make_float2(p[b].x, mirror)
+                                                : make_float2(mirror, p[b].x);
+            v[b] = cmul(z, w[b]);
+        }
+    }
+    __syncthreads();   // twiddle tables in place
+    dft<16>(v);
+    float2 fin[16];
+    if constexpr (T == 1) {
+        // one pass: Z_r in slot r, the thread owns the whole sequence
+#pragma unroll
+        for (int r = 0; r < 16; r++) fin[r] = v[r];
+    } else {
+#pragma unroll
+        for (int r = 0; r < 16; r++) Ws[at(jt * 16 + r)] = v[r];
+        seq_sync<WARP>();
+        Passes<M, 16, WARP>::run(Ws, at, jt, tws, fin);
+    }
+    pdl_trigger();
+    // s_q = Z_q e^{-i pi (q+1/4)/n}; out pair q = (2 Re s_q, -+2 Im s_{M-1-q})
+    float im[16];
+#pragma unroll
+    for (int m = 0; m < 16; m++) {
+        const int q = jt + T * m;
+        const float2 sq = cmul(fin[m], posts[q]);
+        fin[m] = sq;
+        im[m] = sq.y;
+    }
+    float mirror[16];
+    if constexpr (WARP) {
+#pragma unroll
+        for (int m = 0; m < 16; m++) mirror[m] = __shfl_xor_sync(0xffffffffu, im[15 - m], T - 1);
+    } else {
+        // rows wider than a warp: the mirrored parts through shared memory
+        __syncthreads();
+        float* ims = reinterpret_cast<float*>(Ws);
+#pragma unroll
+        for (int m = 0; m < 16; m++) ims[jt + T * m] = im[m];
+        __syncthreads();
+#pragma unroll
+        for (int m = 0; m < 16; m++) mirror[m] = ims[M - 1 - (jt + T * m)];
+    }
+    if (!valid) return;
+    float2* O = reinterpret_cast<float2*>(outf + (size_t)k * 2 * M);
+    const float c2 = 2.f * a.scale;
+    const float sgn = kind == QS_REDFT11 ? -c2 : c2;
+#pragma unroll
+    for (int m = 0; m < 16; m++) O[jt + T * m] = make_float2(c2 * fin[m].x, sgn * mirror[m]);
+}
+
+struct ColArgs {
+    const float* in[kMaxXfFields];
+    float* out[kMaxXfFields];
+    int kind[kMaxXfFields];
+    int ncols;                // row length of the planes (the y size)
+    float scale;
+    const float2* tab;
+};
+
+// Transform along the strided axis: a CTA takes TJ adjacent columns of one
+// plane (TJ floats = whole 32-byte sectors per row); column c's sequence
+// lives at W[e * TJ + c], its T threads are TJ lanes apart.
+template <int M, int TJ>
+__global__ void __launch_bounds__(TJ * (M / 16)) fft_cols_kernel(ColArgs a) {
+    constexpr int T = M / 16;
+    constexpr int NT = TJ * T;
+    extern __shared__ float2 smem_f2[];
+    float2* tws = smem_f2;
+    float2* posts = smem_f2 + M;
+    float2* W = smem_f2 + 2 * M;
+    for (int i = threadIdx.x; i < M; i += NT) {
+        tws[i] = a.tab[i];
+        posts[i] = a.tab[2 * M + i];
+    }
+    const int c = threadIdx.x % TJ, jt = threadIdx.x / TJ;
+    const int f = blockIdx.y;
+    const int col = blockIdx.x * TJ + c;
+    const size_t ld = (size_t)a.ncols;
+    auto at = [c](int e) { return e * TJ + c; };
+    pdl_wait();
+    const float* inf = a.in[0];
+    float* outf = a.out[0];
+    int kind = a.kind[0];
+#pragma unroll
+    for (int q = 1; q < kMaxXfFields; q++)
+        if (q == f) { inf = a.in[q]; outf = a.out[q]; kind = a.kind[q]; }
+    const float2* pre = a.tab + M;
+    float lo[16], hi[16];
+    float2 w[16];
+#pragma unroll
+    for (int b = 0; b < 16; b++) {
+        const int i = jt + bitrev<16>(b) * T;
+        lo[b] = inf[(size_t)(2 * i) * ld + col];
+        hi[b] = inf[(size_t)(2 * M - 1 - 2 * i) * ld + col];
+        w[b] = __ldg(pre + i);
+    }
+    float2 v[16];
+#pragma unroll
+    for (int b = 0; b < 16; b++) {
+        const float2 z = kind == QS_REDFT11 ? make_float2(lo[b], hi[b]) : make_float2(hi[b], lo[b]);
+        v[b] = cmul(z, w[b]);
+    }
+    __syncthreads();
+    dft<16>(v);
+    float2 fin[16];
+    if constexpr (T == 1) {
+#pragma unroll
+        for (int r = 0; r < 16; r++) fin[r] = v[r];
+    } else {
+#pragma unroll
+        for (int r = 0; r < 16; r++) W[at(jt * 16 + r)] = v[r];
+        __syncthreads();
+        Passes<M, 16, false>::run(W, at, jt, tws, fin);
+    }
+    pdl_trigger();
+    float im[16];
+#pragma unroll
+    for (int m = 0; m < 16; m++) {
+        const int q = jt + T * m;
+        fin[m] = cmul(fin[m], posts[q]);
+        im[m] = fin[m].y;
+    }
+    __syncthreads();
+    float* ims = reinterpret_cast<float*>(W);
+#pragma unroll
+    for (int m = 0; m < 16; m++) ims[(jt + T * m) * TJ + c] = im[m];
+    __syncthreads();
+    const float c2 = 2.f * a.scale;
+    const float sgn = kind == QS_REDFT11 ? -c2 : c2;
+#pragma unroll
+    for (int m = 0; m < 16; m++) {
+        const int q = jt + T * m;
+        outf[(size_t)(2 * q) * ld + col] = c2 * fin[m].x;
+        outf[(size_t)(2 * q + 1) * ld + col] = sgn * ims[(M - 1 - q) * TJ + c];
+    }
+}
+
+template <int M>
+__host__ __device__ constexpr int cols_tj() {
+    return (M / 16) >= 64 ? 8 : (M / 16) >= 16 ? 8 : (M / 16) >= 4 ? 16 : 32;
+}
+
+template <int M>
+size_t cols_smem() {
+    return sizeof(float2) * (size_t)M * (2 + cols_tj<M>());
+}
+
+template <int M>
+cudaError_t set_cols_smem() {
+    return cudaFuncSetAttribute(fft_cols_kernel<M, cols_tj<M>()>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cols_smem<M>());
+}
+
+template <int M>
+cudaError_t launch_rows(const RowArgs& a, cudaStream_t st) {
+    constexpr int SEQ = row_threads<M>() / (M / 16);
+    const int blocks = (a.total + SEQ - 1) / SEQ;
+    return launch_pdl(fft_rows_kernel<M>, dim3((unsigned)blocks), dim3(row_threads<M>()), 0, st,
+                      a);
+}
+
+template <int M>
+cudaError_t launch_cols(const ColArgs& a, int nf, cudaStream_t st) {
+    constexpr int TJ = cols_tj<M>();
+    return launch_pdl(fft_cols_kernel<M, TJ>, dim3((unsigned)(a.ncols / TJ), (unsigned)nf),
+                      dim3(TJ * (M / 16)), cols_smem<M>(), st, a);
+}
+
+}  // namespace fft
+
+namespace {
+
+bool fft_size_ok(int n) { return n >= 32 && n <= 2048 && (n & (n - 1)) == 0; }
+
+// table of one size n: tw[M] = e^{-2 pi i k/M}, pre[M] = e^{-i pi i/n},
+// post[M] = e^{-i pi (i+1/4)/n}, M = n/2, built in FP64
+std::vector<float2> fft_table(int n) {
+    const int M = n / 2;
+    std::vector<float2> t(3 * (size_t)M);
+    for (int k = 0; k < M; k++) {
+        const double a = -2.0 * M_PI * k / M;
+        t[k] = make_float2((float)std::cos(a), (float)std::sin(a));
+        const double b = -M_PI * k / n;
+        t[M + k] = make_float2((float)std::cos(b), (float)std::sin(b));
+        const double c = -M_PI * (k + 0.25) / n;
+        t[2 * M + k] = make_float2((float)std::cos(c), (float)std::sin(c));
+    }
+    return t;
+}
+
+}  // namespace
+
+DttFft::~DttFft() {
+    if (tab_y) cudaFree(tab_y);
+    if (tab_z && tab_z != tab_y) cudaFree(tab_z);
+}
+
+DttFft* DttFft::create(int ny, int nz) {
+    if (!fft_size_ok(ny) || !fft_size_ok(nz)) return nullptr;
+    auto* d = new DttFft();
+    d->ny = ny;
+    d->nz = nz;
+    auto up = [](int n, float2** dst) {
+        std::vector<float2> t = fft_table(n);
+        if (cudaMalloc(dst, t.size() * sizeof(float2)) != cudaSuccess) return false;
+        return cudaMemcpy(*dst, t.data(), t.size() * sizeof(float2), cudaMemcpyHostToDevice) ==
+               cudaSuccess;
+    };
+    bool ok = up(ny, &d->tab_y);
+    if (ok) {
+        if (nz == ny) d->tab_z = d->tab_y;
+        else ok = up(nz, &d->tab_z);
+    }
+    cudaError_t e = cudaSuccess;
+    for (int n : {ny, nz}) {
+        switch (n / 2) {
+            case 1024: e = fft::set_cols_smem<1024>(); break;
+            case 512: e = fft::set_cols_smem<512>(); break;
+            case 256: e = fft::set_cols_smem<256>(); break;
+            case 128: e = fft::set_cols_smem<128>(); break;
+            case 64: e = fft::set_cols_smem<64>(); break;
+            case 32: e = fft::set_cols_smem<32>(); break;
+            default: e = fft::set_cols_smem<16>(); break;
+        }
+        if (e != cudaSuccess) ok = false;
+    }
+    if (!ok) {
+        delete d;
+        return nullptr;
+    }
+    return d;
+}
+
+int DttFft::run_pass(int pass, const DttJob<float>& job, float* scratch, cudaStream_t st) const {
+    if (job.nf <= 0 || job.nf > kMaxXfFields) return 0;
+    const size_t plane = (size_t)ny * nz;
+    cudaError_t e = cudaSuccess;
+    if (pass == 0) {   // along y: in -> scratch
+        fft::RowArgs a{};
+        for (int f = 0; f < job.nf; f++) {
+            a.in[f] = job.in[f];
+            a.out[f] = scratch + f * plane;
+            a.kind[f] = job.ky[f];
+        }
+        a.nrows = nz;
+        a.total = job.nf * nz;
+        a.scale = 1.f;
+        a.tab = tab_y;
+        switch (ny / 2) {
+            case 1024: e = fft::launch_rows<1024>(a, st); break;
+            case 512: e = fft::launch_rows<512>(a, st); break;
+            case 256: e = fft::launch_rows<256>(a, st); break;
+            case 128: e = fft::launch_rows<128>(a, st); break;
+            case 64: e = fft::launch_rows<64>(a, st); break;
+            case 32: e = fft::launch_rows<32>(a, st); break;
+            default: e = fft::launch_rows<16>(a, st); break;
+        }
+    } else {           // along z: scratch -> out, scaled
+        fft::ColArgs a{};
+        for (int f = 0; f < job.nf; f++) {
+            a.in[f] = scratch + f * plane;
+            a.out[f] = job.out[f];
+            a.kind[f] = job.kz[f];
+        }
+        a.ncols = ny;
+        a.scale = job.scale;
+        a.tab = tab_z;
+        switch (nz / 2) {
+            case 1024: e = fft::launch_cols<1024>(a, job.nf, st); break;
+            case 512: e = fft::launch_cols<512>(a, job.nf, st); break;
+            case 256: e = fft::launch_cols<256>(a, job.nf, st); break;
+            case 128: e = fft::launch_cols<128>(a, job.nf, st); break;
+            case 64: e = fft::launch_cols<64>(a, job.nf, st); break;
+            case 32: e = fft::launch_cols<32>(a, job.nf, st); break;
+            default: e = fft::launch_cols<16>(a, job.nf, st); break;
+        }
+    }
+    return e == cudaSuccess ? 1 : 0;
+}
+
+}  // namespace qs

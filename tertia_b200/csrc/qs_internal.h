@@ -85,6 +85,19 @@ int launch_convert_back(const T* src, double* dst, size_t n, cudaStream_t st);
 template <class T>
 int run_dtt_simt(const DttJob<T>& job, int ny, int nz, const DttMats<T>& my,
                  const DttMats<T>& mz, T* scratch, cudaStream_t st);
+// FP32 half-integer transforms through half-length complex FFTs
+// (dtt_fft.cu), for power-of-two ny, nz in [32, 2048]: pass 0 along y from
+// the job's inputs into `scratch` (same layout), pass 1 along z from there
+// into the job's outputs with its scale.
+struct DttFft {
+    int ny = 0, nz = 0;
+    float2* tab_y = nullptr;   // twiddle tables of each size
+    float2* tab_z = nullptr;
+    static DttFft* create(int ny, int nz);   // nullptr when a size is not handled
+    int run_pass(int pass, const DttJob<float>& job, float* scratch, cudaStream_t st) const;
+    ~DttFft();
+};
+
 template <class T>
 int run_dtt_simt_pass(int pass, const DttJob<T>& job, int ny, int nz, const DttMats<T>& my,
                       const DttMats<T>& mz, T* scratch, cudaStream_t st);

@@ -11,7 +11,8 @@ TOL = {"fp64": 1e-13, "fp32": 2e-6}
 
 
 @pytest.mark.parametrize("prec", ["fp64", "fp32"])
-@pytest.mark.parametrize("shape", [(32, 32), (64, 128), (128, 64), (256, 256)])
+@pytest.mark.parametrize("shape", [(32, 32), (64, 128), (128, 64), (256, 256), (512, 512),
+                                   (1024, 256), (2048, 32), (48, 40)])
 def test_transform_matches_oracle(oracle_lib, prec, shape):
     from tertia_b200.mesh import Mesh
     nz, ny = shape
