@@ -12,7 +12,7 @@ Default workload (N=1): c1 with CIC deposit, 512 x 512 transverse cells, 1024 la
 particles, synthetic seeded inputs.  The field store (6.4 GB) and beam-current
 store (2.1 GB) are far larger than L2, so every step streams from HBM.
 
-  python bench.py [--gpus N --steps K --warmup W --precision bf16x3 --shape cic]
+  python bench.py [--gpus N --steps K --warmup W --precision fp32 --shape cic]
   python bench.py --impl reference     # the reference's CPU path (oracle port)
 
 Under torchrun (N>1) every rank runs an independent replica: the march is
@@ -47,7 +47,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="c1")
-    ap.add_argument("--precision", default="bf16x3")
+    ap.add_argument("--precision", default="fp32")
     ap.add_argument("--shape", default="cic", choices=["cic", "ngp"],
                     help="plasma particle shape: CIC deposit (default) or the reference's "
                          "live NGP path")
@@ -410,6 +410,26 @@ def run_ours(args):
     # transform pass of the march (6 planes, one y- or z-pass per launch),
     # repeated with the launches queued ahead of the GPU
     gemm = None
+    fftp = None
+    if args.precision == "fp32":
+        # FFT passes (power-of-two grids): 2 launches per transform, each
+        # reading and writing the 6 planes once
+        nf = 6
+        xs = torch.randn(nf, cfg.nz, cfg.ny, device="cuda", dtype=torch.float32)
+        ys = torch.empty_like(xs)
+        for _ in range(3):
+            m.transform2d_dev(0, 1, nf, xs.data_ptr(), ys.data_ptr())
+        m.sync()
+        reps = 200
+        ev0.record(stream)
+        for _ in range(reps):
+            m.transform2d_dev(0, 1, nf, xs.data_ptr(), ys.data_ptr())
+        ev1.record(stream)
+        m.sync()
+        loop_us = ev0.elapsed_time(ev1) * 1e3 / reps
+        fftp = {"planes": nf, "launches_per_transform": 2, "avg_launch_us": loop_us / 2.0,
+                "loop_us_per_transform": loop_us}
+        del xs, ys
     if args.precision in ("bf16x3", "tf32x3", "bf16x6"):
         nf = 6
         xs = torch.randn(nf, cfg.nz, cfg.ny, device="cuda", dtype=torch.float32)
@@ -502,10 +522,22 @@ def run_ours(args):
         # transforms per (layer, split) in the march: 6 (Guess inverse E, B)
         # + (nIter+1) * (3 forward J + 6 inverse E, B) + 2 beam planes
         roof["march_transforms_per_layer"] = 6 + (nit + 1) * 9 + 2
+    elif fftp:
+        # one launch = one pass (along y or z) over 6 N x N FP32 planes: each
+        # plane read once and written once
+        bytes_launch = fftp["planes"] * 2.0 * 4.0 * cfg.ny * cfg.nz
+        achieved = bytes_launch / (fftp["avg_launch_us"] / 1e6) / 1e9
+        roof = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                "frac": achieved / hbm, "peak_source": f"hbm_gbs of {src}",
+                "kernel": "fft_rows_kernel / fft_cols_kernel (transform pass, 6 planes)",
+                "bytes_per_launch": bytes_launch, "avg_launch_us": fftp["avg_launch_us"],
+                "timing": fftp}
+        roof["march_transforms_per_layer"] = 6 + (nit + 1) * 9 + 2
     else:
         roof = {"bound": "hbm", "achieved": None, "peak": hbm, "unit": "GB/s", "frac": None,
                 "kernel": dom}
-    tr = traffic_record("dtt_tc_kernel" if gemm else dom, args.workload, args.precision)
+    tr = traffic_record("dtt_tc_kernel" if gemm else ("fft_pass" if fftp else dom),
+                        args.workload, args.precision)
     roof["traffic"] = tr.get("bytes_per_launch") if tr else None
     if tr:
         roof["traffic_source"] = tr.get("source")
