@@ -20,6 +20,7 @@
 
 #include "qs_common.cuh"
 #include "qs_internal.h"
+#include "pdl.cuh"
 
 namespace qs {
 
@@ -42,6 +43,7 @@ template <class T>
 __global__ void __launch_bounds__(256) push_adjoint_kernel(PushAdjArgs<T> a) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= a.n) return;
+    pdl_wait();
     const int My = a.My, Mz = a.Mz;
     const int cell = a.cell[i];
     const int j = cell % My, k = cell / My;
@@ -235,9 +237,7 @@ __global__ void __launch_bounds__(256) push_adjoint_kernel(PushAdjArgs<T> a) {
     // fields: E = (P + C)/2 and B = (P + C)/2 + external
 #pragma unroll
     for (int c = 0; c < 3; c++) {
-        atomicAdd(a.lamFP + c * plane + n, half * bE[c]);
         atomicAdd(a.lamFC + c * plane + n, half * bE[c]);
-        atomicAdd(a.lamFP + (3 + c) * plane + n, half * bB[c]);
         atomicAdd(a.lamFC + (3 + c) * plane + n, half * bB[c]);
     }
 }
@@ -245,7 +245,7 @@ __global__ void __launch_bounds__(256) push_adjoint_kernel(PushAdjArgs<T> a) {
 template <class T>
 int launch_push_adjoint(const PushAdjArgs<T>& a, cudaStream_t st) {
     if (a.n <= 0) return 0;
-    push_adjoint_kernel<T><<<(unsigned)((a.n + 255) / 256), 256, 0, st>>>(a);
+    launch_pdl(push_adjoint_kernel<T>, dim3((unsigned)((a.n + 255) / 256)), dim3(256), 0, st, a);
     return 1;
 }
 
@@ -263,6 +263,7 @@ template <class T>
 __global__ void __launch_bounds__(256) push_adjoint_cic_kernel(PushAdjArgs<T> a) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= a.n) return;
+    pdl_wait();
     const int My = a.My, Mz = a.Mz;
     const int cell = a.cell[i];
     const int j = cell % My, k = cell / My;
@@ -495,9 +496,7 @@ __global__ void __launch_bounds__(256) push_adjoint_cic_kernel(PushAdjArgs<T> a)
 #pragma unroll
         for (int f = 0; f < 6; f++) {
             bwg[r] += bg[f] * F[f][r];
-            const T v = half * wg[r] * bg[f];
-            atomicAdd(a.lamFP + f * plane + nn[r], v);
-            atomicAdd(a.lamFC + f * plane + nn[r], v);
+            atomicAdd(a.lamFC + f * plane + nn[r], half * wg[r] * bg[f]);
         }
     }
     lyp += (one - zp) * (bwg[1] - bwg[0]) + zp * (bwg[3] - bwg[2]);
@@ -520,7 +519,8 @@ __global__ void __launch_bounds__(256) push_adjoint_cic_kernel(PushAdjArgs<T> a)
 template <class T>
 int launch_push_adjoint_cic(const PushAdjArgs<T>& a, cudaStream_t st) {
     if (a.n <= 0) return 0;
-    push_adjoint_cic_kernel<T><<<(unsigned)((a.n + 255) / 256), 256, 0, st>>>(a);
+    launch_pdl(push_adjoint_cic_kernel<T>, dim3((unsigned)((a.n + 255) / 256)), dim3(256), 0, st,
+               a);
     return 1;
 }
 
@@ -589,6 +589,7 @@ __global__ void corrector_adjoint_kernel(AdjSpecArgs<T> a) {
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
     const int k = blockIdx.y;
     if (j >= a.ny) return;
+    pdl_wait();
     const size_t n = (size_t)j + (size_t)a.ny * k;
     const T d = *a.dens_p, hx = a.hx;
     const T akz = a.piZ * (T(k) + T(0.5));
@@ -629,6 +630,7 @@ __global__ void predictor_adjoint_kernel(AdjSpecArgs<T> a) {
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
     const int k = blockIdx.y;
     if (j >= a.ny) return;
+    pdl_wait();
     const size_t n = (size_t)j + (size_t)a.ny * k;
     const T d = *a.dens_p, hx = a.hx;
     const T akz = a.piZ * (T(k) + T(0.5));
@@ -675,14 +677,32 @@ __global__ void predictor_adjoint_kernel(AdjSpecArgs<T> a) {
 template <class T>
 int launch_corrector_adjoint(const AdjSpecArgs<T>& a, cudaStream_t st) {
     const dim3 g((unsigned)((a.ny + 127) / 128), (unsigned)a.nz);
-    corrector_adjoint_kernel<T><<<g, 128, 0, st>>>(a);
+    launch_pdl(corrector_adjoint_kernel<T>, g, dim3(128), 0, st, a);
     return 1;
 }
 
 template <class T>
 int launch_predictor_adjoint(const AdjSpecArgs<T>& a, cudaStream_t st) {
     const dim3 g((unsigned)((a.ny + 127) / 128), (unsigned)a.nz);
-    predictor_adjoint_kernel<T><<<g, 128, 0, st>>>(a);
+    launch_pdl(predictor_adjoint_kernel<T>, g, dim3(128), 0, st, a);
+    return 1;
+}
+
+// ---------------------------------------------------------------------------
+// acc += x over n values (the P-field adjoint gathers every push's share)
+template <class T>
+__global__ void add_planes_kernel(T* __restrict__ acc, const T* __restrict__ x, size_t n) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    pdl_wait();
+    acc[i] += x[i];
+}
+
+template <class T>
+int launch_add_planes(T* acc, const T* x, size_t n, cudaStream_t st) {
+    if (!n) return 0;
+    launch_pdl(add_planes_kernel<T>, dim3((unsigned)((n + 255) / 256)), dim3(256), 0, st, acc, x,
+               n);
     return 1;
 }
 
@@ -745,6 +765,7 @@ int launch_beam_weight_grad(const BeamGradArgs<T>& a, cudaStream_t st) {
     template int launch_corrector_adjoint<T>(const AdjSpecArgs<T>&, cudaStream_t);       \
     template int launch_predictor_adjoint<T>(const AdjSpecArgs<T>&, cudaStream_t);       \
     template int launch_add_point<T>(T*, size_t, const T*, int, cudaStream_t);           \
+    template int launch_add_planes<T>(T*, const T*, size_t, cudaStream_t);               \
     template int launch_beam_weight_grad<T>(const BeamGradArgs<T>&, cudaStream_t);
 QS_ADJ_INST(float)
 QS_ADJ_INST(double)

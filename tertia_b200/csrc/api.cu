@@ -1621,7 +1621,6 @@ struct Engine : EngineBase {
         a.P = Pf; a.C = Cfield;
         a.lamD = lamp(LAM_D);
         a.lamPm = lam_pm;
-        a.lamFP = lamp(LAM_PF);
         a.lamFC = lamp(LAM_CX);
         a.plane = plane;
         a.sE = (T)(cfg.plasma_q2m * cfg.hx / 2.0);
@@ -1671,6 +1670,8 @@ struct Engine : EngineBase {
         klaunch(KC_PUSH, [&] {
             return push_adjoint(push_adj_args(slot, slot_cell, fs + (size_t)nIter * 6 * plane, 1));
         });
+        // the P layer's field adjoint gathers every push's share
+        klaunch(KC_MISC, [&] { return launch_add_planes<T>(lamp(LAM_PF), lamp(LAM_CX), 6 * plane, st); });
         int rho_in = LAM_RHO0;
         for (int it = nIter - 1; it >= 0; it--) {
             adj_xform(lamp(LAM_CX), lamp(LAM_SPEC), 6, EBz, EBy, sc);
@@ -1691,6 +1692,9 @@ struct Engine : EngineBase {
             CK(cudaMemsetAsync(lamp(LAM_CX), 0, 6 * plane * sizeof(T), st));
             klaunch(KC_PUSH, [&] {
                 return push_adjoint(push_adj_args(slot, slot_cell, fs + (size_t)it * 6 * plane, 0));
+            });
+            klaunch(KC_MISC, [&] {
+                return launch_add_planes<T>(lamp(LAM_PF), lamp(LAM_CX), 6 * plane, st);
             });
         }
         // Guess: C fields <- inverse transforms of the predicted E, B

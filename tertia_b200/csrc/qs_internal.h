@@ -163,8 +163,7 @@ struct PushAdjArgs {
     const T* C;
     const T* lamD;        // 3 planes
     T* lamPm;             // 3 x n
-    T* lamFP;             // 6 planes
-    T* lamFC;             // 6 planes
+    T* lamFC;             // 6 planes: the field adjoint of this push (added to)
     T* lamPos;            // CIC: 2 x n adjoint of the in-cell positions y, z (like lamPm)
     size_t plane;
     T sE, hxhy, hxhz, djx0, djy0, djz0, bxe, bye, bze;
@@ -213,6 +212,9 @@ template <class T>
 int launch_predictor_adjoint(const AdjSpecArgs<T>& a, cudaStream_t st);
 template <class T>
 int launch_add_point(T* plane_ex, size_t idx, const T* v, int layer, cudaStream_t st);
+// acc += x over n values
+template <class T>
+int launch_add_planes(T* acc, const T* x, size_t n, cudaStream_t st);
 
 // d loss / d (beam macro-particle weight) from the adjoint of the real beam
 // currents (lb3: (L+1) layers x 2 planes RhoBeam, JxBeam).
