@@ -1058,6 +1058,19 @@ struct Engine : EngineBase {
             xform(job_stack(stage, 7, outs, kz, ky, T(1)));
             p_valid = true;
         }
+        if (fft_maps()) {
+            // predictor and the inverse y-pass of E, B in one kernel, then the z-pass
+            SpecArgs<T> a = spec_args(iLayer, iSplit);
+            a.zero_src = clear_by_maps() ? Csrc : nullptr;
+            a.write_b = 0;
+            if constexpr (sizeof(T) == 4)
+                klaunch(KC_SPECTRAL, [&] {
+                    return fftx->run_spectral_rows(a, false, nullptr, scratch, 6, st);
+                });
+            eb_zpass(6);
+            CK(cudaGetLastError());
+            return QS_OK;
+        }
         {
             SpecArgs<T> a = spec_args(iLayer, iSplit);
             a.zero_src = clear_by_maps() ? Csrc : nullptr;   // for the push that follows
@@ -1068,6 +1081,22 @@ struct Engine : EngineBase {
         inverse_EB(false);
         CK(cudaGetLastError());
         return QS_OK;
+    }
+
+    // FP32 FFT transforms with the Guess / Iterate maps between their halves
+    bool fft_maps() const { return fftx && fftx->spec_rows; }
+
+    // z-pass of the E, B (and Rho) planes the map kernel left in `scratch`:
+    // E, B into the C layer, Rho into the density plane of the C sources
+    void eb_zpass(int nout) {
+        if constexpr (sizeof(T) == 4) {
+            const float* ins[7];
+            float* outs[7] = {Cf, Cf + plane, Cf + 2 * plane, Cf + 3 * plane, Cf + 4 * plane,
+                              Cf + 5 * plane, Csrc + 3 * plane};
+            const int kz[7] = {CC, CC, SS, SS, SS, CC, CC};
+            for (int f = 0; f < nout; f++) ins[f] = scratch + (size_t)f * plane;
+            klaunch(KC_GEMM, [&] { return fftx->run_cols(nout, ins, outs, kz, inv_scale(), st); });
+        }
     }
 
     // Inside the march (no source store) the deposit planes are cleared by
@@ -1141,22 +1170,42 @@ struct Engine : EngineBase {
                 if (s) return s;
             }
         }
-        {   // :1343-1345
-            T* outs[3] = {bankp(cb, SP_JX), bankp(cb, SP_JY), bankp(cb, SP_JZ)};
-            const int kz[3] = {CC, CC, SS}, ky[3] = {CC, SS, CC};
-            xform(job_stack(Csrc, 3, outs, kz, ky, T(1)));
-        }
         // the last iterate stores Dens too (:1517-1602); inside the march that
         // real-space density is output only, so it is kept when sources are stored
         const bool want_rho = iter < 0 && (!in_march || src3 != nullptr);
-        SpecArgs<T> a = spec_args(iLayer, iSplit);
-        a.split_rho = want_rho ? 1 : 0;
-        // a push follows every Iterate but the last: clear its deposit planes
-        // (the forward J transform above has consumed them)
-        a.zero_src = (clear_by_maps() && iter >= 0) ? Csrc : nullptr;
-        klaunch(KC_SPECTRAL, [&] { return launch_corrector<T>(a, st); });
-        inverse_EB(want_rho);
-        CK(cudaGetLastError());
+        if (fft_maps()) {
+            // :1343-1345 along z, then the y-pass of J, the corrector and the
+            // inverse y-pass of E, B (, Rho) in one kernel, then their z-pass
+            if constexpr (sizeof(T) == 4) {
+                const float* ins[3] = {Csrc, Csrc + plane, Csrc + 2 * plane};
+                float* outs[3] = {scratch, scratch + plane, scratch + 2 * plane};
+                const int kz[3] = {CC, CC, SS};
+                klaunch(KC_GEMM, [&] { return fftx->run_cols(3, ins, outs, kz, 1.f, st); });
+                SpecArgs<T> a = spec_args(iLayer, iSplit);
+                a.write_b = 0;
+                a.zero_src = (clear_by_maps() && iter >= 0) ? Csrc : nullptr;
+                const int nout = want_rho ? 7 : 6;
+                klaunch(KC_SPECTRAL, [&] {
+                    return fftx->run_spectral_rows(a, true, scratch, scratch, nout, st);
+                });
+                eb_zpass(nout);
+            }
+            CK(cudaGetLastError());
+        } else {
+            {   // :1343-1345
+                T* outs[3] = {bankp(cb, SP_JX), bankp(cb, SP_JY), bankp(cb, SP_JZ)};
+                const int kz[3] = {CC, CC, SS}, ky[3] = {CC, SS, CC};
+                xform(job_stack(Csrc, 3, outs, kz, ky, T(1)));
+            }
+            SpecArgs<T> a = spec_args(iLayer, iSplit);
+            a.split_rho = want_rho ? 1 : 0;
+            // a push follows every Iterate but the last: clear its deposit planes
+            // (the forward J transform above has consumed them)
+            a.zero_src = (clear_by_maps() && iter >= 0) ? Csrc : nullptr;
+            klaunch(KC_SPECTRAL, [&] { return launch_corrector<T>(a, st); });
+            inverse_EB(want_rho);
+            CK(cudaGetLastError());
+        }
         if (rel_err) {
             std::vector<double> nw(plane);
             double mx[3] = {1e-5, 1e-5, 1e-5}, df[3] = {0, 0, 0};

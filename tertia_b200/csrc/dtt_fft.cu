@@ -25,6 +25,7 @@
 #include "qs_common.cuh"
 #include "qs_internal.h"
 #include "pdl.cuh"
+#include "spectral_f32.cuh"
 
 namespace qs {
 namespace fft {
@@ -422,6 +423,183 @@ cudaError_t launch_cols(const ColArgs& a, int nf, cudaStream_t st) {
                       dim3(TJ * (M / 16)), cols_smem<M>(), st, a);
 }
 
+// ---------------------------------------------------------------------------
+// The per-mode Guess / Iterate maps between the two halves of a transform.
+// The march transforms along z first (column kernel), so that one kernel can
+// take a z-mode row k through [forward y-transform of the deposit J] ->
+// [corrector or predictor on the row's modes] -> [inverse y-transform of E, B
+// (and Rho)], with the row in shared memory in between; the column kernel
+// then finishes the inverse along z.  A CTA holds one row: 8 groups of
+// T = M/16 lanes (one warp holds whole groups), each group taking one plane's
+// row through a transform; groups without a plane run it on zeros, so that
+// every lane meets every shuffle.
+
+// one row of n = 2M values through the half-integer transform of `kind` by
+// the T lanes of a group: in_pair(i) = (x[2i], x[2i+1]); out_pair(q, v) gets
+// the output pair q; `valid` false runs the group on zeros and stores nothing
+template <int M, class InPair, class OutPair>
+__device__ __forceinline__ void row_dtt_group(InPair in_pair, OutPair out_pair, int kind,
+                                              float scale, bool valid, int jt, float2* Wg,
+                                              const float2* tws, const float2* posts,
+                                              const float2* pre) {
+    constexpr int T = M / 16;
+    static_assert(T >= 1 && T <= 32, "a group within one warp");
+    auto at = [](int e) { return e + (e >> 4); };
+    float2 p[16], w[16];
+#pragma unroll
+    for (int b = 0; b < 16; b++) {
+        const int i = jt + bitrev<16>(b) * T;
+        p[b] = valid ? in_pair(i) : make_float2(0.f, 0.f);
+        w[b] = __ldg(pre + i);
+    }
+    float2 v[16];
+#pragma unroll
+    for (int b = 0; b < 16; b++) {
+        const float mirror = __shfl_xor_sync(0xffffffffu, p[15 - b].y, T - 1);
+        const float2 z = kind == QS_REDFT11 ? make_float2(p[b].x, mirror)
+                                            : make_float2(mirror, p[b].x);
+        v[b] = cmul(z, w[b]);
+    }
+    dft<16>(v);
+    float2 fin[16];
+    if constexpr (T == 1) {
+#pragma unroll
+        for (int r = 0; r < 16; r++) fin[r] = v[r];
+    } else {
+#pragma unroll
+        for (int r = 0; r < 16; r++) Wg[at(jt * 16 + r)] = v[r];
+        __syncwarp();
+        Passes<M, 16, true>::run(Wg, at, jt, tws, fin);
+    }
+    float im[16];
+#pragma unroll
+    for (int m = 0; m < 16; m++) {
+        fin[m] = cmul(fin[m], posts[jt + T * m]);
+        im[m] = fin[m].y;
+    }
+    const float c2 = 2.f * scale;
+    const float sgn = kind == QS_REDFT11 ? -c2 : c2;
+#pragma unroll
+    for (int m = 0; m < 16; m++) {
+        const float mirror = __shfl_xor_sync(0xffffffffu, im[15 - m], T - 1);
+        if (valid) out_pair(jt + T * m, make_float2(c2 * fin[m].x, sgn * mirror));
+    }
+    __syncwarp();   // Wg is free again
+}
+
+struct SpecRowArgs {
+    const float* jin;     // corrector: Jx, Jy, Jz after the z-pass (stride `plane`)
+    float* out;           // Ex, Ey, Ez, Bx, By, Bz (, Rho) after the inverse y-pass
+    int nout;             // 6, or 7 with Rho
+    const float2* tab;    // tables of the y size
+};
+
+constexpr int kSpecGroups = 8;
+
+template <int M>
+__host__ __device__ constexpr size_t spec_rows_smem() {
+    // tables, FFT work of each group, the row's J spectra and E, B, Rho spectra
+    return sizeof(float2) * (2 * (size_t)M + (size_t)kSpecGroups * (M + M / 16)) +
+           sizeof(float) * (3 + 7) * (size_t)(2 * M);
+}
+
+template <int M, bool CORRECT>
+__global__ void __launch_bounds__(kSpecGroups * (M / 16)) spectral_rows_kernel(SpecArgs<float> a,
+                                                                               SpecRowArgs r) {
+    using namespace specf32;
+    constexpr int T = M / 16;
+    constexpr int NT = kSpecGroups * T;
+    constexpr int N = 2 * M;
+    constexpr int LD = M + M / 16;
+    extern __shared__ float2 smem_f2[];
+    float2* tws = smem_f2;
+    float2* posts = tws + M;
+    float2* W = posts + M;
+    float* J = reinterpret_cast<float*>(W + kSpecGroups * LD);   // 3 x N
+    float* EB = J + 3 * N;                                        // 7 x N
+    for (int i = threadIdx.x; i < M; i += NT) {
+        tws[i] = r.tab[i];
+        posts[i] = r.tab[2 * M + i];
+    }
+    const int k = blockIdx.x;
+    const int g = threadIdx.x / T, jt = threadIdx.x % T;
+    float2* Wg = W + g * LD;
+    const float2* pre = r.tab + M;
+    const size_t plane = (size_t)N * a.nz;
+    pdl_wait();
+    __syncthreads();
+    if constexpr (CORRECT) {
+        // forward y-transform of the deposit rows (Jx REDFT11, Jy RODFT11, Jz REDFT11)
+        const bool valid = g < 3;
+        const int gg = valid ? g : 0;
+        const float2* src = reinterpret_cast<const float2*>(r.jin + gg * plane + (size_t)k * N);
+        float2* dst = reinterpret_cast<float2*>(J + gg * N);
+        row_dtt_group<M>([src](int i) { return src[i]; },
+                         [dst](int q, float2 v) { dst[q] = v; },
+                         gg == 1 ? QS_RODFT11 : QS_REDFT11, 1.f, valid, jt, Wg, tws, posts, pre);
+        __syncthreads();
+    }
+    // the maps on the row's modes, two per thread and step
+    for (int pj = threadIdx.x; pj < M; pj += NT) {
+        const int j = 2 * pj;
+        const size_t n = (size_t)j + (size_t)N * k;
+        Modes2 o;
+        if constexpr (CORRECT) {
+            const float2 jx2 = *reinterpret_cast<const float2*>(J + j);
+            const float2 jy2 = *reinterpret_cast<const float2*>(J + N + j);
+            const float2 jz2 = *reinterpret_cast<const float2*>(J + 2 * N + j);
+            st2(const_cast<float*>(a.Jx), n, jx2.x, jx2.y);   // the bank keeps the deposit spectra
+            st2(const_cast<float*>(a.Jy), n, jy2.x, jy2.y);
+            st2(const_cast<float*>(a.Jz), n, jz2.x, jz2.y);
+            o = corrector_modes2(a, j, k, n, jx2, jy2, jz2);
+        } else {
+            o = predictor_modes2(a, j, k, n);
+        }
+        store_modes2(a, n, o);
+        *reinterpret_cast<float2*>(EB + 0 * N + j) = make_float2(o.ex[0], o.ex[1]);
+        *reinterpret_cast<float2*>(EB + 1 * N + j) = make_float2(o.ey[0], o.ey[1]);
+        *reinterpret_cast<float2*>(EB + 2 * N + j) = make_float2(o.ez[0], o.ez[1]);
+        *reinterpret_cast<float2*>(EB + 3 * N + j) = make_float2(o.bx[0], o.bx[1]);
+        *reinterpret_cast<float2*>(EB + 4 * N + j) = make_float2(o.by[0], o.by[1]);
+        *reinterpret_cast<float2*>(EB + 5 * N + j) = make_float2(o.bz[0], o.bz[1]);
+        *reinterpret_cast<float2*>(EB + 6 * N + j) = make_float2(o.rho[0], o.rho[1]);
+    }
+    __syncthreads();
+    pdl_trigger();
+    // inverse y-transform of Ex Ey Ez Bx By Bz Rho (y kinds C S C S C S C)
+    {
+        const bool valid = g < r.nout;
+        const int gg = valid ? g : 0;
+        const float2* src = reinterpret_cast<const float2*>(EB + gg * N);
+        float2* dst = reinterpret_cast<float2*>(r.out + gg * plane + (size_t)k * N);
+        row_dtt_group<M>([src](int i) { return src[i]; },
+                         [dst](int q, float2 v) { dst[q] = v; },
+                         (gg & 1) ? QS_RODFT11 : QS_REDFT11, 1.f, valid, jt, Wg, tws, posts, pre);
+    }
+}
+
+template <int M>
+cudaError_t set_spec_rows_smem() {
+    cudaError_t e = cudaFuncSetAttribute(spectral_rows_kernel<M, true>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)spec_rows_smem<M>());
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(spectral_rows_kernel<M, false>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)spec_rows_smem<M>());
+    return e;
+}
+
+template <int M>
+cudaError_t launch_spec_rows(const SpecArgs<float>& a, const SpecRowArgs& r, bool correct,
+                             cudaStream_t st) {
+    const dim3 grid((unsigned)a.nz), block(kSpecGroups * (M / 16));
+    if (correct)
+        return launch_pdl(spectral_rows_kernel<M, true>, grid, block, spec_rows_smem<M>(), st, a,
+                          r);
+    return launch_pdl(spectral_rows_kernel<M, false>, grid, block, spec_rows_smem<M>(), st, a, r);
+}
+
 }  // namespace fft
 
 namespace {
@@ -468,6 +646,17 @@ DttFft* DttFft::create(int ny, int nz) {
         else ok = up(nz, &d->tab_z);
     }
     cudaError_t e = cudaSuccess;
+    // the maps between the two halves of a transform (rows within one warp)
+    if (ok && ny >= 128 && ny <= 1024) {
+        switch (ny / 2) {
+            case 512: e = fft::set_spec_rows_smem<512>(); break;
+            case 256: e = fft::set_spec_rows_smem<256>(); break;
+            case 128: e = fft::set_spec_rows_smem<128>(); break;
+            default: e = fft::set_spec_rows_smem<64>(); break;
+        }
+        d->spec_rows = e == cudaSuccess;
+        e = cudaSuccess;
+    }
     for (int n : {ny, nz}) {
         switch (n / 2) {
             case 1024: e = fft::set_cols_smem<1024>(); break;
@@ -485,6 +674,49 @@ DttFft* DttFft::create(int ny, int nz) {
         return nullptr;
     }
     return d;
+}
+
+int DttFft::run_cols(int nf, const float* const* in, float* const* out, const int* kind,
+                     float scale, cudaStream_t st) const {
+    if (nf <= 0 || nf > kMaxXfFields) return 0;
+    fft::ColArgs a{};
+    for (int f = 0; f < nf; f++) {
+        a.in[f] = in[f];
+        a.out[f] = out[f];
+        a.kind[f] = kind[f];
+    }
+    a.ncols = ny;
+    a.scale = scale;
+    a.tab = tab_z;
+    cudaError_t e;
+    switch (nz / 2) {
+        case 1024: e = fft::launch_cols<1024>(a, nf, st); break;
+        case 512: e = fft::launch_cols<512>(a, nf, st); break;
+        case 256: e = fft::launch_cols<256>(a, nf, st); break;
+        case 128: e = fft::launch_cols<128>(a, nf, st); break;
+        case 64: e = fft::launch_cols<64>(a, nf, st); break;
+        case 32: e = fft::launch_cols<32>(a, nf, st); break;
+        default: e = fft::launch_cols<16>(a, nf, st); break;
+    }
+    return e == cudaSuccess ? 1 : 0;
+}
+
+int DttFft::run_spectral_rows(const SpecArgs<float>& a, bool correct, const float* jin,
+                              float* out, int nout, cudaStream_t st) const {
+    if (!spec_rows) return 0;
+    fft::SpecRowArgs r{};
+    r.jin = jin;
+    r.out = out;
+    r.nout = nout;
+    r.tab = tab_y;
+    cudaError_t e;
+    switch (ny / 2) {
+        case 512: e = fft::launch_spec_rows<512>(a, r, correct, st); break;
+        case 256: e = fft::launch_spec_rows<256>(a, r, correct, st); break;
+        case 128: e = fft::launch_spec_rows<128>(a, r, correct, st); break;
+        default: e = fft::launch_spec_rows<64>(a, r, correct, st); break;
+    }
+    return e == cudaSuccess ? 1 : 0;
 }
 
 int DttFft::run_pass(int pass, const DttJob<float>& job, float* scratch, cudaStream_t st) const {

@@ -93,8 +93,18 @@ struct DttFft {
     int ny = 0, nz = 0;
     float2* tab_y = nullptr;   // twiddle tables of each size
     float2* tab_z = nullptr;
+    bool spec_rows = false;    // run_spectral_rows available (ny in [128, 1024])
     static DttFft* create(int ny, int nz);   // nullptr when a size is not handled
     int run_pass(int pass, const DttJob<float>& job, float* scratch, cudaStream_t st) const;
+    // the z-pass alone: nf planes in -> out, y-spectral or real alike
+    int run_cols(int nf, const float* const* in, float* const* out, const int* kind, float scale,
+                 cudaStream_t st) const;
+    // one z-mode row per CTA: [forward y-pass of the 3 z-transformed deposit
+    // planes at jin, when `correct`] -> corrector (or predictor) of `a` ->
+    // inverse y-pass of Ex Ey Ez Bx By Bz (, Rho when nout = 7) into `out`
+    // (planes of ny*nz, unscaled); jin and out may be the same planes
+    int run_spectral_rows(const SpecArgs<float>& a, bool correct, const float* jin, float* out,
+                          int nout, cudaStream_t st) const;
     ~DttFft();
 };
 

@@ -123,6 +123,18 @@ def test_cic_adjoint_fp32_close_to_fp64_adjoint():
     assert rel(grads["fp32"], grads["fp64"]) < 1e-4, grads
 
 
+def test_cic_adjoint_fp32_maps_inside_transforms():
+    """ny = 128: the recomputed march of the FP32 adjoint runs the maps
+    between the halves of its FFT transforms."""
+    beta = np.random.default_rng(11).uniform(0.5, 1.5, NBINS)
+    grads = {}
+    for prec in ("fp64", "fp32"):
+        cfg, m, beam, bins, coeff = setup(prec, n=128, layers=32, shape=QS_SHAPE_CIC)
+        grads[prec] = adjoint_grad(m, beam, bins, coeff, beta)
+        m.close()
+    assert rel(grads["fp32"], grads["fp64"]) < 1e-4, grads
+
+
 def test_cic_adjoint_checkpoint_interval_fp32():
     beta = np.random.default_rng(10).uniform(0.5, 1.5, NBINS)
     out = []

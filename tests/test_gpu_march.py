@@ -73,6 +73,21 @@ def test_cic_step_matches_oracle(oracle_lib, prec):
         assert np.any(po["cell"] != wl.front_plasma(cfg, seed=3)["cell"])   # particles moved
 
 
+@pytest.mark.parametrize("shape", [0, QS_SHAPE_CIC], ids=["ngp", "cic"])
+def test_fp32_maps_inside_the_transforms_match_oracle(oracle_lib, shape):
+    """At ny >= 128 the FP32 path applies the Guess / Iterate maps between the
+    two halves of its FFT transforms (one kernel per z-mode row)."""
+    cfg = cfg_for("fp32", n=128, layers=24, shape=shape, pspread_x=0.01, pspread_y=0.01,
+                  pspread_z=0.01)
+    beam = wl.small_beam(cfg, n=8000)
+    o, m = run_pair(oracle_lib, cfg, beam, [wl.front_plasma(cfg, seed=4)] * 2, steps=2)
+    e_o, e_m = o.onaxis_ex(), m.onaxis_ex()
+    assert np.max(np.abs(e_o)) > 1e-3
+    assert rel_l2(e_m, e_o) < TOL["fp32"]
+    assert rel_l2(fields_all(m, cfg, range(0, cfg.nx, 5)), fields_all(o, cfg, range(0, cfg.nx, 5))) \
+        < TOL["fp32"]
+
+
 def test_fine_grained_sequence_matches_march(oracle_lib):
     """qs_begin_march / layer_begin / move_split_layer / layer_end in the
     order of MoveAllSplitLayers give the march's layers."""
