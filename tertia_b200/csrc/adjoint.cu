@@ -21,6 +21,7 @@
 #include "qs_common.cuh"
 #include "qs_internal.h"
 #include "pdl.cuh"
+#include "adjoint_maps.cuh"
 
 namespace qs {
 
@@ -259,17 +260,19 @@ int launch_push_adjoint(const PushAdjArgs<T>& a, cudaStream_t st) {
 // sub-steps is piecewise constant).  Up to kMaxSub sub-steps are followed.
 constexpr int kMaxSub = 8;
 
+// The adjoint of particle i: its momentum and position adjoints are stored,
+// the adjoint of the fields it gathered (6 fields x 4 corners of its cell,
+// index f*4 + r) goes to lf, and its cell is returned (-1 when the forward
+// skipped the particle).
 template <class T>
-__global__ void __launch_bounds__(256) push_adjoint_cic_kernel(PushAdjArgs<T> a) {
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= a.n) return;
-    pdl_wait();
+__device__ __forceinline__ int push_adjoint_cic_one(const PushAdjArgs<T>& a, int64_t i,
+                                                    T (&lf)[24]) {
     const int My = a.My, Mz = a.Mz;
     const int cell = a.cell[i];
     const int j = cell % My, k = cell / My;
     const T one = T(1), half = T(0.5);
     const T yp = a.y[i], zp = a.z[i];
-    if (!(yp >= T(0) && yp <= one && zp >= T(0) && zp <= one)) return;   // forward skipped it
+    if (!(yp >= T(0) && yp <= one && zp >= T(0) && zp <= one)) return -1;   // forward skipped it
     const T px0 = a.px[i], py0 = a.py[i], pz0 = a.pz[i];
     const T w = a.w[i];
     const size_t plane = a.plane;
@@ -496,7 +499,7 @@ __global__ void __launch_bounds__(256) push_adjoint_cic_kernel(PushAdjArgs<T> a)
 #pragma unroll
         for (int f = 0; f < 6; f++) {
             bwg[r] += bg[f] * F[f][r];
-            atomicAdd(a.lamFC + f * plane + nn[r], half * wg[r] * bg[f]);
+            lf[f * 4 + r] = half * wg[r] * bg[f];
         }
     }
     lyp += (one - zp) * (bwg[1] - bwg[0]) + zp * (bwg[3] - bwg[2]);
@@ -513,6 +516,56 @@ __global__ void __launch_bounds__(256) push_adjoint_cic_kernel(PushAdjArgs<T> a)
         a.lamPm[2 * a.n + i] += bp[2];
         a.lamPos[i] += lyp;
         a.lamPos[a.n + i] += lzp;
+    }
+    return cell;
+}
+
+// Sums of v over runs of lanes with equal key (the particles of a warp are
+// grouped by cell): the first lane of each run gets its run's sum and true.
+template <int NV, class T>
+__device__ __forceinline__ bool warp_run_sums(T (&v)[NV], int key) {
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const int prevKey = __shfl_up_sync(full, key, 1);
+    const unsigned starts = __ballot_sync(full, lane == 0 || prevKey != key);
+    const int rs = 31 - __clz(starts & (0xffffffffu >> (31 - lane)));   // run start
+    const unsigned after = starts & ~(0xffffffffu >> (31 - lane));       // starts > lane
+    const int re = after ? __ffs(after) - 2 : 31;                        // run end
+    const int maxrun = (int)__reduce_max_sync(full, key >= 0 ? (unsigned)(re - rs + 1) : 1u);
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        if (maxrun > d) {   // the same for every lane
+            const bool take = lane + d <= re && ((lane - rs) & (2 * d - 1)) == 0;
+#pragma unroll
+            for (int q = 0; q < NV; q++) {
+                const T o = __shfl_down_sync(full, v[q], d);
+                if (take) v[q] += o;
+            }
+        }
+    }
+    return key >= 0 && lane == rs;
+}
+
+template <class T>
+__global__ void __launch_bounds__(256) push_adjoint_cic_kernel(PushAdjArgs<T> a) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    pdl_wait();
+    T lf[24];
+#pragma unroll
+    for (int q = 0; q < 24; q++) lf[q] = T(0);
+    const int cell = i < a.n ? push_adjoint_cic_one(a, i, lf) : -1;
+    // the field adjoints of a cell's particles summed in the warp, then one
+    // atomic per field and corner
+    if (warp_run_sums<24>(lf, cell)) {
+        const int My = a.My, Mz = a.Mz;
+        const int j = cell % My, k = cell / My;
+        const int j1 = wrap_m(j + 1, My), k1 = wrap_m(k + 1, Mz);
+        const size_t nn[4] = {(size_t)j + (size_t)My * k, (size_t)j1 + (size_t)My * k,
+                              (size_t)j + (size_t)My * k1, (size_t)j1 + (size_t)My * k1};
+#pragma unroll
+        for (int f = 0; f < 6; f++)
+#pragma unroll
+            for (int r = 0; r < 4; r++) atomicAdd(a.lamFC + f * a.plane + nn[r], lf[f * 4 + r]);
     }
 }
 
@@ -559,119 +612,33 @@ int launch_permute_adjoint(const int32_t* id_from, const int32_t* id_to, int64_t
 // per-mode adjoints of the spectral maps
 
 template <class T>
-__device__ __forceinline__ void beam_adj(const AdjSpecArgs<T>& a, size_t n, T lrb, T lrbp,
-                                         T ljxb) {
-    if (a.wb0 != T(0)) {
-        a.lRb0[n] += a.wb0 * lrb;
-        a.lJxb0[n] += a.wb0 * ljxb;
-    }
-    if (a.wb1 != T(0)) {
-        a.lRb1[n] += a.wb1 * lrb;
-        a.lJxb1[n] += a.wb1 * ljxb;
-    }
-    if (a.wp0 != T(0)) a.lRbp0[n] += a.wp0 * lrbp;
-    if (a.wp1 != T(0)) a.lRbp1[n] += a.wp1 * lrbp;
-}
-
-template <class T>
-__device__ __forceinline__ T opt(const T* p, size_t n) { return p ? p[n] : T(0); }
-
-template <class T>
-__device__ __forceinline__ void put_lp(const AdjSpecArgs<T>& a, int f, size_t n, T v) {
-    if (a.lP_set) a.lP[f][n] = v;
-    else a.lP[f][n] += v;
-}
-
-// Transpose of corrector_kernel (IterateFieldsHydroLinLayerSplit's per-mode
-// update, movefieldshydrolinlayersplit.cpp:1419-1466).
-template <class T>
 __global__ void corrector_adjoint_kernel(AdjSpecArgs<T> a) {
+    using namespace adjmaps;
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
     const int k = blockIdx.y;
     if (j >= a.ny) return;
     pdl_wait();
     const size_t n = (size_t)j + (size_t)a.ny * k;
-    const T d = *a.dens_p, hx = a.hx;
-    const T akz = a.piZ * (T(k) + T(0.5));
-    const T aky = a.piY * (T(j) + T(0.5));
-    const T k2 = aky * aky + akz * akz;
-    const T lrho = opt(a.lRho, n);
-    const T lex = opt(a.lE[0], n) + opt(a.lEb[0], n);
-    T ley = opt(a.lE[1], n) + opt(a.lEb[1], n);
-    T lez = opt(a.lE[2], n) + opt(a.lEb[2], n);
-    const T lbx = opt(a.lB[0], n), lby = opt(a.lB[1], n), lbz = opt(a.lB[2], n);
-    // by = (-akz (jx + jxb) + d ez)/k2, bz = (aky (jx + jxb) - d ey)/k2
-    lez += d * lby / k2;
-    ley -= d * lbz / k2;
-    const T ljxs = (-akz * lby + aky * lbz) / k2;          // d(by,bz)/d(jx + jxb)
-    T ljx = lrho + ljxs + opt(a.lJb[0], n);
-    T ljy = -hx * T(0.5) * aky * lrho - aky / k2 * lex + akz / k2 * lbx + opt(a.lJb[1], n);
-    T ljz = -hx * T(0.5) * akz * lrho - akz / k2 * lex - aky / k2 * lbx + opt(a.lJb[2], n);
-    const T lsrc = (aky * ley + akz * lez) / (d + k2);     // src = rb + rbp + rp + rho_old
-    a.lJ[0][n] = ljx;
-    a.lJ[1][n] = ljy;
-    a.lJ[2][n] = ljz;
-    a.lRhoOld[n] = lsrc;
-    // P-bank inputs: 0 RhoP, 1 ExP, 2 EyP, 3 EzP, 4 JxP, 5 JyP, 6 JzP
-    put_lp(a, 0, n, lrho + lsrc);
-    if (a.lP_set) a.lP[1][n] = T(0);
-    put_lp(a, 2, n, -ley);
-    put_lp(a, 3, n, -lez);
-    put_lp(a, 4, n, -lrho);
-    put_lp(a, 5, n, -hx * T(0.5) * aky * lrho);
-    put_lp(a, 6, n, -hx * T(0.5) * akz * lrho);
-    beam_adj(a, n, lsrc, lsrc, ljxs);
+    const T le[3] = {opt(a.lE[0], n), opt(a.lE[1], n), opt(a.lE[2], n)};
+    const T lb[3] = {opt(a.lB[0], n), opt(a.lB[1], n), opt(a.lB[2], n)};
+    T lj[3];
+    corrector_adjoint_mode(a, j, k, n, le, lb, lj);
+    a.lJ[0][n] = lj[0];
+    a.lJ[1][n] = lj[1];
+    a.lJ[2][n] = lj[2];
 }
 
-// Transpose of predictor_kernel (GuessFieldsHydroLinLayerSplit's per-mode
-// update, movefieldshydrolinlayersplit.cpp:843-872).
 template <class T>
 __global__ void predictor_adjoint_kernel(AdjSpecArgs<T> a) {
+    using namespace adjmaps;
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
     const int k = blockIdx.y;
     if (j >= a.ny) return;
     pdl_wait();
     const size_t n = (size_t)j + (size_t)a.ny * k;
-    const T d = *a.dens_p, hx = a.hx;
-    const T akz = a.piZ * (T(k) + T(0.5));
-    const T aky = a.piY * (T(j) + T(0.5));
-    const T k2 = aky * aky + akz * akz;
-    const T den = T(4) + d * hx * hx;
-    const T prop = (T(4) - d * hx * hx) / den;
-    const T lrho = opt(a.lRho, n);
-    T lex = opt(a.lE[0], n), ley = opt(a.lE[1], n), lez = opt(a.lE[2], n);
-    const T lbx = opt(a.lB[0], n), lby = opt(a.lB[1], n), lbz = opt(a.lB[2], n);
-    // b from the predicted currents and fields
-    const T ljx = (-akz * lby + aky * lbz) / k2;   // also the jxb adjoint
-    const T ljy = akz * lbx / k2;
-    const T ljz = -aky * lbx / k2;
-    lez += d * lby / k2;
-    ley -= d * lbz / k2;
-    // jx = jxp + hx d (ex + exp)/2 (and y, z)
-    const T hd2 = hx * d * T(0.5);
-    lex += hd2 * ljx;
-    ley += hd2 * ljy;
-    lez += hd2 * ljz;
-    T lexp = hd2 * ljx, leyp = hd2 * ljy, lezp = hd2 * ljz;
-    // ey = -eyp + aky src/(d + k2), src = rb + rbp + rp + rho
-    const T lsrc = (aky * ley + akz * lez) / (d + k2);
-    leyp -= ley;
-    lezp -= lez;
-    const T lrho_t = lrho + lsrc;
-    // rho = prop rp - (rb + rbp) d hx^2/den + 4 exp hx (k2 + d)/den
-    // ex  = prop exp - 2 (2 rp + rb + rbp) d hx / ((k2 + d) den)
-    const T cex = T(2) * d * hx / ((k2 + d) * den);
-    const T lrp = lsrc + prop * lrho_t - T(2) * cex * lex;
-    const T lrb = lsrc - d * hx * hx / den * lrho_t - cex * lex;
-    lexp += T(4) * hx * (k2 + d) / den * lrho_t + prop * lex;
-    put_lp(a, 0, n, lrp);
-    put_lp(a, 1, n, lexp);
-    put_lp(a, 2, n, leyp);
-    put_lp(a, 3, n, lezp);
-    put_lp(a, 4, n, ljx);
-    put_lp(a, 5, n, ljy);
-    put_lp(a, 6, n, ljz);
-    beam_adj(a, n, lrb, lrb, ljx);
+    const T le[3] = {opt(a.lE[0], n), opt(a.lE[1], n), opt(a.lE[2], n)};
+    const T lb[3] = {opt(a.lB[0], n), opt(a.lB[1], n), opt(a.lB[2], n)};
+    predictor_adjoint_mode(a, j, k, n, le, lb);
 }
 
 template <class T>
