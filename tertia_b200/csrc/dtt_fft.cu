@@ -503,12 +503,20 @@ __host__ __device__ constexpr size_t spec_rows_smem() {
            sizeof(float) * (3 + 7) * (size_t)(2 * M);
 }
 
+// threads of a map CTA: the transform groups, or one per mode pair if more
+template <int M>
+__host__ __device__ constexpr int spec_threads() {
+    return kSpecGroups * (M / 16) > M ? kSpecGroups * (M / 16) : M;
+}
+
 template <int M, bool CORRECT>
-__global__ void __launch_bounds__(kSpecGroups * (M / 16)) spectral_rows_kernel(SpecArgs<float> a,
-                                                                               SpecRowArgs r) {
+__global__ void __launch_bounds__(spec_threads<M>()) spectral_rows_kernel(SpecArgs<float> a,
+                                                                          SpecRowArgs r) {
     using namespace specf32;
     constexpr int T = M / 16;
-    constexpr int NT = kSpecGroups * T;
+    constexpr int NTF = kSpecGroups * T;   // the transform groups (whole warps)
+    constexpr int NT = spec_threads<M>();
+    static_assert(NTF % 32 == 0, "transform groups fill whole warps");
     constexpr int N = 2 * M;
     constexpr int LD = M + M / 16;
     extern __shared__ float2 smem_f2[];
@@ -530,16 +538,20 @@ __global__ void __launch_bounds__(kSpecGroups * (M / 16)) spectral_rows_kernel(S
     __syncthreads();
     if constexpr (CORRECT) {
         // forward y-transform of the deposit rows (Jx REDFT11, Jy RODFT11, Jz REDFT11)
-        const bool valid = g < 3;
-        const int gg = valid ? g : 0;
-        const float2* src = reinterpret_cast<const float2*>(r.jin + gg * plane + (size_t)k * N);
-        float2* dst = reinterpret_cast<float2*>(J + gg * N);
-        row_dtt_group<M>([src](int i) { return src[i]; },
-                         [dst](int q, float2 v) { dst[q] = v; },
-                         gg == 1 ? QS_RODFT11 : QS_REDFT11, 1.f, valid, jt, Wg, tws, posts, pre);
+        if (threadIdx.x < NTF) {
+            const bool valid = g < 3;
+            const int gg = valid ? g : 0;
+            const float2* src =
+                reinterpret_cast<const float2*>(r.jin + gg * plane + (size_t)k * N);
+            float2* dst = reinterpret_cast<float2*>(J + gg * N);
+            row_dtt_group<M>([src](int i) { return src[i]; },
+                             [dst](int q, float2 v) { dst[q] = v; },
+                             gg == 1 ? QS_RODFT11 : QS_REDFT11, 1.f, valid, jt, Wg, tws, posts,
+                             pre);
+        }
         __syncthreads();
     }
-    // the maps on the row's modes, two per thread and step
+    // the maps on the row's modes, two per thread
     for (int pj = threadIdx.x; pj < M; pj += NT) {
         const int j = 2 * pj;
         const size_t n = (size_t)j + (size_t)N * k;
@@ -567,7 +579,7 @@ __global__ void __launch_bounds__(kSpecGroups * (M / 16)) spectral_rows_kernel(S
     __syncthreads();
     pdl_trigger();
     // inverse y-transform of Ex Ey Ez Bx By Bz Rho (y kinds C S C S C S C)
-    {
+    if (threadIdx.x < NTF) {
         const bool valid = g < r.nout;
         const int gg = valid ? g : 0;
         const float2* src = reinterpret_cast<const float2*>(EB + gg * N);
@@ -593,7 +605,7 @@ cudaError_t set_spec_rows_smem() {
 template <int M>
 cudaError_t launch_spec_rows(const SpecArgs<float>& a, const SpecRowArgs& r, bool correct,
                              cudaStream_t st) {
-    const dim3 grid((unsigned)a.nz), block(kSpecGroups * (M / 16));
+    const dim3 grid((unsigned)a.nz), block(spec_threads<M>());
     if (correct)
         return launch_pdl(spectral_rows_kernel<M, true>, grid, block, spec_rows_smem<M>(), st, a,
                           r);
