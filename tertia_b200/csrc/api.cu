@@ -1686,6 +1686,31 @@ struct Engine : EngineBase {
         return cic_adj ? launch_push_adjoint_cic<T>(a, st) : launch_push_adjoint<T>(a, st);
     }
 
+    // the adjoint of [inverse transforms of E, B] <- map <- [forward transform
+    // of J] with the map between the halves of the transforms: z-pass of the
+    // six field adjoints at `lf`, y-pass + the map's adjoint (+ the y-pass of
+    // the current adjoints) per z-mode row, then their z-pass into LAM_D
+    void adj_map_fused(const T* lf, const AdjSpecArgs<T>& a, bool correct) {
+        if constexpr (sizeof(T) == 4) {
+            const int EBz[6] = {CC, CC, SS, SS, SS, CC}, Jz[3] = {CC, CC, SS};
+            const float* ins[6];
+            float* outs[6];
+            for (int f = 0; f < 6; f++) {
+                ins[f] = lf + (size_t)f * plane;
+                outs[f] = scratch + (size_t)f * plane;
+            }
+            klaunch(KC_GEMM, [&] { return fftx->run_cols(6, ins, outs, EBz, inv_scale(), st); });
+            klaunch(KC_SPECTRAL, [&] {
+                return fftx->run_adjoint_rows(a, correct, scratch, scratch, st);
+            });
+            if (correct) {
+                const float* ji[3] = {scratch, scratch + plane, scratch + 2 * plane};
+                float* jo[3] = {lamp(LAM_D), lamp(LAM_D + 1), lamp(LAM_D + 2)};
+                klaunch(KC_GEMM, [&] { return fftx->run_cols(3, ji, jo, Jz, 1.f, st); });
+            }
+        }
+    }
+
     qs_status adjoint_layer(int i, const T* slot, const int32_t* slot_cell) {
         const int EBz[6] = {CC, CC, SS, SS, SS, CC}, EBy[6] = {CC, SS, CC, SS, CC, SS};
         const int Jz[3] = {CC, CC, SS}, Jy[3] = {CC, SS, CC};
@@ -1698,7 +1723,7 @@ struct Engine : EngineBase {
                                        d_dloss, i, st);
         });
         // final Iterate: C fields <- inverse transforms of its E, B
-        adj_xform(lamp(LAM_CF), lamp(LAM_SPEC), 6, EBz, EBy, sc);
+        if (!fft_maps()) adj_xform(lamp(LAM_CF), lamp(LAM_SPEC), 6, EBz, EBy, sc);
         {
             AdjSpecArgs<T> a = adj_args(i);
             a.lRho = lamp(LAM_C + 0);
@@ -1712,9 +1737,13 @@ struct Engine : EngineBase {
             a.lRhoOld = lamp(LAM_RHO0);
             for (int f = 0; f < 7; f++) a.lP[f] = lamp(LAM_P + f);
             a.lP_set = 1;
-            klaunch(KC_SPECTRAL, [&] { return launch_corrector_adjoint<T>(a, st); });
+            if (fft_maps()) {
+                adj_map_fused(lamp(LAM_CF), a, true);
+            } else {
+                klaunch(KC_SPECTRAL, [&] { return launch_corrector_adjoint<T>(a, st); });
+                adj_xform(lamp(LAM_J), lamp(LAM_D), 3, Jz, Jy, T(1));
+            }
         }
-        adj_xform(lamp(LAM_J), lamp(LAM_D), 3, Jz, Jy, T(1));
         CK(cudaMemsetAsync(lamp(LAM_CX), 0, 6 * plane * sizeof(T), st));
         klaunch(KC_PUSH, [&] {
             return push_adjoint(push_adj_args(slot, slot_cell, fs + (size_t)nIter * 6 * plane, 1));
@@ -1723,7 +1752,7 @@ struct Engine : EngineBase {
         klaunch(KC_MISC, [&] { return launch_add_planes<T>(lamp(LAM_PF), lamp(LAM_CX), 6 * plane, st); });
         int rho_in = LAM_RHO0;
         for (int it = nIter - 1; it >= 0; it--) {
-            adj_xform(lamp(LAM_CX), lamp(LAM_SPEC), 6, EBz, EBy, sc);
+            if (!fft_maps()) adj_xform(lamp(LAM_CX), lamp(LAM_SPEC), 6, EBz, EBy, sc);
             AdjSpecArgs<T> a = adj_args(i);
             a.lRho = lamp(rho_in);
             const int rho_out = rho_in == LAM_RHO0 ? LAM_RHO0 + 1 : LAM_RHO0;
@@ -1735,9 +1764,13 @@ struct Engine : EngineBase {
             a.lRhoOld = lamp(rho_out);
             for (int f = 0; f < 7; f++) a.lP[f] = lamp(LAM_P + f);
             a.lP_set = 0;
-            klaunch(KC_SPECTRAL, [&] { return launch_corrector_adjoint<T>(a, st); });
+            if (fft_maps()) {
+                adj_map_fused(lamp(LAM_CX), a, true);
+            } else {
+                klaunch(KC_SPECTRAL, [&] { return launch_corrector_adjoint<T>(a, st); });
+                adj_xform(lamp(LAM_J), lamp(LAM_D), 3, Jz, Jy, T(1));
+            }
             rho_in = rho_out;
-            adj_xform(lamp(LAM_J), lamp(LAM_D), 3, Jz, Jy, T(1));
             CK(cudaMemsetAsync(lamp(LAM_CX), 0, 6 * plane * sizeof(T), st));
             klaunch(KC_PUSH, [&] {
                 return push_adjoint(push_adj_args(slot, slot_cell, fs + (size_t)it * 6 * plane, 0));
@@ -1747,7 +1780,7 @@ struct Engine : EngineBase {
             });
         }
         // Guess: C fields <- inverse transforms of the predicted E, B
-        adj_xform(lamp(LAM_CX), lamp(LAM_SPEC), 6, EBz, EBy, sc);
+        if (!fft_maps()) adj_xform(lamp(LAM_CX), lamp(LAM_SPEC), 6, EBz, EBy, sc);
         {
             AdjSpecArgs<T> a = adj_args(i);
             a.lRho = lamp(rho_in);
@@ -1757,7 +1790,8 @@ struct Engine : EngineBase {
             }
             for (int f = 0; f < 7; f++) a.lP[f] = lamp(LAM_P + f);
             a.lP_set = 0;
-            klaunch(KC_SPECTRAL, [&] { return launch_predictor_adjoint<T>(a, st); });
+            if (fft_maps()) adj_map_fused(lamp(LAM_CX), a, false);
+            else klaunch(KC_SPECTRAL, [&] { return launch_predictor_adjoint<T>(a, st); });
         }
         // hand the P-side adjoints to layer i+1 (its final bank and fields)
         CK(cudaMemcpyAsync(lamp(LAM_C), lamp(LAM_P), 7 * plane * sizeof(T),

@@ -26,6 +26,7 @@
 #include "qs_internal.h"
 #include "pdl.cuh"
 #include "spectral_f32.cuh"
+#include "adjoint_maps.cuh"
 
 namespace qs {
 namespace fft {
@@ -612,6 +613,116 @@ cudaError_t launch_spec_rows(const SpecArgs<float>& a, const SpecRowArgs& r, boo
     return launch_pdl(spectral_rows_kernel<M, false>, grid, block, spec_rows_smem<M>(), st, a, r);
 }
 
+// The adjoints of the maps in the same arrangement (the transforms are their
+// own transposes): a CTA takes z-mode row k of the six field adjoints (after
+// their z-pass) through the y-pass, the corrector's (or predictor's) adjoint
+// on the row's modes, one mode per thread, and for the corrector the y-pass
+// of the three current adjoints.
+struct AdjRowArgs {
+    const float* in;      // the 6 field adjoints after the z-pass (stride `plane`)
+    float* out;           // corrector: the 3 current adjoints after the y-pass
+    const float2* tab;
+};
+
+template <int M>
+__host__ __device__ constexpr size_t adj_rows_smem() {
+    return sizeof(float2) * (2 * (size_t)M + (size_t)kSpecGroups * (M + M / 16)) +
+           sizeof(float) * (6 + 3) * (size_t)(2 * M);
+}
+
+template <int M>
+__host__ __device__ constexpr int adj_threads() {
+    return kSpecGroups * (M / 16) > 2 * M ? kSpecGroups * (M / 16) : 2 * M;
+}
+
+template <int M, bool CORRECT>
+__global__ void __launch_bounds__(adj_threads<M>()) adjoint_rows_kernel(AdjSpecArgs<float> a,
+                                                                       AdjRowArgs r) {
+    using namespace adjmaps;
+    constexpr int T = M / 16;
+    constexpr int NTF = kSpecGroups * T;
+    constexpr int NT = adj_threads<M>();
+    constexpr int N = 2 * M;
+    constexpr int LD = M + M / 16;
+    static_assert(NTF % 32 == 0, "transform groups fill whole warps");
+    extern __shared__ float2 smem_f2[];
+    float2* tws = smem_f2;
+    float2* posts = tws + M;
+    float2* W = posts + M;
+    float* IN = reinterpret_cast<float*>(W + kSpecGroups * LD);   // 6 x N
+    float* OUT = IN + 6 * N;                                       // 3 x N
+    for (int i = threadIdx.x; i < M; i += NT) {
+        tws[i] = r.tab[i];
+        posts[i] = r.tab[2 * M + i];
+    }
+    const int k = blockIdx.x;
+    const int g = threadIdx.x / T, jt = threadIdx.x % T;
+    float2* Wg = W + g * LD;
+    const float2* pre = r.tab + M;
+    const size_t plane = (size_t)N * a.nz;
+    pdl_wait();
+    __syncthreads();
+    if (threadIdx.x < NTF) {   // y-pass of the field adjoints (y kinds C S C S C S)
+        const bool valid = g < 6;
+        const int gg = valid ? g : 0;
+        const float2* src = reinterpret_cast<const float2*>(r.in + gg * plane + (size_t)k * N);
+        float2* dst = reinterpret_cast<float2*>(IN + gg * N);
+        row_dtt_group<M>([src](int i) { return src[i]; },
+                         [dst](int q, float2 v) { dst[q] = v; },
+                         (gg & 1) ? QS_RODFT11 : QS_REDFT11, 1.f, valid, jt, Wg, tws, posts, pre);
+    }
+    __syncthreads();
+    for (int j = threadIdx.x; j < N; j += NT) {
+        const size_t n = (size_t)j + (size_t)N * k;
+        const float le[3] = {IN[j], IN[N + j], IN[2 * N + j]};
+        const float lb[3] = {IN[3 * N + j], IN[4 * N + j], IN[5 * N + j]};
+        if constexpr (CORRECT) {
+            float lj[3];
+            corrector_adjoint_mode(a, j, k, n, le, lb, lj);
+            OUT[j] = lj[0];
+            OUT[N + j] = lj[1];
+            OUT[2 * N + j] = lj[2];
+        } else {
+            predictor_adjoint_mode(a, j, k, n, le, lb);
+        }
+    }
+    pdl_trigger();
+    if constexpr (CORRECT) {
+        __syncthreads();
+        if (threadIdx.x < NTF) {   // y-pass of the current adjoints (y kinds C S C)
+            const bool valid = g < 3;
+            const int gg = valid ? g : 0;
+            const float2* src = reinterpret_cast<const float2*>(OUT + gg * N);
+            float2* dst = reinterpret_cast<float2*>(r.out + gg * plane + (size_t)k * N);
+            row_dtt_group<M>([src](int i) { return src[i]; },
+                             [dst](int q, float2 v) { dst[q] = v; },
+                             gg == 1 ? QS_RODFT11 : QS_REDFT11, 1.f, valid, jt, Wg, tws, posts,
+                             pre);
+        }
+    }
+}
+
+template <int M>
+cudaError_t set_adj_rows_smem() {
+    cudaError_t e = cudaFuncSetAttribute(adjoint_rows_kernel<M, true>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)adj_rows_smem<M>());
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(adjoint_rows_kernel<M, false>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)adj_rows_smem<M>());
+    return e;
+}
+
+template <int M>
+cudaError_t launch_adj_rows(const AdjSpecArgs<float>& a, const AdjRowArgs& r, bool correct,
+                            cudaStream_t st) {
+    const dim3 grid((unsigned)a.nz), block(adj_threads<M>());
+    if (correct)
+        return launch_pdl(adjoint_rows_kernel<M, true>, grid, block, adj_rows_smem<M>(), st, a, r);
+    return launch_pdl(adjoint_rows_kernel<M, false>, grid, block, adj_rows_smem<M>(), st, a, r);
+}
+
 }  // namespace fft
 
 namespace {
@@ -661,10 +772,10 @@ DttFft* DttFft::create(int ny, int nz) {
     // the maps between the two halves of a transform (rows within one warp)
     if (ok && ny >= 128 && ny <= 1024) {
         switch (ny / 2) {
-            case 512: e = fft::set_spec_rows_smem<512>(); break;
-            case 256: e = fft::set_spec_rows_smem<256>(); break;
-            case 128: e = fft::set_spec_rows_smem<128>(); break;
-            default: e = fft::set_spec_rows_smem<64>(); break;
+            case 512: e = fft::set_spec_rows_smem<512>(); if (e == cudaSuccess) e = fft::set_adj_rows_smem<512>(); break;
+            case 256: e = fft::set_spec_rows_smem<256>(); if (e == cudaSuccess) e = fft::set_adj_rows_smem<256>(); break;
+            case 128: e = fft::set_spec_rows_smem<128>(); if (e == cudaSuccess) e = fft::set_adj_rows_smem<128>(); break;
+            default: e = fft::set_spec_rows_smem<64>(); if (e == cudaSuccess) e = fft::set_adj_rows_smem<64>(); break;
         }
         d->spec_rows = e == cudaSuccess;
         e = cudaSuccess;
@@ -727,6 +838,23 @@ int DttFft::run_spectral_rows(const SpecArgs<float>& a, bool correct, const floa
         case 256: e = fft::launch_spec_rows<256>(a, r, correct, st); break;
         case 128: e = fft::launch_spec_rows<128>(a, r, correct, st); break;
         default: e = fft::launch_spec_rows<64>(a, r, correct, st); break;
+    }
+    return e == cudaSuccess ? 1 : 0;
+}
+
+int DttFft::run_adjoint_rows(const AdjSpecArgs<float>& a, bool correct, const float* in,
+                             float* out, cudaStream_t st) const {
+    if (!spec_rows) return 0;
+    fft::AdjRowArgs r{};
+    r.in = in;
+    r.out = out;
+    r.tab = tab_y;
+    cudaError_t e;
+    switch (ny / 2) {
+        case 512: e = fft::launch_adj_rows<512>(a, r, correct, st); break;
+        case 256: e = fft::launch_adj_rows<256>(a, r, correct, st); break;
+        case 128: e = fft::launch_adj_rows<128>(a, r, correct, st); break;
+        default: e = fft::launch_adj_rows<64>(a, r, correct, st); break;
     }
     return e == cudaSuccess ? 1 : 0;
 }

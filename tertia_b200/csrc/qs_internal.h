@@ -89,6 +89,9 @@ int run_dtt_simt(const DttJob<T>& job, int ny, int nz, const DttMats<T>& my,
 // (dtt_fft.cu), for power-of-two ny, nz in [32, 2048]: pass 0 along y from
 // the job's inputs into `scratch` (same layout), pass 1 along z from there
 // into the job's outputs with its scale.
+template <class T>
+struct AdjSpecArgs;
+
 struct DttFft {
     int ny = 0, nz = 0;
     float2* tab_y = nullptr;   // twiddle tables of each size
@@ -105,6 +108,11 @@ struct DttFft {
     // (planes of ny*nz, unscaled); jin and out may be the same planes
     int run_spectral_rows(const SpecArgs<float>& a, bool correct, const float* jin, float* out,
                           int nout, cudaStream_t st) const;
+    // the same for the adjoints of the maps: y-pass of the 6 z-transformed
+    // field adjoints at `in`, the corrector's (predictor's) adjoint, and for
+    // the corrector the y-pass of the 3 current adjoints into `out`
+    int run_adjoint_rows(const AdjSpecArgs<float>& a, bool correct, const float* in, float* out,
+                         cudaStream_t st) const;
     ~DttFft();
 };
 
