@@ -260,6 +260,21 @@ int launch_push_adjoint(const PushAdjArgs<T>& a, cudaStream_t st) {
 // sub-steps is piecewise constant).  Up to kMaxSub sub-steps are followed.
 constexpr int kMaxSub = 8;
 
+// FP32 uses the forward push's fast forms (rsqrt, rounded reciprocal, fast
+// divide), so that the recomputed push is the one the forward ran
+template <class T>
+__device__ __forceinline__ T rsq(T x) { return T(1) / sqrt(x); }
+template <>
+__device__ __forceinline__ float rsq<float>(float x) { return rsqrtf(x); }
+template <class T>
+__device__ __forceinline__ T rcp(T x) { return T(1) / x; }
+template <>
+__device__ __forceinline__ float rcp<float>(float x) { return __frcp_rn(x); }
+template <class T>
+__device__ __forceinline__ T fdiv(T a, T b) { return a / b; }
+template <>
+__device__ __forceinline__ float fdiv<float>(float a, float b) { return __fdividef(a, b); }
+
 // The adjoint of particle i: its momentum and position adjoints are stored,
 // the adjoint of the fields it gathered (6 fields x 4 corners of its cell,
 // index f*4 + r) goes to lf, and its cell is returned (-1 when the forward
@@ -297,26 +312,26 @@ __device__ __forceinline__ int push_adjoint_cic_one(const PushAdjArgs<T>& a, int
     // ---- forward recompute of the push (as in push_adjoint_kernel)
     const T p[3] = {px0, py0, pz0};
     const T s0 = one + p[0] * p[0] + p[1] * p[1] + p[2] * p[2];
-    const T r0 = one / sqrt(s0);
+    const T r0 = rsq(s0);
     const T Vp[3] = {p[0] * r0, p[1] * r0, p[2] * r0};
-    const T ia = one / (one - Vp[0]);
+    const T ia = rcp(one - Vp[0]);
     const T kE = a.sE * ia;
     const T e[3] = {E[0] * kE, E[1] * kE, E[2] * kE};
     const T p1[3] = {p[0] + e[0], p[1] + e[1], p[2] + e[2]};
-    const T r1 = one / sqrt(one + p1[0] * p1[0] + p1[1] * p1[1] + p1[2] * p1[2]);
+    const T r1 = rsq(one + p1[0] * p1[0] + p1[1] * p1[1] + p1[2] * p1[2]);
     const T kB = r1 * kE;
     const T b[3] = {B[0] * kB, B[1] * kB, B[2] * kB};
-    const T co = T(2) / (one + b[0] * b[0] + b[1] * b[1] + b[2] * b[2]);
+    const T co = fdiv(T(2), one + b[0] * b[0] + b[1] * b[1] + b[2] * b[2]);
     const T u[3] = {p1[0] + (p1[1] * b[2] - p1[2] * b[1]), p1[1] + (p1[2] * b[0] - p1[0] * b[2]),
                     p1[2] + (p1[0] * b[1] - p1[1] * b[0])};
     const T p3[3] = {u[0] * co, u[1] * co, u[2] * co};
     const T p2[3] = {p1[0] + e[0] + (p3[1] * b[2] - p3[2] * b[1]),
                      p1[1] + e[1] + (p3[2] * b[0] - p3[0] * b[2]),
                      p1[2] + e[2] + (p3[0] * b[1] - p3[1] * b[0])};
-    const T r2 = one / sqrt(one + p2[0] * p2[0] + p2[1] * p2[1] + p2[2] * p2[2]);
+    const T r2 = rsq(one + p2[0] * p2[0] + p2[1] * p2[1] + p2[2] * p2[2]);
     const T Vm[3] = {p2[0] * r2, p2[1] * r2, p2[2] * r2};
     const T V[3] = {half * (Vm[0] + Vp[0]), half * (Vm[1] + Vp[1]), half * (Vm[2] + Vp[2])};
-    const T inv2 = one / (one - V[0]);
+    const T inv2 = rcp(one - V[0]);
     const T wq = w * inv2;
     const T dJ0[3] = {a.djx0, a.djy0, a.djz0};
     const T dq[3] = {wq * dJ0[0] * Vm[0], wq * dJ0[1] * Vm[1], wq * dJ0[2] * Vm[2]};
@@ -349,11 +364,11 @@ __device__ __forceinline__ int push_adjoint_cic_one(const PushAdjArgs<T>& a, int
             T ps;
             if (partdx > one) {
                 partdx -= one;
-                ps = one / step;
-                sdps[ns] = -ps / step;
+                ps = rcp(step);
+                sdps[ns] = -ps * ps;
                 nfull++;
             } else {
-                ps = partdx / step;
+                ps = fdiv(partdx, step);
                 partdx = T(0);
                 sdps[ns] = T(nfull) / (step * step);
             }
