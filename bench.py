@@ -411,6 +411,26 @@ def run_ours(args):
     # repeated with the launches queued ahead of the GPU
     gemm = None
     fftp = None
+    # the CIC push (the dominant kernel of the FP32 march): the half push of the
+    # head layer repeated through the fine-grained entry points, each launch
+    # bracketed by events on the handle's stream (one push per call)
+    pushk = None
+    if cfg.shape == QS_SHAPE_CIC:
+        m.load_front_plasma(wl.front_plasma(cfg, seed=5))
+        m.begin_march()
+        m.layer_begin(cfg.nx - 1, 0)
+        m.guess_fields(cfg.nx - 1, 0)
+        for _ in range(3):
+            m.move_particles_layer(cfg.nx - 1, 0, 0)
+        m.sync()
+        m.profile_enable(True)
+        for _ in range(40):
+            m.move_particles_layer(cfg.nx - 1, 0, 0)
+        pp = m.profile_read()
+        m.profile_enable(False)
+        p_ms, p_n = pp["push_deposit"]
+        pushk = {"launches": p_n, "avg_launch_us": p_ms * 1e3 / max(p_n, 1),
+                 "particles": cfg.ny * cfg.nz * cfg.ppc}
     if args.precision == "fp32":
         # FFT passes (power-of-two grids): 2 launches per transform, each
         # reading and writing the 6 planes once
@@ -522,21 +542,29 @@ def run_ours(args):
         # transforms per (layer, split) in the march: 6 (Guess inverse E, B)
         # + (nIter+1) * (3 forward J + 6 inverse E, B) + 2 beam planes
         roof["march_transforms_per_layer"] = 6 + (nit + 1) * 9 + 2
-    elif fftp:
-        # one launch = one pass (along y or z) over 6 N x N FP32 planes: each
-        # plane read once and written once
-        bytes_launch = fftp["planes"] * 2.0 * 4.0 * cfg.ny * cfg.nz
-        achieved = bytes_launch / (fftp["avg_launch_us"] / 1e6) / 1e9
+    elif pushk:
+        # one launch = one sub-push of every plasma particle: 28 B of particle
+        # state read + the P and C fields (12 values) and the deposit (4
+        # values) of its cell shared by the ppc particles, 4 B each
+        bpp = 28.0 + 16.0 * 4.0 / cfg.ppc
+        bytes_launch = bpp * pushk["particles"]
+        achieved = bytes_launch / (pushk["avg_launch_us"] / 1e6) / 1e9
         roof = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                 "frac": achieved / hbm, "peak_source": f"hbm_gbs of {src}",
-                "kernel": "fft_rows_kernel / fft_cols_kernel (transform pass, 6 planes)",
-                "bytes_per_launch": bytes_launch, "avg_launch_us": fftp["avg_launch_us"],
-                "timing": fftp}
-        roof["march_transforms_per_layer"] = 6 + (nit + 1) * 9 + 2
+                "kernel": "push_cic_warp_kernel (CIC push + deposit, half step)",
+                "bytes_per_particle": bpp, "bytes_per_launch": bytes_launch,
+                "avg_launch_us": pushk["avg_launch_us"], "timing": pushk}
+        if fftp:
+            # the transform pass, for reference: 6 N x N planes read and written
+            tb = fftp["planes"] * 2.0 * 4.0 * cfg.ny * cfg.nz
+            roof["transform_pass"] = {
+                "kernel": "fft_rows_kernel / fft_cols_kernel (6 planes)", "bytes_per_launch": tb,
+                "avg_launch_us": fftp["avg_launch_us"],
+                "achieved_gbs": tb / (fftp["avg_launch_us"] / 1e6) / 1e9, "timing": fftp}
     else:
         roof = {"bound": "hbm", "achieved": None, "peak": hbm, "unit": "GB/s", "frac": None,
                 "kernel": dom}
-    tr = traffic_record("dtt_tc_kernel" if gemm else ("fft_pass" if fftp else dom),
+    tr = traffic_record("dtt_tc_kernel" if gemm else ("push_cic_warp_kernel" if pushk else dom),
                         args.workload, args.precision)
     roof["traffic"] = tr.get("bytes_per_launch") if tr else None
     if tr:

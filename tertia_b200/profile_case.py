@@ -1,6 +1,6 @@
 """A short, self-contained run of the beam step for kernel profiling.
 
-    python -m tertia_b200.profile_case [--layers 256] [--shape cic] [--precision bf16x3]
+    python -m tertia_b200.profile_case [--layers 256] [--shape cic] [--precision fp32]
                                         [--steps 1]
 
 Builds the 512 x 512 grid of the c1 workload with a shorter box (so that a
@@ -19,7 +19,7 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--layers", type=int, default=256)
     ap.add_argument("--shape", default="cic", choices=["cic", "ngp"])
-    ap.add_argument("--precision", default="bf16x3")
+    ap.add_argument("--precision", default="fp32")
     ap.add_argument("--steps", type=int, default=1)
     args = ap.parse_args()
 
