@@ -123,12 +123,12 @@ __device__ __forceinline__ void stockham_store(const float2 (&v)[R], float2* W, 
 }
 
 // One Stockham pass of radix R after NS points have been combined: every
-// thread of a sequence (T = M/16 of them) does (M/R)/T butterfly groups
-// (1, 2, 4 or 8).  `at(e)` maps element e of this thread's sequence to its
-// shared-memory slot.
-template <int M, int R, int NS, bool WARP, class At>
+// thread of a sequence (T = M/V of them, V values each) does (M/R)/T
+// butterfly groups (1, 2, 4 or 8).  `at(e)` maps element e of this thread's
+// sequence to its shared-memory slot.
+template <int M, int V, int R, int NS, bool WARP, class At>
 __device__ __forceinline__ void stockham_pass(float2* W, At at, int jt, const float2* tw) {
-    constexpr int T = M / 16;
+    constexpr int T = M / V;
     constexpr int G = (M / R) / T;
     static_assert(G == 1 || G == 2 || G == 4 || G == 8, "groups per thread");
     if constexpr (G == 1) {
@@ -148,14 +148,14 @@ __device__ __forceinline__ void stockham_pass(float2* W, At at, int jt, const fl
 }
 
 // The last pass keeps its butterfly groups in registers: thread jt ends up
-// with Z_q for q = jt + T*m in slot m (m < 16), and Z_{M-1-q} sits in slot
-// 15 - m of thread T-1-jt.
-template <int M, int R, int NS, class At>
+// with Z_q for q = jt + T*m in slot m (m < V), and Z_{M-1-q} sits in slot
+// V-1-m of thread T-1-jt.
+template <int M, int V, int R, int NS, class At>
 __device__ __forceinline__ void final_pass(const float2* W, At at, int jt, const float2* tw,
-                                           float2 (&fin)[16]) {
-    constexpr int T = M / 16;
+                                           float2 (&fin)[V]) {
+    constexpr int T = M / V;
     constexpr int G = (M / R) / T;
-    static_assert(NS * R == M && G * R == 16, "final pass");
+    static_assert(NS * R == M && G * R == V, "final pass");
 #pragma unroll
     for (int g = 0; g < G; g++) {
         float2 v[R];
@@ -165,21 +165,28 @@ __device__ __forceinline__ void final_pass(const float2* W, At at, int jt, const
     }
 }
 
-// the passes after the first radix-16 one (radix 16, then the remaining factor)
-template <int M, int NS, bool WARP>
+// the passes after the first radix-V one (radix V, then the remaining factor)
+template <int M, int V, int NS, bool WARP>
 struct Passes {
-    static constexpr int R = (M / NS) >= 16 ? 16 : (M / NS);
+    static constexpr int R = (M / NS) >= V ? V : (M / NS);
     template <class At>
     __device__ __forceinline__ static void run(float2* W, At at, int jt, const float2* tw,
-                                               float2 (&fin)[16]) {
+                                               float2 (&fin)[V]) {
         if constexpr (NS * R == M) {
-            final_pass<M, R, NS>(W, at, jt, tw, fin);
+            final_pass<M, V, R, NS>(W, at, jt, tw, fin);
         } else {
-            stockham_pass<M, R, NS, WARP>(W, at, jt, tw);
-            Passes<M, NS * R, WARP>::run(W, at, jt, tw, fin);
+            stockham_pass<M, V, R, NS, WARP>(W, at, jt, tw);
+            Passes<M, V, NS * R, WARP>::run(W, at, jt, tw, fin);
         }
     }
 };
+
+// values per thread: 8 on the small grids (more threads in flight, measured
+// faster at n = 256), 16 from n = 512 on (fewer passes; as fast or faster)
+template <int M>
+__host__ __device__ constexpr int vpt() {
+    return M <= 128 ? 8 : 16;
+}
 
 struct RowArgs {
     const float* in[kMaxXfFields];
@@ -193,23 +200,24 @@ struct RowArgs {
 
 template <int M>
 __host__ __device__ constexpr int row_threads() {
-    return (M / 16) > 64 ? (M / 16) : 64;
+    return (M / vpt<M>()) > 64 ? (M / vpt<M>()) : 64;
 }
 
-// Transform along the contiguous axis: each sequence of T = M/16 threads
+// Transform along the contiguous axis: each sequence of T = M/V threads
 // takes one row of n = 2M values (small blocks, so that the rows of a batch
 // spread evenly over the SMs).  Thread jt holds the pairs P[jt + T*b]
 // (P[i] = (x[2i], x[2i+1])); the mirrored element x[n-1-2i] of the
 // pre-twiddle and the mirrored output of the post-twiddle belong to thread
 // T-1-jt, a shuffle away when a row lies within one warp.  Shared slot of
-// element e: e + e/16 (one pad per 16 keeps the stride-16 stores of the first
+// element e: e + e/V (one pad per V keeps the stride-V stores of the first
 // pass free of bank conflicts).
 template <int M>
 __global__ void __launch_bounds__(row_threads<M>()) fft_rows_kernel(RowArgs a) {
-    constexpr int T = M / 16;
+    constexpr int V = vpt<M>();
+    constexpr int T = M / V;
     constexpr int NT = row_threads<M>();
     constexpr int SEQ = NT / T;
-    constexpr int LD = M + M / 16;
+    constexpr int LD = M + M / V;
     constexpr bool WARP = T <= 32;
     __shared__ float2 W[SEQ * LD];
     __shared__ float2 tws[M];
@@ -223,7 +231,7 @@ __global__ void __launch_bounds__(row_threads<M>()) fft_rows_kernel(RowArgs a) {
     const bool valid = row < a.total;
     const int f = valid ? row / a.nrows : 0, k = valid ? row % a.nrows : 0;
     float2* Ws = W + s * LD;
-    auto at = [](int e) { return e + (e >> 4); };
+    auto at = [](int e) { return e + e / V; };
     pdl_wait();
     const float* inf = a.in[0];
     float* outf = a.out[0];
@@ -233,28 +241,28 @@ __global__ void __launch_bounds__(row_threads<M>()) fft_rows_kernel(RowArgs a) {
         if (q == f) { inf = a.in[q]; outf = a.out[q]; kind = a.kind[q]; }
     const float2* P = reinterpret_cast<const float2*>(inf + (size_t)k * 2 * M);
     const float2* pre = a.tab + M;
-    // the 16 pairs of this thread in bit-reversed order, the pre-twiddle
-    float2 p[16], w[16];
+    // the V pairs of this thread in bit-reversed order, the pre-twiddle
+    float2 p[V], w[V];
 #pragma unroll
-    for (int b = 0; b < 16; b++) {
-        const int i = jt + bitrev<16>(b) * T;
+    for (int b = 0; b < V; b++) {
+        const int i = jt + bitrev<V>(b) * T;
         p[b] = valid ? P[i] : make_float2(0.f, 0.f);
         w[b] = __ldg(pre + i);
     }
-    float2 v[16];
+    float2 v[V];
     if constexpr (WARP) {
-        // x[n-1-2i] = P[M-1-i].y: slot 15-b of thread T-1-jt
+        // x[n-1-2i] = P[M-1-i].y: slot V-1-b of thread T-1-jt
 #pragma unroll
-        for (int b = 0; b < 16; b++) {
-            const float mirror = __shfl_xor_sync(0xffffffffu, p[15 - b].y, T - 1);
+        for (int b = 0; b < V; b++) {
+            const float mirror = __shfl_xor_sync(0xffffffffu, p[V - 1 - b].y, T - 1);
             const float2 z = kind == QS_REDFT11 ? make_float2(p[b].x, mirror)
                                                 : make_float2(mirror, p[b].x);
             v[b] = cmul(z, w[b]);
         }
     } else {
 #pragma unroll
-        for (int b = 0; b < 16; b++) {
-            const int i = jt + bitrev<16>(b) * T;
+        for (int b = 0; b < V; b++) {
+            const int i = jt + bitrev<V>(b) * T;
             const float mirror = valid ? P[M - 1 - i].y : 0.f;
             const float2 z = kind == QS_REDFT11 ? make_float2(p[b].x, mirror)
                                                 : make_float2(mirror, p[b].x);
@@ -262,48 +270,48 @@ __global__ void __launch_bounds__(row_threads<M>()) fft_rows_kernel(RowArgs a) {
         }
     }
     __syncthreads();   // twiddle tables in place
-    dft<16>(v);
-    float2 fin[16];
+    dft<V>(v);
+    float2 fin[V];
     if constexpr (T == 1) {
         // one pass: Z_r in slot r, the thread owns the whole sequence
 #pragma unroll
-        for (int r = 0; r < 16; r++) fin[r] = v[r];
+        for (int r = 0; r < V; r++) fin[r] = v[r];
     } else {
 #pragma unroll
-        for (int r = 0; r < 16; r++) Ws[at(jt * 16 + r)] = v[r];
+        for (int r = 0; r < V; r++) Ws[at(jt * V + r)] = v[r];
         seq_sync<WARP>();
-        Passes<M, 16, WARP>::run(Ws, at, jt, tws, fin);
+        Passes<M, V, V, WARP>::run(Ws, at, jt, tws, fin);
     }
     pdl_trigger();
     // s_q = Z_q e^{-i pi (q+1/4)/n}; out pair q = (2 Re s_q, -+2 Im s_{M-1-q})
-    float im[16];
+    float im[V];
 #pragma unroll
-    for (int m = 0; m < 16; m++) {
+    for (int m = 0; m < V; m++) {
         const int q = jt + T * m;
         const float2 sq = cmul(fin[m], posts[q]);
         fin[m] = sq;
         im[m] = sq.y;
     }
-    float mirror[16];
+    float mirror[V];
     if constexpr (WARP) {
 #pragma unroll
-        for (int m = 0; m < 16; m++) mirror[m] = __shfl_xor_sync(0xffffffffu, im[15 - m], T - 1);
+        for (int m = 0; m < V; m++) mirror[m] = __shfl_xor_sync(0xffffffffu, im[V - 1 - m], T - 1);
     } else {
         // rows wider than a warp: the mirrored parts through shared memory
         __syncthreads();
         float* ims = reinterpret_cast<float*>(Ws);
 #pragma unroll
-        for (int m = 0; m < 16; m++) ims[jt + T * m] = im[m];
+        for (int m = 0; m < V; m++) ims[jt + T * m] = im[m];
         __syncthreads();
 #pragma unroll
-        for (int m = 0; m < 16; m++) mirror[m] = ims[M - 1 - (jt + T * m)];
+        for (int m = 0; m < V; m++) mirror[m] = ims[M - 1 - (jt + T * m)];
     }
     if (!valid) return;
     float2* O = reinterpret_cast<float2*>(outf + (size_t)k * 2 * M);
     const float c2 = 2.f * a.scale;
     const float sgn = kind == QS_REDFT11 ? -c2 : c2;
 #pragma unroll
-    for (int m = 0; m < 16; m++) O[jt + T * m] = make_float2(c2 * fin[m].x, sgn * mirror[m]);
+    for (int m = 0; m < V; m++) O[jt + T * m] = make_float2(c2 * fin[m].x, sgn * mirror[m]);
 }
 
 struct ColArgs {
@@ -319,8 +327,9 @@ struct ColArgs {
 // plane (TJ floats = whole 32-byte sectors per row); column c's sequence
 // lives at W[e * TJ + c], its T threads are TJ lanes apart.
 template <int M, int TJ>
-__global__ void __launch_bounds__(TJ * (M / 16)) fft_cols_kernel(ColArgs a) {
-    constexpr int T = M / 16;
+__global__ void __launch_bounds__(TJ * (M / vpt<M>())) fft_cols_kernel(ColArgs a) {
+    constexpr int V = vpt<M>();
+    constexpr int T = M / V;
     constexpr int NT = TJ * T;
     extern __shared__ float2 smem_f2[];
     float2* tws = smem_f2;
@@ -343,37 +352,37 @@ __global__ void __launch_bounds__(TJ * (M / 16)) fft_cols_kernel(ColArgs a) {
     for (int q = 1; q < kMaxXfFields; q++)
         if (q == f) { inf = a.in[q]; outf = a.out[q]; kind = a.kind[q]; }
     const float2* pre = a.tab + M;
-    float lo[16], hi[16];
-    float2 w[16];
+    float lo[V], hi[V];
+    float2 w[V];
 #pragma unroll
-    for (int b = 0; b < 16; b++) {
-        const int i = jt + bitrev<16>(b) * T;
+    for (int b = 0; b < V; b++) {
+        const int i = jt + bitrev<V>(b) * T;
         lo[b] = inf[(size_t)(2 * i) * ld + col];
         hi[b] = inf[(size_t)(2 * M - 1 - 2 * i) * ld + col];
         w[b] = __ldg(pre + i);
     }
-    float2 v[16];
+    float2 v[V];
 #pragma unroll
-    for (int b = 0; b < 16; b++) {
+    for (int b = 0; b < V; b++) {
         const float2 z = kind == QS_REDFT11 ? make_float2(lo[b], hi[b]) : make_float2(hi[b], lo[b]);
         v[b] = cmul(z, w[b]);
     }
     __syncthreads();
-    dft<16>(v);
-    float2 fin[16];
+    dft<V>(v);
+    float2 fin[V];
     if constexpr (T == 1) {
 #pragma unroll
-        for (int r = 0; r < 16; r++) fin[r] = v[r];
+        for (int r = 0; r < V; r++) fin[r] = v[r];
     } else {
 #pragma unroll
-        for (int r = 0; r < 16; r++) W[at(jt * 16 + r)] = v[r];
+        for (int r = 0; r < V; r++) W[at(jt * V + r)] = v[r];
         __syncthreads();
-        Passes<M, 16, false>::run(W, at, jt, tws, fin);
+        Passes<M, V, V, false>::run(W, at, jt, tws, fin);
     }
     pdl_trigger();
-    float im[16];
+    float im[V];
 #pragma unroll
-    for (int m = 0; m < 16; m++) {
+    for (int m = 0; m < V; m++) {
         const int q = jt + T * m;
         fin[m] = cmul(fin[m], posts[q]);
         im[m] = fin[m].y;
@@ -381,12 +390,12 @@ __global__ void __launch_bounds__(TJ * (M / 16)) fft_cols_kernel(ColArgs a) {
     __syncthreads();
     float* ims = reinterpret_cast<float*>(W);
 #pragma unroll
-    for (int m = 0; m < 16; m++) ims[(jt + T * m) * TJ + c] = im[m];
+    for (int m = 0; m < V; m++) ims[(jt + T * m) * TJ + c] = im[m];
     __syncthreads();
     const float c2 = 2.f * a.scale;
     const float sgn = kind == QS_REDFT11 ? -c2 : c2;
 #pragma unroll
-    for (int m = 0; m < 16; m++) {
+    for (int m = 0; m < V; m++) {
         const int q = jt + T * m;
         outf[(size_t)(2 * q) * ld + col] = c2 * fin[m].x;
         outf[(size_t)(2 * q + 1) * ld + col] = sgn * ims[(M - 1 - q) * TJ + c];
@@ -395,7 +404,7 @@ __global__ void __launch_bounds__(TJ * (M / 16)) fft_cols_kernel(ColArgs a) {
 
 template <int M>
 __host__ __device__ constexpr int cols_tj() {
-    return (M / 16) >= 64 ? 8 : (M / 16) >= 16 ? 8 : (M / 16) >= 4 ? 16 : 32;
+    return (M / vpt<M>()) >= 16 ? 8 : (M / vpt<M>()) >= 4 ? 16 : 32;
 }
 
 template <int M>
@@ -411,7 +420,7 @@ cudaError_t set_cols_smem() {
 
 template <int M>
 cudaError_t launch_rows(const RowArgs& a, cudaStream_t st) {
-    constexpr int SEQ = row_threads<M>() / (M / 16);
+    constexpr int SEQ = row_threads<M>() / (M / vpt<M>());
     const int blocks = (a.total + SEQ - 1) / SEQ;
     return launch_pdl(fft_rows_kernel<M>, dim3((unsigned)blocks), dim3(row_threads<M>()), 0, st,
                       a);
@@ -421,7 +430,7 @@ template <int M>
 cudaError_t launch_cols(const ColArgs& a, int nf, cudaStream_t st) {
     constexpr int TJ = cols_tj<M>();
     return launch_pdl(fft_cols_kernel<M, TJ>, dim3((unsigned)(a.ncols / TJ), (unsigned)nf),
-                      dim3(TJ * (M / 16)), cols_smem<M>(), st, a);
+                      dim3(TJ * (M / vpt<M>())), cols_smem<M>(), st, a);
 }
 
 // ---------------------------------------------------------------------------
@@ -443,46 +452,47 @@ __device__ __forceinline__ void row_dtt_group(InPair in_pair, OutPair out_pair, 
                                               float scale, bool valid, int jt, float2* Wg,
                                               const float2* tws, const float2* posts,
                                               const float2* pre) {
-    constexpr int T = M / 16;
+    constexpr int V = vpt<M>();
+    constexpr int T = M / V;
     static_assert(T >= 1 && T <= 32, "a group within one warp");
-    auto at = [](int e) { return e + (e >> 4); };
-    float2 p[16], w[16];
+    auto at = [](int e) { return e + e / V; };
+    float2 p[V], w[V];
 #pragma unroll
-    for (int b = 0; b < 16; b++) {
-        const int i = jt + bitrev<16>(b) * T;
+    for (int b = 0; b < V; b++) {
+        const int i = jt + bitrev<V>(b) * T;
         p[b] = valid ? in_pair(i) : make_float2(0.f, 0.f);
         w[b] = __ldg(pre + i);
     }
-    float2 v[16];
+    float2 v[V];
 #pragma unroll
-    for (int b = 0; b < 16; b++) {
-        const float mirror = __shfl_xor_sync(0xffffffffu, p[15 - b].y, T - 1);
+    for (int b = 0; b < V; b++) {
+        const float mirror = __shfl_xor_sync(0xffffffffu, p[V - 1 - b].y, T - 1);
         const float2 z = kind == QS_REDFT11 ? make_float2(p[b].x, mirror)
                                             : make_float2(mirror, p[b].x);
         v[b] = cmul(z, w[b]);
     }
-    dft<16>(v);
-    float2 fin[16];
+    dft<V>(v);
+    float2 fin[V];
     if constexpr (T == 1) {
 #pragma unroll
-        for (int r = 0; r < 16; r++) fin[r] = v[r];
+        for (int r = 0; r < V; r++) fin[r] = v[r];
     } else {
 #pragma unroll
-        for (int r = 0; r < 16; r++) Wg[at(jt * 16 + r)] = v[r];
+        for (int r = 0; r < V; r++) Wg[at(jt * V + r)] = v[r];
         __syncwarp();
-        Passes<M, 16, true>::run(Wg, at, jt, tws, fin);
+        Passes<M, V, V, true>::run(Wg, at, jt, tws, fin);
     }
-    float im[16];
+    float im[V];
 #pragma unroll
-    for (int m = 0; m < 16; m++) {
+    for (int m = 0; m < V; m++) {
         fin[m] = cmul(fin[m], posts[jt + T * m]);
         im[m] = fin[m].y;
     }
     const float c2 = 2.f * scale;
     const float sgn = kind == QS_REDFT11 ? -c2 : c2;
 #pragma unroll
-    for (int m = 0; m < 16; m++) {
-        const float mirror = __shfl_xor_sync(0xffffffffu, im[15 - m], T - 1);
+    for (int m = 0; m < V; m++) {
+        const float mirror = __shfl_xor_sync(0xffffffffu, im[V - 1 - m], T - 1);
         if (valid) out_pair(jt + T * m, make_float2(c2 * fin[m].x, sgn * mirror));
     }
     __syncwarp();   // Wg is free again
@@ -500,26 +510,26 @@ constexpr int kSpecGroups = 8;
 template <int M>
 __host__ __device__ constexpr size_t spec_rows_smem() {
     // tables, FFT work of each group, the row's J spectra and E, B, Rho spectra
-    return sizeof(float2) * (2 * (size_t)M + (size_t)kSpecGroups * (M + M / 16)) +
+    return sizeof(float2) * (2 * (size_t)M + (size_t)kSpecGroups * (M + M / vpt<M>())) +
            sizeof(float) * (3 + 7) * (size_t)(2 * M);
 }
 
 // threads of a map CTA: the transform groups, or one per mode pair if more
 template <int M>
 __host__ __device__ constexpr int spec_threads() {
-    return kSpecGroups * (M / 16) > M ? kSpecGroups * (M / 16) : M;
+    return kSpecGroups * (M / vpt<M>()) > M ? kSpecGroups * (M / vpt<M>()) : M;
 }
 
 template <int M, bool CORRECT>
 __global__ void __launch_bounds__(spec_threads<M>()) spectral_rows_kernel(SpecArgs<float> a,
                                                                           SpecRowArgs r) {
     using namespace specf32;
-    constexpr int T = M / 16;
+    constexpr int T = M / vpt<M>();
     constexpr int NTF = kSpecGroups * T;   // the transform groups (whole warps)
     constexpr int NT = spec_threads<M>();
     static_assert(NTF % 32 == 0, "transform groups fill whole warps");
     constexpr int N = 2 * M;
-    constexpr int LD = M + M / 16;
+    constexpr int LD = M + M / vpt<M>();
     extern __shared__ float2 smem_f2[];
     float2* tws = smem_f2;
     float2* posts = tws + M;
@@ -626,24 +636,26 @@ struct AdjRowArgs {
 
 template <int M>
 __host__ __device__ constexpr size_t adj_rows_smem() {
-    return sizeof(float2) * (2 * (size_t)M + (size_t)kSpecGroups * (M + M / 16)) +
+    return sizeof(float2) * (2 * (size_t)M + (size_t)kSpecGroups * (M + M / vpt<M>())) +
            sizeof(float) * (6 + 3) * (size_t)(2 * M);
 }
 
 template <int M>
 __host__ __device__ constexpr int adj_threads() {
-    return kSpecGroups * (M / 16) > 2 * M ? kSpecGroups * (M / 16) : 2 * M;
+    // one mode per thread, at most 512 threads (the rest loop)
+    return kSpecGroups * (M / vpt<M>()) > 2 * M ? kSpecGroups * (M / vpt<M>())
+                                                : (2 * M > 512 ? 512 : 2 * M);
 }
 
 template <int M, bool CORRECT>
 __global__ void __launch_bounds__(adj_threads<M>()) adjoint_rows_kernel(AdjSpecArgs<float> a,
                                                                        AdjRowArgs r) {
     using namespace adjmaps;
-    constexpr int T = M / 16;
+    constexpr int T = M / vpt<M>();
     constexpr int NTF = kSpecGroups * T;
     constexpr int NT = adj_threads<M>();
     constexpr int N = 2 * M;
-    constexpr int LD = M + M / 16;
+    constexpr int LD = M + M / vpt<M>();
     static_assert(NTF % 32 == 0, "transform groups fill whole warps");
     extern __shared__ float2 smem_f2[];
     float2* tws = smem_f2;
