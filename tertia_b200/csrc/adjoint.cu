@@ -295,16 +295,20 @@ __device__ __forceinline__ int push_adjoint_cic_one(const PushAdjArgs<T>& a, int
     const size_t nn[4] = {(size_t)j + (size_t)My * k, (size_t)j1 + (size_t)My * k,
                           (size_t)j + (size_t)My * k1, (size_t)j1 + (size_t)My * k1};
     const T wg[4] = {(one - yp) * (one - zp), yp * (one - zp), (one - yp) * zp, yp * zp};
-    T F[6][4];
-    T g[6];
+    // the gathered fields g and their derivatives in y and z (kept instead of
+    // the 24 corner values for the position adjoint of the gather)
+    T g[6], gy[6], gz[6];
 #pragma unroll
     for (int f = 0; f < 6; f++) {
+        T F[4];
         g[f] = T(0);
 #pragma unroll
         for (int r = 0; r < 4; r++) {
-            F[f][r] = half * (ldg_(a.P + f * plane + nn[r]) + ldg_(a.C + f * plane + nn[r]));
-            g[f] += wg[r] * F[f][r];
+            F[r] = half * (ldg_(a.P + f * plane + nn[r]) + ldg_(a.C + f * plane + nn[r]));
+            g[f] += wg[r] * F[r];
         }
+        gy[f] = (one - zp) * (F[1] - F[0]) + zp * (F[3] - F[2]);
+        gz[f] = (one - yp) * (F[2] - F[0]) + yp * (F[3] - F[1]);
     }
     const T E[3] = {g[0], g[1], g[2]};
     const T B[3] = {g[3] + a.bxe, g[4] + a.bye, g[5] + a.bze};
@@ -340,9 +344,13 @@ __device__ __forceinline__ int push_adjoint_cic_one(const PushAdjArgs<T>& a, int
     // ---- sub-steps (cell-relative moves), kept for the backward pass.  With
     // |dy| or |dz| above one cell the step is the larger of the two and each
     // sub-step's fraction ps depends on it: d ps / d step is -1/step^2 for the
-    // full sub-steps and nfull/step^2 for the last one.
+    // full sub-steps and nfull/step^2 for the last one.  The first sub-step
+    // stays in registers (the only one unless the particle crosses more than
+    // one cell per layer), the others go to the arrays.
     T sry[kMaxSub], srz[kMaxSub], sps[kMaxSub], sdps[kMaxSub];
     int sjb[kMaxSub], skb[kMaxSub];
+    T ry0 = T(0), rz0 = T(0), ps0 = T(0), dps0 = T(0);
+    int jb0 = 0, kb0 = 0;
     int ns = 0;
     T dstep_dy = T(0), dstep_dz = T(0), step = one;
     {
@@ -361,16 +369,16 @@ __device__ __forceinline__ int push_adjoint_cic_one(const PushAdjArgs<T>& a, int
         int jb = j, kb = k;
         int nfull = 0;
         while (partdx > T(0) && ns < kMaxSub) {
-            T ps;
+            T ps, dps;
             if (partdx > one) {
                 partdx -= one;
                 ps = rcp(step);
-                sdps[ns] = -ps * ps;
+                dps = -ps * ps;
                 nfull++;
             } else {
                 ps = fdiv(partdx, step);
                 partdx = T(0);
-                sdps[ns] = T(nfull) / (step * step);
+                dps = T(nfull) / (step * step);
             }
             const T uy = ytmp + dy * ps, uz = ztmp + dz * ps;
             const T fy = floor(uy), fz = floor(uz);
@@ -382,7 +390,12 @@ __device__ __forceinline__ int push_adjoint_cic_one(const PushAdjArgs<T>& a, int
             kb = wrap_m(kb + sz, Mz);
             ytmp = ry;
             ztmp = rz;
-            sry[ns] = ry; srz[ns] = rz; sps[ns] = ps; sjb[ns] = jb; skb[ns] = kb;
+            if (ns == 0) {
+                ry0 = ry; rz0 = rz; ps0 = ps; dps0 = dps; jb0 = jb; kb0 = kb;
+            } else {
+                sry[ns] = ry; srz[ns] = rz; sps[ns] = ps; sdps[ns] = dps;
+                sjb[ns] = jb; skb[ns] = kb;
+            }
             ns++;
         }
     }
@@ -391,10 +404,8 @@ __device__ __forceinline__ int push_adjoint_cic_one(const PushAdjArgs<T>& a, int
     T lyc = a.full ? a.lamPos[i] : T(0), lzc = a.full ? a.lamPos[a.n + i] : T(0);
     T ldy = T(0), ldz = T(0), lstep = T(0);
     T ldq[3] = {T(0), T(0), T(0)};
-    for (int q = ns - 1; q >= 0; q--) {
-        const T ry = sry[q], rz = srz[q], ps = sps[q];
+    auto back = [&](T ry, T rz, T ps, T dps, int jb, int kb) {
         T lps = T(0);
-        const int jb = sjb[q], kb = skb[q];
         const int jb1 = wrap_m(jb + 1, My), kb1 = wrap_m(kb + 1, Mz);
         const size_t nd[4] = {(size_t)jb + (size_t)My * kb, (size_t)jb1 + (size_t)My * kb,
                               (size_t)jb + (size_t)My * kb1, (size_t)jb1 + (size_t)My * kb1};
@@ -417,10 +428,12 @@ __device__ __forceinline__ int push_adjoint_cic_one(const PushAdjArgs<T>& a, int
         ldy += lry * ps;
         ldz += lrz * ps;
         lps += lry * dy + lrz * dz;      // u = y + d ps
-        lstep += lps * sdps[q];
+        lstep += lps * dps;
         lyc = lry;      // the position before this sub-step
         lzc = lrz;
-    }
+    };
+    for (int q = ns - 1; q >= 1; q--) back(sry[q], srz[q], sps[q], sdps[q], sjb[q], skb[q]);
+    if (ns > 0) back(ry0, rz0, ps0, dps0, jb0, kb0);
     T lyp = lyc, lzp = lzc;
     ldy += lstep * dstep_dy;
     ldz += lstep * dstep_dz;
@@ -508,17 +521,13 @@ __device__ __forceinline__ int push_adjoint_cic_one(const PushAdjArgs<T>& a, int
     }
     // ---- backward through the gather g_f = sum_r wg_r F_f,r
     const T bg[6] = {bE[0], bE[1], bE[2], bB[0], bB[1], bB[2]};
-    T bwg[4] = {T(0), T(0), T(0), T(0)};
 #pragma unroll
-    for (int r = 0; r < 4; r++) {
+    for (int f = 0; f < 6; f++) {
+        lyp += bg[f] * gy[f];
+        lzp += bg[f] * gz[f];
 #pragma unroll
-        for (int f = 0; f < 6; f++) {
-            bwg[r] += bg[f] * F[f][r];
-            lf[f * 4 + r] = half * wg[r] * bg[f];
-        }
+        for (int r = 0; r < 4; r++) lf[f * 4 + r] = half * wg[r] * bg[f];
     }
-    lyp += (one - zp) * (bwg[1] - bwg[0]) + zp * (bwg[3] - bwg[2]);
-    lzp += (one - yp) * (bwg[2] - bwg[0]) + yp * (bwg[3] - bwg[1]);
     if (a.full) {
         a.lamPm[i] = bp[0];
         a.lamPm[a.n + i] = bp[1];
@@ -561,8 +570,11 @@ __device__ __forceinline__ bool warp_run_sums(T (&v)[NV], int key) {
     return key >= 0 && lane == rs;
 }
 
+// FP32: 3 blocks per SM (80 registers, the latency of the gathers hidden by
+// more warps); FP64 as many registers as it takes
 template <class T>
-__global__ void __launch_bounds__(256) push_adjoint_cic_kernel(PushAdjArgs<T> a) {
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 1)
+    push_adjoint_cic_kernel(PushAdjArgs<T> a) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     pdl_wait();
     T lf[24];
