@@ -1601,7 +1601,18 @@ struct Engine : EngineBase {
            LAM_D = 41,         // 3: adjoint of the real deposit Jx, Jy, Jz
            LAM_RHO0 = 44,      // 2: adjoint of rho_old along the corrector chain
            LAM_N = 46 };
-    T* lamp(int i) { return lam + (size_t)i * plane; }
+    // The C and P banks (and the CF and PF field sets) swap roles from one
+    // layer to the next: the P side of layer i is the C side of layer i+1.
+    int adj_par = 0;
+    T* lamp(int i) {
+        if (adj_par) {
+            if (i < LAM_P) i += 7;
+            else if (i < LAM_CF) i -= 7;
+            else if (i < LAM_PF) i += 6;
+            else if (i < LAM_CX) i -= 6;
+        }
+        return lam + (size_t)i * plane;
+    }
     T* lam_sbp(int layer, int q) { return lam_sb + ((size_t)layer * 2 + q) * plane; }
 
     // recompute the layers c .. lo of one segment from its checkpoint, storing
@@ -1690,16 +1701,27 @@ struct Engine : EngineBase {
     // of J] with the map between the halves of the transforms: z-pass of the
     // six field adjoints at `lf`, y-pass + the map's adjoint (+ the y-pass of
     // the current adjoints) per z-mode row, then their z-pass into LAM_D
-    void adj_map_fused(const T* lf, const AdjSpecArgs<T>& a, bool correct) {
+    // In the z-pass that reads the field adjoints at lf: with `push_share`
+    // (lf is a push's LAM_CX) they are also added to LAM_PF, the P layer's
+    // share; with `clear` lf is zeroed once read (LAM_CX for the next push,
+    // LAM_CF for its turn as the next layer's LAM_PF).
+    void adj_map_fused(T* lf, const AdjSpecArgs<T>& a, bool correct, bool push_share, bool clear) {
         if constexpr (sizeof(T) == 4) {
             const int EBz[6] = {CC, CC, SS, SS, SS, CC}, Jz[3] = {CC, CC, SS};
             const float* ins[6];
             float* outs[6];
+            float* acc[6];
+            float* clr[6];
             for (int f = 0; f < 6; f++) {
                 ins[f] = lf + (size_t)f * plane;
                 outs[f] = scratch + (size_t)f * plane;
+                acc[f] = lamp(LAM_PF + f);
+                clr[f] = lf + (size_t)f * plane;
             }
-            klaunch(KC_GEMM, [&] { return fftx->run_cols(6, ins, outs, EBz, inv_scale(), st); });
+            klaunch(KC_GEMM, [&] {
+                return fftx->run_cols(6, ins, outs, EBz, inv_scale(), st, push_share ? acc : nullptr,
+                                      clear ? clr : nullptr);
+            });
             klaunch(KC_SPECTRAL, [&] {
                 return fftx->run_adjoint_rows(a, correct, scratch, scratch, st);
             });
@@ -1717,7 +1739,9 @@ struct Engine : EngineBase {
         const T* fs = slot + 5 * (size_t)np;
         const T sc = inv_scale();
         Pf = f3layer(i + 1);
-        CK(cudaMemsetAsync(lamp(LAM_PF), 0, 6 * plane * sizeof(T), st));
+        // LAM_PF gathers this layer's shares from zero (on the fused path the
+        // first map cleared it in the previous layer, as its LAM_CF)
+        if (!fft_maps()) CK(cudaMemsetAsync(lamp(LAM_PF), 0, 6 * plane * sizeof(T), st));
         klaunch(KC_MISC, [&] {
             return launch_add_point<T>(lamp(LAM_CF), (size_t)(My / 2) + (size_t)My * (Mz / 2),
                                        d_dloss, i, st);
@@ -1738,18 +1762,23 @@ struct Engine : EngineBase {
             for (int f = 0; f < 7; f++) a.lP[f] = lamp(LAM_P + f);
             a.lP_set = 1;
             if (fft_maps()) {
-                adj_map_fused(lamp(LAM_CF), a, true);
+                adj_map_fused(lamp(LAM_CF), a, true, false, true);
             } else {
                 klaunch(KC_SPECTRAL, [&] { return launch_corrector_adjoint<T>(a, st); });
                 adj_xform(lamp(LAM_J), lamp(LAM_D), 3, Jz, Jy, T(1));
             }
         }
-        CK(cudaMemsetAsync(lamp(LAM_CX), 0, 6 * plane * sizeof(T), st));
+        // the push field adjoints (LAM_CX) start from zero; on the fused path
+        // the z-pass that reads them clears them and adds the P layer's share
+        if (!fft_maps()) CK(cudaMemsetAsync(lamp(LAM_CX), 0, 6 * plane * sizeof(T), st));
         klaunch(KC_PUSH, [&] {
             return push_adjoint(push_adj_args(slot, slot_cell, fs + (size_t)nIter * 6 * plane, 1));
         });
         // the P layer's field adjoint gathers every push's share
-        klaunch(KC_MISC, [&] { return launch_add_planes<T>(lamp(LAM_PF), lamp(LAM_CX), 6 * plane, st); });
+        if (!fft_maps())
+            klaunch(KC_MISC, [&] {
+                return launch_add_planes<T>(lamp(LAM_PF), lamp(LAM_CX), 6 * plane, st);
+            });
         int rho_in = LAM_RHO0;
         for (int it = nIter - 1; it >= 0; it--) {
             if (!fft_maps()) adj_xform(lamp(LAM_CX), lamp(LAM_SPEC), 6, EBz, EBy, sc);
@@ -1765,19 +1794,20 @@ struct Engine : EngineBase {
             for (int f = 0; f < 7; f++) a.lP[f] = lamp(LAM_P + f);
             a.lP_set = 0;
             if (fft_maps()) {
-                adj_map_fused(lamp(LAM_CX), a, true);
+                adj_map_fused(lamp(LAM_CX), a, true, true, true);
             } else {
                 klaunch(KC_SPECTRAL, [&] { return launch_corrector_adjoint<T>(a, st); });
                 adj_xform(lamp(LAM_J), lamp(LAM_D), 3, Jz, Jy, T(1));
             }
             rho_in = rho_out;
-            CK(cudaMemsetAsync(lamp(LAM_CX), 0, 6 * plane * sizeof(T), st));
+            if (!fft_maps()) CK(cudaMemsetAsync(lamp(LAM_CX), 0, 6 * plane * sizeof(T), st));
             klaunch(KC_PUSH, [&] {
                 return push_adjoint(push_adj_args(slot, slot_cell, fs + (size_t)it * 6 * plane, 0));
             });
-            klaunch(KC_MISC, [&] {
-                return launch_add_planes<T>(lamp(LAM_PF), lamp(LAM_CX), 6 * plane, st);
-            });
+            if (!fft_maps())
+                klaunch(KC_MISC, [&] {
+                    return launch_add_planes<T>(lamp(LAM_PF), lamp(LAM_CX), 6 * plane, st);
+                });
         }
         // Guess: C fields <- inverse transforms of the predicted E, B
         if (!fft_maps()) adj_xform(lamp(LAM_CX), lamp(LAM_SPEC), 6, EBz, EBy, sc);
@@ -1790,14 +1820,11 @@ struct Engine : EngineBase {
             }
             for (int f = 0; f < 7; f++) a.lP[f] = lamp(LAM_P + f);
             a.lP_set = 0;
-            if (fft_maps()) adj_map_fused(lamp(LAM_CX), a, false);
+            if (fft_maps()) adj_map_fused(lamp(LAM_CX), a, false, true, true);
             else klaunch(KC_SPECTRAL, [&] { return launch_predictor_adjoint<T>(a, st); });
         }
         // hand the P-side adjoints to layer i+1 (its final bank and fields)
-        CK(cudaMemcpyAsync(lamp(LAM_C), lamp(LAM_P), 7 * plane * sizeof(T),
-                           cudaMemcpyDeviceToDevice, st));
-        CK(cudaMemcpyAsync(lamp(LAM_CF), lamp(LAM_PF), 6 * plane * sizeof(T),
-                           cudaMemcpyDeviceToDevice, st));
+        adj_par ^= 1;
         CK(cudaGetLastError());
         return QS_OK;
     }
@@ -1805,6 +1832,7 @@ struct Engine : EngineBase {
     // the device part of the adjoint (capturable): clear the adjoints, sweep
     // the segments from layer lo to the head, then d loss / d beam weight
     qs_status adjoint_device(int lo) {
+        adj_par = 0;
         CK(cudaMemsetAsync(lam, 0, (size_t)LAM_N * plane * sizeof(T), st));
         CK(cudaMemsetAsync(lam_pm, 0, 3 * (size_t)np * sizeof(T), st));
         if (lam_pos) CK(cudaMemsetAsync(lam_pos, 0, 2 * (size_t)np * sizeof(T), st));

@@ -317,6 +317,8 @@ __global__ void __launch_bounds__(row_threads<M>()) fft_rows_kernel(RowArgs a) {
 struct ColArgs {
     const float* in[kMaxXfFields];
     float* out[kMaxXfFields];
+    float* acc[kMaxXfFields];   // optional: the input is also added here
+    float* clr[kMaxXfFields];   // optional: the input planes, zeroed once read
     int kind[kMaxXfFields];
     int ncols;                // row length of the planes (the y size)
     float scale;
@@ -347,10 +349,14 @@ __global__ void __launch_bounds__(TJ * (M / vpt<M>())) fft_cols_kernel(ColArgs a
     pdl_wait();
     const float* inf = a.in[0];
     float* outf = a.out[0];
+    float* accf = a.acc[0];
+    float* clrf = a.clr[0];
     int kind = a.kind[0];
 #pragma unroll
     for (int q = 1; q < kMaxXfFields; q++)
-        if (q == f) { inf = a.in[q]; outf = a.out[q]; kind = a.kind[q]; }
+        if (q == f) {
+            inf = a.in[q]; outf = a.out[q]; accf = a.acc[q]; clrf = a.clr[q]; kind = a.kind[q];
+        }
     const float2* pre = a.tab + M;
     float lo[V], hi[V];
     float2 w[V];
@@ -360,6 +366,22 @@ __global__ void __launch_bounds__(TJ * (M / vpt<M>())) fft_cols_kernel(ColArgs a
         lo[b] = inf[(size_t)(2 * i) * ld + col];
         hi[b] = inf[(size_t)(2 * M - 1 - 2 * i) * ld + col];
         w[b] = __ldg(pre + i);
+    }
+    if (accf || clrf) {   // the same for the whole CTA
+#pragma unroll
+        for (int b = 0; b < V; b++) {
+            const int i = jt + bitrev<V>(b) * T;
+            const size_t olo = (size_t)(2 * i) * ld + col;
+            const size_t ohi = (size_t)(2 * M - 1 - 2 * i) * ld + col;
+            if (accf) {
+                accf[olo] += lo[b];
+                accf[ohi] += hi[b];
+            }
+            if (clrf) {
+                clrf[olo] = 0.f;
+                clrf[ohi] = 0.f;
+            }
+        }
     }
     float2 v[V];
 #pragma unroll
@@ -812,12 +834,14 @@ DttFft* DttFft::create(int ny, int nz) {
 }
 
 int DttFft::run_cols(int nf, const float* const* in, float* const* out, const int* kind,
-                     float scale, cudaStream_t st) const {
+                     float scale, cudaStream_t st, float* const* acc, float* const* clr) const {
     if (nf <= 0 || nf > kMaxXfFields) return 0;
     fft::ColArgs a{};
     for (int f = 0; f < nf; f++) {
         a.in[f] = in[f];
         a.out[f] = out[f];
+        a.acc[f] = acc ? acc[f] : nullptr;
+        a.clr[f] = clr ? clr[f] : nullptr;
         a.kind[f] = kind[f];
     }
     a.ncols = ny;

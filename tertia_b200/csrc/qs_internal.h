@@ -99,9 +99,12 @@ struct DttFft {
     bool spec_rows = false;    // run_spectral_rows available (ny in [128, 1024])
     static DttFft* create(int ny, int nz);   // nullptr when a size is not handled
     int run_pass(int pass, const DttJob<float>& job, float* scratch, cudaStream_t st) const;
-    // the z-pass alone: nf planes in -> out, y-spectral or real alike
+    // the z-pass alone: nf planes in -> out, y-spectral or real alike; with
+    // `acc` each input plane is also added to acc[f], with `clr` the planes
+    // clr[f] (the inputs) are zeroed once read
     int run_cols(int nf, const float* const* in, float* const* out, const int* kind, float scale,
-                 cudaStream_t st) const;
+                 cudaStream_t st, float* const* acc = nullptr,
+                 float* const* clr = nullptr) const;
     // one z-mode row per CTA: [forward y-pass of the 3 z-transformed deposit
     // planes at jin, when `correct`] -> corrector (or predictor) of `a` ->
     // inverse y-pass of Ex Ey Ez Bx By Bz (, Rho when nout = 7) into `out`
