@@ -57,8 +57,8 @@ __global__ void __launch_bounds__(256) push_adjoint_kernel(PushAdjArgs<T> a) {
     T E[3], B[3];
 #pragma unroll
     for (int c = 0; c < 3; c++) {
-        E[c] = half * (ldg_(a.P + c * plane + n) + ldg_(a.C + c * plane + n));
-        B[c] = half * (ldg_(a.P + (3 + c) * plane + n) + ldg_(a.C + (3 + c) * plane + n));
+        E[c] = ldg_(a.F + c * plane + n);
+        B[c] = ldg_(a.F + (3 + c) * plane + n);
     }
     B[0] += a.bxe; B[1] += a.bye; B[2] += a.bze;
 
@@ -304,7 +304,7 @@ __device__ __forceinline__ int push_adjoint_cic_one(const PushAdjArgs<T>& a, int
         g[f] = T(0);
 #pragma unroll
         for (int r = 0; r < 4; r++) {
-            F[r] = half * (ldg_(a.P + f * plane + nn[r]) + ldg_(a.C + f * plane + nn[r]));
+            F[r] = ldg_(a.F + f * plane + nn[r]);
             g[f] += wg[r] * F[r];
         }
         gy[f] = (one - zp) * (F[1] - F[0]) + zp * (F[3] - F[2]);
@@ -570,10 +570,11 @@ __device__ __forceinline__ bool warp_run_sums(T (&v)[NV], int key) {
     return key >= 0 && lane == rs;
 }
 
-// FP32: 3 blocks per SM (80 registers, the latency of the gathers hidden by
-// more warps); FP64 as many registers as it takes
+// FP32: 4 blocks per SM (64 registers and a few spills; the latency of the
+// gathers hidden by more warps, measured faster than 2 or 3 blocks); FP64 as
+// many registers as it takes
 template <class T>
-__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 1)
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 1)
     push_adjoint_cic_kernel(PushAdjArgs<T> a) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     pdl_wait();
@@ -700,6 +701,25 @@ int launch_add_planes(T* acc, const T* x, size_t n, cudaStream_t st) {
     return 1;
 }
 
+// out = (P + C) / 2, the push's gathered fields (the same expression as the
+// push, so the adjoint recomputes the push the forward ran)
+template <class T>
+__global__ void avg_planes_kernel(const T* __restrict__ P, const T* __restrict__ C,
+                                  T* __restrict__ out, size_t n) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    pdl_wait();
+    out[i] = T(0.5) * (P[i] + C[i]);
+}
+
+template <class T>
+int launch_avg_planes(const T* P, const T* C, T* out, size_t n, cudaStream_t st) {
+    if (!n) return 0;
+    launch_pdl(avg_planes_kernel<T>, dim3((unsigned)((n + 255) / 256)), dim3(256), 0, st, P, C,
+               out, n);
+    return 1;
+}
+
 // ---------------------------------------------------------------------------
 // out[idx] += v[layer] for the on-axis loss gradient of one layer
 template <class T>
@@ -760,6 +780,7 @@ int launch_beam_weight_grad(const BeamGradArgs<T>& a, cudaStream_t st) {
     template int launch_predictor_adjoint<T>(const AdjSpecArgs<T>&, cudaStream_t);       \
     template int launch_add_point<T>(T*, size_t, const T*, int, cudaStream_t);           \
     template int launch_add_planes<T>(T*, const T*, size_t, cudaStream_t);               \
+    template int launch_avg_planes<T>(const T*, const T*, T*, size_t, cudaStream_t);     \
     template int launch_beam_weight_grad<T>(const BeamGradArgs<T>&, cudaStream_t);
 QS_ADJ_INST(float)
 QS_ADJ_INST(double)

@@ -1632,12 +1632,15 @@ struct Engine : EngineBase {
             T* fs = slot + 5 * (size_t)np;
             if ((s = layer_begin(i, 0))) break;
             if ((s = guess(i, 0))) break;
-            CK(cudaMemcpyAsync(fs, Cf, 6 * plane * sizeof(T), cudaMemcpyDeviceToDevice, st));
+            // each push's gathered fields (P + C) / 2, for its adjoint
+            klaunch(KC_MISC, [&] { return launch_avg_planes<T>(Pf, Cf, fs, 6 * plane, st); });
             for (int it = 0; it < nIter && !s; it++) {
                 if ((s = push(i, 0, 0))) break;
                 if ((s = iterate(i, 0, it, nullptr))) break;
-                CK(cudaMemcpyAsync(fs + (size_t)(it + 1) * 6 * plane, Cf, 6 * plane * sizeof(T),
-                                   cudaMemcpyDeviceToDevice, st));
+                klaunch(KC_MISC, [&] {
+                    return launch_avg_planes<T>(Pf, Cf, fs + (size_t)(it + 1) * 6 * plane,
+                                                6 * plane, st);
+                });
             }
             if (s) break;
             if ((s = push(i, 0, 1))) break;
@@ -1670,7 +1673,7 @@ struct Engine : EngineBase {
         return a;
     }
 
-    PushAdjArgs<T> push_adj_args(const T* slot, const int32_t* slot_cell, const T* Cfield,
+    PushAdjArgs<T> push_adj_args(const T* slot, const int32_t* slot_cell, const T* fields,
                                  int full) {
         PushAdjArgs<T> a{};
         a.n = np; a.My = My; a.Mz = Mz;
@@ -1678,7 +1681,7 @@ struct Engine : EngineBase {
         a.lamPos = lam_pos;
         a.y = slot; a.z = slot + np; a.px = slot + 2 * np; a.py = slot + 3 * np;
         a.pz = slot + 4 * np; a.w = pw;
-        a.P = Pf; a.C = Cfield;
+        a.F = fields;
         a.lamD = lamp(LAM_D);
         a.lamPm = lam_pm;
         a.lamFC = lamp(LAM_CX);

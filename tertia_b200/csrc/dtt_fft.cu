@@ -528,6 +528,9 @@ struct SpecRowArgs {
 };
 
 constexpr int kSpecGroups = 8;
+// one transform group per plane of a row: Ex..Bz and Rho out of the map
+// kernel, the six field adjoints into its adjoint
+static_assert(kSpecGroups >= 7, "a transform group per plane");
 
 template <int M>
 __host__ __device__ constexpr size_t spec_rows_smem() {

@@ -180,8 +180,7 @@ struct PushAdjArgs {
     int My, Mz;
     const int32_t* cell;
     const T *y, *z, *px, *py, *pz, *w;
-    const T* P;
-    const T* C;
+    const T* F;           // 6 planes: the fields the push gathered, (P + C) / 2
     const T* lamD;        // 3 planes
     T* lamPm;             // 3 x n
     T* lamFC;             // 6 planes: the field adjoint of this push (added to)
@@ -236,6 +235,9 @@ int launch_add_point(T* plane_ex, size_t idx, const T* v, int layer, cudaStream_
 // acc += x over n values
 template <class T>
 int launch_add_planes(T* acc, const T* x, size_t n, cudaStream_t st);
+// out = (P + C) / 2 over n values: the fields a push gathers, kept for its adjoint
+template <class T>
+int launch_avg_planes(const T* P, const T* C, T* out, size_t n, cudaStream_t st);
 
 // d loss / d (beam macro-particle weight) from the adjoint of the real beam
 // currents (lb3: (L+1) layers x 2 planes RhoBeam, JxBeam).
