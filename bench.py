@@ -57,6 +57,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64-plain comparison")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the c3 adjoint measurement")
+    ap.add_argument("--no-next", action="store_true",
+                    help="skip the density-profile march and hand-off measurements")
     ap.add_argument("--cpu-seconds", type=float, default=12.0,
                     help="target seconds of the bounded CPU sample")
     return ap.parse_args()
@@ -299,6 +301,84 @@ def adjoint_measure(precision: str):
 
 
 # ------------------------------------------------------------------ our arm
+def next_rows_measure(cfg, beam, uniform_ms, pushes_per_step, steps=2):
+    """The rows beside the march, on the bench's own workload and beam:
+
+    - a march through a non-uniform plasma (a Gaussian channel whose density
+      ramps along xi; the device seeding weights every cell by the profile and
+      the maps read the density at the head each layer), timed like the main
+      line (device events on the handle's stream, one warm-up step);
+    - the xi-pipeline hand-off: PackLayer of the tail layer with the plasma in
+      flight into a pinned host buffer and UnpackLayer of it, by the host
+      clock around the synchronous calls, and a march that starts from the
+      received layer (device events)."""
+    import ctypes as C
+    import numpy as np
+    import torch
+    from tertia_b200 import abi
+    from tertia_b200.mesh import Mesh
+
+    def timed_steps(m, n):
+        stream = torch.cuda.ExternalStream(m.stream())
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(n):
+            m.step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / n
+
+    out = {}
+    xf = cfg.hx * cfg.nx
+    prof = abi.density_profile(distribution=abi.DIST_GAUSS_CHANNEL, density=0.5, density1=1.5,
+                               delta=0.6, radius=0.4, begin=0.0, plateau_begin=0.0,
+                               plateau_end=xf + 4.0, end=1e9)
+    with Mesh(cfg) as m:
+        m.set_density_profile(prof)
+        m.load_beam(beam)
+        m.step()
+        ms = timed_steps(m, steps)
+        out["density_profile"] = {
+            "profile": "Gaussian channel (density 0.5 on axis, 1.5 outside, radius 0.4) "
+                       "ramping up along xi over the box (DIST_GAUSS_CHANNEL)",
+            "steps": steps, "ms_per_step": ms, "value": pushes_per_step / (ms / 1e3),
+            "unit": UNIT, "over_uniform_ms": ms / uniform_ms,
+            "onaxis_ex_max": float(np.abs(m.onaxis_ex()).max())}
+    with Mesh(cfg) as m:
+        m.load_beam(beam)
+        m.step()
+        L, h = m._L, m._h
+        n = int(L.qs_layer_pack_size(h))
+        buf = torch.empty(n, dtype=torch.float64, pin_memory=True)
+        ptr = C.cast(buf.data_ptr(), C.POINTER(C.c_double))
+        reps = 3
+        m.sync()
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            if L.qs_pack_layer(h, ptr, n):
+                raise RuntimeError("qs_pack_layer failed")
+        t_pack = (time.perf_counter() - t0) / reps
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            if L.qs_unpack_layer(h, ptr, n):
+                raise RuntimeError("qs_unpack_layer failed")
+        t_unpack = (time.perf_counter() - t0) / reps
+        m.step()                         # from the received layer: the march is rebuilt
+        if L.qs_unpack_layer(h, ptr, n):
+            raise RuntimeError("qs_unpack_layer failed")
+        ms_recv = timed_steps(m, 1)
+        nbytes = n * 8
+        out["handoff"] = {
+            "buffer_bytes": nbytes, "layout": "12 planes + 12 x Np particle values (doubles)",
+            "pack_ms": t_pack * 1e3, "unpack_ms": t_unpack * 1e3,
+            "pack_gbs": nbytes / t_pack / 1e9, "unpack_gbs": nbytes / t_unpack / 1e9,
+            "march_from_received_layer_ms": ms_recv,
+            "over_uniform_ms": ms_recv / uniform_ms}
+    return out
+
+
 def run_ours(args):
     import numpy as np
     import torch
@@ -579,6 +659,9 @@ def run_ours(args):
     adjoint = None
     if rank == 0 and world == 1 and not args.no_adjoint and not args.layers:
         adjoint = adjoint_measure(args.precision)
+    nxt = None
+    if rank == 0 and world == 1 and not args.no_next and not args.layers:
+        nxt = next_rows_measure(cfg, beam, ms_max, pushes_per_step)
 
     if rank == 0:
         line = {
@@ -601,6 +684,7 @@ def run_ours(args):
             "cpu_baseline": cpu,
             "fp64_plain": fp64,
             "adjoint": adjoint,
+            "next_rows": nxt,
             "clocks": clk,
             "onaxis_ex_max": float(np.max(np.abs(onaxis))),
         }

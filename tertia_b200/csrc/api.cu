@@ -309,6 +309,11 @@ struct Engine : EngineBase {
     int64_t adj_kernels = 0;
     int64_t adj_np = 0, adj_nb = 0;
 
+    // the hand-off buffer assembled on the device, and its ordering scratch
+    double* d_pack = nullptr;
+    int* d_pack_i = nullptr;
+    size_t pack_cap = 0;
+
     T* bankp(int b, int p) { return bank + ((size_t)b * SP_N + p) * plane; }
     T* f3layer(int i) { return f3 + (size_t)i * 6 * plane; }
 
@@ -322,7 +327,7 @@ struct Engine : EngineBase {
                         bpx, bpy, bpz, bw, d_err, dens_dev, front_src, front_beam, ck, seg, lam, lam_pm, lam_sb, lam_b3,
                         d_dloss, d_gradw, acell, pid, apid, ay, az, apx, apy, apz, aw, cic_cnt,
                         cic_loff, cic_bsum, cic_bpref, cic_ticket, ck_cell, ck_id, seg_cell,
-                        adj_inv, lam_pos, adj_tmp};
+                        adj_inv, lam_pos, adj_tmp, d_pack, d_pack_i};
         for (void* p : ptrs)
             if (p) cudaFree(p);
         if (st) cudaStreamDestroy(st);
@@ -1298,66 +1303,79 @@ struct Engine : EngineBase {
             return fail(QS_ERR_INVALID, "qs_pack_layer: n must be qs_layer_pack_size (%lld)",
                         (long long)pack_size());
         if (!tail_ready) return fail(QS_ERR_STATE, "qs_pack_layer: no complete march to pack");
-        qs_status s;
+        {
+            const qs_status s0 = check_device();   // the march's own errors come first
+            if (s0) return s0;
+        }
+        // the buffer is assembled in device memory and leaves in one copy
+        if ((size_t)n > pack_cap) {
+            if (d_pack) cudaFree(d_pack);
+            if (d_pack_i) cudaFree(d_pack_i);
+            d_pack = nullptr;
+            d_pack_i = nullptr;
+            pack_cap = 0;
+            qs_status s = alloc(&d_pack, (size_t)n, "hand-off buffer");
+            if (!s) s = alloc(&d_pack_i, 3 * plane + 1 + (size_t)np, "hand-off buffer order");
+            if (s) return s;
+            pack_cap = (size_t)n;
+        }
         const size_t P = plane;
+        double* dp = d_pack;
         // the tail layer's fields
         const int fsrc[6] = {3, 4, 5, 0, 1, 2};
         for (int f = 0; f < 6; f++)
-            if ((s = get_plane(f3layer(0) + (size_t)fsrc[f] * P, buf + (size_t)f * P))) return s;
+            klaunch(KC_MISC, [&] {
+                return launch_convert_back<T>(f3layer(0) + (size_t)fsrc[f] * P, dp + (size_t)f * P,
+                                              P, st);
+            });
         // its currents: the deposit of its last push, kept as the P sources
         for (int f = 0; f < 3; f++)
-            if ((s = get_plane(Psrc + (size_t)f * P, buf + (size_t)(6 + f) * P))) return s;
+            klaunch(KC_MISC, [&] {
+                return launch_convert_back<T>(Psrc + (size_t)f * P, dp + (size_t)(6 + f) * P, P,
+                                              st);
+            });
         // its Rho: the corrected spectral rho, inverse-transformed and
         // normalised as the Iterate store does (:1546-1602)
         {
             T* outs[1] = {stage};
             const int kz[1] = {CC}, ky[1] = {CC};
             xform(job_stack(bankp(cur ^ 1, SP_RHO), 1, outs, kz, ky, inv_scale()));
-            CK(cudaGetLastError());
-            if ((s = get_plane(stage, buf + 9 * P))) return s;
+            klaunch(KC_MISC, [&] { return launch_convert_back<T>(stage, dp + 9 * P, P, st); });
         }
         // the beam spectra of its last split (fft_of_JxBeam, fft_of_RhoBeam)
         {
-            std::vector<double> t0(P), t1(P);
             const double w0 = 1.0 / S, w1 = (double)(S - 1) / S;
             for (int q = 0; q < 2; q++) {
-                if ((s = get_plane(sbp(0, q), t0.data()))) return s;
-                if (S > 1 && (s = get_plane(sbp(1, q), t1.data()))) return s;
-                double* out = buf + (q == 0 ? 11 : 10) * P;
-                for (size_t i = 0; i < P; i++) out[i] = S > 1 ? w0 * t0[i] + w1 * t1[i] : t0[i];
+                double* out = dp + (q == 0 ? 11 : 10) * P;
+                if (S > 1)
+                    klaunch(KC_MISC, [&] {
+                        return launch_pack_mix<T>(sbp(0, q), sbp(1, q), w0, w1, P, out, st);
+                    });
+                else
+                    klaunch(KC_MISC, [&] { return launch_convert_back<T>(sbp(0, q), out, P, st); });
             }
         }
-        // the plasma in flight, cell by cell (k outer, j inner, as the layer
-        // walk of paraCPUlayers.cu:76-113), load order within a cell
-        const int64_t m = np;
-        if (m > 0) {
-            std::vector<int32_t> cell(m);
-            std::vector<double> y(m), z(m), px(m), py_(m), pz_(m), w(m);
-            if ((s = get_plasma(m, cell.data(), y.data(), z.data(), px.data(), py_.data(),
-                                pz_.data(), w.data())))
-                return s;
-            std::vector<int64_t> ord(m);
-            for (int64_t p = 0; p < m; p++) ord[p] = p;
-            std::stable_sort(ord.begin(), ord.end(),
-                             [&](int64_t a, int64_t b) { return cell[a] < cell[b]; });
-            double* pb = buf + 12 * P;
-            for (int64_t r = 0; r < m; r++) {
-                const int64_t p = ord[r];
-                pb[r] = px[p];
-                pb[r + m] = py_[p];
-                pb[r + 2 * m] = pz_[p];
-                pb[r + 3 * m] = 0.0;                     // in-cell xi: plasma enters at x = 0
-                pb[r + 4 * m] = y[p];
-                pb[r + 5 * m] = z[p];
-                pb[r + 6 * m] = cfg.plasma_q2m;
-                pb[r + 7 * m] = w[p];
-                pb[r + 8 * m] = 0.0;                     // the layer index i_X
-                pb[r + 9 * m] = (double)(cell[p] % My);
-                pb[r + 10 * m] = (double)(cell[p] / My);
-                pb[r + 11 * m] = 0.0;                    // isort: the plasma electrons
-            }
+        // the plasma in flight, cell by cell, load order within a cell
+        if (np > 0) {
+            int* cnt = d_pack_i;
+            int* fill = cnt + P;
+            int* start = fill + P;
+            int32_t* ord = start + P + 1;
+            CK(cudaMemsetAsync(cnt, 0, 2 * P * sizeof(int), st));
+            PackArgs<T> a{};
+            a.m = np; a.My = My; a.ncell = (int)P;
+            a.cell = pcell;
+            a.key = cic_sort ? pid : nullptr;   // regrouped: the load ids give the order
+            a.y = py; a.z = pz; a.px = ppx; a.py = ppy; a.pz = ppz; a.w = pw;
+            a.q2m = cfg.plasma_q2m;
+            a.cnt = cnt; a.start = start; a.fill = fill; a.ord = ord;
+            a.out = dp + 12 * P;
+            a.err = d_err;
+            klaunch(KC_MISC, [&] { return launch_pack_particles<T>(a, st); });
         }
-        return QS_OK;
+        CK(cudaMemcpyAsync(buf, dp, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, st));
+        CK(cudaGetLastError());
+        return check_device();
     }
 
     qs_status unpack_layer(const double* buf, int64_t n) override {

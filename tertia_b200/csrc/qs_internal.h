@@ -235,6 +235,30 @@ int launch_add_point(T* plane_ex, size_t idx, const T* v, int layer, cudaStream_
 // acc += x over n values
 template <class T>
 int launch_add_planes(T* acc, const T* x, size_t n, cudaStream_t st);
+// The particle blocks of the hand-off buffer (pack.cu): the m particles
+// ordered by cell, load order within a cell (key = load ids, or null when the
+// device order is the load order), as 12 double rows at out.  Scratch: cnt
+// and fill (ncell ints, zeroed by the caller), start (ncell + 1), ord (m).
+template <class T>
+struct PackArgs {
+    int64_t m;
+    int My, ncell;
+    const int32_t* cell;
+    const int32_t* key;
+    const T *y, *z, *px, *py, *pz, *w;
+    double q2m;
+    int *cnt, *start, *fill;
+    int32_t* ord;
+    double* out;
+    int* err;
+};
+template <class T>
+int launch_pack_particles(const PackArgs<T>& a, cudaStream_t st);
+// out = w0 a + w1 b over n values, in double
+template <class T>
+int launch_pack_mix(const T* a, const T* b, double w0, double w1, size_t n, double* out,
+                    cudaStream_t st);
+
 // out = (P + C) / 2 over n values: the fields a push gathers, kept for its adjoint
 template <class T>
 int launch_avg_planes(const T* P, const T* C, T* out, size_t n, cudaStream_t st);

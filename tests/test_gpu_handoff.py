@@ -68,6 +68,36 @@ def test_packed_layer_matches_oracle(oracle_lib, prec, shape):
     m.close()
 
 
+@pytest.mark.parametrize("prec,shape", [("fp64", abi.QS_SHAPE_NGP), ("fp64", abi.QS_SHAPE_CIC),
+                                        ("fp32", abi.QS_SHAPE_CIC)])
+def test_packed_particles_are_the_plasma_cell_by_cell(prec, shape):
+    """The particle blocks hold the plasma in flight ordered by cell (k outer,
+    j inner) and by load order within a cell, value for value, and the planes
+    are the tail layer's fields."""
+    from tertia_b200.mesh import Mesh
+    full, half, beam, upper, empty = boxes(prec, shape)
+    with Mesh(half) as m:
+        m.load_beam(upper)
+        m.load_front_plasma(wl.front_plasma(half, seed=5))
+        m.step()
+        buf = m.pack_layer()
+        pl = m.get_plasma()
+        planes, parts = layout(buf, half)
+        for slot, f in zip(range(6), (abi.QS_F_BX, abi.QS_F_BY, abi.QS_F_BZ, abi.QS_F_EX,
+                                      abi.QS_F_EY, abi.QS_F_EZ)):
+            np.testing.assert_array_equal(planes[slot], m.get_field3d(f, 0).ravel())
+    order = np.argsort(pl["cell"], kind="stable")
+    n = order.size
+    assert parts.shape == (12, n)
+    for row, key in ((0, "px"), (1, "py"), (2, "pz"), (4, "y"), (5, "z"), (7, "w")):
+        np.testing.assert_array_equal(parts[row], pl[key][order], err_msg=key)
+    cell = pl["cell"][order]
+    np.testing.assert_array_equal(parts[9], cell % half.ny)
+    np.testing.assert_array_equal(parts[10], cell // half.ny)
+    assert np.all(parts[3] == 0) and np.all(parts[8] == 0) and np.all(parts[11] == 0)
+    assert np.all(parts[6] == half.plasma_q2m)
+
+
 @pytest.mark.parametrize("prec,shape,graph", [("fp64", abi.QS_SHAPE_NGP, 1),
                                               ("fp64", abi.QS_SHAPE_CIC, 0),
                                               ("fp32", abi.QS_SHAPE_CIC, 1)])
