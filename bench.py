@@ -312,7 +312,6 @@ def next_rows_measure(cfg, beam, uniform_ms, pushes_per_step, steps=2):
       flight into a pinned host buffer and UnpackLayer of it, by the host
       clock around the synchronous calls, and a march that starts from the
       received layer (device events)."""
-    import ctypes as C
     import numpy as np
     import torch
     from tertia_b200 import abi
@@ -349,25 +348,20 @@ def next_rows_measure(cfg, beam, uniform_ms, pushes_per_step, steps=2):
     with Mesh(cfg) as m:
         m.load_beam(beam)
         m.step()
-        L, h = m._L, m._h
-        n = int(L.qs_layer_pack_size(h))
-        buf = torch.empty(n, dtype=torch.float64, pin_memory=True)
-        ptr = C.cast(buf.data_ptr(), C.POINTER(C.c_double))
+        n = m.pack_size()
+        buf = torch.empty(n, dtype=torch.float64, pin_memory=True).numpy()
         reps = 3
         m.sync()
         t0 = time.perf_counter()
         for _ in range(reps):
-            if L.qs_pack_layer(h, ptr, n):
-                raise RuntimeError("qs_pack_layer failed")
+            m.pack_layer(out=buf)
         t_pack = (time.perf_counter() - t0) / reps
         t0 = time.perf_counter()
         for _ in range(reps):
-            if L.qs_unpack_layer(h, ptr, n):
-                raise RuntimeError("qs_unpack_layer failed")
+            m.unpack_layer(buf)
         t_unpack = (time.perf_counter() - t0) / reps
         m.step()                         # from the received layer: the march is rebuilt
-        if L.qs_unpack_layer(h, ptr, n):
-            raise RuntimeError("qs_unpack_layer failed")
+        m.unpack_layer(buf)
         ms_recv = timed_steps(m, 1)
         nbytes = n * 8
         out["handoff"] = {

@@ -136,11 +136,20 @@ class Mesh:
         self._chk(self._L.qs_get_phase(self._h, C.byref(out)), "qs_get_phase")
         return out.value
 
-    def pack_layer(self) -> np.ndarray:
+    def pack_size(self) -> int:
+        """Doubles in the hand-off buffer: 12 ny nz + 12 Np."""
+        return int(self._L.qs_layer_pack_size(self._h))
+
+    def pack_layer(self, out: np.ndarray | None = None) -> np.ndarray:
         """PackLayer: the tail layer and the plasma in flight after a march, in
-        the reference's hand-off buffer layout."""
-        n = int(self._L.qs_layer_pack_size(self._h))
-        out = np.empty(n)
+        the reference's hand-off buffer layout.  `out` (contiguous float64 of
+        pack_size() values, pinned host memory for the fastest copy) is filled
+        in place when given."""
+        n = self.pack_size()
+        if out is None:
+            out = np.empty(n)
+        elif out.dtype != np.float64 or out.size != n or not out.flags["C_CONTIGUOUS"]:
+            raise ValueError(f"pack_layer: out must be contiguous float64 of {n} values")
         self._chk(self._L.qs_pack_layer(self._h, _p(out, C.c_double), n), "qs_pack_layer")
         return out
 
