@@ -66,10 +66,8 @@ def parse():
 
 # ------------------------------------------------------------------ helpers
 def dist_env():
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    return rank, world, local
+    from tertia_b200.replicas import dist_env as env
+    return env()
 
 
 class ClockSampler:
@@ -380,13 +378,10 @@ def run_ours(args):
     from tertia_b200.abi import PRECISIONS, QS_SHAPE_CIC, QS_SHAPE_NGP
     from tertia_b200.mesh import Mesh
 
+    from tertia_b200 import replicas
     rank, world, local = dist_env()
     torch.cuda.set_device(local)
-    if world > 1:
-        import torch.distributed as dist
-        from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=300),
-                                device_id=torch.device("cuda", local))
+    replicas.init(world, local, "nccl", timeout_s=300)
     w = wl.make_workload(args.workload, args.precision)
     cfg = w.cfg
     cfg.shape = QS_SHAPE_CIC if args.shape == "cic" else QS_SHAPE_NGP
@@ -404,17 +399,10 @@ def run_ours(args):
     pushes_per_step = npl * cfg.nx * cfg.nx_split
 
     def barrier():
-        if world > 1:
-            import torch.distributed as dist
-            dist.barrier()
+        replicas.barrier(world)
 
     def max_over_ranks(x):
-        if world == 1:
-            return x
-        import torch.distributed as dist
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return replicas.max_over_ranks(x, world, "cuda")
 
     m = Mesh(cfg)
     m.load_beam(beam)
@@ -439,7 +427,7 @@ def run_ours(args):
     clk = clocks.stop()
     launches = m.kernel_launches() - l0
     ms_max = max_over_ranks(ms)
-    value = world * pushes_per_step / (ms_max / 1e3)
+    value = replicas.whole_job_rate(pushes_per_step, world, ms_max)
     onaxis = m.onaxis_ex()
 
     # ---------------- e2e: the public C ABI with host buffers (pinned)
@@ -670,7 +658,8 @@ def run_ours(args):
                        "step": "one beam step: beam push + full xi-march",
                        "l2": "inputs larger than L2 (field store 6.4 GB, beam currents 2.1 GB)",
                        "parallelism": f"replicas x{world}"},
-            "e2e": {"value": world * pushes_per_step / (e2e_ms / 1e3), "unit": UNIT,
+            "e2e": {"value": replicas.whole_job_rate(pushes_per_step, world, e2e_ms),
+                    "unit": UNIT,
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "ms_per_step": e2e_ms},
             "gpu_launches": launches,
@@ -683,9 +672,7 @@ def run_ours(args):
             "onaxis_ex_max": float(np.max(np.abs(onaxis))),
         }
         print(json.dumps(line), flush=True)
-    if world > 1:
-        import torch.distributed as dist
-        dist.destroy_process_group()
+    replicas.finish(world)
 
 
 # ------------------------------------------------------------ reference arm
