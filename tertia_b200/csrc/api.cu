@@ -1400,10 +1400,12 @@ struct Engine : EngineBase {
                                                 "plasma electron species", (long long)r);
             cell[r] = (int32_t)jd + My * (int32_t)kd;
         }
-        std::vector<int64_t> ord(m);
-        for (int64_t r = 0; r < m; r++) ord[r] = r;
-        std::stable_sort(ord.begin(), ord.end(),
-                         [&](int64_t a, int64_t b) { return cell[a] < cell[b]; });
+        // stable counting sort by cell (the buffer order kept within a cell;
+        // every cell was checked to lie inside the layer)
+        std::vector<int64_t> start(plane + 1, 0), ord(m);
+        for (int64_t r = 0; r < m; r++) start[(size_t)cell[r] + 1]++;
+        for (size_t c = 0; c < plane; c++) start[c + 1] += start[c];
+        for (int64_t r = 0; r < m; r++) ord[start[(size_t)cell[r]]++] = r;
         std::vector<int32_t> c2(m);
         std::vector<double> y(m), z(m), px(m), py_(m), pz_(m), w(m);
         for (int64_t r = 0; r < m; r++) {
