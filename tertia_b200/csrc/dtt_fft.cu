@@ -10,9 +10,10 @@
 // A DST-IV is the DCT-IV of the reversed input with the odd outputs negated.
 // The FFT is the Stockham autosort formulation of Govindaraju et al.
 // ("High performance discrete Fourier transforms on graphics processors",
-// SC 2008): a radix-16 pass, then radix-8 passes (4/2 for the rest), each
-// thread holding one radix-R butterfly group in registers and the sequence in
-// shared memory between passes.  Every twiddle comes from one table of
+// SC 2008): a radix-V pass in registers (V values per thread: 8 for
+// n <= 256, 16 above), then Stockham passes of radix V (and the remaining
+// factor) through shared memory, each thread holding one butterfly group in
+// registers and the sequence in shared memory between passes.  Every twiddle comes from one table of
 // e^{-2 pi i k/(n/2)} built in FP64 on the host, so the error is that of an
 // FP32 FFT (a few 1e-7 relative), well below the split-precision GEMMs'.
 //
@@ -462,7 +463,7 @@ cudaError_t launch_cols(const ColArgs& a, int nf, cudaStream_t st) {
 // [corrector or predictor on the row's modes] -> [inverse y-transform of E, B
 // (and Rho)], with the row in shared memory in between; the column kernel
 // then finishes the inverse along z.  A CTA holds one row: 8 groups of
-// T = M/16 lanes (one warp holds whole groups), each group taking one plane's
+// T = M/V lanes (one warp holds whole groups), each group taking one plane's
 // row through a transform; groups without a plane run it on zeros, so that
 // every lane meets every shuffle.
 
