@@ -13,9 +13,10 @@
 // SC 2008): a radix-V pass in registers (V values per thread: 8 for
 // n <= 256, 16 above), then Stockham passes of radix V (and the remaining
 // factor) through shared memory, each thread holding one butterfly group in
-// registers and the sequence in shared memory between passes.  Every twiddle comes from one table of
-// e^{-2 pi i k/(n/2)} built in FP64 on the host, so the error is that of an
-// FP32 FFT (a few 1e-7 relative), well below the split-precision GEMMs'.
+// registers and the sequence in shared memory between passes.  Every twiddle
+// comes from one table of e^{-2 pi i k/(n/2)} built in FP64 on the host, so
+// the error is that of an FP32 FFT (a few 1e-7 relative), well below the
+// split-precision GEMMs'.
 //
 // A 2-D transform is two kernels over a batch of planes (nz rows of ny, y
 // fastest): rows along y into a scratch plane, then columns along z into the
