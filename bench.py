@@ -643,7 +643,11 @@ def run_ours(args):
         adjoint = adjoint_measure(args.precision)
     nxt = None
     if rank == 0 and world == 1 and not args.no_next and not args.layers:
-        nxt = next_rows_measure(cfg, beam, ms_max, pushes_per_step)
+        # auxiliary rows: a failure here is reported in the line, not fatal to it
+        try:
+            nxt = next_rows_measure(cfg, beam, ms_max, pushes_per_step)
+        except Exception as e:   # noqa: BLE001
+            nxt = {"error": f"{type(e).__name__}: {e}"}
 
     if rank == 0:
         line = {
