@@ -223,7 +223,10 @@ int64_t qs_layer_pack_size(const qs_handle* h);
 /* PackLayer + SendLayer's device read (para.cpp:94-150, 286-330): after a
  * march, the tail layer (layer 0: fields, the currents of its last push, the
  * corrected Rho, the beam spectra of its last split) and the plasma in
- * flight.  n must be qs_layer_pack_size(h). */
+ * flight, particles cell by cell and in load order within a cell.  n must be
+ * qs_layer_pack_size(h).  The buffer is assembled in device memory and copied
+ * to buf once (synchronous on return); pinned host memory gives the full
+ * copy rate. */
 qs_status qs_pack_layer(qs_handle* h, double* buf, int64_t n);
 /* ReceiveLayer + UnpackLayer + CUDA_WRAP_setLayerToMesh (para.cpp:332-412,
  * 175-285; paraCPUlayers.cu:178-297): the received layer becomes the front
