@@ -260,6 +260,18 @@ qs_status qs_get_onaxis_ex(qs_handle* h, double* out);
  * compute: psi(nx) = 0, psi(i) = psi(i+1) + hx (Ex_i + Ex_{i+1})/2 on axis. */
 qs_status qs_get_psi(qs_handle* h, double* out);
 
+/* No counterpart in the reference (which has no such diagnostic; the planes
+ * summed are those its Cell array stores).  FP64 global charge sums of every
+ * layer of the last march, computed on the device in FP64 whatever the
+ * precision of the march: the sum over the transverse plane of
+ *   rho[nx]        the corrected density (the Cell's f_Dens after the layer's
+ *                  last Iterate, movefieldshydrolinlayersplit.cpp:1545-1602),
+ *   jx[nx]         the Jx deposit of the layer's full push,
+ *   rho_beam[nx+1] RhoBeam of the beam-current store after the last beam push
+ *                  (MoveBeamInCell, movebeam.cpp:662-774).
+ * Any pointer may be NULL. */
+qs_status qs_get_charge_sums(qs_handle* h, double* rho, double* jx, double* rho_beam);
+
 /* --------------------------------------------------------------- the path */
 
 /* Domain::Step (step.cpp:24-122): phase += Ts, beam push, xi-march. */
@@ -314,8 +326,10 @@ qs_status qs_transform2d_dev(qs_handle* h, int kind_z, int kind_y, int batch,
  * which each GPU that loads the module holds until the process exits; it
  * limits ny and nz to 512 (each a multiple of 8): larger sizes return
  * QS_ERR_INVALID with the reason in qs_last_error(NULL).  The first call on a
- * device looks up the array's device address (once per device), so make that
- * first call before any stream capture.  All calls on a device share the
+ * device looks up the array's device address (again only after the device's
+ * context has changed, e.g. after cudaDeviceReset), so make that first call
+ * before any stream capture.  A CUDA error already pending on the calling
+ * thread is reported as QS_ERR_CUDA and left in place; nothing is launched.  All calls on a device share the
  * array: calls whose GPU work overlaps (other streams, other host threads)
  * race and must be ordered by the caller. */
 qs_status qs_transform2d_noalloc(int kind_z, int kind_y, int ny, int nz, int batch,

@@ -28,7 +28,9 @@ def build(force: bool = False) -> str:
 
 
 REF_LIB_PATH = os.path.join(_HERE, "_ref", "libref_linearized.so")
-REFERENCE = "/root/reference"
+# the reference checkout the recipe compiles from: QS_REFERENCE_DIR, else the
+# path where this build environment mounts it
+REFERENCE = os.environ.get("QS_REFERENCE_DIR", "/root/reference")
 
 
 def build_reference() -> str | None:
@@ -134,6 +136,8 @@ def _declare(L):
     for name in ("qso_get_field3d", "qso_set_beam_currents", "qso_get_beam_currents"):
         getattr(L, name).argtypes = [P, C.c_int, C.c_int, _f64p]
     L.qso_get_onaxis_ex.argtypes = [P, _f64p]
+    L.qso_get_psi.argtypes = [P, _f64p]
+    L.qso_get_charge_sums.argtypes = [P, _f64p, _f64p, _f64p]
     for name in ("qso_step", "qso_move_beam_particles", "qso_move_all_split_layers",
                  "qso_begin_march"):
         getattr(L, name).argtypes = [P]
@@ -324,6 +328,17 @@ class Oracle:
         out = np.empty(self.cfg.nx)
         _check(lib().qso_get_onaxis_ex(self._h, out), "qso_get_onaxis_ex")
         return out
+
+    def psi(self):
+        out = np.empty(self.cfg.nx)
+        _check(lib().qso_get_psi(self._h, out), "qso_get_psi")
+        return out
+
+    def charge_sums(self):
+        """FP64 per-layer sums: rho (nx), jx (nx), rho_beam (nx + 1)."""
+        r, j, b = np.empty(self.cfg.nx), np.empty(self.cfg.nx), np.empty(self.cfg.nx + 1)
+        _check(lib().qso_get_charge_sums(self._h, r, j, b), "qso_get_charge_sums")
+        return {"rho": r, "jx": j, "rho_beam": b}
 
     def step(self):
         _check(lib().qso_step(self._h), "qso_step")

@@ -1693,6 +1693,44 @@ int qso_get_onaxis_ex(qso* h, double* out) {
     return QS_OK;
 }
 
+int qso_get_psi(qso* h, double* out) {
+    if (!h || !out) return QS_ERR_INVALID;
+    const Oracle& o = h->o;
+    // psi(nx) = 0 ahead of the box, trapezoid of on-axis Ex towards the tail
+    double psi = 0.0, prev = 0.0;
+    for (int i = o.L - 1; i >= 0; i--) {
+        psi += o.cfg.hx * 0.5 * (o.onaxis[(size_t)i] + prev);
+        out[i] = psi;
+        prev = o.onaxis[(size_t)i];
+    }
+    return QS_OK;
+}
+
+int qso_get_charge_sums(qso* h, double* rho, double* jx, double* rho_beam) {
+    if (!h) return QS_ERR_INVALID;
+    const Oracle& o = h->o;
+    // stored layer i: plane 9 is f_Dens after the layer's last Iterate (the
+    // corrected density, :1545-1602), plane 6 the Jx deposit of its full push
+    for (int i = 0; i < o.L; i++) {
+        double sr = 0.0, sj = 0.0;
+        for (int k = 0; k < o.Mz; k++)
+            for (int j = 0; j < o.My; j++) {
+                sr += o.A[o.aidx(i, 9, j, k)];
+                sj += o.A[o.aidx(i, 6, j, k)];
+            }
+        if (rho) rho[i] = sr;
+        if (jx) jx[i] = sj;
+    }
+    if (rho_beam)
+        for (int i = 0; i <= o.L; i++) {
+            double sb = 0.0;
+            for (int k = 0; k < o.Mz; k++)
+                for (int j = 0; j < o.My; j++) sb += o.Bm[3][o.bidx(i, j, k)];
+            rho_beam[i] = sb;
+        }
+    return QS_OK;
+}
+
 int qso_step(qso* h) {
     if (!h) return QS_ERR_INVALID;
     h->o.phase += h->o.ts;  // step.cpp:33

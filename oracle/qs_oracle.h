@@ -79,6 +79,16 @@ int qso_set_beam_currents(qso* o, int field, int layer, const double* data);
 int qso_get_beam_currents(qso* o, int field, int layer, double* out);
 int qso_get_onaxis_ex(qso* o, double* out);
 
+/* Wake potential on axis (a derived quantity the reference does not
+ * compute): psi(nx) = 0, psi(i) = psi(i+1) + hx (Ex_i + Ex_{i+1})/2 over the
+ * on-axis Ex of the last march. */
+int qso_get_psi(qso* o, double* out);
+/* FP64 sums over the interior cells of every layer of the last march:
+ * rho[nx] of f_Dens after the layer's last Iterate (the corrected density,
+ * movefieldshydrolinlayersplit.cpp:1545-1602), jx[nx] of the Jx deposit of
+ * its full push, rho_beam[nx+1] of RhoBeam of the beam-current store.  Any
+ * pointer may be NULL. */
+int qso_get_charge_sums(qso* o, double* rho, double* jx, double* rho_beam);
 int qso_step(qso* o);
 /* Specie::Density (plasma.cpp:6-399) of a profile at (x, y, z). */
 double qso_density(const qs_density_profile* p, double x, double y, double z);

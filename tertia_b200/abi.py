@@ -199,6 +199,7 @@ def _declare(L):
     L.qs_get_beam_currents.argtypes = [P, C.c_int, C.c_int, f64p]
     L.qs_get_onaxis_ex.argtypes = [P, f64p]
     L.qs_get_psi.argtypes = [P, f64p]
+    L.qs_get_charge_sums.argtypes = [P, f64p, f64p, f64p]
     for name in ("qs_step", "qs_move_beam_particles", "qs_move_all_split_layers", "qs_begin_march"):
         getattr(L, name).argtypes = [P]
     for name in ("qs_layer_begin", "qs_move_split_layer", "qs_guess_fields", "qs_layer_end"):
@@ -238,7 +239,7 @@ EXPORTED_SYMBOLS = [
     "qs_set_phase", "qs_get_phase", "qs_layer_pack_size", "qs_pack_layer", "qs_unpack_layer",
     "qs_clear_front_layer",
     "qs_set_layer", "qs_get_layer", "qs_get_field3d", "qs_set_beam_currents",
-    "qs_get_beam_currents", "qs_get_onaxis_ex", "qs_get_psi", "qs_step",
+    "qs_get_beam_currents", "qs_get_onaxis_ex", "qs_get_psi", "qs_get_charge_sums", "qs_step",
     "qs_move_beam_particles", "qs_move_all_split_layers", "qs_begin_march", "qs_layer_begin",
     "qs_move_split_layer", "qs_guess_fields", "qs_move_particles_layer", "qs_iterate_fields",
     "qs_layer_end", "qs_transform2d", "qs_transform2d_dev", "qs_transform2d_noalloc",

@@ -8,6 +8,13 @@ bin's value, deposit the beam (qs_move_beam_particles) and march
 (qs_move_all_split_layers) with layer checkpoints.  Backward: qs_adjoint gives
 d loss / d w_p per particle; the bin gradient is sum over the bin of
 w0_p d loss / d w_p.
+
+The adjoint differentiates the state the mesh holds, which is that of its
+most recent forward.  A backward therefore has to come before the next
+forward (or adjoint) on the same mesh: WakeLoss records the mesh's
+state_version after its forward and its backward raises if the mesh has
+changed since, instead of returning the gradient at another point.  Use one
+mesh per loss that is still waiting for its backward.
 """
 from __future__ import annotations
 
@@ -30,15 +37,24 @@ class WakeLoss(torch.autograd.Function):
         c = np.asarray(coeff, dtype=np.float64)
         ctx.mesh, ctx.beam, ctx.bins, ctx.coeff = mesh, beam, bins, c
         ctx.nbins = len(beta)
+        ctx.version = getattr(mesh, "state_version", None)
         return bin_weights.new_tensor(float(np.dot(c, ex)))
 
     @staticmethod
     def backward(ctx, grad_out):
+        version = getattr(ctx.mesh, "state_version", None)
+        if ctx.version is not None and version != ctx.version:
+            raise RuntimeError(
+                "WakeLoss.backward: the mesh has run other calls (another forward, or an adjoint) "
+                "since this loss's forward, so its state is no longer the one this gradient "
+                "belongs to; call backward before the next forward on the same mesh, or use "
+                "one mesh per pending loss")
         g = float(grad_out)
         dw = ctx.mesh.adjoint(g * ctx.coeff)
         w0 = np.asarray(ctx.beam["w"], dtype=np.float64)
         gb = np.bincount(ctx.bins, weights=w0 * dw, minlength=ctx.nbins)
-        return torch.from_numpy(gb).to(grad_out.dtype), None, None, None, None
+        return (torch.from_numpy(gb).to(device=grad_out.device, dtype=grad_out.dtype),
+                None, None, None, None)
 
 
 def xi_bins(beam: dict, cfg, nbins: int, lo: float, hi: float) -> np.ndarray:

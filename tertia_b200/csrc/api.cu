@@ -175,6 +175,7 @@ struct EngineBase {
     virtual qs_status pack_layer(double*, int64_t) = 0;
     virtual qs_status unpack_layer(const double*, int64_t) = 0;
     virtual qs_status clear_front_layer() = 0;
+    virtual qs_status get_charge_sums(double*, double*, double*) = 0;
 
     qs_status check_device() {
         cudaError_t e = cudaStreamSynchronize(st);
@@ -309,6 +310,29 @@ struct Engine : EngineBase {
     int64_t adj_kernels = 0;
     int64_t adj_np = 0, adj_nb = 0;
 
+    // FP64 charge sums (charge.cuh): weight tables c_k(ny), c_k(nz), the
+    // partial sums of the correctors (L x q_nparts x 2) and of the beam check
+    // ((L+1) x kBeamSumParts x 2), and the sums (L x 2 plasma, (L+1) x 2 beam)
+    double *q_cy = nullptr, *q_cz = nullptr, *q_part = nullptr, *qb_part = nullptr;
+    double* q_sums = nullptr;
+    int q_nparts = 0;
+
+    // FP32 attribution study of the FP64 engine (bitmask QS_FP32_STUDY, read
+    // at creation): one part of the march computed or stored in FP32 and the
+    // rest in FP64, to measure what each FP32 quantity adds to the error of
+    // the FP32 march
+    //    1  every transform through the FP32 FFT kernels
+    //    2  the spectral state carried from layer to layer (and the beam
+    //       spectra) rounded to float after each map
+    //    4  the plasma push and deposit through the FP32 push kernel (float
+    //       particle state, float fields and deposit)
+    //    8  the real field planes of each layer rounded to float
+    //   16  the beam currents rounded to float after the beam deposit
+    int fp32_study = 0;
+    DttFft* study_fft = nullptr;
+    float* study_f = nullptr;   // 40 planes: transform in / out / scratch, P and C fields, deposit
+    float* study_p = nullptr;   // 6 x np_cap particle values
+
     // the hand-off buffer assembled on the device, and its ordering scratch
     double* d_pack = nullptr;
     int* d_pack_i = nullptr;
@@ -322,12 +346,14 @@ struct Engine : EngineBase {
         if (adj_exec) cudaGraphExecDestroy(adj_exec);
         delete tcx;
         delete fftx;
+        delete study_fft;
         void* ptrs[] = {f3, b3, src3, splitbuf, srcbuf, Cbeam, sb3, bank, scratch, mats, onaxis_d,
                         stage, stage_d, pcell, py, pz, ppx, ppy, ppz, pw, bi, bj, bk, bx, by, bz,
                         bpx, bpy, bpz, bw, d_err, dens_dev, front_src, front_beam, ck, seg, lam, lam_pm, lam_sb, lam_b3,
                         d_dloss, d_gradw, acell, pid, apid, ay, az, apx, apy, apz, aw, cic_cnt,
                         cic_loff, cic_bsum, cic_bpref, cic_ticket, ck_cell, ck_id, seg_cell,
-                        adj_inv, lam_pos, adj_tmp, d_pack, d_pack_i};
+                        adj_inv, lam_pos, adj_tmp, d_pack, d_pack_i, q_cy, q_cz, q_part,
+                        qb_part, q_sums, study_f, study_p};
         for (void* p : ptrs)
             if (p) cudaFree(p);
         if (st) cudaStreamDestroy(st);
@@ -384,6 +410,31 @@ struct Engine : EngineBase {
         CK(cudaMemset(onaxis_d, 0, L * sizeof(T)));
         if ((s = alloc(&dens_dev, 1, "density"))) return s;
         if ((s = set_march_density())) return s;
+        // charge sums: one partial per corrector block (the largest grid of
+        // the corrector kernels: one block per z-mode row, 256 modes per block,
+        // or 256 mode pairs per row)
+        q_nparts = std::max(Mz, std::max((int)((plane + 255) / 256), ((My / 2 + 127) / 128) * Mz));
+        if ((s = alloc(&q_part, (size_t)L * 2 * q_nparts, "charge sums"))) return s;
+        CK(cudaMemset(q_part, 0, (size_t)L * 2 * q_nparts * sizeof(double)));
+        if ((s = alloc(&qb_part, (size_t)(L + 1) * 2 * kBeamSumParts, "charge sums"))) return s;
+        CK(cudaMemset(qb_part, 0, (size_t)(L + 1) * 2 * kBeamSumParts * sizeof(double)));
+        if ((s = alloc(&q_sums, (size_t)2 * L + 2 * (L + 1), "charge sums"))) return s;
+        CK(cudaMemset(q_sums, 0, ((size_t)2 * L + 2 * (L + 1)) * sizeof(double)));
+        {
+            // c_k(N) = (-1)^k / sin(pi (2k+1) / (4N)): the plane sum of the
+            // inverse REDFT11 basis function k
+            std::vector<double> cy(My), cz(Mz);
+            auto fillc = [](std::vector<double>& c, int N) {
+                for (int k = 0; k < N; k++)
+                    c[k] = (k % 2 ? -1.0 : 1.0) / std::sin(M_PI * (2.0 * k + 1.0) / (4.0 * N));
+            };
+            fillc(cy, My);
+            fillc(cz, Mz);
+            if ((s = alloc(&q_cy, (size_t)My, "charge sums"))) return s;
+            if ((s = alloc(&q_cz, (size_t)Mz, "charge sums"))) return s;
+            CK(cudaMemcpy(q_cy, cy.data(), My * sizeof(double), cudaMemcpyHostToDevice));
+            CK(cudaMemcpy(q_cz, cz.data(), Mz * sizeof(double), cudaMemcpyHostToDevice));
+        }
         // transform matrices 2 cos / 2 sin (pi (j+1/2)(k+1/2)/n); the angle is
         // reduced exactly in integers: (2j+1)(2k+1) mod 8n in units of pi/(4n)
         const size_t ny2 = (size_t)My * My, nz2 = (size_t)Mz * Mz;
@@ -414,6 +465,17 @@ struct Engine : EngineBase {
             fftx = DttFft::create(My, Mz);   // other sizes keep the FP32 matrix passes
             CK(cudaGetLastError());
         }
+        if (sizeof(T) == 8 && getenv("QS_FP32_STUDY")) {
+            fp32_study = atoi(getenv("QS_FP32_STUDY")) & 31;
+            if (fp32_study & 1) {
+                study_fft = DttFft::create(My, Mz);
+                CK(cudaGetLastError());
+                if (!study_fft)
+                    return fail(QS_ERR_UNSUPPORTED, "FP32 study: the FFT transforms need "
+                                                    "power-of-two ny, nz in [32, 2048]");
+            }
+            if ((s = alloc(&study_f, 40 * plane, "FP32 study"))) return s;
+        }
         Pf = splitbuf;
         Cf = splitbuf + 6 * plane;
         Psrc = srcbuf;
@@ -423,8 +485,96 @@ struct Engine : EngineBase {
         return QS_OK;
     }
 
+    // ------------------------------------------- the FP32 attribution study
+    // the job's transforms through the FP32 FFT kernels: inputs rounded to
+    // float, outputs widened back
+    void study_xform(const DttJob<T>& job) {
+        if constexpr (sizeof(T) == 8) {
+            float* fin = study_f;
+            float* fout = study_f + 8 * plane;
+            float* fscr = study_f + 16 * plane;
+            DttJob<float> jf;
+            jf.nf = job.nf;
+            jf.scale = (float)job.scale;
+            for (int f = 0; f < job.nf; f++) {
+                klaunch(KC_MISC, [&] {
+                    return launch_convert<float>(job.in[f], 1, fin + (size_t)f * plane, plane, st);
+                });
+                jf.in[f] = fin + (size_t)f * plane;
+                jf.out[f] = fout + (size_t)f * plane;
+                jf.kz[f] = job.kz[f];
+                jf.ky[f] = job.ky[f];
+            }
+            for (int pass = 0; pass < 2; pass++)
+                klaunch(KC_GEMM, [&] { return study_fft->run_pass(pass, jf, fscr, st); });
+            for (int f = 0; f < job.nf; f++)
+                klaunch(KC_MISC, [&] {
+                    return launch_convert_back<float>(fout + (size_t)f * plane, job.out[f], plane,
+                                                      st);
+                });
+        }
+    }
+    void study_round(T* x, size_t n, int bit) {
+        if constexpr (sizeof(T) == 8) {
+            if (fp32_study & bit) klaunch(KC_MISC, [&] { return launch_round_f32(x, n, st); });
+        }
+    }
+    // the push through the FP32 kernel on float copies of the particles and
+    // the P, C fields; its deposit is added to the double C sources
+    qs_status study_push(int full) {
+        if constexpr (sizeof(T) == 8) {
+            if (!clear_by_maps()) CK(cudaMemsetAsync(Csrc, 0, 4 * plane * sizeof(T), st));
+            if (!np) return QS_OK;
+            float* fP = study_f + 24 * plane;
+            float* fC = fP + 6 * plane;
+            float* fdep = fC + 6 * plane;
+            klaunch(KC_MISC, [&] { return launch_convert<float>(Pf, 1, fP, 6 * plane, st); });
+            klaunch(KC_MISC, [&] { return launch_convert<float>(Cf, 1, fC, 6 * plane, st); });
+            CK(cudaMemsetAsync(fdep, 0, 4 * plane * sizeof(float), st));
+            T* dsrc[6] = {py, pz, ppx, ppy, ppz, pw};
+            float* fp[6];
+            for (int c = 0; c < 6; c++) {
+                fp[c] = study_p + (size_t)c * np_cap;
+                klaunch(KC_MISC, [&] { return launch_convert<float>(dsrc[c], 1, fp[c], np, st); });
+            }
+            PushArgs<float> a{};
+            a.n = np;
+            a.My = My; a.Mz = Mz;
+            a.cell = pcell;
+            a.y = fp[0]; a.z = fp[1]; a.px = fp[2]; a.py = fp[3]; a.pz = fp[4]; a.w = fp[5];
+            a.P = fP; a.C = fC; a.dep = fdep;
+            a.cell_out = pcell;
+            a.dep_cell = nullptr;
+            a.plane = plane;
+            a.hx = (float)(cfg.hx / S); a.hy = (float)cfg.hy; a.hz = (float)cfg.hz;
+            a.q2m = (float)cfg.plasma_q2m;
+            a.djx0 = (float)cfg.plasma_djx0; a.djy0 = (float)cfg.plasma_djy0;
+            a.djz0 = (float)cfg.plasma_djz0; a.drho0 = (float)cfg.plasma_drho0;
+            a.bxe = (float)cfg.bx_ext; a.bye = (float)cfg.by_ext; a.bze = (float)cfg.bz_ext;
+            a.sE = (float)(cfg.plasma_q2m * (cfg.hx / S) / 2.0);
+            a.hxhy = (float)((cfg.hx / S) / cfg.hy);
+            a.hxhz = (float)((cfg.hx / S) / cfg.hz);
+            a.invMy = 1.0f / (float)My;
+            a.full = full;
+            a.err = d_err;
+            klaunch(KC_PUSH, [&] { return launch_push<float>(a, cfg.shape, true, st); });
+            klaunch(KC_MISC, [&] { return launch_add_widened(Csrc, fdep, 4 * plane, st); });
+            if (full)
+                for (int c = 0; c < 5; c++)
+                    klaunch(KC_MISC, [&] {
+                        return launch_convert_back<float>(fp[c], dsrc[c], np, st);
+                    });
+            CK(cudaGetLastError());
+        }
+        return QS_OK;
+    }
+
     // ---------------------------------------------------------- transforms
     void xform(const DttJob<T>& job) {
+        if (fp32_study & 1) {
+            study_xform(job);
+            return;
+        }
         if (tc) {
             for (int stage = 0; stage < 3; stage++)
                 klaunch(stage == 0 ? KC_SPLIT : KC_GEMM, [&] {
@@ -540,6 +690,11 @@ struct Engine : EngineBase {
             if ((s = alloc(&aw, n, "plasma"))) return s;
             if ((s = alloc(&pid, n, "plasma"))) return s;
             if ((s = alloc(&apid, n, "plasma"))) return s;
+        }
+        if (fp32_study & 4) {
+            if (study_p) cudaFree(study_p);
+            study_p = nullptr;
+            if ((s = alloc(&study_p, 6 * (size_t)n, "FP32 study"))) return s;
         }
         np_cap = n;
         if (gexec) {  // the captured march baked the old pointers
@@ -864,8 +1019,15 @@ struct Engine : EngineBase {
     }
 
     qs_status beam_spectra() {
-        klaunch(KC_BEAM_SPECTRA, [&] { return launch_beam_check<T>(b3, L + 1, plane, d_err, st); });
+        klaunch(KC_BEAM_SPECTRA, [&] {
+            return launch_beam_check<T>(b3, L + 1, plane, d_err, qb_part, st);
+        });
+        klaunch(KC_MISC, [&] {
+            return launch_charge_reduce(qb_part, kBeamSumParts, L + 1, 1.0, q_sums + 2 * (size_t)L,
+                                        st);
+        });
         batched_cc(b3, sb3, 2 * (L + 1), KC_GEMM);
+        study_round(sb3, (size_t)(L + 1) * 2 * plane, 2);
         CK(cudaGetLastError());
         sb3_valid = true;
         return QS_OK;
@@ -906,6 +1068,7 @@ struct Engine : EngineBase {
         a.err = d_err;
         klaunch(KC_BEAM_PUSH, [&] { return launch_beam_push<T>(a, st); });
         CK(cudaGetLastError());
+        study_round(b3, (size_t)(L + 1) * 2 * plane, 16);
         return beam_spectra();
     }
 
@@ -1006,6 +1169,7 @@ struct Engine : EngineBase {
     // the device part of MoveAllSplitLayers' set-up (capturable)
     qs_status begin_march_device() {
         if (src3) CK(cudaMemsetAsync(src3, 0, (size_t)(L + 1) * 4 * plane * sizeof(T), st));
+        CK(cudaMemsetAsync(q_part, 0, (size_t)L * 2 * q_nparts * sizeof(double), st));
         Psrc = srcbuf;
         Csrc = srcbuf + 4 * plane;
         CK(cudaMemsetAsync(srcbuf, 0, 8 * plane * sizeof(T), st));
@@ -1080,10 +1244,12 @@ struct Engine : EngineBase {
             SpecArgs<T> a = spec_args(iLayer, iSplit);
             a.zero_src = clear_by_maps() ? Csrc : nullptr;   // for the push that follows
             klaunch(KC_SPECTRAL, [&] { return launch_predictor<T>(a, st); });
+            study_round(bankp(cur, 0), (size_t)SP_RB * plane, 2);
         }
         // :946-967, :1004-1061: E, B into C (the predicted Rho and J planes are
         // cleared before any use by the push that follows)
         inverse_EB(false);
+        study_round(Cf, 6 * plane, 8);
         CK(cudaGetLastError());
         return QS_OK;
     }
@@ -1110,6 +1276,7 @@ struct Engine : EngineBase {
 
     qs_status push(int iLayer, int iSplit, int full) override {
         (void)iLayer; (void)iSplit;
+        if (fp32_study & 4) return study_push(full);
         // ClearCurrentsSplit: inside the march the preceding spectral kernel
         // already cleared Csrc
         if (!clear_by_maps()) CK(cudaMemsetAsync(Csrc, 0, 4 * plane * sizeof(T), st));
@@ -1189,6 +1356,7 @@ struct Engine : EngineBase {
                 SpecArgs<T> a = spec_args(iLayer, iSplit);
                 a.write_b = 0;
                 a.zero_src = (clear_by_maps() && iter >= 0) ? Csrc : nullptr;
+                charge_args(a, iLayer, iSplit, iter);
                 const int nout = want_rho ? 7 : 6;
                 klaunch(KC_SPECTRAL, [&] {
                     return fftx->run_spectral_rows(a, true, scratch, scratch, nout, st);
@@ -1204,11 +1372,14 @@ struct Engine : EngineBase {
             }
             SpecArgs<T> a = spec_args(iLayer, iSplit);
             a.split_rho = want_rho ? 1 : 0;
+            charge_args(a, iLayer, iSplit, iter);
             // a push follows every Iterate but the last: clear its deposit planes
             // (the forward J transform above has consumed them)
             a.zero_src = (clear_by_maps() && iter >= 0) ? Csrc : nullptr;
             klaunch(KC_SPECTRAL, [&] { return launch_corrector<T>(a, st); });
+            study_round(bankp(cb, 0), (size_t)SP_RB * plane, 2);
             inverse_EB(want_rho);
+            study_round(Cf, 6 * plane, 8);
             CK(cudaGetLastError());
         }
         if (rel_err) {
@@ -1224,6 +1395,34 @@ struct Engine : EngineBase {
             }
             *rel_err = std::max(std::max(df[0] / mx[0], df[1] / mx[1]), df[2] / mx[2]);
         }
+        return QS_OK;
+    }
+
+    // the last corrector of a layer writes its FP64 charge partials (not while
+    // the adjoint recomputes a segment: the march's sums stand)
+    void charge_args(SpecArgs<T>& a, int iLayer, int iSplit, int iter) {
+        if (iter >= 0 || iSplit != S - 1 || adj_recompute) return;
+        a.qsum = q_part + (size_t)iLayer * 2 * q_nparts;
+        a.qcy = q_cy;
+        a.qcz = q_cz;
+    }
+
+    qs_status get_charge_sums(double* rho, double* jx, double* rho_beam) override {
+        // the plasma sums of the layers marched so far (the march also runs
+        // this reduction at its end)
+        klaunch(KC_MISC, [&] {
+            return launch_charge_reduce(q_part, q_nparts, L, 1.0 / (4.0 * My * Mz), q_sums, st);
+        });
+        std::vector<double> h((size_t)2 * L + 2 * (L + 1));
+        CK(cudaMemcpyAsync(h.data(), q_sums, h.size() * sizeof(double), cudaMemcpyDeviceToHost,
+                           st));
+        CK(cudaStreamSynchronize(st));
+        for (int i = 0; i < L; i++) {
+            if (rho) rho[i] = h[2 * (size_t)i];
+            if (jx) jx[i] = h[2 * (size_t)i + 1];
+        }
+        if (rho_beam)
+            for (int i = 0; i <= L; i++) rho_beam[i] = h[2 * (size_t)L + 2 * (size_t)i];
         return QS_OK;
     }
 
@@ -1271,6 +1470,9 @@ struct Engine : EngineBase {
         klaunch(KC_MISC, [&] {
             return launch_onaxis<T>(f3, L, plane, (size_t)(My / 2) + (size_t)My * (Mz / 2), onaxis_d,
                                     st);
+        });
+        klaunch(KC_MISC, [&] {
+            return launch_charge_reduce(q_part, q_nparts, L, 1.0 / (4.0 * My * Mz), q_sums, st);
         });
         return QS_OK;
     }
@@ -2310,6 +2512,11 @@ qs_status qs_get_onaxis_ex(qs_handle* h, double* out) {
     H_OR_INVALID(h);
     return E->get_onaxis(out);
 }
+qs_status qs_get_charge_sums(qs_handle* h, double* rho, double* jx, double* rho_beam) {
+    H_OR_INVALID(h);
+    return E->get_charge_sums(rho, jx, rho_beam);
+}
+
 qs_status qs_get_psi(qs_handle* h, double* out) {
     H_OR_INVALID(h);
     if (!out) return QS_ERR_INVALID;

@@ -29,6 +29,7 @@
 #include "pdl.cuh"
 #include "spectral_f32.cuh"
 #include "adjoint_maps.cuh"
+#include "charge.cuh"
 
 namespace qs {
 namespace fft {
@@ -590,6 +591,7 @@ __global__ void __launch_bounds__(spec_threads<M>()) spectral_rows_kernel(SpecAr
         __syncthreads();
     }
     // the maps on the row's modes, two per thread
+    double qr = 0.0, qj = 0.0;   // FP64 charge sums (charge.cuh)
     for (int pj = threadIdx.x; pj < M; pj += NT) {
         const int j = 2 * pj;
         const size_t n = (size_t)j + (size_t)N * k;
@@ -602,6 +604,11 @@ __global__ void __launch_bounds__(spec_threads<M>()) spectral_rows_kernel(SpecAr
             st2(const_cast<float*>(a.Jy), n, jy2.x, jy2.y);
             st2(const_cast<float*>(a.Jz), n, jz2.x, jz2.y);
             o = corrector_modes2(a, j, k, n, jx2, jy2, jz2);
+            if (a.qsum) {
+                const double c0 = a.qcy[j], c1 = a.qcy[j + 1];
+                qr += (double)o.rho[0] * c0 + (double)o.rho[1] * c1;
+                qj += (double)jx2.x * c0 + (double)jx2.y * c1;
+            }
         } else {
             o = predictor_modes2(a, j, k, n);
         }
@@ -613,6 +620,10 @@ __global__ void __launch_bounds__(spec_threads<M>()) spectral_rows_kernel(SpecAr
         *reinterpret_cast<float2*>(EB + 4 * N + j) = make_float2(o.by[0], o.by[1]);
         *reinterpret_cast<float2*>(EB + 5 * N + j) = make_float2(o.bz[0], o.bz[1]);
         *reinterpret_cast<float2*>(EB + 6 * N + j) = make_float2(o.rho[0], o.rho[1]);
+    }
+    if (CORRECT && a.qsum) {
+        const double cz = a.qcz[k];
+        charge_block_sum(qr * cz, qj * cz, a.qsum + 2 * (size_t)k);
     }
     __syncthreads();
     pdl_trigger();

@@ -17,14 +17,19 @@
 //
 // In host code g_noalloc_scratch is only a host-side stand-in for the device
 // array, not a device address: the device address is looked up with
-// cudaGetSymbolAddress, once per device, with that device current, on the
-// first call made on that device.  Every call on a device shares the one
+// cudaGetSymbolAddress, with the device current, on the first call made on a
+// device, and again only when the device's context has changed since (a
+// cudaDeviceReset between calls makes the runtime load the module, and so the
+// array, afresh).  A CUDA error that is already pending on the calling thread
+// when the call starts belongs to the caller: the call reports it without
+// clearing it and does nothing.  Every call on a device shares the one
 // array, and the array keeps whatever the last call left in it.  Nothing in it
 // needs to start at zero: each call writes every element it later reads
 // (both matrices, then the whole intermediate plane of each batch plane).
 // Calls whose GPU work overlaps (two streams, or two host threads on one
 // device) race on the array and give wrong results; callers must order them.
-#include <cuda_runtime.h>
+#include <cuda.h>            // CUcontext / CUresult types only: the driver calls are
+#include <cuda_runtime.h>    // fetched through cudaGetDriverEntryPointByVersion
 
 #include <mutex>
 #include <string>
@@ -46,7 +51,35 @@ constexpr int kMaxDevices = 64;
 static __device__ __align__(256) double g_noalloc_scratch[kScratchDoubles];
 
 std::mutex g_setup_mu;
-double* g_scratch_dev[kMaxDevices] = {};   // device address per device ordinal
+double* g_scratch_dev[kMaxDevices] = {};          // device address per device ordinal
+unsigned long long g_scratch_ctx[kMaxDevices] = {};   // id of the context it was looked up in
+
+typedef CUresult (*CtxGetCurrentFn)(CUcontext*);
+typedef CUresult (*CtxGetIdFn)(CUcontext, unsigned long long*);
+
+// unique id of the calling thread's current context (0 when it cannot be read)
+unsigned long long current_context_id() {
+    static CtxGetCurrentFn get_cur = nullptr;
+    static CtxGetIdFn get_id = nullptr;
+    static bool looked_up = false;
+    if (!looked_up) {   // under g_setup_mu
+        looked_up = true;
+        cudaDriverEntryPointQueryResult q1, q2;
+        if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", (void**)&get_cur, 12000,
+                                             cudaEnableDefault, &q1) != cudaSuccess ||
+            q1 != cudaDriverEntryPointSuccess)
+            get_cur = nullptr;
+        if (cudaGetDriverEntryPointByVersion("cuCtxGetId", (void**)&get_id, 12000,
+                                             cudaEnableDefault, &q2) != cudaSuccess ||
+            q2 != cudaDriverEntryPointSuccess)
+            get_id = nullptr;
+    }
+    CUcontext ctx = nullptr;
+    unsigned long long id = 0;
+    if (get_cur && get_id && get_cur(&ctx) == CUDA_SUCCESS && ctx && get_id(ctx, &id) == CUDA_SUCCESS)
+        return id;
+    return 0;
+}
 
 // 2 cos / 2 sin (pi (j+1/2)(k+1/2) / n), angle reduced exactly in integers:
 // (2j+1)(2k+1) mod 8n in units of pi/(4n) (the same table the handle builds)
@@ -72,12 +105,16 @@ qs_status scratch_on_current_device(double** out) {
     if (e != cudaSuccess) return fail(QS_ERR_CUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
     if (dev < 0 || dev >= kMaxDevices) return fail(QS_ERR_DEVICE, "device ordinal out of range");
     std::lock_guard<std::mutex> lock(g_setup_mu);
-    if (!g_scratch_dev[dev]) {
+    // look the address up again when the current context is not the one it
+    // was found in (or cannot be identified: 0)
+    const unsigned long long ctx = current_context_id();
+    if (!g_scratch_dev[dev] || ctx == 0 || ctx != g_scratch_ctx[dev]) {
         double* p = nullptr;
         e = cudaGetSymbolAddress((void**)&p, g_noalloc_scratch);
         if (e != cudaSuccess || !p)
             return fail(QS_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
         g_scratch_dev[dev] = p;
+        g_scratch_ctx[dev] = current_context_id();   // the lookup made the context current
     }
     *out = g_scratch_dev[dev];
     return QS_OK;
@@ -102,6 +139,15 @@ extern "C" qs_status qs_transform2d_noalloc(int kind_z, int kind_y, int ny, int 
     if (batch < 0) return fail(QS_ERR_INVALID, "batch must be >= 0");
     if (batch == 0) return QS_OK;
     if (!d_in || !d_out) return fail(QS_ERR_INVALID, "null plane pointer");
+    {
+        // an error left by the caller's own earlier CUDA work stays the
+        // caller's: report it, leave it in place, launch nothing
+        const cudaError_t pending = cudaPeekAtLastError();
+        if (pending != cudaSuccess)
+            return fail(QS_ERR_CUDA, std::string("a CUDA error was already pending on this thread "
+                                                 "before the call (left in place): ") +
+                                         cudaGetErrorString(pending));
+    }
     double* scratch = nullptr;
     qs_status s = scratch_on_current_device(&scratch);
     if (s) return s;

@@ -34,6 +34,10 @@ struct SpecArgs {
     // optional: 4 planes (the C-layer deposit) cleared by the kernel for the
     // push that follows it (ClearCurrentsSplit without a separate memset)
     T* zero_src;
+    // optional (correctors): FP64 charge sums (charge.cuh); each block writes
+    // its partial sums of rho c_ky c_kz and Jx c_ky c_kz to qsum[2 * block]
+    double* qsum;
+    const double *qcy, *qcz;   // c_k(ny), c_k(nz)
 };
 
 template <class T>
@@ -49,9 +53,17 @@ int launch_corrector_fast(const SpecArgs<float>& a, cudaStream_t st);
 template <class T>
 int launch_beam_layer(const T* cur, const T* nxt, int S, int s, T* out, size_t plane, int* err,
                       cudaStream_t st);
-// |JxBeam| > 10 anywhere in the beam-current store (layers x [RhoBeam, JxBeam])
+// |JxBeam| > 10 anywhere in the beam-current store (layers x [RhoBeam, JxBeam]),
+// and the FP64 partial sums of each layer's RhoBeam: part[2 * (layer *
+// kBeamSumParts + b)] for the kBeamSumParts blocks b of a layer
+constexpr int kBeamSumParts = 32;
 template <class T>
-int launch_beam_check(const T* b3, int nlayers, size_t plane, int* err, cudaStream_t st);
+int launch_beam_check(const T* b3, int nlayers, size_t plane, int* err, double* part,
+                      cudaStream_t st);
+// out[layer * 2 + q] = scale * sum over p < nparts of part[2 * (layer * nparts + p) + q]
+// (q = 0, 1; in index order)
+int launch_charge_reduce(const double* part, int nparts, int nlayers, double scale, double* out,
+                         cudaStream_t st);
 
 template <class T>
 int launch_onaxis(const T* fields3d, int L, size_t plane, size_t idx, T* out, cudaStream_t st);
@@ -78,6 +90,10 @@ int launch_set_value(T* dst, T v, cudaStream_t st);
 
 template <class T>
 int launch_convert(const void* src, int src_is_double, T* dst, size_t n, cudaStream_t st);
+// x = (double)(float)x over n values (the FP32 attribution study)
+int launch_round_f32(double* x, size_t n, cudaStream_t st);
+// dst += (double)src over n values
+int launch_add_widened(double* dst, const float* src, size_t n, cudaStream_t st);
 template <class T>
 int launch_convert_back(const T* src, double* dst, size_t n, cudaStream_t st);
 

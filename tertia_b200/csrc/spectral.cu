@@ -18,6 +18,7 @@
 #include "qs_internal.h"
 #include "split.cuh"
 #include "density.cuh"
+#include "charge.cuh"
 
 namespace qs {
 
@@ -85,10 +86,22 @@ __global__ void predictor_kernel(SpecArgs<T> a) {
 }
 
 template <class T>
+__device__ __forceinline__ void corrector_mode(const SpecArgs<T>& a, int n1, double& qr,
+                                               double& qj);
+
+template <class T>
 __global__ void corrector_kernel(SpecArgs<T> a) {
     const int n1 = blockIdx.x * blockDim.x + threadIdx.x;
     const int N = a.ny * a.nz;
-    if (n1 >= N) return;
+    double qr = 0.0, qj = 0.0;
+    if (n1 < N) corrector_mode(a, n1, qr, qj);
+    if (a.qsum) charge_block_sum(qr, qj, a.qsum + 2 * (size_t)blockIdx.x);
+}
+
+template <class T>
+__device__ __forceinline__ void corrector_mode(const SpecArgs<T>& a, int n1, double& qr,
+                                               double& qj) {
+    const int N = a.ny * a.nz;
     const int j = n1 % a.ny, k = n1 / a.ny;
     const T d = *a.dens_p, hx = a.hx;
     const T akz = a.piZ * (T(k) + T(0.5));
@@ -111,6 +124,11 @@ __global__ void corrector_kernel(SpecArgs<T> a) {
     a.Ez[n1] = newEz;
     a.Rho[n1] = rho;
     a.Ex[n1] = newEx;
+    if (a.qsum) {
+        const double c = a.qcy[j] * a.qcz[k];
+        qr = (double)rho * c;
+        qj = (double)jx * c;
+    }
     if (a.zero_src)
         for (int q = 0; q < 4; q++) a.zero_src[(size_t)q * N + n1] = T(0);
     if (a.write_b) {
@@ -176,18 +194,48 @@ int launch_beam_layer(const T* cur, const T* nxt, int S, int s, T* out, size_t p
     return 1;
 }
 
+// kBeamSumParts blocks per layer (blockIdx.y): the |JxBeam| > 10 check of
+// :618-621 and the block's FP64 partial sum of RhoBeam
 template <class T>
-__global__ void beam_check_kernel(const T* __restrict__ b3, int nlayers, size_t plane, int* err) {
-    const size_t n = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+__global__ void __launch_bounds__(256) beam_check_kernel(const T* __restrict__ b3, int nlayers,
+                                                         size_t plane, int* err, double* part) {
     const int i = blockIdx.y;
-    if (n >= plane || i >= nlayers) return;
-    if (fabs((double)b3[((size_t)i * 2 + 1) * plane + n]) > 10.0) atomicOr(err, DEV_ERR_BEAM_CURRENT);
+    const T* rb = b3 + (size_t)i * 2 * plane;
+    const T* jxb = rb + plane;
+    double s = 0.0;
+    bool bad = false;
+    for (size_t n = (size_t)blockIdx.x * blockDim.x + threadIdx.x; n < plane;
+         n += (size_t)gridDim.x * blockDim.x) {
+        s += (double)rb[n];
+        bad |= fabs((double)jxb[n]) > 10.0;
+    }
+    if (bad) atomicOr(err, DEV_ERR_BEAM_CURRENT);
+    charge_block_sum(s, 0.0, part + 2 * ((size_t)i * gridDim.x + blockIdx.x));
 }
 
 template <class T>
-int launch_beam_check(const T* b3, int nlayers, size_t plane, int* err, cudaStream_t st) {
-    dim3 g((unsigned)((plane + 255) / 256), nlayers);
-    beam_check_kernel<T><<<g, 256, 0, st>>>(b3, nlayers, plane, err);
+int launch_beam_check(const T* b3, int nlayers, size_t plane, int* err, double* part,
+                      cudaStream_t st) {
+    dim3 g((unsigned)kBeamSumParts, nlayers);
+    beam_check_kernel<T><<<g, 256, 0, st>>>(b3, nlayers, plane, err, part);
+    return 1;
+}
+
+__global__ void charge_reduce_kernel(const double* __restrict__ part, int nparts, int nlayers,
+                                     double scale, double* __restrict__ out) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= 2 * nlayers) return;
+    const int layer = t >> 1, q = t & 1;
+    const double* p = part + 2 * (size_t)layer * nparts + q;
+    double s = 0.0;
+    for (int i = 0; i < nparts; i++) s += p[2 * (size_t)i];
+    out[t] = scale * s;
+}
+
+int launch_charge_reduce(const double* part, int nparts, int nlayers, double scale, double* out,
+                         cudaStream_t st) {
+    charge_reduce_kernel<<<(2 * nlayers + 127) / 128, 128, 0, st>>>(part, nparts, nlayers, scale,
+                                                                   out);
     return 1;
 }
 
@@ -311,13 +359,34 @@ int launch_convert_back(const T* src, double* dst, size_t n, cudaStream_t st) {
     return 1;
 }
 
+// ---- the FP32 attribution study of the FP64 engine (see api.cu)
+__global__ void round_f32_kernel(double* __restrict__ x, size_t n) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) x[i] = (double)(float)x[i];
+}
+int launch_round_f32(double* x, size_t n, cudaStream_t st) {
+    if (!n) return 0;
+    round_f32_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(x, n);
+    return 1;
+}
+__global__ void add_widened_kernel(double* __restrict__ dst, const float* __restrict__ src,
+                                   size_t n) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) dst[i] += (double)src[i];
+}
+int launch_add_widened(double* dst, const float* src, size_t n, cudaStream_t st) {
+    if (!n) return 0;
+    add_widened_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(dst, src, n);
+    return 1;
+}
+
 #define QS_INST(T)                                                                              \
     template int launch_predictor<T>(const SpecArgs<T>&, cudaStream_t);                         \
     template int launch_corrector<T>(const SpecArgs<T>&, cudaStream_t);                         \
     template int launch_beam_layer<T>(const T*, const T*, int, int, T*, size_t, int*,           \
                                       cudaStream_t);                                            \
     template int launch_onaxis<T>(const T*, int, size_t, size_t, T*, cudaStream_t);            \
-    template int launch_beam_check<T>(const T*, int, size_t, int*, cudaStream_t);              \
+    template int launch_beam_check<T>(const T*, int, size_t, int*, double*, cudaStream_t);     \
     template int launch_seed_front<T>(const SeedFront&, int32_t*, T*, T*, T*, T*, T*, T*,       \
                                       cudaStream_t);                                            \
     template int launch_set_value<T>(T*, T, cudaStream_t);                                      \

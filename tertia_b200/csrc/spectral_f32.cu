@@ -10,6 +10,7 @@
 #include "split.cuh"
 #include "pdl.cuh"
 #include "spectral_f32.cuh"
+#include "charge.cuh"
 
 namespace qs {
 namespace {
@@ -63,19 +64,29 @@ template <int KIND, int NSPLIT>
 __global__ void __launch_bounds__(kThreads) corrector_f32_kernel(SpecArgs<float> a) {
     const int j = 2 * (blockIdx.x * kThreads + threadIdx.x);
     const int k = blockIdx.y;
-    if (j >= a.ny) return;
+    double qr = 0.0, qj = 0.0;
     pdl_wait();
-    const size_t n = (size_t)j + (size_t)a.ny * k;
-    const Modes2 o = corrector_modes2(a, j, k, n, ld2(a.Jx, n), ld2(a.Jy, n), ld2(a.Jz, n));
-    pdl_trigger();
-    store_modes2(a, n, o);
-    put_split2<KIND, NSPLIT>(a, 0, n, o.ex[0], o.ex[1]);
-    put_split2<KIND, NSPLIT>(a, 1, n, o.ey[0], o.ey[1]);
-    put_split2<KIND, NSPLIT>(a, 2, n, o.ez[0], o.ez[1]);
-    put_split2<KIND, NSPLIT>(a, 3, n, o.bx[0], o.bx[1]);
-    put_split2<KIND, NSPLIT>(a, 4, n, o.by[0], o.by[1]);
-    put_split2<KIND, NSPLIT>(a, 5, n, o.bz[0], o.bz[1]);
-    if (NSPLIT > 0 && a.split_rho) put_split2<KIND, NSPLIT>(a, 6, n, o.rho[0], o.rho[1]);
+    if (j < a.ny) {
+        const size_t n = (size_t)j + (size_t)a.ny * k;
+        const float2 jx2 = ld2(a.Jx, n);
+        const Modes2 o = corrector_modes2(a, j, k, n, jx2, ld2(a.Jy, n), ld2(a.Jz, n));
+        pdl_trigger();
+        store_modes2(a, n, o);
+        put_split2<KIND, NSPLIT>(a, 0, n, o.ex[0], o.ex[1]);
+        put_split2<KIND, NSPLIT>(a, 1, n, o.ey[0], o.ey[1]);
+        put_split2<KIND, NSPLIT>(a, 2, n, o.ez[0], o.ez[1]);
+        put_split2<KIND, NSPLIT>(a, 3, n, o.bx[0], o.bx[1]);
+        put_split2<KIND, NSPLIT>(a, 4, n, o.by[0], o.by[1]);
+        put_split2<KIND, NSPLIT>(a, 5, n, o.bz[0], o.bz[1]);
+        if (NSPLIT > 0 && a.split_rho) put_split2<KIND, NSPLIT>(a, 6, n, o.rho[0], o.rho[1]);
+        if (a.qsum) {
+            const double cz = a.qcz[k], c0 = a.qcy[j] * cz, c1 = a.qcy[j + 1] * cz;
+            qr = (double)o.rho[0] * c0 + (double)o.rho[1] * c1;
+            qj = (double)jx2.x * c0 + (double)jx2.y * c1;
+        }
+    }
+    if (a.qsum)
+        charge_block_sum(qr, qj, a.qsum + 2 * ((size_t)blockIdx.y * gridDim.x + blockIdx.x));
 }
 
 // (kind, nsplit) of the operand; -1 when there is none or it is not handled

@@ -10,6 +10,7 @@ All arrays are host numpy arrays; the device copies live in the handle.
 from __future__ import annotations
 
 import ctypes as C
+import functools
 
 import numpy as np
 
@@ -29,6 +30,17 @@ def _i32(a):
     return np.ascontiguousarray(a, dtype=np.int32)
 
 
+def _changes_state(f):
+    """Count the calls that change the box's state (beam, plasma, fields,
+    checkpoints): `Mesh.state_version` lets a caller that kept results of an
+    earlier call (the autograd wrapper) see that the mesh has moved on."""
+    @functools.wraps(f)
+    def g(self, *a, **k):
+        self.state_version += 1
+        return f(self, *a, **k)
+    return g
+
+
 class Mesh:
     """One quasi-static box on one GPU (a qs_handle)."""
 
@@ -41,6 +53,7 @@ class Mesh:
             raise QsError(st, self._L.qs_last_error(None).decode())
         self._h = h
         self.plane = cfg.ny * cfg.nz
+        self.state_version = 0
 
     # -------------------------------------------------------------- plumbing
     def _chk(self, st: int, what: str):
@@ -88,6 +101,7 @@ class Mesh:
         return {k: (float(ms[i]), int(cnt[i])) for i, k in enumerate(abi.KERNEL_CLASSES)}
 
     # -------------------------------------------------------------- state
+    @_changes_state
     def load_beam(self, b: dict):
         n = len(b["x"])
         ii, jj, kk = (_i32(b[k]) for k in "ijk")
@@ -106,6 +120,7 @@ class Mesh:
                   "qs_get_beam")
         return out
 
+    @_changes_state
     def load_front_plasma(self, p: dict):
         n = len(p["y"])
         cell = _i32(p["cell"])
@@ -114,9 +129,11 @@ class Mesh:
                                                *[_p(a, C.c_double) for a in f]),
                   "qs_load_front_plasma")
 
+    @_changes_state
     def seed_front_plasma(self, step: int):
         self._chk(self._L.qs_seed_front_plasma(self._h, int(step)), "qs_seed_front_plasma")
 
+    @_changes_state
     def set_density_profile(self, prof):
         """Specie density profile (abi.QsDensityProfile, or None for the
         uniform cfg.plasma_density)."""
@@ -128,6 +145,7 @@ class Mesh:
         self._chk(self._L.qs_plasma_density(self._h, x, y, z, C.byref(out)), "qs_plasma_density")
         return out.value
 
+    @_changes_state
     def set_phase(self, phase: float):
         self._chk(self._L.qs_set_phase(self._h, float(phase)), "qs_set_phase")
 
@@ -153,11 +171,13 @@ class Mesh:
         self._chk(self._L.qs_pack_layer(self._h, _p(out, C.c_double), n), "qs_pack_layer")
         return out
 
+    @_changes_state
     def unpack_layer(self, buf):
         """UnpackLayer: the received layer is the front of the next march."""
         b = _f64(buf)
         self._chk(self._L.qs_unpack_layer(self._h, _p(b, C.c_double), b.size), "qs_unpack_layer")
 
+    @_changes_state
     def clear_front_layer(self):
         self._chk(self._L.qs_clear_front_layer(self._h), "qs_clear_front_layer")
 
@@ -176,6 +196,7 @@ class Mesh:
     def _shape(self, a):
         return a.reshape(self.cfg.nz, self.cfg.ny)
 
+    @_changes_state
     def set_layer(self, which: int, field: int, data):
         d = _f64(data).reshape(-1)
         self._chk(self._L.qs_set_layer(self._h, which, field, _p(d, C.c_double)), "qs_set_layer")
@@ -191,6 +212,7 @@ class Mesh:
                   "qs_get_field3d")
         return self._shape(out)
 
+    @_changes_state
     def set_beam_currents(self, field: int, layer: int, data):
         d = _f64(data).reshape(-1)
         self._chk(self._L.qs_set_beam_currents(self._h, field, layer, _p(d, C.c_double)),
@@ -212,37 +234,56 @@ class Mesh:
         self._chk(self._L.qs_get_psi(self._h, _p(out, C.c_double)), "qs_get_psi")
         return out
 
+    def charge_sums(self) -> dict:
+        """FP64 per-layer sums over the transverse plane (qs_get_charge_sums):
+        rho (nx) of the corrected density, jx (nx) of the full push's Jx
+        deposit, rho_beam (nx + 1) of the beam's RhoBeam."""
+        r, j, b = np.empty(self.cfg.nx), np.empty(self.cfg.nx), np.empty(self.cfg.nx + 1)
+        self._chk(self._L.qs_get_charge_sums(self._h, _p(r, C.c_double), _p(j, C.c_double),
+                                             _p(b, C.c_double)), "qs_get_charge_sums")
+        return {"rho": r, "jx": j, "rho_beam": b}
+
     # -------------------------------------------------------------- the path
+    @_changes_state
     def step(self):
         self._chk(self._L.qs_step(self._h), "qs_step")
 
+    @_changes_state
     def move_beam_particles(self):
         self._chk(self._L.qs_move_beam_particles(self._h), "qs_move_beam_particles")
 
+    @_changes_state
     def move_all_split_layers(self):
         self._chk(self._L.qs_move_all_split_layers(self._h), "qs_move_all_split_layers")
 
+    @_changes_state
     def begin_march(self):
         self._chk(self._L.qs_begin_march(self._h), "qs_begin_march")
 
+    @_changes_state
     def layer_begin(self, i: int, s: int = 0):
         self._chk(self._L.qs_layer_begin(self._h, i, s), "qs_layer_begin")
 
+    @_changes_state
     def move_split_layer(self, i: int, s: int = 0):
         self._chk(self._L.qs_move_split_layer(self._h, i, s), "qs_move_split_layer")
 
+    @_changes_state
     def guess_fields(self, i: int, s: int = 0):
         self._chk(self._L.qs_guess_fields(self._h, i, s), "qs_guess_fields")
 
+    @_changes_state
     def move_particles_layer(self, i: int, s: int, full: int):
         self._chk(self._L.qs_move_particles_layer(self._h, i, s, int(full)),
                   "qs_move_particles_layer")
 
+    @_changes_state
     def iterate_fields(self, i: int, s: int, it: int) -> float:
         e = C.c_double(0.0)
         self._chk(self._L.qs_iterate_fields(self._h, i, s, it, C.byref(e)), "qs_iterate_fields")
         return e.value
 
+    @_changes_state
     def layer_end(self, i: int, s: int = 0):
         self._chk(self._L.qs_layer_end(self._h, i, s), "qs_layer_end")
 
@@ -263,6 +304,7 @@ class Mesh:
         self._chk(self._L.qs_transform2d_dev(self._h, kind_z, kind_y, batch, C.c_void_p(d_in),
                                              C.c_void_p(d_out)), "qs_transform2d_dev")
 
+    @_changes_state
     def step_host(self, b: dict, want_beam: bool = True, out: dict | None = None):
         """One step through host buffers (beam in, beam and on-axis Ex out).
         `out` may supply the output arrays (e.g. views of pinned memory)."""
@@ -283,10 +325,12 @@ class Mesh:
         return (out if want_beam else None), ex
 
     # -------------------------------------------------------------- adjoint
+    @_changes_state
     def adjoint_checkpoints(self, every: int):
         """Store layer checkpoints every `every` layers in the next marches."""
         self._chk(self._L.qs_adjoint_checkpoints(self._h, int(every)), "qs_adjoint_checkpoints")
 
+    @_changes_state
     def adjoint(self, dloss_donaxis_ex) -> np.ndarray:
         """d loss / d (beam weight) of every beam particle, given d loss / d
         (on-axis Ex of each layer) for the last march."""

@@ -143,3 +143,21 @@ def test_cic_adjoint_checkpoint_interval_fp32():
         out.append(adjoint_grad(m, beam, bins, coeff, beta))
         m.close()
     assert rel(out[0], out[1]) < 1e-5
+
+
+def test_wake_loss_with_bin_weights_on_the_gpu():
+    """Bin weights that live on the GPU get their gradient on the GPU, equal
+    to the gradient of the same weights on the host; a second forward on the
+    mesh before the first loss's backward is refused."""
+    cfg, m, beam, bins, coeff = setup("fp64", layers=24)
+    beta = np.random.default_rng(8).uniform(0.5, 1.5, NBINS)
+    g_host = adjoint_grad(m, beam, bins, coeff, beta)
+    t = torch.tensor(beta, dtype=torch.float64, device="cuda", requires_grad=True)
+    wake_loss(t, m, beam, bins, coeff).backward()
+    assert t.grad.device.type == "cuda"
+    assert rel(t.grad.cpu().numpy(), g_host) < 1e-12
+    l1 = wake_loss(t, m, beam, bins, coeff)
+    wake_loss(t.detach(), m, beam, bins, coeff)
+    with pytest.raises(RuntimeError, match="state is no longer"):
+        l1.backward()
+    m.close()

@@ -69,3 +69,32 @@ def test_noalloc_rejects_sizes_beyond_its_scratch():
         assert "qs_transform2d_noalloc" in msg
         if ny > 512 or nz > 512:
             assert "512" in msg
+
+
+def test_noalloc_two_calls_queued_on_a_side_stream():
+    """Two calls of different sizes and kinds enqueued back to back on one
+    non-default stream with no synchronisation between them: the second
+    call's matrix set-up is ordered after the first call's transforms by the
+    stream, so both outputs match the handle transform."""
+    import torch
+    from tertia_b200.abi import load_library
+    L = load_library()
+    torch.cuda.set_device(0)
+    side = torch.cuda.Stream()
+    cases = [(128, 64, 0, 1, 2), (64, 256, 1, 1, 3)]
+    xs, outs = [], []
+    for ny, nz, kz, ky, batch in cases:
+        rng = np.random.default_rng(7 * ny + nz + ky)
+        xs.append(torch.from_numpy(rng.standard_normal((batch, nz, ny))).cuda())
+        outs.append(torch.full_like(xs[-1], float("nan")))
+    torch.cuda.synchronize()
+    for (ny, nz, kz, ky, batch), x, out in zip(cases, xs, outs):
+        st = L.qs_transform2d_noalloc(kz, ky, ny, nz, batch, C.c_void_p(x.data_ptr()),
+                                      C.c_void_p(out.data_ptr()), C.c_void_p(side.cuda_stream))
+        assert st == 0, L.qs_last_error(None).decode()
+    side.synchronize()
+    for (ny, nz, kz, ky, batch), x, out in zip(cases, xs, outs):
+        want = handle_transform(L, ny, nz, kz, ky, x, torch).cpu().numpy()
+        got = out.cpu().numpy()
+        assert np.isfinite(got).all()
+        assert rel_l2(got, want) < TOL, (ny, nz, kz, ky)
