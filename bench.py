@@ -59,6 +59,8 @@ def parse():
     ap.add_argument("--no-adjoint", action="store_true", help="skip the c3 adjoint measurement")
     ap.add_argument("--no-next", action="store_true",
                     help="skip the density-profile march and hand-off measurements")
+    ap.add_argument("--no-c2", action="store_true", help="skip the c2 precision study")
+    ap.add_argument("--no-c4", action="store_true", help="skip the c4 full-form measurement")
     ap.add_argument("--cpu-seconds", type=float, default=12.0,
                     help="target seconds of the bounded CPU sample")
     return ap.parse_args()
@@ -296,6 +298,321 @@ def adjoint_measure(precision: str):
             "fd_step": h, "loss_note": "loss = sum over window layers of hx * on-axis Ex",
             "timing": "forward: device events around the march; adjoint: host wall clock "
                       "around qs_adjoint (it synchronises)"}
+
+
+# ------------------------------------------------------------------ FP64 comparison
+STUDY_BITS = (("transforms", 1), ("spectral_state", 2), ("push", 4), ("fields", 8),
+              ("beam_currents", 16), ("all", 31))
+
+
+def fp64_compare(cfg, beam, pushes_per_step, ours_ms):
+    import numpy as np
+    import torch
+    from tertia_b200.abi import PRECISIONS
+    from tertia_b200.mesh import Mesh
+
+    def run(prec, eps=0.0, study=None):
+        c = cfg.copy()
+        c.precision = PRECISIONS[prec]
+        b = dict(beam)
+        if eps:
+            b["w"] = np.asarray(beam["w"]) * (1.0 + eps)
+        if study is not None:
+            os.environ["QS_FP32_STUDY"] = str(study)
+        try:
+            m = Mesh(c)
+        finally:
+            os.environ.pop("QS_FP32_STUDY", None)
+        m.load_beam(b)
+        m.step()                    # identical first step from identical inputs
+        stream = torch.cuda.ExternalStream(m.stream())
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        m.step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        out = {"ex": m.onaxis_ex(), "psi": m.psi(), "beam": m.get_beam(),
+               "sums": m.charge_sums(), "ms": e0.elapsed_time(e1)}
+        m.close()
+        return out
+
+    rel = lambda a, b: float(np.linalg.norm(np.asarray(a) - np.asarray(b)) /
+                             np.linalg.norm(np.asarray(b)))
+    head = slice(3 * cfg.nx // 4, None)    # the head of the box: the highest layers
+    r64 = run("fp64")
+    r64f = run("fp64fft")
+    r32 = run(cfg_precision_name(cfg))
+
+    def errors(r, ref):
+        e = {"ez_rel_l2": rel(r["ex"], ref["ex"]),
+             "ez_rel_l2_head_quarter": rel(r["ex"][head], ref["ex"][head]),
+             "psi_rel_l2": rel(r["psi"], ref["psi"])}
+        bo, bm = ref["beam"], r["beam"]
+        for k in ("px", "py", "pz"):    # the kicks of the two beam pushes
+            e[f"beam_d{k}_rel_l2"] = rel(np.asarray(bm[k]) - np.asarray(beam[k]),
+                                         np.asarray(bo[k]) - np.asarray(beam[k]))
+        pos = lambda b, c, f: np.asarray(b[c], dtype=np.float64) + np.asarray(b[f])
+        e["beam_position_max_abs_cells"] = float(max(
+            np.max(np.abs(pos(bm, c, f) - pos(bo, c, f))) for c, f in
+            (("i", "x"), ("j", "y"), ("k", "z"))))
+        e["beam_cells_equal_fraction"] = float(np.mean(
+            (np.asarray(bm["i"]) == np.asarray(bo["i"])) &
+            (np.asarray(bm["j"]) == np.asarray(bo["j"])) &
+            (np.asarray(bm["k"]) == np.asarray(bo["k"]))))
+        for q in ("rho", "jx", "rho_beam"):
+            a, b = r["sums"][q], ref["sums"][q]
+            e[f"charge_sum_{q}_max_rel"] = float(np.max(np.abs(a - b)) /
+                                                 max(np.max(np.abs(b)), 1e-300))
+        return e
+
+    out = {"value": pushes_per_step / (r64["ms"] / 1e3), "unit": UNIT,
+           "ms_per_step": r64["ms"],
+           "speedup": r64["ms"] / ours_ms,
+           "transforms": "dense FP64 SIMT matrix passes (O(N^3) per plane)",
+           "fft": {"value": pushes_per_step / (r64f["ms"] / 1e3), "unit": UNIT,
+                   "ms_per_step": r64f["ms"], "speedup": r64f["ms"] / ours_ms,
+                   "transforms": "FP64 half-length complex FFTs, the FP32 path's algorithm",
+                   "ez_rel_l2_vs_fp64": rel(r64f["ex"], r64["ex"])},
+           "errors_vs_fp64": errors(r32, r64),
+           "timing": "device events around the second beam step of each run (the same "
+                     "inputs; the main line's own timing for ours)"}
+    floors = {}
+    for tag, eps in (("perturbed_1e-15", 1e-15), ("perturbed_6e-8", 6e-8)):
+        floors[tag] = rel(run("fp64", eps)["ex"], r64["ex"])
+    out["ez_floor_fp64_vs_itself"] = floors
+    att = {}
+    for name, bit in STUDY_BITS:
+        rs = run("fp64fft", study=bit)
+        att[name] = {"ez_rel_l2": rel(rs["ex"], r64f["ex"]),
+                     "ez_rel_l2_head_quarter": rel(rs["ex"][head], r64f["ex"][head])}
+    out["attribution"] = {
+        "base": "fp64fft (FP64 with FFT transforms)", "components": att,
+        "note": "each entry: the FP64-FFT march with that part in FP32 (transforms through the "
+                "FP32 FFT kernels; spectral state carried between layers rounded to float; the "
+                "push through the FP32 push kernel on float particles and fields; the real "
+                "field planes rounded to float; the beam currents rounded to float), on-axis "
+                "Ez after two beam steps against the plain FP64-FFT march"}
+    out["ez_note"] = ("on-axis Ex (the reference's longitudinal field) over all layers after 2 "
+                      "beam steps; head quarter = the 1/4 of the layers nearest the front")
+    return out
+
+
+def cfg_precision_name(cfg):
+    from tertia_b200.abi import PRECISIONS
+    inv = {v: k for k, v in PRECISIONS.items()}
+    return inv[cfg.precision]
+
+
+# ------------------------------------------------------------------ c2 precision study
+def c2_study(precisions=("fp32", "bf16x3", "tf32x3", "bf16x6"), every=64, shape="cic"):
+    """The c2 precision study: 1024 x 1024 x 2048, 4 ppc, n_b/n_0 = 1, 4e6
+    driver particles; one beam step in FP64 (FFT transforms) and in each
+    FP32 / split-precision mode.  The march runs layer by layer through the
+    fine-grained entry points, and at every `every`-th layer the C layer's
+    Ex, Ey, Ez, Bx, By, Bz and its corrected density rho are read; per-field
+    relative L2 over those layers against FP64.  The beam state stays FP64
+    in every mode."""
+    import numpy as np
+    import torch
+    from tertia_b200 import workload as wl
+    from tertia_b200.abi import PRECISIONS, QS_SHAPE_CIC, QS_SHAPE_NGP, QS_F_DENS
+    from tertia_b200.mesh import Mesh
+
+    w = wl.make_workload("c2")
+    cfg = w.cfg
+    cfg.shape = QS_SHAPE_CIC if shape == "cic" else QS_SHAPE_NGP
+    cfg.use_graph = 0
+    beam = wl.workload_beam(w)
+    front = None
+    names = ["Ex", "Ey", "Ez", "Bx", "By", "Bz", "rho"]
+    sample = set(range(cfg.nx - 1, -1, -every))
+
+    def march(prec, ref=None):
+        c = cfg.copy()
+        c.precision = PRECISIONS[prec]
+        m = Mesh(c)
+        m.load_beam(beam)
+        m.move_beam_particles()
+        m.seed_front_plasma(0)
+        m.begin_march()
+        got = {}
+        num = np.zeros(7)
+        den = np.zeros(7)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for i in range(cfg.nx - 1, -1, -1):
+            m.layer_begin(i, 0)
+            m.move_split_layer(i, 0)
+            if i in sample:
+                planes = [m.get_layer(1, f) for f in range(6)] + [m.get_layer(1, QS_F_DENS)]
+                if ref is None:
+                    got[i] = planes
+                else:
+                    for q in range(7):
+                        num[q] += float(np.sum((planes[q] - ref[i][q]) ** 2))
+                        den[q] += float(np.sum(ref[i][q] ** 2))
+            m.layer_end(i, 0)
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        ex = m.onaxis_ex()
+        m.close()
+        if ref is None:
+            return got, ex, dt
+        return {n: float(np.sqrt(num[q] / den[q])) for q, n in enumerate(names)}, ex, dt
+
+    ref, ex64, t64 = march("fp64fft")
+    out = {"workload": "c2: 1024x1024x2048, 4 ppc, n_b/n_0 = 1, 4e6 driver particles, "
+                       f"{shape.upper()}, one beam step",
+           "reference": "FP64 with FFT transforms (QS_PREC_FP64_FFT)",
+           "sampled_layers": len(sample), "every": every,
+           "fields": names, "march_s": {"fp64fft": t64}, "per_field_rel_l2": {},
+           "ez_onaxis_rel_l2": {}}
+    for prec in precisions:
+        err, ex, dt = march(prec, ref)
+        out["per_field_rel_l2"][prec] = err
+        out["ez_onaxis_rel_l2"][prec] = float(np.linalg.norm(ex - ex64) / np.linalg.norm(ex64))
+        out["march_s"][prec] = dt
+    out["timing"] = ("host clock around the layer-by-layer march (eager launches and the plane "
+                     "reads of the sampled layers included): for scale only")
+    return out
+
+
+# ------------------------------------------------------------------ c4 full form
+def c4_measure(precision="fp32", shape="cic", fp64_head_layers=1024, nbins=64, every=64):
+    """The c4 full form on one GPU: 1024 x 1024 x 4096, 4 ppc with thermal
+    spread 0.01, a 1e7-particle bi-Gaussian driver plus a 1e6-particle
+    witness (sigma_r 0.3, sigma_xi 0.3) at xi = -5.5.
+
+    - memory: device bytes the handle holds (forward, then with the layer
+      checkpoints every `every` layers and the adjoint's buffers), against
+      the GPU's total;
+    - forward: one beam step (beam push + march) timed with device events
+      after an untimed one;
+    - adjoint: the driver's charge profile as `nbins` xi-bins, loss = on-axis
+      Ex integrated over the witness window xi in [-6, -5] behind the driver
+      centre, checkpoints every `every` layers; the adjoint timed against the
+      march over the same layers (device events around both);
+    - error against FP64: the full FP64 field store of c4 (201 GB) exceeds one
+      GPU, so FP64 (FFT transforms) runs the head `fp64_head_layers` layers
+      with the beam particles in them, and the first step's on-axis Ex of
+      those layers is compared (the march runs from the head, so they do not
+      depend on the layers behind them)."""
+    import numpy as np
+    import torch
+    from tertia_b200 import workload as wl
+    from tertia_b200.abi import PRECISIONS, QS_SHAPE_CIC, QS_SHAPE_NGP
+    from tertia_b200.autograd import xi_bins
+    from tertia_b200.mesh import Mesh
+
+    w = wl.make_workload("c4", precision)
+    cfg = w.cfg
+    cfg.shape = QS_SHAPE_CIC if shape == "cic" else QS_SHAPE_NGP
+    beam = wl.workload_beam(w)
+    nb = len(beam["x"])
+    npl = cfg.ny * cfg.nz * cfg.ppc
+    free0, total = torch.cuda.mem_get_info()
+    out = {"workload": f"{w.name}: {w.description}, {shape.upper()}, {precision}",
+           "beam_particles": nb, "plasma_particles_per_layer": npl}
+
+    def events(m):
+        st = torch.cuda.ExternalStream(m.stream())
+        return st, torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    m = Mesh(cfg)
+    m.load_beam(beam)
+    m.step()                                   # untimed: the march graph is captured
+    ex_first = m.onaxis_ex()
+    st, e0, e1 = events(m)
+    torch.cuda.synchronize()
+    e0.record(st)
+    m.step()
+    e1.record(st)
+    torch.cuda.synchronize()
+    fwd_ms = e0.elapsed_time(e1)
+    used_fwd = free0 - torch.cuda.mem_get_info()[0]
+    out["forward"] = {"ms_per_step": fwd_ms,
+                      "value": npl * cfg.nx * cfg.nx_split / (fwd_ms / 1e3), "unit": UNIT,
+                      "timing": "device events around one beam step (beam push + march)"}
+    # the adjoint on the first step's beam (deposited in place, Ts = 0)
+    m.close()
+    c = cfg.copy()
+    c.ts = 0.0
+    c.synchrotron = 0
+    m = Mesh(c)
+    xc = wl.driver_center_x(c, w.beams[0].sigma_xi)
+    sx = w.beams[0].sigma_xi
+    drv = np.arange(nb) < w.beams[0].n
+    bins = xi_bins(beam, c, nbins, xc - 4 * sx, xc + 4 * sx)
+    beta = np.random.default_rng(3).uniform(0.5, 1.5, nbins)
+    bw = dict(beam)
+    bw["w"] = np.where(drv, np.asarray(beam["w"]) * beta[bins], beam["w"])
+    xl = np.arange(c.nx) * c.hx
+    coeff = np.where((xl >= xc - 6.0) & (xl <= xc - 5.0), c.hx, 0.0)
+    m.seed_front_plasma(0)
+    m.adjoint_checkpoints(every)
+    m.load_beam(bw)
+    m.move_beam_particles()
+    m.move_all_split_layers()                  # capture
+    m.adjoint(coeff)                           # capture of the sweep
+    m.seed_front_plasma(0)
+    m.move_all_split_layers()
+    st, e0, e1 = events(m)
+    torch.cuda.synchronize()
+    e0.record(st)
+    m.move_all_split_layers()
+    e1.record(st)
+    torch.cuda.synchronize()
+    march_ms = e0.elapsed_time(e1)
+    e0.record(st)
+    dw = m.adjoint(coeff)
+    e1.record(st)
+    torch.cuda.synchronize()
+    adj_ms = e0.elapsed_time(e1)
+    used_adj = free0 - torch.cuda.mem_get_info()[0]
+    lo = int(np.nonzero(coeff)[0].min())
+    swept = c.nx - lo
+    g = np.bincount(bins[drv], weights=(np.asarray(beam["w"]) * dw)[drv], minlength=nbins)
+    out["adjoint"] = {"checkpoint_every": every, "bins": nbins, "march_ms": march_ms,
+                      "adjoint_ms": adj_ms, "layers_swept": swept, "layers": c.nx,
+                      "adjoint_over_forward_same_layers": adj_ms / (march_ms * swept / c.nx),
+                      "adjoint_over_forward": adj_ms / march_ms,
+                      "grad_norm": float(np.linalg.norm(g)),
+                      "timing": "device events on the handle's stream around the march and "
+                                "around qs_adjoint"}
+    m.close()
+    out["memory"] = {"device_bytes_forward": int(used_fwd),
+                     "device_bytes_with_adjoint": int(used_adj),
+                     "gpu_total_bytes": int(total),
+                     "fraction_of_gpu": used_adj / total,
+                     "layout": "field store (nx+1) x 6 planes, beam currents (nx+1) x 2 planes "
+                               "(their spectra computed in place), layer checkpoints, the "
+                               "adjoint's beam-spectrum adjoint only for the swept layers"}
+    # FP64 over the head layers
+    hl = min(fp64_head_layers, cfg.nx)
+    keep = np.asarray(beam["i"]) >= cfg.nx - hl
+    hb = {k: np.ascontiguousarray(np.asarray(v)[keep]) for k, v in beam.items()}
+    hb["i"] = (hb["i"] - (cfg.nx - hl)).astype(np.int32)
+    res = {}
+    for prec in ("fp64fft", precision):
+        ch = cfg.copy()
+        ch.nx = hl
+        ch.precision = PRECISIONS[prec]
+        mh = Mesh(ch)
+        mh.load_beam(hb)
+        mh.step()
+        res[prec] = mh.onaxis_ex()
+        mh.close()
+    rel = lambda a, b: float(np.linalg.norm(a - b) / np.linalg.norm(b))
+    out["error_vs_fp64"] = {
+        "layers": f"the head {hl} layers (FP64 store of the whole box exceeds one GPU)",
+        "ez_rel_l2_full_box_run": rel(ex_first[cfg.nx - hl + 1:], res["fp64fft"][1:]),
+        "ez_rel_l2_same_head_box": rel(res[precision][1:], res["fp64fft"][1:]),
+        "note": "first beam step, on-axis Ex of the head layers but the last (whose beam "
+                "currents in the head box lack the deposits of the particles behind it); "
+                "full_box_run = the c4 run's own head layers, same_head_box = the same "
+                "precision on the head box"}
+    return out
 
 
 # ------------------------------------------------------------------ our arm
@@ -546,44 +863,21 @@ def run_ours(args):
         del xs, ys
     m.close()
 
-    # ---------------- FP64 plain path on the same inputs: speed and Ez error.
-    # The FP64 path is also run against itself with the beam weights scaled by
-    # (1 + eps): eps = 1e-15 shows the march's response to a last-bit change,
-    # eps = 6e-8 (FP32 rounding scale) the floor that any FP32 computation of
-    # this box faces.  The head quarter of the box is reported separately.
+    # ---------------- FP64 paths on the same inputs: speed and the errors.
+    # Two beam steps each (the second step's beam push sees the first march's
+    # fields); the second step is timed with device events.
+    #  - fp64: the plain FP64 path with dense-matrix transforms (the
+    #    denominator of the >= 5x target); fp64fft: FP64 with the same FFT
+    #    algorithm as the FP32 path (separates algorithm from precision);
+    #  - the FP32 path's errors against fp64: on-axis Ez (the reference's Ex)
+    #    over the whole box and its head quarter, psi, the beam phase space,
+    #    the FP64 charge sums;
+    #  - floors: fp64 against itself with the beam weights x (1 + eps);
+    #  - attribution: the FP64-FFT path with one part of the march in FP32
+    #    at a time (QS_FP32_STUDY), against the plain FP64-FFT path.
     fp64 = None
     if not args.no_fp64:
-        c64 = cfg.copy()
-        c64.precision = PRECISIONS["fp64"]
-        c32 = cfg.copy()
-        ref = {}
-        runs = [("fp64", c64, beam), ("ours", c32, beam)]
-        for tag, eps in (("fp64_pert15", 1e-15), ("fp64_pert7", 6e-8)):
-            bp = dict(beam)
-            bp["w"] = np.asarray(beam["w"]) * (1.0 + eps)
-            runs.append((tag, c64, bp))
-        for tag, c, b in runs:
-            mm = Mesh(c)
-            mm.load_beam(b)
-            mm.step()                   # identical first step from identical inputs
-            torch.cuda.synchronize()
-            t0 = time.perf_counter()
-            mm.step()
-            torch.cuda.synchronize()
-            ref[tag] = (mm.onaxis_ex(), time.perf_counter() - t0)
-            mm.close()
-        e64, t64 = ref["fp64"]
-        rel = lambda a, b: float(np.linalg.norm(a - b) / np.linalg.norm(b))
-        head = slice(3 * cfg.nx // 4, None)    # the head of the box: the highest layers
-        fp64 = {"value": pushes_per_step / t64, "unit": UNIT, "ms_per_step": t64 * 1e3,
-                "speedup": (pushes_per_step / (ms / 1e3)) / (pushes_per_step / t64),
-                "ez_rel_l2_vs_fp64": rel(ref["ours"][0], e64),
-                "ez_rel_l2_vs_fp64_head_quarter": rel(ref["ours"][0][head], e64[head]),
-                "ez_rel_l2_fp64_perturbed_1e-15": rel(ref["fp64_pert15"][0], e64),
-                "ez_rel_l2_fp64_perturbed_6e-8": rel(ref["fp64_pert7"][0], e64),
-                "ez_note": "on-axis Ex (the reference's longitudinal field) over all layers "
-                           "after 2 beam steps; perturbed = the FP64 path against itself with "
-                           "the beam weights x (1 + eps)"}
+        fp64 = fp64_compare(cfg, beam, pushes_per_step, ms)
 
     # ---------------- roofline of the dominant kernel
     hbm, bf16, bf16_sus, src = peaks()
@@ -649,6 +943,19 @@ def run_ours(args):
         except Exception as e:   # noqa: BLE001
             nxt = {"error": f"{type(e).__name__}: {e}"}
 
+    c2 = None
+    if rank == 0 and world == 1 and not args.no_c2 and not args.layers:
+        try:
+            c2 = c2_study(shape=args.shape)
+        except Exception as e:   # noqa: BLE001
+            c2 = {"error": f"{type(e).__name__}: {e}"}
+    c4 = None
+    if rank == 0 and world == 1 and not args.no_c4 and not args.layers:
+        try:
+            c4 = c4_measure(precision=args.precision, shape=args.shape)
+        except Exception as e:   # noqa: BLE001
+            c4 = {"error": f"{type(e).__name__}: {e}"}
+
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
@@ -672,6 +979,8 @@ def run_ours(args):
             "fp64_plain": fp64,
             "adjoint": adjoint,
             "next_rows": nxt,
+            "c2_precision_study": c2,
+            "c4": c4,
             "clocks": clk,
             "onaxis_ex_max": float(np.max(np.abs(onaxis))),
         }

@@ -55,7 +55,10 @@ typedef enum qs_precision {
     QS_PREC_TF32X3 = 2,  /* FP32 push/deposit, transforms as 3-term TF32 split
                             products on the tcgen05 tensor cores, FP32 accumulate   */
     QS_PREC_BF16X3 = 3,  /* as above with 3-term BF16 split products               */
-    QS_PREC_BF16X6 = 4   /* as above with 6-term BF16 split products (3-way split)  */
+    QS_PREC_BF16X6 = 4,  /* as above with 6-term BF16 split products (3-way split)  */
+    QS_PREC_FP64_FFT = 5 /* FP64 everywhere, with the FFT transforms of the FP32 path
+                            computed in FP64 (power-of-two ny, nz in [32, 1024]):
+                            the reference's FFTW algorithm class on the GPU         */
 } qs_precision;
 
 /* Plasma particle shape. */
@@ -254,7 +257,8 @@ qs_status qs_set_beam_currents(qs_handle* h, int field, int layer,
 qs_status qs_get_beam_currents(qs_handle* h, int field, int layer, double* out);
 
 /* On-axis longitudinal field: reference Ex at (My/2, Mz/2) of layers
- * 0..nx-1 after the last march. */
+ * 0..nx-1 of the field store (after the last march, or the layers a march
+ * driven through the fine-grained entry points has finished so far). */
 qs_status qs_get_onaxis_ex(qs_handle* h, double* out);
 /* Wake potential psi(xi_i), a derived quantity the reference does not
  * compute: psi(nx) = 0, psi(i) = psi(i+1) + hx (Ex_i + Ex_{i+1})/2 on axis. */

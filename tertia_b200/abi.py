@@ -30,8 +30,9 @@ QS_PREC_FP32 = 1
 QS_PREC_TF32X3 = 2
 QS_PREC_BF16X3 = 3
 QS_PREC_BF16X6 = 4
+QS_PREC_FP64_FFT = 5
 PRECISIONS = {"fp64": QS_PREC_FP64, "fp32": QS_PREC_FP32, "tf32x3": QS_PREC_TF32X3,
-              "bf16x3": QS_PREC_BF16X3, "bf16x6": QS_PREC_BF16X6}
+              "bf16x3": QS_PREC_BF16X3, "bf16x6": QS_PREC_BF16X6, "fp64fft": QS_PREC_FP64_FFT}
 
 # qs_shape
 QS_SHAPE_NGP = 0

@@ -754,11 +754,12 @@ __global__ void __launch_bounds__(256) beam_weight_grad_kernel(BeamGradArgs<T> a
             for (int dj = 0; dj < 2; dj++)
                 for (int dk = 0; dk < 2; dk++) {
                     const int ii = i + di, jj = j + dj, kk = k + dk;
-                    if (ii > L || jj >= My || kk >= Mz) continue;
+                    if (ii > L || ii < a.lo || jj >= My || kk >= Mz) continue;   // zero below lo
                     const double wc = (di ? ax1 : ax0) * (dj ? ay1 : ay0) * (dk ? az1 : az0);
                     const size_t m = (size_t)jj + (size_t)My * kk;
-                    g += wc * ((double)a.lb3[((size_t)ii * 2 + 0) * plane + m] +
-                               Vx * (double)a.lb3[((size_t)ii * 2 + 1) * plane + m]);
+                    const size_t l = (size_t)(ii - a.lo);
+                    g += wc * ((double)a.lb3[(l * 2 + 0) * plane + m] +
+                               Vx * (double)a.lb3[(l * 2 + 1) * plane + m]);
                 }
     }
     a.out[p] = g * a.polarity;

@@ -3,7 +3,9 @@
 //
 // Data layout in HBM (T = float, or double in QS_PREC_FP64):
 //   f3   : (nx+1) layers x 6 planes (Ex,Ey,Ez,Bx,By,Bz)    Mesh::p_CellArray fields
-//   b3   : (nx+1) layers x 2 planes (RhoBeam, JxBeam)      beam currents
+//   b3   : (nx+1) layers x 2 planes (RhoBeam, JxBeam)      beam currents; after the
+//          beam push's check and sums they are transformed in place into their
+//          REDFT11 x REDFT11 spectra, which the march reads
 //   src3 : (nx+1) layers x 4 planes (Jx,Jy,Jz,Dens)        only with store_sources
 //   P / C layer fields alias f3 during the march: C of the last split of layer
 //   i is f3[i] and P of layer i is f3[i+1], so the reference's copies
@@ -225,8 +227,9 @@ struct Engine : EngineBase {
     T* Psrc = nullptr;
     T* Csrc = nullptr;
     T* Cbeam = nullptr;         // 2 planes (C-layer beam currents, on request)
-    T* sb3 = nullptr;           // (nx+1) layers x 2 planes: spectra of RhoBeam, JxBeam
+    T* sb3 = nullptr;           // the spectra of RhoBeam, JxBeam: b3 itself, transformed in place
     bool sb3_valid = false;
+    bool b3_spec = false;       // b3 holds the spectra (else the real beam currents)
     bool in_march = false;      // inside MoveAllSplitLayers (skip output-only work)
     int cur_layer = -1, cur_split = 0;
     T* bank = nullptr;          // 2 x SP_N planes
@@ -237,6 +240,7 @@ struct Engine : EngineBase {
     DttMats<T> my, mz;
     TcTransformer* tcx = nullptr;
     DttFft* fftx = nullptr;     // FP32 transforms through FFTs (power-of-two sizes)
+    DttFft64* fftx64 = nullptr; // QS_PREC_FP64_FFT: the same FFTs in FP64
     T* onaxis_d = nullptr;
     T* dens_dev = nullptr;      // |Density*q2m| of the march in flight (spectral maps)
     double dens_set = -1.0;     // the value dens_dev holds (-1: none yet)
@@ -293,8 +297,9 @@ struct Engine : EngineBase {
     T* seg = nullptr;           // ck_every x (5 np + (nIter+1) x 6 planes)
     T* lam = nullptr;           // adjoint work planes (see adjoint())
     T* lam_pm = nullptr;        // 3 x np momentum adjoint
-    T* lam_sb = nullptr;        // (nx+1) x 2 planes: adjoint of the beam spectra
-    T* lam_b3 = nullptr;        // (nx+1) x 2 planes: adjoint of the real beam currents
+    T* lam_sb = nullptr;        // layers lam_lo..nx x 2 planes: adjoint of the beam spectra, then
+                                // (in place) of the real beam currents
+    int lam_lo = -1;            // first layer lam_sb holds (the lowest one a sweep reaches)
     T* d_dloss = nullptr;       // nx: d loss / d on-axis Ex of each layer
     double* d_gradw = nullptr;  // nb: d loss / d beam weight
     // CIC adjoint: checkpointed cells and ids, the cells entering each layer of
@@ -346,10 +351,11 @@ struct Engine : EngineBase {
         if (adj_exec) cudaGraphExecDestroy(adj_exec);
         delete tcx;
         delete fftx;
+        delete fftx64;
         delete study_fft;
-        void* ptrs[] = {f3, b3, src3, splitbuf, srcbuf, Cbeam, sb3, bank, scratch, mats, onaxis_d,
+        void* ptrs[] = {f3, b3, src3, splitbuf, srcbuf, Cbeam, bank, scratch, mats, onaxis_d,
                         stage, stage_d, pcell, py, pz, ppx, ppy, ppz, pw, bi, bj, bk, bx, by, bz,
-                        bpx, bpy, bpz, bw, d_err, dens_dev, front_src, front_beam, ck, seg, lam, lam_pm, lam_sb, lam_b3,
+                        bpx, bpy, bpz, bw, d_err, dens_dev, front_src, front_beam, ck, seg, lam, lam_pm, lam_sb,
                         d_dloss, d_gradw, acell, pid, apid, ay, az, apx, apy, apz, aw, cic_cnt,
                         cic_loff, cic_bsum, cic_bpref, cic_ticket, ck_cell, ck_id, seg_cell,
                         adj_inv, lam_pos, adj_tmp, d_pack, d_pack_i, q_cy, q_cz, q_part,
@@ -398,8 +404,8 @@ struct Engine : EngineBase {
             CK(cudaMemset(cic_cnt, 0, plane * sizeof(int)));
             CK(cudaMemset(cic_ticket, 0, sizeof(unsigned)));
         }
-        if ((s = alloc(&sb3, (size_t)(L + 1) * 2 * plane, "beam spectra"))) return s;
-        CK(cudaMemset(sb3, 0, (size_t)(L + 1) * 2 * plane * sizeof(T)));
+        sb3 = b3;   // zero currents have zero spectra
+        b3_spec = true;
         sb3_valid = true;
         if ((s = alloc(&bank, 2 * SP_N * plane, "spectral banks"))) return s;
         CK(cudaMemset(bank, 0, 2 * SP_N * plane * sizeof(T)));
@@ -464,6 +470,12 @@ struct Engine : EngineBase {
         } else if (sizeof(T) == 4) {
             fftx = DttFft::create(My, Mz);   // other sizes keep the FP32 matrix passes
             CK(cudaGetLastError());
+        } else if (cfg.precision == QS_PREC_FP64_FFT) {
+            fftx64 = DttFft64::create(My, Mz);
+            CK(cudaGetLastError());
+            if (!fftx64)
+                return fail(QS_ERR_UNSUPPORTED, "FP64 FFT transforms need power-of-two ny, nz "
+                                                "in [32, 1024]");
         }
         if (sizeof(T) == 8 && getenv("QS_FP32_STUDY")) {
             fp32_study = atoi(getenv("QS_FP32_STUDY")) & 31;
@@ -586,6 +598,10 @@ struct Engine : EngineBase {
             if constexpr (sizeof(T) == 4)
                 for (int pass = 0; pass < 2; pass++)
                     klaunch(KC_GEMM, [&] { return fftx->run_pass(pass, job, scratch, st); });
+        } else if (fftx64) {
+            if constexpr (sizeof(T) == 8)
+                for (int pass = 0; pass < 2; pass++)
+                    klaunch(KC_GEMM, [&] { return fftx64->run_pass(pass, job, scratch, st); });
         } else {
             for (int pass = 0; pass < 2; pass++)
                 klaunch(KC_GEMM, [&] {
@@ -952,10 +968,16 @@ struct Engine : EngineBase {
         if (which == QS_LAYER_C && (field == QS_F_RHOBEAM || field == QS_F_JXBEAM)) {
             // derived from the beam-current store at the current (layer, split)
             const int i = cur_layer < 0 ? L - 1 : cur_layer;
+            const T* cur_b = b3 + (size_t)i * 2 * plane;
+            const T* nxt_b = b3 + (size_t)(i + 1) * 2 * plane;
+            if (b3_spec) {   // the real planes of layers i and i+1 from their spectra
+                beam_real(cur_b, stage, 2);
+                beam_real(nxt_b, stage + 2 * plane, 2);
+                cur_b = stage;
+                nxt_b = stage + 2 * plane;
+            }
             klaunch(KC_MISC, [&] {
-                return launch_beam_layer<T>(b3 + (size_t)i * 2 * plane,
-                                            b3 + (size_t)(i + 1) * 2 * plane, S, cur_split, Cbeam,
-                                            plane, d_err, st);
+                return launch_beam_layer<T>(cur_b, nxt_b, S, cur_split, Cbeam, plane, d_err, st);
             });
             return get_plane(Cbeam + (field == QS_F_JXBEAM ? plane : 0), out);
         }
@@ -984,9 +1006,24 @@ struct Engine : EngineBase {
     qs_status set_beam_currents(int field, int layer, const double* data) override {
         T* p = beam_plane(field, layer);
         if (!p || !data) return fail(QS_ERR_INVALID, "qs_set_beam_currents: bad arguments");
+        if (b3_spec) {   // the whole store back to real currents first
+            batched_cc(b3, b3, 2 * (L + 1), KC_GEMM, inv_scale());
+            b3_spec = false;
+        }
         sb3_valid = false;
         ck_valid = false;
         return put_plane(p, data);
+    }
+
+    // nplanes real beam-current planes from their spectra at `spec` into `out`
+    void beam_real(const T* spec, T* out, int nplanes) {
+        T* outs[kMaxXfFields];
+        int kz[kMaxXfFields], ky[kMaxXfFields];
+        for (int f = 0; f < nplanes; f++) {
+            outs[f] = out + (size_t)f * plane;
+            kz[f] = ky[f] = CC;
+        }
+        xform(job_stack(spec, nplanes, outs, kz, ky, inv_scale()));
     }
 
     // Spectra of every layer's beam currents (RhoBeam, JxBeam: REDFT11 x
@@ -994,15 +1031,18 @@ struct Engine : EngineBase {
     // once per beam push instead of once per layer; plus the |JxBeam| > 10
     // check of :618-621.
     // REDFT11 x REDFT11 transforms of np contiguous planes in large batches
-    void batched_cc(const T* in_planes, T* out_planes, int np, int cls) {
+    // (in place when in_planes == out_planes: every batch is read into the
+    // transform's scratch before its output is written)
+    void batched_cc(const T* in_planes, T* out_planes, int np, int cls, T scale = T(1)) {
         if (tc) {
             for (int b0 = 0; b0 < np; b0 += 64) {
                 const int nf = std::min(64, np - b0);
                 const float* in = (const float*)(in_planes + (size_t)b0 * plane);
                 float* out = (float*)(out_planes + (size_t)b0 * plane);
-                klaunch(KC_SPLIT, [&] { return tcx->run_batched(in, out, nf, 1.0, 0, st); });
-                klaunch(cls, [&] { return tcx->run_batched(in, out, nf, 1.0, 1, st); });
-                klaunch(cls, [&] { return tcx->run_batched(in, out, nf, 1.0, 2, st); });
+                const double sc = (double)scale;
+                klaunch(KC_SPLIT, [&] { return tcx->run_batched(in, out, nf, sc, 0, st); });
+                klaunch(cls, [&] { return tcx->run_batched(in, out, nf, sc, 1, st); });
+                klaunch(cls, [&] { return tcx->run_batched(in, out, nf, sc, 2, st); });
             }
         } else {
             for (int b0 = 0; b0 < np; b0 += kMaxXfFields) {
@@ -1013,7 +1053,7 @@ struct Engine : EngineBase {
                     outs[f] = out_planes + (size_t)(b0 + f) * plane;
                     kz[f] = ky[f] = CC;
                 }
-                xform(job_stack(in_planes + (size_t)b0 * plane, nf, outs, kz, ky, T(1)));
+                xform(job_stack(in_planes + (size_t)b0 * plane, nf, outs, kz, ky, scale));
             }
         }
     }
@@ -1026,7 +1066,8 @@ struct Engine : EngineBase {
             return launch_charge_reduce(qb_part, kBeamSumParts, L + 1, 1.0, q_sums + 2 * (size_t)L,
                                         st);
         });
-        batched_cc(b3, sb3, 2 * (L + 1), KC_GEMM);
+        batched_cc(b3, b3, 2 * (L + 1), KC_GEMM);   // in place: b3 now holds the spectra
+        b3_spec = true;
         study_round(sb3, (size_t)(L + 1) * 2 * plane, 2);
         CK(cudaGetLastError());
         sb3_valid = true;
@@ -1035,11 +1076,21 @@ struct Engine : EngineBase {
     qs_status get_beam_currents(int field, int layer, double* out) override {
         T* p = beam_plane(field, layer);
         if (!p || !out) return fail(QS_ERR_INVALID, "qs_get_beam_currents: bad arguments");
+        if (b3_spec) {   // the real plane from its spectrum
+            beam_real(p, stage, 1);
+            return get_plane(stage, out);
+        }
         return get_plane(p, out);
     }
 
     qs_status get_onaxis(double* out) override {
         if (!out) return fail(QS_ERR_INVALID, "qs_get_onaxis_ex: null");
+        // from the field store, so that a march driven layer by layer through
+        // the fine-grained entry points is read the same way
+        klaunch(KC_MISC, [&] {
+            return launch_onaxis<T>(f3, L, plane, (size_t)(My / 2) + (size_t)My * (Mz / 2), onaxis_d,
+                                    st);
+        });
         std::vector<T> h(L);
         CK(cudaMemcpyAsync(h.data(), onaxis_d, L * sizeof(T), cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
@@ -1051,6 +1102,8 @@ struct Engine : EngineBase {
     qs_status move_beam() override {
         ck_valid = false;
         CK(cudaMemsetAsync(b3, 0, (size_t)(L + 1) * 2 * plane * sizeof(T), st));
+        b3_spec = false;
+        sb3_valid = false;
         BeamArgs<T> a{};
         a.n = nb;
         a.L = L; a.My = My; a.Mz = Mz;
@@ -1771,11 +1824,12 @@ struct Engine : EngineBase {
         if (every > 0 && S != 1)
             return fail(QS_ERR_UNSUPPORTED, "the adjoint supports NxSplit = 1");
         CK(cudaStreamSynchronize(st));
-        void* old[] = {ck, seg, lam, lam_pm, lam_sb, lam_b3, d_dloss, ck_cell, ck_id, seg_cell,
+        void* old[] = {ck, seg, lam, lam_pm, lam_sb, d_dloss, ck_cell, ck_id, seg_cell,
                        lam_pos, adj_inv, adj_tmp};
         for (void* p : old)
             if (p) cudaFree(p);
-        ck = seg = lam = lam_pm = lam_sb = lam_b3 = d_dloss = lam_pos = adj_tmp = nullptr;
+        ck = seg = lam = lam_pm = lam_sb = d_dloss = lam_pos = adj_tmp = nullptr;
+        lam_lo = -1;
         ck_cell = ck_id = seg_cell = adj_inv = nullptr;
         ck_every = 0;
         ck_valid = false;
@@ -1794,8 +1848,6 @@ struct Engine : EngineBase {
         if ((s = alloc(&seg, (size_t)K * seg_stride(), "adjoint segment"))) return s;
         if ((s = alloc(&lam, (size_t)LAM_N * plane, "adjoint planes"))) return s;
         if ((s = alloc(&lam_pm, 3 * (size_t)np, "adjoint momenta"))) return s;
-        if ((s = alloc(&lam_sb, (size_t)(L + 1) * 2 * plane, "adjoint beam spectra"))) return s;
-        if ((s = alloc(&lam_b3, (size_t)(L + 1) * 2 * plane, "adjoint beam currents"))) return s;
         if ((s = alloc(&d_dloss, (size_t)L, "loss gradient"))) return s;
         cic_adj = cfg.shape == QS_SHAPE_CIC;
         if (cic_adj) {
@@ -1835,7 +1887,7 @@ struct Engine : EngineBase {
         }
         return lam + (size_t)i * plane;
     }
-    T* lam_sbp(int layer, int q) { return lam_sb + ((size_t)layer * 2 + q) * plane; }
+    T* lam_sbp(int layer, int q) { return lam_sb + ((size_t)(layer - lam_lo) * 2 + q) * plane; }
 
     // recompute the layers c .. lo of one segment from its checkpoint, storing
     // each layer's entry particles and intermediate C fields
@@ -2061,7 +2113,7 @@ struct Engine : EngineBase {
         CK(cudaMemsetAsync(lam, 0, (size_t)LAM_N * plane * sizeof(T), st));
         CK(cudaMemsetAsync(lam_pm, 0, 3 * (size_t)np * sizeof(T), st));
         if (lam_pos) CK(cudaMemsetAsync(lam_pos, 0, 2 * (size_t)np * sizeof(T), st));
-        CK(cudaMemsetAsync(lam_sb, 0, (size_t)(L + 1) * 2 * plane * sizeof(T), st));
+        CK(cudaMemsetAsync(lam_sb, 0, (size_t)(L + 1 - lam_lo) * 2 * plane * sizeof(T), st));
         int first = L + 1;   // lowest beam-spectrum layer the sweep touches
         if (lo >= 0) {
             const int K = ck_every;
@@ -2101,18 +2153,16 @@ struct Engine : EngineBase {
         }
         // beam spectra adjoint -> real beam-current adjoint (layers first..L;
         // the rest is zero) -> d loss / d w
-        if (first <= L) {
-            CK(cudaMemsetAsync(lam_b3, 0, (size_t)first * 2 * plane * sizeof(T), st));
-            batched_cc(lam_sb + (size_t)first * 2 * plane, lam_b3 + (size_t)first * 2 * plane,
-                       2 * (L + 1 - first), KC_GEMM);
-        } else {
-            CK(cudaMemsetAsync(lam_b3, 0, (size_t)(L + 1) * 2 * plane * sizeof(T), st));
-        }
+        // (in place: lam_sb holds layers lam_lo..L; the sweep wrote layers
+        // first..L, and every layer below lam_lo is zero)
+        if (first <= L)
+            batched_cc(lam_sbp(first, 0), lam_sbp(first, 0), 2 * (L + 1 - first), KC_GEMM);
         BeamGradArgs<T> g{};
         g.n = nb; g.L = L; g.My = My; g.Mz = Mz;
+        g.lo = first <= L ? lam_lo : L + 1;
         g.bi = bi; g.bj = bj; g.bk = bk;
         g.x = bx; g.y = by; g.z = bz; g.px = bpx; g.py = bpy; g.pz = bpz;
-        g.lb3 = lam_b3;
+        g.lb3 = lam_sb;
         g.plane = plane;
         g.polarity = cfg.beam_polarity;
         g.out = d_gradw;
@@ -2142,6 +2192,20 @@ struct Engine : EngineBase {
             drop_adjoint_graph();
         }
         if (nb != adj_graph_nb) drop_adjoint_graph();   // the beam count is baked in
+        {
+            // the beam-spectrum adjoint covers the layers the sweep reaches
+            // (from the lowest layer with a nonzero loss entry to the head)
+            const int need_lo = lo >= 0 ? lo : L;
+            if (!lam_sb || need_lo < lam_lo) {
+                if (lam_sb) cudaFree(lam_sb);
+                lam_sb = nullptr;
+                qs_status s = alloc(&lam_sb, (size_t)(L + 1 - need_lo) * 2 * plane,
+                                    "adjoint beam spectra");
+                if (s) return s;
+                lam_lo = need_lo;
+                drop_adjoint_graph();   // it baked the old array
+            }
+        }
         {
             std::vector<T> h(L);
             for (int i = 0; i < L; i++) h[i] = (T)dloss[i];
@@ -2256,7 +2320,7 @@ static qs_status validate(const qs_config* c, std::string& why) {
     if (c->ppc < 1 || c->ppc > 16) { why = "ppc must be in [1,16]"; return QS_ERR_INVALID; }
     if (!(c->hx > 0) || !(c->hy > 0) || !(c->hz > 0)) { why = "cell sizes must be > 0"; return QS_ERR_INVALID; }
     if (c->shape != QS_SHAPE_NGP && c->shape != QS_SHAPE_CIC) { why = "bad shape"; return QS_ERR_INVALID; }
-    if (c->precision < QS_PREC_FP64 || c->precision > QS_PREC_BF16X6) { why = "bad precision"; return QS_ERR_INVALID; }
+    if (c->precision < QS_PREC_FP64 || c->precision > QS_PREC_FP64_FFT) { why = "bad precision"; return QS_ERR_INVALID; }
     if (!(c->wavelength > 0)) { why = "wavelength must be > 0"; return QS_ERR_INVALID; }
     return QS_OK;
 }
@@ -2300,8 +2364,9 @@ qs_status qs_create(const qs_config* cfg, qs_handle** out) {
         return s;
     }
     EngineBase* e = nullptr;
-    bool tc = cfg->precision >= QS_PREC_TF32X3;
-    if (cfg->precision == QS_PREC_FP64) e = new (std::nothrow) Engine<double>();
+    bool tc = cfg->precision >= QS_PREC_TF32X3 && cfg->precision <= QS_PREC_BF16X6;
+    if (cfg->precision == QS_PREC_FP64 || cfg->precision == QS_PREC_FP64_FFT)
+        e = new (std::nothrow) Engine<double>();
     else {
         auto* ef = new (std::nothrow) Engine<float>();
         if (ef) {

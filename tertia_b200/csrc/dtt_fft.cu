@@ -34,11 +34,26 @@
 namespace qs {
 namespace fft {
 
-__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
-    return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+// The FFT machinery is written once for a complex type C: float2 for the FP32
+// transforms, double2 for the FP64 ones (the same algorithm in FP64).
+template <class C> struct Cx;
+template <> struct Cx<float2> {
+    using Real = float;
+    __device__ __host__ static float2 make(float x, float y) { return make_float2(x, y); }
+};
+template <> struct Cx<double2> {
+    using Real = double;
+    __device__ __host__ static double2 make(double x, double y) { return make_double2(x, y); }
+};
+
+template <class C>
+__device__ __forceinline__ C cmul(C a, C b) {
+    return Cx<C>::make(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
-__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
-__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+template <class C>
+__device__ __forceinline__ C cadd(C a, C b) { return Cx<C>::make(a.x + b.x, a.y + b.y); }
+template <class C>
+__device__ __forceinline__ C csub(C a, C b) { return Cx<C>::make(a.x - b.x, a.y - b.y); }
 
 template <int R>
 __device__ __forceinline__ int bitrev(int i) {
@@ -47,41 +62,43 @@ __device__ __forceinline__ int bitrev(int i) {
 }
 
 // e^{-2 pi i k/16} for k = 0..7 (cos and sin of multiples of pi/8)
-constexpr float kC8 = 0.923879532511286756f;   // cos(pi/8)
-constexpr float kS8 = 0.382683432365089772f;   // sin(pi/8)
-constexpr float kR2 = 0.707106781186547524f;   // cos(pi/4)
+constexpr double kC8 = 0.923879532511286756;   // cos(pi/8)
+constexpr double kS8 = 0.382683432365089772;   // sin(pi/8)
+constexpr double kR2 = 0.707106781186547524;   // cos(pi/4)
 
 // x * e^{-2 pi i k/16}, with the multiplications by 1 and -i left out
-template <int K>
-__device__ __forceinline__ float2 rot16(float2 x) {
+template <int K, class C>
+__device__ __forceinline__ C rot16(C x) {
     static_assert(K >= 0 && K < 8, "rot16");
+    using Real = typename Cx<C>::Real;
+    constexpr Real r2 = (Real)kR2;
     if constexpr (K == 0) return x;
-    else if constexpr (K == 4) return make_float2(x.y, -x.x);
-    else if constexpr (K == 2) return make_float2(kR2 * (x.x + x.y), kR2 * (x.y - x.x));
-    else if constexpr (K == 6) return make_float2(kR2 * (x.y - x.x), -kR2 * (x.x + x.y));
+    else if constexpr (K == 4) return Cx<C>::make(x.y, -x.x);
+    else if constexpr (K == 2) return Cx<C>::make(r2 * (x.x + x.y), r2 * (x.y - x.x));
+    else if constexpr (K == 6) return Cx<C>::make(r2 * (x.y - x.x), -r2 * (x.x + x.y));
     else {
-        constexpr float c = K == 1 ? kC8 : K == 3 ? kS8 : K == 5 ? -kS8 : -kC8;
-        constexpr float s = K == 1 ? kS8 : K == 3 ? kC8 : K == 5 ? kC8 : kS8;
-        return make_float2(c * x.x + s * x.y, c * x.y - s * x.x);
+        constexpr Real c = (Real)(K == 1 ? kC8 : K == 3 ? kS8 : K == 5 ? -kS8 : -kC8);
+        constexpr Real s = (Real)(K == 1 ? kS8 : K == 3 ? kC8 : K == 5 ? kC8 : kS8);
+        return Cx<C>::make(c * x.x + s * x.y, c * x.y - s * x.x);
     }
 }
 
 // one radix-2 stage of butterflies of length LEN over the R registers
-template <int R, int LEN, int T>
-__device__ __forceinline__ void dit_stage_t(float2 (&v)[R]) {
+template <int R, int LEN, int T, class C>
+__device__ __forceinline__ void dit_stage_t(C (&v)[R]) {
     if constexpr (T < LEN / 2) {
 #pragma unroll
         for (int s = 0; s < R; s += LEN) {
-            const float2 u = v[s + T];
-            const float2 x = rot16<T * (16 / LEN)>(v[s + T + LEN / 2]);
+            const C u = v[s + T];
+            const C x = rot16<T * (16 / LEN)>(v[s + T + LEN / 2]);
             v[s + T] = cadd(u, x);
             v[s + T + LEN / 2] = csub(u, x);
         }
         dit_stage_t<R, LEN, T + 1>(v);
     }
 }
-template <int R, int LEN>
-__device__ __forceinline__ void dit_stages(float2 (&v)[R]) {
+template <int R, int LEN, class C>
+__device__ __forceinline__ void dit_stages(C (&v)[R]) {
     if constexpr (LEN <= R) {
         dit_stage_t<R, LEN, 0>(v);
         dit_stages<R, 2 * LEN>(v);
@@ -92,8 +109,8 @@ __device__ __forceinline__ void dit_stages(float2 (&v)[R]) {
 // constant twiddles).  The input is loaded in bit-reversed order
 // (v[i] = x[bitrev(i)]), so only memory addresses are permuted and every
 // register index is static; the output is in natural order.
-template <int R>
-__device__ __forceinline__ void dft(float2 (&v)[R]) {
+template <int R, class C>
+__device__ __forceinline__ void dft(C (&v)[R]) {
     dit_stages<R, 2>(v);
 }
 
@@ -106,9 +123,8 @@ __device__ __forceinline__ void seq_sync() {
 }
 
 // load, twiddle and transform butterfly group j of a pass (registers only)
-template <int M, int R, int NS, class At>
-__device__ __forceinline__ void stockham_group(float2 (&v)[R], const float2* W, At at, int j,
-                                               const float2* tw) {
+template <int M, int R, int NS, class C, class At>
+__device__ __forceinline__ void stockham_group(C (&v)[R], const C* W, At at, int j, const C* tw) {
 #pragma unroll
     for (int i = 0; i < R; i++) {
         const int r = bitrev<R>(i);
@@ -118,8 +134,8 @@ __device__ __forceinline__ void stockham_group(float2 (&v)[R], const float2* W, 
     dft<R>(v);
 }
 
-template <int R, int NS, class At>
-__device__ __forceinline__ void stockham_store(const float2 (&v)[R], float2* W, At at, int j) {
+template <int R, int NS, class C, class At>
+__device__ __forceinline__ void stockham_store(const C (&v)[R], C* W, At at, int j) {
     const int d = (j / NS) * NS * R + (j % NS);
 #pragma unroll
     for (int r = 0; r < R; r++) W[at(d + r * NS)] = v[r];
@@ -129,18 +145,18 @@ __device__ __forceinline__ void stockham_store(const float2 (&v)[R], float2* W, 
 // thread of a sequence (T = M/V of them, V values each) does (M/R)/T
 // butterfly groups (1, 2, 4 or 8).  `at(e)` maps element e of this thread's
 // sequence to its shared-memory slot.
-template <int M, int V, int R, int NS, bool WARP, class At>
-__device__ __forceinline__ void stockham_pass(float2* W, At at, int jt, const float2* tw) {
+template <int M, int V, int R, int NS, bool WARP, class C, class At>
+__device__ __forceinline__ void stockham_pass(C* W, At at, int jt, const C* tw) {
     constexpr int T = M / V;
     constexpr int G = (M / R) / T;
     static_assert(G == 1 || G == 2 || G == 4 || G == 8, "groups per thread");
     if constexpr (G == 1) {
-        float2 v[R];
+        C v[R];
         stockham_group<M, R, NS>(v, W, at, jt, tw);
         seq_sync<WARP>();
         stockham_store<R, NS>(v, W, at, jt);
     } else {
-        float2 v[G][R];
+        C v[G][R];
 #pragma unroll
         for (int g = 0; g < G; g++) stockham_group<M, R, NS>(v[g], W, at, jt + g * T, tw);
         seq_sync<WARP>();
@@ -153,15 +169,14 @@ __device__ __forceinline__ void stockham_pass(float2* W, At at, int jt, const fl
 // The last pass keeps its butterfly groups in registers: thread jt ends up
 // with Z_q for q = jt + T*m in slot m (m < V), and Z_{M-1-q} sits in slot
 // V-1-m of thread T-1-jt.
-template <int M, int V, int R, int NS, class At>
-__device__ __forceinline__ void final_pass(const float2* W, At at, int jt, const float2* tw,
-                                           float2 (&fin)[V]) {
+template <int M, int V, int R, int NS, class C, class At>
+__device__ __forceinline__ void final_pass(const C* W, At at, int jt, const C* tw, C (&fin)[V]) {
     constexpr int T = M / V;
     constexpr int G = (M / R) / T;
     static_assert(NS * R == M && G * R == V, "final pass");
 #pragma unroll
     for (int g = 0; g < G; g++) {
-        float2 v[R];
+        C v[R];
         stockham_group<M, R, NS>(v, W, at, jt + g * T, tw);
 #pragma unroll
         for (int r = 0; r < R; r++) fin[g + G * r] = v[r];
@@ -172,9 +187,8 @@ __device__ __forceinline__ void final_pass(const float2* W, At at, int jt, const
 template <int M, int V, int NS, bool WARP>
 struct Passes {
     static constexpr int R = (M / NS) >= V ? V : (M / NS);
-    template <class At>
-    __device__ __forceinline__ static void run(float2* W, At at, int jt, const float2* tw,
-                                               float2 (&fin)[V]) {
+    template <class C, class At>
+    __device__ __forceinline__ static void run(C* W, At at, int jt, const C* tw, C (&fin)[V]) {
         if constexpr (NS * R == M) {
             final_pass<M, V, R, NS>(W, at, jt, tw, fin);
         } else {
@@ -190,20 +204,30 @@ template <int M>
 __host__ __device__ constexpr int vpt() {
     return M <= 128 ? 8 : 16;
 }
+// values per thread of the FP64 transforms: 8 (twice the registers per value)
+template <int M, class C>
+__host__ __device__ constexpr int vpt_c() {
+    return sizeof(C) == sizeof(float2) ? vpt<M>() : 8;
+}
+template <class Real> struct CxOf;
+template <> struct CxOf<float> { using type = float2; };
+template <> struct CxOf<double> { using type = double2; };
 
-struct RowArgs {
-    const float* in[kMaxXfFields];
-    float* out[kMaxXfFields];
+template <class Real>
+struct RowArgsT {
+    const Real* in[kMaxXfFields];
+    Real* out[kMaxXfFields];
     int kind[kMaxXfFields];   // QS_REDFT11 / QS_RODFT11 of each field
     int nrows;                // rows per plane
     int total;                // nf * nrows
-    float scale;
-    const float2* tab;        // tw[M], pre[M], post[M]
+    Real scale;
+    const typename CxOf<Real>::type* tab;   // tw[M], pre[M], post[M]
 };
+using RowArgs = RowArgsT<float>;
 
-template <int M>
+template <int M, class C = float2>
 __host__ __device__ constexpr int row_threads() {
-    return (M / vpt<M>()) > 64 ? (M / vpt<M>()) : 64;
+    return (M / vpt_c<M, C>()) > 64 ? (M / vpt_c<M, C>()) : 64;
 }
 
 // Transform along the contiguous axis: each sequence of T = M/V threads
@@ -214,17 +238,19 @@ __host__ __device__ constexpr int row_threads() {
 // T-1-jt, a shuffle away when a row lies within one warp.  Shared slot of
 // element e: e + e/V (one pad per V keeps the stride-V stores of the first
 // pass free of bank conflicts).
-template <int M>
-__global__ void __launch_bounds__(row_threads<M>()) fft_rows_kernel(RowArgs a) {
-    constexpr int V = vpt<M>();
+template <int M, class C>
+__global__ void __launch_bounds__(row_threads<M, C>())
+    fft_rows_kernel(RowArgsT<typename Cx<C>::Real> a) {
+    using Real = typename Cx<C>::Real;
+    constexpr int V = vpt_c<M, C>();
     constexpr int T = M / V;
-    constexpr int NT = row_threads<M>();
+    constexpr int NT = row_threads<M, C>();
     constexpr int SEQ = NT / T;
     constexpr int LD = M + M / V;
     constexpr bool WARP = T <= 32;
-    __shared__ float2 W[SEQ * LD];
-    __shared__ float2 tws[M];
-    __shared__ float2 posts[M];
+    __shared__ C W[SEQ * LD];
+    __shared__ C tws[M];
+    __shared__ C posts[M];
     for (int i = threadIdx.x; i < M; i += NT) {
         tws[i] = a.tab[i];
         posts[i] = a.tab[2 * M + i];
@@ -233,48 +259,48 @@ __global__ void __launch_bounds__(row_threads<M>()) fft_rows_kernel(RowArgs a) {
     const int row = blockIdx.x * SEQ + s;
     const bool valid = row < a.total;
     const int f = valid ? row / a.nrows : 0, k = valid ? row % a.nrows : 0;
-    float2* Ws = W + s * LD;
+    C* Ws = W + s * LD;
     auto at = [](int e) { return e + e / V; };
     pdl_wait();
-    const float* inf = a.in[0];
-    float* outf = a.out[0];
+    const Real* inf = a.in[0];
+    Real* outf = a.out[0];
     int kind = a.kind[0];
 #pragma unroll
     for (int q = 1; q < kMaxXfFields; q++)
         if (q == f) { inf = a.in[q]; outf = a.out[q]; kind = a.kind[q]; }
-    const float2* P = reinterpret_cast<const float2*>(inf + (size_t)k * 2 * M);
-    const float2* pre = a.tab + M;
+    const C* P = reinterpret_cast<const C*>(inf + (size_t)k * 2 * M);
+    const C* pre = a.tab + M;
     // the V pairs of this thread in bit-reversed order, the pre-twiddle
-    float2 p[V], w[V];
+    C p[V], w[V];
 #pragma unroll
     for (int b = 0; b < V; b++) {
         const int i = jt + bitrev<V>(b) * T;
-        p[b] = valid ? P[i] : make_float2(0.f, 0.f);
+        p[b] = valid ? P[i] : Cx<C>::make(Real(0), Real(0));
         w[b] = __ldg(pre + i);
     }
-    float2 v[V];
+    C v[V];
     if constexpr (WARP) {
         // x[n-1-2i] = P[M-1-i].y: slot V-1-b of thread T-1-jt
 #pragma unroll
         for (int b = 0; b < V; b++) {
-            const float mirror = __shfl_xor_sync(0xffffffffu, p[V - 1 - b].y, T - 1);
-            const float2 z = kind == QS_REDFT11 ? make_float2(p[b].x, mirror)
-                                                : make_float2(mirror, p[b].x);
+            const Real mirror = __shfl_xor_sync(0xffffffffu, p[V - 1 - b].y, T - 1);
+            const C z = kind == QS_REDFT11 ? Cx<C>::make(p[b].x, mirror)
+                                           : Cx<C>::make(mirror, p[b].x);
             v[b] = cmul(z, w[b]);
         }
     } else {
 #pragma unroll
         for (int b = 0; b < V; b++) {
             const int i = jt + bitrev<V>(b) * T;
-            const float mirror = valid ? P[M - 1 - i].y : 0.f;
-            const float2 z = kind == QS_REDFT11 ? make_float2(p[b].x, mirror)
-                                                : make_float2(mirror, p[b].x);
+            const Real mirror = valid ? P[M - 1 - i].y : Real(0);
+            const C z = kind == QS_REDFT11 ? Cx<C>::make(p[b].x, mirror)
+                                           : Cx<C>::make(mirror, p[b].x);
             v[b] = cmul(z, w[b]);
         }
     }
     __syncthreads();   // twiddle tables in place
     dft<V>(v);
-    float2 fin[V];
+    C fin[V];
     if constexpr (T == 1) {
         // one pass: Z_r in slot r, the thread owns the whole sequence
 #pragma unroll
@@ -287,22 +313,22 @@ __global__ void __launch_bounds__(row_threads<M>()) fft_rows_kernel(RowArgs a) {
     }
     pdl_trigger();
     // s_q = Z_q e^{-i pi (q+1/4)/n}; out pair q = (2 Re s_q, -+2 Im s_{M-1-q})
-    float im[V];
+    Real im[V];
 #pragma unroll
     for (int m = 0; m < V; m++) {
         const int q = jt + T * m;
-        const float2 sq = cmul(fin[m], posts[q]);
+        const C sq = cmul(fin[m], posts[q]);
         fin[m] = sq;
         im[m] = sq.y;
     }
-    float mirror[V];
+    Real mirror[V];
     if constexpr (WARP) {
 #pragma unroll
         for (int m = 0; m < V; m++) mirror[m] = __shfl_xor_sync(0xffffffffu, im[V - 1 - m], T - 1);
     } else {
         // rows wider than a warp: the mirrored parts through shared memory
         __syncthreads();
-        float* ims = reinterpret_cast<float*>(Ws);
+        Real* ims = reinterpret_cast<Real*>(Ws);
 #pragma unroll
         for (int m = 0; m < V; m++) ims[jt + T * m] = im[m];
         __syncthreads();
@@ -310,36 +336,40 @@ __global__ void __launch_bounds__(row_threads<M>()) fft_rows_kernel(RowArgs a) {
         for (int m = 0; m < V; m++) mirror[m] = ims[M - 1 - (jt + T * m)];
     }
     if (!valid) return;
-    float2* O = reinterpret_cast<float2*>(outf + (size_t)k * 2 * M);
-    const float c2 = 2.f * a.scale;
-    const float sgn = kind == QS_REDFT11 ? -c2 : c2;
+    C* O = reinterpret_cast<C*>(outf + (size_t)k * 2 * M);
+    const Real c2 = Real(2) * a.scale;
+    const Real sgn = kind == QS_REDFT11 ? -c2 : c2;
 #pragma unroll
-    for (int m = 0; m < V; m++) O[jt + T * m] = make_float2(c2 * fin[m].x, sgn * mirror[m]);
+    for (int m = 0; m < V; m++) O[jt + T * m] = Cx<C>::make(c2 * fin[m].x, sgn * mirror[m]);
 }
 
-struct ColArgs {
-    const float* in[kMaxXfFields];
-    float* out[kMaxXfFields];
-    float* acc[kMaxXfFields];   // optional: the input is also added here
-    float* clr[kMaxXfFields];   // optional: the input planes, zeroed once read
+template <class Real>
+struct ColArgsT {
+    const Real* in[kMaxXfFields];
+    Real* out[kMaxXfFields];
+    Real* acc[kMaxXfFields];    // optional: the input is also added here
+    Real* clr[kMaxXfFields];    // optional: the input planes, zeroed once read
     int kind[kMaxXfFields];
     int ncols;                // row length of the planes (the y size)
-    float scale;
-    const float2* tab;
+    Real scale;
+    const typename CxOf<Real>::type* tab;
 };
+using ColArgs = ColArgsT<float>;
 
 // Transform along the strided axis: a CTA takes TJ adjacent columns of one
 // plane (TJ floats = whole 32-byte sectors per row); column c's sequence
 // lives at W[e * TJ + c], its T threads are TJ lanes apart.
-template <int M, int TJ>
-__global__ void __launch_bounds__(TJ * (M / vpt<M>())) fft_cols_kernel(ColArgs a) {
-    constexpr int V = vpt<M>();
+template <int M, int TJ, class C>
+__global__ void __launch_bounds__(TJ * (M / vpt_c<M, C>()))
+    fft_cols_kernel(ColArgsT<typename Cx<C>::Real> a) {
+    using Real = typename Cx<C>::Real;
+    constexpr int V = vpt_c<M, C>();
     constexpr int T = M / V;
     constexpr int NT = TJ * T;
-    extern __shared__ float2 smem_f2[];
-    float2* tws = smem_f2;
-    float2* posts = smem_f2 + M;
-    float2* W = smem_f2 + 2 * M;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C* tws = reinterpret_cast<C*>(smem_raw);
+    C* posts = tws + M;
+    C* W = tws + 2 * M;
     for (int i = threadIdx.x; i < M; i += NT) {
         tws[i] = a.tab[i];
         posts[i] = a.tab[2 * M + i];
@@ -350,19 +380,19 @@ __global__ void __launch_bounds__(TJ * (M / vpt<M>())) fft_cols_kernel(ColArgs a
     const size_t ld = (size_t)a.ncols;
     auto at = [c](int e) { return e * TJ + c; };
     pdl_wait();
-    const float* inf = a.in[0];
-    float* outf = a.out[0];
-    float* accf = a.acc[0];
-    float* clrf = a.clr[0];
+    const Real* inf = a.in[0];
+    Real* outf = a.out[0];
+    Real* accf = a.acc[0];
+    Real* clrf = a.clr[0];
     int kind = a.kind[0];
 #pragma unroll
     for (int q = 1; q < kMaxXfFields; q++)
         if (q == f) {
             inf = a.in[q]; outf = a.out[q]; accf = a.acc[q]; clrf = a.clr[q]; kind = a.kind[q];
         }
-    const float2* pre = a.tab + M;
-    float lo[V], hi[V];
-    float2 w[V];
+    const C* pre = a.tab + M;
+    Real lo[V], hi[V];
+    C w[V];
 #pragma unroll
     for (int b = 0; b < V; b++) {
         const int i = jt + bitrev<V>(b) * T;
@@ -381,20 +411,20 @@ __global__ void __launch_bounds__(TJ * (M / vpt<M>())) fft_cols_kernel(ColArgs a
                 accf[ohi] += hi[b];
             }
             if (clrf) {
-                clrf[olo] = 0.f;
-                clrf[ohi] = 0.f;
+                clrf[olo] = Real(0);
+                clrf[ohi] = Real(0);
             }
         }
     }
-    float2 v[V];
+    C v[V];
 #pragma unroll
     for (int b = 0; b < V; b++) {
-        const float2 z = kind == QS_REDFT11 ? make_float2(lo[b], hi[b]) : make_float2(hi[b], lo[b]);
+        const C z = kind == QS_REDFT11 ? Cx<C>::make(lo[b], hi[b]) : Cx<C>::make(hi[b], lo[b]);
         v[b] = cmul(z, w[b]);
     }
     __syncthreads();
     dft<V>(v);
-    float2 fin[V];
+    C fin[V];
     if constexpr (T == 1) {
 #pragma unroll
         for (int r = 0; r < V; r++) fin[r] = v[r];
@@ -405,7 +435,7 @@ __global__ void __launch_bounds__(TJ * (M / vpt<M>())) fft_cols_kernel(ColArgs a
         Passes<M, V, V, false>::run(W, at, jt, tws, fin);
     }
     pdl_trigger();
-    float im[V];
+    Real im[V];
 #pragma unroll
     for (int m = 0; m < V; m++) {
         const int q = jt + T * m;
@@ -413,12 +443,12 @@ __global__ void __launch_bounds__(TJ * (M / vpt<M>())) fft_cols_kernel(ColArgs a
         im[m] = fin[m].y;
     }
     __syncthreads();
-    float* ims = reinterpret_cast<float*>(W);
+    Real* ims = reinterpret_cast<Real*>(W);
 #pragma unroll
     for (int m = 0; m < V; m++) ims[(jt + T * m) * TJ + c] = im[m];
     __syncthreads();
-    const float c2 = 2.f * a.scale;
-    const float sgn = kind == QS_REDFT11 ? -c2 : c2;
+    const Real c2 = Real(2) * a.scale;
+    const Real sgn = kind == QS_REDFT11 ? -c2 : c2;
 #pragma unroll
     for (int m = 0; m < V; m++) {
         const int q = jt + T * m;
@@ -427,35 +457,36 @@ __global__ void __launch_bounds__(TJ * (M / vpt<M>())) fft_cols_kernel(ColArgs a
     }
 }
 
-template <int M>
+template <int M, class C = float2>
 __host__ __device__ constexpr int cols_tj() {
-    return (M / vpt<M>()) >= 16 ? 8 : (M / vpt<M>()) >= 4 ? 16 : 32;
+    return (M / vpt_c<M, C>()) >= 16 ? 8 : (M / vpt_c<M, C>()) >= 4 ? 16 : 32;
 }
 
-template <int M>
+template <int M, class C = float2>
 size_t cols_smem() {
-    return sizeof(float2) * (size_t)M * (2 + cols_tj<M>());
+    return sizeof(C) * (size_t)M * (2 + cols_tj<M, C>());
 }
 
-template <int M>
+template <int M, class C = float2>
 cudaError_t set_cols_smem() {
-    return cudaFuncSetAttribute(fft_cols_kernel<M, cols_tj<M>()>,
-                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cols_smem<M>());
+    return cudaFuncSetAttribute(fft_cols_kernel<M, cols_tj<M, C>(), C>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)cols_smem<M, C>());
 }
 
-template <int M>
-cudaError_t launch_rows(const RowArgs& a, cudaStream_t st) {
-    constexpr int SEQ = row_threads<M>() / (M / vpt<M>());
+template <int M, class C = float2>
+cudaError_t launch_rows(const RowArgsT<typename Cx<C>::Real>& a, cudaStream_t st) {
+    constexpr int SEQ = row_threads<M, C>() / (M / vpt_c<M, C>());
     const int blocks = (a.total + SEQ - 1) / SEQ;
-    return launch_pdl(fft_rows_kernel<M>, dim3((unsigned)blocks), dim3(row_threads<M>()), 0, st,
-                      a);
+    return launch_pdl(fft_rows_kernel<M, C>, dim3((unsigned)blocks), dim3(row_threads<M, C>()), 0,
+                      st, a);
 }
 
-template <int M>
-cudaError_t launch_cols(const ColArgs& a, int nf, cudaStream_t st) {
-    constexpr int TJ = cols_tj<M>();
-    return launch_pdl(fft_cols_kernel<M, TJ>, dim3((unsigned)(a.ncols / TJ), (unsigned)nf),
-                      dim3(TJ * (M / vpt<M>())), cols_smem<M>(), st, a);
+template <int M, class C = float2>
+cudaError_t launch_cols(const ColArgsT<typename Cx<C>::Real>& a, int nf, cudaStream_t st) {
+    constexpr int TJ = cols_tj<M, C>();
+    return launch_pdl(fft_cols_kernel<M, TJ, C>, dim3((unsigned)(a.ncols / TJ), (unsigned)nf),
+                      dim3(TJ * (M / vpt_c<M, C>())), cols_smem<M, C>(), st, a);
 }
 
 // ---------------------------------------------------------------------------
@@ -781,16 +812,18 @@ bool fft_size_ok(int n) { return n >= 32 && n <= 2048 && (n & (n - 1)) == 0; }
 
 // table of one size n: tw[M] = e^{-2 pi i k/M}, pre[M] = e^{-i pi i/n},
 // post[M] = e^{-i pi (i+1/4)/n}, M = n/2, built in FP64
-std::vector<float2> fft_table(int n) {
+template <class C>
+std::vector<C> fft_table(int n) {
+    using Real = typename fft::Cx<C>::Real;
     const int M = n / 2;
-    std::vector<float2> t(3 * (size_t)M);
+    std::vector<C> t(3 * (size_t)M);
     for (int k = 0; k < M; k++) {
         const double a = -2.0 * M_PI * k / M;
-        t[k] = make_float2((float)std::cos(a), (float)std::sin(a));
+        t[k] = fft::Cx<C>::make((Real)std::cos(a), (Real)std::sin(a));
         const double b = -M_PI * k / n;
-        t[M + k] = make_float2((float)std::cos(b), (float)std::sin(b));
+        t[M + k] = fft::Cx<C>::make((Real)std::cos(b), (Real)std::sin(b));
         const double c = -M_PI * (k + 0.25) / n;
-        t[2 * M + k] = make_float2((float)std::cos(c), (float)std::sin(c));
+        t[2 * M + k] = fft::Cx<C>::make((Real)std::cos(c), (Real)std::sin(c));
     }
     return t;
 }
@@ -808,7 +841,7 @@ DttFft* DttFft::create(int ny, int nz) {
     d->ny = ny;
     d->nz = nz;
     auto up = [](int n, float2** dst) {
-        std::vector<float2> t = fft_table(n);
+        std::vector<float2> t = fft_table<float2>(n);
         if (cudaMalloc(dst, t.size() * sizeof(float2)) != cudaSuccess) return false;
         return cudaMemcpy(*dst, t.data(), t.size() * sizeof(float2), cudaMemcpyHostToDevice) ==
                cudaSuccess;
@@ -953,6 +986,98 @@ int DttFft::run_pass(int pass, const DttJob<float>& job, float* scratch, cudaStr
             case 64: e = fft::launch_cols<64>(a, job.nf, st); break;
             case 32: e = fft::launch_cols<32>(a, job.nf, st); break;
             default: e = fft::launch_cols<16>(a, job.nf, st); break;
+        }
+    }
+    return e == cudaSuccess ? 1 : 0;
+}
+
+// ---------------------------------------------------------------- FP64
+namespace {
+bool fft64_size_ok(int n) { return n >= 32 && n <= 1024 && (n & (n - 1)) == 0; }
+}  // namespace
+
+DttFft64::~DttFft64() {
+    if (tab_y) cudaFree(tab_y);
+    if (tab_z && tab_z != tab_y) cudaFree(tab_z);
+}
+
+DttFft64* DttFft64::create(int ny, int nz) {
+    if (!fft64_size_ok(ny) || !fft64_size_ok(nz)) return nullptr;
+    auto* d = new DttFft64();
+    d->ny = ny;
+    d->nz = nz;
+    auto up = [](int n, double2** dst) {
+        std::vector<double2> t = fft_table<double2>(n);
+        if (cudaMalloc(dst, t.size() * sizeof(double2)) != cudaSuccess) return false;
+        return cudaMemcpy(*dst, t.data(), t.size() * sizeof(double2), cudaMemcpyHostToDevice) ==
+               cudaSuccess;
+    };
+    bool ok = up(ny, &d->tab_y);
+    if (ok) {
+        if (nz == ny) d->tab_z = d->tab_y;
+        else ok = up(nz, &d->tab_z);
+    }
+    for (int n : {ny, nz}) {
+        if (!ok) break;
+        cudaError_t e;
+        switch (n / 2) {
+            case 512: e = fft::set_cols_smem<512, double2>(); break;
+            case 256: e = fft::set_cols_smem<256, double2>(); break;
+            case 128: e = fft::set_cols_smem<128, double2>(); break;
+            case 64: e = fft::set_cols_smem<64, double2>(); break;
+            case 32: e = fft::set_cols_smem<32, double2>(); break;
+            default: e = fft::set_cols_smem<16, double2>(); break;
+        }
+        if (e != cudaSuccess) ok = false;
+    }
+    if (!ok) {
+        delete d;
+        return nullptr;
+    }
+    return d;
+}
+
+int DttFft64::run_pass(int pass, const DttJob<double>& job, double* scratch,
+                       cudaStream_t st) const {
+    if (job.nf <= 0 || job.nf > kMaxXfFields) return 0;
+    const size_t plane = (size_t)ny * nz;
+    cudaError_t e = cudaSuccess;
+    if (pass == 0) {   // along y: in -> scratch
+        fft::RowArgsT<double> a{};
+        for (int f = 0; f < job.nf; f++) {
+            a.in[f] = job.in[f];
+            a.out[f] = scratch + f * plane;
+            a.kind[f] = job.ky[f];
+        }
+        a.nrows = nz;
+        a.total = job.nf * nz;
+        a.scale = 1.0;
+        a.tab = tab_y;
+        switch (ny / 2) {
+            case 512: e = fft::launch_rows<512, double2>(a, st); break;
+            case 256: e = fft::launch_rows<256, double2>(a, st); break;
+            case 128: e = fft::launch_rows<128, double2>(a, st); break;
+            case 64: e = fft::launch_rows<64, double2>(a, st); break;
+            case 32: e = fft::launch_rows<32, double2>(a, st); break;
+            default: e = fft::launch_rows<16, double2>(a, st); break;
+        }
+    } else {           // along z: scratch -> out, scaled
+        fft::ColArgsT<double> a{};
+        for (int f = 0; f < job.nf; f++) {
+            a.in[f] = scratch + f * plane;
+            a.out[f] = job.out[f];
+            a.kind[f] = job.kz[f];
+        }
+        a.ncols = ny;
+        a.scale = job.scale;
+        a.tab = tab_z;
+        switch (nz / 2) {
+            case 512: e = fft::launch_cols<512, double2>(a, job.nf, st); break;
+            case 256: e = fft::launch_cols<256, double2>(a, job.nf, st); break;
+            case 128: e = fft::launch_cols<128, double2>(a, job.nf, st); break;
+            case 64: e = fft::launch_cols<64, double2>(a, job.nf, st); break;
+            case 32: e = fft::launch_cols<32, double2>(a, job.nf, st); break;
+            default: e = fft::launch_cols<16, double2>(a, job.nf, st); break;
         }
     }
     return e == cudaSuccess ? 1 : 0;

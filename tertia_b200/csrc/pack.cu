@@ -9,7 +9,9 @@
 // per-cell atomic cursor), then one thread per cell puts its few particles
 // back in load order (insertion sort on the load id; the ids are a
 // permutation, so the order is unique), then one thread per output row entry
-// gathers and widens the particle's values.
+// gathers and widens the particle's values.  The unpack runs the same sort the
+// other way: the buffer checked on the device, its particles ordered by cell
+// (buffer order within a cell) and narrowed into the plasma arrays.
 #include "qs_internal.h"
 
 namespace qs {
@@ -121,7 +123,87 @@ __global__ void pack_mix_kernel(const T* __restrict__ a, const T* __restrict__ b
     out[i] = __dadd_rn(__dmul_rn(w0, (double)a[i]), __dmul_rn(w1, (double)b[i]));
 }
 
+// ---- UnpackLayer (para.cpp:175-285) on the device: the buffer's particle
+// blocks checked row by row, then ordered by cell (stable: buffer order within
+// a cell) and gathered into the plasma arrays.
+
+// a row's cell, or -1 and the lowest bad row recorded: the cell must be a
+// whole (j, k) inside the layer, the in-cell position in [0, 1], the species
+// the plasma electrons (Q2m, isort 0) - the host reports the row's reason
+__global__ void unpack_check_kernel(const double* __restrict__ pb, int64_t m, int My, int Mz,
+                                    double q2m, int32_t* __restrict__ key_cell,
+                                    int* __restrict__ cnt, unsigned long long* __restrict__ bad) {
+    const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= m) return;
+    const double jd = pb[r + 9 * m], kd = pb[r + 10 * m];
+    const double yy = pb[r + 4 * m], zz = pb[r + 5 * m];
+    const bool cell_ok = jd >= 0 && jd < My && kd >= 0 && kd < Mz && jd == (double)(int)jd &&
+                         kd == (double)(int)kd;
+    const bool pos_ok = yy >= 0 && yy <= 1 && zz >= 0 && zz <= 1;
+    const bool sort_ok = pb[r + 6 * m] == q2m && pb[r + 11 * m] == 0.0;
+    if (!(cell_ok && pos_ok && sort_ok)) {
+        atomicMin(bad, (unsigned long long)r);
+        key_cell[r] = -1;
+        return;
+    }
+    const int c = (int)jd + My * (int)kd;
+    key_cell[r] = c;
+    atomicAdd(cnt + c, 1);
+}
+
+__global__ void unpack_place_kernel(const int32_t* __restrict__ key_cell, int64_t m,
+                                    const int* __restrict__ start, int* __restrict__ fill,
+                                    int32_t* __restrict__ ord) {
+    const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= m) return;
+    const int c = key_cell[r];
+    if (c < 0) return;
+    ord[start[c] + atomicAdd(fill + c, 1)] = (int32_t)r;
+}
+
+template <class T>
+__global__ void unpack_gather_kernel(UnpackArgs<T> a) {
+    const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t m = a.m;
+    if (r >= m) return;
+    const int32_t q = a.ord[r];
+    if (q < 0 || q >= m) {
+        atomicOr(a.err, DEV_ERR_INTERNAL);
+        return;
+    }
+    const double* pb = a.buf;
+    const int c = a.key_cell[q];
+    a.cell[r] = c;
+    a.px[r] = (T)pb[q];
+    a.py[r] = (T)pb[q + m];
+    a.pz[r] = (T)pb[q + 2 * m];
+    a.y[r] = (T)pb[q + 4 * m];
+    a.z[r] = (T)pb[q + 5 * m];
+    a.w[r] = (T)pb[q + 7 * m];
+    if (a.ppc <= 0 || c != (int)(r / a.ppc)) atomicOr(a.nonuniform, 1);
+}
+
 }  // namespace
+
+template <class T>
+int launch_unpack_check(const UnpackArgs<T>& a, cudaStream_t st) {
+    if (a.m <= 0) return 0;
+    unpack_check_kernel<<<(unsigned)((a.m + 255) / 256), 256, 0, st>>>(
+        a.buf, a.m, a.My, a.Mz, a.q2m, a.key_cell, a.cnt, a.bad);
+    return 1;
+}
+
+template <class T>
+int launch_unpack_order(const UnpackArgs<T>& a, cudaStream_t st) {
+    if (a.m <= 0) return 0;
+    const unsigned gm = (unsigned)((a.m + 255) / 256);
+    const unsigned gc = (unsigned)((a.ncell + 255) / 256);
+    pack_scan_kernel<<<1, 1024, 0, st>>>(a.cnt, a.ncell, a.start);
+    unpack_place_kernel<<<gm, 256, 0, st>>>(a.key_cell, a.m, a.start, a.fill, a.ord);
+    pack_cell_order_kernel<<<gc, 256, 0, st>>>(a.start, a.ncell, nullptr, a.ord);
+    unpack_gather_kernel<T><<<gm, 256, 0, st>>>(a);
+    return 4;
+}
 
 template <class T>
 int launch_pack_particles(const PackArgs<T>& a, cudaStream_t st) {
@@ -146,6 +228,10 @@ int launch_pack_mix(const T* a, const T* b, double w0, double w1, size_t n, doub
 
 template int launch_pack_particles<float>(const PackArgs<float>&, cudaStream_t);
 template int launch_pack_particles<double>(const PackArgs<double>&, cudaStream_t);
+template int launch_unpack_check<float>(const UnpackArgs<float>&, cudaStream_t);
+template int launch_unpack_check<double>(const UnpackArgs<double>&, cudaStream_t);
+template int launch_unpack_order<float>(const UnpackArgs<float>&, cudaStream_t);
+template int launch_unpack_order<double>(const UnpackArgs<double>&, cudaStream_t);
 template int launch_pack_mix<float>(const float*, const float*, double, double, size_t, double*,
                                     cudaStream_t);
 template int launch_pack_mix<double>(const double*, const double*, double, double, size_t,

@@ -135,6 +135,18 @@ struct DttFft {
     ~DttFft();
 };
 
+// FP64 half-integer transforms through half-length complex FFTs: the same
+// algorithm and kernels as DttFft in FP64, for power-of-two ny, nz in
+// [32, 1024] (pass 0 along y into `scratch`, pass 1 along z with the scale)
+struct DttFft64 {
+    int ny = 0, nz = 0;
+    double2* tab_y = nullptr;
+    double2* tab_z = nullptr;
+    static DttFft64* create(int ny, int nz);   // nullptr when a size is not handled
+    int run_pass(int pass, const DttJob<double>& job, double* scratch, cudaStream_t st) const;
+    ~DttFft64();
+};
+
 template <class T>
 int run_dtt_simt_pass(int pass, const DttJob<T>& job, int ny, int nz, const DttMats<T>& my,
                       const DttMats<T>& mz, T* scratch, cudaStream_t st);
@@ -270,6 +282,33 @@ struct PackArgs {
 };
 template <class T>
 int launch_pack_particles(const PackArgs<T>& a, cudaStream_t st);
+// UnpackLayer's particle blocks on the device (pack.cu): `buf` holds the 12
+// double rows of m particles.  launch_unpack_check gives every row its cell
+// (key_cell; -1 for a bad row), counts the cells into cnt (ncell ints, zeroed
+// by the caller) and lowers *bad (set to m by the caller) to the lowest bad
+// row.  launch_unpack_order (after a clean check) orders the rows by cell,
+// buffer order within a cell (start: ncell + 1, fill: ncell zeroed, ord: m),
+// and writes them into the plasma arrays; *nonuniform is set unless row r
+// lies in cell r / ppc for every r.
+template <class T>
+struct UnpackArgs {
+    int64_t m;
+    int My, Mz, ncell, ppc;
+    const double* buf;
+    double q2m;
+    int32_t* key_cell;
+    int *cnt, *start, *fill;
+    int32_t* ord;
+    unsigned long long* bad;
+    int* nonuniform;
+    int32_t* cell;
+    T *y, *z, *px, *py, *pz, *w;
+    int* err;
+};
+template <class T>
+int launch_unpack_check(const UnpackArgs<T>& a, cudaStream_t st);
+template <class T>
+int launch_unpack_order(const UnpackArgs<T>& a, cudaStream_t st);
 // out = w0 a + w1 b over n values, in double
 template <class T>
 int launch_pack_mix(const T* a, const T* b, double w0, double w1, size_t n, double* out,
@@ -280,11 +319,12 @@ template <class T>
 int launch_avg_planes(const T* P, const T* C, T* out, size_t n, cudaStream_t st);
 
 // d loss / d (beam macro-particle weight) from the adjoint of the real beam
-// currents (lb3: (L+1) layers x 2 planes RhoBeam, JxBeam).
+// currents (lb3: layers lo .. L x 2 planes RhoBeam, JxBeam; zero below lo).
 template <class T>
 struct BeamGradArgs {
     int64_t n;
     int L, My, Mz;
+    int lo;
     const int32_t *bi, *bj, *bk;
     const double *x, *y, *z, *px, *py, *pz;
     const T* lb3;
