@@ -33,14 +33,31 @@ REF_LIB_PATH = os.path.join(_HERE, "_ref", "libref_linearized.so")
 REFERENCE = os.environ.get("QS_REFERENCE_DIR", "/root/reference")
 
 
+REFPIN_LIB_PATH = os.path.join(_HERE, "_ref", "librefpin.so")
+
+
 def build_reference() -> str | None:
-    """Compile the reference's CUDA twins of the per-mode spectral maps into
-    oracle/_ref/ (only where the reference checkout is present); returns the
-    library path or None."""
+    """Compile, where the reference checkout is present, its CUDA twins of the
+    per-mode spectral maps and its host plasma push and beam push into
+    oracle/_ref/; returns the spectral-map library path or None."""
     if os.path.isdir(os.path.join(REFERENCE, "CUDA_WRAP")):
-        subprocess.run(["make", "-C", _HERE, "ref", f"REFERENCE={REFERENCE}"], check=True,
-                       capture_output=True)
+        subprocess.run(["make", "-C", _HERE, "ref", "refpin", f"REFERENCE={REFERENCE}"],
+                       check=True, capture_output=True)
     return REF_LIB_PATH if os.path.exists(REF_LIB_PATH) else None
+
+
+def refpin_lib():
+    """The reference's own host plasma push and beam push (oracle/ref_pin.cpp
+    over the reference files), or None when they were not built."""
+    if not os.path.exists(REFPIN_LIB_PATH):
+        return None
+    from tertia_b200.abi import QsConfig
+    L = C.CDLL(REFPIN_LIB_PATH)
+    L.refpin_push_layer.argtypes = [C.POINTER(QsConfig), C.c_int64, _i32p] + [_f64p] * 6 + [
+        _f64p, _f64p, _f64p, _i32p, C.c_int]
+    L.refpin_beam_push.argtypes = [C.POINTER(QsConfig), C.c_int64] + [_i32p] * 3 + [_f64p] * 7 + [
+        _f64p, _f64p]
+    return L
 
 
 def reference_lib():
@@ -137,6 +154,7 @@ def _declare(L):
         getattr(L, name).argtypes = [P, C.c_int, C.c_int, _f64p]
     L.qso_get_onaxis_ex.argtypes = [P, _f64p]
     L.qso_get_psi.argtypes = [P, _f64p]
+    L.qso_set_field3d.argtypes = [P, C.c_int, C.c_int, _f64p]
     L.qso_get_charge_sums.argtypes = [P, _f64p, _f64p, _f64p]
     for name in ("qso_step", "qso_move_beam_particles", "qso_move_all_split_layers",
                  "qso_begin_march"):
@@ -339,6 +357,11 @@ class Oracle:
         r, j, b = np.empty(self.cfg.nx), np.empty(self.cfg.nx), np.empty(self.cfg.nx + 1)
         _check(lib().qso_get_charge_sums(self._h, r, j, b), "qso_get_charge_sums")
         return {"rho": r, "jx": j, "rho_beam": b}
+
+    def set_field3d(self, field, layer, data):
+        _check(lib().qso_set_field3d(self._h, field, layer,
+                                     np.ascontiguousarray(data, dtype=np.float64).reshape(-1)),
+               "qso_set_field3d")
 
     def step(self):
         _check(lib().qso_step(self._h), "qso_step")

@@ -1693,6 +1693,18 @@ int qso_get_onaxis_ex(qso* h, double* out) {
     return QS_OK;
 }
 
+int qso_set_field3d(qso* h, int field, int layer, const double* data) {
+    if (!h || !data || field < 0 || field > 5 || layer < 0 || layer > h->o.L) return QS_ERR_INVALID;
+    Oracle& o = h->o;
+    // interior and the whole guard ring, periodic in y and z
+    for (int k = -o.G; k < o.Mz + o.G; k++)
+        for (int j = -o.G; j < o.My + o.G; j++) {
+            const int jj = (j + o.My) % o.My, kk = (k + o.Mz) % o.Mz;
+            o.A[o.aidx(layer, field, j, k)] = data[(size_t)jj + (size_t)o.My * kk];
+        }
+    return QS_OK;
+}
+
 int qso_get_psi(qso* h, double* out) {
     if (!h || !out) return QS_ERR_INVALID;
     const Oracle& o = h->o;

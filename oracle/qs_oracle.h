@@ -79,6 +79,9 @@ int qso_set_beam_currents(qso* o, int field, int layer, const double* data);
 int qso_get_beam_currents(qso* o, int field, int layer, double* out);
 int qso_get_onaxis_ex(qso* o, double* out);
 
+/* Fields (Ex..Bz, field 0..5) of stored layer 0..nx: the interior plane and
+ * its periodic guard ring, as the march leaves them for the beam push. */
+int qso_set_field3d(qso* o, int field, int layer, const double* data);
 /* Wake potential on axis (a derived quantity the reference does not
  * compute): psi(nx) = 0, psi(i) = psi(i+1) + hx (Ex_i + Ex_{i+1})/2 over the
  * on-axis Ex of the last march. */

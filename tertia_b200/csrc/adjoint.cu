@@ -20,6 +20,7 @@
 
 #include "qs_common.cuh"
 #include "qs_internal.h"
+#include "pushmath.cuh"
 #include "pdl.cuh"
 #include "adjoint_maps.cuh"
 
@@ -39,6 +40,22 @@ __device__ __forceinline__ int wrap_m(int j, int M) {
 }  // namespace
 
 // ---------------------------------------------------------------------------
+// 1 - Vx of momentum p with inv_g = 1/gamma, and 1 - (Vxm + Vxp)/2 from the
+// two: FP32 in the push kernels' cancellation-free forms (pushmath.cuh), FP64
+// in the reference's expression order, as the forward ran them
+template <class T>
+__device__ __forceinline__ T omv(T px, T, T, T inv_g) { return T(1) - px * inv_g; }
+template <>
+__device__ __forceinline__ float omv<float>(float px, float py, float pz, float inv_g) {
+    return one_minus_vx(px, py, pz, inv_g);
+}
+template <class T>
+__device__ __forceinline__ T omv_mean(T vxm, T vxp, T, T) { return T(1) - T(0.5) * (vxm + vxp); }
+template <>
+__device__ __forceinline__ float omv_mean<float>(float, float, float omm, float omp) {
+    return 0.5f * (omm + omp);
+}
+
 // push adjoint: one thread per particle
 template <class T>
 __global__ void __launch_bounds__(256) push_adjoint_kernel(PushAdjArgs<T> a) {
@@ -67,7 +84,7 @@ __global__ void __launch_bounds__(256) push_adjoint_kernel(PushAdjArgs<T> a) {
     const T s0 = one + p[0] * p[0] + p[1] * p[1] + p[2] * p[2];
     const T r0 = one / sqrt(s0);
     const T Vp[3] = {p[0] * r0, p[1] * r0, p[2] * r0};
-    const T av = one - Vp[0];
+    const T av = omv(p[0], p[1], p[2], r0);
     const T ia = one / av;
     const T kE = a.sE * ia;
     const T e[3] = {E[0] * kE, E[1] * kE, E[2] * kE};
@@ -88,7 +105,7 @@ __global__ void __launch_bounds__(256) push_adjoint_kernel(PushAdjArgs<T> a) {
     const T r2 = one / sqrt(s2);
     const T Vm[3] = {p2[0] * r2, p2[1] * r2, p2[2] * r2};
     const T V[3] = {half * (Vm[0] + Vp[0]), half * (Vm[1] + Vp[1]), half * (Vm[2] + Vp[2])};
-    const T cv = one - V[0];
+    const T cv = omv_mean(Vm[0], Vp[0], omv(p2[0], p2[1], p2[2], r2), av);
     const T inv2 = one / cv;
     const T wq = w * inv2;
     const T dJ0[3] = {a.djx0, a.djy0, a.djz0};
@@ -318,7 +335,8 @@ __device__ __forceinline__ int push_adjoint_cic_one(const PushAdjArgs<T>& a, int
     const T s0 = one + p[0] * p[0] + p[1] * p[1] + p[2] * p[2];
     const T r0 = rsq(s0);
     const T Vp[3] = {p[0] * r0, p[1] * r0, p[2] * r0};
-    const T ia = rcp(one - Vp[0]);
+    const T omp = omv(p[0], p[1], p[2], r0);
+    const T ia = rcp(omp);
     const T kE = a.sE * ia;
     const T e[3] = {E[0] * kE, E[1] * kE, E[2] * kE};
     const T p1[3] = {p[0] + e[0], p[1] + e[1], p[2] + e[2]};
@@ -335,7 +353,7 @@ __device__ __forceinline__ int push_adjoint_cic_one(const PushAdjArgs<T>& a, int
     const T r2 = rsq(one + p2[0] * p2[0] + p2[1] * p2[1] + p2[2] * p2[2]);
     const T Vm[3] = {p2[0] * r2, p2[1] * r2, p2[2] * r2};
     const T V[3] = {half * (Vm[0] + Vp[0]), half * (Vm[1] + Vp[1]), half * (Vm[2] + Vp[2])};
-    const T inv2 = rcp(one - V[0]);
+    const T inv2 = rcp(omv_mean(Vm[0], Vp[0], omv(p2[0], p2[1], p2[2], r2), omp));
     const T wq = w * inv2;
     const T dJ0[3] = {a.djx0, a.djy0, a.djz0};
     const T dq[3] = {wq * dJ0[0] * Vm[0], wq * dJ0[1] * Vm[1], wq * dJ0[2] * Vm[2]};

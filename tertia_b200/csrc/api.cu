@@ -341,7 +341,7 @@ struct Engine : EngineBase {
     // the hand-off buffer assembled on the device, and its ordering scratch
     double* d_pack = nullptr;
     int* d_pack_i = nullptr;
-    size_t pack_cap = 0;
+    size_t pack_cap = 0, pack_icap = 0;
 
     T* bankp(int b, int p) { return bank + ((size_t)b * SP_N + p) * plane; }
     T* f3layer(int i) { return f3 + (size_t)i * 6 * plane; }
@@ -1563,16 +1563,9 @@ struct Engine : EngineBase {
             if (s0) return s0;
         }
         // the buffer is assembled in device memory and leaves in one copy
-        if ((size_t)n > pack_cap) {
-            if (d_pack) cudaFree(d_pack);
-            if (d_pack_i) cudaFree(d_pack_i);
-            d_pack = nullptr;
-            d_pack_i = nullptr;
-            pack_cap = 0;
-            qs_status s = alloc(&d_pack, (size_t)n, "hand-off buffer");
-            if (!s) s = alloc(&d_pack_i, 3 * plane + 1 + (size_t)np, "hand-off buffer order");
+        {
+            qs_status s = ensure_pack_space(n, np);
             if (s) return s;
-            pack_cap = (size_t)n;
         }
         const size_t P = plane;
         double* dp = d_pack;
@@ -1638,9 +1631,41 @@ struct Engine : EngineBase {
         if (!buf || n < fixed || (n - fixed) % 12)
             return fail(QS_ERR_INVALID, "qs_unpack_layer: n must be 12*ny*nz + 12*Np");
         const int64_t m = (n - fixed) / 12;
-        const double* pb = buf + fixed;
-        std::vector<int32_t> cell(m);
-        for (int64_t r = 0; r < m; r++) {
+        if (m > INT32_MAX) return fail(QS_ERR_INVALID, "qs_unpack_layer: too many particles");
+        // the buffer enters the device in one copy; the particle rows are
+        // checked there, and only a clean buffer changes the handle's state
+        qs_status s = ensure_pack_space(n, m);
+        if (s) return s;
+        const size_t P = plane;
+        int* cnt = d_pack_i;
+        int* fill = cnt + P;
+        int* start = fill + P;
+        int32_t* ord = start + P + 1;
+        int32_t* key_cell = ord + m;
+        unsigned long long* bad = (unsigned long long*)(key_cell + m + 1);   // 8-byte aligned below
+        bad = (unsigned long long*)(((uintptr_t)bad + 7) & ~(uintptr_t)7);
+        int* nonuniform = (int*)(bad + 1);
+        CK(cudaMemcpyAsync(d_pack, buf, (size_t)n * sizeof(double), cudaMemcpyHostToDevice, st));
+        CK(cudaMemsetAsync(cnt, 0, 2 * P * sizeof(int), st));
+        const unsigned long long none = (unsigned long long)m;
+        CK(cudaMemcpyAsync(bad, &none, sizeof(none), cudaMemcpyHostToDevice, st));
+        CK(cudaMemsetAsync(nonuniform, 0, sizeof(int), st));
+        UnpackArgs<T> a{};
+        a.m = m; a.My = My; a.Mz = Mz; a.ncell = (int)P; a.ppc = cfg.ppc;
+        a.buf = d_pack + fixed;
+        a.q2m = cfg.plasma_q2m;
+        a.key_cell = key_cell;
+        a.cnt = cnt; a.start = start; a.fill = fill; a.ord = ord;
+        a.bad = bad; a.nonuniform = nonuniform;
+        a.err = d_err;
+        klaunch(KC_MISC, [&] { return launch_unpack_check<T>(a, st); });
+        unsigned long long first_bad = none;
+        CK(cudaMemcpyAsync(&first_bad, bad, sizeof(first_bad), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        if (first_bad < (unsigned long long)m) {
+            // the lowest bad row, reported as the reference-format check of it
+            const int64_t r = (int64_t)first_bad;
+            const double* pb = buf + fixed;
             const double jd = pb[r + 9 * m], kd = pb[r + 10 * m];
             if (!(jd >= 0 && jd < My && kd >= 0 && kd < Mz) || jd != (double)(int)jd ||
                 kd != (double)(int)kd)
@@ -1650,45 +1675,64 @@ struct Engine : EngineBase {
             if (!(yy >= 0 && yy <= 1 && zz >= 0 && zz <= 1))
                 return fail(QS_ERR_PARTICLE_RANGE, "qs_unpack_layer: particle %lld has in-cell "
                                                    "position outside [0,1]", (long long)r);
-            if (pb[r + 6 * m] != cfg.plasma_q2m || pb[r + 11 * m] != 0.0)
-                return fail(QS_ERR_UNSUPPORTED, "qs_unpack_layer: particle %lld is not of the "
-                                                "plasma electron species", (long long)r);
-            cell[r] = (int32_t)jd + My * (int32_t)kd;
+            return fail(QS_ERR_UNSUPPORTED, "qs_unpack_layer: particle %lld is not of the "
+                                            "plasma electron species", (long long)r);
         }
-        // stable counting sort by cell (the buffer order kept within a cell;
-        // every cell was checked to lie inside the layer)
-        std::vector<int64_t> start(plane + 1, 0), ord(m);
-        for (int64_t r = 0; r < m; r++) start[(size_t)cell[r] + 1]++;
-        for (size_t c = 0; c < plane; c++) start[c + 1] += start[c];
-        for (int64_t r = 0; r < m; r++) ord[start[(size_t)cell[r]]++] = r;
-        std::vector<int32_t> c2(m);
-        std::vector<double> y(m), z(m), px(m), py_(m), pz_(m), w(m);
-        for (int64_t r = 0; r < m; r++) {
-            const int64_t q = ord[r];
-            c2[r] = cell[q];
-            px[r] = pb[q];
-            py_[r] = pb[q + m];
-            pz_[r] = pb[q + 2 * m];
-            y[r] = pb[q + 4 * m];
-            z[r] = pb[q + 5 * m];
-            w[r] = pb[q + 7 * m];
-        }
-        qs_status s;
         if (!front_src && (s = alloc(&front_src, 4 * plane, "received layer"))) return s;
         if (!front_beam && (s = alloc(&front_beam, 2 * plane, "received layer"))) return s;
-        const size_t P = plane;
+        if ((s = ensure_plasma(m))) return s;
+        if (grp.flip) swap_sets();   // the march graph starts from the first set
+        a.cell = pcell;
+        a.y = py; a.z = pz; a.px = ppx; a.py = ppy; a.pz = ppz; a.w = pw;
+        klaunch(KC_MISC, [&] { return launch_unpack_order<T>(a, st); });
+        // the planes: Bx By Bz Ex Ey Ez into the front layer's fields, Jx Jy
+        // Jz Rho into its sources, fftJxBeamHydro / fftRhoBeamHydro
         const int fdst[6] = {3, 4, 5, 0, 1, 2};
         for (int f = 0; f < 6; f++)
-            if ((s = put_plane(f3layer(L) + (size_t)fdst[f] * P, buf + (size_t)f * P))) return s;
-        for (int f = 0; f < 4; f++)
-            if ((s = put_plane(front_src + (size_t)f * P, buf + (size_t)(6 + f) * P))) return s;
-        if ((s = put_plane(front_beam, buf + 11 * P))) return s;       // RhoBeam
-        if ((s = put_plane(front_beam + P, buf + 10 * P))) return s;   // JxBeam
-        if ((s = load_front(m, c2.data(), y.data(), z.data(), px.data(), py_.data(), pz_.data(),
-                            w.data())))
-            return s;
+            klaunch(KC_MISC, [&] {
+                return launch_convert<T>(d_pack + (size_t)f * P, 1, f3layer(L) + (size_t)fdst[f] * P,
+                                         P, st);
+            });
+        klaunch(KC_MISC, [&] {
+            return launch_convert<T>(d_pack + 6 * P, 1, front_src, 4 * P, st);
+        });
+        klaunch(KC_MISC, [&] { return launch_convert<T>(d_pack + 11 * P, 1, front_beam, P, st); });
+        klaunch(KC_MISC, [&] {
+            return launch_convert<T>(d_pack + 10 * P, 1, front_beam + P, P, st);
+        });
+        int nonu = 1;
+        CK(cudaMemcpyAsync(&nonu, nonuniform, sizeof(int), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        {
+            const qs_status s0 = check_device();
+            if (s0) return s0;
+        }
+        np = m;
+        uniform_layout = m == (int64_t)plane * cfg.ppc && !nonu;
+        if ((s = cic_fresh_front())) return s;
+        front_pending = true;
         front_layer = true;
         front_used = false;
+        return QS_OK;
+    }
+
+    // device space of the hand-off buffer (n doubles) and its ordering
+    // scratch for m particles: counts, fill cursors, offsets, order, the
+    // rows' cells and two status words
+    qs_status ensure_pack_space(int64_t n, int64_t m) {
+        const size_t ints = 3 * plane + 1 + 2 * (size_t)m + 8;
+        if ((size_t)n > pack_cap || ints > pack_icap) {
+            if (d_pack) cudaFree(d_pack);
+            if (d_pack_i) cudaFree(d_pack_i);
+            d_pack = nullptr;
+            d_pack_i = nullptr;
+            pack_cap = pack_icap = 0;
+            qs_status s = alloc(&d_pack, (size_t)n, "hand-off buffer");
+            if (!s) s = alloc(&d_pack_i, ints, "hand-off buffer order");
+            if (s) return s;
+            pack_cap = (size_t)n;
+            pack_icap = ints;
+        }
         return QS_OK;
     }
 

@@ -23,6 +23,7 @@
 #include "qs_common.cuh"
 #include "qs_internal.h"
 #include "pdl.cuh"
+#include "pushmath.cuh"
 
 namespace qs {
 
@@ -208,8 +209,9 @@ __global__ void __launch_bounds__(256) push_kernel(PushArgs<T> a) {
         if (!(yp >= T(0) && yp <= one && zp >= T(0) && zp <= one)) {
             atomicOr(a.err, DEV_ERR_RANGE);
         } else {
-            if (FAST) {
-            // ---- FP32: the same update with the divisions factored out
+            if constexpr (FAST) {
+            // ---- FP32: the same update with the divisions factored out, and
+            // 1 - Vx in its cancellation-free form (pushmath.cuh)
             const T inv_gp = one / sqrt_t<T>(one + px * px + py * py + pz * pz);
             const T Vxp = px * inv_gp, Vyp = py * inv_gp, Vzp = pz * inv_gp;
             const T q2m = a.q2m;
@@ -242,7 +244,8 @@ __global__ void __launch_bounds__(256) push_kernel(PushArgs<T> a) {
                 }
                 ex = g[0]; ey = g[1]; ez = g[2]; bx = g[3]; by = g[4]; bz = g[5];
             }
-            const T inv1 = one / (one - Vxp);
+            const T omp = one_minus_vx(px, py, pz, inv_gp);   // 1 - Vx before the kick
+            const T inv1 = one / omp;
             const T kE = a.sE * inv1;                 // q2m*hx/2 / (1 - Vx)
             ex *= kE;
             ey *= kE;
@@ -264,10 +267,10 @@ __global__ void __launch_bounds__(256) push_kernel(PushArgs<T> a) {
             pz += ez + (p3x * by - p3y * bx);
             const T inv_g = one / sqrt_t<T>(one + px * px + py * py + pz * pz);
             const T Vxm = px * inv_g, Vym = py * inv_g, Vzm = pz * inv_g;
-            const T Vx = half * (Vxm + Vxp);
             const T Vy = half * (Vym + Vyp);
             const T Vz = half * (Vzm + Vzp);
-            const T inv2 = one / (one - Vx);
+            // 1 - (Vxm + Vxp)/2 = ((1 - Vxm) + (1 - Vxp))/2
+            const T inv2 = one / (half * (one_minus_vx(px, py, pz, inv_g) + omp));
             const T wq = weight * inv2;
             const T djx = wq * a.djx0 * Vxm;
             const T djy = wq * a.djy0 * Vym;
@@ -442,8 +445,9 @@ __global__ void __launch_bounds__(128) push_cell_kernel(PushArgs<float> a) {
         }
         float px = pxv[q], py = pyv[q], pz = pzv[q];
         const float inv_gp = rsqrtf(1.f + px * px + py * py + pz * pz);
-        const float Vxp = px * inv_gp, Vyp = py * inv_gp, Vzp = pz * inv_gp;
-        const float kE = a.sE * __frcp_rn(1.f - Vxp);
+        const float Vyp = py * inv_gp, Vzp = pz * inv_gp;
+        const float omp = one_minus_vx(px, py, pz, inv_gp);   // 1 - Vx before the kick
+        const float kE = a.sE * __frcp_rn(omp);
         const float ex = ex0 * kE, ey = ey0 * kE, ez = ez0 * kE;
         px += ex; py += ey; pz += ez;
         const float kB = rsqrtf(1.f + px * px + py * py + pz * pz) * kE;
@@ -457,8 +461,8 @@ __global__ void __launch_bounds__(128) push_cell_kernel(PushArgs<float> a) {
         pz += ez + (p3x * by - p3y * bx);
         const float inv_g = rsqrtf(1.f + px * px + py * py + pz * pz);
         const float Vxm = px * inv_g, Vym = py * inv_g, Vzm = pz * inv_g;
-        const float Vx = 0.5f * (Vxm + Vxp), Vy = 0.5f * (Vym + Vyp), Vz = 0.5f * (Vzm + Vzp);
-        const float inv2 = __frcp_rn(1.f - Vx);
+        const float Vy = 0.5f * (Vym + Vyp), Vz = 0.5f * (Vzm + Vzp);
+        const float inv2 = __frcp_rn(0.5f * (one_minus_vx(px, py, pz, inv_g) + omp));
         const float wq = wv[q] * inv2;
         const float djx = wq * a.djx0 * Vxm, djy = wq * a.djy0 * Vym, djz = wq * a.djz0 * Vzm;
         const float drho = wq * a.drho0;
@@ -634,8 +638,9 @@ __global__ void __launch_bounds__(32 * TY) push_cic_warp_kernel(PushArgs<float> 
                     }
                 }
                 const float inv_gp = rsqrtf(1.f + px * px + py * py + pz * pz);
-                const float Vxp = px * inv_gp, Vyp = py * inv_gp, Vzp = pz * inv_gp;
-                const float kE = a.sE * __frcp_rn(1.f - Vxp);
+                const float Vyp = py * inv_gp, Vzp = pz * inv_gp;
+                const float omp = one_minus_vx(px, py, pz, inv_gp);   // 1 - Vx before the kick
+                const float kE = a.sE * __frcp_rn(omp);
                 const float ex = g[0] * kE, ey = g[1] * kE, ez = g[2] * kE;
                 px += ex; py += ey; pz += ez;
                 const float kB = rsqrtf(1.f + px * px + py * py + pz * pz) * kE;
@@ -650,9 +655,8 @@ __global__ void __launch_bounds__(32 * TY) push_cic_warp_kernel(PushArgs<float> 
                 pz += ez + (p3x * by - p3y * bx);
                 const float inv_g = rsqrtf(1.f + px * px + py * py + pz * pz);
                 const float Vxm = px * inv_g, Vym = py * inv_g, Vzm = pz * inv_g;
-                const float Vx = 0.5f * (Vxm + Vxp), Vy = 0.5f * (Vym + Vyp),
-                            Vz = 0.5f * (Vzm + Vzp);
-                const float inv2 = __frcp_rn(1.f - Vx);
+                const float Vy = 0.5f * (Vym + Vyp), Vz = 0.5f * (Vzm + Vzp);
+                const float inv2 = __frcp_rn(0.5f * (one_minus_vx(px, py, pz, inv_g) + omp));
                 const float wq = w * inv2;
                 const float dq[4] = {wq * a.djx0 * Vxm, wq * a.djy0 * Vym, wq * a.djz0 * Vzm,
                                      wq * a.drho0};

@@ -189,14 +189,24 @@ def test_bad_buffers_are_rejected():
         with pytest.raises(abi.QsError):
             m.unpack_layer(buf[:-1])                           # not 12 P + 12 Np
         planes, parts = layout(buf.copy(), half)
+        cases = [((9, 0), half.ny, abi.QS_ERR_INVALID, "outside the layer"),        # cell j
+                 ((10, 5), 1.5, abi.QS_ERR_INVALID, "outside the layer"),           # k not whole
+                 ((4, 2), 1.25, abi.QS_ERR_PARTICLE_RANGE, "position"),              # in-cell y
+                 ((6, 3), 1.0, abi.QS_ERR_UNSUPPORTED, "species")]                   # Q2m
+        for (row, col), value, status, text in cases:
+            bad = buf.copy()
+            layout(bad, half)[1][row, col] = value
+            with pytest.raises(abi.QsError, match=text) as e:
+                m.unpack_layer(bad)
+            assert e.value.status == status
+            assert f"particle {col} " in str(e.value)   # the lowest bad row is named
+        # two bad rows: the lower one is reported
         bad = buf.copy()
-        layout(bad, half)[1][9, 0] = half.ny                    # cell j outside the layer
-        with pytest.raises(abi.QsError):
+        layout(bad, half)[1][4, 7] = -0.5
+        layout(bad, half)[1][9, 9] = -1.0
+        with pytest.raises(abi.QsError, match="particle 7 ") as e:
             m.unpack_layer(bad)
-        bad = buf.copy()
-        layout(bad, half)[1][6, 3] = 1.0                        # another species
-        with pytest.raises(abi.QsError):
-            m.unpack_layer(bad)
+        assert e.value.status == abi.QS_ERR_PARTICLE_RANGE
         m.unpack_layer(buf)
         m.clear_front_layer()
         m.load_front_plasma(wl.front_plasma(half, seed=5))
