@@ -12,12 +12,21 @@
  * RODFT11 definitions (FFTW 3 is a system library of the reference, not
  * vendored, version unpinned).
  *
- * Parity status: the transforms are pinned against scipy.fft dct/dst type 4
- * (the same published definitions) and direct O(N^2) sums; the push, solver
- * and beam are pinned by known-answer tests derived from the reference
- * formulas.  The reference itself cannot be built here (it needs FFTW3,
- * HDF5 and MPI), so no reference outputs pin them: parity unpinned for the
- * push/solver/beam beyond those known-answer tests.
+ * Parity status (the pins, each run by the tests):
+ *  - the plasma push with its deposit and guard fold, and the beam push with
+ *    its synchrotron loss and 3-D deposit, against the reference's own host
+ *    code (movepart_splitlayer.cpp:781-1544, 1685-1711; movebeam.cpp:14-774)
+ *    compiled from the reference checkout (oracle/ref_pin.cpp, make refpin):
+ *    particle states and cells bit for bit, deposits to the order of the
+ *    additions;
+ *  - the per-mode predictor and corrector against the reference's CUDA twins
+ *    of them (CUDA_WRAP/linearized.cu, oracle/ref_harness.cu, make ref);
+ *  - the transforms against scipy.fft dct/dst type 4 (FFTW's published
+ *    REDFT11 / RODFT11 definitions) and direct O(N^2) sums, FFTW itself being
+ *    a system dependency of the reference that is not present here;
+ *  - the march's orchestration (gathers, normalisation, the P / C layer
+ *    swaps) by its line-cited restatement and known answers: zero beam, the
+ *    linear response of the predictor's propagator, charge bookkeeping.
  */
 #ifndef QS_ORACLE_H
 #define QS_ORACLE_H

@@ -156,6 +156,7 @@ struct World {
     UnitsCGS* cgs = nullptr;
     Synchrotron* syn = nullptr;
     Specie* electrons = nullptr;
+    Specie* beam = nullptr;
     Specie* species[2] = {nullptr, nullptr};
 };
 
@@ -185,7 +186,7 @@ World make_world(const qs_config* c, int nx) {
     d->f_Ylength = c->hy * c->ny;
     d->f_Zlength = c->hz * c->nz;
     d->f_Wavelength = c->wavelength;
-    d->i_Nsorts = 1;
+    d->i_Nsorts = 2;
     d->f_BxExternal = c->bx_ext;
     d->f_ByExternal = c->by_ext;
     d->f_BzExternal = c->bz_ext;
@@ -212,11 +213,19 @@ World make_world(const qs_config* c, int nx) {
     s->i_ScatterFlag = 0;
     s->i_BeamFlag = 0;
     w.species[0] = s;
+    // the driver: a beam species (sort 1), electrons of the deck's q/m
+    w.beam = new Specie((char*)"Beam", nullptr);
+    w.beam->i_Sort = 1;
+    w.beam->f_q2m = c->beam_q2m;
+    w.beam->i_BeamFlag = 1;
+    w.beam->i_ScatterFlag = 0;
+    w.species[1] = w.beam;
     return w;
 }
 
 void free_world(World& w) {
     delete w.electrons;
+    delete w.beam;
     w.d->out_Flog.~basic_ofstream();
     w.d->out_Fig8.~basic_ofstream();
     ::operator delete(w.d);
@@ -321,6 +330,9 @@ int refpin_beam_push(const qs_config* c, int64_t nb, int32_t* bi, int32_t* bj, i
     world.syn->f_SynMin = c->synchrotron ? c->syn_min : 1e300;
     Mesh* m = make_mesh(L, My, Mz);
     m->p_CellArray = new Cell[m->l_sizeXYZ];
+    // each cell's per-species density (MoveBeamInCell adds the beam's into
+    // it); the Cell destructor frees it
+    for (long n = 0; n < m->l_sizeXYZ; n++) m->p_CellArray[n].f_DensArray = new double[2]();
     const size_t pl = (size_t)My * Mz;
     for (int i = 0; i <= L; i++)
         for (int k = -2; k < Mz + 2; k++)
@@ -332,7 +344,7 @@ int refpin_beam_push(const qs_config* c, int64_t nb, int32_t* bi, int32_t* bj, i
     std::vector<Particle*> parts((size_t)nb, nullptr);
     for (int64_t q = nb - 1; q >= 0; q--) {
         Particle* p = new Particle(nullptr, w[q], x[q], y[q], z[q], px[q], py[q], pz[q],
-                                   c->beam_q2m, 0);
+                                   c->beam_q2m, 1);
         m->p_CellArray[m->GetN(bi[q], bj[q], bk[q])].AddBeamParticle(p);
         parts[(size_t)q] = p;
     }
