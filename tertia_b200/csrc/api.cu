@@ -333,6 +333,10 @@ struct Engine : EngineBase {
     //       particle state, float fields and deposit)
     //    8  the real field planes of each layer rounded to float
     //   16  the beam currents rounded to float after the beam deposit
+    //   32  the front plasma (positions, momenta, weights) rounded to float
+    //       when it is seeded or loaded: the FP32 path's starting state
+    //   64  the plasma state rounded to float after every full push (its
+    //       storage in FP32, the push arithmetic in FP64)
     int fp32_study = 0;
     DttFft* study_fft = nullptr;
     float* study_f = nullptr;   // 40 planes: transform in / out / scratch, P and C fields, deposit
@@ -478,7 +482,7 @@ struct Engine : EngineBase {
                                                 "in [32, 1024]");
         }
         if (sizeof(T) == 8 && getenv("QS_FP32_STUDY")) {
-            fp32_study = atoi(getenv("QS_FP32_STUDY")) & 31;
+            fp32_study = atoi(getenv("QS_FP32_STUDY")) & 127;
             if (fp32_study & 1) {
                 study_fft = DttFft::create(My, Mz);
                 CK(cudaGetLastError());
@@ -525,6 +529,11 @@ struct Engine : EngineBase {
                                                       st);
                 });
         }
+    }
+    // the plasma arrays (with the weights when `weights`) rounded to float
+    void study_round_plasma(int bit, bool weights) {
+        T* arr[6] = {py, pz, ppx, ppy, ppz, pw};
+        for (int c = 0; c < (weights ? 6 : 5); c++) study_round(arr[c], (size_t)np, bit);
     }
     void study_round(T* x, size_t n, int bit) {
         if constexpr (sizeof(T) == 8) {
@@ -820,6 +829,7 @@ struct Engine : EngineBase {
             }
             CK(cudaStreamSynchronize(st));
         }
+        study_round_plasma(32, true);
         if ((s = cic_fresh_front())) return s;
         front_pending = true;
         return QS_OK;
@@ -872,6 +882,7 @@ struct Engine : EngineBase {
             return launch_seed_front<T>(sf, pcell, py, pz, ppx, ppy, ppz, pw, st);
         });
         CK(cudaGetLastError());
+        study_round_plasma(32, true);
         if ((s = cic_fresh_front())) return s;
         front_pending = true;
         return QS_OK;
@@ -1371,6 +1382,7 @@ struct Engine : EngineBase {
         const bool precise = sizeof(T) == 4;
         klaunch(KC_PUSH, [&] { return launch_push<T>(a, cfg.shape, precise, st); });
         CK(cudaGetLastError());
+        if (full) study_round_plasma(64, false);
         if (cic_sort && full && !adj_recompute) {
             if (regroup) {   // regroup before the next push
                 grp.grouped = false;
