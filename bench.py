@@ -431,17 +431,27 @@ def c2_study(precisions=("fp32", "bf16x3", "tf32x3", "bf16x6"), every=64, shape=
     names = ["Ex", "Ey", "Ez", "Bx", "By", "Bz", "rho"]
     sample = set(range(cfg.nx - 1, -1, -every))
 
-    def march(prec, ref=None):
+    head_lo = 3 * cfg.nx // 4     # the head quarter of the box: layers head_lo .. nx-1
+
+    def march(prec, ref=None, eps=0.0, study=None):
         c = cfg.copy()
         c.precision = PRECISIONS[prec]
-        m = Mesh(c)
-        m.load_beam(beam)
+        if study is not None:
+            os.environ["QS_FP32_STUDY"] = str(study)
+        try:
+            m = Mesh(c)
+        finally:
+            os.environ.pop("QS_FP32_STUDY", None)
+        b = dict(beam)
+        if eps:
+            b["w"] = np.asarray(beam["w"]) * (1.0 + eps)
+        m.load_beam(b)
         m.move_beam_particles()
         m.seed_front_plasma(0)
         m.begin_march()
         got = {}
-        num = np.zeros(7)
-        den = np.zeros(7)
+        num = np.zeros((2, 7))
+        den = np.zeros((2, 7))
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         for i in range(cfg.nx - 1, -1, -1):
@@ -452,9 +462,12 @@ def c2_study(precisions=("fp32", "bf16x3", "tf32x3", "bf16x6"), every=64, shape=
                 if ref is None:
                     got[i] = planes
                 else:
-                    for q in range(7):
-                        num[q] += float(np.sum((planes[q] - ref[i][q]) ** 2))
-                        den[q] += float(np.sum(ref[i][q] ** 2))
+                    for part in (0, 1):
+                        if part == 1 and i < head_lo:
+                            continue
+                        for q in range(7):
+                            num[part, q] += float(np.sum((planes[q] - ref[i][q]) ** 2))
+                            den[part, q] += float(np.sum(ref[i][q] ** 2))
             m.layer_end(i, 0)
         torch.cuda.synchronize()
         dt = time.perf_counter() - t0
@@ -462,20 +475,35 @@ def c2_study(precisions=("fp32", "bf16x3", "tf32x3", "bf16x6"), every=64, shape=
         m.close()
         if ref is None:
             return got, ex, dt
-        return {n: float(np.sqrt(num[q] / den[q])) for q, n in enumerate(names)}, ex, dt
+        errs = {part: {n: float(np.sqrt(num[p_, q] / den[p_, q])) for q, n in enumerate(names)}
+                for p_, part in enumerate(("whole_box", "head_quarter"))}
+        return errs, ex, dt
 
     ref, ex64, t64 = march("fp64fft")
+    rel = lambda a, b: float(np.linalg.norm(a - b) / np.linalg.norm(b))
     out = {"workload": "c2: 1024x1024x2048, 4 ppc, n_b/n_0 = 1, 4e6 driver particles, "
                        f"{shape.upper()}, one beam step",
            "reference": "FP64 with FFT transforms (QS_PREC_FP64_FFT)",
-           "sampled_layers": len(sample), "every": every,
+           "sampled_layers": len(sample), "every": every, "head_quarter_from_layer": head_lo,
            "fields": names, "march_s": {"fp64fft": t64}, "per_field_rel_l2": {},
-           "ez_onaxis_rel_l2": {}}
+           "ez_onaxis_rel_l2": {}, "ez_onaxis_rel_l2_head_quarter": {}}
+    head = slice(head_lo, None)
     for prec in precisions:
         err, ex, dt = march(prec, ref)
         out["per_field_rel_l2"][prec] = err
-        out["ez_onaxis_rel_l2"][prec] = float(np.linalg.norm(ex - ex64) / np.linalg.norm(ex64))
+        out["ez_onaxis_rel_l2"][prec] = rel(ex, ex64)
+        out["ez_onaxis_rel_l2_head_quarter"][prec] = rel(ex[head], ex64[head])
         out["march_s"][prec] = dt
+    # floors: FP64 against itself with the beam weights x (1 + 6e-8), and
+    # with only the front plasma's starting state rounded to float (what any
+    # FP32 representation of the plasma starts from)
+    floors = {}
+    for tag, kw in (("fp64_beam_weights_x(1+6e-8)", {"eps": 6e-8}),
+                    ("fp64_front_plasma_rounded_to_float", {"study": 32})):
+        err, ex, _ = march("fp64fft", ref, **kw)
+        floors[tag] = {"per_field_rel_l2": err, "ez_onaxis_rel_l2": rel(ex, ex64),
+                       "ez_onaxis_rel_l2_head_quarter": rel(ex[head], ex64[head])}
+    out["floors"] = floors
     out["timing"] = ("host clock around the layer-by-layer march (eager launches and the plane "
                      "reads of the sampled layers included): for scale only")
     return out

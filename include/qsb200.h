@@ -264,6 +264,28 @@ qs_status qs_get_onaxis_ex(qs_handle* h, double* out);
  * compute: psi(nx) = 0, psi(i) = psi(i+1) + hx (Ex_i + Ex_{i+1})/2 on axis. */
 qs_status qs_get_psi(qs_handle* h, double* out);
 
+/* Layer output.  The reference writes HDF5 (Mesh::Save's field file,
+ * save.cpp:520-838, vsNNN_3d_fields.h5; Mesh::SaveCadrMovie2's frames,
+ * mesh.cpp:976-1090); HDF5 is not part of this library, so the same datasets
+ * go into a plain self-describing file, QSF1 (little-endian):
+ *   bytes 0-7   "QSF1" and four zero bytes
+ *   int32 ndatasets, int32 0
+ *   ndatasets entries of 72 bytes: char name[32] (zero padded), int32 dtype
+ *   (1 int32, 2 float64), int32 rank, int64 dims[3] (fastest first, unused
+ *   ones 1), int64 byte offset of the data in the file
+ *   the data blocks (8-byte aligned)
+ * qs_save_fields: "meshinfo" (16 int32: Mx, 0, Mx, 0, My, 0, My, 0, Mz, 0,
+ * Mz, 0 and four zeros, the reference's l_Mx, l_dMx, l_sizeX, l_offsetX ...
+ * without guard cells), "phase", the axes "X" (i hx + phase), "Y"
+ * (j hy - Ylength/2), "Z", and the 3-D arrays "Ex" "Ey" "Ez" "Bx" "By" "Bz"
+ * (and "Jx" "Jy" "Jz" "Dens" with store_sources = 1) of the field store, dims
+ * (nx, ny, nz), the layer index fastest as in the reference's files.
+ * qs_save_movie_frame: the same axes and, for each of those quantities, its
+ * plane through the axis in (x, y) at z = nz/2 ("Ex_xy", dims (nx, ny)) and
+ * in (x, z) at y = ny/2 ("Ex_xz", dims (nx, nz)).  Both are synchronous. */
+qs_status qs_save_fields(qs_handle* h, const char* path);
+qs_status qs_save_movie_frame(qs_handle* h, const char* path);
+
 /* No counterpart in the reference (which has no such diagnostic; the planes
  * summed are those its Cell array stores).  FP64 global charge sums of every
  * layer of the last march, computed on the device in FP64 whatever the

@@ -22,6 +22,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <functional>
 #include <new>
 #include <string>
 #include <vector>
@@ -178,6 +179,7 @@ struct EngineBase {
     virtual qs_status unpack_layer(const double*, int64_t) = 0;
     virtual qs_status clear_front_layer() = 0;
     virtual qs_status get_charge_sums(double*, double*, double*) = 0;
+    virtual qs_status save_output(const char*, bool movie) = 0;
 
     qs_status check_device() {
         cudaError_t e = cudaStreamSynchronize(st);
@@ -1472,6 +1474,142 @@ struct Engine : EngineBase {
         a.qcz = q_cz;
     }
 
+    // ------------------------------------------------------- layer output
+    // Mesh::Save's field file (save.cpp:520-838) and Mesh::SaveCadrMovie2's
+    // central slices (mesh.cpp:976-1090), in the QSF1 layout of qsb200.h:
+    // the reference's dataset names, x (the layer index) fastest.
+    qs_status save_output(const char* path, bool movie) override {
+        if (!path) return fail(QS_ERR_INVALID, "qs_save: null path");
+        struct Set {
+            std::string name;
+            int dtype;               // 1 int32, 2 float64
+            int64_t d[3];
+            std::function<qs_status(FILE*)> write;
+        };
+        std::vector<Set> sets;
+        auto host_set = [&](const char* name, std::vector<double> v) {
+            const int64_t n = (int64_t)v.size();
+            sets.push_back({name, 2, {n, 1, 1}, [v](FILE* f) {
+                                return fwrite(v.data(), sizeof(double), v.size(), f) == v.size()
+                                           ? QS_OK : QS_ERR_INVALID;
+                            }});
+        };
+        {
+            // meshinfo: l_Mx, l_dMx, l_sizeX, l_offsetX and the same for y and
+            // z (no guard cells here), then four zeros
+            std::vector<int32_t> mi = {L, 0, L, 0, My, 0, My, 0, Mz, 0, Mz, 0, 0, 0, 0, 0};
+            sets.push_back({"meshinfo", 1, {16, 1, 1}, [mi](FILE* f) {
+                                return fwrite(mi.data(), sizeof(int32_t), mi.size(), f) ==
+                                               mi.size() ? QS_OK : QS_ERR_INVALID;
+                            }});
+        }
+        host_set("phase", {phase});
+        {
+            std::vector<double> X(L), Y(My), Z(Mz);
+            for (int i = 0; i < L; i++) X[i] = cfg.hx * i + phase;
+            for (int j = 0; j < My; j++) Y[j] = cfg.hy * j - My * cfg.hy / 2.;
+            for (int k = 0; k < Mz; k++) Z[k] = cfg.hz * k - Mz * cfg.hz / 2.;
+            host_set("X", X);
+            host_set("Y", Y);
+            host_set("Z", Z);
+        }
+        // a block of the store in x-fastest order through the staging buffer
+        const size_t cap = 8 * plane;
+        auto gathered = [this, cap](const T* base, size_t stride, int j0, int nj, int k0, int nk,
+                                    FILE* f) -> qs_status {
+            std::vector<double> h;
+            const size_t row = (size_t)L * nj;           // one kk of the block
+            for (int kk = 0; kk < nk;) {
+                int nkc = (int)std::max<size_t>(1, cap / std::max<size_t>(row, 1));
+                nkc = std::min(nkc, nk - kk);
+                if (row > cap) {                          // a row in pieces of whole x runs
+                    const int njc = (int)std::max<size_t>(1, cap / L);
+                    for (int jj = 0; jj < nj; jj += njc) {
+                        const int n = std::min(njc, nj - jj);
+                        klaunch(KC_MISC, [&] {
+                            return launch_gather_xfast<T>(base, stride, L, My, j0 + jj, n,
+                                                          k0 + kk, 1, stage_d, st);
+                        });
+                        h.resize((size_t)L * n);
+                        CK(cudaMemcpyAsync(h.data(), stage_d, h.size() * 8, cudaMemcpyDeviceToHost,
+                                           st));
+                        CK(cudaStreamSynchronize(st));
+                        if (fwrite(h.data(), 8, h.size(), f) != h.size()) return QS_ERR_INVALID;
+                    }
+                    kk += 1;
+                    continue;
+                }
+                klaunch(KC_MISC, [&] {
+                    return launch_gather_xfast<T>(base, stride, L, My, j0, nj, k0 + kk, nkc,
+                                                  stage_d, st);
+                });
+                h.resize(row * nkc);
+                CK(cudaMemcpyAsync(h.data(), stage_d, h.size() * 8, cudaMemcpyDeviceToHost, st));
+                CK(cudaStreamSynchronize(st));
+                if (fwrite(h.data(), 8, h.size(), f) != h.size()) return QS_ERR_INVALID;
+                kk += nkc;
+            }
+            return QS_OK;
+        };
+        struct Src { const char* name; const T* base; size_t stride; };
+        std::vector<Src> srcs = {{"Ex", f3, 6 * plane}, {"Ey", f3 + plane, 6 * plane},
+                                 {"Ez", f3 + 2 * plane, 6 * plane}, {"Bx", f3 + 3 * plane, 6 * plane},
+                                 {"By", f3 + 4 * plane, 6 * plane}, {"Bz", f3 + 5 * plane, 6 * plane}};
+        if (src3) {   // the sources of every layer (kept with store_sources = 1)
+            srcs.push_back({"Jx", src3, 4 * plane});
+            srcs.push_back({"Jy", src3 + plane, 4 * plane});
+            srcs.push_back({"Jz", src3 + 2 * plane, 4 * plane});
+            srcs.push_back({"Dens", src3 + 3 * plane, 4 * plane});
+        }
+        for (const Src& q : srcs) {
+            if (!movie) {
+                sets.push_back({q.name, 2, {L, My, Mz}, [=](FILE* f) {
+                                    return gathered(q.base, q.stride, 0, My, 0, Mz, f);
+                                }});
+            } else {   // the (x, y) plane through the axis and the (x, z) plane
+                sets.push_back({std::string(q.name) + "_xy", 2, {L, My, 1}, [=](FILE* f) {
+                                    return gathered(q.base, q.stride, 0, My, Mz / 2, 1, f);
+                                }});
+                sets.push_back({std::string(q.name) + "_xz", 2, {L, Mz, 1}, [=](FILE* f) {
+                                    return gathered(q.base, q.stride, My / 2, 1, 0, Mz, f);
+                                }});
+            }
+        }
+        // header: magic, count, then one 72-byte entry per set (name[32],
+        // dtype, rank, dims[3] fastest first, byte offset of the data)
+        const int64_t hdr = 16 + 72 * (int64_t)sets.size();
+        std::vector<int64_t> off(sets.size());
+        int64_t pos = hdr;
+        for (size_t d = 0; d < sets.size(); d++) {
+            off[d] = pos;
+            const int64_t n = sets[d].d[0] * sets[d].d[1] * sets[d].d[2];
+            pos += n * (sets[d].dtype == 1 ? 4 : 8);
+            pos = (pos + 7) & ~(int64_t)7;
+        }
+        FILE* f = fopen(path, "wb");
+        if (!f) return fail(QS_ERR_INVALID, "qs_save: cannot open %s", path);
+        bool ok = fwrite("QSF1\0\0\0\0", 1, 8, f) == 8;
+        const int32_t cnt[2] = {(int32_t)sets.size(), 0};
+        ok = ok && fwrite(cnt, 4, 2, f) == 2;
+        for (size_t d = 0; d < sets.size() && ok; d++) {
+            char name[32] = {};
+            std::strncpy(name, sets[d].name.c_str(), 31);
+            const int rank = sets[d].d[2] > 1 ? 3 : (sets[d].d[1] > 1 ? 2 : 1);
+            const int32_t ty[2] = {sets[d].dtype, rank};
+            ok = fwrite(name, 1, 32, f) == 32 && fwrite(ty, 4, 2, f) == 2 &&
+                 fwrite(sets[d].d, 8, 3, f) == 3 && fwrite(&off[d], 8, 1, f) == 1;
+        }
+        qs_status s = ok ? QS_OK : QS_ERR_INVALID;
+        for (size_t d = 0; d < sets.size() && !s; d++) {
+            if (fseek(f, (long)off[d], SEEK_SET) != 0) s = QS_ERR_INVALID;
+            else s = sets[d].write(f);
+        }
+        if (fclose(f) != 0 && !s) s = QS_ERR_INVALID;
+        if (s == QS_ERR_INVALID) return fail(s, "qs_save: write to %s failed", path);
+        if (s) return s;
+        return check_device();
+    }
+
     qs_status get_charge_sums(double* rho, double* jx, double* rho_beam) override {
         // the plasma sums of the layers marched so far (the march also runs
         // this reduction at its end)
@@ -2633,6 +2771,15 @@ qs_status qs_get_onaxis_ex(qs_handle* h, double* out) {
     H_OR_INVALID(h);
     return E->get_onaxis(out);
 }
+qs_status qs_save_fields(qs_handle* h, const char* path) {
+    H_OR_INVALID(h);
+    return E->save_output(path, false);
+}
+qs_status qs_save_movie_frame(qs_handle* h, const char* path) {
+    H_OR_INVALID(h);
+    return E->save_output(path, true);
+}
+
 qs_status qs_get_charge_sums(qs_handle* h, double* rho, double* jx, double* rho_beam) {
     H_OR_INVALID(h);
     return E->get_charge_sums(rho, jx, rho_beam);

@@ -67,6 +67,12 @@ int launch_charge_reduce(const double* part, int nparts, int nlayers, double sca
 
 template <class T>
 int launch_onaxis(const T* fields3d, int L, size_t plane, size_t idx, T* out, cudaStream_t st);
+// a block of a 3-D store (L layers, `layer_stride` values apart, planes of
+// rows of My) in x-fastest order, widened to double:
+// out[i + L (jj + nj kk)] = base[i * layer_stride + (j0 + jj) + My (k0 + kk)]
+template <class T>
+int launch_gather_xfast(const T* base, size_t layer_stride, int L, int My, int j0, int nj, int k0,
+                        int nk, double* out, cudaStream_t st);
 
 // Front-layer seeding (Mesh::SeedParticles, mesh.cpp:413-548): ppc
 // particles per cell on the in-cell lattice, thermal momenta from a

@@ -359,6 +359,30 @@ int launch_convert_back(const T* src, double* dst, size_t n, cudaStream_t st) {
     return 1;
 }
 
+// ---- layer output: a block of the 3-D store in x-fastest order
+// out[i + L (jj + nj kk)] = base[i * layer_stride + (j0 + jj) + My (k0 + kk)]
+template <class T>
+__global__ void gather_xfast_kernel(const T* __restrict__ base, size_t layer_stride, int L,
+                                    int My, int j0, int nj, int k0, int nk,
+                                    double* __restrict__ out) {
+    const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const size_t total = (size_t)L * nj * nk;
+    if (idx >= total) return;
+    const int i = (int)(idx % L);
+    const size_t rest = idx / L;
+    const int jj = (int)(rest % nj), kk = (int)(rest / nj);
+    out[idx] = (double)base[(size_t)i * layer_stride + (size_t)(j0 + jj) + (size_t)My * (k0 + kk)];
+}
+template <class T>
+int launch_gather_xfast(const T* base, size_t layer_stride, int L, int My, int j0, int nj, int k0,
+                        int nk, double* out, cudaStream_t st) {
+    const size_t total = (size_t)L * nj * nk;
+    if (!total) return 0;
+    gather_xfast_kernel<T><<<(unsigned)((total + 255) / 256), 256, 0, st>>>(
+        base, layer_stride, L, My, j0, nj, k0, nk, out);
+    return 1;
+}
+
 // ---- the FP32 attribution study of the FP64 engine (see api.cu)
 __global__ void round_f32_kernel(double* __restrict__ x, size_t n) {
     const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -386,6 +410,8 @@ int launch_add_widened(double* dst, const float* src, size_t n, cudaStream_t st)
     template int launch_beam_layer<T>(const T*, const T*, int, int, T*, size_t, int*,           \
                                       cudaStream_t);                                            \
     template int launch_onaxis<T>(const T*, int, size_t, size_t, T*, cudaStream_t);            \
+    template int launch_gather_xfast<T>(const T*, size_t, int, int, int, int, int, int, double*, \
+                                        cudaStream_t);                                          \
     template int launch_beam_check<T>(const T*, int, size_t, int*, double*, cudaStream_t);     \
     template int launch_seed_front<T>(const SeedFront&, int32_t*, T*, T*, T*, T*, T*, T*,       \
                                       cudaStream_t);                                            \

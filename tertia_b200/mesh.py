@@ -243,6 +243,16 @@ class Mesh:
                                              _p(b, C.c_double)), "qs_get_charge_sums")
         return {"rho": r, "jx": j, "rho_beam": b}
 
+    def save_fields(self, path: str):
+        """Mesh::Save's field file (save.cpp:520-838) as a QSF1 file at
+        `path` (read it with tertia_b200.fields_io.read_qsf)."""
+        self._chk(self._L.qs_save_fields(self._h, str(path).encode()), "qs_save_fields")
+
+    def save_movie_frame(self, path: str):
+        """Mesh::SaveCadrMovie2's central slices as a QSF1 file at `path`."""
+        self._chk(self._L.qs_save_movie_frame(self._h, str(path).encode()),
+                  "qs_save_movie_frame")
+
     # -------------------------------------------------------------- the path
     @_changes_state
     def step(self):
