@@ -303,7 +303,7 @@ def adjoint_measure(precision: str):
 # ------------------------------------------------------------------ FP64 comparison
 STUDY_BITS = (("transforms", 1), ("spectral_state", 2), ("push", 4), ("fields", 8),
               ("beam_currents", 16), ("front_plasma_input", 32), ("particle_state_storage", 64),
-              ("all", 31))
+              ("push_arithmetic", 128), ("all", 31))
 
 
 def fp64_compare(cfg, beam, pushes_per_step, ours_ms):
@@ -394,8 +394,9 @@ def fp64_compare(cfg, beam, pushes_per_step, ours_ms):
                 "push through the FP32 push kernel on float particles and fields; the real "
                 "field planes rounded to float; the beam currents rounded to float; only the "
                 "front plasma's starting state rounded to float; the plasma state rounded to "
-                "float after every full push of an FP64 push), on-axis Ez after two beam steps "
-                "against the plain FP64-FFT march"}
+                "float after every full push of an FP64 push; the FP32 push kernel's increments "
+                "added to an FP64 state), on-axis Ez after two beam steps against the plain "
+                "FP64-FFT march"}
     out["ez_note"] = ("on-axis Ex (the reference's longitudinal field) over all layers after 2 "
                       "beam steps; head quarter = the 1/4 of the layers nearest the front")
     return out

@@ -339,10 +339,13 @@ struct Engine : EngineBase {
     //       when it is seeded or loaded: the FP32 path's starting state
     //   64  the plasma state rounded to float after every full push (its
     //       storage in FP32, the push arithmetic in FP64)
+    //  128  the push through the FP32 push kernel as with 4, but the FP64
+    //       state takes the push's increments (its arithmetic in FP32, its
+    //       storage in FP64)
     int fp32_study = 0;
     DttFft* study_fft = nullptr;
     float* study_f = nullptr;   // 40 planes: transform in / out / scratch, P and C fields, deposit
-    float* study_p = nullptr;   // 6 x np_cap particle values
+    float* study_p = nullptr;   // 11 x np_cap: 6 particle values, 5 of them before the push
 
     // the hand-off buffer assembled on the device, and its ordering scratch
     double* d_pack = nullptr;
@@ -484,7 +487,7 @@ struct Engine : EngineBase {
                                                 "in [32, 1024]");
         }
         if (sizeof(T) == 8 && getenv("QS_FP32_STUDY")) {
-            fp32_study = atoi(getenv("QS_FP32_STUDY")) & 127;
+            fp32_study = atoi(getenv("QS_FP32_STUDY")) & 255;
             if (fp32_study & 1) {
                 study_fft = DttFft::create(My, Mz);
                 CK(cudaGetLastError());
@@ -580,13 +583,24 @@ struct Engine : EngineBase {
             a.invMy = 1.0f / (float)My;
             a.full = full;
             a.err = d_err;
+            float* before = study_p + 6 * (size_t)np_cap;   // the float state before the push
+            if ((fp32_study & 128) && full)
+                CK(cudaMemcpyAsync(before, study_p, 5 * (size_t)np_cap * sizeof(float),
+                                   cudaMemcpyDeviceToDevice, st));
             klaunch(KC_PUSH, [&] { return launch_push<float>(a, cfg.shape, true, st); });
             klaunch(KC_MISC, [&] { return launch_add_widened(Csrc, fdep, 4 * plane, st); });
             if (full)
-                for (int c = 0; c < 5; c++)
-                    klaunch(KC_MISC, [&] {
-                        return launch_convert_back<float>(fp[c], dsrc[c], np, st);
-                    });
+                for (int c = 0; c < 5; c++) {
+                    if (fp32_study & 128)   // the FP64 state takes the increment
+                        klaunch(KC_MISC, [&] {
+                            return launch_add_increment(dsrc[c], fp[c], before + (size_t)c * np_cap,
+                                                        np, c < 2, st);
+                        });
+                    else
+                        klaunch(KC_MISC, [&] {
+                            return launch_convert_back<float>(fp[c], dsrc[c], np, st);
+                        });
+                }
             CK(cudaGetLastError());
         }
         return QS_OK;
@@ -718,10 +732,10 @@ struct Engine : EngineBase {
             if ((s = alloc(&pid, n, "plasma"))) return s;
             if ((s = alloc(&apid, n, "plasma"))) return s;
         }
-        if (fp32_study & 4) {
+        if (fp32_study & (4 | 128)) {
             if (study_p) cudaFree(study_p);
             study_p = nullptr;
-            if ((s = alloc(&study_p, 6 * (size_t)n, "FP32 study"))) return s;
+            if ((s = alloc(&study_p, 11 * (size_t)n, "FP32 study"))) return s;
         }
         np_cap = n;
         if (gexec) {  // the captured march baked the old pointers
@@ -1342,7 +1356,7 @@ struct Engine : EngineBase {
 
     qs_status push(int iLayer, int iSplit, int full) override {
         (void)iLayer; (void)iSplit;
-        if (fp32_study & 4) return study_push(full);
+        if (fp32_study & (4 | 128)) return study_push(full);
         // ClearCurrentsSplit: inside the march the preceding spectral kernel
         // already cleared Csrc
         if (!clear_by_maps()) CK(cudaMemsetAsync(Csrc, 0, 4 * plane * sizeof(T), st));

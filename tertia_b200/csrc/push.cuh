@@ -513,26 +513,26 @@ __global__ void __launch_bounds__(128) push_cell_kernel(PushArgs<float> a) {
 
 // ---------------------------------------------------------------------------
 // FP32 CIC push over particles grouped by cell (the counting sort in sort.cu
-// regroups them every few full pushes).  A block owns a tile of 32 x TY cells,
-// one warp per row of 32 cells, and stages the four corners of each tile
-// cell's fields (P and C averaged) in shared memory for the gather.
-//
-// Each lane takes a chunk of 4 consecutive particles of its warp's row (the
-// row's particles are contiguous, 4 per cell on average), loaded and stored as
-// float4 / int4 vectors, and pushes them one after another.  Consecutive
-// particles mostly deposit into the same cell, so the lane sums the ND x 4
-// corner values of a run of equal destination cell in registers and adds them
-// into the block's deposit tile (shared memory atomics) only when the cell
-// changes: no per-particle shuffle reduction, and the per-batch overhead
-// (loads, range and key bookkeeping, the flush) is paid once per 4 particles.
-// The tile is flushed with one global atomic per touched node and current.
-// Particles whose cell or deposit lies outside the tile (moved since the last
-// regrouping) gather and deposit through global memory.  ND = 3 leaves out the
-// density deposit, which the march does not read.  The full push stores the
-// particles in place with their new cell and, when a regrouping follows,
-// counts the new cells.  Same physics as push_kernel<float, CIC, precise,
-// fast> (movepart_layer_CIC.cpp:165-193, 449-496 weights) with approximate
-// reciprocals for the divisions and 1 - Vx in its cancellation-free form.
+// regroups them every few full pushes).  A block owns a tile of 32 x TY
+// cells, one warp per row of 32 cells; the warp pushes the particles of its
+// row 32 at a time (particle-parallel, so dense and empty cells do not
+// unbalance it).  The block stages the four corners of each tile cell's
+// fields (P and C averaged) in shared memory for the gather.  Deposits: the
+// warp sums the ND x 4 corner values over runs of lanes whose particles
+// deposit into the same cell (3-level segmented shuffle reduction, chunks of
+// up to 8 lanes), merges chunks that share a cell (match), and one lane per
+// cell adds them to the warp's per-cell accumulator in shared memory - no
+// shared-memory atomics.  At the end each lane spreads its cell's corner
+// values (the right-hand corners through a shuffle to the next lane), the
+// warps combine their rows in the block tile in two ordered phases, and the
+// tile is flushed with one global atomic per touched cell and current.
+// Particles whose cell or deposit lies outside the warp's row (moved since
+// the last regrouping) gather and deposit through global memory.  ND = 3
+// leaves out the density deposit, which the march does not read.  The full
+// push stores the particles in place with their new cell and, when a
+// regrouping follows, counts the new cells.  Same physics as
+// push_kernel<float, CIC, precise, fast> (movepart_layer_CIC.cpp:165-193,
+// 449-496 weights) with approximate reciprocals for the divisions.
 __device__ __forceinline__ int cell_offset(const PushArgs<float>& a, int c) {
     return a.loff[c] + a.bpref[c >> 10];
 }
@@ -558,204 +558,227 @@ __device__ __forceinline__ void cic_substep(float dy, float dz, float ps, float&
     wc[3] = ry * rz;
 }
 
-// the 4 x ND corner values v (index corner * ND + current) of cell (j, k)
-// into the block tile T (tile-local cell (tj, tk)) or, outside the tile,
-// straight to the global deposit
 template <int TY, int ND>
-__device__ __forceinline__ void cic_flush(const PushArgs<float>& a, float (*T)[TY + 1][33],
-                                          int key, int j0, int k0, const float (&v)[4 * ND]) {
-    const int My = a.My, Mz = a.Mz;
-    int j, k;
-    cell_jk(key, My, a.invMy, j, k);
-    const int tj = j - j0, tk = k - k0;
-    if (tj >= 0 && tj < 32 && tk >= 0 && tk < TY) {
-#pragma unroll
-        for (int d = 0; d < ND; d++) {
-            atomicAdd(&T[d][tk][tj], v[0 * ND + d]);
-            atomicAdd(&T[d][tk][tj + 1], v[1 * ND + d]);
-            atomicAdd(&T[d][tk + 1][tj], v[2 * ND + d]);
-            atomicAdd(&T[d][tk + 1][tj + 1], v[3 * ND + d]);
-        }
-    } else {
-        const size_t plane = a.plane;
-        const int j1 = wrap1(j + 1, My), k1 = wrap1(k + 1, Mz);
-        const size_t nd[4] = {(size_t)j + (size_t)My * k, (size_t)j1 + (size_t)My * k,
-                              (size_t)j + (size_t)My * k1, (size_t)j1 + (size_t)My * k1};
-#pragma unroll
-        for (int r = 0; r < 4; r++)
-#pragma unroll
-            for (int d = 0; d < ND; d++) atomicAdd(a.dep + d * plane + nd[r], v[r * ND + d]);
-    }
-}
-
-// blocks per SM the register allocation of the chunk kernel is bounded for
-#ifndef QS_PUSH_CHUNK_MINB
-#define QS_PUSH_CHUNK_MINB 1
-#endif
-
-template <int TY, int ND>
-__global__ void __launch_bounds__(32 * TY, QS_PUSH_CHUNK_MINB)
-    push_cic_chunk_kernel(PushArgs<float> a) {
-    constexpr int TX = 32, W = TX + 1, H = TY + 1, NV = 4 * ND, CH = 4;
-    __shared__ float Fs[6][H][W];   // fields of the tile cells + one row/column (P, C averaged)
-    __shared__ float T[ND][H][W];   // block deposit tile [current][row][col]
+__global__ void __launch_bounds__(32 * TY) push_cic_warp_kernel(PushArgs<float> a) {
+    constexpr int TX = 32, W = TX + 1, H = TY + 1, NV = 4 * ND;
+    __shared__ float Fs[6][H][W];        // fields of the tile cells + one row/column (P, C averaged)
+    __shared__ float Acc[TY][NV][TX];    // per-warp sums [corner*ND + current][cell]
+    __shared__ float T[ND][H][W];        // block deposit tile [current][row][col]
     const int lane = threadIdx.x & 31, wr = threadIdx.x >> 5;
     const int My = a.My, Mz = a.Mz;
     const size_t plane = a.plane;
     const int tiles_x = My / TX;
     const int j0 = (blockIdx.x % tiles_x) * TX, k0 = (blockIdx.x / tiles_x) * TY;
     for (int i = threadIdx.x; i < ND * H * W; i += 32 * TY) (&T[0][0][0])[i] = 0.f;
+#pragma unroll
+    for (int i = 0; i < NV; i++) Acc[wr][i][lane] = 0.f;
     pdl_wait();
     for (int i = threadIdx.x; i < H * W; i += 32 * TY) {
         const int r = i / W, cc = i - r * W;
         const size_t m = (size_t)wrap1(j0 + cc, My) + (size_t)My * wrap1(k0 + r, Mz);
 #pragma unroll
-        for (int f = 0; f < 6; f++)
-            Fs[f][r][cc] = 0.5f * (ld(a.P + f * plane + m) + ld(a.C + f * plane + m));
+        for (int f = 0; f < 6; f++) Fs[f][r][cc] = 0.5f * (ld(a.P + f * plane + m) + ld(a.C + f * plane + m));
     }
     __syncthreads();
+    const unsigned full = 0xffffffffu;
     const int c0 = j0 + My * (k0 + wr);   // this warp's 32 cells: c0 .. c0+31
     const int pbeg = cell_offset(a, c0);
     const int pend = (size_t)(c0 + TX) < plane ? cell_offset(a, c0 + TX) : (int)a.n;
-    int acc_key = -1;                     // destination cell of the run being summed
-    float acc[NV];
+    // the particle of the next pass is loaded while this one is pushed
+    int nx_cell = 0;
+    float nx_y = 0.f, nx_z = 0.f, nx_px = 0.f, nx_py = 0.f, nx_pz = 0.f, nx_w = 0.f;
+    if (pbeg + lane < pend) {
+        const int q = pbeg + lane;
+        nx_cell = a.cell[q]; nx_y = a.y[q]; nx_z = a.z[q];
+        nx_px = a.px[q]; nx_py = a.py[q]; nx_pz = a.pz[q]; nx_w = a.w[q];
+    }
+    for (int base = pbeg; base < pend; base += 32) {
+        const int p = base + lane;
+        const int cell = nx_cell;
+        const float yp = nx_y, zp = nx_z, w = nx_w;
+        float px = nx_px, py = nx_py, pz = nx_pz;
+        if (p + 32 < pend) {
+            const int q = p + 32;
+            nx_cell = a.cell[q]; nx_y = a.y[q]; nx_z = a.z[q];
+            nx_px = a.px[q]; nx_py = a.py[q]; nx_pz = a.pz[q]; nx_w = a.w[q];
+        }
+        int key = -1;                     // destination cell of the first sub-step
+        float v[NV];
 #pragma unroll
-    for (int i = 0; i < NV; i++) acc[i] = 0.f;
-    for (int base = pbeg & ~(CH - 1); base < pend; base += CH * 32) {
-        const int q = base + CH * lane;   // this lane's particles q .. q+3 (16-byte aligned)
-        if (q >= pend) break;             // the lanes above are past the row
-        float4 Y = *reinterpret_cast<const float4*>(a.y + q);
-        float4 Z = *reinterpret_cast<const float4*>(a.z + q);
-        float4 PX = *reinterpret_cast<const float4*>(a.px + q);
-        float4 PY = *reinterpret_cast<const float4*>(a.py + q);
-        float4 PZ = *reinterpret_cast<const float4*>(a.pz + q);
-        const float4 Wt = __ldg(reinterpret_cast<const float4*>(a.w + q));
-        int4 CL = *reinterpret_cast<const int4*>(a.cell + q);
-        float* yv = &Y.x; float* zv = &Z.x; float* pxv = &PX.x; float* pyv = &PY.x;
-        float* pzv = &PZ.x; const float* wv = &Wt.x; int* cv = &CL.x;
-#pragma unroll
-        for (int s = 0; s < CH; s++) {
-            const int p = q + s;
-            if (p < pbeg || p >= pend) continue;
-            const int cell = cv[s];
-            const float yp = yv[s], zp = zv[s];
+        for (int i = 0; i < NV; i++) v[i] = 0.f;
+        if (p < pend) {
             if (!(yp >= 0.f && yp <= 1.f && zp >= 0.f && zp <= 1.f)) {
                 atomicOr(a.err, DEV_ERR_RANGE);
                 if (a.full && a.cnt) atomicAdd(a.cnt + cell, 1);   // it stays in its cell
-                continue;
-            }
-            float px = pxv[s], py = pyv[s], pz = pzv[s];
-            int j, k;
-            cell_jk(cell, My, a.invMy, j, k);
-            const float wg[4] = {(1.f - yp) * (1.f - zp), yp * (1.f - zp), (1.f - yp) * zp,
-                                 yp * zp};
-            float g[6];
-            const int tj = j - j0, tk = k - k0;
-            if (tj >= 0 && tj < TX && tk >= 0 && tk < TY) {
-#pragma unroll
-                for (int f = 0; f < 6; f++)
-                    g[f] = wg[0] * Fs[f][tk][tj] + wg[1] * Fs[f][tk][tj + 1] +
-                           wg[2] * Fs[f][tk + 1][tj] + wg[3] * Fs[f][tk + 1][tj + 1];
             } else {
-                const int j1 = wrap1(j + 1, My), k1 = wrap1(k + 1, Mz);
-                const size_t nn[4] = {(size_t)j + (size_t)My * k, (size_t)j1 + (size_t)My * k,
-                                      (size_t)j + (size_t)My * k1, (size_t)j1 + (size_t)My * k1};
+                int j, k;
+                cell_jk(cell, My, a.invMy, j, k);
+                const float wg[4] = {(1.f - yp) * (1.f - zp), yp * (1.f - zp), (1.f - yp) * zp,
+                                     yp * zp};
+                float g[6];
+                const int tj = j - j0, tk = k - k0;
+                if (tj >= 0 && tj < TX && tk >= 0 && tk < TY) {
 #pragma unroll
-                for (int f = 0; f < 6; f++) {
-                    float gs = 0.f;
+                    for (int f = 0; f < 6; f++)
+                        g[f] = wg[0] * Fs[f][tk][tj] + wg[1] * Fs[f][tk][tj + 1] +
+                               wg[2] * Fs[f][tk + 1][tj] + wg[3] * Fs[f][tk + 1][tj + 1];
+                } else {
+                    const int j1 = wrap1(j + 1, My), k1 = wrap1(k + 1, Mz);
+                    const size_t nn[4] = {(size_t)j + (size_t)My * k, (size_t)j1 + (size_t)My * k,
+                                          (size_t)j + (size_t)My * k1,
+                                          (size_t)j1 + (size_t)My * k1};
 #pragma unroll
-                    for (int r = 0; r < 4; r++)
-                        gs += wg[r] * 0.5f * (ld(a.P + f * plane + nn[r]) +
-                                              ld(a.C + f * plane + nn[r]));
-                    g[f] = gs;
+                    for (int f = 0; f < 6; f++) {
+                        float acc = 0.f;
+#pragma unroll
+                        for (int r = 0; r < 4; r++)
+                            acc += wg[r] * 0.5f * (ld(a.P + f * plane + nn[r]) +
+                                                   ld(a.C + f * plane + nn[r]));
+                        g[f] = acc;
+                    }
                 }
-            }
-            const float inv_gp = rsqrtf(1.f + px * px + py * py + pz * pz);
-            const float Vyp = py * inv_gp, Vzp = pz * inv_gp;
-            const float omp = one_minus_vx(px, py, pz, inv_gp);   // 1 - Vx before the kick
-            const float kE = a.sE * __frcp_rn(omp);
-            const float ex = g[0] * kE, ey = g[1] * kE, ez = g[2] * kE;
-            px += ex; py += ey; pz += ez;
-            const float kB = rsqrtf(1.f + px * px + py * py + pz * pz) * kE;
-            const float bx = (g[3] + a.bxe) * kB, by = (g[4] + a.bye) * kB,
-                        bz = (g[5] + a.bze) * kB;
-            const float co = __fdividef(2.f, 1.f + bx * bx + by * by + bz * bz);
-            const float p3x = (py * bz - pz * by + px) * co;
-            const float p3y = (pz * bx - px * bz + py) * co;
-            const float p3z = (px * by - py * bx + pz) * co;
-            px += ex + (p3y * bz - p3z * by);
-            py += ey + (p3z * bx - p3x * bz);
-            pz += ez + (p3x * by - p3y * bx);
-            const float inv_g = rsqrtf(1.f + px * px + py * py + pz * pz);
-            const float Vxm = px * inv_g, Vym = py * inv_g, Vzm = pz * inv_g;
-            const float Vy = 0.5f * (Vym + Vyp), Vz = 0.5f * (Vzm + Vzp);
-            const float inv2 = __frcp_rn(0.5f * (one_minus_vx(px, py, pz, inv_g) + omp));
-            const float wq = wv[s] * inv2;
-            const float dq[4] = {wq * a.djx0 * Vxm, wq * a.djy0 * Vym, wq * a.djz0 * Vzm,
-                                 wq * a.drho0};
-            const float dy = Vy * a.hxhy * inv2, dz = Vz * a.hxhz * inv2;
-            float partdx = 0.f, step = 1.f;
-            if (fabsf(dy) > 1.f || fabsf(dz) > 1.f) step = partdx = fmaxf(fabsf(dy), fabsf(dz));
-            if (partdx < 1.f) partdx = step = 1.f;
-            float ytmp = yp, ztmp = zp;
-            int jb = j, kb = k;
-            // first sub-step: its deposit joins the lane's run of equal cell
-            float ps;
-            if (partdx > 1.f) { partdx -= 1.f; ps = __frcp_rn(step); }
-            else { ps = __fdividef(partdx, step); partdx = 0.f; }
-            float wc[4];
-            cic_substep(dy, dz, ps, ytmp, ztmp, jb, kb, My, Mz, wc);
-            const int key = jb + My * kb;
-            if (key != acc_key) {
-                if (acc_key >= 0) cic_flush<TY, ND>(a, T, acc_key, j0, k0, acc);
-                acc_key = key;
-#pragma unroll
-                for (int i = 0; i < NV; i++) acc[i] = 0.f;
-            }
-#pragma unroll
-            for (int r = 0; r < 4; r++)
-#pragma unroll
-                for (int d = 0; d < ND; d++) acc[r * ND + d] += dq[d] * ps * wc[r];
-            // further sub-steps (|dy| or |dz| > 1 cell, rare): straight to the tile
-            while (partdx > 0.f) {
+                const float inv_gp = rsqrtf(1.f + px * px + py * py + pz * pz);
+                const float Vyp = py * inv_gp, Vzp = pz * inv_gp;
+                const float omp = one_minus_vx(px, py, pz, inv_gp);   // 1 - Vx before the kick
+                const float kE = a.sE * __frcp_rn(omp);
+                const float ex = g[0] * kE, ey = g[1] * kE, ez = g[2] * kE;
+                px += ex; py += ey; pz += ez;
+                const float kB = rsqrtf(1.f + px * px + py * py + pz * pz) * kE;
+                const float bx = (g[3] + a.bxe) * kB, by = (g[4] + a.bye) * kB,
+                            bz = (g[5] + a.bze) * kB;
+                const float co = __fdividef(2.f, 1.f + bx * bx + by * by + bz * bz);
+                const float p3x = (py * bz - pz * by + px) * co;
+                const float p3y = (pz * bx - px * bz + py) * co;
+                const float p3z = (px * by - py * bx + pz) * co;
+                px += ex + (p3y * bz - p3z * by);
+                py += ey + (p3z * bx - p3x * bz);
+                pz += ez + (p3x * by - p3y * bx);
+                const float inv_g = rsqrtf(1.f + px * px + py * py + pz * pz);
+                const float Vxm = px * inv_g, Vym = py * inv_g, Vzm = pz * inv_g;
+                const float Vy = 0.5f * (Vym + Vyp), Vz = 0.5f * (Vzm + Vzp);
+                const float inv2 = __frcp_rn(0.5f * (one_minus_vx(px, py, pz, inv_g) + omp));
+                const float wq = w * inv2;
+                const float dq[4] = {wq * a.djx0 * Vxm, wq * a.djy0 * Vym, wq * a.djz0 * Vzm,
+                                     wq * a.drho0};
+                const float dy = Vy * a.hxhy * inv2, dz = Vz * a.hxhz * inv2;
+                float partdx = 0.f, step = 1.f;
+                if (fabsf(dy) > 1.f || fabsf(dz) > 1.f)
+                    step = partdx = fmaxf(fabsf(dy), fabsf(dz));
+                if (partdx < 1.f) partdx = step = 1.f;
+                float ytmp = yp, ztmp = zp;
+                int jb = j, kb = k;
+                // first sub-step: its deposit goes through the warp reduction
+                float ps;
                 if (partdx > 1.f) { partdx -= 1.f; ps = __frcp_rn(step); }
                 else { ps = __fdividef(partdx, step); partdx = 0.f; }
+                float wc[4];
                 cic_substep(dy, dz, ps, ytmp, ztmp, jb, kb, My, Mz, wc);
-                float v[NV];
+                key = jb + My * kb;
 #pragma unroll
                 for (int r = 0; r < 4; r++)
 #pragma unroll
                     for (int d = 0; d < ND; d++) v[r * ND + d] = dq[d] * ps * wc[r];
-                cic_flush<TY, ND>(a, T, jb + My * kb, j0, k0, v);
-            }
-            if (a.full) {
-                const int nc = jb + My * kb;
-                yv[s] = ytmp; zv[s] = ztmp; pxv[s] = px; pyv[s] = py; pzv[s] = pz;
-                cv[s] = nc;
-                if (a.cnt) atomicAdd(a.cnt + nc, 1);
-            }
-        }
-        if (a.full) {
-            if (q >= pbeg && q + CH <= pend) {   // all four in this row: vector stores
-                *reinterpret_cast<float4*>(a.y + q) = Y;
-                *reinterpret_cast<float4*>(a.z + q) = Z;
-                *reinterpret_cast<float4*>(a.px + q) = PX;
-                *reinterpret_cast<float4*>(a.py + q) = PY;
-                *reinterpret_cast<float4*>(a.pz + q) = PZ;
-                *reinterpret_cast<int4*>(a.cell_out + q) = CL;
-            } else {                            // the row's ends: its own particles only
+                // further sub-steps (|dy| or |dz| > 1 cell, rare): direct atomics
+                while (partdx > 0.f) {
+                    if (partdx > 1.f) { partdx -= 1.f; ps = __frcp_rn(step); }
+                    else { ps = __fdividef(partdx, step); partdx = 0.f; }
+                    cic_substep(dy, dz, ps, ytmp, ztmp, jb, kb, My, Mz, wc);
+                    const int jb1 = wrap1(jb + 1, My), kb1 = wrap1(kb + 1, Mz);
+                    const size_t nd[4] = {(size_t)jb + (size_t)My * kb,
+                                          (size_t)jb1 + (size_t)My * kb,
+                                          (size_t)jb + (size_t)My * kb1,
+                                          (size_t)jb1 + (size_t)My * kb1};
 #pragma unroll
-                for (int s = 0; s < CH; s++) {
-                    const int p = q + s;
-                    if (p < pbeg || p >= pend) continue;
-                    a.y[p] = yv[s]; a.z[p] = zv[s]; a.px[p] = pxv[s]; a.py[p] = pyv[s];
-                    a.pz[p] = pzv[s]; a.cell_out[p] = cv[s];
+                    for (int r = 0; r < 4; r++)
+#pragma unroll
+                        for (int d = 0; d < ND; d++)
+                            atomicAdd(a.dep + d * plane + nd[r], dq[d] * ps * wc[r]);
+                }
+                if (a.full) {
+                    const int nc = jb + My * kb;
+                    a.y[p] = ytmp; a.z[p] = ztmp; a.px[p] = px; a.py[p] = py; a.pz[p] = pz;
+                    a.cell_out[p] = nc;
+                    if (a.cnt) atomicAdd(a.cnt + nc, 1);
                 }
             }
         }
+        // segmented sums over runs of equal destination cell, chunks of <= 8 lanes
+        const int prevKey = __shfl_up_sync(full, key, 1);
+        const bool start = (lane == 0) || (prevKey != key);
+        const unsigned starts = __ballot_sync(full, start);
+        const int rs = 31 - __clz(starts & (0xffffffffu >> (31 - lane)));   // run start
+        const unsigned after = starts & ~(0xffffffffu >> (31 - lane));       // starts > lane
+        const int re = after ? __ffs(after) - 2 : 31;                        // run end
+#pragma unroll
+        for (int d = 1; d <= 4; d <<= 1) {
+            const bool take = lane + d <= re && ((lane - rs) & (2 * d - 1)) == 0;
+#pragma unroll
+            for (int i = 0; i < NV; i++) {
+                const float o = __shfl_down_sync(full, v[i], d);
+                if (take) v[i] += o;
+            }
+        }
+        const bool head = key >= 0 && ((lane - rs) & 7) == 0;
+        const int dd = key - c0;
+        const bool local = head && dd >= 0 && dd < TX;
+        const unsigned lmask = __ballot_sync(full, local);
+        if (local) {
+            // chunks of the same cell (long runs, or runs split by a moved
+            // particle) are merged into their first lane before the store
+            const unsigned peers = __match_any_sync(lmask, key);
+            const int leader = __ffs(peers) - 1;
+            unsigned rest = peers & (peers - 1);
+            while (rest) {
+                const int src = __ffs(rest) - 1;
+                rest &= rest - 1;
+#pragma unroll
+                for (int i = 0; i < NV; i++) {
+                    const float o = __shfl_sync(peers, v[i], src);
+                    if (lane == leader) v[i] += o;
+                }
+            }
+            if (lane == leader) {
+#pragma unroll
+                for (int i = 0; i < NV; i++) Acc[wr][i][dd] += v[i];
+            }
+        } else if (head) {
+            int kj, kk;
+            cell_jk(key, My, a.invMy, kj, kk);
+            const int kj1 = wrap1(kj + 1, My), kk1 = wrap1(kk + 1, Mz);
+            const size_t nd[4] = {(size_t)kj + (size_t)My * kk, (size_t)kj1 + (size_t)My * kk,
+                                  (size_t)kj + (size_t)My * kk1, (size_t)kj1 + (size_t)My * kk1};
+#pragma unroll
+            for (int r = 0; r < 4; r++)
+#pragma unroll
+                for (int d = 0; d < ND; d++) atomicAdd(a.dep + d * plane + nd[r], v[r * ND + d]);
+        }
+        __syncwarp();
     }
-    if (acc_key >= 0) cic_flush<TY, ND>(a, T, acc_key, j0, k0, acc);
     pdl_trigger();
+    // spread the per-cell sums to the corners: the lane of cell (l, row) owns
+    // column l of rows row and row+1; the right-hand corners go to lane l+1
+    float row0[ND], row1[ND], edge0[ND], edge1[ND];
+#pragma unroll
+    for (int d = 0; d < ND; d++) {
+        const float c00 = Acc[wr][0 * ND + d][lane], c10 = Acc[wr][1 * ND + d][lane];
+        const float c01 = Acc[wr][2 * ND + d][lane], c11 = Acc[wr][3 * ND + d][lane];
+        const float l10 = __shfl_up_sync(full, c10, 1), l11 = __shfl_up_sync(full, c11, 1);
+        row0[d] = c00 + (lane > 0 ? l10 : 0.f);
+        row1[d] = c01 + (lane > 0 ? l11 : 0.f);
+        edge0[d] = c10;   // used by lane 31 only: column 32
+        edge1[d] = c11;
+    }
+#pragma unroll
+    for (int d = 0; d < ND; d++) {
+        T[d][wr][lane] += row0[d];
+        if (lane == 31) T[d][wr][TX] += edge0[d];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int d = 0; d < ND; d++) {
+        T[d][wr + 1][lane] += row1[d];
+        if (lane == 31) T[d][wr + 1][TX] += edge1[d];
+    }
     __syncthreads();
     for (int i = threadIdx.x; i < H * W; i += 32 * TY) {
         const int r = i / W, cc = i - r * W;
@@ -792,9 +815,9 @@ int launch_push(const PushArgs<T>& a, int shape, bool precise, cudaStream_t st) 
             if (a.loff && !a.dep_cell) {   // grouped by cell with offsets (the engine checks the shape)
                 const dim3 grid((a.My / 32) * (a.Mz / TY));
                 if (a.skip_dens)
-                    launch_pdl(push_cic_chunk_kernel<TY, 3>, grid, dim3(32 * TY), 0, st, a);
+                    launch_pdl(push_cic_warp_kernel<TY, 3>, grid, dim3(32 * TY), 0, st, a);
                 else
-                    launch_pdl(push_cic_chunk_kernel<TY, 4>, grid, dim3(32 * TY), 0, st, a);
+                    launch_pdl(push_cic_warp_kernel<TY, 4>, grid, dim3(32 * TY), 0, st, a);
                 return 1;
             }
         }

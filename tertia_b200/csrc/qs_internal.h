@@ -100,6 +100,9 @@ int launch_convert(const void* src, int src_is_double, T* dst, size_t n, cudaStr
 int launch_round_f32(double* x, size_t n, cudaStream_t st);
 // dst += (double)src over n values
 int launch_add_widened(double* dst, const float* src, size_t n, cudaStream_t st);
+// dst += (double)now - (double)before over n values; with frac, dst stays in [0, 1]
+int launch_add_increment(double* dst, const float* now, const float* before, size_t n, int frac,
+                         cudaStream_t st);
 template <class T>
 int launch_convert_back(const T* src, double* dst, size_t n, cudaStream_t st);
 

@@ -398,6 +398,21 @@ __global__ void add_widened_kernel(double* __restrict__ dst, const float* __rest
     const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) dst[i] += (double)src[i];
 }
+// dst += (double)now - (double)before; in-cell fractions (frac) kept in [0, 1]
+__global__ void add_increment_kernel(double* __restrict__ dst, const float* __restrict__ now,
+                                     const float* __restrict__ before, size_t n, int frac) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double v = dst[i] + ((double)now[i] - (double)before[i]);
+    if (frac) v = v < 0.0 ? 0.0 : (v > 1.0 ? 1.0 : v);
+    dst[i] = v;
+}
+int launch_add_increment(double* dst, const float* now, const float* before, size_t n, int frac,
+                         cudaStream_t st) {
+    if (!n) return 0;
+    add_increment_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(dst, now, before, n, frac);
+    return 1;
+}
 int launch_add_widened(double* dst, const float* src, size_t n, cudaStream_t st) {
     if (!n) return 0;
     add_widened_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(dst, src, n);
