@@ -303,7 +303,8 @@ def adjoint_measure(precision: str):
 # ------------------------------------------------------------------ FP64 comparison
 STUDY_BITS = (("transforms", 1), ("spectral_state", 2), ("push", 4), ("fields", 8),
               ("beam_currents", 16), ("front_plasma_input", 32), ("particle_state_storage", 64),
-              ("push_arithmetic", 128), ("all", 31))
+              ("push_arithmetic", 128), ("position_storage", 256), ("momentum_storage", 512),
+              ("all", 31))
 
 
 def fp64_compare(cfg, beam, pushes_per_step, ours_ms):

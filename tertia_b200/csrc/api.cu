@@ -342,6 +342,8 @@ struct Engine : EngineBase {
     //  128  the push through the FP32 push kernel as with 4, but the FP64
     //       state takes the push's increments (its arithmetic in FP32, its
     //       storage in FP64)
+    //  256  as 64 for the in-cell positions only
+    //  512  as 64 for the momenta only
     int fp32_study = 0;
     DttFft* study_fft = nullptr;
     float* study_f = nullptr;   // 40 planes: transform in / out / scratch, P and C fields, deposit
@@ -487,7 +489,7 @@ struct Engine : EngineBase {
                                                 "in [32, 1024]");
         }
         if (sizeof(T) == 8 && getenv("QS_FP32_STUDY")) {
-            fp32_study = atoi(getenv("QS_FP32_STUDY")) & 255;
+            fp32_study = atoi(getenv("QS_FP32_STUDY")) & 1023;
             if (fp32_study & 1) {
                 study_fft = DttFft::create(My, Mz);
                 CK(cudaGetLastError());
@@ -535,10 +537,14 @@ struct Engine : EngineBase {
                 });
         }
     }
-    // the plasma arrays (with the weights when `weights`) rounded to float
+    // the plasma arrays (with the weights when `weights`) rounded to float:
+    // positions and momenta, or with bit 256 / 512 the positions / momenta only
     void study_round_plasma(int bit, bool weights) {
         T* arr[6] = {py, pz, ppx, ppy, ppz, pw};
-        for (int c = 0; c < (weights ? 6 : 5); c++) study_round(arr[c], (size_t)np, bit);
+        for (int c = 0; c < (weights ? 6 : 5); c++) {
+            study_round(arr[c], (size_t)np, bit);
+            if (bit == 64) study_round(arr[c], (size_t)np, c < 2 ? 256 : (c < 5 ? 512 : 0));
+        }
     }
     void study_round(T* x, size_t n, int bit) {
         if constexpr (sizeof(T) == 8) {
