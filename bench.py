@@ -368,17 +368,30 @@ def fp64_compare(cfg, beam, pushes_per_step, ours_ms):
                                                  max(np.max(np.abs(b)), 1e-300))
         return e
 
+    e64f = rel(r64f["ex"], r64["ex"])
+    e32 = errors(r32, r64)
     out = {"value": pushes_per_step / (r64["ms"] / 1e3), "unit": UNIT,
            "ms_per_step": r64["ms"],
            "speedup": r64["ms"] / ours_ms,
            "transforms": "dense FP64 SIMT matrix passes (O(N^3) per plane)",
            "fft": {"value": pushes_per_step / (r64f["ms"] / 1e3), "unit": UNIT,
-                   "ms_per_step": r64f["ms"], "speedup": r64f["ms"] / ours_ms,
-                   "transforms": "FP64 half-length complex FFTs, the FP32 path's algorithm",
-                   "ez_rel_l2_vs_fp64": rel(r64f["ex"], r64["ex"])},
-           "errors_vs_fp64": errors(r32, r64),
+                   "ms_per_step": r64f["ms"],
+                   "speedup_over_fp64_plain": r64["ms"] / r64f["ms"],
+                   "ours_speedup_over_it": r64f["ms"] / ours_ms,
+                   "transforms": "FP64 half-length complex FFTs, the FP32 path's algorithm; "
+                                 "CIC push grouped by cell as in FP32, FP64 with FMA",
+                   "ez_rel_l2_vs_fp64": e64f},
+           "errors_vs_fp64": e32,
            "timing": "device events around the second beam step of each run (the same "
                      "inputs; the main line's own timing for ours)"}
+    # the fastest path whose whole-box on-axis Ez is within 1e-5 of the plain FP64 path
+    cands = [(cfg_precision_name(cfg), ours_ms, e32["ez_rel_l2"]), ("fp64fft", r64f["ms"], e64f)]
+    ok = [c for c in cands if c[2] <= 1e-5]
+    if ok:
+        name, ms, err = min(ok, key=lambda c: c[1])
+        out["at_ez_1e-5"] = {"path": name, "value": pushes_per_step / (ms / 1e3), "unit": UNIT,
+                             "ms_per_step": ms, "ez_rel_l2_vs_fp64_plain": err,
+                             "speedup_over_fp64_plain": r64["ms"] / ms}
     floors = {}
     for tag, eps in (("perturbed_1e-15", 1e-15), ("perturbed_6e-8", 6e-8)):
         floors[tag] = rel(run("fp64", eps)["ex"], r64["ex"])
@@ -940,7 +953,7 @@ def run_ours(args):
         achieved = bytes_launch / (pushk["avg_launch_us"] / 1e6) / 1e9
         roof = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                 "frac": achieved / hbm, "peak_source": f"hbm_gbs of {src}",
-                "kernel": "push_cic_warp_kernel (CIC push + deposit, half step)",
+                "kernel": "push_cic_row_kernel (CIC push + deposit, half step)",
                 "bytes_per_particle": bpp, "bytes_per_launch": bytes_launch,
                 "avg_launch_us": pushk["avg_launch_us"], "timing": pushk}
         if fftp:
@@ -953,7 +966,7 @@ def run_ours(args):
     else:
         roof = {"bound": "hbm", "achieved": None, "peak": hbm, "unit": "GB/s", "frac": None,
                 "kernel": dom}
-    tr = traffic_record("dtt_tc_kernel" if gemm else ("push_cic_warp_kernel" if pushk else dom),
+    tr = traffic_record("dtt_tc_kernel" if gemm else ("push_cic_row_kernel" if pushk else dom),
                         args.workload, args.precision)
     roof["traffic"] = tr.get("bytes_per_launch") if tr else None
     if tr:

@@ -18,7 +18,7 @@ BASE = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "
 # Translation units whose arithmetic must follow the reference's expression
 # order without FMA contraction (bit-exact FP64 against the oracle).
 NO_FMAD = {"push_f64.cu", "spectral.cu", "beam.cu"}
-SOURCES = ["api.cu", "dtt_simt.cu", "dtt_tc.cu", "push_f64.cu", "push_f32.cu", "spectral.cu",
+SOURCES = ["api.cu", "dtt_simt.cu", "dtt_tc.cu", "push_f64.cu", "push_f64fma.cu", "push_f32.cu", "spectral.cu",
            "spectral_f32.cu", "beam.cu", "noalloc.cu", "adjoint.cu", "sort.cu", "dtt_fft.cu",
            "pack.cu"]
 

@@ -261,9 +261,10 @@ struct Engine : EngineBase {
     bool graph_front = false;   // the captured march was built with a received front
     T* front_src = nullptr;     // Jx, Jy, Jz, Rho of the received layer
     T* front_beam = nullptr;    // RhoBeam, JxBeam spectra of the received layer
-    // FP32 CIC keeps the plasma grouped by cell (sort.cu): a second set of
-    // particle arrays for the regrouping scatter, load-order ids, per-cell
-    // counts and offsets, and where the grouping stands
+    // CIC in FP32, and in FP64 on FFT transforms, keeps the plasma grouped by
+    // cell (sort.cu): a second set of particle arrays for the regrouping
+    // scatter, load-order ids, per-cell counts and offsets, and where the
+    // grouping stands
     bool cic_sort = false;
     int32_t *acell = nullptr, *pid = nullptr, *apid = nullptr;
     T *ay = nullptr, *az = nullptr, *apx = nullptr, *apy = nullptr, *apz = nullptr, *aw = nullptr;
@@ -404,7 +405,9 @@ struct Engine : EngineBase {
         CK(cudaMemset(srcbuf, 0, 8 * plane * sizeof(T)));
         if ((s = alloc(&Cbeam, 2 * plane, "beam layer"))) return s;
         CK(cudaMemset(Cbeam, 0, 2 * plane * sizeof(T)));
-        cic_sort = cfg.shape == QS_SHAPE_CIC && sizeof(T) == 4 && My % 32 == 0 && Mz % 4 == 0;
+        cic_sort = cfg.shape == QS_SHAPE_CIC &&
+                   (sizeof(T) == 4 || cfg.precision == QS_PREC_FP64_FFT) && My % 32 == 0 &&
+                   Mz % 4 == 0;
         if (cic_sort) {
             const int nb_scan = scan_blocks_count((int)plane);
             if ((s = alloc(&cic_cnt, plane, "cell counts"))) return s;

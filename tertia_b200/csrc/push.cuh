@@ -512,272 +512,305 @@ __global__ void __launch_bounds__(128) push_cell_kernel(PushArgs<float> a) {
 }
 
 // ---------------------------------------------------------------------------
-// FP32 CIC push over particles grouped by cell (the counting sort in sort.cu
-// regroups them every few full pushes).  A block owns a tile of 32 x TY
-// cells, one warp per row of 32 cells; the warp pushes the particles of its
-// row 32 at a time (particle-parallel, so dense and empty cells do not
-// unbalance it).  The block stages the four corners of each tile cell's
-// fields (P and C averaged) in shared memory for the gather.  Deposits: the
-// warp sums the ND x 4 corner values over runs of lanes whose particles
-// deposit into the same cell (3-level segmented shuffle reduction, chunks of
-// up to 8 lanes), merges chunks that share a cell (match), and one lane per
-// cell adds them to the warp's per-cell accumulator in shared memory - no
-// shared-memory atomics.  At the end each lane spreads its cell's corner
-// values (the right-hand corners through a shuffle to the next lane), the
-// warps combine their rows in the block tile in two ordered phases, and the
-// tile is flushed with one global atomic per touched cell and current.
-// Particles whose cell or deposit lies outside the warp's row (moved since
-// the last regrouping) gather and deposit through global memory.  ND = 3
-// leaves out the density deposit, which the march does not read.  The full
-// push stores the particles in place with their new cell and, when a
-// regrouping follows, counts the new cells.  Same physics as
-// push_kernel<float, CIC, precise, fast> (movepart_layer_CIC.cpp:165-193,
-// 449-496 weights) with approximate reciprocals for the divisions.
-__device__ __forceinline__ int cell_offset(const PushArgs<float>& a, int c) {
+// CIC push over particles grouped by cell (the counting sort in sort.cu
+// regroups them every few full pushes), FP32, or FP64 with FMA contraction
+// for the FP64 path on FFT transforms.  A block owns a tile of 32 x TY cells
+// and stages the fields (P and C averaged) of the tile's cells plus one row
+// and column in shared memory for the gather.  A warp owns one row of 32
+// cells for the whole launch and lane l owns cell c0 + l.  The row's
+// particles are processed in windows of WIN slots:
+//  - phase 1, particle-parallel (lane = particle, the next one prefetched):
+//    the push; the first sub-step's charges q = dq * ps, its in-cell position
+//    and its cell (and the final cell) are staged in shared memory, further
+//    sub-steps (|dy| or |dz| above a cell, rare) deposit by global atomics;
+//  - phase 2, cell-parallel (lane = cell): each lane walks the slots of its
+//    own cell inside the window (regrouped, they are [offset(c),
+//    offset(c + 1))), rebuilds the 4 corner weights and adds the 4 x ND
+//    corner values to registers.  A particle whose first sub-step ended in
+//    another cell (it moved since the last regrouping) is added by global
+//    atomics instead; on a full push followed by a regrouping the lane counts
+//    the particles that stay in its cell and adds one count per cell.
+// No shuffles or matches sum the deposits.  The window's slots carry one pad
+// word per 32, so that lanes reading slots about ppc apart hit distinct
+// banks.  At the end each lane spreads its cell's corner sums (the right-hand
+// corners through a shuffle to the next lane), the warps combine their rows
+// in the block tile in two ordered phases, and the tile is flushed with one
+// global atomic per touched cell and current.  Particles gathered outside
+// the tile (moved since the regrouping) read the fields from global memory.
+// ND = 3 leaves out the density deposit, which the march does not read.  The
+// full push stores the particles in place with their new cell.  Same physics
+// as push_kernel<T, CIC, precise, fast> (movepart_layer_CIC.cpp:165-193,
+// 449-496 weights), the divisions factored into reciprocals.
+template <class T>
+__device__ __forceinline__ int cell_offset(const PushArgs<T>& a, int c) {
     return a.loff[c] + a.bpref[c >> 10];
 }
 
+// the reciprocal forms of the grouped push: approximate in FP32, IEEE in FP64
+template <class T>
+struct RowMath;
+template <>
+struct RowMath<float> {
+    static __device__ __forceinline__ float rsq(float x) { return rsqrtf(x); }
+    static __device__ __forceinline__ float rcp(float x) { return __frcp_rn(x); }
+    static __device__ __forceinline__ float div(float a, float b) { return __fdividef(a, b); }
+};
+template <>
+struct RowMath<double> {
+    static __device__ __forceinline__ double rsq(double x) { return rsqrt(x); }
+    static __device__ __forceinline__ double rcp(double x) { return 1.0 / x; }
+    static __device__ __forceinline__ double div(double a, double b) { return a / b; }
+};
+
 // one CIC sub-step of a particle (cell-relative move from base cell (jb, kb),
 // periodic wrap, the 4 corner weights of the new position)
-__device__ __forceinline__ void cic_substep(float dy, float dz, float ps, float& ytmp,
-                                            float& ztmp, int& jb, int& kb, int My, int Mz,
-                                            float (&wc)[4]) {
-    const float uy = ytmp + dy * ps, uz = ztmp + dz * ps;
-    const float fy = floorf(uy), fz = floorf(uz);
-    float ry = uy - fy, rz = uz - fz;
+template <class T>
+__device__ __forceinline__ void cic_substep(T dy, T dz, T ps, T& ytmp, T& ztmp, int& jb, int& kb,
+                                            int My, int Mz, T (&wc)[4]) {
+    const T one = T(1);
+    const T uy = ytmp + dy * ps, uz = ztmp + dz * ps;
+    const T fy = floor_t<T>(uy), fz = floor_t<T>(uz);
+    T ry = uy - fy, rz = uz - fz;
     int sy = (int)fy, sz = (int)fz;
-    if (ry >= 1.f) { ry = 0.f; sy += 1; }
-    if (rz >= 1.f) { rz = 0.f; sz += 1; }
+    if (ry >= one) { ry = T(0); sy += 1; }
+    if (rz >= one) { rz = T(0); sz += 1; }
     jb = wrap1(jb + sy, My);   // |dy * ps| <= 1: the shift is at most one cell
     kb = wrap1(kb + sz, Mz);
     ytmp = ry;
     ztmp = rz;
-    wc[0] = (1.f - ry) * (1.f - rz);
-    wc[1] = ry * (1.f - rz);
-    wc[2] = (1.f - ry) * rz;
+    wc[0] = (one - ry) * (one - rz);
+    wc[1] = ry * (one - rz);
+    wc[2] = (one - ry) * rz;
     wc[3] = ry * rz;
 }
 
-template <int TY, int ND>
-__global__ void __launch_bounds__(32 * TY) push_cic_warp_kernel(PushArgs<float> a) {
+template <int TY, int ND, int WIN, class T>
+__global__ void __launch_bounds__(32 * TY) push_cic_row_kernel(PushArgs<T> a) {
+    using M = RowMath<T>;
     constexpr int TX = 32, W = TX + 1, H = TY + 1, NV = 4 * ND;
-    __shared__ float Fs[6][H][W];        // fields of the tile cells + one row/column (P, C averaged)
-    __shared__ float Acc[TY][NV][TX];    // per-warp sums [corner*ND + current][cell]
-    __shared__ float T[ND][H][W];        // block deposit tile [current][row][col]
+    constexpr int NS = ND + 2;           // staged per slot: ND charges, in-cell y and z
+    constexpr int WP = WIN + WIN / 32;   // one pad word per 32 slots
+    static_assert(WIN % 32 == 0, "whole warps per window");
+    const T one = T(1), zero = T(0), half = T(0.5);
+    __shared__ T Fs[6][H][W];            // fields of the tile cells + one row/column (P, C averaged)
+    __shared__ T Tt[ND][H][W];           // block deposit tile [current][row][col]
+    __shared__ T S[TY][NS][WP];          // staged deposits of the window
+    __shared__ int K[TY][2][WP];         // [0]: first sub-step's cell (-1: none); [1]: final cell
     const int lane = threadIdx.x & 31, wr = threadIdx.x >> 5;
     const int My = a.My, Mz = a.Mz;
     const size_t plane = a.plane;
     const int tiles_x = My / TX;
     const int j0 = (blockIdx.x % tiles_x) * TX, k0 = (blockIdx.x / tiles_x) * TY;
-    for (int i = threadIdx.x; i < ND * H * W; i += 32 * TY) (&T[0][0][0])[i] = 0.f;
-#pragma unroll
-    for (int i = 0; i < NV; i++) Acc[wr][i][lane] = 0.f;
+    for (int i = threadIdx.x; i < ND * H * W; i += 32 * TY) (&Tt[0][0][0])[i] = zero;
     pdl_wait();
     for (int i = threadIdx.x; i < H * W; i += 32 * TY) {
         const int r = i / W, cc = i - r * W;
         const size_t m = (size_t)wrap1(j0 + cc, My) + (size_t)My * wrap1(k0 + r, Mz);
 #pragma unroll
-        for (int f = 0; f < 6; f++) Fs[f][r][cc] = 0.5f * (ld(a.P + f * plane + m) + ld(a.C + f * plane + m));
+        for (int f = 0; f < 6; f++) Fs[f][r][cc] = half * (ld(a.P + f * plane + m) + ld(a.C + f * plane + m));
     }
     __syncthreads();
-    const unsigned full = 0xffffffffu;
     const int c0 = j0 + My * (k0 + wr);   // this warp's 32 cells: c0 .. c0+31
-    const int pbeg = cell_offset(a, c0);
-    const int pend = (size_t)(c0 + TX) < plane ? cell_offset(a, c0 + TX) : (int)a.n;
+    const int mycell = c0 + lane;
+    const int lo = cell_offset(a, mycell);
+    const int hi = (size_t)(mycell + 1) < plane ? cell_offset(a, mycell + 1) : (int)a.n;
+    const int pbeg = __shfl_sync(0xffffffffu, lo, 0);
+    const int pend = __shfl_sync(0xffffffffu, hi, 31);
+    const bool count = a.full && a.cnt;
+    int stay = 0;                        // particles that end the full push in mycell
+    T acc[NV];
+#pragma unroll
+    for (int i = 0; i < NV; i++) acc[i] = zero;
     // the particle of the next pass is loaded while this one is pushed
     int nx_cell = 0;
-    float nx_y = 0.f, nx_z = 0.f, nx_px = 0.f, nx_py = 0.f, nx_pz = 0.f, nx_w = 0.f;
+    T nx_y = zero, nx_z = zero, nx_px = zero, nx_py = zero, nx_pz = zero, nx_w = zero;
     if (pbeg + lane < pend) {
         const int q = pbeg + lane;
         nx_cell = a.cell[q]; nx_y = a.y[q]; nx_z = a.z[q];
         nx_px = a.px[q]; nx_py = a.py[q]; nx_pz = a.pz[q]; nx_w = a.w[q];
     }
-    for (int base = pbeg; base < pend; base += 32) {
-        const int p = base + lane;
-        const int cell = nx_cell;
-        const float yp = nx_y, zp = nx_z, w = nx_w;
-        float px = nx_px, py = nx_py, pz = nx_pz;
-        if (p + 32 < pend) {
-            const int q = p + 32;
-            nx_cell = a.cell[q]; nx_y = a.y[q]; nx_z = a.z[q];
-            nx_px = a.px[q]; nx_py = a.py[q]; nx_pz = a.pz[q]; nx_w = a.w[q];
-        }
-        int key = -1;                     // destination cell of the first sub-step
-        float v[NV];
+    for (int wbase = pbeg; wbase < pend; wbase += WIN) {
+        const int wend = min(pend, wbase + WIN);
+        // phase 1: lane = particle
+        for (int base = wbase; base < wend; base += 32) {
+            const int p = base + lane;
+            const int cell = nx_cell;
+            const T yp = nx_y, zp = nx_z, w = nx_w;
+            T px = nx_px, py = nx_py, pz = nx_pz;
+            if (p + 32 < pend) {
+                const int q = p + 32;
+                nx_cell = a.cell[q]; nx_y = a.y[q]; nx_z = a.z[q];
+                nx_px = a.px[q]; nx_py = a.py[q]; nx_pz = a.pz[q]; nx_w = a.w[q];
+            }
+            int key = -1, last = cell;
+            T qv[ND], ay = zero, az = zero;
 #pragma unroll
-        for (int i = 0; i < NV; i++) v[i] = 0.f;
-        if (p < pend) {
-            if (!(yp >= 0.f && yp <= 1.f && zp >= 0.f && zp <= 1.f)) {
-                atomicOr(a.err, DEV_ERR_RANGE);
-                if (a.full && a.cnt) atomicAdd(a.cnt + cell, 1);   // it stays in its cell
-            } else {
-                int j, k;
-                cell_jk(cell, My, a.invMy, j, k);
-                const float wg[4] = {(1.f - yp) * (1.f - zp), yp * (1.f - zp), (1.f - yp) * zp,
-                                     yp * zp};
-                float g[6];
-                const int tj = j - j0, tk = k - k0;
-                if (tj >= 0 && tj < TX && tk >= 0 && tk < TY) {
-#pragma unroll
-                    for (int f = 0; f < 6; f++)
-                        g[f] = wg[0] * Fs[f][tk][tj] + wg[1] * Fs[f][tk][tj + 1] +
-                               wg[2] * Fs[f][tk + 1][tj] + wg[3] * Fs[f][tk + 1][tj + 1];
+            for (int d = 0; d < ND; d++) qv[d] = zero;
+            if (p < pend) {
+                if (!(yp >= zero && yp <= one && zp >= zero && zp <= one)) {
+                    atomicOr(a.err, DEV_ERR_RANGE);   // no deposit; it stays in its cell
                 } else {
-                    const int j1 = wrap1(j + 1, My), k1 = wrap1(k + 1, Mz);
-                    const size_t nn[4] = {(size_t)j + (size_t)My * k, (size_t)j1 + (size_t)My * k,
-                                          (size_t)j + (size_t)My * k1,
-                                          (size_t)j1 + (size_t)My * k1};
+                    int j, k;
+                    cell_jk(cell, My, a.invMy, j, k);
+                    const T wg[4] = {(one - yp) * (one - zp), yp * (one - zp), (one - yp) * zp,
+                                     yp * zp};
+                    T g[6];
+                    const int tj = j - j0, tk = k - k0;
+                    if (tj >= 0 && tj < TX && tk >= 0 && tk < TY) {
 #pragma unroll
-                    for (int f = 0; f < 6; f++) {
-                        float acc = 0.f;
+                        for (int f = 0; f < 6; f++)
+                            g[f] = wg[0] * Fs[f][tk][tj] + wg[1] * Fs[f][tk][tj + 1] +
+                                   wg[2] * Fs[f][tk + 1][tj] + wg[3] * Fs[f][tk + 1][tj + 1];
+                    } else {
+                        const int j1 = wrap1(j + 1, My), k1 = wrap1(k + 1, Mz);
+                        const size_t nn[4] = {(size_t)j + (size_t)My * k,
+                                              (size_t)j1 + (size_t)My * k,
+                                              (size_t)j + (size_t)My * k1,
+                                              (size_t)j1 + (size_t)My * k1};
+#pragma unroll
+                        for (int f = 0; f < 6; f++) {
+                            T s = zero;
+#pragma unroll
+                            for (int r = 0; r < 4; r++)
+                                s += wg[r] * half * (ld(a.P + f * plane + nn[r]) +
+                                                     ld(a.C + f * plane + nn[r]));
+                            g[f] = s;
+                        }
+                    }
+                    const T inv_gp = M::rsq(one + px * px + py * py + pz * pz);
+                    const T Vyp = py * inv_gp, Vzp = pz * inv_gp;
+                    const T omp = one_minus_vx(px, py, pz, inv_gp);   // 1 - Vx before the kick
+                    const T kE = a.sE * M::rcp(omp);
+                    const T ex = g[0] * kE, ey = g[1] * kE, ez = g[2] * kE;
+                    px += ex; py += ey; pz += ez;
+                    const T kB = M::rsq(one + px * px + py * py + pz * pz) * kE;
+                    const T bx = (g[3] + a.bxe) * kB, by = (g[4] + a.bye) * kB,
+                            bz = (g[5] + a.bze) * kB;
+                    const T co = M::div(T(2), one + bx * bx + by * by + bz * bz);
+                    const T p3x = (py * bz - pz * by + px) * co;
+                    const T p3y = (pz * bx - px * bz + py) * co;
+                    const T p3z = (px * by - py * bx + pz) * co;
+                    px += ex + (p3y * bz - p3z * by);
+                    py += ey + (p3z * bx - p3x * bz);
+                    pz += ez + (p3x * by - p3y * bx);
+                    const T inv_g = M::rsq(one + px * px + py * py + pz * pz);
+                    const T Vxm = px * inv_g, Vym = py * inv_g, Vzm = pz * inv_g;
+                    const T Vy = half * (Vym + Vyp), Vz = half * (Vzm + Vzp);
+                    const T inv2 = M::rcp(half * (one_minus_vx(px, py, pz, inv_g) + omp));
+                    const T wq = w * inv2;
+                    const T dq[4] = {wq * a.djx0 * Vxm, wq * a.djy0 * Vym, wq * a.djz0 * Vzm,
+                                     wq * a.drho0};
+                    const T dy = Vy * a.hxhy * inv2, dz = Vz * a.hxhz * inv2;
+                    T partdx = zero, step = one;
+                    if (fabs_t(dy) > one || fabs_t(dz) > one)
+                        step = partdx = fabs_t(dy) > fabs_t(dz) ? fabs_t(dy) : fabs_t(dz);
+                    if (partdx < one) partdx = step = one;
+                    T ytmp = yp, ztmp = zp;
+                    int jb = j, kb = k;
+                    // first sub-step: staged for the cell-parallel sum
+                    T ps;
+                    if (partdx > one) { partdx -= one; ps = M::rcp(step); }
+                    else { ps = M::div(partdx, step); partdx = zero; }
+                    T wc[4];
+                    cic_substep<T>(dy, dz, ps, ytmp, ztmp, jb, kb, My, Mz, wc);
+                    key = jb + My * kb;
+#pragma unroll
+                    for (int d = 0; d < ND; d++) qv[d] = dq[d] * ps;
+                    ay = ytmp;
+                    az = ztmp;
+                    // further sub-steps: direct atomics
+                    while (partdx > zero) {
+                        if (partdx > one) { partdx -= one; ps = M::rcp(step); }
+                        else { ps = M::div(partdx, step); partdx = zero; }
+                        cic_substep<T>(dy, dz, ps, ytmp, ztmp, jb, kb, My, Mz, wc);
+                        const int jb1 = wrap1(jb + 1, My), kb1 = wrap1(kb + 1, Mz);
+                        const size_t nd[4] = {(size_t)jb + (size_t)My * kb,
+                                              (size_t)jb1 + (size_t)My * kb,
+                                              (size_t)jb + (size_t)My * kb1,
+                                              (size_t)jb1 + (size_t)My * kb1};
 #pragma unroll
                         for (int r = 0; r < 4; r++)
-                            acc += wg[r] * 0.5f * (ld(a.P + f * plane + nn[r]) +
-                                                   ld(a.C + f * plane + nn[r]));
-                        g[f] = acc;
+#pragma unroll
+                            for (int d = 0; d < ND; d++)
+                                atomicAdd(a.dep + d * plane + nd[r], dq[d] * ps * wc[r]);
+                    }
+                    last = jb + My * kb;
+                    if (a.full) {
+                        a.y[p] = ytmp; a.z[p] = ztmp; a.px[p] = px; a.py[p] = py; a.pz[p] = pz;
+                        a.cell_out[p] = last;
                     }
                 }
-                const float inv_gp = rsqrtf(1.f + px * px + py * py + pz * pz);
-                const float Vyp = py * inv_gp, Vzp = pz * inv_gp;
-                const float omp = one_minus_vx(px, py, pz, inv_gp);   // 1 - Vx before the kick
-                const float kE = a.sE * __frcp_rn(omp);
-                const float ex = g[0] * kE, ey = g[1] * kE, ez = g[2] * kE;
-                px += ex; py += ey; pz += ez;
-                const float kB = rsqrtf(1.f + px * px + py * py + pz * pz) * kE;
-                const float bx = (g[3] + a.bxe) * kB, by = (g[4] + a.bye) * kB,
-                            bz = (g[5] + a.bze) * kB;
-                const float co = __fdividef(2.f, 1.f + bx * bx + by * by + bz * bz);
-                const float p3x = (py * bz - pz * by + px) * co;
-                const float p3y = (pz * bx - px * bz + py) * co;
-                const float p3z = (px * by - py * bx + pz) * co;
-                px += ex + (p3y * bz - p3z * by);
-                py += ey + (p3z * bx - p3x * bz);
-                pz += ez + (p3x * by - p3y * bx);
-                const float inv_g = rsqrtf(1.f + px * px + py * py + pz * pz);
-                const float Vxm = px * inv_g, Vym = py * inv_g, Vzm = pz * inv_g;
-                const float Vy = 0.5f * (Vym + Vyp), Vz = 0.5f * (Vzm + Vzp);
-                const float inv2 = __frcp_rn(0.5f * (one_minus_vx(px, py, pz, inv_g) + omp));
-                const float wq = w * inv2;
-                const float dq[4] = {wq * a.djx0 * Vxm, wq * a.djy0 * Vym, wq * a.djz0 * Vzm,
-                                     wq * a.drho0};
-                const float dy = Vy * a.hxhy * inv2, dz = Vz * a.hxhz * inv2;
-                float partdx = 0.f, step = 1.f;
-                if (fabsf(dy) > 1.f || fabsf(dz) > 1.f)
-                    step = partdx = fmaxf(fabsf(dy), fabsf(dz));
-                if (partdx < 1.f) partdx = step = 1.f;
-                float ytmp = yp, ztmp = zp;
-                int jb = j, kb = k;
-                // first sub-step: its deposit goes through the warp reduction
-                float ps;
-                if (partdx > 1.f) { partdx -= 1.f; ps = __frcp_rn(step); }
-                else { ps = __fdividef(partdx, step); partdx = 0.f; }
-                float wc[4];
-                cic_substep(dy, dz, ps, ytmp, ztmp, jb, kb, My, Mz, wc);
-                key = jb + My * kb;
+            }
+            const int s = base - wbase + lane, sp = s + (s >> 5);
+            K[wr][0][sp] = key;
+            K[wr][1][sp] = last;
+#pragma unroll
+            for (int d = 0; d < ND; d++) S[wr][d][sp] = qv[d];
+            S[wr][ND][sp] = ay;
+            S[wr][ND + 1][sp] = az;
+        }
+        __syncwarp();
+        // phase 2: lane = cell
+        const int qa = max(lo, wbase), qb = min(hi, wend);
+        for (int q = qa; q < qb; q++) {
+            const int s = q - wbase, sp = s + (s >> 5);
+            const int key = K[wr][0][sp];
+            if (count) {
+                const int last = K[wr][1][sp];
+                if (last == mycell) stay++;
+                else atomicAdd(a.cnt + last, 1);
+            }
+            if (key < 0) continue;
+            const T ry = S[wr][ND][sp], rz = S[wr][ND + 1][sp];
+            const T wc[4] = {(one - ry) * (one - rz), ry * (one - rz), (one - ry) * rz, ry * rz};
+            T qv[ND];
+#pragma unroll
+            for (int d = 0; d < ND; d++) qv[d] = S[wr][d][sp];
+            if (key == mycell) {
 #pragma unroll
                 for (int r = 0; r < 4; r++)
 #pragma unroll
-                    for (int d = 0; d < ND; d++) v[r * ND + d] = dq[d] * ps * wc[r];
-                // further sub-steps (|dy| or |dz| > 1 cell, rare): direct atomics
-                while (partdx > 0.f) {
-                    if (partdx > 1.f) { partdx -= 1.f; ps = __frcp_rn(step); }
-                    else { ps = __fdividef(partdx, step); partdx = 0.f; }
-                    cic_substep(dy, dz, ps, ytmp, ztmp, jb, kb, My, Mz, wc);
-                    const int jb1 = wrap1(jb + 1, My), kb1 = wrap1(kb + 1, Mz);
-                    const size_t nd[4] = {(size_t)jb + (size_t)My * kb,
-                                          (size_t)jb1 + (size_t)My * kb,
-                                          (size_t)jb + (size_t)My * kb1,
-                                          (size_t)jb1 + (size_t)My * kb1};
+                    for (int d = 0; d < ND; d++) acc[r * ND + d] += qv[d] * wc[r];
+            } else {
+                int kj, kk;
+                cell_jk(key, My, a.invMy, kj, kk);
+                const int kj1 = wrap1(kj + 1, My), kk1 = wrap1(kk + 1, Mz);
+                const size_t nd[4] = {(size_t)kj + (size_t)My * kk, (size_t)kj1 + (size_t)My * kk,
+                                      (size_t)kj + (size_t)My * kk1, (size_t)kj1 + (size_t)My * kk1};
 #pragma unroll
-                    for (int r = 0; r < 4; r++)
+                for (int r = 0; r < 4; r++)
 #pragma unroll
-                        for (int d = 0; d < ND; d++)
-                            atomicAdd(a.dep + d * plane + nd[r], dq[d] * ps * wc[r]);
-                }
-                if (a.full) {
-                    const int nc = jb + My * kb;
-                    a.y[p] = ytmp; a.z[p] = ztmp; a.px[p] = px; a.py[p] = py; a.pz[p] = pz;
-                    a.cell_out[p] = nc;
-                    if (a.cnt) atomicAdd(a.cnt + nc, 1);
-                }
+                    for (int d = 0; d < ND; d++) atomicAdd(a.dep + d * plane + nd[r], qv[d] * wc[r]);
             }
-        }
-        // segmented sums over runs of equal destination cell, chunks of <= 8 lanes
-        const int prevKey = __shfl_up_sync(full, key, 1);
-        const bool start = (lane == 0) || (prevKey != key);
-        const unsigned starts = __ballot_sync(full, start);
-        const int rs = 31 - __clz(starts & (0xffffffffu >> (31 - lane)));   // run start
-        const unsigned after = starts & ~(0xffffffffu >> (31 - lane));       // starts > lane
-        const int re = after ? __ffs(after) - 2 : 31;                        // run end
-#pragma unroll
-        for (int d = 1; d <= 4; d <<= 1) {
-            const bool take = lane + d <= re && ((lane - rs) & (2 * d - 1)) == 0;
-#pragma unroll
-            for (int i = 0; i < NV; i++) {
-                const float o = __shfl_down_sync(full, v[i], d);
-                if (take) v[i] += o;
-            }
-        }
-        const bool head = key >= 0 && ((lane - rs) & 7) == 0;
-        const int dd = key - c0;
-        const bool local = head && dd >= 0 && dd < TX;
-        const unsigned lmask = __ballot_sync(full, local);
-        if (local) {
-            // chunks of the same cell (long runs, or runs split by a moved
-            // particle) are merged into their first lane before the store
-            const unsigned peers = __match_any_sync(lmask, key);
-            const int leader = __ffs(peers) - 1;
-            unsigned rest = peers & (peers - 1);
-            while (rest) {
-                const int src = __ffs(rest) - 1;
-                rest &= rest - 1;
-#pragma unroll
-                for (int i = 0; i < NV; i++) {
-                    const float o = __shfl_sync(peers, v[i], src);
-                    if (lane == leader) v[i] += o;
-                }
-            }
-            if (lane == leader) {
-#pragma unroll
-                for (int i = 0; i < NV; i++) Acc[wr][i][dd] += v[i];
-            }
-        } else if (head) {
-            int kj, kk;
-            cell_jk(key, My, a.invMy, kj, kk);
-            const int kj1 = wrap1(kj + 1, My), kk1 = wrap1(kk + 1, Mz);
-            const size_t nd[4] = {(size_t)kj + (size_t)My * kk, (size_t)kj1 + (size_t)My * kk,
-                                  (size_t)kj + (size_t)My * kk1, (size_t)kj1 + (size_t)My * kk1};
-#pragma unroll
-            for (int r = 0; r < 4; r++)
-#pragma unroll
-                for (int d = 0; d < ND; d++) atomicAdd(a.dep + d * plane + nd[r], v[r * ND + d]);
         }
         __syncwarp();
     }
+    if (stay) atomicAdd(a.cnt + mycell, stay);
     pdl_trigger();
     // spread the per-cell sums to the corners: the lane of cell (l, row) owns
     // column l of rows row and row+1; the right-hand corners go to lane l+1
-    float row0[ND], row1[ND], edge0[ND], edge1[ND];
+    const unsigned full = 0xffffffffu;
+    T row0[ND], row1[ND], edge0[ND], edge1[ND];
 #pragma unroll
     for (int d = 0; d < ND; d++) {
-        const float c00 = Acc[wr][0 * ND + d][lane], c10 = Acc[wr][1 * ND + d][lane];
-        const float c01 = Acc[wr][2 * ND + d][lane], c11 = Acc[wr][3 * ND + d][lane];
-        const float l10 = __shfl_up_sync(full, c10, 1), l11 = __shfl_up_sync(full, c11, 1);
-        row0[d] = c00 + (lane > 0 ? l10 : 0.f);
-        row1[d] = c01 + (lane > 0 ? l11 : 0.f);
+        const T c00 = acc[0 * ND + d], c10 = acc[1 * ND + d];
+        const T c01 = acc[2 * ND + d], c11 = acc[3 * ND + d];
+        const T l10 = __shfl_up_sync(full, c10, 1), l11 = __shfl_up_sync(full, c11, 1);
+        row0[d] = c00 + (lane > 0 ? l10 : zero);
+        row1[d] = c01 + (lane > 0 ? l11 : zero);
         edge0[d] = c10;   // used by lane 31 only: column 32
         edge1[d] = c11;
     }
 #pragma unroll
     for (int d = 0; d < ND; d++) {
-        T[d][wr][lane] += row0[d];
-        if (lane == 31) T[d][wr][TX] += edge0[d];
+        Tt[d][wr][lane] += row0[d];
+        if (lane == 31) Tt[d][wr][TX] += edge0[d];
     }
     __syncthreads();
 #pragma unroll
     for (int d = 0; d < ND; d++) {
-        T[d][wr + 1][lane] += row1[d];
-        if (lane == 31) T[d][wr + 1][TX] += edge1[d];
+        Tt[d][wr + 1][lane] += row1[d];
+        if (lane == 31) Tt[d][wr + 1][TX] += edge1[d];
     }
     __syncthreads();
     for (int i = threadIdx.x; i < H * W; i += 32 * TY) {
@@ -785,11 +818,26 @@ __global__ void __launch_bounds__(32 * TY) push_cic_warp_kernel(PushArgs<float> 
         const size_t m = (size_t)wrap1(j0 + cc, My) + (size_t)My * wrap1(k0 + r, Mz);
 #pragma unroll
         for (int d = 0; d < ND; d++) {
-            const float x = T[d][r][cc];
-            if (x != 0.f) atomicAdd(a.dep + d * plane + m, x);
+            const T x = Tt[d][r][cc];
+            if (x != zero) atomicAdd(a.dep + d * plane + m, x);
         }
     }
 }
+
+// the grouped CIC push (both widths): 0 when the layout does not fit it
+template <class T>
+int launch_push_rows(const PushArgs<T>& a, cudaStream_t st) {
+    constexpr int TY = 4, WIN = 128;
+    if (!a.loff || a.dep_cell) return 0;   // grouped by cell with offsets (the engine checks the shape)
+    const dim3 grid((a.My / 32) * (a.Mz / TY));
+    if (a.skip_dens)
+        launch_pdl(push_cic_row_kernel<TY, 3, WIN, T>, grid, dim3(32 * TY), 0, st, a);
+    else
+        launch_pdl(push_cic_row_kernel<TY, 4, WIN, T>, grid, dim3(32 * TY), 0, st, a);
+    return 1;
+}
+
+int launch_push_rows_f64(const PushArgs<double>& a, cudaStream_t st);   // push_f64fma.cu
 
 template <class T>
 int launch_push(const PushArgs<T>& a, int shape, bool precise, cudaStream_t st) {
@@ -811,15 +859,9 @@ int launch_push(const PushArgs<T>& a, int shape, bool precise, cudaStream_t st) 
         }
     } else {
         if constexpr (F32) {
-            constexpr int TY = 4;
-            if (a.loff && !a.dep_cell) {   // grouped by cell with offsets (the engine checks the shape)
-                const dim3 grid((a.My / 32) * (a.Mz / TY));
-                if (a.skip_dens)
-                    launch_pdl(push_cic_warp_kernel<TY, 3>, grid, dim3(32 * TY), 0, st, a);
-                else
-                    launch_pdl(push_cic_warp_kernel<TY, 4>, grid, dim3(32 * TY), 0, st, a);
-                return 1;
-            }
+            if (launch_push_rows<float>(a, st)) return 1;
+        } else {
+            if (a.loff && !a.dep_cell) return launch_push_rows_f64(a, st);
         }
         push_kernel<T, QS_SHAPE_CIC, true, F32><<<blocks, threads, 0, st>>>(a);
     }

@@ -1,17 +1,18 @@
-// pushmath.cuh — the FP32 forms of the plasma push's velocity factors, shared
-// by the push kernels (push.cuh) and the push adjoint's recompute
-// (adjoint.cu), so that the adjoint recomputes exactly the push the forward
-// ran.
+// pushmath.cuh — the velocity factor 1 - Vx of the plasma push in the form
+// the fast push kernels use, shared by the push kernels (push.cuh) and the
+// push adjoint's recompute (adjoint.cu), so that the adjoint recomputes
+// exactly the push the forward ran.
 //
 // The push divides by 1 - Vx (movepart_splitlayer.cpp:1258-1371: the kicks
 // q2m hx/2 E/(1-Vx), the deposits w dJ V/(1-Vx), the transverse move
 // V hx/h/(1-Vx)).  For an electron moving forward fast (px > 0, Vx -> 1) the
 // difference 1 - px/gamma cancels: in FP32 its relative error grows as
-// 6e-8 / (1 - Vx).  The FP32 path therefore uses the equal form
+// 6e-8 / (1 - Vx).  The fast kernels therefore use the equal form
 //     1 - px/g = (g - px)/g = (1 + py^2 + pz^2) / (g (g + px)),   g = sqrt(1 + p^2),
 // for px > 0, which has no cancellation, and 1 - px/g itself for px <= 0
-// (no cancellation there either).  The FP64 path keeps the reference's own
-// expression order for bit-exact parity.
+// (no cancellation there either): in FP32, and in FP64 for the grouped push
+// of the FP64 path on FFT transforms.  The plain FP64 path keeps the
+// reference's own expression order for bit-exact parity.
 #pragma once
 #include <cuda_runtime.h>
 
@@ -24,6 +25,14 @@ __device__ __forceinline__ float one_minus_vx(float px, float py, float pz, floa
     const float fwd = (1.f + pt2) * inv_g * __frcp_rn(g + px);
     const float bwd = fmaf(-px, inv_g, 1.f);
     return px > 0.f ? fwd : bwd;
+}
+
+__device__ __forceinline__ double one_minus_vx(double px, double py, double pz, double inv_g) {
+    const double pt2 = fma(py, py, pz * pz);
+    const double g = (1.0 + fma(px, px, pt2)) * inv_g;
+    const double fwd = (1.0 + pt2) * inv_g / (g + px);
+    const double bwd = fma(-px, inv_g, 1.0);
+    return px > 0.0 ? fwd : bwd;
 }
 
 }  // namespace qs
