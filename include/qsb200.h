@@ -58,7 +58,9 @@ typedef enum qs_precision {
     QS_PREC_BF16X6 = 4,  /* as above with 6-term BF16 split products (3-way split)  */
     QS_PREC_FP64_FFT = 5 /* FP64 everywhere, with the FFT transforms of the FP32 path
                             computed in FP64 (power-of-two ny, nz in [32, 1024]):
-                            the reference's FFTW algorithm class on the GPU         */
+                            the reference's FFTW algorithm class on the GPU; with
+                            CIC the plasma is grouped by cell as in FP32 and the
+                            push uses FMA (not bit-identical to QS_PREC_FP64)    */
 } qs_precision;
 
 /* Plasma particle shape. */
@@ -355,9 +357,10 @@ qs_status qs_transform2d_dev(qs_handle* h, int kind_z, int kind_y, int batch,
  * device looks up the array's device address (again only after the device's
  * context has changed, e.g. after cudaDeviceReset), so make that first call
  * before any stream capture.  A CUDA error already pending on the calling
- * thread is reported as QS_ERR_CUDA and left in place; nothing is launched.  All calls on a device share the
- * array: calls whose GPU work overlaps (other streams, other host threads)
- * race and must be ordered by the caller. */
+ * thread is reported as QS_ERR_CUDA and left in place; nothing is launched.
+ * All calls on a device share the array: calls whose GPU work overlaps
+ * (other streams, other host threads) race and must be ordered by the
+ * caller. */
 qs_status qs_transform2d_noalloc(int kind_z, int kind_y, int ny, int nz, int batch,
                                  const double* d_in, double* d_out, void* stream);
 
@@ -372,7 +375,7 @@ qs_status qs_transform2d_noalloc(int kind_z, int kind_y, int ny, int nz, int bat
  * qs_adjoint_checkpoints(h, K): from the next march on, store the plasma
  * particles and the P-bank spectra every K layers (K = 0 turns it off and
  * frees the storage).  Call it after the front plasma is loaded or seeded.
- * Supported for the NGP shape and NxSplit = 1. */
+ * Supported for the NGP and CIC shapes and NxSplit = 1. */
 qs_status qs_adjoint_checkpoints(qs_handle* h, int every);
 /* Given dloss_donaxis_ex[nx] = d loss / d (on-axis Ex of layer i) for the last
  * march (which must have stored checkpoints, with no beam change since),

@@ -238,6 +238,16 @@ struct Engine : EngineBase {
     int cur = 0;                // bank index of the current (layer, split)
     bool p_valid = true;        // P-bank spectra match the P real planes
     T* scratch = nullptr;       // transform intermediate, 8 planes
+    // Side streams of the march.  [0]: the last z-pass of a layer (its real
+    // E, B, read by the next layer's pushes) runs beside the next layer's
+    // predictor, which then writes its half-transformed E, B into scratch2;
+    // [1]: the plasma regrouping after a full push runs beside the Iterate
+    // and Guess that follow.  Every reader of their outputs joins first.
+    cudaStream_t st_side[2] = {nullptr, nullptr};
+    cudaEvent_t ev_fork[2] = {nullptr, nullptr}, ev_join[2] = {nullptr, nullptr};
+    bool side_pending[2] = {false, false};
+    bool side_z = false, side_sort = false;   // set for one march
+    T* scratch2 = nullptr;      // 6 planes
     T* mats = nullptr;          // transform matrices
     DttMats<T> my, mz;
     TcTransformer* tcx = nullptr;
@@ -371,9 +381,14 @@ struct Engine : EngineBase {
                         d_dloss, d_gradw, acell, pid, apid, ay, az, apx, apy, apz, aw, cic_cnt,
                         cic_loff, cic_bsum, cic_bpref, cic_ticket, ck_cell, ck_id, seg_cell,
                         adj_inv, lam_pos, adj_tmp, d_pack, d_pack_i, q_cy, q_cz, q_part,
-                        qb_part, q_sums, study_f, study_p};
+                        qb_part, q_sums, study_f, study_p, scratch2};
         for (void* p : ptrs)
             if (p) cudaFree(p);
+        for (int k = 0; k < 2; k++) {
+            if (ev_fork[k]) cudaEventDestroy(ev_fork[k]);
+            if (ev_join[k]) cudaEventDestroy(ev_join[k]);
+            if (st_side[k]) cudaStreamDestroy(st_side[k]);
+        }
         if (st) cudaStreamDestroy(st);
     }
 
@@ -388,6 +403,11 @@ struct Engine : EngineBase {
         plane = (size_t)My * Mz;
         CK(cudaSetDevice(dev));
         CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+        for (int k = 0; k < 2; k++) {
+            CK(cudaStreamCreateWithFlags(&st_side[k], cudaStreamNonBlocking));
+            CK(cudaEventCreateWithFlags(&ev_fork[k], cudaEventDisableTiming));
+            CK(cudaEventCreateWithFlags(&ev_join[k], cudaEventDisableTiming));
+        }
         qs_status s;
         if ((s = alloc(&d_err, 1, "error flag"))) return s;
         CK(cudaMemset(d_err, 0, sizeof(int)));
@@ -484,6 +504,7 @@ struct Engine : EngineBase {
         } else if (sizeof(T) == 4) {
             fftx = DttFft::create(My, Mz);   // other sizes keep the FP32 matrix passes
             CK(cudaGetLastError());
+            if (fftx && (s = alloc(&scratch2, 6 * plane, "transform scratch"))) return s;
         } else if (cfg.precision == QS_PREC_FP64_FFT) {
             fftx64 = DttFft64::create(My, Mz);
             CK(cudaGetLastError());
@@ -1293,6 +1314,7 @@ struct Engine : EngineBase {
 
     qs_status guess(int iLayer, int iSplit) override {
         const int pb = cur ^ 1;
+        if (!sb3_valid || !p_valid) join_sides();   // these transforms use scratch
         if (!sb3_valid) {
             qs_status s = beam_spectra();
             if (s) return s;
@@ -1321,11 +1343,14 @@ struct Engine : EngineBase {
             SpecArgs<T> a = spec_args(iLayer, iSplit);
             a.zero_src = clear_by_maps() ? Csrc : nullptr;
             a.write_b = 0;
+            // beside a pending last z-pass of the previous layer (reading
+            // scratch) the map writes scratch2
+            T* out = side_z ? scratch2 : scratch;
             if constexpr (sizeof(T) == 4)
                 klaunch(KC_SPECTRAL, [&] {
-                    return fftx->run_spectral_rows(a, false, nullptr, scratch, 6, st);
+                    return fftx->run_spectral_rows(a, false, nullptr, out, 6, st);
                 });
-            eb_zpass(6);
+            eb_zpass(6, out);
             CK(cudaGetLastError());
             return QS_OK;
         }
@@ -1346,15 +1371,15 @@ struct Engine : EngineBase {
     // FP32 FFT transforms with the Guess / Iterate maps between their halves
     bool fft_maps() const { return fftx && fftx->spec_rows; }
 
-    // z-pass of the E, B (and Rho) planes the map kernel left in `scratch`:
+    // z-pass of the E, B (and Rho) planes the map kernel left in `from`:
     // E, B into the C layer, Rho into the density plane of the C sources
-    void eb_zpass(int nout) {
+    void eb_zpass(int nout, const T* from) {
         if constexpr (sizeof(T) == 4) {
             const float* ins[7];
             float* outs[7] = {Cf, Cf + plane, Cf + 2 * plane, Cf + 3 * plane, Cf + 4 * plane,
                               Cf + 5 * plane, Csrc + 3 * plane};
             const int kz[7] = {CC, CC, SS, SS, SS, CC, CC};
-            for (int f = 0; f < nout; f++) ins[f] = scratch + (size_t)f * plane;
+            for (int f = 0; f < nout; f++) ins[f] = from + (size_t)f * plane;
             klaunch(KC_GEMM, [&] { return fftx->run_cols(nout, ins, outs, kz, inv_scale(), st); });
         }
     }
@@ -1365,6 +1390,7 @@ struct Engine : EngineBase {
 
     qs_status push(int iLayer, int iSplit, int full) override {
         (void)iLayer; (void)iSplit;
+        join_sides();   // the fields and the plasma this push reads
         if (fp32_study & (4 | 128)) return study_push(full);
         // ClearCurrentsSplit: inside the march the preceding spectral kernel
         // already cleared Csrc
@@ -1418,7 +1444,35 @@ struct Engine : EngineBase {
                 grp.since++;
             }
         }
+        if (regroup && side_sort) {   // beside the Iterate and Guess that follow
+            qs_status s = QS_OK;
+            const cudaError_t e = on_side(1, [&] { s = cic_prepare(); });
+            if (e != cudaSuccess) return cuda_fail(e, "side stream");
+            if (s) return s;
+        }
         return QS_OK;
+    }
+
+    // run f() on side stream k after the work queued so far on st; the
+    // launches inside f() go to the side stream
+    template <class F>
+    cudaError_t on_side(int k, F&& f) {
+        cudaError_t e = cudaEventRecord(ev_fork[k], st);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(st_side[k], ev_fork[k], 0);
+        if (e != cudaSuccess) return e;
+        std::swap(st, st_side[k]);
+        f();
+        std::swap(st, st_side[k]);
+        side_pending[k] = true;
+        return cudaEventRecord(ev_join[k], st_side[k]);
+    }
+    // make st wait for the side streams' pending work
+    void join_sides() {
+        for (int k = 0; k < 2; k++)
+            if (side_pending[k]) {
+                cudaStreamWaitEvent(st, ev_join[k], 0);
+                side_pending[k] = false;
+            }
     }
 
     qs_status iterate(int iLayer, int iSplit, int iter, double* rel_err) override {
@@ -1451,7 +1505,13 @@ struct Engine : EngineBase {
                 klaunch(KC_SPECTRAL, [&] {
                     return fftx->run_spectral_rows(a, true, scratch, scratch, nout, st);
                 });
-                eb_zpass(nout);
+                if (side_z && iter < 0 && nout == 6) {
+                    // the layer's last z-pass: only the next layer's pushes read it
+                    const cudaError_t e = on_side(0, [&] { eb_zpass(nout, scratch); });
+                    if (e != cudaSuccess) return cuda_fail(e, "side stream");
+                } else {
+                    eb_zpass(nout, scratch);
+                }
             }
             CK(cudaGetLastError());
         } else {
@@ -1676,7 +1736,13 @@ struct Engine : EngineBase {
     qs_status march_device() {
         in_march = true;
         g_pdl = use_pdl && !prof;   // event pairs between kernels would break the chain
+        // side streams: not under per-kernel event timing or the precision study
+        const bool side = !prof && !fp32_study;
+        side_z = side && fft_maps() && S == 1 && !src3;
+        side_sort = side && cic_sort;
         qs_status s = march_device_body();
+        join_sides();
+        side_z = side_sort = false;
         g_pdl = false;
         in_march = false;
         return s;
@@ -1693,6 +1759,7 @@ struct Engine : EngineBase {
                 if ((s = move_split_layer(i, sp))) return s;
                 if ((s = layer_end(i, sp))) return s;
             }
+        join_sides();
         klaunch(KC_MISC, [&] {
             return launch_onaxis<T>(f3, L, plane, (size_t)(My / 2) + (size_t)My * (Mz / 2), onaxis_d,
                                     st);
@@ -1987,6 +2054,7 @@ struct Engine : EngineBase {
 
     qs_status save_checkpoint(int m) {
         if (m >= ck_count || np != adj_np) return fail(QS_ERR_STATE, "checkpoint storage");
+        join_sides();   // the regrouped plasma
         T* dst = ck + (size_t)m * ck_stride();
         for (int c = 0; c < 5; c++)
             CK(cudaMemcpyAsync(dst + (size_t)c * np, particle_arrays(c), np * sizeof(T),
