@@ -277,8 +277,8 @@ int launch_push_adjoint(const PushAdjArgs<T>& a, cudaStream_t st) {
 // sub-steps is piecewise constant).  Up to kMaxSub sub-steps are followed.
 constexpr int kMaxSub = 8;
 
-// FP32 uses the forward push's fast forms (rsqrt, rounded reciprocal, fast
-// divide), so that the recomputed push is the one the forward ran
+// FP32 uses the forward push's fast forms (rsqrt, approximate reciprocal,
+// fast divide), so that the recomputed push is the one the forward ran
 template <class T>
 __device__ __forceinline__ T rsq(T x) { return T(1) / sqrt(x); }
 template <>
@@ -286,7 +286,7 @@ __device__ __forceinline__ float rsq<float>(float x) { return rsqrtf(x); }
 template <class T>
 __device__ __forceinline__ T rcp(T x) { return T(1) / x; }
 template <>
-__device__ __forceinline__ float rcp<float>(float x) { return __frcp_rn(x); }
+__device__ __forceinline__ float rcp<float>(float x) { return rcp_approx(x); }
 template <class T>
 __device__ __forceinline__ T fdiv(T a, T b) { return a / b; }
 template <>

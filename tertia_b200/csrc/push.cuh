@@ -447,7 +447,7 @@ __global__ void __launch_bounds__(128) push_cell_kernel(PushArgs<float> a) {
         const float inv_gp = rsqrtf(1.f + px * px + py * py + pz * pz);
         const float Vyp = py * inv_gp, Vzp = pz * inv_gp;
         const float omp = one_minus_vx(px, py, pz, inv_gp);   // 1 - Vx before the kick
-        const float kE = a.sE * __frcp_rn(omp);
+        const float kE = a.sE * rcp_approx(omp);
         const float ex = ex0 * kE, ey = ey0 * kE, ez = ez0 * kE;
         px += ex; py += ey; pz += ez;
         const float kB = rsqrtf(1.f + px * px + py * py + pz * pz) * kE;
@@ -462,7 +462,7 @@ __global__ void __launch_bounds__(128) push_cell_kernel(PushArgs<float> a) {
         const float inv_g = rsqrtf(1.f + px * px + py * py + pz * pz);
         const float Vxm = px * inv_g, Vym = py * inv_g, Vzm = pz * inv_g;
         const float Vy = 0.5f * (Vym + Vyp), Vz = 0.5f * (Vzm + Vzp);
-        const float inv2 = __frcp_rn(0.5f * (one_minus_vx(px, py, pz, inv_g) + omp));
+        const float inv2 = rcp_approx(0.5f * (one_minus_vx(px, py, pz, inv_g) + omp));
         const float wq = wv[q] * inv2;
         const float djx = wq * a.djx0 * Vxm, djy = wq * a.djy0 * Vym, djz = wq * a.djz0 * Vzm;
         const float drho = wq * a.drho0;
@@ -473,7 +473,7 @@ __global__ void __launch_bounds__(128) push_cell_kernel(PushArgs<float> a) {
         float ytmp = yp, ztmp = zp;
         while (partdx > 0.f) {
             float ps;
-            if (partdx > 1.f) { partdx -= 1.f; ps = __frcp_rn(step); }
+            if (partdx > 1.f) { partdx -= 1.f; ps = rcp_approx(step); }
             else { ps = __fdividef(partdx, step); partdx = 0.f; }
             // cell-relative update; the base cell stays the seeded cell (the
             // reference adds the outer j_jump = j at every sub-step)
@@ -552,7 +552,7 @@ struct RowMath;
 template <>
 struct RowMath<float> {
     static __device__ __forceinline__ float rsq(float x) { return rsqrtf(x); }
-    static __device__ __forceinline__ float rcp(float x) { return __frcp_rn(x); }
+    static __device__ __forceinline__ float rcp(float x) { return rcp_approx(x); }
     static __device__ __forceinline__ float div(float a, float b) { return __fdividef(a, b); }
 };
 template <>

@@ -1,7 +1,8 @@
 """A short, self-contained run of the beam step for kernel profiling.
 
     python -m tertia_b200.profile_case [--layers 256] [--shape cic] [--precision fp32]
-                                        [--steps 1] [--adjoint]
+                                        [--steps 1] [--adjoint] [--grid N]
+                                        [--checkpoint-every K]
 
 Builds the 512 x 512 grid of the c1 workload with a shorter box (so that a
 profiler capture stays small), the c1 driver beam (bi-Gaussian, 1e6
@@ -10,6 +11,8 @@ and runs `steps` beam steps eagerly (no graph, so that every kernel is a
 separate launch), then synchronises.  With --adjoint: the 256 x 256 grid of
 the c3 workload with `layers` layers, a checkpointed march (every 16 layers)
 and one adjoint sweep of the loss sum(hx Ex) over 8 layers of the box.
+--grid N replaces the transverse grid by N x N cells of the same size (the
+c4 grid is 1024); --checkpoint-every sets the adjoint's checkpoint interval.
 Nothing is timed here: the timings come from the profiler.
 """
 from __future__ import annotations
@@ -24,6 +27,8 @@ def main():
     ap.add_argument("--precision", default="fp32")
     ap.add_argument("--steps", type=int, default=1)
     ap.add_argument("--adjoint", action="store_true")
+    ap.add_argument("--grid", type=int, default=0)
+    ap.add_argument("--checkpoint-every", type=int, default=16)
     args = ap.parse_args()
     if args.adjoint:
         return adjoint_case(args)
@@ -36,6 +41,8 @@ def main():
     w = wl.make_workload("c1", args.precision)
     cfg = w.cfg
     cfg.nx = args.layers
+    if args.grid:
+        cfg.ny = cfg.nz = args.grid
     cfg.shape = QS_SHAPE_CIC if args.shape == "cic" else QS_SHAPE_NGP
     cfg.use_graph = 0
     spec = w.beams[0]
@@ -63,6 +70,8 @@ def adjoint_case(args):
     w = wl.make_workload("c3", args.precision)
     cfg = w.cfg
     cfg.nx = args.layers
+    if args.grid:
+        cfg.ny = cfg.nz = args.grid
     cfg.shape = QS_SHAPE_CIC if args.shape == "cic" else QS_SHAPE_NGP
     cfg.ts = 0.0
     cfg.synchrotron = 0
@@ -75,7 +84,7 @@ def adjoint_case(args):
     dloss[lo:lo + 8] = cfg.hx
     with Mesh(cfg) as m:
         m.seed_front_plasma(0)
-        m.adjoint_checkpoints(16)
+        m.adjoint_checkpoints(args.checkpoint_every)
         m.load_beam(beam)
         m.move_beam_particles()
         m.move_all_split_layers()

@@ -123,6 +123,18 @@ def test_cic_adjoint_fp32_close_to_fp64_adjoint():
     assert rel(grads["fp32"], grads["fp64"]) < 1e-4, grads
 
 
+def test_cic_adjoint_fp64_fft_matches_fp64_adjoint():
+    """The FP64 path on FFT transforms regroups the plasma by cell like FP32
+    and pushes with FMA; its gradient is the plain FP64 path's to rounding."""
+    beta = np.random.default_rng(10).uniform(0.5, 1.5, NBINS)
+    grads = {}
+    for prec in ("fp64", "fp64fft"):
+        cfg, m, beam, bins, coeff = setup(prec, shape=QS_SHAPE_CIC)
+        grads[prec] = adjoint_grad(m, beam, bins, coeff, beta)
+        m.close()
+    assert rel(grads["fp64fft"], grads["fp64"]) < 1e-9, grads
+
+
 def test_cic_adjoint_fp32_maps_inside_transforms():
     """ny = 128: the recomputed march of the FP32 adjoint runs the maps
     between the halves of its FFT transforms."""

@@ -11,7 +11,7 @@ from gpu_helpers import cfg_for, rel_l2
 
 pytestmark = pytest.mark.gpu
 
-TOL = {"fp64": 1e-10, "fp32": 5e-4}
+TOL = {"fp64": 1e-10, "fp64fft": 1e-10, "fp32": 5e-4}
 
 
 def boxes(prec, shape, L=12, n=32):
@@ -40,7 +40,7 @@ def by_cell(parts):
 
 
 @pytest.mark.parametrize("prec,shape", [("fp64", abi.QS_SHAPE_NGP), ("fp64", abi.QS_SHAPE_CIC),
-                                        ("fp32", abi.QS_SHAPE_CIC)])
+                                        ("fp64fft", abi.QS_SHAPE_CIC), ("fp32", abi.QS_SHAPE_CIC)])
 def test_packed_layer_matches_oracle(oracle_lib, prec, shape):
     from tertia_b200.mesh import Mesh
     full, half, beam, upper, empty = boxes(prec, shape)
@@ -59,7 +59,7 @@ def test_packed_layer_matches_oracle(oracle_lib, prec, shape):
         assert rel_l2(pm[slot], po[slot]) < TOL[prec] * (10 if slot >= 6 else 1), slot
     cm = qm[9] + half.ny * qm[10]
     assert np.all(np.diff(cm) >= 0)                            # cell by cell
-    if prec == "fp64":
+    if prec in ("fp64", "fp64fft"):
         np.testing.assert_allclose(by_cell(qm), by_cell(qo), rtol=1e-9, atol=1e-11)
     else:
         np.testing.assert_array_equal(np.sort(qm[7]), np.sort(qo[7]).astype(np.float32))
@@ -69,7 +69,7 @@ def test_packed_layer_matches_oracle(oracle_lib, prec, shape):
 
 
 @pytest.mark.parametrize("prec,shape", [("fp64", abi.QS_SHAPE_NGP), ("fp64", abi.QS_SHAPE_CIC),
-                                        ("fp32", abi.QS_SHAPE_CIC)])
+                                        ("fp64fft", abi.QS_SHAPE_CIC), ("fp32", abi.QS_SHAPE_CIC)])
 def test_packed_particles_are_the_plasma_cell_by_cell(prec, shape):
     """The particle blocks hold the plasma in flight ordered by cell (k outer,
     j inner) and by load order within a cell, value for value, and the planes
@@ -100,6 +100,7 @@ def test_packed_particles_are_the_plasma_cell_by_cell(prec, shape):
 
 @pytest.mark.parametrize("prec,shape,graph", [("fp64", abi.QS_SHAPE_NGP, 1),
                                               ("fp64", abi.QS_SHAPE_CIC, 0),
+                                              ("fp64fft", abi.QS_SHAPE_CIC, 1),
                                               ("fp32", abi.QS_SHAPE_CIC, 1)])
 def test_march_from_a_received_layer_matches_oracle(oracle_lib, prec, shape, graph):
     from tertia_b200.mesh import Mesh
