@@ -790,6 +790,25 @@ int launch_beam_weight_grad(const BeamGradArgs<T>& a, cudaStream_t st) {
     return 1;
 }
 
+template <class T>
+__global__ void __launch_bounds__(256) save_state_kernel(StateCopy<T> c) {
+    pdl_wait();
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < c.n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+#pragma unroll
+        for (int q = 0; q < 5; q++) c.dst[q][i] = c.src[q][i];
+        if (c.csrc) c.cdst[i] = c.csrc[i];
+    }
+}
+
+template <class T>
+int launch_save_state(const StateCopy<T>& c, cudaStream_t st) {
+    if (c.n <= 0) return 0;
+    const int64_t blocks = std::min<int64_t>((c.n + 255) / 256, 148 * 8);
+    launch_pdl(save_state_kernel<T>, dim3((unsigned)blocks), dim3(256), 0, st, c);
+    return 1;
+}
+
 #define QS_ADJ_INST(T)                                                                   \
     template int launch_push_adjoint<T>(const PushAdjArgs<T>&, cudaStream_t);            \
     template int launch_push_adjoint_cic<T>(const PushAdjArgs<T>&, cudaStream_t);        \
@@ -800,6 +819,7 @@ int launch_beam_weight_grad(const BeamGradArgs<T>& a, cudaStream_t st) {
     template int launch_add_point<T>(T*, size_t, const T*, int, cudaStream_t);           \
     template int launch_add_planes<T>(T*, const T*, size_t, cudaStream_t);               \
     template int launch_avg_planes<T>(const T*, const T*, T*, size_t, cudaStream_t);     \
+    template int launch_save_state<T>(const StateCopy<T>&, cudaStream_t);                \
     template int launch_beam_weight_grad<T>(const BeamGradArgs<T>&, cudaStream_t);
 QS_ADJ_INST(float)
 QS_ADJ_INST(double)

@@ -248,6 +248,14 @@ struct Engine : EngineBase {
     bool side_pending[2] = {false, false};
     bool side_z = false, side_sort = false;   // set for one march
     T* scratch2 = nullptr;      // 6 planes
+    // the layer whose predictor the previous layer's last corrector kernel
+    // has already run (its E, B after the y-pass in scratch2), or -1
+    int pred_next = -1;
+    int fuse_lo = 0;            // lowest layer of the march (or recomputed segment)
+    // adjoint sweep: the predictor adjoint of a layer runs on side stream 0
+    // beside the next layer's first field z-pass (which then uses scratch2)
+    bool side_adj = false, adj_pred_pending = false;
+    T* push_favg = nullptr;     // the next push writes its gathered fields here
     T* mats = nullptr;          // transform matrices
     DttMats<T> my, mz;
     TcTransformer* tcx = nullptr;
@@ -1338,6 +1346,14 @@ struct Engine : EngineBase {
             xform(job_stack(stage, 7, outs, kz, ky, T(1)));
             p_valid = true;
         }
+        if (fft_maps() && pred_next == iLayer && iSplit == 0 && p_valid && sb3_valid) {
+            // the previous layer's last corrector kernel ran this predictor
+            pred_next = -1;
+            eb_zpass(6, scratch2);
+            CK(cudaGetLastError());
+            return QS_OK;
+        }
+        pred_next = -1;
         if (fft_maps()) {
             // predictor and the inverse y-pass of E, B in one kernel, then the z-pass
             SpecArgs<T> a = spec_args(iLayer, iSplit);
@@ -1423,6 +1439,8 @@ struct Engine : EngineBase {
         a.full = full;
         a.err = d_err;
         a.skip_dens = clear_by_maps() ? 1 : 0;   // the march never reads the density deposit
+        a.favg = push_favg;
+        push_favg = nullptr;
         bool regroup = false;
         if (cic_sort) {
             a.loff = cic_loff;
@@ -1502,9 +1520,23 @@ struct Engine : EngineBase {
                 a.zero_src = (clear_by_maps() && iter >= 0) ? Csrc : nullptr;
                 charge_args(a, iLayer, iSplit, iter);
                 const int nout = want_rho ? 7 : 6;
+                // the layer's last corrector also runs the next layer's
+                // predictor on its rows (the next Guess then only z-passes)
+                const bool fuse = side_z && iter < 0 && nout == 6 && iLayer > fuse_lo && S == 1;
+                SpecArgs<T> an{};
+                if (fuse) {
+                    cur ^= 1;   // the banks as layer_end leaves them
+                    an = spec_args(iLayer - 1, 0);
+                    cur ^= 1;
+                    an.zero_src = clear_by_maps() ? Psrc : nullptr;   // the next push's deposit
+                    an.write_b = 0;
+                }
                 klaunch(KC_SPECTRAL, [&] {
-                    return fftx->run_spectral_rows(a, true, scratch, scratch, nout, st);
+                    return fftx->run_spectral_rows(a, true, scratch, scratch, nout, st,
+                                                   fuse ? &an : nullptr,
+                                                   fuse ? scratch2 : nullptr);
                 });
+                pred_next = fuse ? iLayer - 1 : -1;
                 if (side_z && iter < 0 && nout == 6) {
                     // the layer's last z-pass: only the next layer's pushes read it
                     const cudaError_t e = on_side(0, [&] { eb_zpass(nout, scratch); });
@@ -1740,9 +1772,12 @@ struct Engine : EngineBase {
         const bool side = !prof && !fp32_study;
         side_z = side && fft_maps() && S == 1 && !src3;
         side_sort = side && cic_sort;
+        pred_next = -1;
+        fuse_lo = 0;
         qs_status s = march_device_body();
         join_sides();
         side_z = side_sort = false;
+        pred_next = -1;
         g_pdl = false;
         in_march = false;
         return s;
@@ -2179,33 +2214,53 @@ struct Engine : EngineBase {
     qs_status recompute_segment(int m, int c, int lo) {
         in_march = true;
         adj_recompute = true;
+        // the forward's side stream for the last z-pass of a layer and its
+        // fused next predictor (the plasma is not regrouped here)
+        side_z = !prof && !fp32_study && fft_maps() && S == 1 && !src3;
+        pred_next = -1;
+        fuse_lo = lo;
         qs_status s = restore_checkpoint(m);
         for (int i = c; !s && i >= lo; i--) {
             T* slot = seg + (size_t)(c - i) * seg_stride();
-            for (int q = 0; q < 5; q++)
-                CK(cudaMemcpyAsync(slot + (size_t)q * np, particle_arrays(q), np * sizeof(T),
-                                   cudaMemcpyDeviceToDevice, st));
-            if (cic_adj)
-                CK(cudaMemcpyAsync(seg_cell + (size_t)(c - i) * np, pcell, np * sizeof(int32_t),
-                                   cudaMemcpyDeviceToDevice, st));
+            {   // the layer's entry particles (and cells), in one launch
+                StateCopy<T> sc{};
+                for (int q = 0; q < 5; q++) {
+                    sc.src[q] = particle_arrays(q);
+                    sc.dst[q] = slot + (size_t)q * np;
+                }
+                if (cic_adj) {
+                    sc.csrc = pcell;
+                    sc.cdst = seg_cell + (size_t)(c - i) * np;
+                }
+                sc.n = np;
+                klaunch(KC_MISC, [&] { return launch_save_state<T>(sc, st); });
+            }
             T* fs = slot + 5 * (size_t)np;
             if ((s = layer_begin(i, 0))) break;
             if ((s = guess(i, 0))) break;
-            // each push's gathered fields (P + C) / 2, for its adjoint
-            klaunch(KC_MISC, [&] { return launch_avg_planes<T>(Pf, Cf, fs, 6 * plane, st); });
+            join_sides();   // P: the previous layer's last z-pass
+            // each push's gathered fields (P + C) / 2, for its adjoint: the
+            // grouped push writes them itself
+            auto gathered = [&](T* out) {
+                if (cic_sort && clear_by_maps()) push_favg = out;
+                else klaunch(KC_MISC, [&] { return launch_avg_planes<T>(Pf, Cf, out, 6 * plane, st); });
+            };
+            gathered(fs);
             for (int it = 0; it < nIter && !s; it++) {
                 if ((s = push(i, 0, 0))) break;
                 if ((s = iterate(i, 0, it, nullptr))) break;
-                klaunch(KC_MISC, [&] {
-                    return launch_avg_planes<T>(Pf, Cf, fs + (size_t)(it + 1) * 6 * plane,
-                                                6 * plane, st);
-                });
+                gathered(fs + (size_t)(it + 1) * 6 * plane);
             }
             if (s) break;
             if ((s = push(i, 0, 1))) break;
             if ((s = iterate(i, 0, -1, nullptr))) break;
             if ((s = layer_end(i, 0))) break;
         }
+        join_sides();
+        side_z = false;
+        pred_next = -1;
+        fuse_lo = 0;
+        push_favg = nullptr;
         in_march = false;
         adj_recompute = false;
         return s;
@@ -2268,15 +2323,20 @@ struct Engine : EngineBase {
     // share; with `clear` lf is zeroed once read (LAM_CX for the next push,
     // LAM_CF for its turn as the next layer's LAM_PF).
     void adj_map_fused(T* lf, const AdjSpecArgs<T>& a, bool correct, bool push_share, bool clear) {
+        adj_zpass_fields(lf, push_share, clear, scratch);
+        adj_rows_then_j(a, correct, scratch);
+    }
+    // its first part: the z-pass of the six field adjoints into `work`
+    void adj_zpass_fields(T* lf, bool push_share, bool clear, T* work) {
         if constexpr (sizeof(T) == 4) {
-            const int EBz[6] = {CC, CC, SS, SS, SS, CC}, Jz[3] = {CC, CC, SS};
+            const int EBz[6] = {CC, CC, SS, SS, SS, CC};
             const float* ins[6];
             float* outs[6];
             float* acc[6];
             float* clr[6];
             for (int f = 0; f < 6; f++) {
                 ins[f] = lf + (size_t)f * plane;
-                outs[f] = scratch + (size_t)f * plane;
+                outs[f] = work + (size_t)f * plane;
                 acc[f] = lamp(LAM_PF + f);
                 clr[f] = lf + (size_t)f * plane;
             }
@@ -2284,11 +2344,16 @@ struct Engine : EngineBase {
                 return fftx->run_cols(6, ins, outs, EBz, inv_scale(), st, push_share ? acc : nullptr,
                                       clear ? clr : nullptr);
             });
-            klaunch(KC_SPECTRAL, [&] {
-                return fftx->run_adjoint_rows(a, correct, scratch, scratch, st);
-            });
+        }
+    }
+    // its second part: the map adjoint rows on `work` and the z-pass of the
+    // current adjoints into LAM_D
+    void adj_rows_then_j(const AdjSpecArgs<T>& a, bool correct, T* work) {
+        if constexpr (sizeof(T) == 4) {
+            const int Jz[3] = {CC, CC, SS};
+            klaunch(KC_SPECTRAL, [&] { return fftx->run_adjoint_rows(a, correct, work, work, st); });
             if (correct) {
-                const float* ji[3] = {scratch, scratch + plane, scratch + 2 * plane};
+                const float* ji[3] = {work, work + plane, work + 2 * plane};
                 float* jo[3] = {lamp(LAM_D), lamp(LAM_D + 1), lamp(LAM_D + 2)};
                 klaunch(KC_GEMM, [&] { return fftx->run_cols(3, ji, jo, Jz, 1.f, st); });
             }
@@ -2324,7 +2389,14 @@ struct Engine : EngineBase {
             for (int f = 0; f < 7; f++) a.lP[f] = lamp(LAM_P + f);
             a.lP_set = 1;
             if (fft_maps()) {
-                adj_map_fused(lamp(LAM_CF), a, true, false, true);
+                // beside a pending predictor adjoint of the previous layer
+                // (on the side stream, in scratch) the field z-pass uses
+                // scratch2; the rows need that predictor adjoint's LAM_C
+                T* work = adj_pred_pending ? scratch2 : scratch;
+                adj_pred_pending = false;
+                adj_zpass_fields(lamp(LAM_CF), false, true, work);
+                join_sides();
+                adj_rows_then_j(a, true, work);
             } else {
                 klaunch(KC_SPECTRAL, [&] { return launch_corrector_adjoint<T>(a, st); });
                 adj_xform(lamp(LAM_J), lamp(LAM_D), 3, Jz, Jy, T(1));
@@ -2382,8 +2454,18 @@ struct Engine : EngineBase {
             }
             for (int f = 0; f < 7; f++) a.lP[f] = lamp(LAM_P + f);
             a.lP_set = 0;
-            if (fft_maps()) adj_map_fused(lamp(LAM_CX), a, false, true, true);
-            else klaunch(KC_SPECTRAL, [&] { return launch_predictor_adjoint<T>(a, st); });
+            if (fft_maps()) {
+                adj_zpass_fields(lamp(LAM_CX), true, true, scratch);
+                if (side_adj) {   // beside the next layer's add_point and field z-pass
+                    const cudaError_t e = on_side(0, [&] { adj_rows_then_j(a, false, scratch); });
+                    if (e != cudaSuccess) return cuda_fail(e, "side stream");
+                    adj_pred_pending = true;
+                } else {
+                    adj_rows_then_j(a, false, scratch);
+                }
+            } else {
+                klaunch(KC_SPECTRAL, [&] { return launch_predictor_adjoint<T>(a, st); });
+            }
         }
         // hand the P-side adjoints to layer i+1 (its final bank and fields)
         adj_par ^= 1;
@@ -2429,10 +2511,15 @@ struct Engine : EngineBase {
                 cur = 0;
                 qs_status s = recompute_segment(m, c, end);
                 if (s) return s;
-                for (int i = end; i <= c; i++) {
+                side_adj = !prof && !fp32_study && fft_maps();
+                adj_pred_pending = false;
+                for (int i = end; i <= c && !s; i++) {
                     const int32_t* sc = cic_adj ? seg_cell + (size_t)(c - i) * np : nullptr;
-                    if ((s = adjoint_layer(i, seg + (size_t)(c - i) * seg_stride(), sc))) return s;
+                    s = adjoint_layer(i, seg + (size_t)(c - i) * seg_stride(), sc);
                 }
+                join_sides();   // the next recomputation rewrites what the sweep reads
+                side_adj = adj_pred_pending = false;
+                if (s) return s;
             }
             first = lo;
         }

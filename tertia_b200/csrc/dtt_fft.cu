@@ -559,6 +559,7 @@ struct SpecRowArgs {
     float* out;           // Ex, Ey, Ez, Bx, By, Bz (, Rho) after the inverse y-pass
     int nout;             // 6, or 7 with Rho
     const float2* tab;    // tables of the y size
+    float* out_next;      // with the next layer's predictor: its Ex..Bz after the y-pass
 };
 
 constexpr int kSpecGroups = 8;
@@ -579,9 +580,17 @@ __host__ __device__ constexpr int spec_threads() {
     return kSpecGroups * (M / vpt<M>()) > M ? kSpecGroups * (M / vpt<M>()) : M;
 }
 
-template <int M, bool CORRECT>
+// PRED_NEXT (with CORRECT): the layer's last corrector, then the next
+// layer's predictor (`an`, whose P bank is the bank the corrector has just
+// written) on the same row, and its inverse y-pass into r.out_next.  The maps
+// are per mode and each thread keeps its mode pairs in both loops, so the
+// predictor reads what the same thread stored; it overwrites the corrector's
+// P bank (no longer needed) only at those modes.
+template <int M, bool CORRECT, bool PRED_NEXT>
 __global__ void __launch_bounds__(spec_threads<M>()) spectral_rows_kernel(SpecArgs<float> a,
-                                                                          SpecRowArgs r) {
+                                                                          SpecRowArgs r,
+                                                                          SpecArgs<float> an) {
+    static_assert(CORRECT || !PRED_NEXT, "the next layer's predictor follows a corrector");
     using namespace specf32;
     constexpr int T = M / vpt<M>();
     constexpr int NTF = kSpecGroups * T;   // the transform groups (whole warps)
@@ -657,7 +666,7 @@ __global__ void __launch_bounds__(spec_threads<M>()) spectral_rows_kernel(SpecAr
         charge_block_sum(qr * cz, qj * cz, a.qsum + 2 * (size_t)k);
     }
     __syncthreads();
-    pdl_trigger();
+    if constexpr (!PRED_NEXT) pdl_trigger();
     // inverse y-transform of Ex Ey Ez Bx By Bz Rho (y kinds C S C S C S C)
     if (threadIdx.x < NTF) {
         const bool valid = g < r.nout;
@@ -668,15 +677,46 @@ __global__ void __launch_bounds__(spec_threads<M>()) spectral_rows_kernel(SpecAr
                          [dst](int q, float2 v) { dst[q] = v; },
                          (gg & 1) ? QS_RODFT11 : QS_REDFT11, 1.f, valid, jt, Wg, tws, posts, pre);
     }
+    if constexpr (PRED_NEXT) {
+        __syncthreads();   // EB is free again
+        for (int pj = threadIdx.x; pj < M; pj += NT) {
+            const int j = 2 * pj;
+            const size_t n = (size_t)j + (size_t)N * k;
+            const Modes2 o = predictor_modes2(an, j, k, n);
+            store_modes2(an, n, o);
+            *reinterpret_cast<float2*>(EB + 0 * N + j) = make_float2(o.ex[0], o.ex[1]);
+            *reinterpret_cast<float2*>(EB + 1 * N + j) = make_float2(o.ey[0], o.ey[1]);
+            *reinterpret_cast<float2*>(EB + 2 * N + j) = make_float2(o.ez[0], o.ez[1]);
+            *reinterpret_cast<float2*>(EB + 3 * N + j) = make_float2(o.bx[0], o.bx[1]);
+            *reinterpret_cast<float2*>(EB + 4 * N + j) = make_float2(o.by[0], o.by[1]);
+            *reinterpret_cast<float2*>(EB + 5 * N + j) = make_float2(o.bz[0], o.bz[1]);
+        }
+        __syncthreads();
+        pdl_trigger();
+        if (threadIdx.x < NTF) {
+            const bool valid = g < 6;
+            const int gg = valid ? g : 0;
+            const float2* src = reinterpret_cast<const float2*>(EB + gg * N);
+            float2* dst = reinterpret_cast<float2*>(r.out_next + gg * plane + (size_t)k * N);
+            row_dtt_group<M>([src](int i) { return src[i]; },
+                             [dst](int q, float2 v) { dst[q] = v; },
+                             (gg & 1) ? QS_RODFT11 : QS_REDFT11, 1.f, valid, jt, Wg, tws, posts,
+                             pre);
+        }
+    }
 }
 
 template <int M>
 cudaError_t set_spec_rows_smem() {
-    cudaError_t e = cudaFuncSetAttribute(spectral_rows_kernel<M, true>,
+    cudaError_t e = cudaFuncSetAttribute(spectral_rows_kernel<M, true, false>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)spec_rows_smem<M>());
     if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(spectral_rows_kernel<M, false>,
+        e = cudaFuncSetAttribute(spectral_rows_kernel<M, false, false>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)spec_rows_smem<M>());
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(spectral_rows_kernel<M, true, true>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)spec_rows_smem<M>());
     return e;
@@ -684,12 +724,14 @@ cudaError_t set_spec_rows_smem() {
 
 template <int M>
 cudaError_t launch_spec_rows(const SpecArgs<float>& a, const SpecRowArgs& r, bool correct,
-                             cudaStream_t st) {
+                             const SpecArgs<float>* next, cudaStream_t st) {
     const dim3 grid((unsigned)a.nz), block(spec_threads<M>());
+    const size_t sm = spec_rows_smem<M>();
+    if (next)
+        return launch_pdl(spectral_rows_kernel<M, true, true>, grid, block, sm, st, a, r, *next);
     if (correct)
-        return launch_pdl(spectral_rows_kernel<M, true>, grid, block, spec_rows_smem<M>(), st, a,
-                          r);
-    return launch_pdl(spectral_rows_kernel<M, false>, grid, block, spec_rows_smem<M>(), st, a, r);
+        return launch_pdl(spectral_rows_kernel<M, true, false>, grid, block, sm, st, a, r, a);
+    return launch_pdl(spectral_rows_kernel<M, false, false>, grid, block, sm, st, a, r, a);
 }
 
 // The adjoints of the maps in the same arrangement (the transforms are their
@@ -910,19 +952,22 @@ int DttFft::run_cols(int nf, const float* const* in, float* const* out, const in
 }
 
 int DttFft::run_spectral_rows(const SpecArgs<float>& a, bool correct, const float* jin,
-                              float* out, int nout, cudaStream_t st) const {
+                              float* out, int nout, cudaStream_t st,
+                              const SpecArgs<float>* next, float* out_next) const {
     if (!spec_rows) return 0;
+    if (next && (!correct || !out_next || nout != 6)) return 0;
     fft::SpecRowArgs r{};
     r.jin = jin;
     r.out = out;
     r.nout = nout;
     r.tab = tab_y;
+    r.out_next = out_next;
     cudaError_t e;
     switch (ny / 2) {
-        case 512: e = fft::launch_spec_rows<512>(a, r, correct, st); break;
-        case 256: e = fft::launch_spec_rows<256>(a, r, correct, st); break;
-        case 128: e = fft::launch_spec_rows<128>(a, r, correct, st); break;
-        default: e = fft::launch_spec_rows<64>(a, r, correct, st); break;
+        case 512: e = fft::launch_spec_rows<512>(a, r, correct, next, st); break;
+        case 256: e = fft::launch_spec_rows<256>(a, r, correct, next, st); break;
+        case 128: e = fft::launch_spec_rows<128>(a, r, correct, next, st); break;
+        default: e = fft::launch_spec_rows<64>(a, r, correct, next, st); break;
     }
     return e == cudaSuccess ? 1 : 0;
 }

@@ -584,8 +584,11 @@ __device__ __forceinline__ void cic_substep(T dy, T dz, T ps, T& ytmp, T& ztmp, 
     wc[3] = ry * rz;
 }
 
+// FP32: 8 blocks per SM without the density deposit (64 registers), 7 with
+// it (72); FP64: 4 (126)
 template <int TY, int ND, int WIN, class T>
-__global__ void __launch_bounds__(32 * TY) push_cic_row_kernel(PushArgs<T> a) {
+__global__ void __launch_bounds__(32 * TY, sizeof(T) == 4 ? (ND == 3 ? 8 : 7) : 4)
+    push_cic_row_kernel(PushArgs<T> a) {
     using M = RowMath<T>;
     constexpr int TX = 32, W = TX + 1, H = TY + 1, NV = 4 * ND;
     constexpr int NS = ND + 2;           // staged per slot: ND charges, in-cell y and z
@@ -610,6 +613,16 @@ __global__ void __launch_bounds__(32 * TY) push_cic_row_kernel(PushArgs<T> a) {
         for (int f = 0; f < 6; f++) Fs[f][r][cc] = half * (ld(a.P + f * plane + m) + ld(a.C + f * plane + m));
     }
     __syncthreads();
+    // the tile's own cells of the gathered fields, for the push adjoint (the
+    // march, which skips the density deposit, is what the adjoint recomputes)
+    if constexpr (ND == 3)
+        if (a.favg)
+            for (int i = threadIdx.x; i < TY * TX; i += 32 * TY) {
+                const int r = i / TX, cc = i - r * TX;
+                const size_t m = (size_t)(j0 + cc) + (size_t)My * (k0 + r);
+#pragma unroll
+                for (int f = 0; f < 6; f++) a.favg[f * plane + m] = Fs[f][r][cc];
+            }
     const int c0 = j0 + My * (k0 + wr);   // this warp's 32 cells: c0 .. c0+31
     const int mycell = c0 + lane;
     const int lo = cell_offset(a, mycell);

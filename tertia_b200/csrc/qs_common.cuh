@@ -73,6 +73,9 @@ struct PushArgs {
     const int* bpref;
     int* cnt;
     int skip_dens;        // 1: leave out the density deposit (plane 3), unused by the caller
+    T* favg;              // grouped CIC without the density deposit: when set, the fields
+                          // the push gathers, (P + C) / 2, are written here (6 planes),
+                          // for the push adjoint
     int full;
     int* err;
 };

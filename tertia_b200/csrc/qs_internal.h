@@ -134,8 +134,11 @@ struct DttFft {
     // planes at jin, when `correct`] -> corrector (or predictor) of `a` ->
     // inverse y-pass of Ex Ey Ez Bx By Bz (, Rho when nout = 7) into `out`
     // (planes of ny*nz, unscaled); jin and out may be the same planes
+    // with `next` (the layer's last corrector, nout = 6): the next layer's
+    // predictor too, its E, B after the y-pass into out_next
     int run_spectral_rows(const SpecArgs<float>& a, bool correct, const float* jin, float* out,
-                          int nout, cudaStream_t st) const;
+                          int nout, cudaStream_t st, const SpecArgs<float>* next = nullptr,
+                          float* out_next = nullptr) const;
     // the same for the adjoints of the maps: y-pass of the 6 z-transformed
     // field adjoints at `in`, the corrector's (predictor's) adjoint, and for
     // the corrector the y-pass of the 3 current adjoints into `out`
@@ -326,6 +329,20 @@ int launch_pack_mix(const T* a, const T* b, double w0, double w1, size_t n, doub
 // out = (P + C) / 2 over n values: the fields a push gathers, kept for its adjoint
 template <class T>
 int launch_avg_planes(const T* P, const T* C, T* out, size_t n, cudaStream_t st);
+
+// dst[q][i] = src[q][i] for the 5 particle arrays (y, z, px, py, pz) and
+// cdst[i] = csrc[i] when csrc is set, i < n: a layer's entry state, saved by
+// the adjoint's recomputation in one launch
+template <class T>
+struct StateCopy {
+    const T* src[5];
+    T* dst[5];
+    const int32_t* csrc;
+    int32_t* cdst;
+    int64_t n;
+};
+template <class T>
+int launch_save_state(const StateCopy<T>& c, cudaStream_t st);
 
 // d loss / d (beam macro-particle weight) from the adjoint of the real beam
 // currents (lb3: layers lo .. L x 2 planes RhoBeam, JxBeam; zero below lo).
