@@ -519,6 +519,7 @@ struct Engine : EngineBase {
             if (!fftx64)
                 return fail(QS_ERR_UNSUPPORTED, "FP64 FFT transforms need power-of-two ny, nz "
                                                 "in [32, 1024]");
+            if ((s = alloc(&scratch2, 6 * plane, "transform scratch"))) return s;
         }
         if (sizeof(T) == 8 && getenv("QS_FP32_STUDY")) {
             fp32_study = atoi(getenv("QS_FP32_STUDY")) & 1023;
@@ -645,7 +646,8 @@ struct Engine : EngineBase {
     }
 
     // ---------------------------------------------------------- transforms
-    void xform(const DttJob<T>& job) {
+    void xform(const DttJob<T>& job, T* work = nullptr) {
+        if (!work) work = scratch;
         if (fp32_study & 1) {
             study_xform(job);
             return;
@@ -660,15 +662,15 @@ struct Engine : EngineBase {
         } else if (fftx) {
             if constexpr (sizeof(T) == 4)
                 for (int pass = 0; pass < 2; pass++)
-                    klaunch(KC_GEMM, [&] { return fftx->run_pass(pass, job, scratch, st); });
+                    klaunch(KC_GEMM, [&] { return fftx->run_pass(pass, job, work, st); });
         } else if (fftx64) {
             if constexpr (sizeof(T) == 8)
                 for (int pass = 0; pass < 2; pass++)
-                    klaunch(KC_GEMM, [&] { return fftx64->run_pass(pass, job, scratch, st); });
+                    klaunch(KC_GEMM, [&] { return fftx64->run_pass(pass, job, work, st); });
         } else {
             for (int pass = 0; pass < 2; pass++)
                 klaunch(KC_GEMM, [&] {
-                    return run_dtt_simt_pass<T>(pass, job, My, Mz, my, mz, scratch, st);
+                    return run_dtt_simt_pass<T>(pass, job, My, Mz, my, mz, work, st);
                 });
         }
     }
@@ -1244,7 +1246,7 @@ struct Engine : EngineBase {
     }
 
     // inverse transforms of the spectral E, B (+ Rho) into the C layer
-    void inverse_EB(bool with_rho) {
+    void inverse_EB(bool with_rho, T* work = nullptr) {
         const int cb = cur;
         const int nf = with_rho ? 7 : 6;
         T* outs[7] = {Cf, Cf + plane, Cf + 2 * plane, Cf + 3 * plane, Cf + 4 * plane,
@@ -1268,7 +1270,7 @@ struct Engine : EngineBase {
                 j.ky[f] = ky[f];
             }
             j.scale = inv_scale();
-            xform(j);
+            xform(j, work);
         }
     }
 
@@ -1560,7 +1562,14 @@ struct Engine : EngineBase {
             a.zero_src = (clear_by_maps() && iter >= 0) ? Csrc : nullptr;
             klaunch(KC_SPECTRAL, [&] { return launch_corrector<T>(a, st); });
             study_round(bankp(cb, 0), (size_t)SP_RB * plane, 2);
-            inverse_EB(want_rho);
+            if (side_z && iter < 0 && !want_rho) {
+                // the layer's last inverse transform: only the next layer's
+                // pushes read it, and nothing writes its bank before them
+                const cudaError_t e = on_side(0, [&] { inverse_EB(false, scratch2); });
+                if (e != cudaSuccess) return cuda_fail(e, "side stream");
+            } else {
+                inverse_EB(want_rho);
+            }
             study_round(Cf, 6 * plane, 8);
             CK(cudaGetLastError());
         }
@@ -1770,7 +1779,7 @@ struct Engine : EngineBase {
         g_pdl = use_pdl && !prof;   // event pairs between kernels would break the chain
         // side streams: not under per-kernel event timing or the precision study
         const bool side = !prof && !fp32_study;
-        side_z = side && fft_maps() && S == 1 && !src3;
+        side_z = side && (fft_maps() || fftx64) && S == 1 && !src3;
         side_sort = side && cic_sort;
         pred_next = -1;
         fuse_lo = 0;
@@ -2216,7 +2225,7 @@ struct Engine : EngineBase {
         adj_recompute = true;
         // the forward's side stream for the last z-pass of a layer and its
         // fused next predictor (the plasma is not regrouped here)
-        side_z = !prof && !fp32_study && fft_maps() && S == 1 && !src3;
+        side_z = !prof && !fp32_study && (fft_maps() || fftx64) && S == 1 && !src3;
         pred_next = -1;
         fuse_lo = lo;
         qs_status s = restore_checkpoint(m);

@@ -584,11 +584,8 @@ __device__ __forceinline__ void cic_substep(T dy, T dz, T ps, T& ytmp, T& ztmp, 
     wc[3] = ry * rz;
 }
 
-// FP32: 8 blocks per SM without the density deposit (64 registers), 7 with
-// it (72); FP64: 4 (126)
 template <int TY, int ND, int WIN, class T>
-__global__ void __launch_bounds__(32 * TY, sizeof(T) == 4 ? (ND == 3 ? 8 : 7) : 4)
-    push_cic_row_kernel(PushArgs<T> a) {
+__global__ void __launch_bounds__(32 * TY) push_cic_row_kernel(PushArgs<T> a) {
     using M = RowMath<T>;
     constexpr int TX = 32, W = TX + 1, H = TY + 1, NV = 4 * ND;
     constexpr int NS = ND + 2;           // staged per slot: ND charges, in-cell y and z
