@@ -300,6 +300,15 @@ qs_status qs_save_movie_frame(qs_handle* h, const char* path);
  * Any pointer may be NULL. */
 qs_status qs_get_charge_sums(qs_handle* h, double* rho, double* jx, double* rho_beam);
 
+/* No counterpart in the reference.  A self-test of the bounded device waits
+ * (the waits of the tensor-core transform kernel give up after a fixed number
+ * of tries, set QS_ERR_TIMEOUT's device flag, release what they hold and
+ * return): one CTA waits, through the same wait routine, on a barrier that
+ * nothing completes, for `tries` tries (1 .. 2^22).  Returns QS_ERR_TIMEOUT
+ * when the limit and the error path work (the flag is then cleared and the
+ * handle stays usable), an earlier pending error first. */
+qs_status qs_selftest_wait_limit(qs_handle* h, unsigned tries);
+
 /* --------------------------------------------------------------- the path */
 
 /* Domain::Step (step.cpp:24-122): phase += Ts, beam push, xi-march. */

@@ -201,6 +201,7 @@ def _declare(L):
     L.qs_get_onaxis_ex.argtypes = [P, f64p]
     L.qs_get_psi.argtypes = [P, f64p]
     L.qs_get_charge_sums.argtypes = [P, f64p, f64p, f64p]
+    L.qs_selftest_wait_limit.argtypes = [P, C.c_uint]
     L.qs_save_fields.argtypes = [P, C.c_char_p]
     L.qs_save_movie_frame.argtypes = [P, C.c_char_p]
     for name in ("qs_step", "qs_move_beam_particles", "qs_move_all_split_layers", "qs_begin_march"):
@@ -242,7 +243,7 @@ EXPORTED_SYMBOLS = [
     "qs_set_phase", "qs_get_phase", "qs_layer_pack_size", "qs_pack_layer", "qs_unpack_layer",
     "qs_clear_front_layer",
     "qs_set_layer", "qs_get_layer", "qs_get_field3d", "qs_set_beam_currents",
-    "qs_get_beam_currents", "qs_get_onaxis_ex", "qs_get_psi", "qs_get_charge_sums", "qs_save_fields",
+    "qs_get_beam_currents", "qs_get_onaxis_ex", "qs_get_psi", "qs_get_charge_sums", "qs_selftest_wait_limit", "qs_save_fields",
     "qs_save_movie_frame", "qs_step",
     "qs_move_beam_particles", "qs_move_all_split_layers", "qs_begin_march", "qs_layer_begin",
     "qs_move_split_layer", "qs_guess_fields", "qs_move_particles_layer", "qs_iterate_fields",

@@ -1364,10 +1364,7 @@ struct Engine : EngineBase {
             // beside a pending last z-pass of the previous layer (reading
             // scratch) the map writes scratch2
             T* out = side_z ? scratch2 : scratch;
-            if constexpr (sizeof(T) == 4)
-                klaunch(KC_SPECTRAL, [&] {
-                    return fftx->run_spectral_rows(a, false, nullptr, out, 6, st);
-                });
+            klaunch(KC_SPECTRAL, [&] { return spec_rows_run(a, false, nullptr, out, 6); });
             eb_zpass(6, out);
             CK(cudaGetLastError());
             return QS_OK;
@@ -1387,19 +1384,33 @@ struct Engine : EngineBase {
     }
 
     // FP32 FFT transforms with the Guess / Iterate maps between their halves
-    bool fft_maps() const { return fftx && fftx->spec_rows; }
+    bool fft_maps() const {
+        // (the precision study rounds the state between separate map kernels)
+        return (fftx && fftx->spec_rows) || (fftx64 && fftx64->spec_rows && !fp32_study);
+    }
+    // the adjoint's maps between the halves of its transforms (FP32)
+    bool adj_fused() const { return fftx && fftx->spec_rows; }
+    int spec_rows_run(const SpecArgs<T>& a, bool correct, const T* jin, T* out, int nout,
+                      const SpecArgs<T>* next = nullptr, T* out_next = nullptr) {
+        if constexpr (sizeof(T) == 4)
+            return fftx->run_spectral_rows(a, correct, jin, out, nout, st, next, out_next);
+        else
+            return fftx64->run_spectral_rows(a, correct, jin, out, nout, st, next, out_next);
+    }
+    int cols_run(int nf, const T* const* in, T* const* out, const int* kind, T scale) {
+        if constexpr (sizeof(T) == 4) return fftx->run_cols(nf, in, out, kind, scale, st);
+        else return fftx64->run_cols(nf, in, out, kind, scale, st);
+    }
 
     // z-pass of the E, B (and Rho) planes the map kernel left in `from`:
     // E, B into the C layer, Rho into the density plane of the C sources
     void eb_zpass(int nout, const T* from) {
-        if constexpr (sizeof(T) == 4) {
-            const float* ins[7];
-            float* outs[7] = {Cf, Cf + plane, Cf + 2 * plane, Cf + 3 * plane, Cf + 4 * plane,
-                              Cf + 5 * plane, Csrc + 3 * plane};
-            const int kz[7] = {CC, CC, SS, SS, SS, CC, CC};
-            for (int f = 0; f < nout; f++) ins[f] = from + (size_t)f * plane;
-            klaunch(KC_GEMM, [&] { return fftx->run_cols(nout, ins, outs, kz, inv_scale(), st); });
-        }
+        const T* ins[7];
+        T* outs[7] = {Cf, Cf + plane, Cf + 2 * plane, Cf + 3 * plane, Cf + 4 * plane,
+                      Cf + 5 * plane, Csrc + 3 * plane};
+        const int kz[7] = {CC, CC, SS, SS, SS, CC, CC};
+        for (int f = 0; f < nout; f++) ins[f] = from + (size_t)f * plane;
+        klaunch(KC_GEMM, [&] { return cols_run(nout, ins, outs, kz, inv_scale()); });
     }
 
     // Inside the march (no source store) the deposit planes are cleared by
@@ -1512,11 +1523,11 @@ struct Engine : EngineBase {
         if (fft_maps()) {
             // :1343-1345 along z, then the y-pass of J, the corrector and the
             // inverse y-pass of E, B (, Rho) in one kernel, then their z-pass
-            if constexpr (sizeof(T) == 4) {
-                const float* ins[3] = {Csrc, Csrc + plane, Csrc + 2 * plane};
-                float* outs[3] = {scratch, scratch + plane, scratch + 2 * plane};
+            {
+                const T* ins[3] = {Csrc, Csrc + plane, Csrc + 2 * plane};
+                T* outs[3] = {scratch, scratch + plane, scratch + 2 * plane};
                 const int kz[3] = {CC, CC, SS};
-                klaunch(KC_GEMM, [&] { return fftx->run_cols(3, ins, outs, kz, 1.f, st); });
+                klaunch(KC_GEMM, [&] { return cols_run(3, ins, outs, kz, T(1)); });
                 SpecArgs<T> a = spec_args(iLayer, iSplit);
                 a.write_b = 0;
                 a.zero_src = (clear_by_maps() && iter >= 0) ? Csrc : nullptr;
@@ -1534,9 +1545,8 @@ struct Engine : EngineBase {
                     an.write_b = 0;
                 }
                 klaunch(KC_SPECTRAL, [&] {
-                    return fftx->run_spectral_rows(a, true, scratch, scratch, nout, st,
-                                                   fuse ? &an : nullptr,
-                                                   fuse ? scratch2 : nullptr);
+                    return spec_rows_run(a, true, scratch, scratch, nout, fuse ? &an : nullptr,
+                                         fuse ? scratch2 : nullptr);
                 });
                 pred_next = fuse ? iLayer - 1 : -1;
                 if (side_z && iter < 0 && nout == 6) {
@@ -2377,13 +2387,13 @@ struct Engine : EngineBase {
         Pf = f3layer(i + 1);
         // LAM_PF gathers this layer's shares from zero (on the fused path the
         // first map cleared it in the previous layer, as its LAM_CF)
-        if (!fft_maps()) CK(cudaMemsetAsync(lamp(LAM_PF), 0, 6 * plane * sizeof(T), st));
+        if (!adj_fused()) CK(cudaMemsetAsync(lamp(LAM_PF), 0, 6 * plane * sizeof(T), st));
         klaunch(KC_MISC, [&] {
             return launch_add_point<T>(lamp(LAM_CF), (size_t)(My / 2) + (size_t)My * (Mz / 2),
                                        d_dloss, i, st);
         });
         // final Iterate: C fields <- inverse transforms of its E, B
-        if (!fft_maps()) adj_xform(lamp(LAM_CF), lamp(LAM_SPEC), 6, EBz, EBy, sc);
+        if (!adj_fused()) adj_xform(lamp(LAM_CF), lamp(LAM_SPEC), 6, EBz, EBy, sc);
         {
             AdjSpecArgs<T> a = adj_args(i);
             a.lRho = lamp(LAM_C + 0);
@@ -2397,7 +2407,7 @@ struct Engine : EngineBase {
             a.lRhoOld = lamp(LAM_RHO0);
             for (int f = 0; f < 7; f++) a.lP[f] = lamp(LAM_P + f);
             a.lP_set = 1;
-            if (fft_maps()) {
+            if (adj_fused()) {
                 // beside a pending predictor adjoint of the previous layer
                 // (on the side stream, in scratch) the field z-pass uses
                 // scratch2; the rows need that predictor adjoint's LAM_C
@@ -2413,18 +2423,18 @@ struct Engine : EngineBase {
         }
         // the push field adjoints (LAM_CX) start from zero; on the fused path
         // the z-pass that reads them clears them and adds the P layer's share
-        if (!fft_maps()) CK(cudaMemsetAsync(lamp(LAM_CX), 0, 6 * plane * sizeof(T), st));
+        if (!adj_fused()) CK(cudaMemsetAsync(lamp(LAM_CX), 0, 6 * plane * sizeof(T), st));
         klaunch(KC_PUSH, [&] {
             return push_adjoint(push_adj_args(slot, slot_cell, fs + (size_t)nIter * 6 * plane, 1));
         });
         // the P layer's field adjoint gathers every push's share
-        if (!fft_maps())
+        if (!adj_fused())
             klaunch(KC_MISC, [&] {
                 return launch_add_planes<T>(lamp(LAM_PF), lamp(LAM_CX), 6 * plane, st);
             });
         int rho_in = LAM_RHO0;
         for (int it = nIter - 1; it >= 0; it--) {
-            if (!fft_maps()) adj_xform(lamp(LAM_CX), lamp(LAM_SPEC), 6, EBz, EBy, sc);
+            if (!adj_fused()) adj_xform(lamp(LAM_CX), lamp(LAM_SPEC), 6, EBz, EBy, sc);
             AdjSpecArgs<T> a = adj_args(i);
             a.lRho = lamp(rho_in);
             const int rho_out = rho_in == LAM_RHO0 ? LAM_RHO0 + 1 : LAM_RHO0;
@@ -2436,24 +2446,24 @@ struct Engine : EngineBase {
             a.lRhoOld = lamp(rho_out);
             for (int f = 0; f < 7; f++) a.lP[f] = lamp(LAM_P + f);
             a.lP_set = 0;
-            if (fft_maps()) {
+            if (adj_fused()) {
                 adj_map_fused(lamp(LAM_CX), a, true, true, true);
             } else {
                 klaunch(KC_SPECTRAL, [&] { return launch_corrector_adjoint<T>(a, st); });
                 adj_xform(lamp(LAM_J), lamp(LAM_D), 3, Jz, Jy, T(1));
             }
             rho_in = rho_out;
-            if (!fft_maps()) CK(cudaMemsetAsync(lamp(LAM_CX), 0, 6 * plane * sizeof(T), st));
+            if (!adj_fused()) CK(cudaMemsetAsync(lamp(LAM_CX), 0, 6 * plane * sizeof(T), st));
             klaunch(KC_PUSH, [&] {
                 return push_adjoint(push_adj_args(slot, slot_cell, fs + (size_t)it * 6 * plane, 0));
             });
-            if (!fft_maps())
+            if (!adj_fused())
                 klaunch(KC_MISC, [&] {
                     return launch_add_planes<T>(lamp(LAM_PF), lamp(LAM_CX), 6 * plane, st);
                 });
         }
         // Guess: C fields <- inverse transforms of the predicted E, B
-        if (!fft_maps()) adj_xform(lamp(LAM_CX), lamp(LAM_SPEC), 6, EBz, EBy, sc);
+        if (!adj_fused()) adj_xform(lamp(LAM_CX), lamp(LAM_SPEC), 6, EBz, EBy, sc);
         {
             AdjSpecArgs<T> a = adj_args(i);
             a.lRho = lamp(rho_in);
@@ -2463,7 +2473,7 @@ struct Engine : EngineBase {
             }
             for (int f = 0; f < 7; f++) a.lP[f] = lamp(LAM_P + f);
             a.lP_set = 0;
-            if (fft_maps()) {
+            if (adj_fused()) {
                 adj_zpass_fields(lamp(LAM_CX), true, true, scratch);
                 if (side_adj) {   // beside the next layer's add_point and field z-pass
                     const cudaError_t e = on_side(0, [&] { adj_rows_then_j(a, false, scratch); });
@@ -2520,7 +2530,7 @@ struct Engine : EngineBase {
                 cur = 0;
                 qs_status s = recompute_segment(m, c, end);
                 if (s) return s;
-                side_adj = !prof && !fp32_study && fft_maps();
+                side_adj = !prof && !fp32_study && adj_fused();
                 adj_pred_pending = false;
                 for (int i = end; i <= c && !s; i++) {
                     const int32_t* sc = cic_adj ? seg_cell + (size_t)(c - i) * np : nullptr;
@@ -2970,6 +2980,18 @@ qs_status qs_save_movie_frame(qs_handle* h, const char* path) {
 qs_status qs_get_charge_sums(qs_handle* h, double* rho, double* jx, double* rho_beam) {
     H_OR_INVALID(h);
     return E->get_charge_sums(rho, jx, rho_beam);
+}
+
+qs_status qs_selftest_wait_limit(qs_handle* h, unsigned tries) {
+    H_OR_INVALID(h);
+    if (tries == 0 || tries > (1u << 22))
+        return E->fail(QS_ERR_INVALID, "qs_selftest_wait_limit: tries must be in [1, 2^22]");
+    qs_status s = E->check_device();   // earlier errors first
+    if (s) return s;
+    launch_wait_limit_probe(E->d_err, tries, E->st);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return E->cuda_fail(e, "wait-limit probe launch");
+    return E->check_device();          // QS_ERR_TIMEOUT, and the flag cleared
 }
 
 qs_status qs_get_psi(qs_handle* h, double* out) {

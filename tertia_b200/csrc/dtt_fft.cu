@@ -503,32 +503,33 @@ cudaError_t launch_cols(const ColArgsT<typename Cx<C>::Real>& a, int nf, cudaStr
 // one row of n = 2M values through the half-integer transform of `kind` by
 // the T lanes of a group: in_pair(i) = (x[2i], x[2i+1]); out_pair(q, v) gets
 // the output pair q; `valid` false runs the group on zeros and stores nothing
-template <int M, class InPair, class OutPair>
+template <int M, class C = float2, class InPair, class OutPair>
 __device__ __forceinline__ void row_dtt_group(InPair in_pair, OutPair out_pair, int kind,
-                                              float scale, bool valid, int jt, float2* Wg,
-                                              const float2* tws, const float2* posts,
-                                              const float2* pre) {
-    constexpr int V = vpt<M>();
+                                              typename Cx<C>::Real scale, bool valid, int jt,
+                                              C* Wg, const C* tws, const C* posts,
+                                              const C* pre) {
+    using Real = typename Cx<C>::Real;
+    constexpr int V = vpt_c<M, C>();
     constexpr int T = M / V;
     static_assert(T >= 1 && T <= 32, "a group within one warp");
     auto at = [](int e) { return e + e / V; };
-    float2 p[V], w[V];
+    C p[V], w[V];
 #pragma unroll
     for (int b = 0; b < V; b++) {
         const int i = jt + bitrev<V>(b) * T;
-        p[b] = valid ? in_pair(i) : make_float2(0.f, 0.f);
+        p[b] = valid ? in_pair(i) : Cx<C>::make(Real(0), Real(0));
         w[b] = __ldg(pre + i);
     }
-    float2 v[V];
+    C v[V];
 #pragma unroll
     for (int b = 0; b < V; b++) {
-        const float mirror = __shfl_xor_sync(0xffffffffu, p[V - 1 - b].y, T - 1);
-        const float2 z = kind == QS_REDFT11 ? make_float2(p[b].x, mirror)
-                                            : make_float2(mirror, p[b].x);
+        const Real mirror = __shfl_xor_sync(0xffffffffu, p[V - 1 - b].y, T - 1);
+        const C z = kind == QS_REDFT11 ? Cx<C>::make(p[b].x, mirror)
+                                       : Cx<C>::make(mirror, p[b].x);
         v[b] = cmul(z, w[b]);
     }
     dft<V>(v);
-    float2 fin[V];
+    C fin[V];
     if constexpr (T == 1) {
 #pragma unroll
         for (int r = 0; r < V; r++) fin[r] = v[r];
@@ -538,46 +539,48 @@ __device__ __forceinline__ void row_dtt_group(InPair in_pair, OutPair out_pair, 
         __syncwarp();
         Passes<M, V, V, true>::run(Wg, at, jt, tws, fin);
     }
-    float im[V];
+    Real im[V];
 #pragma unroll
     for (int m = 0; m < V; m++) {
         fin[m] = cmul(fin[m], posts[jt + T * m]);
         im[m] = fin[m].y;
     }
-    const float c2 = 2.f * scale;
-    const float sgn = kind == QS_REDFT11 ? -c2 : c2;
+    const Real c2 = Real(2) * scale;
+    const Real sgn = kind == QS_REDFT11 ? -c2 : c2;
 #pragma unroll
     for (int m = 0; m < V; m++) {
-        const float mirror = __shfl_xor_sync(0xffffffffu, im[V - 1 - m], T - 1);
-        if (valid) out_pair(jt + T * m, make_float2(c2 * fin[m].x, sgn * mirror));
+        const Real mirror = __shfl_xor_sync(0xffffffffu, im[V - 1 - m], T - 1);
+        if (valid) out_pair(jt + T * m, Cx<C>::make(c2 * fin[m].x, sgn * mirror));
     }
     __syncwarp();   // Wg is free again
 }
 
-struct SpecRowArgs {
-    const float* jin;     // corrector: Jx, Jy, Jz after the z-pass (stride `plane`)
-    float* out;           // Ex, Ey, Ez, Bx, By, Bz (, Rho) after the inverse y-pass
+template <class Real>
+struct SpecRowArgsT {
+    const Real* jin;      // corrector: Jx, Jy, Jz after the z-pass (stride `plane`)
+    Real* out;            // Ex, Ey, Ez, Bx, By, Bz (, Rho) after the inverse y-pass
     int nout;             // 6, or 7 with Rho
-    const float2* tab;    // tables of the y size
-    float* out_next;      // with the next layer's predictor: its Ex..Bz after the y-pass
+    const typename CxOf<Real>::type* tab;   // tables of the y size
+    Real* out_next;       // with the next layer's predictor: its Ex..Bz after the y-pass
 };
+using SpecRowArgs = SpecRowArgsT<float>;
 
 constexpr int kSpecGroups = 8;
 // one transform group per plane of a row: Ex..Bz and Rho out of the map
 // kernel, the six field adjoints into its adjoint
 static_assert(kSpecGroups >= 7, "a transform group per plane");
 
-template <int M>
+template <int M, class C = float2>
 __host__ __device__ constexpr size_t spec_rows_smem() {
     // tables, FFT work of each group, the row's J spectra and E, B, Rho spectra
-    return sizeof(float2) * (2 * (size_t)M + (size_t)kSpecGroups * (M + M / vpt<M>())) +
-           sizeof(float) * (3 + 7) * (size_t)(2 * M);
+    return sizeof(C) * (2 * (size_t)M + (size_t)kSpecGroups * (M + M / vpt_c<M, C>())) +
+           sizeof(typename Cx<C>::Real) * (3 + 7) * (size_t)(2 * M);
 }
 
 // threads of a map CTA: the transform groups, or one per mode pair if more
-template <int M>
+template <int M, class C = float2>
 __host__ __device__ constexpr int spec_threads() {
-    return kSpecGroups * (M / vpt<M>()) > M ? kSpecGroups * (M / vpt<M>()) : M;
+    return kSpecGroups * (M / vpt_c<M, C>()) > M ? kSpecGroups * (M / vpt_c<M, C>()) : M;
 }
 
 // PRED_NEXT (with CORRECT): the layer's last corrector, then the next
@@ -585,33 +588,35 @@ __host__ __device__ constexpr int spec_threads() {
 // written) on the same row, and its inverse y-pass into r.out_next.  The maps
 // are per mode and each thread keeps its mode pairs in both loops, so the
 // predictor reads what the same thread stored; it overwrites the corrector's
-// P bank (no longer needed) only at those modes.
-template <int M, bool CORRECT, bool PRED_NEXT>
-__global__ void __launch_bounds__(spec_threads<M>()) spectral_rows_kernel(SpecArgs<float> a,
-                                                                          SpecRowArgs r,
-                                                                          SpecArgs<float> an) {
+// P bank (no longer needed) only at those modes.  C: float2 (FP32) or
+// double2 (FP64 on FFT transforms).
+template <int M, bool CORRECT, bool PRED_NEXT, class C = float2>
+__global__ void __launch_bounds__(spec_threads<M, C>())
+    spectral_rows_kernel(SpecArgs<typename Cx<C>::Real> a, SpecRowArgsT<typename Cx<C>::Real> r,
+                         SpecArgs<typename Cx<C>::Real> an) {
     static_assert(CORRECT || !PRED_NEXT, "the next layer's predictor follows a corrector");
     using namespace specf32;
-    constexpr int T = M / vpt<M>();
+    using Real = typename Cx<C>::Real;
+    constexpr int T = M / vpt_c<M, C>();
     constexpr int NTF = kSpecGroups * T;   // the transform groups (whole warps)
-    constexpr int NT = spec_threads<M>();
+    constexpr int NT = spec_threads<M, C>();
     static_assert(NTF % 32 == 0, "transform groups fill whole warps");
     constexpr int N = 2 * M;
-    constexpr int LD = M + M / vpt<M>();
-    extern __shared__ float2 smem_f2[];
-    float2* tws = smem_f2;
-    float2* posts = tws + M;
-    float2* W = posts + M;
-    float* J = reinterpret_cast<float*>(W + kSpecGroups * LD);   // 3 x N
-    float* EB = J + 3 * N;                                        // 7 x N
+    constexpr int LD = M + M / vpt_c<M, C>();
+    extern __shared__ __align__(16) unsigned char smem_spec[];
+    C* tws = reinterpret_cast<C*>(smem_spec);
+    C* posts = tws + M;
+    C* W = posts + M;
+    Real* J = reinterpret_cast<Real*>(W + kSpecGroups * LD);   // 3 x N
+    Real* EB = J + 3 * N;                                       // 7 x N
     for (int i = threadIdx.x; i < M; i += NT) {
         tws[i] = r.tab[i];
         posts[i] = r.tab[2 * M + i];
     }
     const int k = blockIdx.x;
     const int g = threadIdx.x / T, jt = threadIdx.x % T;
-    float2* Wg = W + g * LD;
-    const float2* pre = r.tab + M;
+    C* Wg = W + g * LD;
+    const C* pre = r.tab + M;
     const size_t plane = (size_t)N * a.nz;
     pdl_wait();
     __syncthreads();
@@ -620,29 +625,37 @@ __global__ void __launch_bounds__(spec_threads<M>()) spectral_rows_kernel(SpecAr
         if (threadIdx.x < NTF) {
             const bool valid = g < 3;
             const int gg = valid ? g : 0;
-            const float2* src =
-                reinterpret_cast<const float2*>(r.jin + gg * plane + (size_t)k * N);
-            float2* dst = reinterpret_cast<float2*>(J + gg * N);
-            row_dtt_group<M>([src](int i) { return src[i]; },
-                             [dst](int q, float2 v) { dst[q] = v; },
-                             gg == 1 ? QS_RODFT11 : QS_REDFT11, 1.f, valid, jt, Wg, tws, posts,
-                             pre);
+            const C* src = reinterpret_cast<const C*>(r.jin + gg * plane + (size_t)k * N);
+            C* dst = reinterpret_cast<C*>(J + gg * N);
+            row_dtt_group<M, C>([src](int i) { return src[i]; },
+                                [dst](int q, C v) { dst[q] = v; },
+                                gg == 1 ? QS_RODFT11 : QS_REDFT11, Real(1), valid, jt, Wg, tws,
+                                posts, pre);
         }
         __syncthreads();
     }
+    auto to_eb = [&](int j, const Modes2<Real>& o) {
+        *reinterpret_cast<C*>(EB + 0 * N + j) = Cx<C>::make(o.ex[0], o.ex[1]);
+        *reinterpret_cast<C*>(EB + 1 * N + j) = Cx<C>::make(o.ey[0], o.ey[1]);
+        *reinterpret_cast<C*>(EB + 2 * N + j) = Cx<C>::make(o.ez[0], o.ez[1]);
+        *reinterpret_cast<C*>(EB + 3 * N + j) = Cx<C>::make(o.bx[0], o.bx[1]);
+        *reinterpret_cast<C*>(EB + 4 * N + j) = Cx<C>::make(o.by[0], o.by[1]);
+        *reinterpret_cast<C*>(EB + 5 * N + j) = Cx<C>::make(o.bz[0], o.bz[1]);
+        *reinterpret_cast<C*>(EB + 6 * N + j) = Cx<C>::make(o.rho[0], o.rho[1]);
+    };
     // the maps on the row's modes, two per thread
     double qr = 0.0, qj = 0.0;   // FP64 charge sums (charge.cuh)
     for (int pj = threadIdx.x; pj < M; pj += NT) {
         const int j = 2 * pj;
         const size_t n = (size_t)j + (size_t)N * k;
-        Modes2 o;
+        Modes2<Real> o;
         if constexpr (CORRECT) {
-            const float2 jx2 = *reinterpret_cast<const float2*>(J + j);
-            const float2 jy2 = *reinterpret_cast<const float2*>(J + N + j);
-            const float2 jz2 = *reinterpret_cast<const float2*>(J + 2 * N + j);
-            st2(const_cast<float*>(a.Jx), n, jx2.x, jx2.y);   // the bank keeps the deposit spectra
-            st2(const_cast<float*>(a.Jy), n, jy2.x, jy2.y);
-            st2(const_cast<float*>(a.Jz), n, jz2.x, jz2.y);
+            const C jx2 = *reinterpret_cast<const C*>(J + j);
+            const C jy2 = *reinterpret_cast<const C*>(J + N + j);
+            const C jz2 = *reinterpret_cast<const C*>(J + 2 * N + j);
+            st2(const_cast<Real*>(a.Jx), n, jx2.x, jx2.y);   // the bank keeps the deposit spectra
+            st2(const_cast<Real*>(a.Jy), n, jy2.x, jy2.y);
+            st2(const_cast<Real*>(a.Jz), n, jz2.x, jz2.y);
             o = corrector_modes2(a, j, k, n, jx2, jy2, jz2);
             if (a.qsum) {
                 const double c0 = a.qcy[j], c1 = a.qcy[j + 1];
@@ -653,13 +666,7 @@ __global__ void __launch_bounds__(spec_threads<M>()) spectral_rows_kernel(SpecAr
             o = predictor_modes2(a, j, k, n);
         }
         store_modes2(a, n, o);
-        *reinterpret_cast<float2*>(EB + 0 * N + j) = make_float2(o.ex[0], o.ex[1]);
-        *reinterpret_cast<float2*>(EB + 1 * N + j) = make_float2(o.ey[0], o.ey[1]);
-        *reinterpret_cast<float2*>(EB + 2 * N + j) = make_float2(o.ez[0], o.ez[1]);
-        *reinterpret_cast<float2*>(EB + 3 * N + j) = make_float2(o.bx[0], o.bx[1]);
-        *reinterpret_cast<float2*>(EB + 4 * N + j) = make_float2(o.by[0], o.by[1]);
-        *reinterpret_cast<float2*>(EB + 5 * N + j) = make_float2(o.bz[0], o.bz[1]);
-        *reinterpret_cast<float2*>(EB + 6 * N + j) = make_float2(o.rho[0], o.rho[1]);
+        to_eb(j, o);
     }
     if (CORRECT && a.qsum) {
         const double cz = a.qcz[k];
@@ -671,67 +678,64 @@ __global__ void __launch_bounds__(spec_threads<M>()) spectral_rows_kernel(SpecAr
     if (threadIdx.x < NTF) {
         const bool valid = g < r.nout;
         const int gg = valid ? g : 0;
-        const float2* src = reinterpret_cast<const float2*>(EB + gg * N);
-        float2* dst = reinterpret_cast<float2*>(r.out + gg * plane + (size_t)k * N);
-        row_dtt_group<M>([src](int i) { return src[i]; },
-                         [dst](int q, float2 v) { dst[q] = v; },
-                         (gg & 1) ? QS_RODFT11 : QS_REDFT11, 1.f, valid, jt, Wg, tws, posts, pre);
+        const C* src = reinterpret_cast<const C*>(EB + gg * N);
+        C* dst = reinterpret_cast<C*>(r.out + gg * plane + (size_t)k * N);
+        row_dtt_group<M, C>([src](int i) { return src[i]; },
+                            [dst](int q, C v) { dst[q] = v; },
+                            (gg & 1) ? QS_RODFT11 : QS_REDFT11, Real(1), valid, jt, Wg, tws, posts,
+                            pre);
     }
     if constexpr (PRED_NEXT) {
         __syncthreads();   // EB is free again
         for (int pj = threadIdx.x; pj < M; pj += NT) {
             const int j = 2 * pj;
             const size_t n = (size_t)j + (size_t)N * k;
-            const Modes2 o = predictor_modes2(an, j, k, n);
+            const Modes2<Real> o = predictor_modes2(an, j, k, n);
             store_modes2(an, n, o);
-            *reinterpret_cast<float2*>(EB + 0 * N + j) = make_float2(o.ex[0], o.ex[1]);
-            *reinterpret_cast<float2*>(EB + 1 * N + j) = make_float2(o.ey[0], o.ey[1]);
-            *reinterpret_cast<float2*>(EB + 2 * N + j) = make_float2(o.ez[0], o.ez[1]);
-            *reinterpret_cast<float2*>(EB + 3 * N + j) = make_float2(o.bx[0], o.bx[1]);
-            *reinterpret_cast<float2*>(EB + 4 * N + j) = make_float2(o.by[0], o.by[1]);
-            *reinterpret_cast<float2*>(EB + 5 * N + j) = make_float2(o.bz[0], o.bz[1]);
+            to_eb(j, o);
         }
         __syncthreads();
         pdl_trigger();
         if (threadIdx.x < NTF) {
             const bool valid = g < 6;
             const int gg = valid ? g : 0;
-            const float2* src = reinterpret_cast<const float2*>(EB + gg * N);
-            float2* dst = reinterpret_cast<float2*>(r.out_next + gg * plane + (size_t)k * N);
-            row_dtt_group<M>([src](int i) { return src[i]; },
-                             [dst](int q, float2 v) { dst[q] = v; },
-                             (gg & 1) ? QS_RODFT11 : QS_REDFT11, 1.f, valid, jt, Wg, tws, posts,
-                             pre);
+            const C* src = reinterpret_cast<const C*>(EB + gg * N);
+            C* dst = reinterpret_cast<C*>(r.out_next + gg * plane + (size_t)k * N);
+            row_dtt_group<M, C>([src](int i) { return src[i]; },
+                                [dst](int q, C v) { dst[q] = v; },
+                                (gg & 1) ? QS_RODFT11 : QS_REDFT11, Real(1), valid, jt, Wg, tws,
+                                posts, pre);
         }
     }
 }
 
-template <int M>
+template <int M, class C = float2>
 cudaError_t set_spec_rows_smem() {
-    cudaError_t e = cudaFuncSetAttribute(spectral_rows_kernel<M, true, false>,
+    cudaError_t e = cudaFuncSetAttribute(spectral_rows_kernel<M, true, false, C>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)spec_rows_smem<M>());
+                                         (int)spec_rows_smem<M, C>());
     if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(spectral_rows_kernel<M, false, false>,
+        e = cudaFuncSetAttribute(spectral_rows_kernel<M, false, false, C>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)spec_rows_smem<M>());
+                                 (int)spec_rows_smem<M, C>());
     if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(spectral_rows_kernel<M, true, true>,
+        e = cudaFuncSetAttribute(spectral_rows_kernel<M, true, true, C>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)spec_rows_smem<M>());
+                                 (int)spec_rows_smem<M, C>());
     return e;
 }
 
-template <int M>
-cudaError_t launch_spec_rows(const SpecArgs<float>& a, const SpecRowArgs& r, bool correct,
-                             const SpecArgs<float>* next, cudaStream_t st) {
-    const dim3 grid((unsigned)a.nz), block(spec_threads<M>());
-    const size_t sm = spec_rows_smem<M>();
+template <int M, class C = float2>
+cudaError_t launch_spec_rows(const SpecArgs<typename Cx<C>::Real>& a,
+                             const SpecRowArgsT<typename Cx<C>::Real>& r, bool correct,
+                             const SpecArgs<typename Cx<C>::Real>* next, cudaStream_t st) {
+    const dim3 grid((unsigned)a.nz), block(spec_threads<M, C>());
+    const size_t sm = spec_rows_smem<M, C>();
     if (next)
-        return launch_pdl(spectral_rows_kernel<M, true, true>, grid, block, sm, st, a, r, *next);
+        return launch_pdl(spectral_rows_kernel<M, true, true, C>, grid, block, sm, st, a, r, *next);
     if (correct)
-        return launch_pdl(spectral_rows_kernel<M, true, false>, grid, block, sm, st, a, r, a);
-    return launch_pdl(spectral_rows_kernel<M, false, false>, grid, block, sm, st, a, r, a);
+        return launch_pdl(spectral_rows_kernel<M, true, false, C>, grid, block, sm, st, a, r, a);
+    return launch_pdl(spectral_rows_kernel<M, false, false, C>, grid, block, sm, st, a, r, a);
 }
 
 // The adjoints of the maps in the same arrangement (the transforms are their
@@ -1079,7 +1083,63 @@ DttFft64* DttFft64::create(int ny, int nz) {
         delete d;
         return nullptr;
     }
+    // the map kernels between the halves: a row group must fit in one warp
+    // (8 values per thread), so ny up to 512
+    if (ny >= 128 && ny <= 512) {
+        cudaError_t e;
+        switch (ny / 2) {
+            case 256: e = fft::set_spec_rows_smem<256, double2>(); break;
+            case 128: e = fft::set_spec_rows_smem<128, double2>(); break;
+            default: e = fft::set_spec_rows_smem<64, double2>(); break;
+        }
+        d->spec_rows = e == cudaSuccess;
+        cudaGetLastError();
+    }
     return d;
+}
+
+int DttFft64::run_cols(int nf, const double* const* in, double* const* out, const int* kind,
+                       double scale, cudaStream_t st) const {
+    if (nf <= 0 || nf > kMaxXfFields) return 0;
+    fft::ColArgsT<double> a{};
+    for (int f = 0; f < nf; f++) {
+        a.in[f] = in[f];
+        a.out[f] = out[f];
+        a.kind[f] = kind[f];
+    }
+    a.ncols = ny;
+    a.scale = scale;
+    a.tab = tab_z;
+    cudaError_t e;
+    switch (nz / 2) {
+        case 512: e = fft::launch_cols<512, double2>(a, nf, st); break;
+        case 256: e = fft::launch_cols<256, double2>(a, nf, st); break;
+        case 128: e = fft::launch_cols<128, double2>(a, nf, st); break;
+        case 64: e = fft::launch_cols<64, double2>(a, nf, st); break;
+        case 32: e = fft::launch_cols<32, double2>(a, nf, st); break;
+        default: e = fft::launch_cols<16, double2>(a, nf, st); break;
+    }
+    return e == cudaSuccess ? 1 : 0;
+}
+
+int DttFft64::run_spectral_rows(const SpecArgs<double>& a, bool correct, const double* jin,
+                                double* out, int nout, cudaStream_t st,
+                                const SpecArgs<double>* next, double* out_next) const {
+    if (!spec_rows) return 0;
+    if (next && (!correct || !out_next || nout != 6)) return 0;
+    fft::SpecRowArgsT<double> r{};
+    r.jin = jin;
+    r.out = out;
+    r.nout = nout;
+    r.tab = tab_y;
+    r.out_next = out_next;
+    cudaError_t e;
+    switch (ny / 2) {
+        case 256: e = fft::launch_spec_rows<256, double2>(a, r, correct, next, st); break;
+        case 128: e = fft::launch_spec_rows<128, double2>(a, r, correct, next, st); break;
+        default: e = fft::launch_spec_rows<64, double2>(a, r, correct, next, st); break;
+    }
+    return e == cudaSuccess ? 1 : 0;
 }
 
 int DttFft64::run_pass(int pass, const DttJob<double>& job, double* scratch,

@@ -87,8 +87,9 @@ __device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
 }
 
 // bounded wait: false on timeout or when another role aborted
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int* abort_flag) {
-    for (uint32_t i = 0; i < SPIN_LIMIT; i++) {
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int* abort_flag,
+                                          uint32_t limit = SPIN_LIMIT) {
+    for (uint32_t i = 0; i < limit; i++) {
         if (mbar_try(bar, parity)) return true;
         if ((i & 255u) == 255u && *abort_flag) return false;
     }
@@ -487,7 +488,30 @@ __global__ void split_planes_kernel(const float* __restrict__ in, size_t stride,
     }
 }
 
+// A self-test of the bounded waits: one thread initialises an mbarrier that
+// nothing arrives at and waits on it through mbar_wait with `limit` tries;
+// the wait gives up and the kernel sets DEV_ERR_TIMEOUT, as the roles of the
+// transform kernel do.  No copy, TMEM or other CTA is involved, so the
+// kernel ends after at most `limit` tries.
+__global__ void wait_limit_probe_kernel(int* err, uint32_t limit) {
+    __shared__ __align__(8) uint64_t bar;
+    __shared__ int abort_flag;
+    if (threadIdx.x == 0) {
+        abort_flag = 0;
+        mbar_init(smem_u32(&bar), 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    if (threadIdx.x == 0 && !mbar_wait(smem_u32(&bar), 0, &abort_flag, limit))
+        atomicOr(err, DEV_ERR_TIMEOUT);
+}
+
 }  // namespace tcx
+
+int launch_wait_limit_probe(int* err, unsigned limit, cudaStream_t st) {
+    tcx::wait_limit_probe_kernel<<<1, 32, 0, st>>>(err, limit);
+    return 1;
+}
 
 // ---------------------------------------------------------------- host side
 namespace {

@@ -6,6 +6,10 @@
 
 namespace qs {
 
+// the bounded-wait self-test (dtt_tc.cu): sets DEV_ERR_TIMEOUT in *err after
+// `limit` tries of an mbarrier wait nothing completes
+int launch_wait_limit_probe(int* err, unsigned limit, cudaStream_t st);
+
 class TcTransformer {
 public:
     // mode: QS_PREC_TF32X3 / QS_PREC_BF16X3 / QS_PREC_BF16X6.  Returns nullptr

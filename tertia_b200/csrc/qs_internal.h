@@ -154,8 +154,15 @@ struct DttFft64 {
     int ny = 0, nz = 0;
     double2* tab_y = nullptr;
     double2* tab_z = nullptr;
+    bool spec_rows = false;    // run_spectral_rows available (ny in [128, 512])
     static DttFft64* create(int ny, int nz);   // nullptr when a size is not handled
     int run_pass(int pass, const DttJob<double>& job, double* scratch, cudaStream_t st) const;
+    // as DttFft's, in FP64
+    int run_cols(int nf, const double* const* in, double* const* out, const int* kind,
+                 double scale, cudaStream_t st) const;
+    int run_spectral_rows(const SpecArgs<double>& a, bool correct, const double* jin, double* out,
+                          int nout, cudaStream_t st, const SpecArgs<double>* next = nullptr,
+                          double* out_next = nullptr) const;
     ~DttFft64();
 };
 

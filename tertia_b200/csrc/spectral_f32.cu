@@ -49,7 +49,7 @@ __global__ void __launch_bounds__(kThreads) predictor_f32_kernel(SpecArgs<float>
     if (j >= a.ny) return;
     pdl_wait();
     const size_t n = (size_t)j + (size_t)a.ny * k;
-    const Modes2 o = predictor_modes2(a, j, k, n);
+    const Modes2<float> o = predictor_modes2(a, j, k, n);
     pdl_trigger();
     store_modes2(a, n, o);
     put_split2<KIND, NSPLIT>(a, 0, n, o.ex[0], o.ex[1]);
@@ -69,7 +69,7 @@ __global__ void __launch_bounds__(kThreads) corrector_f32_kernel(SpecArgs<float>
     if (j < a.ny) {
         const size_t n = (size_t)j + (size_t)a.ny * k;
         const float2 jx2 = ld2(a.Jx, n);
-        const Modes2 o = corrector_modes2(a, j, k, n, jx2, ld2(a.Jy, n), ld2(a.Jz, n));
+        const Modes2<float> o = corrector_modes2(a, j, k, n, jx2, ld2(a.Jy, n), ld2(a.Jz, n));
         pdl_trigger();
         store_modes2(a, n, o);
         put_split2<KIND, NSPLIT>(a, 0, n, o.ex[0], o.ex[1]);

@@ -1,15 +1,16 @@
-// spectral_f32.cuh — the FP32 per-mode predictor / corrector maps
+// spectral_f32.cuh — the fast per-mode predictor / corrector maps
 // (GuessFieldsHydroLinLayerSplit, movefieldshydrolinlayersplit.cpp:808-900;
 // IterateFieldsHydroLinLayerSplit, :1374-1477) on two adjacent modes, shared
-// by the map kernels (spectral_f32.cu) and the transform kernels that apply
-// them between the two halves of a transform (dtt_fft.cu).
+// by the FP32 map kernels (spectral_f32.cu) and the kernels that apply them
+// between the two halves of a transform (dtt_fft.cu: FP32, and FP64 on the
+// FFT path).  R is the real type.
 //
 // Same algebra as predictor_kernel / corrector_kernel in spectral.cu, arranged
 // for the GPU rather than for bit-exact agreement with the oracle: the five
 // divisions of a mode become two reciprocals, 1/k^2 and 1/(k^2 + density),
 // plus uniform constants; beam-spectrum terms whose xi-interpolation weight
 // is zero are not read; FMA contraction is allowed.  The results differ from
-// the literal forms by a few FP32 ulp.
+// the literal forms by a few ulp.
 #pragma once
 #include "qs_common.cuh"
 #include "qs_internal.h"
@@ -17,33 +18,45 @@
 namespace qs {
 namespace specf32 {
 
-__device__ __forceinline__ float2 ld2(const float* p, size_t n) {
-    return __ldg(reinterpret_cast<const float2*>(p + n));
+template <class R> struct Pair2;
+template <> struct Pair2<float> { using type = float2; };
+template <> struct Pair2<double> { using type = double2; };
+template <class R> using pair_t = typename Pair2<R>::type;
+
+template <class R>
+__device__ __forceinline__ pair_t<R> ld2(const R* p, size_t n) {
+    return __ldg(reinterpret_cast<const pair_t<R>*>(p + n));
 }
-__device__ __forceinline__ void st2(float* p, size_t n, float a, float b) {
-    *reinterpret_cast<float2*>(p + n) = make_float2(a, b);
+template <class R>
+__device__ __forceinline__ void st2(R* p, size_t n, R a, R b) {
+    pair_t<R> v;
+    v.x = a;
+    v.y = b;
+    *reinterpret_cast<pair_t<R>*>(p + n) = v;
 }
 
 // beam terms of two modes; layers whose weight is zero are not read
-struct BeamPair { float rb[2], rbp[2], jxb[2]; };
+template <class R>
+struct BeamPair { R rb[2], rbp[2], jxb[2]; };
 
-__device__ __forceinline__ BeamPair beam_pair(const SpecArgs<float>& a, size_t n) {
-    BeamPair b;
-    float2 r = ld2(a.Rb0, n), jx = ld2(a.Jxb0, n);
+template <class R>
+__device__ __forceinline__ BeamPair<R> beam_pair(const SpecArgs<R>& a, size_t n) {
+    BeamPair<R> b;
+    pair_t<R> r = ld2(a.Rb0, n), jx = ld2(a.Jxb0, n);
     b.rb[0] = a.wb0 * r.x; b.rb[1] = a.wb0 * r.y;
     b.jxb[0] = a.wb0 * jx.x; b.jxb[1] = a.wb0 * jx.y;
-    if (a.wb1 != 0.f) {
+    if (a.wb1 != R(0)) {
         r = ld2(a.Rb1, n);
         jx = ld2(a.Jxb1, n);
         b.rb[0] += a.wb1 * r.x; b.rb[1] += a.wb1 * r.y;
         b.jxb[0] += a.wb1 * jx.x; b.jxb[1] += a.wb1 * jx.y;
     }
-    b.rbp[0] = b.rbp[1] = 0.f;
-    if (a.wp0 != 0.f) {
+    b.rbp[0] = b.rbp[1] = R(0);
+    if (a.wp0 != R(0)) {
         r = ld2(a.Rbp0, n);
         b.rbp[0] = a.wp0 * r.x; b.rbp[1] = a.wp0 * r.y;
     }
-    if (a.wp1 != 0.f) {
+    if (a.wp1 != R(0)) {
         r = ld2(a.Rbp1, n);
         b.rbp[0] += a.wp1 * r.x; b.rbp[1] += a.wp1 * r.y;
     }
@@ -51,53 +64,56 @@ __device__ __forceinline__ BeamPair beam_pair(const SpecArgs<float>& a, size_t n
 }
 
 // clear two modes of the 4 deposit planes the next push adds to
-__device__ __forceinline__ void zero_src2(const SpecArgs<float>& a, size_t n) {
+template <class R>
+__device__ __forceinline__ void zero_src2(const SpecArgs<R>& a, size_t n) {
     if (a.zero_src) {
         const size_t N = (size_t)a.ny * a.nz;
 #pragma unroll
-        for (int q = 0; q < 4; q++) st2(a.zero_src + q * N, n, 0.f, 0.f);
+        for (int q = 0; q < 4; q++) st2(a.zero_src + q * N, n, R(0), R(0));
     }
 }
 
 // outputs of the maps on two modes
+template <class R>
 struct Modes2 {
-    float rho[2], ex[2], ey[2], ez[2], bx[2], by[2], bz[2];
+    R rho[2], ex[2], ey[2], ez[2], bx[2], by[2], bz[2];
 };
 
 // Guess (:843-872) on modes (j, k), (j+1, k); n = j + ny k
-__device__ __forceinline__ Modes2 predictor_modes2(const SpecArgs<float>& a, int j, int k,
-                                                   size_t n) {
-    const float d = *a.dens_p, hx = a.hx;
-    const float dh2 = d * hx * hx;
-    const float inv_den = 1.f / (4.f + dh2);
-    const float propagator = (4.f - dh2) * inv_den;
-    const float c_rb = dh2 * inv_den;            // (rb + rbp) d hx^2 / denominator
-    const float c_ex = 4.f * hx * inv_den;       // 4 Ex hx (k^2 + d) / denominator
-    const float c_rho = 2.f * d * hx * inv_den;  // 2 (2 rp + rb + rbp) d hx / ((k^2+d) den)
-    const float akz = a.piZ * ((float)k + 0.5f);
-    const float2 rp2 = ld2(a.RhoP, n), jxp2 = ld2(a.JxP, n), jyp2 = ld2(a.JyP, n),
-                 jzp2 = ld2(a.JzP, n), exp2 = ld2(a.ExP, n), eyp2 = ld2(a.EyP, n),
-                 ezp2 = ld2(a.EzP, n);
-    const BeamPair b = beam_pair(a, n);
-    const float rp_[2] = {rp2.x, rp2.y}, jxp_[2] = {jxp2.x, jxp2.y}, jyp_[2] = {jyp2.x, jyp2.y},
-                jzp_[2] = {jzp2.x, jzp2.y}, exp_[2] = {exp2.x, exp2.y},
-                eyp_[2] = {eyp2.x, eyp2.y}, ezp_[2] = {ezp2.x, ezp2.y};
-    Modes2 o;
+template <class R>
+__device__ __forceinline__ Modes2<R> predictor_modes2(const SpecArgs<R>& a, int j, int k,
+                                                      size_t n) {
+    const R d = *a.dens_p, hx = a.hx;
+    const R dh2 = d * hx * hx;
+    const R inv_den = R(1) / (R(4) + dh2);
+    const R propagator = (R(4) - dh2) * inv_den;
+    const R c_rb = dh2 * inv_den;            // (rb + rbp) d hx^2 / denominator
+    const R c_ex = R(4) * hx * inv_den;      // 4 Ex hx (k^2 + d) / denominator
+    const R c_rho = R(2) * d * hx * inv_den; // 2 (2 rp + rb + rbp) d hx / ((k^2+d) den)
+    const R akz = a.piZ * ((R)k + R(0.5));
+    const pair_t<R> rp2 = ld2(a.RhoP, n), jxp2 = ld2(a.JxP, n), jyp2 = ld2(a.JyP, n),
+                    jzp2 = ld2(a.JzP, n), exp2 = ld2(a.ExP, n), eyp2 = ld2(a.EyP, n),
+                    ezp2 = ld2(a.EzP, n);
+    const BeamPair<R> b = beam_pair(a, n);
+    const R rp_[2] = {rp2.x, rp2.y}, jxp_[2] = {jxp2.x, jxp2.y}, jyp_[2] = {jyp2.x, jyp2.y},
+            jzp_[2] = {jzp2.x, jzp2.y}, exp_[2] = {exp2.x, exp2.y},
+            eyp_[2] = {eyp2.x, eyp2.y}, ezp_[2] = {ezp2.x, ezp2.y};
+    Modes2<R> o;
 #pragma unroll
     for (int q = 0; q < 2; q++) {
-        const float aky = a.piY * ((float)(j + q) + 0.5f);
-        const float ak2 = aky * aky + akz * akz;
-        const float inv_ak2 = 1.f / ak2;
-        const float inv_dk = 1.f / (d + ak2);
-        const float rp = rp_[q], rbs = b.rb[q] + b.rbp[q];
+        const R aky = a.piY * ((R)(j + q) + R(0.5));
+        const R ak2 = aky * aky + akz * akz;
+        const R inv_ak2 = R(1) / ak2;
+        const R inv_dk = R(1) / (d + ak2);
+        const R rp = rp_[q], rbs = b.rb[q] + b.rbp[q];
         o.rho[q] = propagator * rp - rbs * c_rb + c_ex * exp_[q] * (ak2 + d);
-        o.ex[q] = propagator * exp_[q] - (2.f * rp + rbs) * c_rho * inv_dk;
-        const float srcE = (rbs + rp + o.rho[q]) * inv_dk;
+        o.ex[q] = propagator * exp_[q] - (R(2) * rp + rbs) * c_rho * inv_dk;
+        const R srcE = (rbs + rp + o.rho[q]) * inv_dk;
         o.ey[q] = -eyp_[q] + aky * srcE;
         o.ez[q] = -ezp_[q] + akz * srcE;
-        const float jy = jyp_[q] + 0.5f * hx * d * (o.ey[q] + eyp_[q]);
-        const float jz = jzp_[q] + 0.5f * hx * d * (o.ez[q] + ezp_[q]);
-        const float jx = jxp_[q] + 0.5f * hx * d * (o.ex[q] + exp_[q]);
+        const R jy = jyp_[q] + R(0.5) * hx * d * (o.ey[q] + eyp_[q]);
+        const R jz = jzp_[q] + R(0.5) * hx * d * (o.ez[q] + ezp_[q]);
+        const R jx = jxp_[q] + R(0.5) * hx * d * (o.ex[q] + exp_[q]);
         o.bx[q] = (akz * jy - aky * jz) * inv_ak2;
         o.by[q] = (-akz * (jx + b.jxb[q]) + d * o.ez[q]) * inv_ak2;
         o.bz[q] = (aky * (jx + b.jxb[q]) - d * o.ey[q]) * inv_ak2;
@@ -107,30 +123,31 @@ __device__ __forceinline__ Modes2 predictor_modes2(const SpecArgs<float>& a, int
 
 // Iterate (:1419-1466) on modes (j, k), (j+1, k) with the C-deposit spectra
 // jx2, jy2, jz2 of the two modes
-__device__ __forceinline__ Modes2 corrector_modes2(const SpecArgs<float>& a, int j, int k,
-                                                   size_t n, float2 jx2, float2 jy2,
-                                                   float2 jz2) {
-    const float d = *a.dens_p, hx = a.hx;
-    const float akz = a.piZ * ((float)k + 0.5f);
-    const float2 rp2 = ld2(a.RhoP, n), jxp2 = ld2(a.JxP, n), jyp2 = ld2(a.JyP, n),
-                 jzp2 = ld2(a.JzP, n), eyp2 = ld2(a.EyP, n), ezp2 = ld2(a.EzP, n),
-                 rold2 = ld2(a.Rho, n);
-    const BeamPair b = beam_pair(a, n);
-    const float rp_[2] = {rp2.x, rp2.y}, jx_[2] = {jx2.x, jx2.y}, jy_[2] = {jy2.x, jy2.y},
-                jz_[2] = {jz2.x, jz2.y}, jxp_[2] = {jxp2.x, jxp2.y}, jyp_[2] = {jyp2.x, jyp2.y},
-                jzp_[2] = {jzp2.x, jzp2.y}, eyp_[2] = {eyp2.x, eyp2.y},
-                ezp_[2] = {ezp2.x, ezp2.y}, rold_[2] = {rold2.x, rold2.y};
-    Modes2 o;
+template <class R>
+__device__ __forceinline__ Modes2<R> corrector_modes2(const SpecArgs<R>& a, int j, int k,
+                                                      size_t n, pair_t<R> jx2, pair_t<R> jy2,
+                                                      pair_t<R> jz2) {
+    const R d = *a.dens_p, hx = a.hx;
+    const R akz = a.piZ * ((R)k + R(0.5));
+    const pair_t<R> rp2 = ld2(a.RhoP, n), jxp2 = ld2(a.JxP, n), jyp2 = ld2(a.JyP, n),
+                    jzp2 = ld2(a.JzP, n), eyp2 = ld2(a.EyP, n), ezp2 = ld2(a.EzP, n),
+                    rold2 = ld2(a.Rho, n);
+    const BeamPair<R> b = beam_pair(a, n);
+    const R rp_[2] = {rp2.x, rp2.y}, jx_[2] = {jx2.x, jx2.y}, jy_[2] = {jy2.x, jy2.y},
+            jz_[2] = {jz2.x, jz2.y}, jxp_[2] = {jxp2.x, jxp2.y}, jyp_[2] = {jyp2.x, jyp2.y},
+            jzp_[2] = {jzp2.x, jzp2.y}, eyp_[2] = {eyp2.x, eyp2.y},
+            ezp_[2] = {ezp2.x, ezp2.y}, rold_[2] = {rold2.x, rold2.y};
+    Modes2<R> o;
 #pragma unroll
     for (int q = 0; q < 2; q++) {
-        const float aky = a.piY * ((float)(j + q) + 0.5f);
-        const float ak2 = aky * aky + akz * akz;
-        const float inv_ak2 = 1.f / ak2;
-        const float inv_dk = 1.f / (d + ak2);
-        const float jx = jx_[q], jy = jy_[q], jz = jz_[q];
-        o.rho[q] = rp_[q] + jx - jxp_[q] - 0.5f * hx * (aky * (jy + jyp_[q]) + akz * (jz + jzp_[q]));
+        const R aky = a.piY * ((R)(j + q) + R(0.5));
+        const R ak2 = aky * aky + akz * akz;
+        const R inv_ak2 = R(1) / ak2;
+        const R inv_dk = R(1) / (d + ak2);
+        const R jx = jx_[q], jy = jy_[q], jz = jz_[q];
+        o.rho[q] = rp_[q] + jx - jxp_[q] - R(0.5) * hx * (aky * (jy + jyp_[q]) + akz * (jz + jzp_[q]));
         o.ex[q] = -(aky * jy + akz * jz) * inv_ak2;
-        const float srcE = (b.rb[q] + b.rbp[q] + rp_[q] + rold_[q]) * inv_dk;
+        const R srcE = (b.rb[q] + b.rbp[q] + rp_[q] + rold_[q]) * inv_dk;
         o.ey[q] = -eyp_[q] + aky * srcE;
         o.ez[q] = -ezp_[q] + akz * srcE;
         o.bx[q] = (akz * jy - aky * jz) * inv_ak2;
@@ -142,7 +159,8 @@ __device__ __forceinline__ Modes2 corrector_modes2(const SpecArgs<float>& a, int
 
 // Rho, Ex, Ey, Ez (and B when kept) into the spectral bank, and the two modes
 // of the next push's deposit planes cleared
-__device__ __forceinline__ void store_modes2(const SpecArgs<float>& a, size_t n, const Modes2& o) {
+template <class R>
+__device__ __forceinline__ void store_modes2(const SpecArgs<R>& a, size_t n, const Modes2<R>& o) {
     st2(a.Rho, n, o.rho[0], o.rho[1]);
     st2(a.Ex, n, o.ex[0], o.ex[1]);
     st2(a.Ey, n, o.ey[0], o.ey[1]);
