@@ -7,7 +7,7 @@ into QS_ERR_TIMEOUT.  qs_selftest_wait_limit runs that wait routine on a
 barrier that nothing completes (a flag nobody sets) for a few tries.
 The call must report QS_ERR_TIMEOUT, clear the flag, and leave the handle
 usable: a march on the same handle afterwards agrees with one on a fresh
-handle.
+handle (to FP32 rounding: the deposits add by atomics).
 """
 import numpy as np
 import pytest
@@ -34,5 +34,7 @@ def test_wait_limit_runs_out_and_reports():
             h.load_beam(beam)
             h.load_front_plasma(front)
             h.step()
-        np.testing.assert_array_equal(m.onaxis_ex(), ref.onaxis_ex())
-        assert np.abs(ref.onaxis_ex()).max() > 0
+        # FP32 deposits add by atomics, so two marches agree to rounding only
+        scale = np.abs(ref.onaxis_ex()).max()
+        assert scale > 0
+        np.testing.assert_allclose(m.onaxis_ex(), ref.onaxis_ex(), rtol=0, atol=1e-6 * scale)
