@@ -156,3 +156,38 @@ def test_device_seeding_is_deterministic():
     assert not np.array_equal(a["px"], c["px"])
     assert abs(np.std(a["py"]) - 0.01) < 1e-3
     assert np.allclose(a["w"], cfg.plasma_density / cfg.ppc)
+
+
+@pytest.mark.parametrize("prec,tol", [("fp64fft", 1e-12), ("fp32", 1e-5)])
+def test_side_streams_and_fused_maps_match_the_sequential_march(prec, tol):
+    """Inside a march the last E/B transform of each layer and the plasma
+    regrouping run on side streams, and (with the maps between the halves of
+    the transforms, ny >= 128) the last corrector kernel of a layer also runs
+    the next layer's predictor.  With per-kernel timing on, the same march runs
+    strictly in order with a predictor kernel of its own per layer.  Both give
+    the same fields and plasma (FP32: to the rounding of its atomic deposits)."""
+    from tertia_b200.mesh import Mesh
+    cfg = cfg_for(prec, n=128, layers=24, pspread_x=0.01, pspread_y=0.01, pspread_z=0.01)
+    beam = wl.small_beam(cfg, n=20000)
+    front = wl.front_plasma(cfg, seed=3)
+    out = {}
+    for timed in (False, True):
+        with Mesh(cfg) as m:
+            m.profile_enable(timed)
+            m.load_beam(beam)
+            m.load_front_plasma(front)
+            m.step()
+            out[timed] = (m.onaxis_ex(), fields_all(m, cfg), m.get_plasma())
+            if timed:
+                prof = m.profile_read()
+                assert sum(n for _, n in prof.values()) > 0   # it did run per kernel
+    (e0, f0, p0), (e1, f1, p1) = out[False], out[True]
+    assert np.max(np.abs(e1)) > 1e-4
+    assert rel_l2(e0, e1) < tol
+    assert rel_l2(f0, f1) < tol
+    if prec == "fp64fft":
+        assert np.array_equal(p0["cell"], p1["cell"])
+    else:
+        assert np.mean(p0["cell"] == p1["cell"]) > 0.9999
+    for k in ("px", "py", "pz"):
+        assert rel_l2(p0[k], p1[k]) < tol * 10
