@@ -159,16 +159,6 @@ __device__ __forceinline__ void tmem_wait_ld() {
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
-#ifdef QS_TC_TRACE
-// stage timestamps of CTA (0,0,0), read by a probe build only
-__device__ long long g_tc_trace[256];
-__device__ __forceinline__ void trace(int slot) {
-    if (blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0 && slot < 256)
-        g_tc_trace[slot] = clock64();
-}
-#else
-__device__ __forceinline__ void trace(int) {}
-#endif
 
 // ------------------------------------------------------------ the GEMM
 // Product terms (matrix split index, data split index), small terms first.
@@ -228,7 +218,6 @@ __global__ void __launch_bounds__(THREADS_V2, 1)
     const int promo = p.promo;
     const int nchunks = nkb / promo;
     const int kind = (int)((p.kindmask >> f) & 1ull);
-    if (threadIdx.x == 0) trace(0);
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < STAGES; s++) {
@@ -254,7 +243,6 @@ __global__ void __launch_bounds__(THREADS_V2, 1)
     fence_after();
     const uint32_t tmem = tmem_slot;
     volatile int* abortp = &abort_flag;
-    if (threadIdx.x == 0) trace(1);
     qs::pdl_wait();   // operands and outputs are the previous kernel's
 
     if (warp == 0) {
@@ -275,7 +263,6 @@ __global__ void __launch_bounds__(THREADS_V2, 1)
                     break;
                 }
                 const uint32_t fb = smem_u32(&full_bar[s]);
-                trace(16 + kb);
                 mbar_expect_tx(fb, STAGE);
                 uint8_t* st = smem + (size_t)s * STAGE;
 #pragma unroll
@@ -319,7 +306,6 @@ __global__ void __launch_bounds__(THREADS_V2, 1)
                         ok = false;
                         break;
                     }
-                    trace(64 + kb);
                     fence_after();
                     const uint32_t st = smem_u32(smem + (size_t)s * STAGE);
                     const uint64_t dM = sw128_desc(st);
@@ -337,7 +323,6 @@ __global__ void __launch_bounds__(THREADS_V2, 1)
                         }
                     }
                     mma_commit(smem_u32(&empty_bar[s]));
-                    trace(112 + kb);
                 }
                 if (ok) mma_commit(smem_u32(&accf[b]));
             }
@@ -361,7 +346,6 @@ __global__ void __launch_bounds__(THREADS_V2, 1)
                 *abortp = 1;
                 break;
             }
-            if (threadIdx.x == 64) trace(160 + c);
             fence_after();
 #pragma unroll
             for (int j = 0; j < HC; j += 16) {
@@ -441,11 +425,9 @@ __global__ void __launch_bounds__(THREADS_V2, 1)
         } else if (lane == 0 && e == 0) {
             atomicOr(p.err, DEV_ERR_TIMEOUT);
         }
-        if (threadIdx.x == 64) trace(200);
     }
     fence_before();
     __syncthreads();
-    if (threadIdx.x == 0) trace(201);
     if (warp == 2) {
         fence_after();
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
@@ -799,11 +781,6 @@ public:
 
 }  // namespace
 
-#ifdef QS_TC_TRACE
-extern "C" int qs_tc_trace_read(long long* out) {
-    return (int)cudaMemcpyFromSymbol(out, tcx::g_tc_trace, sizeof(long long) * 256);
-}
-#endif
 
 TcTransformer* TcTransformer::create(int mode, int ny, int nz, int* err_flag, std::string& why) {
     auto* t = new TcImpl();
