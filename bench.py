@@ -838,26 +838,31 @@ def run_ours(args):
     # repeated with the launches queued ahead of the GPU
     gemm = None
     fftp = None
-    # the CIC push (the dominant kernel of the FP32 march): the half push of the
-    # head layer repeated through the fine-grained entry points, each launch
-    # bracketed by events on the handle's stream (one push per call)
+    # the CIC push (the dominant kernel of the FP32 march): the half push and
+    # the full push of the head layer, each repeated through the fine-grained
+    # entry points with every launch bracketed by events on the handle's
+    # stream (one push per call; the full push stores the particles, and every
+    # second one is followed by the regrouping, timed apart)
     pushk = None
     if cfg.shape == QS_SHAPE_CIC:
         m.load_front_plasma(wl.front_plasma(cfg, seed=5))
         m.begin_march()
         m.layer_begin(cfg.nx - 1, 0)
         m.guess_fields(cfg.nx - 1, 0)
-        for _ in range(3):
-            m.move_particles_layer(cfg.nx - 1, 0, 0)
-        m.sync()
-        m.profile_enable(True)
-        for _ in range(40):
-            m.move_particles_layer(cfg.nx - 1, 0, 0)
-        pp = m.profile_read()
-        m.profile_enable(False)
-        p_ms, p_n = pp["push_deposit"]
-        pushk = {"launches": p_n, "avg_launch_us": p_ms * 1e3 / max(p_n, 1),
-                 "particles": cfg.ny * cfg.nz * cfg.ppc}
+        pushk = {"particles": cfg.ny * cfg.nz * cfg.ppc}
+        for kind, full in (("half", 0), ("full", 1)):
+            for _ in range(3):
+                m.move_particles_layer(cfg.nx - 1, 0, full)
+            m.sync()
+            m.profile_enable(True)
+            for _ in range(40):
+                m.move_particles_layer(cfg.nx - 1, 0, full)
+            pp = m.profile_read()
+            m.profile_enable(False)
+            p_ms, p_n = pp["push_deposit"]
+            pushk[kind] = {"launches": p_n, "avg_launch_us": p_ms * 1e3 / max(p_n, 1)}
+        pushk["avg_launch_us"] = 0.5 * (pushk["half"]["avg_launch_us"] +
+                                        pushk["full"]["avg_launch_us"])
     if args.precision == "fp32":
         # FFT passes (power-of-two grids): 2 launches per transform, each
         # reading and writing the 6 planes once
@@ -947,15 +952,24 @@ def run_ours(args):
         # + (nIter+1) * (3 forward J + 6 inverse E, B) + 2 beam planes
         roof["march_transforms_per_layer"] = 6 + (nit + 1) * 9 + 2
     elif pushk:
-        # one launch = one sub-push of every plasma particle: 28 B of particle
-        # state read + the P and C fields (12 values) and the deposit (4
-        # values) of its cell shared by the ppc particles, 4 B each
-        bpp = 28.0 + 16.0 * 4.0 / cfg.ppc
+        # a layer pushes every plasma particle twice (nIter = 1): the half push
+        # reads 28 B of particle state plus the P and C fields (12 values) and
+        # the deposit (4 values) of its cell shared by the ppc particles, 4 B
+        # each; the full push also writes the 24 B of state.  112 B per
+        # particle-layer push over the two launches, 56 B per launch on average
+        b_half = 28.0 + 16.0 * 4.0 / cfg.ppc
+        b_full = b_half + 24.0
+        bpp = 0.5 * (b_half + b_full)
         bytes_launch = bpp * pushk["particles"]
         achieved = bytes_launch / (pushk["avg_launch_us"] / 1e6) / 1e9
+        for kind, b in (("half", b_half), ("full", b_full)):
+            pushk[kind]["bytes_per_particle"] = b
+            pushk[kind]["achieved_gbs"] = (b * pushk["particles"] /
+                                           (pushk[kind]["avg_launch_us"] / 1e6) / 1e9)
         roof = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                 "frac": achieved / hbm, "peak_source": f"hbm_gbs of {src}",
-                "kernel": "push_cic_row_kernel (CIC push + deposit, half step)",
+                "kernel": "push_cic_row_kernel (CIC push + deposit; the half and the full push "
+                          "of a layer, averaged per launch)",
                 "bytes_per_particle": bpp, "bytes_per_launch": bytes_launch,
                 "avg_launch_us": pushk["avg_launch_us"], "timing": pushk}
         if fftp:
