@@ -191,3 +191,28 @@ def test_side_streams_and_fused_maps_match_the_sequential_march(prec, tol):
         assert np.mean(p0["cell"] == p1["cell"]) > 0.9999
     for k in ("px", "py", "pz"):
         assert rel_l2(p0[k], p1[k]) < tol * 10
+
+
+@pytest.mark.parametrize("prec,shape", [("fp64", "ngp"), ("fp64", "cic"), ("fp64fft", "cic"),
+                                        ("fp32", "cic")])
+def test_split_layers_match_oracle(oracle_lib, prec, shape):
+    """NxSplit = 2: each layer is marched in two sub-layers of hx/2 with the
+    beam currents interpolated between the layers (movepart_splitlayer.cpp:
+    561-778, the split weights of :430-445); in FP32 and in FP64 on FFT
+    transforms the plasma is regrouped across the splits as well."""
+    from tertia_b200.abi import QS_SHAPE_NGP
+    cfg = cfg_for(prec, n=32, layers=24, pspread_x=0.01, pspread_y=0.01, pspread_z=0.01)
+    cfg.nx_split = 2
+    cfg.shape = QS_SHAPE_CIC if shape == "cic" else QS_SHAPE_NGP
+    beam = wl.small_beam(cfg, n=6000)
+    fronts = [wl.front_plasma(cfg, seed=7)]
+    o, m = run_pair(oracle_lib, cfg, beam, fronts)
+    e_o, e_m = o.onaxis_ex(), m.onaxis_ex()
+    assert np.max(np.abs(e_o)) > 1e-3
+    assert rel_l2(e_m, e_o) < TOL[prec]
+    assert rel_l2(fields_all(m, cfg), fields_all(o, cfg)) < TOL[prec]
+    po, pm = o.get_plasma(), m.get_plasma()
+    if prec.startswith("fp64"):
+        assert np.array_equal(pm["cell"], po["cell"])
+    for k in ("px", "py", "pz"):
+        assert rel_l2(pm[k], po[k]) < TOL[prec] * 10
