@@ -216,3 +216,26 @@ def test_split_layers_match_oracle(oracle_lib, prec, shape):
         assert np.array_equal(pm["cell"], po["cell"])
     for k in ("px", "py", "pz"):
         assert rel_l2(pm[k], po[k]) < TOL[prec] * 10
+
+
+@pytest.mark.parametrize("prec", ["fp64", "fp64fft", "fp32"])
+def test_two_corrector_iterations_match_oracle(oracle_lib, prec):
+    """nIter = 2 (two predictor-corrector passes before the full push,
+    movepart_splitlayer.cpp:561-778) on a 128 x 128 grid, where the FP32 and
+    FP64-FFT paths run the maps between the halves of their transforms and
+    fuse the next layer's predictor into the last corrector."""
+    cfg = cfg_for(prec, n=128, layers=16, pspread_x=0.01, pspread_y=0.01, pspread_z=0.01)
+    cfg.n_iter = 2
+    cfg.shape = QS_SHAPE_CIC
+    beam = wl.small_beam(cfg, n=20000)
+    fronts = [wl.front_plasma(cfg, seed=9)]
+    o, m = run_pair(oracle_lib, cfg, beam, fronts)
+    e_o, e_m = o.onaxis_ex(), m.onaxis_ex()
+    assert np.max(np.abs(e_o)) > 1e-3
+    assert rel_l2(e_m, e_o) < TOL[prec]
+    assert rel_l2(fields_all(m, cfg), fields_all(o, cfg)) < TOL[prec]
+    po, pm = o.get_plasma(), m.get_plasma()
+    if prec.startswith("fp64"):
+        assert np.array_equal(pm["cell"], po["cell"])
+    for k in ("px", "py", "pz"):
+        assert rel_l2(pm[k], po[k]) < TOL[prec] * 10
