@@ -562,6 +562,39 @@ struct RowMath<double> {
     static __device__ __forceinline__ double div(double a, double b) { return a / b; }
 };
 
+// Field pairs of the grouped push's tile, (Ex, Ey), (Ez, Bx), (By, Bz): in
+// FP32 the packed instructions of sm_100 (__ffma2_rn and friends: two FP32
+// lanes, each rounded as fmaf, so the sums are those of the scalar chain),
+// in FP64 two FMAs.
+template <class T>
+struct FPair;
+template <>
+struct FPair<float> {
+    using type = float2;
+    static __device__ __forceinline__ float2 make(float x, float y) { return make_float2(x, y); }
+    static __device__ __forceinline__ float2 add(float2 a, float2 b) { return __fadd2_rn(a, b); }
+    static __device__ __forceinline__ float2 mul(float s, float2 v) {
+        return __fmul2_rn(make_float2(s, s), v);
+    }
+    static __device__ __forceinline__ float2 fma(float s, float2 v, float2 c) {
+        return __ffma2_rn(make_float2(s, s), v, c);
+    }
+};
+template <>
+struct FPair<double> {
+    using type = double2;
+    static __device__ __forceinline__ double2 make(double x, double y) { return make_double2(x, y); }
+    static __device__ __forceinline__ double2 add(double2 a, double2 b) {
+        return make_double2(a.x + b.x, a.y + b.y);
+    }
+    static __device__ __forceinline__ double2 mul(double s, double2 v) {
+        return make_double2(s * v.x, s * v.y);
+    }
+    static __device__ __forceinline__ double2 fma(double s, double2 v, double2 c) {
+        return make_double2(::fma(s, v.x, c.x), ::fma(s, v.y, c.y));
+    }
+};
+
 // one CIC sub-step of a particle (cell-relative move from base cell (jb, kb),
 // periodic wrap, the 4 corner weights of the new position)
 template <class T>
@@ -587,12 +620,14 @@ __device__ __forceinline__ void cic_substep(T dy, T dz, T ps, T& ytmp, T& ztmp, 
 template <int TY, int ND, int WIN, class T>
 __global__ void __launch_bounds__(32 * TY) push_cic_row_kernel(PushArgs<T> a) {
     using M = RowMath<T>;
-    constexpr int TX = 32, W = TX + 1, H = TY + 1, NV = 4 * ND;
+    using FP = FPair<T>;
+    using P2 = typename FP::type;
+    constexpr int TX = 32, W = TX + 1, H = TY + 1;
     constexpr int NS = ND + 2;           // staged per slot: ND charges, in-cell y and z
     constexpr int WP = WIN + WIN / 32;   // one pad word per 32 slots
     static_assert(WIN % 32 == 0, "whole warps per window");
     const T one = T(1), zero = T(0), half = T(0.5);
-    __shared__ T Fs[6][H][W];            // fields of the tile cells + one row/column (P, C averaged)
+    __shared__ P2 Fs[3][H][W];           // field pairs of the tile cells + one row/column (P, C averaged)
     __shared__ T Tt[ND][H][W];           // block deposit tile [current][row][col]
     __shared__ T S[TY][NS][WP];          // staged deposits of the window
     __shared__ int K[TY][2][WP];         // [0]: first sub-step's cell (-1: none); [1]: final cell
@@ -607,7 +642,11 @@ __global__ void __launch_bounds__(32 * TY) push_cic_row_kernel(PushArgs<T> a) {
         const int r = i / W, cc = i - r * W;
         const size_t m = (size_t)wrap1(j0 + cc, My) + (size_t)My * wrap1(k0 + r, Mz);
 #pragma unroll
-        for (int f = 0; f < 6; f++) Fs[f][r][cc] = half * (ld(a.P + f * plane + m) + ld(a.C + f * plane + m));
+        for (int q = 0; q < 3; q++) {
+            const P2 pp = FP::make(ld(a.P + 2 * q * plane + m), ld(a.P + (2 * q + 1) * plane + m));
+            const P2 cp = FP::make(ld(a.C + 2 * q * plane + m), ld(a.C + (2 * q + 1) * plane + m));
+            Fs[q][r][cc] = FP::mul(half, FP::add(pp, cp));
+        }
     }
     __syncthreads();
     // the tile's own cells of the gathered fields, for the push adjoint (the
@@ -618,7 +657,10 @@ __global__ void __launch_bounds__(32 * TY) push_cic_row_kernel(PushArgs<T> a) {
                 const int r = i / TX, cc = i - r * TX;
                 const size_t m = (size_t)(j0 + cc) + (size_t)My * (k0 + r);
 #pragma unroll
-                for (int f = 0; f < 6; f++) a.favg[f * plane + m] = Fs[f][r][cc];
+                for (int q = 0; q < 3; q++) {
+                    a.favg[2 * q * plane + m] = Fs[q][r][cc].x;
+                    a.favg[(2 * q + 1) * plane + m] = Fs[q][r][cc].y;
+                }
             }
     const int c0 = j0 + My * (k0 + wr);   // this warp's 32 cells: c0 .. c0+31
     const int mycell = c0 + lane;
@@ -628,9 +670,10 @@ __global__ void __launch_bounds__(32 * TY) push_cic_row_kernel(PushArgs<T> a) {
     const int pend = __shfl_sync(0xffffffffu, hi, 31);
     const bool count = a.full && a.cnt;
     int stay = 0;                        // particles that end the full push in mycell
-    T acc[NV];
+    // the cell's sums of current d at its corners (0, 1) and (2, 3)
+    P2 acc[ND][2];
 #pragma unroll
-    for (int i = 0; i < NV; i++) acc[i] = zero;
+    for (int d = 0; d < ND; d++) acc[d][0] = acc[d][1] = FP::make(zero, zero);
     // the particle of the next pass is loaded while this one is pushed
     int nx_cell = 0;
     T nx_y = zero, nx_z = zero, nx_px = zero, nx_py = zero, nx_pz = zero, nx_w = zero;
@@ -668,9 +711,14 @@ __global__ void __launch_bounds__(32 * TY) push_cic_row_kernel(PushArgs<T> a) {
                     const int tj = j - j0, tk = k - k0;
                     if (tj >= 0 && tj < TX && tk >= 0 && tk < TY) {
 #pragma unroll
-                        for (int f = 0; f < 6; f++)
-                            g[f] = wg[0] * Fs[f][tk][tj] + wg[1] * Fs[f][tk][tj + 1] +
-                                   wg[2] * Fs[f][tk + 1][tj] + wg[3] * Fs[f][tk + 1][tj + 1];
+                        for (int q = 0; q < 3; q++) {
+                            P2 gq = FP::mul(wg[0], Fs[q][tk][tj]);
+                            gq = FP::fma(wg[1], Fs[q][tk][tj + 1], gq);
+                            gq = FP::fma(wg[2], Fs[q][tk + 1][tj], gq);
+                            gq = FP::fma(wg[3], Fs[q][tk + 1][tj + 1], gq);
+                            g[2 * q] = gq.x;
+                            g[2 * q + 1] = gq.y;
+                        }
                     } else {
                         const int j1 = wrap1(j + 1, My), k1 = wrap1(k + 1, Mz);
                         const size_t nn[4] = {(size_t)j + (size_t)My * k,
@@ -711,16 +759,15 @@ __global__ void __launch_bounds__(32 * TY) push_cic_row_kernel(PushArgs<T> a) {
                     const T dq[4] = {wq * a.djx0 * Vxm, wq * a.djy0 * Vym, wq * a.djz0 * Vzm,
                                      wq * a.drho0};
                     const T dy = Vy * a.hxhy * inv2, dz = Vz * a.hxhz * inv2;
-                    T partdx = zero, step = one;
-                    if (fabs_t(dy) > one || fabs_t(dz) > one)
-                        step = partdx = fabs_t(dy) > fabs_t(dz) ? fabs_t(dy) : fabs_t(dz);
-                    if (partdx < one) partdx = step = one;
+                    // sub-steps of at most one cell: the first covers 1/step of
+                    // the move, partdx what remains of it after the first
+                    const T ady = fabs_t(dy), adz = fabs_t(dz);
+                    const T mx = ady > adz ? ady : adz;
+                    T partdx = zero, step = one, ps = one;
+                    if (mx > one) { step = mx; partdx = mx - one; ps = M::rcp(step); }
                     T ytmp = yp, ztmp = zp;
                     int jb = j, kb = k;
                     // first sub-step: staged for the cell-parallel sum
-                    T ps;
-                    if (partdx > one) { partdx -= one; ps = M::rcp(step); }
-                    else { ps = M::div(partdx, step); partdx = zero; }
                     T wc[4];
                     cic_substep<T>(dy, dz, ps, ytmp, ztmp, jb, kb, My, Mz, wc);
                     key = jb + My * kb;
@@ -753,7 +800,7 @@ __global__ void __launch_bounds__(32 * TY) push_cic_row_kernel(PushArgs<T> a) {
             }
             const int s = base - wbase + lane, sp = s + (s >> 5);
             K[wr][0][sp] = key;
-            K[wr][1][sp] = last;
+            if (count) K[wr][1][sp] = last;
 #pragma unroll
             for (int d = 0; d < ND; d++) S[wr][d][sp] = qv[d];
             S[wr][ND][sp] = ay;
@@ -772,16 +819,21 @@ __global__ void __launch_bounds__(32 * TY) push_cic_row_kernel(PushArgs<T> a) {
             }
             if (key < 0) continue;
             const T ry = S[wr][ND][sp], rz = S[wr][ND + 1][sp];
-            const T wc[4] = {(one - ry) * (one - rz), ry * (one - rz), (one - ry) * rz, ry * rz};
             T qv[ND];
 #pragma unroll
             for (int d = 0; d < ND; d++) qv[d] = S[wr][d][sp];
             if (key == mycell) {
+                // corner weights in pairs: (1 - rz) (1 - ry, ry) and rz (1 - ry, ry)
+                const P2 wy = FP::make(one - ry, ry);
+                const P2 w01 = FP::mul(one - rz, wy), w23 = FP::mul(rz, wy);
 #pragma unroll
-                for (int r = 0; r < 4; r++)
-#pragma unroll
-                    for (int d = 0; d < ND; d++) acc[r * ND + d] += qv[d] * wc[r];
+                for (int d = 0; d < ND; d++) {
+                    acc[d][0] = FP::fma(qv[d], w01, acc[d][0]);
+                    acc[d][1] = FP::fma(qv[d], w23, acc[d][1]);
+                }
             } else {
+                const T wc[4] = {(one - ry) * (one - rz), ry * (one - rz), (one - ry) * rz,
+                                 ry * rz};
                 int kj, kk;
                 cell_jk(key, My, a.invMy, kj, kk);
                 const int kj1 = wrap1(kj + 1, My), kk1 = wrap1(kk + 1, Mz);
@@ -803,8 +855,8 @@ __global__ void __launch_bounds__(32 * TY) push_cic_row_kernel(PushArgs<T> a) {
     T row0[ND], row1[ND], edge0[ND], edge1[ND];
 #pragma unroll
     for (int d = 0; d < ND; d++) {
-        const T c00 = acc[0 * ND + d], c10 = acc[1 * ND + d];
-        const T c01 = acc[2 * ND + d], c11 = acc[3 * ND + d];
+        const T c00 = acc[d][0].x, c10 = acc[d][0].y;
+        const T c01 = acc[d][1].x, c11 = acc[d][1].y;
         const T l10 = __shfl_up_sync(full, c10, 1), l11 = __shfl_up_sync(full, c11, 1);
         row0[d] = c00 + (lane > 0 ? l10 : zero);
         row1[d] = c01 + (lane > 0 ? l11 : zero);
