@@ -209,6 +209,15 @@ template <int M, class C>
 __host__ __device__ constexpr int vpt_c() {
     return sizeof(C) == sizeof(float2) ? vpt<M>() : 8;
 }
+// values per thread of the map kernels' row transforms: 8 on the 512-wide
+// FP32 grid, so that a transform group is one whole warp, every thread of the
+// CTA takes part in the transforms and the CTA needs fewer registers (four
+// CTAs per SM: the 512 z-mode rows run in one wave); elsewhere those of the
+// plain row transforms
+template <int M, class C = float2>
+__host__ __device__ constexpr int spec_vpt() {
+    return (sizeof(C) == sizeof(float2) && M == 256) ? 8 : vpt_c<M, C>();
+}
 template <class Real> struct CxOf;
 template <> struct CxOf<float> { using type = float2; };
 template <> struct CxOf<double> { using type = double2; };
@@ -503,13 +512,12 @@ cudaError_t launch_cols(const ColArgsT<typename Cx<C>::Real>& a, int nf, cudaStr
 // one row of n = 2M values through the half-integer transform of `kind` by
 // the T lanes of a group: in_pair(i) = (x[2i], x[2i+1]); out_pair(q, v) gets
 // the output pair q; `valid` false runs the group on zeros and stores nothing
-template <int M, class C = float2, class InPair, class OutPair>
+template <int M, class C = float2, int V = vpt_c<M, C>(), class InPair, class OutPair>
 __device__ __forceinline__ void row_dtt_group(InPair in_pair, OutPair out_pair, int kind,
                                               typename Cx<C>::Real scale, bool valid, int jt,
                                               C* Wg, const C* tws, const C* posts,
                                               const C* pre) {
     using Real = typename Cx<C>::Real;
-    constexpr int V = vpt_c<M, C>();
     constexpr int T = M / V;
     static_assert(T >= 1 && T <= 32, "a group within one warp");
     auto at = [](int e) { return e + e / V; };
@@ -573,14 +581,14 @@ static_assert(kSpecGroups >= 7, "a transform group per plane");
 template <int M, class C = float2>
 __host__ __device__ constexpr size_t spec_rows_smem() {
     // tables, FFT work of each group, the row's J spectra and E, B, Rho spectra
-    return sizeof(C) * (2 * (size_t)M + (size_t)kSpecGroups * (M + M / vpt_c<M, C>())) +
+    return sizeof(C) * (2 * (size_t)M + (size_t)kSpecGroups * (M + M / spec_vpt<M, C>())) +
            sizeof(typename Cx<C>::Real) * (3 + 7) * (size_t)(2 * M);
 }
 
 // threads of a map CTA: the transform groups, or one per mode pair if more
 template <int M, class C = float2>
 __host__ __device__ constexpr int spec_threads() {
-    return kSpecGroups * (M / vpt_c<M, C>()) > M ? kSpecGroups * (M / vpt_c<M, C>()) : M;
+    return kSpecGroups * (M / spec_vpt<M, C>()) > M ? kSpecGroups * (M / spec_vpt<M, C>()) : M;
 }
 
 // PRED_NEXT (with CORRECT): the layer's last corrector, then the next
@@ -590,19 +598,20 @@ __host__ __device__ constexpr int spec_threads() {
 // predictor reads what the same thread stored; it overwrites the corrector's
 // P bank (no longer needed) only at those modes.  C: float2 (FP32) or
 // double2 (FP64 on FFT transforms).
-template <int M, bool CORRECT, bool PRED_NEXT, class C = float2>
-__global__ void __launch_bounds__(spec_threads<M, C>())
-    spectral_rows_kernel(SpecArgs<typename Cx<C>::Real> a, SpecRowArgsT<typename Cx<C>::Real> r,
-                         SpecArgs<typename Cx<C>::Real> an) {
+template <int M, bool CORRECT, bool PRED_NEXT, class C>
+__device__ __forceinline__ void spectral_rows_body(SpecArgs<typename Cx<C>::Real> a,
+                                                   SpecRowArgsT<typename Cx<C>::Real> r,
+                                                   SpecArgs<typename Cx<C>::Real> an) {
     static_assert(CORRECT || !PRED_NEXT, "the next layer's predictor follows a corrector");
     using namespace specf32;
     using Real = typename Cx<C>::Real;
-    constexpr int T = M / vpt_c<M, C>();
+    constexpr int V = spec_vpt<M, C>();
+    constexpr int T = M / V;
     constexpr int NTF = kSpecGroups * T;   // the transform groups (whole warps)
     constexpr int NT = spec_threads<M, C>();
     static_assert(NTF % 32 == 0, "transform groups fill whole warps");
     constexpr int N = 2 * M;
-    constexpr int LD = M + M / vpt_c<M, C>();
+    constexpr int LD = M + M / V;
     extern __shared__ __align__(16) unsigned char smem_spec[];
     C* tws = reinterpret_cast<C*>(smem_spec);
     C* posts = tws + M;
@@ -615,6 +624,9 @@ __global__ void __launch_bounds__(spec_threads<M, C>())
     }
     const int k = blockIdx.x;
     const int g = threadIdx.x / T, jt = threadIdx.x % T;
+    // the first group of this thread's warp: a warp whose groups all lack a
+    // plane skips the transform (its lanes meet no shuffle of another warp)
+    const int wg0 = (threadIdx.x / 32) * (32 / T);
     C* Wg = W + g * LD;
     const C* pre = r.tab + M;
     const size_t plane = (size_t)N * a.nz;
@@ -622,12 +634,12 @@ __global__ void __launch_bounds__(spec_threads<M, C>())
     __syncthreads();
     if constexpr (CORRECT) {
         // forward y-transform of the deposit rows (Jx REDFT11, Jy RODFT11, Jz REDFT11)
-        if (threadIdx.x < NTF) {
+        if (threadIdx.x < NTF && wg0 < 3) {
             const bool valid = g < 3;
             const int gg = valid ? g : 0;
             const C* src = reinterpret_cast<const C*>(r.jin + gg * plane + (size_t)k * N);
             C* dst = reinterpret_cast<C*>(J + gg * N);
-            row_dtt_group<M, C>([src](int i) { return src[i]; },
+            row_dtt_group<M, C, V>([src](int i) { return src[i]; },
                                 [dst](int q, C v) { dst[q] = v; },
                                 gg == 1 ? QS_RODFT11 : QS_REDFT11, Real(1), valid, jt, Wg, tws,
                                 posts, pre);
@@ -675,12 +687,12 @@ __global__ void __launch_bounds__(spec_threads<M, C>())
     __syncthreads();
     if constexpr (!PRED_NEXT) pdl_trigger();
     // inverse y-transform of Ex Ey Ez Bx By Bz Rho (y kinds C S C S C S C)
-    if (threadIdx.x < NTF) {
+    if (threadIdx.x < NTF && wg0 < r.nout) {
         const bool valid = g < r.nout;
         const int gg = valid ? g : 0;
         const C* src = reinterpret_cast<const C*>(EB + gg * N);
         C* dst = reinterpret_cast<C*>(r.out + gg * plane + (size_t)k * N);
-        row_dtt_group<M, C>([src](int i) { return src[i]; },
+        row_dtt_group<M, C, V>([src](int i) { return src[i]; },
                             [dst](int q, C v) { dst[q] = v; },
                             (gg & 1) ? QS_RODFT11 : QS_REDFT11, Real(1), valid, jt, Wg, tws, posts,
                             pre);
@@ -696,12 +708,12 @@ __global__ void __launch_bounds__(spec_threads<M, C>())
         }
         __syncthreads();
         pdl_trigger();
-        if (threadIdx.x < NTF) {
+        if (threadIdx.x < NTF && wg0 < 6) {
             const bool valid = g < 6;
             const int gg = valid ? g : 0;
             const C* src = reinterpret_cast<const C*>(EB + gg * N);
             C* dst = reinterpret_cast<C*>(r.out_next + gg * plane + (size_t)k * N);
-            row_dtt_group<M, C>([src](int i) { return src[i]; },
+            row_dtt_group<M, C, V>([src](int i) { return src[i]; },
                                 [dst](int q, C v) { dst[q] = v; },
                                 (gg & 1) ? QS_RODFT11 : QS_REDFT11, Real(1), valid, jt, Wg, tws,
                                 posts, pre);
@@ -709,17 +721,46 @@ __global__ void __launch_bounds__(spec_threads<M, C>())
     }
 }
 
+template <int M, bool CORRECT, bool PRED_NEXT, class C = float2>
+__global__ void __launch_bounds__(spec_threads<M, C>())
+    spectral_rows_kernel(SpecArgs<typename Cx<C>::Real> a, SpecRowArgsT<typename Cx<C>::Real> r,
+                         SpecArgs<typename Cx<C>::Real> an) {
+    spectral_rows_body<M, CORRECT, PRED_NEXT, C>(a, r, an);
+}
+
+// The same map kernel compiled for four CTAs per SM (at most 64 registers):
+// on the 512-wide FP32 grid its 512 z-mode rows then run in one wave on the
+// 148 SMs, where three CTAs per SM leave 68 rows for a second one.
+template <int M, bool CORRECT, bool PRED_NEXT, class C = float2>
+__global__ void __launch_bounds__(spec_threads<M, C>(), 4)
+    spectral_rows_wave_kernel(SpecArgs<typename Cx<C>::Real> a,
+                              SpecRowArgsT<typename Cx<C>::Real> r,
+                              SpecArgs<typename Cx<C>::Real> an) {
+    spectral_rows_body<M, CORRECT, PRED_NEXT, C>(a, r, an);
+}
+
+template <int M, class C>
+constexpr bool spec_one_wave() {
+    return sizeof(C) == sizeof(float2) && M == 256;
+}
+
+template <int M, bool CORRECT, bool PRED_NEXT, class C>
+constexpr auto spec_rows_fn() {
+    if constexpr (spec_one_wave<M, C>()) return spectral_rows_wave_kernel<M, CORRECT, PRED_NEXT, C>;
+    else return spectral_rows_kernel<M, CORRECT, PRED_NEXT, C>;
+}
+
 template <int M, class C = float2>
 cudaError_t set_spec_rows_smem() {
-    cudaError_t e = cudaFuncSetAttribute(spectral_rows_kernel<M, true, false, C>,
+    cudaError_t e = cudaFuncSetAttribute(spec_rows_fn<M, true, false, C>(),
                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)spec_rows_smem<M, C>());
     if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(spectral_rows_kernel<M, false, false, C>,
+        e = cudaFuncSetAttribute(spec_rows_fn<M, false, false, C>(),
                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)spec_rows_smem<M, C>());
     if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(spectral_rows_kernel<M, true, true, C>,
+        e = cudaFuncSetAttribute(spec_rows_fn<M, true, true, C>(),
                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)spec_rows_smem<M, C>());
     return e;
@@ -732,10 +773,10 @@ cudaError_t launch_spec_rows(const SpecArgs<typename Cx<C>::Real>& a,
     const dim3 grid((unsigned)a.nz), block(spec_threads<M, C>());
     const size_t sm = spec_rows_smem<M, C>();
     if (next)
-        return launch_pdl(spectral_rows_kernel<M, true, true, C>, grid, block, sm, st, a, r, *next);
+        return launch_pdl(spec_rows_fn<M, true, true, C>(), grid, block, sm, st, a, r, *next);
     if (correct)
-        return launch_pdl(spectral_rows_kernel<M, true, false, C>, grid, block, sm, st, a, r, a);
-    return launch_pdl(spectral_rows_kernel<M, false, false, C>, grid, block, sm, st, a, r, a);
+        return launch_pdl(spec_rows_fn<M, true, false, C>(), grid, block, sm, st, a, r, a);
+    return launch_pdl(spec_rows_fn<M, false, false, C>(), grid, block, sm, st, a, r, a);
 }
 
 // The adjoints of the maps in the same arrangement (the transforms are their
@@ -784,12 +825,13 @@ __global__ void __launch_bounds__(adj_threads<M>()) adjoint_rows_kernel(AdjSpecA
     }
     const int k = blockIdx.x;
     const int g = threadIdx.x / T, jt = threadIdx.x % T;
+    const int wg0 = (threadIdx.x / 32) * (32 / T);   // a warp without planes skips a transform
     float2* Wg = W + g * LD;
     const float2* pre = r.tab + M;
     const size_t plane = (size_t)N * a.nz;
     pdl_wait();
     __syncthreads();
-    if (threadIdx.x < NTF) {   // y-pass of the field adjoints (y kinds C S C S C S)
+    if (threadIdx.x < NTF && wg0 < 6) {   // y-pass of the field adjoints (y kinds C S C S C S)
         const bool valid = g < 6;
         const int gg = valid ? g : 0;
         const float2* src = reinterpret_cast<const float2*>(r.in + gg * plane + (size_t)k * N);
@@ -816,7 +858,7 @@ __global__ void __launch_bounds__(adj_threads<M>()) adjoint_rows_kernel(AdjSpecA
     pdl_trigger();
     if constexpr (CORRECT) {
         __syncthreads();
-        if (threadIdx.x < NTF) {   // y-pass of the current adjoints (y kinds C S C)
+        if (threadIdx.x < NTF && wg0 < 3) {   // y-pass of the current adjoints (y kinds C S C)
             const bool valid = g < 3;
             const int gg = valid ? g : 0;
             const float2* src = reinterpret_cast<const float2*>(OUT + gg * N);
