@@ -251,6 +251,11 @@ struct Engine : EngineBase {
     // the layer whose predictor the previous layer's last corrector kernel
     // has already run (its E, B after the y-pass in scratch2), or -1
     int pred_next = -1;
+    // next_avg: the fused predictor wrote the average of the layer's E, B and
+    // the predicted ones; half_avg: the C layer holds that average after the
+    // next Guess, so its first push gathers from C alone and does not wait for
+    // the layer's last z-pass (side stream 0)
+    bool next_avg = false, half_avg = false;
     int fuse_lo = 0;            // lowest layer of the march (or recomputed segment)
     // adjoint sweep: the predictor adjoint of a layer runs on side stream 0
     // beside the next layer's first field z-pass (which then uses scratch2)
@@ -410,9 +415,14 @@ struct Engine : EngineBase {
     qs_status init() override {
         plane = (size_t)My * Mz;
         CK(cudaSetDevice(dev));
-        CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+        // the march's chain runs at the highest stream priority and its side
+        // work (the last z-pass of a layer, the plasma regrouping) at the
+        // lowest, so that the CTA scheduler gives free SM slots to the chain
+        int prio_lo = 0, prio_hi = 0;
+        CK(cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi));
+        CK(cudaStreamCreateWithPriority(&st, cudaStreamNonBlocking, prio_hi));
         for (int k = 0; k < 2; k++) {
-            CK(cudaStreamCreateWithFlags(&st_side[k], cudaStreamNonBlocking));
+            CK(cudaStreamCreateWithPriority(&st_side[k], cudaStreamNonBlocking, prio_lo));
             CK(cudaEventCreateWithFlags(&ev_fork[k], cudaEventDisableTiming));
             CK(cudaEventCreateWithFlags(&ev_join[k], cudaEventDisableTiming));
         }
@@ -1351,11 +1361,14 @@ struct Engine : EngineBase {
         if (fft_maps() && pred_next == iLayer && iSplit == 0 && p_valid && sb3_valid) {
             // the previous layer's last corrector kernel ran this predictor
             pred_next = -1;
+            half_avg = next_avg;
+            next_avg = false;
             eb_zpass(6, scratch2);
             CK(cudaGetLastError());
             return QS_OK;
         }
         pred_next = -1;
+        next_avg = half_avg = false;
         if (fft_maps()) {
             // predictor and the inverse y-pass of E, B in one kernel, then the z-pass
             SpecArgs<T> a = spec_args(iLayer, iSplit);
@@ -1391,11 +1404,14 @@ struct Engine : EngineBase {
     // the adjoint's maps between the halves of its transforms (FP32)
     bool adj_fused() const { return fftx && fftx->spec_rows; }
     int spec_rows_run(const SpecArgs<T>& a, bool correct, const T* jin, T* out, int nout,
-                      const SpecArgs<T>* next = nullptr, T* out_next = nullptr) {
+                      const SpecArgs<T>* next = nullptr, T* out_next = nullptr,
+                      bool avg_next = false) {
         if constexpr (sizeof(T) == 4)
-            return fftx->run_spectral_rows(a, correct, jin, out, nout, st, next, out_next);
+            return fftx->run_spectral_rows(a, correct, jin, out, nout, st, next, out_next,
+                                           avg_next);
         else
-            return fftx64->run_spectral_rows(a, correct, jin, out, nout, st, next, out_next);
+            return fftx64->run_spectral_rows(a, correct, jin, out, nout, st, next, out_next,
+                                             avg_next);
     }
     int cols_run(int nf, const T* const* in, T* const* out, const int* kind, T scale) {
         if constexpr (sizeof(T) == 4) return fftx->run_cols(nf, in, out, kind, scale, st);
@@ -1419,7 +1435,12 @@ struct Engine : EngineBase {
 
     qs_status push(int iLayer, int iSplit, int full) override {
         (void)iLayer; (void)iSplit;
-        join_sides();   // the fields and the plasma this push reads
+        // the fields and the plasma this push reads: with the averaged fields
+        // in C the previous layer's last z-pass (side 0) is not among them
+        const bool from_avg = !full && half_avg;
+        half_avg = false;
+        if (from_avg) join_side(1);
+        else join_sides();
         if (fp32_study & (4 | 128)) return study_push(full);
         // ClearCurrentsSplit: inside the march the preceding spectral kernel
         // already cleared Csrc
@@ -1433,7 +1454,9 @@ struct Engine : EngineBase {
         a.My = My; a.Mz = Mz;
         a.cell = pcell;
         a.y = py; a.z = pz; a.px = ppx; a.py = ppy; a.pz = ppz; a.w = pw;
-        a.P = Pf; a.C = Cf; a.dep = Csrc;
+        a.P = from_avg ? Cf : Pf;   // (C + C) / 2 = C exactly
+        a.C = Cf;
+        a.dep = Csrc;
         a.cell_out = pcell;
         a.dep_cell = nullptr;
         a.plane = plane;
@@ -1497,6 +1520,13 @@ struct Engine : EngineBase {
         side_pending[k] = true;
         return cudaEventRecord(ev_join[k], st_side[k]);
     }
+    // make st wait for side stream k's pending work
+    void join_side(int k) {
+        if (side_pending[k]) {
+            cudaStreamWaitEvent(st, ev_join[k], 0);
+            side_pending[k] = false;
+        }
+    }
     // make st wait for the side streams' pending work
     void join_sides() {
         for (int k = 0; k < 2; k++)
@@ -1524,6 +1554,7 @@ struct Engine : EngineBase {
             // :1343-1345 along z, then the y-pass of J, the corrector and the
             // inverse y-pass of E, B (, Rho) in one kernel, then their z-pass
             {
+                join_side(0);   // a pending last z-pass of the previous layer reads scratch
                 const T* ins[3] = {Csrc, Csrc + plane, Csrc + 2 * plane};
                 T* outs[3] = {scratch, scratch + plane, scratch + 2 * plane};
                 const int kz[3] = {CC, CC, SS};
@@ -1544,11 +1575,17 @@ struct Engine : EngineBase {
                     an.zero_src = clear_by_maps() ? Psrc : nullptr;   // the next push's deposit
                     an.write_b = 0;
                 }
+                // the next layer's first push gathers the average of this
+                // layer's fields and the predicted ones: with the grouped CIC
+                // push (whose gathered fields the adjoint reads) the map
+                // kernel forms it, so that push needs one z-pass, not two
+                const bool avg = fuse && cic_sort && clear_by_maps();
                 klaunch(KC_SPECTRAL, [&] {
                     return spec_rows_run(a, true, scratch, scratch, nout, fuse ? &an : nullptr,
-                                         fuse ? scratch2 : nullptr);
+                                         fuse ? scratch2 : nullptr, avg);
                 });
                 pred_next = fuse ? iLayer - 1 : -1;
+                next_avg = avg;
                 if (side_z && iter < 0 && nout == 6) {
                     // the layer's last z-pass: only the next layer's pushes read it
                     const cudaError_t e = on_side(0, [&] { eb_zpass(nout, scratch); });
@@ -1792,11 +1829,13 @@ struct Engine : EngineBase {
         side_z = side && (fft_maps() || fftx64) && S == 1 && !src3;
         side_sort = side && cic_sort;
         pred_next = -1;
+        next_avg = half_avg = false;
         fuse_lo = 0;
         qs_status s = march_device_body();
         join_sides();
         side_z = side_sort = false;
         pred_next = -1;
+        next_avg = half_avg = false;
         g_pdl = false;
         in_march = false;
         return s;
@@ -2076,7 +2115,7 @@ struct Engine : EngineBase {
                 return s;
             }
             if (e != cudaSuccess) return cuda_fail(e, "march capture");
-            e = cudaGraphInstantiate(&gexec, g, 0);
+            e = cudaGraphInstantiate(&gexec, g, cudaGraphInstantiateFlagUseNodePriority);
             cudaGraphDestroy(g);
             if (e != cudaSuccess) {
                 gexec = nullptr;
@@ -2237,6 +2276,7 @@ struct Engine : EngineBase {
         // fused next predictor (the plasma is not regrouped here)
         side_z = !prof && !fp32_study && (fft_maps() || fftx64) && S == 1 && !src3;
         pred_next = -1;
+        next_avg = half_avg = false;
         fuse_lo = lo;
         qs_status s = restore_checkpoint(m);
         for (int i = c; !s && i >= lo; i--) {
@@ -2278,6 +2318,7 @@ struct Engine : EngineBase {
         join_sides();
         side_z = false;
         pred_next = -1;
+        next_avg = half_avg = false;
         fuse_lo = 0;
         push_favg = nullptr;
         in_march = false;
@@ -2622,7 +2663,7 @@ struct Engine : EngineBase {
                     return s;
                 }
                 if (e != cudaSuccess) return cuda_fail(e, "adjoint capture");
-                e = cudaGraphInstantiate(&adj_exec, g, 0);
+                e = cudaGraphInstantiate(&adj_exec, g, cudaGraphInstantiateFlagUseNodePriority);
                 cudaGraphDestroy(g);
                 if (e != cudaSuccess) {
                     adj_exec = nullptr;

@@ -570,6 +570,7 @@ struct SpecRowArgsT {
     int nout;             // 6, or 7 with Rho
     const typename CxOf<Real>::type* tab;   // tables of the y size
     Real* out_next;       // with the next layer's predictor: its Ex..Bz after the y-pass
+    int avg_next;         // out_next gets (this layer's E, B + the predicted ones) / 2
 };
 using SpecRowArgs = SpecRowArgsT<float>;
 
@@ -704,7 +705,21 @@ __device__ __forceinline__ void spectral_rows_body(SpecArgs<typename Cx<C>::Real
             const size_t n = (size_t)j + (size_t)N * k;
             const Modes2<Real> o = predictor_modes2(an, j, k, n);
             store_modes2(an, n, o);
-            to_eb(j, o);
+            if (r.avg_next) {
+                // the fields the next layer's first push gathers: this
+                // layer's (still in EB) and the predicted ones, averaged
+                const Real h = Real(0.5);
+                C* eb = reinterpret_cast<C*>(EB + j);
+                const Real v[6][2] = {{o.ex[0], o.ex[1]}, {o.ey[0], o.ey[1]}, {o.ez[0], o.ez[1]},
+                                      {o.bx[0], o.bx[1]}, {o.by[0], o.by[1]}, {o.bz[0], o.bz[1]}};
+#pragma unroll
+                for (int f = 0; f < 6; f++) {
+                    const C e = eb[f * (N / 2)];
+                    eb[f * (N / 2)] = Cx<C>::make(h * (e.x + v[f][0]), h * (e.y + v[f][1]));
+                }
+            } else {
+                to_eb(j, o);
+            }
         }
         __syncthreads();
         pdl_trigger();
@@ -999,7 +1014,8 @@ int DttFft::run_cols(int nf, const float* const* in, float* const* out, const in
 
 int DttFft::run_spectral_rows(const SpecArgs<float>& a, bool correct, const float* jin,
                               float* out, int nout, cudaStream_t st,
-                              const SpecArgs<float>* next, float* out_next) const {
+                              const SpecArgs<float>* next, float* out_next,
+                              bool avg_next) const {
     if (!spec_rows) return 0;
     if (next && (!correct || !out_next || nout != 6)) return 0;
     fft::SpecRowArgs r{};
@@ -1008,6 +1024,7 @@ int DttFft::run_spectral_rows(const SpecArgs<float>& a, bool correct, const floa
     r.nout = nout;
     r.tab = tab_y;
     r.out_next = out_next;
+    r.avg_next = (next && avg_next) ? 1 : 0;
     cudaError_t e;
     switch (ny / 2) {
         case 512: e = fft::launch_spec_rows<512>(a, r, correct, next, st); break;
@@ -1166,7 +1183,8 @@ int DttFft64::run_cols(int nf, const double* const* in, double* const* out, cons
 
 int DttFft64::run_spectral_rows(const SpecArgs<double>& a, bool correct, const double* jin,
                                 double* out, int nout, cudaStream_t st,
-                                const SpecArgs<double>* next, double* out_next) const {
+                                const SpecArgs<double>* next, double* out_next,
+                                bool avg_next) const {
     if (!spec_rows) return 0;
     if (next && (!correct || !out_next || nout != 6)) return 0;
     fft::SpecRowArgsT<double> r{};
@@ -1175,6 +1193,7 @@ int DttFft64::run_spectral_rows(const SpecArgs<double>& a, bool correct, const d
     r.nout = nout;
     r.tab = tab_y;
     r.out_next = out_next;
+    r.avg_next = (next && avg_next) ? 1 : 0;
     cudaError_t e;
     switch (ny / 2) {
         case 256: e = fft::launch_spec_rows<256, double2>(a, r, correct, next, st); break;

@@ -32,13 +32,23 @@ inline cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, s
     cfg.blockDim = block;
     cfg.dynamicSmemBytes = smem;
     cfg.stream = st;
-    cudaLaunchAttribute attr[1];
+    cudaLaunchAttribute attr[2];
+    unsigned n = 0;
     if (g_pdl) {
-        attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-        attr[0].val.programmaticStreamSerializationAllowed = 1;
-        cfg.attrs = attr;
-        cfg.numAttrs = 1;
+        attr[n].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        attr[n].val.programmaticStreamSerializationAllowed = 1;
+        n++;
     }
+    // the stream's priority, also as a node attribute when the launch is
+    // captured into a graph
+    int prio = 0;
+    if (cudaStreamGetPriority(st, &prio) == cudaSuccess && prio != 0) {
+        attr[n].id = cudaLaunchAttributePriority;
+        attr[n].val.priority = prio;
+        n++;
+    }
+    cfg.attrs = n ? attr : nullptr;
+    cfg.numAttrs = n;
     return cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...);
 }
 

@@ -135,10 +135,11 @@ struct DttFft {
     // inverse y-pass of Ex Ey Ez Bx By Bz (, Rho when nout = 7) into `out`
     // (planes of ny*nz, unscaled); jin and out may be the same planes
     // with `next` (the layer's last corrector, nout = 6): the next layer's
-    // predictor too, its E, B after the y-pass into out_next
+    // predictor too, its E, B after the y-pass into out_next, or with
+    // avg_next the average of this layer's E, B and the predicted ones
     int run_spectral_rows(const SpecArgs<float>& a, bool correct, const float* jin, float* out,
                           int nout, cudaStream_t st, const SpecArgs<float>* next = nullptr,
-                          float* out_next = nullptr) const;
+                          float* out_next = nullptr, bool avg_next = false) const;
     // the same for the adjoints of the maps: y-pass of the 6 z-transformed
     // field adjoints at `in`, the corrector's (predictor's) adjoint, and for
     // the corrector the y-pass of the 3 current adjoints into `out`
@@ -162,7 +163,7 @@ struct DttFft64 {
                  double scale, cudaStream_t st) const;
     int run_spectral_rows(const SpecArgs<double>& a, bool correct, const double* jin, double* out,
                           int nout, cudaStream_t st, const SpecArgs<double>* next = nullptr,
-                          double* out_next = nullptr) const;
+                          double* out_next = nullptr, bool avg_next = false) const;
     ~DttFft64();
 };
 
