@@ -156,6 +156,19 @@ class QsError(RuntimeError):
         self.status = status
 
 
+TRACE_LIB_PATH = os.path.join(_PKG, "libqsb200_trace.so")
+
+
+def use_trace_library():
+    """Make this process load libqsb200_trace.so (the same library with the
+    march kernels' device timeline, include/qsb200_trace.h) instead of
+    libqsb200.so; must come before the first load_library()."""
+    global LIB_PATH
+    if _lib is not None and LIB_PATH != TRACE_LIB_PATH:
+        raise RuntimeError("libqsb200.so is already loaded in this process")
+    LIB_PATH = TRACE_LIB_PATH
+
+
 def load_library():
     """Load the in-tree libqsb200.so (raises if it was not built)."""
     global _lib

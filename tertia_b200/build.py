@@ -1,5 +1,8 @@
 """Build libqsb200.so in-tree: every CUDA source compiled for sm_100a with
-nvcc, then linked into one shared library with a static CUDA runtime."""
+nvcc, then linked into one shared library with a static CUDA runtime.  Beside
+it, libqsb200_trace.so: the same library with the march kernels' device
+timeline compiled in (csrc/trace.cuh; the units that hold those kernels are
+compiled again with -DQS_TRACE, and trace.cu adds qs_trace_attach)."""
 from __future__ import annotations
 
 import concurrent.futures as cf
@@ -12,6 +15,7 @@ PKG = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(PKG, "csrc")
 BUILD = os.path.join(PKG, "_build")
 OUT = os.path.join(PKG, "libqsb200.so")
+OUT_TRACE = os.path.join(PKG, "libqsb200_trace.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 BASE = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-Wall",
         "-Xptxas", "-warn-spills"]
@@ -21,6 +25,9 @@ NO_FMAD = {"push_f64.cu", "spectral.cu", "beam.cu"}
 SOURCES = ["api.cu", "dtt_simt.cu", "dtt_tc.cu", "push_f64.cu", "push_f64fma.cu", "push_f32.cu", "spectral.cu",
            "spectral_f32.cu", "beam.cu", "noalloc.cu", "adjoint.cu", "sort.cu", "dtt_fft.cu",
            "pack.cu"]
+# the units holding instrumented kernels, and the unit only the traced library has
+TRACED = ["push_f32.cu", "push_f64fma.cu", "dtt_fft.cu", "sort.cu"]
+TRACE_ONLY = ["trace.cu"]
 
 
 def nvcc() -> str:
@@ -30,15 +37,16 @@ def nvcc() -> str:
     raise RuntimeError("nvcc not found")
 
 
-def _compile(src: str, verbose: bool) -> str:
-    obj = os.path.join(BUILD, src.replace(".cu", ".o"))
+def _compile(src: str, verbose: bool, traced: bool = False) -> str:
+    out_dir = os.path.join(BUILD, "trace") if traced else BUILD
+    obj = os.path.join(out_dir, src.replace(".cu", ".o"))
     path = os.path.join(CSRC, src)
     deps = [path] + [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".h", ".cuh"))]
-    deps.append(os.path.join(PKG, "..", "include", "qsb200.h"))
+    deps += [os.path.join(PKG, "..", "include", h) for h in ("qsb200.h", "qsb200_trace.h")]
     if os.path.exists(obj) and all(os.path.getmtime(obj) >= os.path.getmtime(d) for d in deps):
         return obj
     cmd = [nvcc()] + ARCH + BASE + (["-fmad=false"] if src in NO_FMAD else []) + \
-          ["-c", path, "-o", obj]
+          (["-DQS_TRACE"] if traced else []) + ["-c", path, "-o", obj]
     if verbose:
         cmd += ["-Xptxas", "-v"]
     r = subprocess.run(cmd, capture_output=True, text=True)
@@ -49,16 +57,26 @@ def _compile(src: str, verbose: bool) -> str:
     return obj
 
 
-def build(verbose: bool = False) -> str:
-    os.makedirs(BUILD, exist_ok=True)
-    with cf.ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 1)) as ex:
-        objs = list(ex.map(lambda s: _compile(s, verbose), SOURCES))
-    if os.path.exists(OUT) and all(os.path.getmtime(OUT) >= os.path.getmtime(o) for o in objs):
-        return OUT
-    cmd = [nvcc()] + ARCH + ["-shared", "-cudart", "static", "-o", OUT] + objs
+def _link(out: str, objs: list[str]) -> None:
+    if os.path.exists(out) and all(os.path.getmtime(out) >= os.path.getmtime(o) for o in objs):
+        return
+    cmd = [nvcc()] + ARCH + ["-shared", "-cudart", "static", "-o", out] + objs
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
+
+
+def build(verbose: bool = False) -> str:
+    """Build libqsb200.so and libqsb200_trace.so; returns the former's path."""
+    os.makedirs(os.path.join(BUILD, "trace"), exist_ok=True)
+    jobs = [(s, False) for s in SOURCES] + [(s, True) for s in TRACED + TRACE_ONLY]
+    with cf.ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 1)) as ex:
+        objs = list(ex.map(lambda j: _compile(j[0], verbose, j[1]), jobs))
+    plain = objs[:len(SOURCES)]
+    traced = dict(zip(TRACED + TRACE_ONLY, objs[len(SOURCES):]))
+    _link(OUT, plain)
+    _link(OUT_TRACE, [traced.get(s, o) for s, o in zip(SOURCES, plain)] +
+          [traced[s] for s in TRACE_ONLY])
     return OUT
 
 

@@ -30,6 +30,7 @@
 #include "spectral_f32.cuh"
 #include "adjoint_maps.cuh"
 #include "charge.cuh"
+#include "trace.cuh"
 
 namespace qs {
 namespace fft {
@@ -270,7 +271,9 @@ __global__ void __launch_bounds__(row_threads<M, C>())
     const int f = valid ? row / a.nrows : 0, k = valid ? row % a.nrows : 0;
     C* Ws = W + s * LD;
     auto at = [](int e) { return e + e / V; };
+    QS_TRACE_ENTRY();
     pdl_wait();
+    QS_TRACE_WAITED();
     const Real* inf = a.in[0];
     Real* outf = a.out[0];
     int kind = a.kind[0];
@@ -344,6 +347,7 @@ __global__ void __launch_bounds__(row_threads<M, C>())
 #pragma unroll
         for (int m = 0; m < V; m++) mirror[m] = ims[M - 1 - (jt + T * m)];
     }
+    QS_TRACE_END(trace::K_YPASS);
     if (!valid) return;
     C* O = reinterpret_cast<C*>(outf + (size_t)k * 2 * M);
     const Real c2 = Real(2) * a.scale;
@@ -388,7 +392,9 @@ __global__ void __launch_bounds__(TJ * (M / vpt_c<M, C>()))
     const int col = blockIdx.x * TJ + c;
     const size_t ld = (size_t)a.ncols;
     auto at = [c](int e) { return e * TJ + c; };
+    QS_TRACE_ENTRY();
     pdl_wait();
+    QS_TRACE_WAITED();
     const Real* inf = a.in[0];
     Real* outf = a.out[0];
     Real* accf = a.acc[0];
@@ -464,6 +470,7 @@ __global__ void __launch_bounds__(TJ * (M / vpt_c<M, C>()))
         outf[(size_t)(2 * q) * ld + col] = c2 * fin[m].x;
         outf[(size_t)(2 * q + 1) * ld + col] = sgn * ims[(M - 1 - q) * TJ + c];
     }
+    QS_TRACE_END(trace::K_ZPASS);
 }
 
 template <int M, class C = float2>
@@ -631,7 +638,9 @@ __device__ __forceinline__ void spectral_rows_body(SpecArgs<typename Cx<C>::Real
     C* Wg = W + g * LD;
     const C* pre = r.tab + M;
     const size_t plane = (size_t)N * a.nz;
+    QS_TRACE_ENTRY();
     pdl_wait();
+    QS_TRACE_WAITED();
     __syncthreads();
     if constexpr (CORRECT) {
         // forward y-transform of the deposit rows (Jx REDFT11, Jy RODFT11, Jz REDFT11)
@@ -734,6 +743,8 @@ __device__ __forceinline__ void spectral_rows_body(SpecArgs<typename Cx<C>::Real
                                 posts, pre);
         }
     }
+    QS_TRACE_END(PRED_NEXT ? trace::K_MAP_CORR_PRED
+                           : (CORRECT ? trace::K_MAP_CORR : trace::K_MAP_PRED));
 }
 
 template <int M, bool CORRECT, bool PRED_NEXT, class C = float2>
@@ -1250,3 +1261,5 @@ int DttFft64::run_pass(int pass, const DttJob<double>& job, double* scratch,
 }
 
 }  // namespace qs
+
+QS_TRACE_UNIT(fft)

@@ -24,6 +24,7 @@
 #include "qs_internal.h"
 #include "pdl.cuh"
 #include "pushmath.cuh"
+#include "trace.cuh"
 
 namespace qs {
 
@@ -637,7 +638,9 @@ __global__ void __launch_bounds__(32 * TY) push_cic_row_kernel(PushArgs<T> a) {
     const int tiles_x = My / TX;
     const int j0 = (blockIdx.x % tiles_x) * TX, k0 = (blockIdx.x / tiles_x) * TY;
     for (int i = threadIdx.x; i < ND * H * W; i += 32 * TY) (&Tt[0][0][0])[i] = zero;
+    QS_TRACE_ENTRY();
     pdl_wait();
+    QS_TRACE_WAITED();
     for (int i = threadIdx.x; i < H * W; i += 32 * TY) {
         const int r = i / W, cc = i - r * W;
         const size_t m = (size_t)wrap1(j0 + cc, My) + (size_t)My * wrap1(k0 + r, Mz);
@@ -884,6 +887,7 @@ __global__ void __launch_bounds__(32 * TY) push_cic_row_kernel(PushArgs<T> a) {
             if (x != zero) atomicAdd(a.dep + d * plane + m, x);
         }
     }
+    QS_TRACE_END(a.full ? trace::K_PUSH_FULL : trace::K_PUSH_HALF);
 }
 
 // the grouped CIC push (both widths): 0 when the layout does not fit it

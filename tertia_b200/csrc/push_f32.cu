@@ -5,3 +5,5 @@
 namespace qs {
 template int launch_push<float>(const PushArgs<float>&, int, bool, cudaStream_t);
 }  // namespace qs
+
+QS_TRACE_UNIT(push)

@@ -9,3 +9,5 @@ int launch_push_rows_f64(const PushArgs<double>& a, cudaStream_t st) {
     return launch_push_rows<double>(a, st);
 }
 }  // namespace qs
+
+QS_TRACE_UNIT(push64)

@@ -15,6 +15,7 @@
 #include "qs_common.cuh"
 #include "qs_internal.h"
 #include "pdl.cuh"
+#include "trace.cuh"
 
 namespace qs {
 
@@ -70,7 +71,9 @@ __global__ void __launch_bounds__(kScanBlock) scan_cells_kernel(int* __restrict_
                                                                 int clear) {
     __shared__ int wsum[kScanBlock / 32];
     __shared__ bool last;
+    QS_TRACE_ENTRY();
     pdl_wait();
+    QS_TRACE_WAITED();
     const int c = blockIdx.x * kScanBlock + threadIdx.x;
     const int v = c < ncell ? cnt[c] : 0;
     if (clear && c < ncell) cnt[c] = 0;
@@ -83,6 +86,7 @@ __global__ void __launch_bounds__(kScanBlock) scan_cells_kernel(int* __restrict_
         last = atomicAdd(ticket, 1u) == gridDim.x - 1;
     }
     __syncthreads();
+    QS_TRACE_END(trace::K_SCAN);
     if (!last) return;
     __threadfence();
     const int nb = gridDim.x;
@@ -105,7 +109,9 @@ __global__ void __launch_bounds__(256) scatter_kernel(PlasmaSet<T> in, PlasmaSet
                                                       const int* __restrict__ loff,
                                                       const int* __restrict__ bpref,
                                                       int* __restrict__ err) {
+    QS_TRACE_ENTRY();
     pdl_wait();
+    QS_TRACE_WAITED();
     const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= n) return;
     const int c = in.cell[p];
@@ -125,6 +131,7 @@ __global__ void __launch_bounds__(256) scatter_kernel(PlasmaSet<T> in, PlasmaSet
     out.cell[q] = c;
     out.y[q] = y; out.z[q] = z; out.px[q] = px; out.py[q] = py; out.pz[q] = pz; out.w[q] = w;
     out.id[q] = id;
+    QS_TRACE_END(trace::K_SCATTER);
 }
 
 __global__ void iota_kernel(int32_t* __restrict__ id, int64_t n) {
@@ -173,3 +180,5 @@ template int launch_scatter<double>(const PlasmaSet<double>&, const PlasmaSet<do
                                     int, int*, const int*, const int*, int*, cudaStream_t);
 
 }  // namespace qs
+
+QS_TRACE_UNIT(sort)
