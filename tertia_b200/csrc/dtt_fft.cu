@@ -816,28 +816,38 @@ struct AdjRowArgs {
     const float2* tab;
 };
 
+// values per thread of the adjoint map kernel's row transforms: as in the
+// forward map kernel, 8 on the 512-wide grid (a group is one warp and every
+// thread of the CTA transforms), else those of the plain row transforms
+template <int M>
+__host__ __device__ constexpr int adj_vpt() {
+    return M == 256 ? 8 : vpt<M>();
+}
+
 template <int M>
 __host__ __device__ constexpr size_t adj_rows_smem() {
-    return sizeof(float2) * (2 * (size_t)M + (size_t)kSpecGroups * (M + M / vpt<M>())) +
+    return sizeof(float2) * (2 * (size_t)M + (size_t)kSpecGroups * (M + M / adj_vpt<M>())) +
            sizeof(float) * (6 + 3) * (size_t)(2 * M);
 }
 
 template <int M>
 __host__ __device__ constexpr int adj_threads() {
-    // one mode per thread, at most 512 threads (the rest loop)
-    return kSpecGroups * (M / vpt<M>()) > 2 * M ? kSpecGroups * (M / vpt<M>())
-                                                : (2 * M > 512 ? 512 : 2 * M);
+    // the transform groups on the 512-wide grid (two modes per thread, four
+    // CTAs per SM); elsewhere one mode per thread, at most 512 (the rest loop)
+    return M == 256 ? kSpecGroups * (M / adj_vpt<M>())
+           : kSpecGroups * (M / vpt<M>()) > 2 * M ? kSpecGroups * (M / vpt<M>())
+                                                  : (2 * M > 512 ? 512 : 2 * M);
 }
 
 template <int M, bool CORRECT>
-__global__ void __launch_bounds__(adj_threads<M>()) adjoint_rows_kernel(AdjSpecArgs<float> a,
-                                                                       AdjRowArgs r) {
+__device__ __forceinline__ void adjoint_rows_body(AdjSpecArgs<float> a, AdjRowArgs r) {
     using namespace adjmaps;
-    constexpr int T = M / vpt<M>();
+    constexpr int V = adj_vpt<M>();
+    constexpr int T = M / V;
     constexpr int NTF = kSpecGroups * T;
     constexpr int NT = adj_threads<M>();
     constexpr int N = 2 * M;
-    constexpr int LD = M + M / vpt<M>();
+    constexpr int LD = M + M / V;
     static_assert(NTF % 32 == 0, "transform groups fill whole warps");
     extern __shared__ float2 smem_f2[];
     float2* tws = smem_f2;
@@ -862,7 +872,7 @@ __global__ void __launch_bounds__(adj_threads<M>()) adjoint_rows_kernel(AdjSpecA
         const int gg = valid ? g : 0;
         const float2* src = reinterpret_cast<const float2*>(r.in + gg * plane + (size_t)k * N);
         float2* dst = reinterpret_cast<float2*>(IN + gg * N);
-        row_dtt_group<M>([src](int i) { return src[i]; },
+        row_dtt_group<M, float2, V>([src](int i) { return src[i]; },
                          [dst](int q, float2 v) { dst[q] = v; },
                          (gg & 1) ? QS_RODFT11 : QS_REDFT11, 1.f, valid, jt, Wg, tws, posts, pre);
     }
@@ -889,7 +899,7 @@ __global__ void __launch_bounds__(adj_threads<M>()) adjoint_rows_kernel(AdjSpecA
             const int gg = valid ? g : 0;
             const float2* src = reinterpret_cast<const float2*>(OUT + gg * N);
             float2* dst = reinterpret_cast<float2*>(r.out + gg * plane + (size_t)k * N);
-            row_dtt_group<M>([src](int i) { return src[i]; },
+            row_dtt_group<M, float2, V>([src](int i) { return src[i]; },
                              [dst](int q, float2 v) { dst[q] = v; },
                              gg == 1 ? QS_RODFT11 : QS_REDFT11, 1.f, valid, jt, Wg, tws, posts,
                              pre);
@@ -897,13 +907,33 @@ __global__ void __launch_bounds__(adj_threads<M>()) adjoint_rows_kernel(AdjSpecA
     }
 }
 
+template <int M, bool CORRECT>
+__global__ void __launch_bounds__(adj_threads<M>()) adjoint_rows_kernel(AdjSpecArgs<float> a,
+                                                                       AdjRowArgs r) {
+    adjoint_rows_body<M, CORRECT>(a, r);
+}
+
+// The same compiled for four CTAs per SM (at most 64 registers): the 512
+// z-mode rows of the 512-wide grid in one wave on the 148 SMs.
+template <int M, bool CORRECT>
+__global__ void __launch_bounds__(adj_threads<M>(), 4)
+    adjoint_rows_wave_kernel(AdjSpecArgs<float> a, AdjRowArgs r) {
+    adjoint_rows_body<M, CORRECT>(a, r);
+}
+
+template <int M, bool CORRECT>
+constexpr auto adj_rows_fn() {
+    if constexpr (M == 256) return adjoint_rows_wave_kernel<M, CORRECT>;
+    else return adjoint_rows_kernel<M, CORRECT>;
+}
+
 template <int M>
 cudaError_t set_adj_rows_smem() {
-    cudaError_t e = cudaFuncSetAttribute(adjoint_rows_kernel<M, true>,
+    cudaError_t e = cudaFuncSetAttribute(adj_rows_fn<M, true>(),
                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)adj_rows_smem<M>());
     if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(adjoint_rows_kernel<M, false>,
+        e = cudaFuncSetAttribute(adj_rows_fn<M, false>(),
                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)adj_rows_smem<M>());
     return e;
@@ -914,8 +944,8 @@ cudaError_t launch_adj_rows(const AdjSpecArgs<float>& a, const AdjRowArgs& r, bo
                             cudaStream_t st) {
     const dim3 grid((unsigned)a.nz), block(adj_threads<M>());
     if (correct)
-        return launch_pdl(adjoint_rows_kernel<M, true>, grid, block, adj_rows_smem<M>(), st, a, r);
-    return launch_pdl(adjoint_rows_kernel<M, false>, grid, block, adj_rows_smem<M>(), st, a, r);
+        return launch_pdl(adj_rows_fn<M, true>(), grid, block, adj_rows_smem<M>(), st, a, r);
+    return launch_pdl(adj_rows_fn<M, false>(), grid, block, adj_rows_smem<M>(), st, a, r);
 }
 
 }  // namespace fft
