@@ -2139,9 +2139,10 @@ struct Engine : EngineBase {
 
     // ------------------------------------------------------------ adjoint
     // Checkpoint m holds the state entering layer L-1-m*K: the plasma
-    // particles (y, z, px, py, pz) and the P-bank spectra (Rho, Ex, Ey, Ez,
-    // Jx, Jy, Jz); the P-layer fields are layer L-m*K of the field store.
-    size_t ck_stride() const { return 5 * (size_t)adj_np + 7 * plane; }
+    // particles (y, z, px, py, pz, and their weights, which the regrouping
+    // carries along) and the P-bank spectra (Rho, Ex, Ey, Ez, Jx, Jy, Jz);
+    // the P-layer fields are layer L-m*K of the field store.
+    size_t ck_stride() const { return 6 * (size_t)adj_np + 7 * plane; }
     size_t seg_stride() const { return 5 * (size_t)adj_np + (size_t)(nIter + 1) * 6 * plane; }
     T* particle_arrays(int c) { T* a[5] = {py, pz, ppx, ppy, ppz}; return a[c]; }
 
@@ -2152,8 +2153,10 @@ struct Engine : EngineBase {
         for (int c = 0; c < 5; c++)
             CK(cudaMemcpyAsync(dst + (size_t)c * np, particle_arrays(c), np * sizeof(T),
                                cudaMemcpyDeviceToDevice, st));
+        CK(cudaMemcpyAsync(dst + 5 * (size_t)np, pw, np * sizeof(T), cudaMemcpyDeviceToDevice,
+                           st));
         const int pb = cur ^ 1;
-        T* b = dst + 5 * (size_t)np;
+        T* b = dst + 6 * (size_t)np;
         CK(cudaMemcpyAsync(b, bankp(pb, SP_RHO), 4 * plane * sizeof(T), cudaMemcpyDeviceToDevice,
                            st));
         CK(cudaMemcpyAsync(b + 4 * plane, bankp(pb, SP_JX), 3 * plane * sizeof(T),
@@ -2173,8 +2176,12 @@ struct Engine : EngineBase {
         for (int c = 0; c < 5; c++)
             CK(cudaMemcpyAsync(particle_arrays(c), src + (size_t)c * np, np * sizeof(T),
                                cudaMemcpyDeviceToDevice, st));
+        // the weights in this checkpoint's particle order (the plasma may
+        // have been regrouped since)
+        CK(cudaMemcpyAsync(pw, src + 5 * (size_t)np, np * sizeof(T), cudaMemcpyDeviceToDevice,
+                           st));
         const int pb = cur ^ 1;
-        const T* b = src + 5 * (size_t)np;
+        const T* b = src + 6 * (size_t)np;
         CK(cudaMemcpyAsync(bankp(pb, SP_RHO), b, 4 * plane * sizeof(T), cudaMemcpyDeviceToDevice,
                            st));
         CK(cudaMemcpyAsync(bankp(pb, SP_JX), b + 4 * plane, 3 * plane * sizeof(T),

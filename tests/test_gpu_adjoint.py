@@ -19,7 +19,7 @@ pytestmark = pytest.mark.gpu
 NBINS = 8
 
 
-def setup(prec, layers=48, n=32, every=8, shape=QS_SHAPE_NGP):
+def setup(prec, layers=48, n=32, every=8, shape=QS_SHAPE_NGP, weights=False):
     from tertia_b200.mesh import Mesh
     cfg = wl.small_config(n=n, layers=layers, ts=0.0, synchrotron=0, shape=shape)
     cfg.precision = PRECISIONS[prec]
@@ -27,7 +27,11 @@ def setup(prec, layers=48, n=32, every=8, shape=QS_SHAPE_NGP):
     x = (beam["i"] + beam["x"]) * cfg.hx
     bins = xi_bins(beam, cfg, NBINS, float(x.min()), float(x.max()) + 1e-9)
     m = Mesh(cfg)
-    m.load_front_plasma(wl.front_plasma(cfg, thermal=False))
+    front = wl.front_plasma(cfg, thermal=False)
+    if weights:   # unequal particle weights (seeded)
+        front["w"] = np.asarray(front["w"]) * np.random.default_rng(5).uniform(
+            0.5, 1.5, len(front["w"]))
+    m.load_front_plasma(front)
     m.adjoint_checkpoints(every)
     # window: a band of layers in the middle of the box, behind the driver
     coeff = np.zeros(cfg.nx)
@@ -118,6 +122,20 @@ def test_cic_adjoint_fp32_close_to_fp64_adjoint():
     grads = {}
     for prec in ("fp64", "fp32"):
         cfg, m, beam, bins, coeff = setup(prec, shape=QS_SHAPE_CIC)
+        grads[prec] = adjoint_grad(m, beam, bins, coeff, beta)
+        m.close()
+    assert rel(grads["fp32"], grads["fp64"]) < 1e-4, grads
+
+
+def test_cic_adjoint_fp32_unequal_weights_close_to_fp64_adjoint():
+    """Particles of unequal weight: the FP32 march regroups them, weights
+    included, by cell; the checkpoints keep each particle's weight with it, so
+    that a recomputed segment pushes every particle with its own weight (the
+    plain FP64 path keeps the load order)."""
+    beta = np.random.default_rng(12).uniform(0.5, 1.5, NBINS)
+    grads = {}
+    for prec in ("fp64", "fp32"):
+        cfg, m, beam, bins, coeff = setup(prec, shape=QS_SHAPE_CIC, weights=True)
         grads[prec] = adjoint_grad(m, beam, bins, coeff, beta)
         m.close()
     assert rel(grads["fp32"], grads["fp64"]) < 1e-4, grads
