@@ -261,6 +261,15 @@ struct Engine : EngineBase {
     // beside the next layer's first field z-pass (which then uses scratch2)
     bool side_adj = false, adj_pred_pending = false;
     T* push_favg = nullptr;     // the next push writes its gathered fields here
+    // The adjoint's store of the fields every push of the last march gathered,
+    // (nIter + 1) x 6 planes per layer, kept when checkpoints are on, the push
+    // is the grouped CIC one and the store fits in free device memory: the
+    // adjoint then recomputes a segment's particle states by its full pushes
+    // alone, each gathering the stored fields (the march's pushes, bit for
+    // bit), instead of by the whole march.  QS_ADJ_FIELDS=0 leaves it out.
+    T* fstore = nullptr;
+    bool fstore_wanted = !(getenv("QS_ADJ_FIELDS") && getenv("QS_ADJ_FIELDS")[0] == '0');
+    const T* push_fields = nullptr;   // the next push gathers these planes alone
     T* mats = nullptr;          // transform matrices
     DttMats<T> my, mz;
     TcTransformer* tcx = nullptr;
@@ -394,7 +403,7 @@ struct Engine : EngineBase {
                         d_dloss, d_gradw, acell, pid, apid, ay, az, apx, apy, apz, aw, cic_cnt,
                         cic_loff, cic_bsum, cic_bpref, cic_ticket, ck_cell, ck_id, seg_cell,
                         adj_inv, lam_pos, adj_tmp, d_pack, d_pack_i, q_cy, q_cz, q_part,
-                        qb_part, q_sums, study_f, study_p, scratch2};
+                        qb_part, q_sums, study_f, study_p, scratch2, fstore};
         for (void* p : ptrs)
             if (p) cudaFree(p);
         for (int k = 0; k < 2; k++) {
@@ -1456,6 +1465,10 @@ struct Engine : EngineBase {
         a.y = py; a.z = pz; a.px = ppx; a.py = ppy; a.pz = ppz; a.w = pw;
         a.P = from_avg ? Cf : Pf;   // (C + C) / 2 = C exactly
         a.C = Cf;
+        if (push_fields) {   // the adjoint's recomputation: the stored gathered fields
+            a.P = a.C = push_fields;
+            push_fields = nullptr;
+        }
         a.dep = Csrc;
         a.cell_out = pcell;
         a.dep_cell = nullptr;
@@ -1801,12 +1814,16 @@ struct Engine : EngineBase {
     }
 
     qs_status move_split_layer(int iLayer, int iSplit) override {
+        // with the adjoint's field store, each push leaves its gathered fields there
+        const bool keep = in_march && !adj_recompute && fstore_ok();
         qs_status s = guess(iLayer, iSplit);
         if (s) return s;
         for (int it = 0; it < nIter; it++) {
+            if (keep) push_favg = fstore_at(iLayer, it);
             if ((s = push(iLayer, iSplit, 0))) return s;
             if ((s = iterate(iLayer, iSplit, it, nullptr))) return s;
         }
+        if (keep) push_favg = fstore_at(iLayer, nIter);
         if ((s = push(iLayer, iSplit, 1))) return s;
         return iterate(iLayer, iSplit, -1, nullptr);
     }
@@ -2210,10 +2227,10 @@ struct Engine : EngineBase {
             return fail(QS_ERR_UNSUPPORTED, "the adjoint supports NxSplit = 1");
         CK(cudaStreamSynchronize(st));
         void* old[] = {ck, seg, lam, lam_pm, lam_sb, d_dloss, ck_cell, ck_id, seg_cell,
-                       lam_pos, adj_inv, adj_tmp};
+                       lam_pos, adj_inv, adj_tmp, fstore};
         for (void* p : old)
             if (p) cudaFree(p);
-        ck = seg = lam = lam_pm = lam_sb = d_dloss = lam_pos = adj_tmp = nullptr;
+        ck = seg = lam = lam_pm = lam_sb = d_dloss = lam_pos = adj_tmp = fstore = nullptr;
         lam_lo = -1;
         ck_cell = ck_id = seg_cell = adj_inv = nullptr;
         ck_every = 0;
@@ -2245,8 +2262,20 @@ struct Engine : EngineBase {
                 if ((s = alloc(&adj_tmp, 5 * (size_t)np, "adjoint reorder"))) return s;
             }
         }
+        if (cic_sort && fstore_wanted && !fp32_study) {
+            // only where it leaves an eighth of the device free
+            const size_t n = (size_t)L * (nIter + 1) * 6 * plane;
+            size_t fr = 0, tot = 0;
+            if (cudaMemGetInfo(&fr, &tot) == cudaSuccess && n * sizeof(T) + tot / 8 < fr)
+                if ((s = alloc(&fstore, n, "adjoint field store"))) return s;
+        }
         ck_every = K;
         return QS_OK;
+    }
+
+    bool fstore_ok() const { return fstore && ck_every > 0 && cic_sort && !src3 && !fp32_study; }
+    T* fstore_at(int layer, int q) {
+        return fstore + ((size_t)layer * (nIter + 1) + q) * 6 * plane;
     }
 
     // adjoint work planes
@@ -2274,6 +2303,41 @@ struct Engine : EngineBase {
     }
     T* lam_sbp(int layer, int q) { return lam_sb + ((size_t)(layer - lam_lo) * 2 + q) * plane; }
 
+    // save the particles (and cells) entering layer i into the segment's slot
+    void save_entry(T* slot, int i, int c) {
+        StateCopy<T> sc{};
+        for (int q = 0; q < 5; q++) {
+            sc.src[q] = particle_arrays(q);
+            sc.dst[q] = slot + (size_t)q * np;
+        }
+        if (cic_adj) {
+            sc.csrc = pcell;
+            sc.cdst = seg_cell + (size_t)(c - i) * np;
+        }
+        sc.n = np;
+        klaunch(KC_MISC, [&] { return launch_save_state<T>(sc, st); });
+    }
+
+    // with the field store: recompute the particles entering layers c .. lo
+    // of one segment from its checkpoint by the full pushes alone, each
+    // gathering the fields the march stored for it (its deposit is not read)
+    qs_status recompute_states(int m, int c, int lo) {
+        in_march = true;
+        adj_recompute = true;
+        qs_status s = restore_checkpoint(m);
+        for (int i = c; !s && i >= lo; i--) {
+            save_entry(seg + (size_t)(c - i) * seg_stride(), i, c);
+            if (i > lo) {
+                push_fields = fstore_at(i, nIter);
+                s = push(i, 0, 1);
+            }
+        }
+        push_fields = nullptr;
+        in_march = false;
+        adj_recompute = false;
+        return s;
+    }
+
     // recompute the layers c .. lo of one segment from its checkpoint, storing
     // each layer's entry particles and intermediate C fields
     qs_status recompute_segment(int m, int c, int lo) {
@@ -2288,19 +2352,7 @@ struct Engine : EngineBase {
         qs_status s = restore_checkpoint(m);
         for (int i = c; !s && i >= lo; i--) {
             T* slot = seg + (size_t)(c - i) * seg_stride();
-            {   // the layer's entry particles (and cells), in one launch
-                StateCopy<T> sc{};
-                for (int q = 0; q < 5; q++) {
-                    sc.src[q] = particle_arrays(q);
-                    sc.dst[q] = slot + (size_t)q * np;
-                }
-                if (cic_adj) {
-                    sc.csrc = pcell;
-                    sc.cdst = seg_cell + (size_t)(c - i) * np;
-                }
-                sc.n = np;
-                klaunch(KC_MISC, [&] { return launch_save_state<T>(sc, st); });
-            }
+            save_entry(slot, i, c);   // the layer's entry particles (and cells), in one launch
             T* fs = slot + 5 * (size_t)np;
             if ((s = layer_begin(i, 0))) break;
             if ((s = guess(i, 0))) break;
@@ -2427,10 +2479,10 @@ struct Engine : EngineBase {
         }
     }
 
-    qs_status adjoint_layer(int i, const T* slot, const int32_t* slot_cell) {
+    // fs: the fields each push of the layer gathered, 6 planes per push
+    qs_status adjoint_layer(int i, const T* slot, const int32_t* slot_cell, const T* fs) {
         const int EBz[6] = {CC, CC, SS, SS, SS, CC}, EBy[6] = {CC, SS, CC, SS, CC, SS};
         const int Jz[3] = {CC, CC, SS}, Jy[3] = {CC, SS, CC};
-        const T* fs = slot + 5 * (size_t)np;
         const T sc = inv_scale();
         Pf = f3layer(i + 1);
         // LAM_PF gathers this layer's shares from zero (on the fused path the
@@ -2576,13 +2628,15 @@ struct Engine : EngineBase {
                     });
                 }
                 cur = 0;
-                qs_status s = recompute_segment(m, c, end);
+                const bool stored = fstore_ok();
+                qs_status s = stored ? recompute_states(m, c, end) : recompute_segment(m, c, end);
                 if (s) return s;
                 side_adj = !prof && !fp32_study && adj_fused();
                 adj_pred_pending = false;
                 for (int i = end; i <= c && !s; i++) {
                     const int32_t* sc = cic_adj ? seg_cell + (size_t)(c - i) * np : nullptr;
-                    s = adjoint_layer(i, seg + (size_t)(c - i) * seg_stride(), sc);
+                    const T* slot = seg + (size_t)(c - i) * seg_stride();
+                    s = adjoint_layer(i, slot, sc, stored ? fstore_at(i, 0) : slot + 5 * (size_t)np);
                 }
                 join_sides();   // the next recomputation rewrites what the sweep reads
                 side_adj = adj_pred_pending = false;

@@ -141,6 +141,24 @@ def test_cic_adjoint_fp32_unequal_weights_close_to_fp64_adjoint():
     assert rel(grads["fp32"], grads["fp64"]) < 1e-4, grads
 
 
+@pytest.mark.parametrize("prec,tol", [("fp32", 1e-5), ("fp64fft", 1e-12)])
+def test_cic_adjoint_from_stored_fields_matches_full_recomputation(prec, tol, monkeypatch):
+    """With the field store (the fields each push gathered, kept by the
+    checkpointed march) a segment is recomputed by its full pushes alone;
+    without it (QS_ADJ_FIELDS=0, read when a handle is created) by the whole
+    march.  Both give the same gradient."""
+    beta = np.random.default_rng(13).uniform(0.5, 1.5, NBINS)
+    grads = []
+    for store in ("1", "0"):
+        monkeypatch.setenv("QS_ADJ_FIELDS", store)
+        cfg, m, beam, bins, coeff = setup(prec, n=128, layers=32, shape=QS_SHAPE_CIC,
+                                          weights=True)
+        grads.append(adjoint_grad(m, beam, bins, coeff, beta))
+        m.close()
+    assert np.linalg.norm(grads[0]) > 0
+    assert rel(grads[0], grads[1]) < tol, grads
+
+
 def test_cic_adjoint_fp64_fft_matches_fp64_adjoint():
     """The FP64 path on FFT transforms regroups the plasma by cell like FP32
     and pushes with FMA; its gradient is the plain FP64 path's to rounding."""
