@@ -300,6 +300,63 @@ def adjoint_measure(precision: str):
                       "around qs_adjoint (it synchronises)"}
 
 
+def adjoint_grid_measure(workload="c1", precision="fp32", every=32, nbins=64):
+    """The adjoint on the forward's own grid (c1: 512 x 512 x 1024, the
+    size the adjoint's cost target is quoted at), with the c3 adjoint's
+    loss, bins and checkpoint interval: the driver's charge profile as
+    `nbins` xi-bins, loss = on-axis Ex integrated over xi in [-6, -5] behind
+    the driver centre, beam deposited in place.  Timing only: the march
+    (device events) and qs_adjoint (host clock; it synchronises), the third
+    of three runs."""
+    import numpy as np
+    import torch
+    from tertia_b200 import workload as wl
+    from tertia_b200.abi import QS_SHAPE_CIC
+    from tertia_b200.autograd import xi_bins
+    from tertia_b200.mesh import Mesh
+
+    w = wl.make_workload(workload, precision)
+    cfg = w.cfg
+    cfg.shape = QS_SHAPE_CIC
+    cfg.ts = 0.0
+    cfg.synchrotron = 0
+    beam = wl.workload_beam(w)
+    xc = wl.driver_center_x(cfg, w.beams[0].sigma_xi)
+    sx = w.beams[0].sigma_xi
+    bins = xi_bins(beam, cfg, nbins, xc - 4 * sx, xc + 4 * sx)
+    xl = np.arange(cfg.nx) * cfg.hx
+    coeff = np.where((xl >= xc - 6.0) & (xl <= xc - 5.0), cfg.hx, 0.0)
+    beta = np.random.default_rng(3).uniform(0.5, 1.5, nbins)
+    bb = dict(beam)
+    bb["w"] = np.asarray(beam["w"]) * beta[bins]
+    with Mesh(cfg) as m:
+        m.seed_front_plasma(0)
+        m.adjoint_checkpoints(every)
+        st = torch.cuda.ExternalStream(m.stream())
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        for _ in range(3):
+            m.load_beam(bb)
+            m.move_beam_particles()
+            torch.cuda.synchronize()
+            e0.record(st)
+            m.move_all_split_layers()
+            e1.record(st)
+            torch.cuda.synchronize()
+            fwd = e0.elapsed_time(e1)
+            t0 = time.perf_counter()
+            m.adjoint(coeff)
+            torch.cuda.synchronize()
+            adj = (time.perf_counter() - t0) * 1e3
+    lo = int(np.nonzero(coeff)[0].min())
+    swept = cfg.nx - lo
+    return {"workload": f"{w.name} grid: {cfg.ny}x{cfg.nz}x{cfg.nx} CIC {precision}, the c3 "
+                        f"adjoint's loss and {nbins} xi-bins, checkpoints every {every} layers",
+            "forward_ms": fwd, "adjoint_ms": adj, "layers_swept": swept, "layers": cfg.nx,
+            "adjoint_over_forward_same_layers": adj / (fwd * swept / cfg.nx),
+            "timing": "forward: device events around the checkpointed march; adjoint: host "
+                      "wall clock around qs_adjoint (it synchronises); third of three runs"}
+
+
 # ------------------------------------------------------------------ FP64 comparison
 STUDY_BITS = (("transforms", 1), ("spectral_state", 2), ("push", 4), ("fields", 8),
               ("beam_currents", 16), ("front_plasma_input", 32), ("particle_state_storage", 64),
@@ -997,6 +1054,11 @@ def run_ours(args):
     adjoint = None
     if rank == 0 and world == 1 and not args.no_adjoint and not args.layers:
         adjoint = adjoint_measure(args.precision)
+        # the same adjoint on the forward's grid (a failure is reported, not fatal)
+        try:
+            adjoint["on_forward_grid"] = adjoint_grid_measure(args.workload, args.precision)
+        except Exception as e:   # noqa: BLE001
+            adjoint["on_forward_grid"] = {"error": f"{type(e).__name__}: {e}"}
     nxt = None
     if rank == 0 and world == 1 and not args.no_next and not args.layers:
         # auxiliary rows: a failure here is reported in the line, not fatal to it

@@ -262,13 +262,17 @@ struct Engine : EngineBase {
     bool side_adj = false, adj_pred_pending = false;
     T* push_favg = nullptr;     // the next push writes its gathered fields here
     // The adjoint's store of the fields every push of the last march gathered,
-    // (nIter + 1) x 6 planes per layer, kept when checkpoints are on, the push
-    // is the grouped CIC one and the store fits in free device memory: the
-    // adjoint then recomputes a segment's particle states by its full pushes
+    // (nIter + 1) x 6 planes per layer, kept when checkpoints are on and the
+    // push is the grouped CIC one, for the fstore_n layers nearest the head
+    // that fit in free device memory (all of them where they fit): the adjoint
+    // recomputes a segment whose layers are all stored by its full pushes
     // alone, each gathering the stored fields (the march's pushes, bit for
-    // bit), instead of by the whole march.  QS_ADJ_FIELDS=0 leaves it out.
+    // bit), instead of by the whole march.  The adjoint sweeps from the head
+    // down to the loss window, so the head layers are the ones it reads.
+    // QS_ADJ_FIELDS=n stores at most n layers (0: no store).
     T* fstore = nullptr;
-    bool fstore_wanted = !(getenv("QS_ADJ_FIELDS") && getenv("QS_ADJ_FIELDS")[0] == '0');
+    int fstore_n = 0;
+    long fstore_cap = getenv("QS_ADJ_FIELDS") ? atol(getenv("QS_ADJ_FIELDS")) : -1;
     const T* push_fields = nullptr;   // the next push gathers these planes alone
     T* mats = nullptr;          // transform matrices
     DttMats<T> my, mz;
@@ -1815,7 +1819,7 @@ struct Engine : EngineBase {
 
     qs_status move_split_layer(int iLayer, int iSplit) override {
         // with the adjoint's field store, each push leaves its gathered fields there
-        const bool keep = in_march && !adj_recompute && fstore_ok();
+        const bool keep = in_march && !adj_recompute && fstored(iLayer);
         qs_status s = guess(iLayer, iSplit);
         if (s) return s;
         for (int it = 0; it < nIter; it++) {
@@ -2262,20 +2266,33 @@ struct Engine : EngineBase {
                 if ((s = alloc(&adj_tmp, 5 * (size_t)np, "adjoint reorder"))) return s;
             }
         }
-        if (cic_sort && fstore_wanted && !fp32_study) {
-            // only where it leaves an eighth of the device free
-            const size_t n = (size_t)L * (nIter + 1) * 6 * plane;
+        fstore_n = 0;
+        if (cic_sort && fstore_cap != 0 && !fp32_study) {
+            // as many head layers as leave a sixteenth of the device free
+            // (for the adjoint's own buffers, allocated when it first runs)
+            const size_t per = (size_t)(nIter + 1) * 6 * plane * sizeof(T);
             size_t fr = 0, tot = 0;
-            if (cudaMemGetInfo(&fr, &tot) == cudaSuccess && n * sizeof(T) + tot / 8 < fr)
-                if ((s = alloc(&fstore, n, "adjoint field store"))) return s;
+            if (cudaMemGetInfo(&fr, &tot) == cudaSuccess && fr > tot / 16) {
+                const size_t fit = (fr - tot / 16) / per;
+                size_t cap = std::min<size_t>((size_t)L, fit);
+                if (fstore_cap > 0) cap = std::min<size_t>(cap, (size_t)fstore_cap);
+                const int n = (int)cap;
+                if (n >= K) {   // at least one whole segment
+                    if ((s = alloc(&fstore, (size_t)n * per / sizeof(T), "adjoint field store")))
+                        return s;
+                    fstore_n = n;
+                }
+            }
         }
         ck_every = K;
         return QS_OK;
     }
 
     bool fstore_ok() const { return fstore && ck_every > 0 && cic_sort && !src3 && !fp32_study; }
+    // the store holds layers L - fstore_n .. L - 1, the head layer first
+    bool fstored(int layer) const { return fstore_ok() && layer >= L - fstore_n; }
     T* fstore_at(int layer, int q) {
-        return fstore + ((size_t)layer * (nIter + 1) + q) * 6 * plane;
+        return fstore + ((size_t)(L - 1 - layer) * (nIter + 1) + q) * 6 * plane;
     }
 
     // adjoint work planes
@@ -2628,7 +2645,7 @@ struct Engine : EngineBase {
                     });
                 }
                 cur = 0;
-                const bool stored = fstore_ok();
+                const bool stored = fstored(end);   // then every layer of the segment
                 qs_status s = stored ? recompute_states(m, c, end) : recompute_segment(m, c, end);
                 if (s) return s;
                 side_adj = !prof && !fp32_study && adj_fused();

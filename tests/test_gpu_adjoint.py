@@ -146,17 +146,23 @@ def test_cic_adjoint_from_stored_fields_matches_full_recomputation(prec, tol, mo
     """With the field store (the fields each push gathered, kept by the
     checkpointed march) a segment is recomputed by its full pushes alone;
     without it (QS_ADJ_FIELDS=0, read when a handle is created) by the whole
-    march.  Both give the same gradient."""
+    march; with the store cut to the 16 head layers (QS_ADJ_FIELDS=16) the
+    two head segments of the sweep come from it and the third from the
+    march.  All three give the same gradient."""
     beta = np.random.default_rng(13).uniform(0.5, 1.5, NBINS)
     grads = []
-    for store in ("1", "0"):
-        monkeypatch.setenv("QS_ADJ_FIELDS", store)
+    for store in ("", "16", "0"):
+        if store:
+            monkeypatch.setenv("QS_ADJ_FIELDS", store)
+        else:
+            monkeypatch.delenv("QS_ADJ_FIELDS", raising=False)
         cfg, m, beam, bins, coeff = setup(prec, n=128, layers=32, shape=QS_SHAPE_CIC,
                                           weights=True)
         grads.append(adjoint_grad(m, beam, bins, coeff, beta))
         m.close()
     assert np.linalg.norm(grads[0]) > 0
-    assert rel(grads[0], grads[1]) < tol, grads
+    assert rel(grads[0], grads[2]) < tol, grads
+    assert rel(grads[1], grads[2]) < tol, grads
 
 
 def test_cic_adjoint_fp64_fft_matches_fp64_adjoint():
