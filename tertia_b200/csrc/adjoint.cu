@@ -296,36 +296,49 @@ __device__ __forceinline__ float fdiv<float>(float a, float b) { return __fdivid
 // the adjoint of the fields it gathered (6 fields x 4 corners of its cell,
 // index f*4 + r) goes to lf, and its cell is returned (-1 when the forward
 // skipped the particle).
+// Offsets into the planes and the per-particle arrays are 32-bit (the
+// adjoint's set-up checks 6 ny nz and 3 n below 2^31), so that an address is
+// one wide multiply-add from its base.  (j, k) of the cell is returned too.
+// The gathered fields' y and z slopes, needed only at the end, wait in
+// shared memory (sg: 12 x blockDim values, this thread's column) instead of
+// 12 registers through the recompute and the backward.
 template <class T>
-__device__ __forceinline__ int push_adjoint_cic_one(const PushAdjArgs<T>& a, int64_t i,
-                                                    T (&lf)[24]) {
+__device__ __forceinline__ int push_adjoint_cic_one(const PushAdjArgs<T>& a, uint32_t i,
+                                                    T (&lf)[24], int& jo, int& ko, T* sg) {
     const int My = a.My, Mz = a.Mz;
     const int cell = a.cell[i];
-    const int j = cell % My, k = cell / My;
+    int j, k;
+    cell_jk(cell, My, a.invMy, j, k);
+    jo = j;
+    ko = k;
     const T one = T(1), half = T(0.5);
     const T yp = a.y[i], zp = a.z[i];
     if (!(yp >= T(0) && yp <= one && zp >= T(0) && zp <= one)) return -1;   // forward skipped it
     const T px0 = a.px[i], py0 = a.py[i], pz0 = a.pz[i];
     const T w = a.w[i];
-    const size_t plane = a.plane;
-    const int j1 = wrap_m(j + 1, My), k1 = wrap_m(k + 1, Mz);
-    const size_t nn[4] = {(size_t)j + (size_t)My * k, (size_t)j1 + (size_t)My * k,
-                          (size_t)j + (size_t)My * k1, (size_t)j1 + (size_t)My * k1};
-    const T wg[4] = {(one - yp) * (one - zp), yp * (one - zp), (one - yp) * zp, yp * zp};
+    const uint32_t plane = (uint32_t)a.plane, un = (uint32_t)a.n;
+    const int j1 = wrap1(j + 1, My), k1 = wrap1(k + 1, Mz);
+    const uint32_t row0 = (uint32_t)My * (uint32_t)k, row1 = (uint32_t)My * (uint32_t)k1;
+    const uint32_t nn[4] = {(uint32_t)j + row0, (uint32_t)j1 + row0, (uint32_t)j + row1,
+                            (uint32_t)j1 + row1};
+    const int tid = threadIdx.x, nt = blockDim.x;
     // the gathered fields g and their derivatives in y and z (kept instead of
     // the 24 corner values for the position adjoint of the gather)
-    T g[6], gy[6], gz[6];
+    T g[6];
+    {
+        const T wg[4] = {(one - yp) * (one - zp), yp * (one - zp), (one - yp) * zp, yp * zp};
 #pragma unroll
-    for (int f = 0; f < 6; f++) {
-        T F[4];
-        g[f] = T(0);
+        for (int f = 0; f < 6; f++) {
+            T F[4];
+            g[f] = T(0);
 #pragma unroll
-        for (int r = 0; r < 4; r++) {
-            F[r] = ldg_(a.F + f * plane + nn[r]);
-            g[f] += wg[r] * F[r];
+            for (int r = 0; r < 4; r++) {
+                F[r] = ldg_(a.F + (f * plane + nn[r]));
+                g[f] += wg[r] * F[r];
+            }
+            sg[f * nt + tid] = (one - zp) * (F[1] - F[0]) + zp * (F[3] - F[2]);
+            sg[(6 + f) * nt + tid] = (one - yp) * (F[2] - F[0]) + yp * (F[3] - F[1]);
         }
-        gy[f] = (one - zp) * (F[1] - F[0]) + zp * (F[3] - F[2]);
-        gz[f] = (one - yp) * (F[2] - F[0]) + yp * (F[3] - F[1]);
     }
     const T E[3] = {g[0], g[1], g[2]};
     const T B[3] = {g[3] + a.bxe, g[4] + a.bye, g[5] + a.bze};
@@ -404,8 +417,8 @@ __device__ __forceinline__ int push_adjoint_cic_one(const PushAdjArgs<T>& a, int
             int sy = (int)fy, sz = (int)fz;
             if (ry >= one) { ry = T(0); sy += 1; }
             if (rz >= one) { rz = T(0); sz += 1; }
-            jb = wrap_m(jb + sy, My);
-            kb = wrap_m(kb + sz, Mz);
+            jb = wrap1(jb + sy, My);     // |sy|, |sz| <= 2: a sub-step moves at most a cell
+            kb = wrap1(kb + sz, Mz);
             ytmp = ry;
             ztmp = rz;
             if (ns == 0) {
@@ -419,14 +432,15 @@ __device__ __forceinline__ int push_adjoint_cic_one(const PushAdjArgs<T>& a, int
     }
 
     // ---- backward through the sub-steps: deposits and position chain
-    T lyc = a.full ? a.lamPos[i] : T(0), lzc = a.full ? a.lamPos[a.n + i] : T(0);
+    T lyc = a.full ? a.lamPos[i] : T(0), lzc = a.full ? a.lamPos[un + i] : T(0);
     T ldy = T(0), ldz = T(0), lstep = T(0);
     T ldq[3] = {T(0), T(0), T(0)};
     auto back = [&](T ry, T rz, T ps, T dps, int jb, int kb) {
         T lps = T(0);
-        const int jb1 = wrap_m(jb + 1, My), kb1 = wrap_m(kb + 1, Mz);
-        const size_t nd[4] = {(size_t)jb + (size_t)My * kb, (size_t)jb1 + (size_t)My * kb,
-                              (size_t)jb + (size_t)My * kb1, (size_t)jb1 + (size_t)My * kb1};
+        const int jb1 = wrap1(jb + 1, My), kb1 = wrap1(kb + 1, Mz);
+        const uint32_t rb0 = (uint32_t)My * (uint32_t)kb, rb1 = (uint32_t)My * (uint32_t)kb1;
+        const uint32_t nd[4] = {(uint32_t)jb + rb0, (uint32_t)jb1 + rb0, (uint32_t)jb + rb1,
+                                (uint32_t)jb1 + rb1};
         const T wc[4] = {(one - ry) * (one - rz), ry * (one - rz), (one - ry) * rz, ry * rz};
         T lwc[4];
 #pragma unroll
@@ -434,7 +448,7 @@ __device__ __forceinline__ int push_adjoint_cic_one(const PushAdjArgs<T>& a, int
             T acc = T(0);
 #pragma unroll
             for (int d = 0; d < 3; d++) {
-                const T G = ldg_(a.lamD + d * plane + nd[r]);
+                const T G = ldg_(a.lamD + (d * plane + nd[r]));
                 ldq[d] += ps * wc[r] * G;
                 acc += dq[d] * G;
             }
@@ -460,8 +474,8 @@ __device__ __forceinline__ int push_adjoint_cic_one(const PushAdjArgs<T>& a, int
     T bp2[3] = {T(0), T(0), T(0)};
     if (a.full) {
         bp2[0] = a.lamPm[i];
-        bp2[1] = a.lamPm[a.n + i];
-        bp2[2] = a.lamPm[2 * a.n + i];
+        bp2[1] = a.lamPm[un + i];
+        bp2[2] = a.lamPm[2 * un + i];
     }
     T bVm[3], bwq = T(0);
 #pragma unroll
@@ -539,25 +553,26 @@ __device__ __forceinline__ int push_adjoint_cic_one(const PushAdjArgs<T>& a, int
     }
     // ---- backward through the gather g_f = sum_r wg_r F_f,r
     const T bg[6] = {bE[0], bE[1], bE[2], bB[0], bB[1], bB[2]};
+    const T wg[4] = {(one - yp) * (one - zp), yp * (one - zp), (one - yp) * zp, yp * zp};
 #pragma unroll
     for (int f = 0; f < 6; f++) {
-        lyp += bg[f] * gy[f];
-        lzp += bg[f] * gz[f];
+        lyp += bg[f] * sg[f * nt + tid];
+        lzp += bg[f] * sg[(6 + f) * nt + tid];
 #pragma unroll
         for (int r = 0; r < 4; r++) lf[f * 4 + r] = half * wg[r] * bg[f];
     }
     if (a.full) {
         a.lamPm[i] = bp[0];
-        a.lamPm[a.n + i] = bp[1];
-        a.lamPm[2 * a.n + i] = bp[2];
+        a.lamPm[un + i] = bp[1];
+        a.lamPm[2 * un + i] = bp[2];
         a.lamPos[i] = lyp;
-        a.lamPos[a.n + i] = lzp;
+        a.lamPos[un + i] = lzp;
     } else {
         a.lamPm[i] += bp[0];
-        a.lamPm[a.n + i] += bp[1];
-        a.lamPm[2 * a.n + i] += bp[2];
+        a.lamPm[un + i] += bp[1];
+        a.lamPm[2 * un + i] += bp[2];
         a.lamPos[i] += lyp;
-        a.lamPos[a.n + i] += lzp;
+        a.lamPos[un + i] += lzp;
     }
     return cell;
 }
@@ -594,24 +609,27 @@ __device__ __forceinline__ bool warp_run_sums(T (&v)[NV], int key) {
 template <class T>
 __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 1)
     push_adjoint_cic_kernel(PushAdjArgs<T> a) {
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    __shared__ T sg[12 * 256];
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     pdl_wait();
     T lf[24];
 #pragma unroll
     for (int q = 0; q < 24; q++) lf[q] = T(0);
-    const int cell = i < a.n ? push_adjoint_cic_one(a, i, lf) : -1;
+    int j = 0, k = 0;
+    const int cell = i < (uint32_t)a.n ? push_adjoint_cic_one(a, i, lf, j, k, sg) : -1;
     // the field adjoints of a cell's particles summed in the warp, then one
     // atomic per field and corner
     if (warp_run_sums<24>(lf, cell)) {
         const int My = a.My, Mz = a.Mz;
-        const int j = cell % My, k = cell / My;
-        const int j1 = wrap_m(j + 1, My), k1 = wrap_m(k + 1, Mz);
-        const size_t nn[4] = {(size_t)j + (size_t)My * k, (size_t)j1 + (size_t)My * k,
-                              (size_t)j + (size_t)My * k1, (size_t)j1 + (size_t)My * k1};
+        const uint32_t plane = (uint32_t)a.plane;
+        const int j1 = wrap1(j + 1, My), k1 = wrap1(k + 1, Mz);
+        const uint32_t row0 = (uint32_t)My * (uint32_t)k, row1 = (uint32_t)My * (uint32_t)k1;
+        const uint32_t nn[4] = {(uint32_t)j + row0, (uint32_t)j1 + row0, (uint32_t)j + row1,
+                                (uint32_t)j1 + row1};
 #pragma unroll
         for (int f = 0; f < 6; f++)
 #pragma unroll
-            for (int r = 0; r < 4; r++) atomicAdd(a.lamFC + f * a.plane + nn[r], lf[f * 4 + r]);
+            for (int r = 0; r < 4; r++) atomicAdd(a.lamFC + (f * plane + nn[r]), lf[f * 4 + r]);
     }
 }
 

@@ -2229,6 +2229,10 @@ struct Engine : EngineBase {
         if (every < 0) return fail(QS_ERR_INVALID, "qs_adjoint_checkpoints: every must be >= 0");
         if (every > 0 && S != 1)
             return fail(QS_ERR_UNSUPPORTED, "the adjoint supports NxSplit = 1");
+        // the push adjoint indexes the planes and per-particle arrays with 32-bit offsets
+        if (every > 0 && (6 * (uint64_t)plane >= (1ull << 31) || 3 * (uint64_t)np >= (1ull << 31)))
+            return fail(QS_ERR_UNSUPPORTED, "the adjoint needs 6 ny nz and 3 x the particle count "
+                                            "below 2^31");
         CK(cudaStreamSynchronize(st));
         void* old[] = {ck, seg, lam, lam_pm, lam_sb, d_dloss, ck_cell, ck_id, seg_cell,
                        lam_pos, adj_inv, adj_tmp, fstore};
@@ -2427,6 +2431,7 @@ struct Engine : EngineBase {
                                  int full) {
         PushAdjArgs<T> a{};
         a.n = np; a.My = My; a.Mz = Mz;
+        a.invMy = 1.0f / (float)My;
         a.cell = cic_adj ? slot_cell : pcell;   // NGP: the seeded cells never change
         a.lamPos = lam_pos;
         a.y = slot; a.z = slot + np; a.px = slot + 2 * np; a.py = slot + 3 * np;

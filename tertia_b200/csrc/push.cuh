@@ -55,22 +55,6 @@ __device__ __forceinline__ int wrap_idx(int j, int M) {
     return j;
 }
 
-// j within one period of [0, M) (a shift of at most one cell): no loop
-__device__ __forceinline__ int wrap1(int j, int M) {
-    j += (j < 0) ? M : 0;
-    return j - ((j >= M) ? M : 0);
-}
-
-// k = cell / My, j = cell % My through a float reciprocal with correction
-// (exact for cell < 2^24)
-__device__ __forceinline__ void cell_jk(int cell, int My, float invMy, int& j, int& k) {
-    int q = (int)((float)cell * invMy);
-    int r = cell - q * My;
-    if (r < 0) { q -= 1; r += My; }
-    else if (r >= My) { q += 1; r -= My; }
-    j = r;
-    k = q;
-}
 
 // Sub-cycled transverse move and deposit of one particle (:1389-1479 with
 // DepositCurrentsInCellSplit :1547-1615 or the CIC of MoveInCell), then the

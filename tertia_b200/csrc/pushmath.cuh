@@ -1,7 +1,7 @@
 // pushmath.cuh — the velocity factor 1 - Vx of the plasma push in the form
 // the fast push kernels use, shared by the push kernels (push.cuh) and the
 // push adjoint's recompute (adjoint.cu), so that the adjoint recomputes
-// exactly the push the forward ran.
+// exactly the push the forward ran; and the cell index helpers both use.
 //
 // The push divides by 1 - Vx (movepart_splitlayer.cpp:1258-1371: the kicks
 // q2m hx/2 E/(1-Vx), the deposits w dJ V/(1-Vx), the transverse move
@@ -42,6 +42,23 @@ __device__ __forceinline__ double one_minus_vx(double px, double py, double pz, 
     const double fwd = (1.0 + pt2) * inv_g / (g + px);
     const double bwd = fma(-px, inv_g, 1.0);
     return px > 0.0 ? fwd : bwd;
+}
+
+// j within one period of [0, M) (a shift of at most one period): no loop
+__device__ __forceinline__ int wrap1(int j, int M) {
+    j += (j < 0) ? M : 0;
+    return j - ((j >= M) ? M : 0);
+}
+
+// k = cell / My, j = cell % My through a float reciprocal with correction
+// (exact for cell < 2^24)
+__device__ __forceinline__ void cell_jk(int cell, int My, float invMy, int& j, int& k) {
+    int q = (int)((float)cell * invMy);
+    int r = cell - q * My;
+    if (r < 0) { q -= 1; r += My; }
+    else if (r >= My) { q += 1; r -= My; }
+    j = r;
+    k = q;
 }
 
 }  // namespace qs

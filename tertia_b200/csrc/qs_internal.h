@@ -236,6 +236,7 @@ struct PushAdjArgs {
     size_t plane;
     T sE, hxhy, hxhz, djx0, djy0, djz0, bxe, bye, bze;
     int full, precise;
+    float invMy;          // 1 / My (cell -> (j, k) without an integer division)
 };
 template <class T>
 int launch_push_adjoint(const PushAdjArgs<T>& a, cudaStream_t st);
