@@ -293,18 +293,22 @@ template <>
 __device__ __forceinline__ float fdiv<float>(float a, float b) { return __fdividef(a, b); }
 
 // The adjoint of particle i: its momentum and position adjoints are stored,
-// the adjoint of the fields it gathered (6 fields x 4 corners of its cell,
-// index f*4 + r) goes to lf, and its cell is returned (-1 when the forward
+// the adjoint of the fields it gathered (6 fields x 4 corners of its cell, as
+// pairs: lf[2f] = corners 0 and 1 of field f, lf[2f + 1] = corners 2 and 3)
+// goes to lf, and its cell is returned (-1, lf unset, when the forward
 // skipped the particle).
 // Offsets into the planes and the per-particle arrays are 32-bit (the
 // adjoint's set-up checks 6 ny nz and 3 n below 2^31), so that an address is
-// one wide multiply-add from its base.  (j, k) of the cell is returned too.
+// one wide multiply-add from its plane's base.  (j, k) of the cell is
+// returned too.
 // The gathered fields' y and z slopes, needed only at the end, wait in
 // shared memory (sg: 12 x blockDim values, this thread's column) instead of
 // 12 registers through the recompute and the backward.
 template <class T>
 __device__ __forceinline__ int push_adjoint_cic_one(const PushAdjArgs<T>& a, uint32_t i,
-                                                    T (&lf)[24], int& jo, int& ko, T* sg) {
+                                                    typename FPair<T>::type (&lf)[12], int& jo,
+                                                    int& ko, T* sg) {
+    using P = FPair<T>;
     const int My = a.My, Mz = a.Mz;
     const int cell = a.cell[i];
     int j, k;
@@ -327,13 +331,14 @@ __device__ __forceinline__ int push_adjoint_cic_one(const PushAdjArgs<T>& a, uin
     T g[6];
     {
         const T wg[4] = {(one - yp) * (one - zp), yp * (one - zp), (one - yp) * zp, yp * zp};
+        const T* Fb = a.F;
 #pragma unroll
-        for (int f = 0; f < 6; f++) {
+        for (int f = 0; f < 6; f++, Fb += plane) {
             T F[4];
             g[f] = T(0);
 #pragma unroll
             for (int r = 0; r < 4; r++) {
-                F[r] = ldg_(a.F + (f * plane + nn[r]));
+                F[r] = ldg_(Fb + nn[r]);
                 g[f] += wg[r] * F[r];
             }
             sg[f * nt + tid] = (one - zp) * (F[1] - F[0]) + zp * (F[3] - F[2]);
@@ -409,7 +414,7 @@ __device__ __forceinline__ int push_adjoint_cic_one(const PushAdjArgs<T>& a, uin
             } else {
                 ps = fdiv(partdx, step);
                 partdx = T(0);
-                dps = T(nfull) / (step * step);
+                dps = fdiv(T(nfull), step * step);
             }
             const T uy = ytmp + dy * ps, uz = ztmp + dz * ps;
             const T fy = floor(uy), fz = floor(uz);
@@ -442,18 +447,22 @@ __device__ __forceinline__ int push_adjoint_cic_one(const PushAdjArgs<T>& a, uin
         const uint32_t nd[4] = {(uint32_t)jb + rb0, (uint32_t)jb1 + rb0, (uint32_t)jb + rb1,
                                 (uint32_t)jb1 + rb1};
         const T wc[4] = {(one - ry) * (one - rz), ry * (one - rz), (one - ry) * rz, ry * rz};
+        T acc[4] = {T(0), T(0), T(0), T(0)};
+        const T* Db = a.lamD;
+#pragma unroll
+        for (int d = 0; d < 3; d++, Db += plane) {
+#pragma unroll
+            for (int r = 0; r < 4; r++) {
+                const T G = ldg_(Db + nd[r]);
+                ldq[d] += ps * wc[r] * G;
+                acc[r] += dq[d] * G;
+            }
+        }
         T lwc[4];
 #pragma unroll
         for (int r = 0; r < 4; r++) {
-            T acc = T(0);
-#pragma unroll
-            for (int d = 0; d < 3; d++) {
-                const T G = ldg_(a.lamD + (d * plane + nd[r]));
-                ldq[d] += ps * wc[r] * G;
-                acc += dq[d] * G;
-            }
-            lwc[r] = ps * acc;
-            lps += wc[r] * acc;
+            lwc[r] = ps * acc[r];
+            lps += wc[r] * acc[r];
         }
         const T lry = lyc + (one - rz) * (lwc[1] - lwc[0]) + rz * (lwc[3] - lwc[2]);
         const T lrz = lzc + (one - ry) * (lwc[2] - lwc[0]) + ry * (lwc[3] - lwc[1]);
@@ -553,13 +562,15 @@ __device__ __forceinline__ int push_adjoint_cic_one(const PushAdjArgs<T>& a, uin
     }
     // ---- backward through the gather g_f = sum_r wg_r F_f,r
     const T bg[6] = {bE[0], bE[1], bE[2], bB[0], bB[1], bB[2]};
-    const T wg[4] = {(one - yp) * (one - zp), yp * (one - zp), (one - yp) * zp, yp * zp};
+    const auto w01 = P::make((one - yp) * (one - zp), yp * (one - zp));
+    const auto w23 = P::make((one - yp) * zp, yp * zp);
 #pragma unroll
     for (int f = 0; f < 6; f++) {
         lyp += bg[f] * sg[f * nt + tid];
         lzp += bg[f] * sg[(6 + f) * nt + tid];
-#pragma unroll
-        for (int r = 0; r < 4; r++) lf[f * 4 + r] = half * wg[r] * bg[f];
+        const T hb = half * bg[f];
+        lf[2 * f] = P::mul(hb, w01);
+        lf[2 * f + 1] = P::mul(hb, w23);
     }
     if (a.full) {
         a.lamPm[i] = bp[0];
@@ -579,8 +590,10 @@ __device__ __forceinline__ int push_adjoint_cic_one(const PushAdjArgs<T>& a, uin
 
 // Sums of v over runs of lanes with equal key (the particles of a warp are
 // grouped by cell): the first lane of each run gets its run's sum and true.
-template <int NV, class T>
-__device__ __forceinline__ bool warp_run_sums(T (&v)[NV], int key) {
+// The values are pairs (two shuffles, one packed add in FP32).
+template <int NV, class V>
+__device__ __forceinline__ bool warp_run_sums(V (&v)[NV], int key) {
+    using P = FPair<decltype(v[0].x)>;
     const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const int prevKey = __shfl_up_sync(full, key, 1);
@@ -595,8 +608,10 @@ __device__ __forceinline__ bool warp_run_sums(T (&v)[NV], int key) {
             const bool take = lane + d <= re && ((lane - rs) & (2 * d - 1)) == 0;
 #pragma unroll
             for (int q = 0; q < NV; q++) {
-                const T o = __shfl_down_sync(full, v[q], d);
-                if (take) v[q] += o;
+                V o;
+                o.x = __shfl_down_sync(full, v[q].x, d);
+                o.y = __shfl_down_sync(full, v[q].y, d);
+                if (take) v[q] = P::add(v[q], o);
             }
         }
     }
@@ -612,24 +627,30 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 1)
     __shared__ T sg[12 * 256];
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     pdl_wait();
-    T lf[24];
-#pragma unroll
-    for (int q = 0; q < 24; q++) lf[q] = T(0);
+    typename FPair<T>::type lf[12];
     int j = 0, k = 0;
     const int cell = i < (uint32_t)a.n ? push_adjoint_cic_one(a, i, lf, j, k, sg) : -1;
+    if (cell < 0) {
+#pragma unroll
+        for (int q = 0; q < 12; q++) lf[q] = FPair<T>::make(T(0), T(0));
+    }
     // the field adjoints of a cell's particles summed in the warp, then one
     // atomic per field and corner
-    if (warp_run_sums<24>(lf, cell)) {
+    if (warp_run_sums<12>(lf, cell)) {
         const int My = a.My, Mz = a.Mz;
         const uint32_t plane = (uint32_t)a.plane;
         const int j1 = wrap1(j + 1, My), k1 = wrap1(k + 1, Mz);
         const uint32_t row0 = (uint32_t)My * (uint32_t)k, row1 = (uint32_t)My * (uint32_t)k1;
         const uint32_t nn[4] = {(uint32_t)j + row0, (uint32_t)j1 + row0, (uint32_t)j + row1,
                                 (uint32_t)j1 + row1};
+        T* Lb = a.lamFC;
 #pragma unroll
-        for (int f = 0; f < 6; f++)
-#pragma unroll
-            for (int r = 0; r < 4; r++) atomicAdd(a.lamFC + (f * plane + nn[r]), lf[f * 4 + r]);
+        for (int f = 0; f < 6; f++, Lb += plane) {
+            atomicAdd(Lb + nn[0], lf[2 * f].x);
+            atomicAdd(Lb + nn[1], lf[2 * f].y);
+            atomicAdd(Lb + nn[2], lf[2 * f + 1].x);
+            atomicAdd(Lb + nn[3], lf[2 * f + 1].y);
+        }
     }
 }
 

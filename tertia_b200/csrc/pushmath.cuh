@@ -1,7 +1,8 @@
 // pushmath.cuh — the velocity factor 1 - Vx of the plasma push in the form
 // the fast push kernels use, shared by the push kernels (push.cuh) and the
 // push adjoint's recompute (adjoint.cu), so that the adjoint recomputes
-// exactly the push the forward ran; and the cell index helpers both use.
+// exactly the push the forward ran; and the cell index helpers and value
+// pairs both use.
 //
 // The push divides by 1 - Vx (movepart_splitlayer.cpp:1258-1371: the kicks
 // q2m hx/2 E/(1-Vx), the deposits w dJ V/(1-Vx), the transverse move
@@ -60,5 +61,39 @@ __device__ __forceinline__ void cell_jk(int cell, int My, float invMy, int& j, i
     j = r;
     k = q;
 }
+
+// Value pairs: the field pairs of the grouped push's tile, (Ex, Ey), (Ez,
+// Bx), (By, Bz), and the push adjoint's field-adjoint pairs.  In FP32 the
+// packed instructions of sm_100 (__ffma2_rn and friends: two FP32 lanes,
+// each rounded as fmaf, so the sums are those of the scalar chain), in FP64
+// two FMAs.
+template <class T>
+struct FPair;
+template <>
+struct FPair<float> {
+    using type = float2;
+    static __device__ __forceinline__ float2 make(float x, float y) { return make_float2(x, y); }
+    static __device__ __forceinline__ float2 add(float2 a, float2 b) { return __fadd2_rn(a, b); }
+    static __device__ __forceinline__ float2 mul(float s, float2 v) {
+        return __fmul2_rn(make_float2(s, s), v);
+    }
+    static __device__ __forceinline__ float2 fma(float s, float2 v, float2 c) {
+        return __ffma2_rn(make_float2(s, s), v, c);
+    }
+};
+template <>
+struct FPair<double> {
+    using type = double2;
+    static __device__ __forceinline__ double2 make(double x, double y) { return make_double2(x, y); }
+    static __device__ __forceinline__ double2 add(double2 a, double2 b) {
+        return make_double2(a.x + b.x, a.y + b.y);
+    }
+    static __device__ __forceinline__ double2 mul(double s, double2 v) {
+        return make_double2(s * v.x, s * v.y);
+    }
+    static __device__ __forceinline__ double2 fma(double s, double2 v, double2 c) {
+        return make_double2(::fma(s, v.x, c.x), ::fma(s, v.y, c.y));
+    }
+};
 
 }  // namespace qs
