@@ -251,10 +251,11 @@ def adjoint_measure(precision: str):
     e1.record(stream)
     torch.cuda.synchronize()
     fwd_ms = e0.elapsed_time(e1)
-    t0 = time.perf_counter()
+    e0.record(stream)
     dw = m.adjoint(coeff)
+    e1.record(stream)
     torch.cuda.synchronize()
-    adj_ms = (time.perf_counter() - t0) * 1e3
+    adj_ms = e0.elapsed_time(e1)
     g = np.bincount(bins, weights=np.asarray(beam["w"]) * dw, minlength=nbins)
     lo = int(np.nonzero(coeff)[0].min())
     swept = cfg.nx - lo
@@ -297,8 +298,8 @@ def adjoint_measure(precision: str):
             "fd_note": "central differences of the loss; in BF16x3 they carry the FP32 rounding "
                        "of the loss divided by 2h, hence the FP64 differences as reference",
             "fd_step": h, "loss_note": "loss = sum over window layers of hx * on-axis Ex",
-            "timing": "forward: device events around the march; adjoint: host wall clock "
-                      "around qs_adjoint (it synchronises)"}
+            "timing": "device events on the handle's stream around the march and around "
+                      "qs_adjoint"}
 
 
 def adjoint_grid_measure(workload="c1", precision="fp32", every=32, nbins=64):
@@ -307,7 +308,7 @@ def adjoint_grid_measure(workload="c1", precision="fp32", every=32, nbins=64):
     loss, bins and checkpoint interval: the driver's charge profile as
     `nbins` xi-bins, loss = on-axis Ex integrated over xi in [-6, -5] behind
     the driver centre, beam deposited in place.  Timing only: the march
-    (device events) and qs_adjoint (host clock; it synchronises), the third
+    and qs_adjoint (device events on the handle's stream), the third
     of three runs."""
     import numpy as np
     import torch
@@ -344,18 +345,19 @@ def adjoint_grid_measure(workload="c1", precision="fp32", every=32, nbins=64):
             e1.record(st)
             torch.cuda.synchronize()
             fwd = e0.elapsed_time(e1)
-            t0 = time.perf_counter()
+            e0.record(st)
             m.adjoint(coeff)
+            e1.record(st)
             torch.cuda.synchronize()
-            adj = (time.perf_counter() - t0) * 1e3
+            adj = e0.elapsed_time(e1)
     lo = int(np.nonzero(coeff)[0].min())
     swept = cfg.nx - lo
     return {"workload": f"{w.name} grid: {cfg.ny}x{cfg.nz}x{cfg.nx} CIC {precision}, the c3 "
                         f"adjoint's loss and {nbins} xi-bins, checkpoints every {every} layers",
             "forward_ms": fwd, "adjoint_ms": adj, "layers_swept": swept, "layers": cfg.nx,
             "adjoint_over_forward_same_layers": adj / (fwd * swept / cfg.nx),
-            "timing": "forward: device events around the checkpointed march; adjoint: host "
-                      "wall clock around qs_adjoint (it synchronises); third of three runs"}
+            "timing": "device events on the handle's stream around the checkpointed march and "
+                      "around qs_adjoint; third of three runs"}
 
 
 # ------------------------------------------------------------------ FP64 comparison

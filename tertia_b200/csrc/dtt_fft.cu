@@ -747,8 +747,11 @@ __device__ __forceinline__ void spectral_rows_body(SpecArgs<typename Cx<C>::Real
                            : (CORRECT ? trace::K_MAP_CORR : trace::K_MAP_PRED));
 }
 
+// On the 1024-wide FP32 grid (M = 512): 512 threads at most 64 registers, two
+// CTAs per SM (their shared memory, 84 KB each, fits twice).
 template <int M, bool CORRECT, bool PRED_NEXT, class C = float2>
-__global__ void __launch_bounds__(spec_threads<M, C>())
+__global__ void __launch_bounds__(spec_threads<M, C>(),
+                                  (M == 512 && sizeof(C) == sizeof(float2)) ? 2 : 1)
     spectral_rows_kernel(SpecArgs<typename Cx<C>::Real> a, SpecRowArgsT<typename Cx<C>::Real> r,
                          SpecArgs<typename Cx<C>::Real> an) {
     spectral_rows_body<M, CORRECT, PRED_NEXT, C>(a, r, an);
@@ -907,9 +910,11 @@ __device__ __forceinline__ void adjoint_rows_body(AdjSpecArgs<float> a, AdjRowAr
     }
 }
 
+// On the 1024-wide grid (M = 512): 512 threads at most 64 registers, two CTAs
+// per SM (their shared memory, 80 KB each, fits twice).
 template <int M, bool CORRECT>
-__global__ void __launch_bounds__(adj_threads<M>()) adjoint_rows_kernel(AdjSpecArgs<float> a,
-                                                                       AdjRowArgs r) {
+__global__ void __launch_bounds__(adj_threads<M>(), M == 512 ? 2 : 1)
+    adjoint_rows_kernel(AdjSpecArgs<float> a, AdjRowArgs r) {
     adjoint_rows_body<M, CORRECT>(a, r);
 }
 
