@@ -79,9 +79,11 @@ class ClockSampler:
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, device: int):
+    def __init__(self, device: int, interval_ms: int = 100):
         self.device = device
+        self.interval_ms = interval_ms
         self.rows = []
+        self.first = 0
         self.proc = None
         self.thread = None
 
@@ -89,7 +91,7 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
-                 "-lms", "200", "-i", str(self.device)],
+                 "-lms", str(self.interval_ms), "-i", str(self.device)],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except Exception:
             self.proc = None
@@ -101,6 +103,15 @@ class ClockSampler:
                     self.rows.append(parts)
         self.thread = threading.Thread(target=reader, daemon=True)
         self.thread.start()
+        # nvidia-smi takes a moment to print its first row: wait for it (at
+        # most 5 s), so that the samples cover the whole timed region.
+        t_end = time.monotonic() + 5.0
+        while not self.rows and self.proc.poll() is None and time.monotonic() < t_end:
+            time.sleep(0.01)
+
+    def mark(self):
+        """Start of the timed region: stop() summarises the rows from here on."""
+        self.first = len(self.rows)
 
     def stop(self):
         if self.proc:
@@ -113,7 +124,8 @@ class ClockSampler:
             self.thread.join(timeout=2)
         sm, mx, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for r in self.rows:
+        rows = self.rows[self.first:] or self.rows[-1:]
+        for r in rows:
             try:
                 sm.append(float(r[1]))
                 mx = float(r[2])
@@ -840,6 +852,7 @@ def run_ours(args):
     l0 = m.kernel_launches()
     barrier()
     torch.cuda.synchronize()
+    clocks.mark()
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
     ev0.record(stream)
